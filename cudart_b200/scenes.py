@@ -1,0 +1,124 @@
+"""Seeded synthetic scenes and cameras for the LBVH build / closest-hit workloads.
+
+The reference ships no data sets; its meshes come from an external model
+library. These generators produce the host-side inputs that both the CUDA path
+and the CPU oracle consume: float32 vertices as float4 (w = 0, the layout of
+``CUDAMesh`` vertices, CUDAMesh.h) and uint32 faces as uint4 (a, b, c,
+material), the layout of ``CUDAMesh`` faces. All randomness comes from numpy's
+PCG64 generator seeded explicitly, so a (generator, seed) pair always yields
+the same bytes on any host.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class Mesh:
+    vertices: np.ndarray  # (V, 4) float32, w = 0
+    faces: np.ndarray  # (N, 4) uint32, (a, b, c, material)
+
+    @property
+    def face_count(self) -> int:
+        return int(self.faces.shape[0])
+
+    @property
+    def vertex_count(self) -> int:
+        return int(self.vertices.shape[0])
+
+    def hitbox(self) -> np.ndarray:
+        """min/max over every vertex, float4 each (CUDAModel grows its box per vertex)."""
+        v = self.vertices
+        return np.concatenate([v.min(axis=0), v.max(axis=0)]).astype(np.float32)
+
+
+@dataclass
+class Camera:
+    center: tuple  # (x, y, z)
+    target: tuple  # lookAt point
+    fov: float  # radians, vertical (CUDA_calcPrimaryRays uses tan(fov/2) for up)
+    width: int
+    height: int
+
+    @property
+    def ratio(self) -> float:
+        return float(np.float32(self.width) / np.float32(self.height))
+
+
+def terrain(grid: int = 128, seed: int = 0, amplitude: float = 0.1, offset=(0.0, 0.0, 0.0), scale=(1.0, 1.0)) -> Mesh:
+    """Height field on a grid x grid vertex lattice over x, z in [-1, 1].
+
+    y = amplitude * sum_{k<4} sin(f_k * (cos(theta_k) x + sin(theta_k) z) + phi_k) with
+    f_k ~ U[1, 8], phi_k ~ U[0, 2 pi), theta_k ~ U[0, 2 pi). Two triangles per
+    cell: 2 (grid - 1)^2 faces (32,258 for grid = 128).
+    """
+    rng = np.random.default_rng(seed)
+    f = rng.uniform(1.0, 8.0, 4)
+    phi = rng.uniform(0.0, 2.0 * math.pi, 4)
+    theta = rng.uniform(0.0, 2.0 * math.pi, 4)
+    xs = np.linspace(-1.0, 1.0, grid)
+    X, Z = np.meshgrid(xs, xs)  # rows: z, columns: x
+    Y = np.zeros_like(X)
+    for k in range(4):
+        Y += np.sin(f[k] * (math.cos(theta[k]) * X + math.sin(theta[k]) * Z) + phi[k])
+    Y *= amplitude
+    verts = np.zeros((grid * grid, 4), dtype=np.float32)
+    verts[:, 0] = (X.ravel() * scale[0] + offset[0]).astype(np.float32)
+    verts[:, 1] = (Y.ravel() + offset[1]).astype(np.float32)
+    verts[:, 2] = (Z.ravel() * scale[1] + offset[2]).astype(np.float32)
+    i, j = np.meshgrid(np.arange(grid - 1), np.arange(grid - 1), indexing="ij")
+    v00 = (i * grid + j).ravel()
+    v01 = v00 + 1
+    v10 = v00 + grid
+    v11 = v10 + 1
+    faces = np.zeros((2 * v00.size, 4), dtype=np.uint32)
+    faces[0::2, 0], faces[0::2, 1], faces[0::2, 2] = v00, v10, v01
+    faces[1::2, 0], faces[1::2, 1], faces[1::2, 2] = v01, v10, v11
+    return Mesh(verts, faces)
+
+
+def soup(n: int, seed: int = 1, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), sigma: float = 0.01) -> Mesh:
+    """Triangle soup: centroids uniform in the box [lo, hi], each vertex = centroid + N(0, sigma^2) per axis."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(lo, hi, (n, 3))
+    v = c[:, None, :] + rng.normal(0.0, sigma, (n, 3, 3))
+    verts = np.zeros((3 * n, 4), dtype=np.float32)
+    verts[:, :3] = v.reshape(3 * n, 3).astype(np.float32)
+    faces = np.zeros((n, 4), dtype=np.uint32)
+    faces[:, 0] = np.arange(0, 3 * n, 3, dtype=np.uint32)
+    faces[:, 1] = faces[:, 0] + 1
+    faces[:, 2] = faces[:, 0] + 2
+    return Mesh(verts, faces)
+
+
+def concat(*meshes: Mesh) -> Mesh:
+    verts, faces, base = [], [], 0
+    for m in meshes:
+        verts.append(m.vertices)
+        f = m.faces.copy()
+        f[:, :3] += np.uint32(base)
+        faces.append(f)
+        base += m.vertex_count
+    return Mesh(np.concatenate(verts), np.concatenate(faces))
+
+
+# ----------------------------------------------------------------------------
+# Workloads
+# ----------------------------------------------------------------------------
+FOV_60 = float(np.float32(math.pi / 3.0))
+
+
+def terrain_small_scene(width: int = 512, height: int = 512, seed: int = 0):
+    """Height-field terrain, 128 x 128 vertices (32,258 triangles); 512 x 512
+    pinhole rays, 60 degree field of view, camera (0, 1.5, -2.5) looking at the origin."""
+    return terrain(128, seed), Camera((0.0, 1.5, -2.5), (0.0, 0.0, 0.0), FOV_60, width, height)
+
+
+def soup_1m_scene(width: int = 1920, height: int = 1080, seed: int = 1, n: int = 1 << 20):
+    """Incoherent single scene: 2^20-triangle soup in the unit cube (vertex noise
+    sigma 0.01); 1920 x 1080 primary rays from (0.5, 0.5, -0.4) looking at the
+    cube's centre, so that the cube fills the frame, plus one diffuse bounce per hit."""
+    return soup(n, seed), Camera((0.5, 0.5, -0.4), (0.5, 0.5, 0.5), FOV_60, width, height)
