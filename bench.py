@@ -1,0 +1,404 @@
+"""Benchmark: LBVH build + closest-hit traversal on the incoherent 1M-triangle scene.
+
+Workload (one "step"): a 2^20-triangle soup in the unit cube (vertex noise
+sigma 0.01), LBVH build (tree depth 12, complete), 1920 x 1080 primary rays,
+closest-hit trace, one cosine-weighted diffuse bounce per hit, closest-hit trace
+of the bounces. Build and trace are timed separately with CUDA events on the
+launching stream; `value` is closest-hit Mrays/s over both trace passes
+(primary + active bounce rays), `build` carries LBVH Mtri/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank runs its own replica of the
+workload (weak scaling); the time is the max over ranks.
+`--impl reference` times the reference algorithm's CPU implementation (the
+oracle restatement; the reference's own GPU code cannot be built with CUDA 12)
+on the host cores, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "closest-hit Mrays/s (plain vs NN-proposal, bit-exact) and LBVH build Mtri/s"
+WORKLOAD = "soup 2^20 triangles, 1920x1080 primary rays + 1 diffuse bounce per hit"
+SEED_MESH = 1
+SEED_BOUNCE = 1234
+L2_FLUSH_BYTES = 512 << 20  # > 126 MB L2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--faces", type=int, default=1 << 20)
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of the trace kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "trace_soup1m_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from cudart_b200 import _abi, core, scenes
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if not core.device_check():
+        raise RuntimeError("no CUDA device: the CUDA path has no CPU fallback")
+    mesh, cam = scenes.soup_1m_scene(n=args.faces, seed=SEED_MESH)
+    N = mesh.face_count
+    W, H = cam.width, cam.height
+    R = W * H
+    v = torch.from_numpy(mesh.vertices).to(dev)
+    f = torch.from_numpy(mesh.faces.view(np.int32)).to(dev)
+    camera = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
+    stream = torch.cuda.current_stream()
+
+    tree = core.build_lbvh(v, f)
+    rays = core.primary_rays(camera, W, H)
+    hits1 = core.trace(tree, rays[0], rays[1])
+    bounce = core.bounce_rays(tree.tris, rays[0], rays[1], hits1["id"], hits1["t"], SEED_BOUNCE)
+    hits2 = core.trace(tree, bounce[0], bounce[1], tmax=bounce[2])
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def step(ev):
+        ev[0].record(stream)
+        core.build_lbvh(v, f, out=tree)
+        ev[1].record(stream)
+        core.primary_rays(camera, W, H, out=rays)
+        ev[2].record(stream)
+        core.trace(tree, rays[0], rays[1], out=hits1)
+        ev[3].record(stream)
+        core.bounce_rays(tree.tris, rays[0], rays[1], hits1["id"], hits1["t"], SEED_BOUNCE, out=bounce)
+        ev[4].record(stream)
+        core.trace(tree, bounce[0], bounce[1], tmax=bounce[2], out=hits2)
+        ev[5].record(stream)
+
+    def new_events():
+        return [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step(new_events())
+    torch.cuda.synchronize()
+    info = tree.info_host()
+    n_primary_hits = int((hits1["id"] >= 0).sum().item())
+    n_active_bounce = int((bounce[2] > 0).sum().item())
+    rays_per_step = R + n_active_bounce
+
+    # counted pass (untimed): per-ray node visits and triangle tests of both trace launches
+    cnt1 = core.trace(tree, rays[0], rays[1], counters=True)
+    cnt2 = core.trace(tree, bounce[0], bounce[1], tmax=bounce[2], counters=True)
+    torch.cuda.synchronize()
+    vis = int(cnt1["visits"].sum().item()) + int(cnt2["visits"].sum().item())
+    tst = int(cnt1["tests"].sum().item()) + int(cnt2["tests"].sum().item())
+    same = torch.equal(cnt1["id"], hits1["id"]) and torch.equal(cnt2["id"], hits2["id"])
+    trace_bytes = 48 * (R + R) + 32 * vis + 48 * tst  # 32 B ray in + 16 B hit out per ray slot, nodes, triangles
+
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = _abi.lib().rt_launch_count()
+    evs = []
+    with ClockSampler(local_rank) as clk:
+        t_wall = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (outside the event brackets)
+            ev = new_events()
+            step(ev)
+            evs.append(ev)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall
+    launches = _abi.lib().rt_launch_count() - launches0
+    build_ms = sum(e[0].elapsed_time(e[1]) for e in evs)
+    trace1_ms = sum(e[2].elapsed_time(e[3]) for e in evs)
+    trace2_ms = sum(e[4].elapsed_time(e[5]) for e in evs)
+    step_ms = sum(e[0].elapsed_time(e[5]) for e in evs)
+    trace_ms = trace1_ms + trace2_ms
+    times = torch.tensor([build_ms, trace_ms, step_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    build_ms, trace_ms, step_ms = times.tolist()
+    K = args.steps
+    value = world * rays_per_step * K / (trace_ms * 1e-3) / 1e6
+    build_mtri = world * N * K / (build_ms * 1e-3) / 1e6
+    peak, peak_kind = load_peaks()
+    achieved = trace_bytes * K / (trace_ms * 1e-3) / 1e9 / world * world  # per GPU, all trace launches
+    traffic = load_traffic()
+
+    result = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": "Mrays/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": args.warmup,
+        "ms_per_step": round(step_ms / K, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded numpy PCG64 soup; PCG32 bounce directions)",
+        "config": {"workload": WORKLOAD, "faces": N, "primary_rays": R, "bounce_rays_active": n_active_bounce,
+                   "rays_per_step": rays_per_step, "tree_depth": 12, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between steps (512 MB write)"},
+        "build": {"value": round(build_mtri, 3), "unit": "Mtri/s", "ms": round(build_ms / K, 4), "node_count": info["node_count"],
+                  "leaf_count": info["leaf_count"], "real_depth": info["real_depth"]},
+        "trace": {"ms": round(trace_ms / K, 4), "primary_ms": round(trace1_ms / K, 4), "bounce_ms": round(trace2_ms / K, 4),
+                  "primary_hits": n_primary_hits, "mean_visits": round(vis / (2 * R), 3), "mean_tests": round(tst / (2 * R), 3),
+                  "counted_run_identical": bool(same)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": None if traffic is None else traffic.get("bytes_per_step"),
+                     "kernel": "k_trace (primary + bounce launches)",
+                     "algorithmic_bytes_per_step": trace_bytes},
+        "gpu_launches": int(launches),
+        "wall_s_timed": round(t_wall, 3),
+    }
+    clocks = clk.summary()
+    result["clocks"] = {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]}
+    if not args.no_e2e:
+        result["e2e"] = run_e2e(args, mesh, camera, W, H, dev, world)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(mesh, cam, budget_s=12.0)
+    return result
+
+
+def run_e2e(args, mesh, camera, W, H, dev, world):
+    """Same metric through the public API with host buffers: pinned host mesh ->
+    device, build, rays, trace, bounce, trace, hits -> pinned host, every step."""
+    import torch
+
+    from cudart_b200 import core
+
+    vh = torch.from_numpy(mesh.vertices).pin_memory()
+    fh = torch.from_numpy(mesh.faces.view(np.int32)).pin_memory()
+    R = W * H
+    v = torch.empty_like(vh, device=dev)
+    f = torch.empty_like(fh, device=dev)
+    out_id = torch.empty((2, R), dtype=torch.int32).pin_memory()
+    out_t = torch.empty((2, R), dtype=torch.float32).pin_memory()
+    out_uv = torch.empty((2, R, 2), dtype=torch.float32).pin_memory()
+    v.copy_(vh, non_blocking=True)
+    f.copy_(fh, non_blocking=True)
+    tree = core.build_lbvh(v, f)
+    rays = core.primary_rays(camera, W, H)
+    h1 = core.trace(tree, rays[0], rays[1])
+    b = core.bounce_rays(tree.tris, rays[0], rays[1], h1["id"], h1["t"], SEED_BOUNCE)
+    h2 = core.trace(tree, b[0], b[1], tmax=b[2])
+    stream = torch.cuda.current_stream()
+
+    def step():
+        v.copy_(vh, non_blocking=True)
+        f.copy_(fh, non_blocking=True)
+        core.build_lbvh(v, f, out=tree)
+        core.primary_rays(camera, W, H, out=rays)
+        core.trace(tree, rays[0], rays[1], out=h1)
+        core.bounce_rays(tree.tris, rays[0], rays[1], h1["id"], h1["t"], SEED_BOUNCE, out=b)
+        core.trace(tree, b[0], b[1], tmax=b[2], out=h2)
+        for i, h in enumerate((h1, h2)):
+            out_id[i].copy_(h["id"], non_blocking=True)
+            out_t[i].copy_(h["t"], non_blocking=True)
+            out_uv[i].copy_(h["uv"], non_blocking=True)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    active = int((b[2] > 0).sum().item())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = t.item()
+    rays_per_step = R + active
+    h2d = vh.numel() * 4 + fh.numel() * 4
+    d2h = out_id.numel() * 4 + out_t.numel() * 4 + out_uv.numel() * 4
+    return {"value": round(world * rays_per_step * args.steps / (ms * 1e-3) / 1e6, 3), "unit": "Mrays/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": round(ms / args.steps, 4)}
+
+
+# ----------------------------------------------------------------------------
+# CPU baseline / reference arm: the oracle (the reference algorithm restated in
+# C++, checked against the reference's own code) on the host cores
+# ----------------------------------------------------------------------------
+def cpu_baseline(mesh, cam, budget_s=12.0, threads=0):
+    from oracle import api as O
+
+    t0 = time.perf_counter()
+    ref = O.lbvh_build(mesh.vertices, mesh.faces)
+    t_build = time.perf_counter() - t0
+    o, d, _, _ = O.primary_rays(cam)
+    R = len(o)
+    # bounded sample of rays: grow until ~budget seconds of trace work
+    n = 20000
+    t_trace = 0.0
+    traced = 0
+    while True:
+        sl = slice(0, min(n, R))
+        oo, dd = np.ascontiguousarray(o[sl]), np.ascontiguousarray(d[sl])
+        t0 = time.perf_counter()
+        e = O.trace(ref["nodes"], ref["tris"], ref["indices"], oo, dd, threads=threads)
+        t1 = time.perf_counter() - t0
+        bo, bd, bt = O.bounce_rays(ref["tris"], oo, dd, e["id"], e["t"], SEED_BOUNCE)
+        t0 = time.perf_counter()
+        O.trace(ref["nodes"], ref["tris"], ref["indices"], bo, bd, bt, threads=threads)
+        t2 = time.perf_counter() - t0
+        t_trace, traced = t1 + t2, len(oo) + int((bt > 0).sum())
+        if t_trace > budget_s / 4 or n >= R:
+            break
+        n = min(R, int(n * max(2.0, (budget_s / 4) / max(t_trace, 1e-3))))
+    cores = threads if threads > 0 else O.max_threads()
+    return {"value": round(traced / t_trace / 1e6, 4), "unit": "Mrays/s", "cores": cores, "kind": "port",
+            "sample": f"build of all {mesh.face_count} faces ({mesh.face_count / t_build / 1e6:.3f} Mtri/s, 1 thread topology); "
+                      f"trace of the first {len(oo)} primary rays + their bounces ({traced} rays)",
+            "build_mtri_s": round(mesh.face_count / t_build / 1e6, 4)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from cudart_b200 import scenes
+    from oracle import api as O
+
+    mesh, cam = scenes.soup_1m_scene(n=args.faces, seed=SEED_MESH)
+    O.lbvh_build(mesh.vertices[:3 * 4096], mesh.faces[:4096])  # load / warm the library
+    vals, builds = [], []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(mesh, cam, budget_s=8.0)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+            builds.append(cb["build_mtri_s"])
+    value = statistics.median(vals)
+    return {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded numpy PCG64 soup; PCG32 bounce directions)",
+        "config": {"workload": WORKLOAD, "faces": mesh.face_count, "primary_rays": cam.width * cam.height, "tree_depth": 12,
+                   "parallelism": "host cores (OpenMP)"},
+        "impl": "reference",
+        "build": {"value": statistics.median(builds), "unit": "Mtri/s"},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": O.max_threads(), "kind": "port",
+                         "sample": cb["sample"]},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's GPU kernels use texture references and string-named symbol copies that CUDA 12 removed; "
+                "its algorithm runs here as the oracle port (checked bit-exact against the reference's own code)",
+    }
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

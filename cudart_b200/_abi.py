@@ -1,0 +1,98 @@
+"""ctypes declarations of the C ABI in include/rt_core.h (librt_core.so).
+
+Loading fails loudly when the shared library is missing: there is no CPU
+fallback for any compute entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librt_core.so")
+
+RT_OK = 0
+STATUS_NAMES = {0: "RT_OK", 1: "RT_ERR_INVALID_ARGUMENT", 2: "RT_ERR_NO_DEVICE", 3: "RT_ERR_CUDA",
+                4: "RT_ERR_SCRATCH_TOO_SMALL", 5: "RT_ERR_CAPACITY", 6: "RT_ERR_UNSUPPORTED"}
+DEVERR_NODE_CAPACITY = 0x1
+DEVERR_STACK_OVERFLOW = 0x2
+DEVERR_MORTON_CAPACITY = 0x4
+
+# every symbol include/rt_core.h declares
+EXPORTS = (
+    "rt_lbvh_scratch_bytes", "rt_lbvh_build", "rt_mesh_boxes", "rt_reorder_faces", "rt_sort_scratch_bytes",
+    "rt_radix_sort_pairs", "rt_radix_sort_keys", "rt_camera_look_at", "rt_camera_basis", "rt_primary_rays",
+    "rt_trace_closest", "rt_bounce_rays", "rt_status_string", "rt_version", "rt_device_check", "rt_launch_count",
+)
+
+_P = C.c_void_p
+_U32 = C.c_uint32
+
+
+class RtError(RuntimeError):
+    def __init__(self, fn, status):
+        super().__init__(f"{fn} failed: {STATUS_NAMES.get(status, status)}")
+        self.status = status
+
+
+class BuildParams(C.Structure):
+    _fields_ = [("tree_depth", _U32), ("tree_complete", _U32), ("min_leaf", _U32), ("max_leaf", _U32), ("morton_bits", _U32)]
+
+
+class BuildInfo(C.Structure):
+    _fields_ = [(k, _U32) for k in ("node_count", "leaf_count", "real_depth", "split_count", "overrun_visits",
+                                     "nondet_reads", "past_end_reads", "error")]
+
+
+class BuildDesc(C.Structure):
+    _fields_ = [("vertices", _P), ("vertex_count", _U32), ("face_count", _U32), ("faces_in", _P), ("faces_out", _P),
+                ("hitbox", _P), ("params", BuildParams), ("boxes", _P), ("indices", _P), ("codes", _P), ("nodes", _P),
+                ("max_nodes", _U32), ("tris", _P), ("info", _P), ("scratch", _P), ("scratch_bytes", C.c_size_t)]
+
+
+class TraceDesc(C.Structure):
+    _fields_ = [("nodes", _P), ("tris", _P), ("vertices", _P), ("faces", _P), ("indices", _P), ("orig", _P), ("dir", _P),
+                ("tmax", _P), ("ray_count", _U32), ("id_mode", _U32), ("hit_id", _P), ("hit_t", _P), ("hit_uv", _P),
+                ("ray_visits", _P), ("ray_tests", _P), ("error_word", _P)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("center", C.c_float * 3), ("angle", C.c_float * 3), ("fov", C.c_float), ("ratio", C.c_float)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C cudart_b200/csrc` (no CPU fallback exists)")
+        L = C.CDLL(LIB_PATH)
+        L.rt_lbvh_scratch_bytes.argtypes = [_U32, C.POINTER(BuildParams), C.POINTER(C.c_size_t), C.POINTER(_U32)]
+        L.rt_lbvh_build.argtypes = [C.POINTER(BuildDesc), _P]
+        L.rt_mesh_boxes.argtypes = [_P, _P, _U32, _P, _P, _P]
+        L.rt_reorder_faces.argtypes = [_P, _P, _U32, _P, _P]
+        L.rt_sort_scratch_bytes.argtypes = [_U32, C.POINTER(C.c_size_t)]
+        L.rt_radix_sort_pairs.argtypes = [_P, _P, _U32, _U32, C.c_int, _P, C.c_size_t, _P]
+        L.rt_radix_sort_keys.argtypes = [_P, _U32, _U32, _P, C.c_size_t, _P]
+        L.rt_camera_look_at.argtypes = [C.POINTER(Camera), C.POINTER(C.c_float)]
+        L.rt_camera_basis.argtypes = [C.POINTER(Camera), _U32, _U32, C.POINTER(C.c_float)]
+        L.rt_primary_rays.argtypes = [C.POINTER(Camera), _U32, _U32, _P, _P, _P]
+        L.rt_trace_closest.argtypes = [C.POINTER(TraceDesc), _P]
+        L.rt_bounce_rays.argtypes = [_P, _P, _P, _P, _P, _U32, C.c_uint64, _P, _P, _P, _P]
+        L.rt_status_string.restype = C.c_char_p
+        L.rt_status_string.argtypes = [C.c_int]
+        L.rt_version.restype = _U32
+        L.rt_device_check.restype = C.c_int
+        L.rt_launch_count.restype = C.c_uint64
+        for name in EXPORTS:
+            if name not in ("rt_status_string", "rt_version", "rt_device_check", "rt_launch_count"):
+                getattr(L, name).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def check(fn: str, status: int):
+    if status != RT_OK:
+        raise RtError(fn, status)

@@ -1,0 +1,263 @@
+"""Python host side over the C ABI, on torch CUDA tensors.
+
+Mirrors the reference's host interface for the path: ``build_lbvh`` is
+CUDAMeshTree::buildMeshTreeLBVH (CUDAMeshTree.cpp:88-91), ``primary_rays`` is
+CUDARaytracer::calcPrimaryRays (CUDARaytracer.cpp:125-128), ``trace`` is
+CUDARaytracer::raytraceMeshTree (CUDARaytracer.cpp:130-135), ``sort_pairs`` /
+``sort_keys`` are CUDA_radixSortGeneral / CUDA_radixSort. torch only supplies
+device memory and streams; every computation runs in librt_core.so. Calls are
+asynchronous on the current torch stream; nothing here synchronizes except
+the explicit ``*_host`` helpers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import torch
+
+from . import _abi
+
+HUGE = 3.402823466e38
+
+
+def _p(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def _stream(stream=None):
+    s = torch.cuda.current_stream() if stream is None else stream
+    return C.c_void_p(s.cuda_stream)
+
+
+def _need_cuda(t, name, dtype=None, cols=None):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if dtype is not None and t.dtype not in dtype:
+        raise ValueError(f"{name} has dtype {t.dtype}, expected one of {dtype}")
+    if cols is not None and (t.dim() != 2 or t.shape[1] != cols):
+        raise ValueError(f"{name} must have shape (*, {cols})")
+
+
+_I32 = (torch.int32, torch.uint32)
+_F32 = (torch.float32,)
+
+
+class _Scratch:
+    """Grow-only scratch buffer per device (the C ABI allocates nothing)."""
+
+    def __init__(self):
+        self.buf = {}
+
+    def get(self, nbytes: int, device) -> torch.Tensor:
+        key = torch.device(device).index or 0
+        b = self.buf.get(key)
+        if b is None or b.numel() < nbytes:
+            b = torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8, device=device)
+            self.buf[key] = b
+        return b
+
+
+_SCRATCH = _Scratch()
+
+
+def device_check() -> bool:
+    return _abi.lib().rt_device_check() == _abi.RT_OK
+
+
+@dataclass
+class Tree:
+    """Device state of a built tree (CUDAMeshTree: nodes, boxes, indices) plus
+    the reordered faces and the pre-gathered triangle stream."""
+
+    nodes: torch.Tensor  # int32 (max_nodes, 8) bvnode words
+    boxes: torch.Tensor  # float32 (N, 8) aabox per original face
+    indices: torch.Tensor  # int32 (N,) position -> original face id
+    codes: torch.Tensor  # int32 (N,) sorted Morton codes (uint32 bits)
+    faces: torch.Tensor  # int32 (N, 4) faces in position order
+    tris: torch.Tensor  # float32 (N, 12) {v0, e1, e2}
+    info: torch.Tensor  # int32 (8,) rt_build_info, on the device
+
+    def info_host(self) -> dict:
+        vals = self.info.cpu().tolist()
+        keys = [f[0] for f in _abi.BuildInfo._fields_]
+        return {k: v & 0xFFFFFFFF for k, v in zip(keys, vals)}
+
+    @property
+    def node_count(self) -> int:
+        return int(self.info[0].item())
+
+    def nodes_host(self):
+        return self.nodes[: self.node_count].cpu()
+
+
+def lbvh_scratch_bytes(face_count: int, tree_depth=12, tree_complete=True, morton_bits=32):
+    params = _abi.BuildParams(tree_depth, int(tree_complete), 0, 0, morton_bits)
+    nb = C.c_size_t(0)
+    mx = C.c_uint32(0)
+    _abi.check("rt_lbvh_scratch_bytes", _abi.lib().rt_lbvh_scratch_bytes(face_count, C.byref(params), C.byref(nb), C.byref(mx)))
+    return nb.value, mx.value
+
+
+def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_depth: int = 12, tree_complete: bool = True,
+               morton_bits: int = 32, out: Tree | None = None, stream=None) -> Tree:
+    """LBVH build of a mesh given as float4 vertices (V, 4) and uint4 faces (N, 4).
+    hitbox: host sequence of 8 floats (min xyzw, max xyzw) or None for the
+    vertices' min/max."""
+    _need_cuda(vertices, "vertices", _F32, 4)
+    _need_cuda(faces, "faces", _I32, 4)
+    n = faces.shape[0]
+    dev = vertices.device
+    nbytes, max_nodes = lbvh_scratch_bytes(n, tree_depth, tree_complete, morton_bits)
+    if out is None:
+        out = Tree(
+            nodes=torch.empty((max_nodes, 8), dtype=torch.int32, device=dev),
+            boxes=torch.empty((n, 8), dtype=torch.float32, device=dev),
+            indices=torch.empty(n, dtype=torch.int32, device=dev),
+            codes=torch.empty(n, dtype=torch.int32, device=dev),
+            faces=torch.empty((n, 4), dtype=torch.int32, device=dev),
+            tris=torch.empty((n, 12), dtype=torch.float32, device=dev),
+            info=torch.zeros(8, dtype=torch.int32, device=dev),
+        )
+    scratch = _SCRATCH.get(nbytes, dev)
+    hb = None
+    if hitbox is not None:
+        hb = (C.c_float * 8)(*[float(x) for x in hitbox])
+    d = _abi.BuildDesc()
+    d.vertices = vertices.data_ptr()
+    d.vertex_count = vertices.shape[0]
+    d.face_count = n
+    d.faces_in = faces.data_ptr()
+    d.faces_out = out.faces.data_ptr()
+    d.hitbox = C.cast(hb, C.c_void_p).value if hb is not None else None
+    d.params = _abi.BuildParams(tree_depth, int(tree_complete), 0, 0, morton_bits)
+    d.boxes = out.boxes.data_ptr()
+    d.indices = out.indices.data_ptr()
+    d.codes = out.codes.data_ptr()
+    d.nodes = out.nodes.data_ptr()
+    d.max_nodes = out.nodes.shape[0]
+    d.tris = out.tris.data_ptr()
+    d.info = out.info.data_ptr()
+    d.scratch = scratch.data_ptr()
+    d.scratch_bytes = scratch.numel()
+    _abi.check("rt_lbvh_build", _abi.lib().rt_lbvh_build(C.byref(d), _stream(stream)))
+    return out
+
+
+def trace(tree: Tree, orig: torch.Tensor, dir: torch.Tensor, tmax: torch.Tensor | None = None, id_mode: int = 0,
+          counters: bool = False, use_tris: bool = True, vertices: torch.Tensor | None = None, out: dict | None = None,
+          ray_count: int | None = None, stream=None) -> dict:
+    """Closest hit per ray. Returns dict(id=int32, t=float32, uv=float32 (R, 2), err=int32 (1,))."""
+    _need_cuda(orig, "orig", _F32, 4)
+    _need_cuda(dir, "dir", _F32, 4)
+    R = orig.shape[0] if ray_count is None else ray_count
+    dev = orig.device
+    if out is None:
+        out = dict(id=torch.empty(R, dtype=torch.int32, device=dev), t=torch.empty(R, dtype=torch.float32, device=dev),
+                   uv=torch.empty((R, 2), dtype=torch.float32, device=dev), err=torch.zeros(1, dtype=torch.int32, device=dev))
+        if counters:
+            out["visits"] = torch.empty(R, dtype=torch.int32, device=dev)
+            out["tests"] = torch.empty(R, dtype=torch.int32, device=dev)
+    d = _abi.TraceDesc()
+    d.nodes = tree.nodes.data_ptr()
+    if use_tris:
+        d.tris = tree.tris.data_ptr()
+    else:
+        if vertices is None:
+            raise ValueError("use_tris=False needs the mesh vertices")
+        d.vertices = vertices.data_ptr()
+        d.faces = tree.faces.data_ptr()
+    d.indices = tree.indices.data_ptr()
+    d.orig = orig.data_ptr()
+    d.dir = dir.data_ptr()
+    d.tmax = tmax.data_ptr() if tmax is not None else None
+    d.ray_count = R
+    d.id_mode = id_mode
+    d.hit_id = out["id"].data_ptr()
+    d.hit_t = out["t"].data_ptr()
+    d.hit_uv = out["uv"].data_ptr()
+    if "visits" in out:
+        d.ray_visits = out["visits"].data_ptr()
+        d.ray_tests = out["tests"].data_ptr()
+    d.error_word = out["err"].data_ptr()
+    _abi.check("rt_trace_closest", _abi.lib().rt_trace_closest(C.byref(d), _stream(stream)))
+    return out
+
+
+def make_camera(center, target=None, angle=None, fov=3.14159265359 * 0.5, ratio=4.0 / 3.0) -> _abi.Camera:
+    """CUDACamera state; with a target, the angles come from CUDACamera::lookAt."""
+    cam = _abi.Camera()
+    cam.center[:] = [float(c) for c in center]
+    # CUDACamera's constructor angles (CUDACamera.cpp:41-43)
+    cam.angle[:] = [float(a) for a in (angle if angle is not None else (3.14159265359 * 0.5, 0.0, 0.0))]
+    cam.fov = fov
+    cam.ratio = ratio
+    if target is not None:
+        tgt = (C.c_float * 3)(*[float(t) for t in target])
+        _abi.check("rt_camera_look_at", _abi.lib().rt_camera_look_at(C.byref(cam), tgt))
+    return cam
+
+
+def camera_basis(cam: _abi.Camera, width: int, height: int):
+    b = (C.c_float * 16)()
+    _abi.check("rt_camera_basis", _abi.lib().rt_camera_basis(C.byref(cam), width, height, b))
+    return list(b)
+
+
+def primary_rays(cam: _abi.Camera, width: int, height: int, out=None, device="cuda", stream=None):
+    R = width * height
+    if out is None:
+        out = (torch.empty((R, 4), dtype=torch.float32, device=device), torch.empty((R, 4), dtype=torch.float32, device=device))
+    _abi.check("rt_primary_rays", _abi.lib().rt_primary_rays(C.byref(cam), width, height, _p(out[0]), _p(out[1]), _stream(stream)))
+    return out
+
+
+def bounce_rays(tris, orig, dir, hit_pos, hit_t, seed: int, out=None, ray_count: int | None = None, stream=None):
+    R = orig.shape[0] if ray_count is None else ray_count
+    dev = orig.device
+    if out is None:
+        out = (torch.empty((R, 4), dtype=torch.float32, device=dev), torch.empty((R, 4), dtype=torch.float32, device=dev),
+               torch.empty(R, dtype=torch.float32, device=dev))
+    _abi.check("rt_bounce_rays", _abi.lib().rt_bounce_rays(_p(tris), _p(orig), _p(dir), _p(hit_pos), _p(hit_t), R, C.c_uint64(seed),
+                                                           _p(out[0]), _p(out[1]), _p(out[2]), _stream(stream)))
+    return out
+
+
+def sort_pairs(keys: torch.Tensor, values: torch.Tensor, bit_depth: int = 32, init_values: bool = False, stream=None):
+    """In place, stable (CUDA_radixSortGeneral)."""
+    _need_cuda(keys, "keys", _I32)
+    _need_cuda(values, "values", _I32)
+    n = keys.numel()
+    nb = C.c_size_t(0)
+    _abi.lib().rt_sort_scratch_bytes(n, C.byref(nb))
+    s = _SCRATCH.get(nb.value, keys.device)
+    _abi.check("rt_radix_sort_pairs", _abi.lib().rt_radix_sort_pairs(_p(keys), _p(values), n, bit_depth, int(init_values), _p(s),
+                                                                     s.numel(), _stream(stream)))
+    return keys, values
+
+
+def sort_keys(keys: torch.Tensor, bit_depth: int = 32, stream=None):
+    """In place (CUDA_radixSort)."""
+    _need_cuda(keys, "keys", _I32)
+    n = keys.numel()
+    nb = C.c_size_t(0)
+    _abi.lib().rt_sort_scratch_bytes(n, C.byref(nb))
+    s = _SCRATCH.get(nb.value, keys.device)
+    _abi.check("rt_radix_sort_keys", _abi.lib().rt_radix_sort_keys(_p(keys), n, bit_depth, _p(s), s.numel(), _stream(stream)))
+    return keys
+
+
+def mesh_boxes(vertices, faces, stream=None):
+    n = faces.shape[0]
+    boxes = torch.empty((n, 8), dtype=torch.float32, device=vertices.device)
+    idx = torch.empty(n, dtype=torch.int32, device=vertices.device)
+    _abi.check("rt_mesh_boxes", _abi.lib().rt_mesh_boxes(_p(vertices), _p(faces), n, _p(boxes), _p(idx), _stream(stream)))
+    return boxes, idx
+
+
+def reorder_faces(faces, indices, stream=None):
+    out = torch.empty_like(faces)
+    _abi.check("rt_reorder_faces", _abi.lib().rt_reorder_faces(_p(faces), _p(indices), faces.shape[0], _p(out), _stream(stream)))
+    return out

@@ -1,0 +1,764 @@
+// rt_build.cu -- LBVH build for sm_100a.
+//
+// Replaces CUDA_buildMeshTreeLBVH (kernels/CUDA_buildMeshTreeLBVH.cu:457-681)
+// and its helpers. The reference runs ~10 launches with a host sync after
+// each, copies the split list to the host, builds the topology with a
+// sequential host recursion (:309-455), copies the nodes back, then runs
+// real_depth full passes for the boxes. Here everything stays on the device,
+// with no host round trip:
+//
+//   k_boxes_morton   per face: box (4-wide min/max of the 3 vertices), index,
+//                    Morton code (reference 11/11/10 layout or 10/10/10)
+//   radix sort       (code, index) pairs, stable (rt_sort.cu)
+//   k_levels         split level of each adjacent code pair (clz of the xor)
+//   radix pass       stable partition of split positions by level, which is
+//                    the per-level ascending split list the recursion walks
+//   k_topo_morton    one CTA: the Morton levels of the tree, level by level,
+//                    with the reference's split-pointer semantics (see below);
+//                    leaf counts, pre-order ranks and node ids
+//   k_leaves         one warp per final leaf: expands median subtrees, writes
+//                    node records, reorders faces, pre-gathers triangles
+//                    {v0, e1, e2}, reduces the leaf box and propagates boxes to
+//                    the root with per-node arrival counters (the second
+//                    arrival merges; nobody waits)
+//
+// Node numbering follows the reference's recursion: the k-th internal node in
+// pre-order gets children 2k+1 and 2k+2. A node's pre-order rank among
+// internal nodes is computed from subtree leaf counts (rank(left) = rank + 1,
+// rank(right) = rank + leaves(left)).
+//
+// Split-pointer semantics (host recursion :360-411): each level L keeps a
+// pointer into the concatenated, level-ordered split list C. A Morton visit of
+// a range [a, b) at level L (b - a >= min_leaf, L < tree_depth) is a leaf when
+// the pointer sits exactly at the start of level L+1's list; otherwise the
+// pointer advances past every entry <= a -- it may run into deeper levels'
+// lists -- and the entry found cuts the range if it is < b. Because visits at a
+// level come in increasing a, the pointer after a visit is "the first index at
+// or after start(L) holding a value > a"; it sticks at start(L+1) exactly when
+// the first visit with a >= last(P_L) finds C[start(L+1)] > a. Both facts make
+// every visit of a level independent once that one visit is known.
+#include "rt_common.cuh"
+
+namespace rt {
+namespace {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr int kTopoThreads = 1024;
+constexpr int kTopoWarps = kTopoThreads / 32;
+
+// ----------------------------------------------------------------------------
+// hit box (when the caller gives none): min/max over all vertices
+// ----------------------------------------------------------------------------
+__global__ void k_set_hitbox(float4* hit, float4 mn, float4 mx) {
+  hit[0] = mn;
+  hit[1] = mx;
+}
+
+__global__ __launch_bounds__(256) void k_hitbox_partial(const float4* __restrict__ v, uint32_t count, float4* __restrict__ partial) {
+  float4 mn = make_float4(kHuge, kHuge, kHuge, kHuge), mx = make_float4(-kHuge, -kHuge, -kHuge, -kHuge);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    float4 p = ldg4(v + i);
+    mn = f4min(mn, p);
+    mx = f4max(mx, p);
+  }
+  __shared__ float4 s_mn[256], s_mx[256];
+  s_mn[threadIdx.x] = mn;
+  s_mx[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      s_mn[threadIdx.x] = f4min(s_mn[threadIdx.x], s_mn[threadIdx.x + o]);
+      s_mx[threadIdx.x] = f4max(s_mx[threadIdx.x], s_mx[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = s_mn[0];
+    partial[2 * blockIdx.x + 1] = s_mx[0];
+  }
+}
+
+__global__ void k_hitbox_final(const float4* __restrict__ partial, uint32_t parts, float4* __restrict__ hit) {
+  if (threadIdx.x != 0) return;
+  float4 mn = make_float4(kHuge, kHuge, kHuge, kHuge), mx = make_float4(-kHuge, -kHuge, -kHuge, -kHuge);
+  for (uint32_t i = 0; i < parts; ++i) {
+    mn = f4min(mn, partial[2 * i]);
+    mx = f4max(mx, partial[2 * i + 1]);
+  }
+  hit[0] = mn;
+  hit[1] = mx;
+}
+
+// ----------------------------------------------------------------------------
+// boxes + Morton + iota
+// ----------------------------------------------------------------------------
+// float -> uint with the saturating round-toward-zero rule of cvt.rzi.u32.f32.
+__device__ __forceinline__ uint32_t f2u_sat(float x) { return __float2uint_rz(x); }
+
+__device__ __forceinline__ uint32_t spread_code(uint32_t qx, uint32_t qy, uint32_t qz, int layout) {
+  uint32_t code = 0;
+  if (layout == 30) {
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+      code |= ((qz >> k) & 1u) << (3 * k + 2);
+      code |= ((qy >> k) & 1u) << (3 * k + 3);
+      code |= ((qx >> k) & 1u) << (3 * k + 4);
+    }
+  } else {
+    // kernels/CUDA_buildMeshTreeLBVH.cu:138-169: bit 3k = y_k, 3k+1 = x_k, 3k+2 = z_k
+#pragma unroll
+    for (int k = 0; k < 11; ++k) {
+      code |= ((qy >> k) & 1u) << (3 * k + 0);
+      code |= ((qx >> k) & 1u) << (3 * k + 1);
+      if (k < 10) code |= ((qz >> k) & 1u) << (3 * k + 2);
+    }
+  }
+  return code;
+}
+
+// kernels/CUDA_calcMeshBoxes.cu:30-58 (boxes, iota) fused with
+// kernels/CUDA_buildMeshTreeLBVH.cu:115-173 (Morton code of the box centre).
+__global__ __launch_bounds__(256) void k_boxes_morton(const float4* __restrict__ verts, const uint4* __restrict__ faces, uint32_t n,
+                                                     const float4* __restrict__ hit, int layout, float4* __restrict__ boxes,
+                                                     uint32_t* __restrict__ codes, uint32_t* __restrict__ idx) {
+  const float4 hmin = codes ? hit[0] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 hmax = codes ? hit[1] : make_float4(1.f, 1.f, 1.f, 1.f);
+  const float lx = hmax.x - hmin.x, ly = hmax.y - hmin.y, lz = hmax.z - hmin.z;
+  const float sx = (layout == 30 ? 1023.0f : 2047.0f) / lx;
+  const float sy = (layout == 30 ? 1023.0f : 2047.0f) / ly;
+  const float sz = 1023.0f / lz;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    uint4 f = ldg4(faces + k);
+    float4 v0 = ldg4(verts + f.x), v1 = ldg4(verts + f.y), v2 = ldg4(verts + f.z);
+    float4 mn = f4min(f4min(v0, v1), v2);
+    float4 mx = f4max(f4max(v0, v1), v2);
+    boxes[2 * (size_t)k] = mn;
+    boxes[2 * (size_t)k + 1] = mx;
+    if (idx) idx[k] = k;
+    if (codes) {
+      float cx = 0.5f * (mn.x + mx.x), cy = 0.5f * (mn.y + mx.y), cz = 0.5f * (mn.z + mx.z);
+      uint32_t qx = f2u_sat((cx - hmin.x) * sx);
+      uint32_t qy = f2u_sat((cy - hmin.y) * sy);
+      uint32_t qz = f2u_sat((cz - hmin.z) * sz);
+      codes[k] = spread_code(qx, qy, qz, layout);
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// split levels: key = clz(code[i] ^ code[i+1]) (32 when equal), value = i + 1
+// (kernels/CUDA_buildMeshTreeLBVH.cu:175-233)
+// ----------------------------------------------------------------------------
+__global__ __launch_bounds__(256) void k_levels(const uint32_t* __restrict__ codes, uint32_t n, uint32_t* __restrict__ lev,
+                                               uint32_t* __restrict__ pos) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i + 1 < n; i += gridDim.x * blockDim.x) {
+    uint32_t d = __ldg(codes + i) ^ __ldg(codes + i + 1);
+    lev[i] = d ? (uint32_t)__clz(d) : 32u;
+    pos[i] = i + 1;
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Morton top tree (one CTA)
+// ----------------------------------------------------------------------------
+struct TopoArgs {
+  const uint32_t* C;         // split positions, level ordered
+  const uint32_t* lev_count; // [33] per-level counts (level 32 = no split)
+  uint32_t n, D, min_leaf, max_leaf, complete;
+  uint32_t cap_m;
+  // BFS arrays
+  uint32_t *ra, *rb, *parent, *info, *child, *leaves, *mleaves, *rank, *lambda, *ord, *id;
+  // Morton leaves in position order
+  uint32_t* ml_lambda;
+  uint4* ml_rec;     // (node id, first, count, depth | median << 31)
+  uint32_t* ml_rank; // pre-order rank (median roots)
+  uint32_t* parent_id; // [max_nodes] parent node id of Morton nodes
+  uint32_t* nodes;     // bvnode words
+  uint32_t max_nodes;
+  uint32_t* hdr;       // [16] header: 0 leaf_count, 1 morton_leaves, 2 node_count, 3 real_depth, 4 split_count,
+                       //             5 overrun, 6 nondet, 7 past_end, 8 error
+};
+
+// Leaves of the median subtree of a range of s faces entered from a leaf
+// (s > max_leaf): recursive floor/ceil halving, a node of fewer than max_leaf
+// faces is a leaf (kernels/CUDA_buildMeshTreeLBVH.cu:314-339). The sizes at
+// depth j are floor(s/2^j) and floor(s/2^j)+1, the latter s mod 2^j times.
+__device__ __forceinline__ uint32_t median_leaves(uint32_t s, uint32_t maxl) {
+  if (s < maxl) return 1u;
+  uint32_t j0 = 0;
+  while ((s >> j0) >= maxl) ++j0;
+  uint32_t q0 = s >> j0;
+  uint32_t r = s & ((1u << j0) - 1u);
+  return (1u << j0) + ((q0 + 1u == maxl) ? r : 0u);
+}
+__device__ __forceinline__ uint32_t median_depth(uint32_t s, uint32_t maxl) {
+  if (s < maxl) return 0u;
+  uint32_t j0 = 0;
+  while ((s >> j0) >= maxl) ++j0;
+  uint32_t q0 = s >> j0;
+  uint32_t r = s & ((1u << j0) - 1u);
+  return j0 + ((q0 + 1u == maxl && r) ? 1u : 0u);
+}
+
+template <int NT>
+__device__ __forceinline__ uint32_t block_excl_scan_nt(uint32_t v, uint32_t* s_warp, uint32_t& total) {
+  constexpr int W = NT / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < W ? s_warp[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < W) s_warp[lane] = w;
+  }
+  __syncthreads();
+  uint32_t prefix = warp ? s_warp[warp - 1] : 0u;
+  total = s_warp[W - 1];
+  __syncthreads();
+  return prefix + x - v;
+}
+
+// First index j >= start[L] of C with C[j] > a, scanning the level lists in
+// order (each is ascending). Returns S when none.
+__device__ uint32_t split_scan(const uint32_t* __restrict__ C, const uint32_t* s_start, uint32_t L, uint32_t a) {
+  for (uint32_t l = L; l < 32; ++l) {
+    uint32_t st = s_start[l], en = s_start[l + 1];
+    if (st < en && __ldg(C + en - 1) > a) {
+      uint32_t lo = st, hi = en - 1;
+      while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(C + mid) > a) hi = mid; else lo = mid + 1;
+      }
+      return lo;
+    }
+  }
+  return s_start[32];
+}
+
+__global__ __launch_bounds__(kTopoThreads) void k_topo_morton(TopoArgs A) {
+  __shared__ uint32_t s_start[34];
+  __shared__ uint32_t s_level_lo[34];
+  __shared__ uint32_t s_warp[kTopoWarps];
+  __shared__ uint32_t s_vstar, s_stuck, s_levels;
+  __shared__ uint32_t s_overrun, s_nondet, s_past, s_err, s_depth;
+  const uint32_t tid = threadIdx.x;
+  if (tid == 0) {
+    uint32_t acc = 0;
+    for (int l = 0; l < 33; ++l) { s_start[l] = acc; acc += (l < 32) ? A.lev_count[l] : 0u; }
+    s_start[33] = s_start[32];
+    s_overrun = s_nondet = s_past = s_err = s_depth = 0;
+    A.ra[0] = 0; A.rb[0] = A.n; A.parent[0] = kNone;
+  }
+  __syncthreads();
+  const uint32_t S = s_start[32];
+  const uint32_t D = A.D;
+  uint32_t lo = 0, hi = 1, L = 0;
+  for (; lo < hi; ++L) {
+    if (tid == 0) { s_level_lo[L] = lo; s_vstar = kNone; s_stuck = 0; }
+    __syncthreads();
+    const bool nonempty = L < 32 && s_start[L] < s_start[L + 1];
+    const uint32_t lastL = nonempty ? __ldg(A.C + s_start[L + 1] - 1) : 0u;
+    if (nonempty && L < D) {
+      for (uint32_t i = lo + tid; i < hi; i += kTopoThreads) {
+        uint32_t a = A.ra[i], b = A.rb[i];
+        if (b - a >= A.min_leaf && a >= lastL) atomicMin(&s_vstar, i);
+      }
+    }
+    __syncthreads();
+    if (tid == 0 && s_vstar != kNone) {
+      uint32_t j = split_scan(A.C, s_start, L, A.ra[s_vstar]);
+      s_stuck = (j == s_start[L + 1]) ? 1u : 0u;
+    }
+    __syncthreads();
+    uint32_t running = hi;
+    for (uint32_t base = lo; base < hi; base += kTopoThreads) {
+      const uint32_t i = base + tid;
+      bool internal = false;
+      uint32_t a = 0, b = 0, s = 0, inf = 0;
+      if (i < hi) {
+        a = A.ra[i]; b = A.rb[i];
+        const bool visit = (b - a >= A.min_leaf) && L < D && nonempty;
+        if (visit && !(s_vstar != kNone && i > s_vstar && s_stuck)) {
+          uint32_t j = split_scan(A.C, s_start, L, a);
+          s = (j < S) ? __ldg(A.C + j) : kNone;
+          internal = s < b;
+          if (j >= s_start[L + 1]) atomicAdd(&s_overrun, 1u);
+          if (j < S && j >= s_start[min(D + 1, 32u)]) atomicAdd(&s_nondet, 1u);
+          if (j == S) atomicAdd(&s_past, 1u);
+        }
+        const bool median = !internal && A.complete && (b - a > A.max_leaf);
+        inf = L | (internal ? 0x100u : 0u) | (median ? 0x200u : 0u);
+      }
+      uint32_t total;
+      uint32_t ex = block_excl_scan_nt<kTopoThreads>(internal ? 2u : 0u, s_warp, total);
+      if (i < hi) {
+        uint32_t c = kNone;
+        if (internal) {
+          c = running + ex;
+          if (c + 1 < A.cap_m) {
+            A.ra[c] = a; A.rb[c] = s; A.ra[c + 1] = s; A.rb[c + 1] = b;
+            A.parent[c] = i; A.parent[c + 1] = i;
+          } else {
+            // cannot happen (the Morton levels hold at most min(2^(D+1), 2n) - 1
+            // nodes); kept as a guarded leaf so that no index leaves its array
+            atomicOr(&s_err, (uint32_t)RT_DEVERR_MORTON_CAPACITY);
+            c = kNone;
+            inf &= ~0x100u;
+          }
+        }
+        A.child[i] = c;
+        A.info[i] = inf;
+      }
+      running += total;
+    }
+    __syncthreads();
+    lo = hi;
+    hi = min(running, A.cap_m);
+  }
+  if (tid == 0) { s_level_lo[L] = lo; s_levels = L; }
+  __syncthreads();
+  const uint32_t levels = s_levels;
+  const uint32_t maxl = A.max_leaf;
+
+  // bottom-up: leaves (final tree) and Morton leaves per subtree
+  for (int l = (int)levels - 1; l >= 0; --l) {
+    for (uint32_t i = s_level_lo[l] + tid; i < s_level_lo[l + 1]; i += kTopoThreads) {
+      uint32_t inf = A.info[i];
+      if (inf & 0x100u) {
+        uint32_t c = A.child[i];
+        A.leaves[i] = A.leaves[c] + A.leaves[c + 1];
+        A.mleaves[i] = A.mleaves[c] + A.mleaves[c + 1];
+      } else {
+        uint32_t size = A.rb[i] - A.ra[i];
+        A.leaves[i] = (inf & 0x200u) ? median_leaves(size, maxl) : 1u;
+        A.mleaves[i] = 1u;
+      }
+    }
+    __syncthreads();
+  }
+  // top-down: rank, lambda (leaves to the left), Morton-leaf ordinal, node id
+  if (tid == 0) { A.rank[0] = 0; A.lambda[0] = 0; A.ord[0] = 0; A.id[0] = 0; }
+  __syncthreads();
+  for (uint32_t l = 0; l < levels; ++l) {
+    for (uint32_t i = s_level_lo[l] + tid; i < s_level_lo[l + 1]; i += kTopoThreads) {
+      if (A.info[i] & 0x100u) {
+        uint32_t c = A.child[i];
+        uint32_t r = A.rank[i], lam = A.lambda[i], o = A.ord[i];
+        uint32_t ll = A.leaves[c];
+        A.rank[c] = r + 1; A.lambda[c] = lam; A.ord[c] = o; A.id[c] = 2 * r + 1;
+        A.rank[c + 1] = r + ll; A.lambda[c + 1] = lam + ll; A.ord[c + 1] = o + A.mleaves[c]; A.id[c + 1] = 2 * r + 2;
+      }
+    }
+    __syncthreads();
+  }
+  // emit Morton node records and the Morton-leaf table
+  const uint32_t total_m = s_level_lo[levels];
+  for (uint32_t i = tid; i < total_m; i += kTopoThreads) {
+    const uint32_t inf = A.info[i];
+    const uint32_t lvl = inf & 0xFFu;
+    const uint32_t nid = A.id[i];
+    if (nid >= A.max_nodes) { atomicOr(&s_err, (uint32_t)RT_DEVERR_NODE_CAPACITY); continue; }
+    A.parent_id[nid] = (i == 0) ? kNone : A.id[A.parent[i]];
+    if (inf & 0x100u) {
+      uint2 w = make_uint2((lvl % 3u) << 1, 2 * A.rank[i] + 1);
+      *(uint2*)(A.nodes + 8 * (size_t)nid) = w;
+    } else {
+      const uint32_t k = A.ord[i];
+      const uint32_t first = A.ra[i], cnt = A.rb[i] - A.ra[i];
+      const bool median = (inf & 0x200u) != 0;
+      A.ml_lambda[k] = A.lambda[i];
+      A.ml_rec[k] = make_uint4(nid, first, cnt, lvl | (median ? 0x80000000u : 0u));
+      A.ml_rank[k] = A.rank[i];
+      uint32_t depth = lvl + (median ? median_depth(cnt, maxl) : 0u) + 1u;
+      atomicMax(&s_depth, depth);
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const uint32_t leaves = A.leaves[0];
+    A.hdr[0] = leaves;
+    A.hdr[1] = A.mleaves[0];
+    A.hdr[2] = 2 * leaves - 1;
+    A.hdr[3] = s_depth;
+    A.hdr[4] = S;
+    A.hdr[5] = s_overrun;
+    A.hdr[6] = s_nondet;
+    A.hdr[7] = s_past;
+    A.hdr[8] = s_err | ((2 * leaves - 1 > A.max_nodes) ? (uint32_t)RT_DEVERR_NODE_CAPACITY : 0u);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// leaves: one warp per final leaf
+// ----------------------------------------------------------------------------
+struct LeafArgs {
+  const float4* verts;
+  const uint4* faces_in;
+  uint4* faces_out;      // may be null (tree_complete == 0)
+  float4* tris;          // may be null
+  const uint32_t* indices;
+  const uint32_t* ml_lambda;
+  const uint4* ml_rec;
+  const uint32_t* ml_rank;
+  const uint32_t* parent_id;
+  uint32_t* arrive;
+  uint32_t* nodes;
+  uint32_t max_nodes;
+  uint32_t max_leaf;
+  const uint32_t* hdr;
+  uint32_t* err;
+};
+
+constexpr int kMaxMedianDepth = 40;
+
+__device__ __forceinline__ void write_box(uint32_t* node, float3 mn, float3 mx) {
+  float* f = (float*)node;
+  __stcg(f + 2, mn.x); __stcg(f + 3, mn.y); __stcg(f + 4, mn.z);
+  __stcg(f + 5, mx.x); __stcg(f + 6, mx.y); __stcg(f + 7, mx.z);
+}
+
+__global__ __launch_bounds__(256) void k_leaves(LeafArgs A) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t leaf_count = A.hdr[0];
+  const uint32_t mleaf_count = A.hdr[1];
+  if (A.hdr[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) return;
+  for (uint32_t g = warp_global; g < leaf_count; g += nwarps) {
+    uint32_t leaf_id = 0, first = 0, cnt = 0;
+    // median path (ids and ranks from the median root down to the leaf's parent)
+    uint32_t path_id[kMaxMedianDepth], path_rank[kMaxMedianDepth];
+    int plen = 0;
+    if (lane == 0) {
+      // Morton leaf owning global leaf slot g: last k with ml_lambda[k] <= g
+      uint32_t lo = 0, hi = mleaf_count - 1;
+      while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (A.ml_lambda[mid] <= g) lo = mid; else hi = mid - 1;
+      }
+      const uint4 rec = A.ml_rec[lo];
+      leaf_id = rec.x; first = rec.y; cnt = rec.z;
+      if (rec.w & 0x80000000u) {
+        uint32_t q = g - A.ml_lambda[lo];
+        uint32_t rank = A.ml_rank[lo];
+        uint32_t depth = rec.w & 0xFFFFu;
+        uint32_t nid = rec.x, size = rec.z, a = rec.y;
+        while (size >= A.max_leaf && plen < kMaxMedianDepth) {
+          const uint32_t left = size >> 1, right = size - left;
+          const uint32_t ll = median_leaves(left, A.max_leaf);
+          if (q == 0 && nid < A.max_nodes)
+            *(uint2*)(A.nodes + 8 * (size_t)nid) = make_uint2((depth % 3u) << 1, 2 * rank + 1);
+          path_id[plen] = nid; path_rank[plen] = rank; ++plen;
+          if (q < ll) { nid = 2 * rank + 1; rank = rank + 1; size = left; }
+          else { q -= ll; nid = 2 * rank + 2; rank = rank + ll; a += left; size = right; }
+          ++depth;
+        }
+        leaf_id = nid; first = a; cnt = size;
+      }
+    }
+    leaf_id = __shfl_sync(0xffffffffu, leaf_id, 0);
+    first = __shfl_sync(0xffffffffu, first, 0);
+    cnt = __shfl_sync(0xffffffffu, cnt, 0);
+
+    float3 mn = make_float3(kHuge, kHuge, kHuge), mx = make_float3(-kHuge, -kHuge, -kHuge);
+    for (uint32_t i = first + lane; i < first + cnt; i += 32) {
+      const uint32_t orig = __ldg(A.indices + i);
+      const uint4 f = ldg4(A.faces_in + orig);
+      const float4 v0 = ldg4(A.verts + f.x), v1 = ldg4(A.verts + f.y), v2 = ldg4(A.verts + f.z);
+      if (A.faces_out) A.faces_out[i] = f;
+      if (A.tris) {
+        float4 e1 = make_float4(v1.x - v0.x, v1.y - v0.y, v1.z - v0.z, 0.0f);
+        float4 e2 = make_float4(v2.x - v0.x, v2.y - v0.y, v2.z - v0.z, 0.0f);
+        A.tris[3 * (size_t)i + 0] = make_float4(v0.x, v0.y, v0.z, 0.0f);
+        A.tris[3 * (size_t)i + 1] = e1;
+        A.tris[3 * (size_t)i + 2] = e2;
+      }
+      mn.x = fmin_sel(mn.x, fmin_sel(fmin_sel(v0.x, v1.x), v2.x));
+      mn.y = fmin_sel(mn.y, fmin_sel(fmin_sel(v0.y, v1.y), v2.y));
+      mn.z = fmin_sel(mn.z, fmin_sel(fmin_sel(v0.z, v1.z), v2.z));
+      mx.x = fmax_sel(mx.x, fmax_sel(fmax_sel(v0.x, v1.x), v2.x));
+      mx.y = fmax_sel(mx.y, fmax_sel(fmax_sel(v0.y, v1.y), v2.y));
+      mx.z = fmax_sel(mx.z, fmax_sel(fmax_sel(v0.z, v1.z), v2.z));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn.x = fmin_sel(mn.x, __shfl_xor_sync(0xffffffffu, mn.x, o));
+      mn.y = fmin_sel(mn.y, __shfl_xor_sync(0xffffffffu, mn.y, o));
+      mn.z = fmin_sel(mn.z, __shfl_xor_sync(0xffffffffu, mn.z, o));
+      mx.x = fmax_sel(mx.x, __shfl_xor_sync(0xffffffffu, mx.x, o));
+      mx.y = fmax_sel(mx.y, __shfl_xor_sync(0xffffffffu, mx.y, o));
+      mx.z = fmax_sel(mx.z, __shfl_xor_sync(0xffffffffu, mx.z, o));
+    }
+    if (lane == 0) {
+      if (leaf_id >= A.max_nodes) { atomicOr(A.err, (uint32_t)RT_DEVERR_NODE_CAPACITY); continue; }
+      uint32_t* nd = A.nodes + 8 * (size_t)leaf_id;
+      *(uint2*)nd = make_uint2(1u | (cnt << 1), first);
+      write_box(nd, mn, mx);
+      // propagate up: the second child to arrive merges the two boxes
+      uint32_t cur = leaf_id;
+      for (;;) {
+        uint32_t p, c0;
+        if (plen > 0) { --plen; p = path_id[plen]; c0 = 2 * path_rank[plen] + 1; }
+        else {
+          p = A.parent_id[cur];
+          if (p == kNone) break;
+          c0 = A.nodes[8 * (size_t)p + 1];
+        }
+        __threadfence();
+        if (atomicAdd(A.arrive + p, 1u) == 0u) break;
+        __threadfence();
+        const float* l = (const float*)(A.nodes + 8 * (size_t)c0);
+        const float* r = (const float*)(A.nodes + 8 * (size_t)(c0 + 1));
+        float lb[6], rb[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) { lb[q] = __ldcg(l + 2 + q); rb[q] = __ldcg(r + 2 + q); }
+        float3 bmn, bmx;
+        // kernels/CUDA_buildMeshTreeLBVH.cu:269-300: merged only when both children have a positive z extent
+        if (lb[5] - lb[2] > 0.0f && rb[5] - rb[2] > 0.0f) {
+          bmn = make_float3(fmin_sel(lb[0], rb[0]), fmin_sel(lb[1], rb[1]), fmin_sel(lb[2], rb[2]));
+          bmx = make_float3(fmax_sel(lb[3], rb[3]), fmax_sel(lb[4], rb[4]), fmax_sel(lb[5], rb[5]));
+        } else {
+          bmn = make_float3(kHuge, kHuge, kHuge);
+          bmx = make_float3(-kHuge, -kHuge, -kHuge);
+        }
+        write_box(A.nodes + 8 * (size_t)p, bmn, bmx);
+        cur = p;
+      }
+    }
+  }
+}
+
+__global__ void k_write_info(const uint32_t* __restrict__ hdr, const uint32_t* __restrict__ err, rt_build_info* info) {
+  if (threadIdx.x != 0) return;
+  info->leaf_count = hdr[0];
+  info->node_count = hdr[2];
+  info->real_depth = hdr[3];
+  info->split_count = hdr[4];
+  info->overrun_visits = hdr[5];
+  info->nondet_reads = hdr[6];
+  info->past_end_reads = hdr[7];
+  info->error = hdr[8] | *err;
+}
+
+struct BuildLayout {
+  uint32_t n, cap_m, max_nodes, tiles;
+  float4* hit;
+  float4* partial;
+  uint32_t* codes;
+  uint32_t* lev;
+  uint32_t* C;
+  uint32_t* lev_count;
+  void* sort_scratch;
+  size_t sort_bytes;
+  uint32_t *ra, *rb, *parent, *info, *child, *leaves, *mleaves, *rank, *lambda, *ord, *id;
+  uint32_t* ml_lambda;
+  uint4* ml_rec;
+  uint32_t* ml_rank;
+  uint32_t* parent_id;
+  uint32_t* arrive;
+  uint32_t* hdr;
+  uint32_t* err;
+  uint4* faces_tmp;
+};
+
+constexpr uint32_t kHitParts = 296;
+
+uint32_t morton_cap(uint32_t n, uint32_t D) {
+  uint64_t a = (D >= 31) ? (1ull << 32) : ((1ull << (D + 1)) - 1);
+  uint64_t b = 2ull * n + 1;
+  uint64_t c = a < b ? a : b;
+  return (uint32_t)(c + 2);
+}
+
+size_t carve_build(Carve& c, BuildLayout& L, uint32_t n, uint32_t D, bool need_codes, bool need_faces_tmp) {
+  L.n = n;
+  L.cap_m = morton_cap(n, D);
+  L.max_nodes = 2 * n - 1;
+  L.hit = c.take<float4>(2);
+  L.partial = c.take<float4>(2 * kHitParts);
+  L.codes = need_codes ? c.take<uint32_t>(n) : nullptr;
+  L.lev = c.take<uint32_t>(n);
+  L.C = c.take<uint32_t>(n);
+  L.lev_count = c.take<uint32_t>(256);
+  L.sort_bytes = radix_scratch_bytes(n);
+  L.sort_scratch = c.take<char>(L.sort_bytes);
+  uint32_t** bfs[] = {&L.ra, &L.rb, &L.parent, &L.info, &L.child, &L.leaves, &L.mleaves, &L.rank, &L.lambda, &L.ord, &L.id};
+  for (auto p : bfs) *p = c.take<uint32_t>(L.cap_m);
+  L.ml_lambda = c.take<uint32_t>(L.cap_m);
+  L.ml_rec = c.take<uint4>(L.cap_m);
+  L.ml_rank = c.take<uint32_t>(L.cap_m);
+  L.parent_id = c.take<uint32_t>(L.max_nodes);
+  L.arrive = c.take<uint32_t>(L.max_nodes);
+  L.hdr = c.take<uint32_t>(16);
+  L.err = c.take<uint32_t>(4);
+  L.faces_tmp = need_faces_tmp ? c.take<uint4>(n) : nullptr;
+  return c.off + 256;
+}
+
+int sm_count() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+}  // namespace
+}  // namespace rt
+
+using namespace rt;
+
+static rt_build_params normalized(const rt_build_params* p) {
+  rt_build_params q = p ? *p : rt_build_params{12, 1, 0, 0, 32};
+  if (q.tree_depth == 0) q.tree_depth = 12;
+  if (q.tree_depth > 32) q.tree_depth = 32;
+  if (q.min_leaf == 0) q.min_leaf = kMinLeafDefault;
+  if (q.max_leaf == 0) q.max_leaf = kMaxLeafDefault;
+  if (q.morton_bits == 0) q.morton_bits = 32;
+  return q;
+}
+
+extern "C" rt_status rt_lbvh_scratch_bytes(uint32_t face_count, const rt_build_params* params, size_t* scratch_bytes, uint32_t* max_nodes) {
+  if (!scratch_bytes || face_count == 0) return RT_ERR_INVALID_ARGUMENT;
+  rt_build_params q = normalized(params);
+  Carve c(nullptr, 0);
+  BuildLayout L;
+  *scratch_bytes = carve_build(c, L, face_count, q.tree_depth, true, true);
+  if (max_nodes) *max_nodes = 2 * face_count - 1;
+  return RT_OK;
+}
+
+extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
+  if (!d || d->face_count == 0 || !d->vertices || !d->faces_in || !d->boxes || !d->indices || !d->nodes || d->max_nodes == 0)
+    return RT_ERR_INVALID_ARGUMENT;
+  if (d->face_count > 0x7FFFFFFFu) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  const rt_build_params q = normalized(&d->params);
+  if (q.morton_bits != 32 && q.morton_bits != 30) return RT_ERR_INVALID_ARGUMENT;
+  const uint32_t n = d->face_count;
+  cudaStream_t st = (cudaStream_t)stream_;
+  const bool complete = q.tree_complete != 0;
+  const bool in_place = complete && d->faces_out && (d->faces_out == d->faces_in);
+  Carve c(d->scratch, d->scratch_bytes);
+  BuildLayout L;
+  carve_build(c, L, n, q.tree_depth, d->codes == nullptr, in_place);
+  if (!d->scratch || !c.ok()) return RT_ERR_SCRATCH_TOO_SMALL;
+  uint32_t* codes = d->codes ? d->codes : L.codes;
+  const int sms = sm_count();
+
+  // 1. hit box
+  if (d->hitbox) {
+    float4 mn = make_float4(d->hitbox[0], d->hitbox[1], d->hitbox[2], d->hitbox[3]);
+    float4 mx = make_float4(d->hitbox[4], d->hitbox[5], d->hitbox[6], d->hitbox[7]);
+    k_set_hitbox<<<1, 1, 0, st>>>(L.hit, mn, mx);
+    note_launch();
+  } else {
+    k_hitbox_partial<<<kHitParts, 256, 0, st>>>((const float4*)d->vertices, d->vertex_count, L.partial);
+    k_hitbox_final<<<1, 32, 0, st>>>(L.partial, kHitParts, L.hit);
+    note_launch(2);
+  }
+  RT_CHECK_LAUNCH();
+  // 2. boxes, indices, codes
+  {
+    uint32_t blocks = (uint32_t)hmin<uint64_t>((n + 255) / 256, (uint64_t)sms * 16);
+    k_boxes_morton<<<blocks, 256, 0, st>>>((const float4*)d->vertices, (const uint4*)d->faces_in, n, L.hit, (int)q.morton_bits,
+                                           (float4*)d->boxes, codes, d->indices);
+    note_launch();
+    RT_CHECK_LAUNCH();
+  }
+  // 3. sort (code, index)
+  rt_status s = radix_sort_pairs(codes, d->indices, n, 0, 32, 0, L.sort_scratch, L.sort_bytes, st, nullptr);
+  if (s != RT_OK) return s;
+  // 4. per-level split lists
+  if (cudaMemsetAsync(L.lev_count, 0, 256 * 4, st) != cudaSuccess) return RT_ERR_CUDA;
+  if (n > 1) {
+    uint32_t blocks = (uint32_t)hmin<uint64_t>((n + 255) / 256, (uint64_t)sms * 16);
+    k_levels<<<blocks, 256, 0, st>>>(codes, n, L.lev, L.C);
+    note_launch();
+    RT_CHECK_LAUNCH();
+    s = radix_sort_pairs(L.lev, L.C, n - 1, 0, 8, 0, L.sort_scratch, L.sort_bytes, st, L.lev_count);
+    if (s != RT_OK) return s;
+  }
+  // 5. Morton top tree
+  if (cudaMemsetAsync(L.err, 0, 16, st) != cudaSuccess) return RT_ERR_CUDA;
+  {
+    TopoArgs A;
+    A.C = L.C; A.lev_count = L.lev_count; A.n = n; A.D = q.tree_depth; A.min_leaf = q.min_leaf; A.max_leaf = q.max_leaf;
+    A.complete = complete ? 1u : 0u; A.cap_m = L.cap_m;
+    A.ra = L.ra; A.rb = L.rb; A.parent = L.parent; A.info = L.info; A.child = L.child; A.leaves = L.leaves; A.mleaves = L.mleaves;
+    A.rank = L.rank; A.lambda = L.lambda; A.ord = L.ord; A.id = L.id;
+    A.ml_lambda = L.ml_lambda; A.ml_rec = L.ml_rec; A.ml_rank = L.ml_rank; A.parent_id = L.parent_id;
+    A.nodes = d->nodes; A.max_nodes = d->max_nodes; A.hdr = L.hdr;
+    k_topo_morton<<<1, kTopoThreads, 0, st>>>(A);
+    note_launch();
+    RT_CHECK_LAUNCH();
+  }
+  // 6. leaves: median subtrees, reorder, triangles, boxes bottom-up
+  {
+    uint32_t count = d->max_nodes < L.max_nodes ? d->max_nodes : L.max_nodes;
+    if (cudaMemsetAsync(L.arrive, 0, (size_t)count * 4, st) != cudaSuccess) return RT_ERR_CUDA;
+    LeafArgs A;
+    A.verts = (const float4*)d->vertices;
+    A.faces_in = (const uint4*)d->faces_in;
+    A.faces_out = complete && d->faces_out ? (in_place ? L.faces_tmp : (uint4*)d->faces_out) : nullptr;
+    A.tris = complete ? (float4*)d->tris : nullptr;
+    A.indices = d->indices; A.ml_lambda = L.ml_lambda; A.ml_rec = L.ml_rec; A.ml_rank = L.ml_rank; A.parent_id = L.parent_id;
+    A.arrive = L.arrive; A.nodes = d->nodes; A.max_nodes = d->max_nodes; A.max_leaf = q.max_leaf; A.hdr = L.hdr; A.err = L.err;
+    k_leaves<<<sms * 8, 256, 0, st>>>(A);
+    note_launch();
+    RT_CHECK_LAUNCH();
+  }
+  if (in_place && cudaMemcpyAsync(d->faces_out, L.faces_tmp, (size_t)n * 16, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return RT_ERR_CUDA;
+  if (d->info) {
+    k_write_info<<<1, 32, 0, st>>>(L.hdr, L.err, d->info);
+    note_launch();
+    RT_CHECK_LAUNCH();
+  }
+  return RT_OK;
+}
+
+extern "C" rt_status rt_mesh_boxes(const float* vertices, const uint32_t* faces, uint32_t n, float* boxes, uint32_t* indices, rt_stream st) {
+  if (n == 0) return RT_OK;
+  if (!vertices || !faces || !boxes) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  uint32_t blocks = (uint32_t)hmin<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 16);
+  k_boxes_morton<<<blocks, 256, 0, (cudaStream_t)st>>>((const float4*)vertices, (const uint4*)faces, n, nullptr, 32, (float4*)boxes,
+                                                      nullptr, indices);
+    note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+namespace rt { namespace {
+__global__ __launch_bounds__(256) void k_reorder(const uint4* __restrict__ in, const uint32_t* __restrict__ idx, uint32_t n, uint4* __restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = ldg4(in + __ldg(idx + i));
+}
+}}  // namespace rt
+
+extern "C" rt_status rt_reorder_faces(const uint32_t* faces_in, const uint32_t* indices, uint32_t n, uint32_t* faces_out, rt_stream st) {
+  if (n == 0) return RT_OK;
+  if (!faces_in || !indices || !faces_out) return RT_ERR_INVALID_ARGUMENT;
+  const char* a = (const char*)faces_in;
+  const char* b = (const char*)faces_out;
+  if (a < b + (size_t)n * 16 && b < a + (size_t)n * 16) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  uint32_t blocks = (uint32_t)hmin<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 16);
+  k_reorder<<<blocks, 256, 0, (cudaStream_t)st>>>((const uint4*)faces_in, indices, n, (uint4*)faces_out);
+    note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}

@@ -1,0 +1,72 @@
+// rt_common.cuh -- shared device helpers for the LBVH build and traversal.
+//
+// Floating-point work that must match the reference bit for bit is compiled
+// with -fmad=false (no FMA contraction), IEEE division and square root
+// (nvcc's defaults -prec-div=true / -prec-sqrt=true), and min/max written as
+// the selects of the reference's host helpers (types/_cuda_float.h:11-19).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/rt_core.h"
+
+namespace rt {
+
+constexpr float kHuge = 3.402823466e+38f;  // CUDART_NORM_HUGE_F
+constexpr uint32_t kMinLeafDefault = 16;   // kernels/CUDA_buildMeshTreeLBVH.cu:39
+constexpr uint32_t kMaxLeafDefault = 224;  // kernels/CUDA_buildMeshTreeLBVH.cu:40
+
+__device__ __forceinline__ float fmin_sel(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float fmax_sel(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float4 f4min(float4 a, float4 b) {
+  return make_float4(fmin_sel(a.x, b.x), fmin_sel(a.y, b.y), fmin_sel(a.z, b.z), fmin_sel(a.w, b.w));
+}
+__device__ __forceinline__ float4 f4max(float4 a, float4 b) {
+  return make_float4(fmax_sel(a.x, b.x), fmax_sel(a.y, b.y), fmax_sel(a.z, b.z), fmax_sel(a.w, b.w));
+}
+
+// 128-bit read-only loads (ld.global.nc.v4) for data that no kernel writes
+// while the reading kernel runs.
+__device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ uint4 ldg4(const uint4* p) { return __ldg(p); }
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+template <typename T>
+inline T hmin(T a, T b) { return a < b ? a : b; }
+
+// Bump allocator over a caller-provided scratch buffer.
+struct Carve {
+  char* base;
+  size_t off = 0;
+  size_t cap;
+  Carve(void* p, size_t c) : base((char*)p), cap(c) {}
+  template <typename T>
+  T* take(size_t count) {
+    off = align_up(off, 256);
+    T* p = (T*)(base ? base + off : nullptr);
+    off += count * sizeof(T);
+    return p;
+  }
+  bool ok() const { return off <= cap; }
+};
+
+inline rt_status cuda_status(cudaError_t e) { return e == cudaSuccess ? RT_OK : RT_ERR_CUDA; }
+
+#define RT_CHECK_LAUNCH()                                   \
+  do {                                                      \
+    cudaError_t _e = cudaGetLastError();                    \
+    if (_e != cudaSuccess) return RT_ERR_CUDA;              \
+  } while (0)
+
+// Number of kernels this library has launched (process-wide); exported as
+// rt_launch_count() so that a caller can count the kernels inside a timed region.
+void note_launch(uint32_t kernels = 1);
+
+// Radix sort internals shared by the build (rt_sort.cu).
+size_t radix_scratch_bytes(uint32_t n);
+rt_status radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t begin_bit, uint32_t end_bit, int init_vals,
+                           void* scratch, size_t scratch_bytes, cudaStream_t stream, uint32_t* digit_totals_out);
+
+}  // namespace rt

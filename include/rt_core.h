@@ -1,0 +1,179 @@
+/* rt_core.h -- C ABI of the B200 LBVH build + closest-hit traversal core.
+ *
+ * A drop-in for the reference's LBVH / ray-tracing path (gatouillatpy/cudart):
+ * every entry point below names the reference function it replaces
+ * (file:line in the reference tree). Conventions:
+ *   - all pointers are device pointers unless a comment says "host";
+ *   - all calls are asynchronous on the caller's stream and never synchronize
+ *     (no host round trips: counts stay on the device);
+ *   - the library allocates nothing on its hot paths: callers pass scratch
+ *     buffers sized by the *_scratch_bytes queries;
+ *   - errors are returned as rt_status (the reference printed and exit()ed,
+ *     CUDACommon.h:123-133); device-side failures (stack or capacity overflow)
+ *     are reported in rt_build_info.error / the trace error word;
+ *   - there is no CPU fallback: without a CUDA device every compute call
+ *     returns RT_ERR_NO_DEVICE.
+ * Layouts match the reference: vertices are float4 (CUDAMesh.h), faces uint4
+ * (a, b, c, material), aabox is float4 min + float4 max (CUDABox.h:17-148),
+ * bvnode is 32 bytes (CUDANode.h:20-50): word0 bit0 = leaf flag, bits 1-2 =
+ * split axis (internal) or bits 1-31 = triangle count (leaf), word1 = left
+ * child id (right = left + 1) or first triangle position, then float3 box_min,
+ * float3 box_max.
+ */
+#ifndef RT_CORE_H
+#define RT_CORE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* rt_stream; /* a cudaStream_t; NULL = legacy default stream */
+
+typedef enum rt_status {
+  RT_OK = 0,
+  RT_ERR_INVALID_ARGUMENT = 1,
+  RT_ERR_NO_DEVICE = 2,
+  RT_ERR_CUDA = 3,
+  RT_ERR_SCRATCH_TOO_SMALL = 4,
+  RT_ERR_CAPACITY = 5,
+  RT_ERR_UNSUPPORTED = 6
+} rt_status;
+
+/* Device-side error bits (rt_build_info.error, trace error word). */
+#define RT_DEVERR_NODE_CAPACITY 0x1u  /* more nodes than max_nodes */
+#define RT_DEVERR_STACK_OVERFLOW 0x2u /* traversal stack exhausted (result of that ray may be wrong) */
+#define RT_DEVERR_MORTON_CAPACITY 0x4u
+
+typedef struct rt_build_params {
+  uint32_t tree_depth;    /* Morton levels; reference default 12 (CUDAMeshTree.h:118); 1..32 */
+  uint32_t tree_complete; /* 1: split leaves above max_leaf by median and reorder faces (CUDAMeshTree.cpp:88-91) */
+  uint32_t min_leaf;      /* 16, kernels/CUDA_buildMeshTreeLBVH.cu:39 (0 = default) */
+  uint32_t max_leaf;      /* 224, kernels/CUDA_buildMeshTreeLBVH.cu:40 (0 = default) */
+  uint32_t morton_bits;   /* 32: reference 11/11/10 interleave; 30: 10/10/10 left-aligned (0 = 32) */
+} rt_build_params;
+
+/* Written by rt_lbvh_build on the device. */
+typedef struct rt_build_info {
+  uint32_t node_count;     /* nodes written (2 * leaf_count - 1) */
+  uint32_t leaf_count;
+  uint32_t real_depth;     /* max leaf level + 1, as the reference computes it (:450-452) */
+  uint32_t split_count;    /* adjacent code pairs that differ */
+  uint32_t overrun_visits; /* Morton visits whose split search ran past the level's own list */
+  uint32_t nondet_reads;   /* split reads from levels deeper than tree_depth (unordered in the reference) */
+  uint32_t past_end_reads; /* split reads past the end of the list (undefined in the reference) */
+  uint32_t error;          /* RT_DEVERR_* bits */
+} rt_build_info;
+
+typedef struct rt_build_desc {
+  const float* vertices;    /* float4[vertex_count] */
+  uint32_t vertex_count;
+  uint32_t face_count;      /* N */
+  const uint32_t* faces_in; /* uint4[N] */
+  uint32_t* faces_out;      /* uint4[N]: faces in Morton (position) order; may equal faces_in */
+  const float* hitbox;      /* HOST float[8] = min xyzw, max xyzw (CUDAMesh::getHitbox); NULL = min/max of all vertices */
+  rt_build_params params;
+  float* boxes;             /* aabox[N] per original face (CUDAMeshTree::boxes) */
+  uint32_t* indices;        /* uint[N]: position -> original face id (CUDAMeshTree::indices) */
+  uint32_t* codes;          /* uint[N]: sorted Morton codes; NULL = kept in scratch */
+  uint32_t* nodes;          /* bvnode[max_nodes] (CUDAMeshTree::nodes) */
+  uint32_t max_nodes;       /* >= rt_lbvh_scratch_bytes' max_nodes guarantees no overflow */
+  float* tris;              /* float4[3N] {v0, v1 - v0, v2 - v0} per position (w = 0); NULL = not produced */
+  rt_build_info* info;      /* device pointer, may be NULL */
+  void* scratch;
+  size_t scratch_bytes;
+} rt_build_desc;
+
+/* Scratch bytes and the node-count bound for an N-face build.
+ * Replaces the temporaries CUDA_buildMeshTreeLBVH cudaMalloc'd per call
+ * (kernels/CUDA_buildMeshTreeLBVH.cu:462-471). */
+rt_status rt_lbvh_scratch_bytes(uint32_t face_count, const rt_build_params* params, size_t* scratch_bytes, uint32_t* max_nodes);
+
+/* LBVH build: boxes, Morton codes, key+index sort, split lists, topology,
+ * node boxes, face reorder and triangle pre-gather.
+ * Replaces CUDA_buildMeshTreeLBVH (kernels/CUDA_buildMeshTreeLBVH.cu:457-681),
+ * called by CUDAMeshTree::buildMeshTreeLBVH (CUDAMeshTree.cpp:88-91). */
+rt_status rt_lbvh_build(const rt_build_desc* desc, rt_stream stream);
+
+/* Per-face boxes and indices[k] = k.
+ * Replaces CUDA_calcMeshBoxes (kernels/CUDA_calcMeshBoxes.cu:65-104). */
+rt_status rt_mesh_boxes(const float* vertices, const uint32_t* faces, uint32_t face_count, float* boxes, uint32_t* indices, rt_stream stream);
+
+/* faces_out[n] = faces_in[indices[n]]; faces_out must not overlap faces_in.
+ * Replaces CUDA_reorderMeshFaces (kernels/CUDA_reorderMeshFaces.cu:44-83). */
+rt_status rt_reorder_faces(const uint32_t* faces_in, const uint32_t* indices, uint32_t face_count, uint32_t* faces_out, rt_stream stream);
+
+/* Stable LSD radix sort of (key, value) pairs on the low 8*ceil(bit_depth/8)
+ * bits of the keys; init_values = 1 sets values to 0..n-1 first.
+ * Replaces CUDA_radixSortGeneral (kernels/CUDA_radixSortGeneral.cu:397-482)
+ * and its small-size targets CUDA_bubbleSort512 (kernels/CUDA_bubbleSort512.cu:114)
+ * and CUDA_bitonicSortGeneral<uint,uint> (kernels/CUDA_bitonicSortGeneral.cu:505),
+ * which only guarantee ascending keys; ties here keep the input order. */
+rt_status rt_sort_scratch_bytes(uint32_t n, size_t* scratch_bytes);
+rt_status rt_radix_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t n, uint32_t bit_depth, int init_values,
+                              void* scratch, size_t scratch_bytes, rt_stream stream);
+/* Keys only. Replaces CUDA_radixSort (kernels/CUDA_radixSort.cu:357) and
+ * CUDA_bitonicSort<uint> (kernels/CUDA_bitonicSort.cu:403). */
+rt_status rt_radix_sort_keys(uint32_t* keys, uint32_t n, uint32_t bit_depth, void* scratch, size_t scratch_bytes, rt_stream stream);
+
+/* Camera state of CUDACamera (CUDACamera.h:15-321) that ray generation reads. */
+typedef struct rt_camera {
+  float center[3];
+  float angle[3]; /* pitch, yaw, roll (CUDACamera::pitch/yaw/roll) */
+  float fov;      /* radians; CUDACamera default PI/2 */
+  float ratio;    /* width / height; CUDACamera default 4/3 */
+} rt_camera;
+
+/* HOST. CUDACamera::lookAt (CUDACamera.cpp:126-132 -> angleFromDir :70-88). */
+rt_status rt_camera_look_at(rt_camera* camera, const float target[3]);
+/* HOST. The four float4 (origin, dir, step x, step y) of CUDA_calcPrimaryRays
+ * (kernels/CUDA_calcPrimaryRays.cu:43-55). */
+rt_status rt_camera_basis(const rt_camera* camera, uint32_t width, uint32_t height, float basis[16]);
+/* One pinhole ray per pixel, row-major, float4 origin and direction.
+ * Replaces CUDA_calcPrimaryRays (kernels/CUDA_calcPrimaryRays.cu:20-69). */
+rt_status rt_primary_rays(const rt_camera* camera, uint32_t width, uint32_t height, float* orig, float* dir, rt_stream stream);
+
+typedef struct rt_trace_desc {
+  const uint32_t* nodes;    /* bvnode[] from rt_lbvh_build */
+  const float* tris;        /* float4[3N] from rt_lbvh_build; NULL = read vertices + faces as the reference does */
+  const float* vertices;    /* float4[], used when tris == NULL */
+  const uint32_t* faces;    /* uint4[] in position order (the reordered faces), used when tris == NULL */
+  const uint32_t* indices;  /* position -> original id, used when id_mode == 1 */
+  const float* orig;        /* float4[ray_count] */
+  const float* dir;         /* float4[ray_count] */
+  const float* tmax;        /* float[ray_count] initial depth; NULL = CUDART_NORM_HUGE_F. A ray with tmax <= 0 misses. */
+  uint32_t ray_count;
+  uint32_t id_mode;         /* 0: position in the reordered faces (the reference's faces_id); 1: original face id */
+  int32_t* hit_id;          /* out: -1 on a miss */
+  float* hit_t;             /* out: t of the hit, or tmax on a miss (may alias tmax, as CUDABuffer depths do) */
+  float* hit_uv;            /* out: float2 (u, v); (0, 0) on a miss */
+  uint32_t* ray_visits;     /* optional out: nodes popped per ray */
+  uint32_t* ray_tests;      /* optional out: triangles tested per ray */
+  uint32_t* error_word;     /* optional device word: RT_DEVERR_* bits are OR-ed in */
+} rt_trace_desc;
+
+/* Closest hit per ray: the minimum (t, position) over all triangles that the
+ * Moller-Trumbore test of kernels/CUDA_raytraceMeshTree.cu:57-89 accepts with
+ * t < tmax. Replaces CUDA_raytraceMeshTree (kernels/CUDA_raytraceMeshTree.cu:434-480)
+ * called by CUDARaytracer::raytraceMeshTree (CUDARaytracer.cpp:130-135). */
+rt_status rt_trace_closest(const rt_trace_desc* desc, rt_stream stream);
+
+/* One cosine-weighted diffuse bounce per hit (PCG32 stream = ray index);
+ * misses give an inactive ray with tmax = -1. Workload generation for the
+ * incoherent scene; no reference counterpart. */
+rt_status rt_bounce_rays(const float* tris, const float* orig, const float* dir, const int32_t* hit_pos, const float* hit_t,
+                         uint32_t ray_count, uint64_t seed, float* orig_out, float* dir_out, float* tmax_out, rt_stream stream);
+
+const char* rt_status_string(rt_status status);
+uint32_t rt_version(void);
+/* RT_OK when a CUDA device is usable, RT_ERR_NO_DEVICE otherwise. */
+rt_status rt_device_check(void);
+/* Kernels this library has launched in this process (to count the kernels of a timed region). */
+uint64_t rt_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RT_CORE_H */

@@ -217,8 +217,8 @@ static void find_splits(const u32* codes, u32 n, SplitLists& sl) {
 struct TopoStats {
   u32 node_count, leaf_count, real_depth, split_count;
   u32 overrun_visits;   // visits whose split search left the level's own list
-  u32 nondet_reads;     // reads from lists deeper than tree_depth (unsorted in the reference)
-  u32 past_end_reads;   // reads past the end of the split list (undefined in the reference)
+  u32 nondet_reads;     // visits whose scan stopped in a list deeper than tree_depth (unsorted in the reference)
+  u32 past_end_reads;   // visits whose scan ran past the end of the split list (undefined in the reference)
   u32 error;            // 1 = node capacity exceeded
 };
 
@@ -272,13 +272,19 @@ static void morton_node(Topo& t, u32 a, u32 b, u32 lvl, u32 id) {
   for (;;) {
     u32 j = t.ptr[lvl];
     if (j >= sl.start[lvl + 1]) left_own_list = true;
-    if (j >= S) { t.st.past_end_reads++; s = 0xFFFFFFFFu; }
-    else { if (j >= sl.start[t.D + 1]) t.st.nondet_reads++; s = sl.C[j]; }
-    if (s >= b) { if (left_own_list) t.st.overrun_visits++; leaf_node(t, a, b, lvl, id); return; }
-    if (s > a) break;
+    if (j >= S) s = 0xFFFFFFFFu;
+    else s = sl.C[j];
+    if (s >= b || s > a) break;
     t.ptr[lvl]++;
   }
-  if (left_own_list) t.st.overrun_visits++;
+  {
+    // per-visit statistics on the index where the scan stopped
+    u32 j = t.ptr[lvl];
+    if (left_own_list) t.st.overrun_visits++;
+    if (j >= S) t.st.past_end_reads++;
+    else if (sl.start[t.D + 1] < S && j >= sl.start[t.D + 1]) t.st.nondet_reads++;
+  }
+  if (s >= b) { leaf_node(t, a, b, lvl, id); return; }
   u32 left = ++t.count, right = ++t.count;
   put_node(t, id, make_internal(lvl % 3, left));
   morton_node(t, a, s, lvl + 1, left);

@@ -1,0 +1,75 @@
+"""C-ABI library checks that need no GPU: it loads, exports every function
+include/rt_core.h declares, refuses compute without a device (no CPU
+fallback), and its host-side camera math equals the oracle's bit for bit."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from tests.conftest import cuda_available
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    return sorted(set(re.findall(r"^\s*(?:rt_status|const char\*|uint32_t|uint64_t)\s+(rt_\w+)\s*\(", text, re.M)))
+
+
+def test_header_declarations_are_exported():
+    from cudart_b200 import _abi
+    lib = _abi.lib()
+    declared = _declared("rt_core.h")
+    assert len(declared) >= 15
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(declared) <= set(_abi.EXPORTS)
+
+
+def test_status_strings_and_version():
+    from cudart_b200 import _abi
+    lib = _abi.lib()
+    assert lib.rt_status_string(0) == b"ok"
+    assert lib.rt_status_string(2) == b"no CUDA device"
+    assert lib.rt_version() >= 100
+
+
+@pytest.mark.skipif(cuda_available(), reason="checks the no-device path")
+def test_no_cpu_fallback():
+    from cudart_b200 import _abi
+    lib = _abi.lib()
+    assert lib.rt_device_check() == 2
+    assert lib.rt_radix_sort_pairs(None, None, 0, 32, 0, None, 0, None) == 2
+    desc = _abi.TraceDesc()
+    desc.nodes = desc.orig = desc.dir = desc.hit_id = desc.hit_t = desc.hit_uv = desc.tris = 16  # never dereferenced
+    assert lib.rt_trace_closest(C.byref(desc), None) == 2
+
+
+def test_invalid_arguments_rejected():
+    from cudart_b200 import _abi
+    lib = _abi.lib()
+    assert lib.rt_lbvh_build(None, None) == 1
+    nb = C.c_size_t(0)
+    assert lib.rt_lbvh_scratch_bytes(0, None, C.byref(nb), None) == 1
+    assert lib.rt_reorder_faces(C.c_void_p(4096), C.c_void_p(64), 100, C.c_void_p(4096 + 16), None) == 1  # overlap
+
+
+def test_scratch_queries():
+    from cudart_b200 import core
+    nb, mx = core.lbvh_scratch_bytes(1 << 20)
+    assert mx == 2 * (1 << 20) - 1
+    assert nb > 8 * (1 << 20)
+
+
+@pytest.mark.parametrize("scene", ["terrain", "soup"])
+def test_camera_host_math_matches_oracle(oracle, scene):
+    from cudart_b200 import core, scenes
+    cam = scenes.terrain_small_scene()[1] if scene == "terrain" else scenes.soup_1m_scene()[1]
+    c = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
+    ang = np.array(list(c.angle), np.float32)
+    assert np.array_equal(ang.view(np.uint32), oracle.camera_look_at(cam.center, cam.target).view(np.uint32))
+    basis = np.array(core.camera_basis(c, cam.width, cam.height), np.float32)
+    ob = oracle.camera_basis(cam.center, ang, cam.fov, cam.ratio, cam.width, cam.height)
+    assert np.array_equal(basis.view(np.uint32), ob.view(np.uint32))

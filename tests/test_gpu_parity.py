@@ -1,0 +1,270 @@
+"""GPU parity: every stage of the CUDA path, called through the C ABI, against
+the CPU oracle (which is pinned to the reference's own code) and the golden
+fixtures. Integer/byte/index outputs and the pinned FP32 outputs are compared
+bit for bit (tolerance: exact)."""
+import os
+
+import numpy as np
+import pytest
+
+from cudart_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def T():
+    import torch
+    assert torch.cuda.is_available()
+    from cudart_b200 import core
+    assert core.device_check()
+    return torch
+
+
+def _u32(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+def _dev(T, a):
+    return T.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _host(t):
+    return t.cpu().numpy()
+
+
+def _build(T, mesh, **kw):
+    from cudart_b200 import core
+    v = _dev(T, mesh.vertices)
+    f = _dev(T, mesh.faces.view(np.int32))
+    tree = core.build_lbvh(v, f, **kw)
+    T.cuda.synchronize()
+    return v, f, tree
+
+
+def _check_build(T, oracle, mesh, tree_depth=12, morton_bits=32, hitbox=None):
+    v, f, tree = _build(T, mesh, tree_depth=tree_depth, morton_bits=morton_bits, hitbox=hitbox)
+    ref = oracle.lbvh_build(mesh.vertices, mesh.faces, hitbox if hitbox is not None else oracle.hitbox(mesh.vertices),
+                            tree_depth=tree_depth, layout=morton_bits)
+    info = tree.info_host()
+    for k in ("node_count", "leaf_count", "real_depth", "split_count", "overrun_visits", "nondet_reads", "past_end_reads"):
+        assert info[k] == ref["info"][k], (k, info[k], ref["info"][k])
+    assert info["error"] == 0
+    nc = info["node_count"]
+    assert np.array_equal(_u32(_host(tree.codes)), ref["codes"])
+    assert np.array_equal(_u32(_host(tree.indices)), ref["indices"])
+    assert np.array_equal(_u32(_host(tree.boxes)), _u32(ref["boxes"]))
+    assert np.array_equal(_u32(_host(tree.nodes)[:nc]), _u32(ref["nodes"]))
+    assert np.array_equal(_u32(_host(tree.faces)), _u32(ref["faces"]))
+    assert np.array_equal(_u32(_host(tree.tris)), _u32(ref["tris"]))
+    return v, f, tree, ref
+
+
+# ----------------------------------------------------------------------------- sort
+@pytest.mark.parametrize("n", [1, 2, 100, 4096, 4097, 100000, 1 << 20])
+@pytest.mark.parametrize("bits", [8, 21, 32])
+def test_sort_pairs_matches_oracle(T, oracle, n, bits):
+    from cudart_b200 import core
+    rng = np.random.default_rng(n + bits)
+    keys = rng.integers(0, 1 << min(bits, 31), n, dtype=np.int64).astype(np.uint32)
+    if n > 10:
+        keys[: n // 3] = keys[0]  # many ties
+    k, v = _dev(T, keys.view(np.int32)), T.empty(n, dtype=T.int32, device="cuda")
+    core.sort_pairs(k, v, bits, init_values=True)
+    ek, ev = oracle.sort_pairs(keys, None, bits, init_vals=True)
+    assert np.array_equal(_u32(_host(k)), ek)
+    assert np.array_equal(_u32(_host(v)), ev)
+
+
+def test_sort_keys_and_given_values(T, oracle):
+    from cudart_b200 import core
+    rng = np.random.default_rng(7)
+    keys = rng.integers(0, 1 << 21, 1397121, dtype=np.int64).astype(np.uint32)  # samples/09_how_to_use_a_sorter.cpp:54
+    vals = rng.integers(0, 1 << 30, keys.size, dtype=np.int64).astype(np.uint32)
+    k = _dev(T, keys.view(np.int32))
+    core.sort_keys(k, 21)
+    assert np.array_equal(_u32(_host(k)), np.sort(keys))
+    k, v = _dev(T, keys.view(np.int32)), _dev(T, vals.view(np.int32))
+    core.sort_pairs(k, v, 32)
+    ek, ev = oracle.sort_pairs(keys, vals, 32)
+    assert np.array_equal(_u32(_host(k)), ek) and np.array_equal(_u32(_host(v)), ev)
+
+
+# ----------------------------------------------------------------------------- build
+def test_build_terrain_c0_matches_golden(T, oracle):
+    g = np.load(os.path.join(GOLD, "terrain_c0.npz"))
+    mesh, _ = scenes.terrain_small_scene()
+    v, f, tree, ref = _check_build(T, oracle, mesh, hitbox=g["hitbox"])
+    nc = tree.node_count
+    assert np.array_equal(_u32(_host(tree.nodes)[:nc]), g["nodes"])
+    assert np.array_equal(_u32(_host(tree.codes)), g["codes"])
+    assert np.array_equal(_u32(_host(tree.faces)), g["faces"])
+    assert tree.info_host()["overrun_visits"] > 0
+
+
+@pytest.mark.parametrize("n", [1, 2, 15, 16, 17, 223, 224, 225, 511, 512, 513, 4096, 4097, 32768, 32769, 100000])
+def test_build_soup_sizes(T, oracle, n):
+    _check_build(T, oracle, scenes.soup(n, seed=1000 + n))
+
+
+@pytest.mark.parametrize("depth", [1, 3, 7, 20, 31, 32])
+def test_build_tree_depths(T, oracle, depth):
+    _check_build(T, oracle, scenes.soup(20000, seed=11), tree_depth=depth)
+
+
+def test_build_morton30_and_device_hitbox(T, oracle):
+    mesh = scenes.soup(50000, seed=12)
+    _check_build(T, oracle, mesh, morton_bits=30)
+    _check_build(T, oracle, mesh, hitbox=None)
+
+
+def test_build_degenerate_inputs(T, oracle):
+    from tests.golden.make_golden import flat_z_mesh
+    _, _, tree, _ = _check_build(T, oracle, flat_z_mesh())
+    g = np.load(os.path.join(GOLD, "flatz.npz"))
+    assert np.array_equal(_u32(_host(tree.nodes)[: tree.node_count]), g["nodes"])
+    _check_build(T, oracle, scenes.soup(3000, seed=5, lo=(0.3, 0.3, 0.3), hi=(0.3, 0.3, 0.3), sigma=0.0))
+    m = scenes.soup(500, seed=9)
+    vv = m.vertices.copy()
+    vv[1::3] = vv[0::3]
+    _check_build(T, oracle, scenes.Mesh(vv, m.faces))
+
+
+def test_build_terrain_large_overrun(T, oracle):
+    _check_build(T, oracle, scenes.terrain(256, 4))
+
+
+def test_build_in_place_faces(T, oracle):
+    from cudart_b200 import core
+    mesh = scenes.soup(30000, seed=3)
+    v = _dev(T, mesh.vertices)
+    f = _dev(T, mesh.faces.view(np.int32))
+    tree = core.build_lbvh(v, f)
+    tree2 = core.Tree(nodes=T.empty_like(tree.nodes), boxes=T.empty_like(tree.boxes), indices=T.empty_like(tree.indices),
+                      codes=T.empty_like(tree.codes), faces=f, tris=T.empty_like(tree.tris), info=T.zeros_like(tree.info))
+    core.build_lbvh(v, f, out=tree2)  # faces_out == faces_in: reordered in place, as the reference does
+    T.cuda.synchronize()
+    assert T.equal(tree2.faces, tree.faces) and T.equal(tree2.nodes[: tree.node_count], tree.nodes[: tree.node_count])
+
+
+# ----------------------------------------------------------------------------- rays and traversal
+def _rays(T, cam):
+    from cudart_b200 import core
+    c = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
+    o, d = core.primary_rays(c, cam.width, cam.height)
+    T.cuda.synchronize()
+    return o, d
+
+
+@pytest.mark.parametrize("scene", ["terrain", "soup"])
+def test_primary_rays_match_oracle(T, oracle, scene):
+    cam = scenes.terrain_small_scene()[1] if scene == "terrain" else scenes.soup_1m_scene()[1]
+    o, d = _rays(T, cam)
+    eo, ed, _, _ = oracle.primary_rays(cam)
+    assert np.array_equal(_u32(_host(o)), _u32(eo))
+    assert np.array_equal(_u32(_host(d)), _u32(ed))
+
+
+def _check_trace(T, oracle, tree, ref, o, d, tmax=None, id_mode=0, use_tris=True, vertices=None, sel=None):
+    from cudart_b200 import core
+    out = core.trace(tree, o, d, tmax=tmax, id_mode=id_mode, counters=True, use_tris=use_tris, vertices=vertices)
+    T.cuda.synchronize()
+    oo, dd = _host(o), _host(d)
+    tm = None if tmax is None else _host(tmax)
+    e = oracle.trace(ref["nodes"], ref["tris"], ref["indices"], oo, dd, tm, mode=0, id_mode=id_mode, counters=True)
+    assert int(_host(out["err"])[0]) == 0
+    assert np.array_equal(_host(out["id"]), e["id"])
+    assert np.array_equal(_u32(_host(out["t"])), _u32(e["t"]))
+    assert np.array_equal(_u32(_host(out["uv"])), _u32(e["uv"]))
+    assert np.array_equal(_u32(_host(out["visits"])), e["visits"])
+    assert np.array_equal(_u32(_host(out["tests"])), e["tests"])
+    return out, e
+
+
+def test_trace_terrain_c0_matches_golden_and_oracle(T, oracle):
+    g = np.load(os.path.join(GOLD, "terrain_c0.npz"))
+    mesh, cam = scenes.terrain_small_scene()
+    v, f, tree, ref = _check_build(T, oracle, mesh)
+    o, d = _rays(T, cam)
+    out, _ = _check_trace(T, oracle, tree, ref, o, d)
+    sel = g["ray_sel"]
+    assert np.array_equal(_host(out["id"])[sel], g["hit_id"])
+    assert np.array_equal(_u32(_host(out["t"])[sel]), _u32(g["hit_t"]))
+    assert np.array_equal(_u32(_host(out["uv"])[sel]), _u32(g["hit_uv"]))
+    # reference data path (vertices + reordered faces, edges computed per test) gives the same bits
+    _check_trace(T, oracle, tree, ref, o, d, use_tris=False, vertices=v)
+    # original ids
+    _check_trace(T, oracle, tree, ref, o, d, id_mode=1)
+
+
+def test_trace_soup_incoherent(T, oracle):
+    mesh = scenes.soup(200000, seed=21)
+    v, f, tree, ref = _check_build(T, oracle, mesh)
+    cam = scenes.Camera((0.5, 0.5, -0.4), (0.5, 0.5, 0.5), scenes.FOV_60, 320, 240)
+    o, d = _rays(T, cam)
+    out, e = _check_trace(T, oracle, tree, ref, o, d)
+    assert (e["id"] >= 0).mean() > 0.95
+    # bounce rays: bit-exact with the oracle, then traced
+    from cudart_b200 import core
+    bo, bd, bt = core.bounce_rays(tree.tris, o, d, out["id"], out["t"], 1234)
+    T.cuda.synchronize()
+    eo, ed, et = oracle.bounce_rays(ref["tris"], _host(o), _host(d), e["id"], e["t"], 1234)
+    assert np.array_equal(_u32(_host(bo)), _u32(eo)) and np.array_equal(_u32(_host(bd)), _u32(ed))
+    assert np.array_equal(_u32(_host(bt)), _u32(et))
+    _check_trace(T, oracle, tree, ref, bo, bd, tmax=bt)
+
+
+def test_trace_tmax_and_degenerate_rays(T, oracle):
+    mesh = scenes.soup(20000, seed=22)
+    v, f, tree, ref = _check_build(T, oracle, mesh)
+    cam = scenes.Camera((0.5, 0.5, -0.4), (0.5, 0.5, 0.5), scenes.FOV_60, 64, 64)
+    o, d = _rays(T, cam)
+    dd = d.clone()
+    dd[::7, 0] = 0.0  # exactly zero direction components
+    dd[::11, 1] = 0.0
+    dd[::13] = 0.0
+    tm = T.full((o.shape[0],), 3.402823466e38, dtype=T.float32, device="cuda")
+    tm[::5] = 0.3
+    tm[::17] = 0.0
+    tm[::19] = -1.0
+    _check_trace(T, oracle, tree, ref, o, dd.contiguous(), tmax=tm)
+
+
+def test_trace_matches_brute_force(T, oracle):
+    mesh = scenes.soup(3000, seed=23)
+    v, f, tree, ref = _check_build(T, oracle, mesh)
+    cam = scenes.Camera((0.5, 0.5, -0.4), (0.5, 0.5, 0.5), scenes.FOV_60, 96, 64)
+    o, d = _rays(T, cam)
+    from cudart_b200 import core
+    out = core.trace(tree, o, d)
+    T.cuda.synchronize()
+    bf = oracle.trace_brute(ref["tris"], _host(o), _host(d))
+    assert np.array_equal(_host(out["id"]), bf["id"])
+    assert np.array_equal(_u32(_host(out["t"])), _u32(bf["t"]))
+
+
+def test_soup_1m_full_size(T, oracle):
+    """The 2^20-triangle workload at full size: the whole build bit-exact, all
+    1920x1080 primary rays bit-exact, a bounded sample of bounce rays bit-exact."""
+    mesh, cam = scenes.soup_1m_scene()
+    v, f, tree, ref = _check_build(T, oracle, mesh)
+    o, d = _rays(T, cam)
+    from cudart_b200 import core
+    out = core.trace(tree, o, d)
+    T.cuda.synchronize()
+    oo, dd = _host(o), _host(d)
+    e = oracle.trace(ref["nodes"], ref["tris"], ref["indices"], oo, dd)
+    assert np.array_equal(_host(out["id"]), e["id"])
+    assert np.array_equal(_u32(_host(out["t"])), _u32(e["t"]))
+    assert (e["id"] >= 0).mean() > 0.99
+    bo, bd, bt = core.bounce_rays(tree.tris, o, d, out["id"], out["t"], 99)
+    out2 = core.trace(tree, bo, bd, tmax=bt)
+    T.cuda.synchronize()
+    sel = np.arange(0, oo.shape[0], 37)
+    eo, ed, et = oracle.bounce_rays(ref["tris"], oo, dd, e["id"], e["t"], 99)
+    assert np.array_equal(_u32(_host(bo)), _u32(eo))
+    e2 = oracle.trace(ref["nodes"], ref["tris"], ref["indices"], np.ascontiguousarray(eo[sel]), np.ascontiguousarray(ed[sel]),
+                      np.ascontiguousarray(et[sel]))
+    assert np.array_equal(_host(out2["id"])[sel], e2["id"])
+    assert np.array_equal(_u32(_host(out2["t"])[sel]), _u32(e2["t"]))
