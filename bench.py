@@ -58,12 +58,13 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic():
-    """Per-launch DRAM bytes of the trace kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "trace_soup1m_traffic.json")
+def load_traffic(kernel: str):
+    """DRAM bytes (read + write) of one primary-ray trace launch of this workload,
+    from the committed ncu summary for that kernel (profiles/trace_traffic.json)."""
+    p = os.path.join(ROOT, "profiles", "trace_traffic.json")
     if os.path.exists(p):
         with open(p) as f:
-            return json.load(f)
+            return json.load(f).get(kernel)
     return None
 
 
@@ -169,10 +170,13 @@ def run_ours(args, rank, world, local_rank):
     cnt1 = core.trace(tree, rays[0], rays[1], counters=True)
     cnt2 = core.trace(tree, bounce[0], bounce[1], tmax=bounce[2], counters=True)
     torch.cuda.synchronize()
-    vis = int(cnt1["visits"].sum().item()) + int(cnt2["visits"].sum().item())
-    tst = int(cnt1["tests"].sum().item()) + int(cnt2["tests"].sum().item())
+    vis1, tst1 = int(cnt1["visits"].sum().item()), int(cnt1["tests"].sum().item())
+    vis = vis1 + int(cnt2["visits"].sum().item())
+    tst = tst1 + int(cnt2["tests"].sum().item())
     same = torch.equal(cnt1["id"], hits1["id"]) and torch.equal(cnt2["id"], hits2["id"])
-    trace_bytes = 48 * (R + R) + 32 * vis + 48 * tst  # 32 B ray in + 16 B hit out per ray slot, nodes, triangles
+    # algorithmic bytes: 32 B ray in + 16 B hit out per ray slot, 32 B per box record read, 48 B per triangle tested
+    primary_bytes = 48 * R + 32 * vis1 + 48 * tst1
+    trace_bytes = 48 * (R + R) + 32 * vis + 48 * tst
 
     if world > 1:
         import torch.distributed as dist
@@ -205,8 +209,10 @@ def run_ours(args, rank, world, local_rank):
     value = world * rays_per_step * K / (trace_ms * 1e-3) / 1e6
     build_mtri = world * N * K / (build_ms * 1e-3) / 1e6
     peak, peak_kind = load_peaks()
-    achieved = trace_bytes * K / (trace_ms * 1e-3) / 1e9 / world * world  # per GPU, all trace launches
-    traffic = load_traffic()
+    launch_ms = trace1_ms / K  # primary-ray launch, per launch (this rank)
+    achieved = primary_bytes / (launch_ms * 1e-3) / 1e9  # GB/s of one GPU primary-ray launch
+    kernel_name = "k_trace_accel" if getattr(tree, "accel", None) is not None else "k_trace"
+    traffic = load_traffic(kernel_name)
 
     result = {
         "metric": METRIC,
@@ -231,9 +237,9 @@ def run_ours(args, rank, world, local_rank):
                   "counted_run_identical": bool(same)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "traffic": None if traffic is None else traffic.get("bytes_per_step"),
-                     "kernel": "k_trace (primary + bounce launches)",
-                     "algorithmic_bytes_per_step": trace_bytes},
+                     "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
+                     "kernel": f"{kernel_name} (primary-ray launch, {R} rays)",
+                     "algorithmic_bytes_per_launch": primary_bytes, "launch_ms": round(launch_ms, 4)},
         "gpu_launches": int(launches),
         "wall_s_timed": round(t_wall, 3),
     }
