@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--faces", type=int, default=1 << 20)
+    ap.add_argument("--build16m", type=int, default=1, help="also time the LBVH build alone on a 2^24-face soup")
     return ap.parse_args()
 
 
@@ -243,6 +244,9 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "wall_s_timed": round(t_wall, 3),
     }
+    if args.build16m:
+        del flush
+        result["build_16m"] = build_only(24, args, dev, world)
     clocks = clk.summary()
     result["clocks"] = {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]}
     if not args.no_e2e:
@@ -250,6 +254,43 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(mesh, cam, budget_s=12.0)
     return result
+
+
+def build_only(log2n, args, dev, world):
+    """LBVH build alone on a 2^log2n-face soup (the 16M-face build target), CUDA events, L2 flushed between builds."""
+    import torch
+
+    from cudart_b200 import core, scenes
+
+    mesh = scenes.soup(1 << log2n, seed=7)
+    v = torch.from_numpy(mesh.vertices).to(dev)
+    f = torch.from_numpy(mesh.faces.view(np.int32)).to(dev)
+    del mesh
+    tree = core.build_lbvh(v, f)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(2):
+        core.build_lbvh(v, f, out=tree)
+    torch.cuda.synchronize()
+    ms = 0.0
+    reps = max(3, min(args.steps, 10))
+    for _ in range(reps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        core.build_lbvh(v, f, out=tree)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    info = tree.info_host()
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = t.item() / reps
+    n = 1 << log2n
+    return {"faces": n, "value": round(world * n / (ms * 1e-3) / 1e6, 2), "unit": "Mtri/s", "ms": round(ms, 4),
+            "node_count": info["node_count"], "reps": reps}
 
 
 def run_e2e(args, mesh, camera, W, H, dev, world):

@@ -20,7 +20,7 @@ DEVERR_MORTON_CAPACITY = 0x4
 
 # every symbol include/rt_core.h declares
 EXPORTS = (
-    "rt_lbvh_scratch_bytes", "rt_lbvh_build", "rt_mesh_boxes", "rt_reorder_faces", "rt_sort_scratch_bytes",
+    "rt_lbvh_scratch_bytes", "rt_lbvh_accel_bytes", "rt_lbvh_build", "rt_mesh_boxes", "rt_reorder_faces", "rt_sort_scratch_bytes",
     "rt_radix_sort_pairs", "rt_radix_sort_keys", "rt_camera_look_at", "rt_camera_basis", "rt_primary_rays",
     "rt_trace_closest", "rt_bounce_rays", "rt_status_string", "rt_version", "rt_device_check", "rt_launch_count",
 )
@@ -47,13 +47,14 @@ class BuildInfo(C.Structure):
 class BuildDesc(C.Structure):
     _fields_ = [("vertices", _P), ("vertex_count", _U32), ("face_count", _U32), ("faces_in", _P), ("faces_out", _P),
                 ("hitbox", _P), ("params", BuildParams), ("boxes", _P), ("indices", _P), ("codes", _P), ("nodes", _P),
-                ("max_nodes", _U32), ("tris", _P), ("info", _P), ("scratch", _P), ("scratch_bytes", C.c_size_t)]
+                ("max_nodes", _U32), ("tris", _P), ("info", _P), ("scratch", _P), ("scratch_bytes", C.c_size_t),
+                ("accel", _P), ("accel_bytes", C.c_size_t)]
 
 
 class TraceDesc(C.Structure):
     _fields_ = [("nodes", _P), ("tris", _P), ("vertices", _P), ("faces", _P), ("indices", _P), ("orig", _P), ("dir", _P),
                 ("tmax", _P), ("ray_count", _U32), ("id_mode", _U32), ("hit_id", _P), ("hit_t", _P), ("hit_uv", _P),
-                ("ray_visits", _P), ("ray_tests", _P), ("error_word", _P)]
+                ("ray_visits", _P), ("ray_tests", _P), ("error_word", _P), ("accel", _P), ("face_count_hint", _U32)]
 
 
 class Camera(C.Structure):
@@ -71,6 +72,7 @@ def lib():
         L = C.CDLL(LIB_PATH)
         L.rt_lbvh_scratch_bytes.argtypes = [_U32, C.POINTER(BuildParams), C.POINTER(C.c_size_t), C.POINTER(_U32)]
         L.rt_lbvh_build.argtypes = [C.POINTER(BuildDesc), _P]
+        L.rt_lbvh_accel_bytes.argtypes = [_U32, C.POINTER(C.c_size_t)]
         L.rt_mesh_boxes.argtypes = [_P, _P, _U32, _P, _P, _P]
         L.rt_reorder_faces.argtypes = [_P, _P, _U32, _P, _P]
         L.rt_sort_scratch_bytes.argtypes = [_U32, C.POINTER(C.c_size_t)]

@@ -79,6 +79,7 @@ class Tree:
     faces: torch.Tensor  # int32 (N, 4) faces in position order
     tris: torch.Tensor  # float32 (N, 12) {v0, e1, e2}
     info: torch.Tensor  # int32 (8,) rt_build_info, on the device
+    accel: torch.Tensor | None = None  # uint8 traversal blob (two-child records, leaf table, group boxes)
 
     def info_host(self) -> dict:
         vals = self.info.cpu().tolist()
@@ -101,8 +102,14 @@ def lbvh_scratch_bytes(face_count: int, tree_depth=12, tree_complete=True, morto
     return nb.value, mx.value
 
 
+def accel_bytes(face_count: int) -> int:
+    nb = C.c_size_t(0)
+    _abi.check("rt_lbvh_accel_bytes", _abi.lib().rt_lbvh_accel_bytes(face_count, C.byref(nb)))
+    return nb.value
+
+
 def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_depth: int = 12, tree_complete: bool = True,
-               morton_bits: int = 32, out: Tree | None = None, stream=None) -> Tree:
+               morton_bits: int = 32, out: Tree | None = None, accel: bool = True, stream=None) -> Tree:
     """LBVH build of a mesh given as float4 vertices (V, 4) and uint4 faces (N, 4).
     hitbox: host sequence of 8 floats (min xyzw, max xyzw) or None for the
     vertices' min/max."""
@@ -120,6 +127,7 @@ def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_de
             faces=torch.empty((n, 4), dtype=torch.int32, device=dev),
             tris=torch.empty((n, 12), dtype=torch.float32, device=dev),
             info=torch.zeros(8, dtype=torch.int32, device=dev),
+            accel=torch.empty(accel_bytes(n), dtype=torch.uint8, device=dev) if (accel and tree_complete) else None,
         )
     scratch = _SCRATCH.get(nbytes, dev)
     hb = None
@@ -142,13 +150,16 @@ def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_de
     d.info = out.info.data_ptr()
     d.scratch = scratch.data_ptr()
     d.scratch_bytes = scratch.numel()
+    if out.accel is not None:
+        d.accel = out.accel.data_ptr()
+        d.accel_bytes = out.accel.numel()
     _abi.check("rt_lbvh_build", _abi.lib().rt_lbvh_build(C.byref(d), _stream(stream)))
     return out
 
 
 def trace(tree: Tree, orig: torch.Tensor, dir: torch.Tensor, tmax: torch.Tensor | None = None, id_mode: int = 0,
           counters: bool = False, use_tris: bool = True, vertices: torch.Tensor | None = None, out: dict | None = None,
-          ray_count: int | None = None, stream=None) -> dict:
+          ray_count: int | None = None, use_accel: bool = True, stream=None) -> dict:
     """Closest hit per ray. Returns dict(id=int32, t=float32, uv=float32 (R, 2), err=int32 (1,))."""
     _need_cuda(orig, "orig", _F32, 4)
     _need_cuda(dir, "dir", _F32, 4)
@@ -182,6 +193,9 @@ def trace(tree: Tree, orig: torch.Tensor, dir: torch.Tensor, tmax: torch.Tensor 
         d.ray_visits = out["visits"].data_ptr()
         d.ray_tests = out["tests"].data_ptr()
     d.error_word = out["err"].data_ptr()
+    if use_accel and use_tris and tree.accel is not None:
+        d.accel = tree.accel.data_ptr()
+        d.face_count_hint = tree.faces.shape[0]
     _abi.check("rt_trace_closest", _abi.lib().rt_trace_closest(C.byref(d), _stream(stream)))
     return out
 

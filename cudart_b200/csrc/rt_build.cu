@@ -79,14 +79,25 @@ __global__ __launch_bounds__(256) void k_hitbox_partial(const float4* __restrict
 }
 
 __global__ void k_hitbox_final(const float4* __restrict__ partial, uint32_t parts, float4* __restrict__ hit) {
-  if (threadIdx.x != 0) return;
+  // one warp: strided accumulation, then a shuffle reduction
   float4 mn = make_float4(kHuge, kHuge, kHuge, kHuge), mx = make_float4(-kHuge, -kHuge, -kHuge, -kHuge);
-  for (uint32_t i = 0; i < parts; ++i) {
+  for (uint32_t i = threadIdx.x; i < parts; i += 32) {
     mn = f4min(mn, partial[2 * i]);
     mx = f4max(mx, partial[2 * i + 1]);
   }
-  hit[0] = mn;
-  hit[1] = mx;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    float4 omn = make_float4(__shfl_xor_sync(0xffffffffu, mn.x, o), __shfl_xor_sync(0xffffffffu, mn.y, o),
+                             __shfl_xor_sync(0xffffffffu, mn.z, o), __shfl_xor_sync(0xffffffffu, mn.w, o));
+    float4 omx = make_float4(__shfl_xor_sync(0xffffffffu, mx.x, o), __shfl_xor_sync(0xffffffffu, mx.y, o),
+                             __shfl_xor_sync(0xffffffffu, mx.z, o), __shfl_xor_sync(0xffffffffu, mx.w, o));
+    mn = f4min(mn, omn);
+    mx = f4max(mx, omx);
+  }
+  if (threadIdx.x == 0) {
+    hit[0] = mn;
+    hit[1] = mx;
+  }
 }
 
 // ----------------------------------------------------------------------------
@@ -417,9 +428,23 @@ struct LeafArgs {
   uint32_t max_leaf;
   const uint32_t* hdr;
   uint32_t* err;
+  // traversal blob (optional): leaf table in leaf order, 8-triangle group boxes
+  uint4* acc_leaves;
+  float4* acc_groups;
+  uint32_t* leaf_lambda;  // node id -> leaf order index
 };
 
 constexpr int kMaxMedianDepth = 40;
+constexpr float kAccelPad = 1.220703125e-4f;  // 2^-13 of the largest coordinate magnitude per axis
+
+// Box padded for the traversal's conservative slab test.
+__device__ __forceinline__ void pad_box(float3& mn, float3& mx) {
+  const float px = fmax_sel(fabsf(mn.x), fabsf(mx.x)) * kAccelPad;
+  const float py = fmax_sel(fabsf(mn.y), fabsf(mx.y)) * kAccelPad;
+  const float pz = fmax_sel(fabsf(mn.z), fabsf(mx.z)) * kAccelPad;
+  mn.x = mn.x - px; mn.y = mn.y - py; mn.z = mn.z - pz;
+  mx.x = mx.x + px; mx.y = mx.y + py; mx.z = mx.z + pz;
+}
 
 __device__ __forceinline__ void write_box(uint32_t* node, float3 mn, float3 mx) {
   float* f = (float*)node;
@@ -471,24 +496,48 @@ __global__ __launch_bounds__(256) void k_leaves(LeafArgs A) {
     cnt = __shfl_sync(0xffffffffu, cnt, 0);
 
     float3 mn = make_float3(kHuge, kHuge, kHuge), mx = make_float3(-kHuge, -kHuge, -kHuge);
-    for (uint32_t i = first + lane; i < first + cnt; i += 32) {
-      const uint32_t orig = __ldg(A.indices + i);
-      const uint4 f = ldg4(A.faces_in + orig);
-      const float4 v0 = ldg4(A.verts + f.x), v1 = ldg4(A.verts + f.y), v2 = ldg4(A.verts + f.z);
-      if (A.faces_out) A.faces_out[i] = f;
-      if (A.tris) {
-        float4 e1 = make_float4(v1.x - v0.x, v1.y - v0.y, v1.z - v0.z, 0.0f);
-        float4 e2 = make_float4(v2.x - v0.x, v2.y - v0.y, v2.z - v0.z, 0.0f);
-        A.tris[3 * (size_t)i + 0] = make_float4(v0.x, v0.y, v0.z, 0.0f);
-        A.tris[3 * (size_t)i + 1] = e1;
-        A.tris[3 * (size_t)i + 2] = e2;
+    const uint32_t gbase = (first >> 3) + g;  // leaf g's groups: disjoint across leaves, no scan needed
+    if (A.acc_leaves && lane == 0) {
+      A.acc_leaves[g] = make_uint4(first, cnt, gbase, leaf_id);
+      A.leaf_lambda[leaf_id] = g;
+    }
+    for (uint32_t base = 0; base < cnt; base += 32) {
+      const uint32_t i = first + base + lane;
+      float3 tmn = make_float3(kHuge, kHuge, kHuge), tmx = make_float3(-kHuge, -kHuge, -kHuge);
+      if (base + lane < cnt) {
+        const uint32_t orig = __ldg(A.indices + i);
+        const uint4 f = ldg4(A.faces_in + orig);
+        const float4 v0 = ldg4(A.verts + f.x), v1 = ldg4(A.verts + f.y), v2 = ldg4(A.verts + f.z);
+        if (A.faces_out) A.faces_out[i] = f;
+        if (A.tris) {
+          float4 e1 = make_float4(v1.x - v0.x, v1.y - v0.y, v1.z - v0.z, 0.0f);
+          float4 e2 = make_float4(v2.x - v0.x, v2.y - v0.y, v2.z - v0.z, 0.0f);
+          A.tris[3 * (size_t)i + 0] = make_float4(v0.x, v0.y, v0.z, 0.0f);
+          A.tris[3 * (size_t)i + 1] = e1;
+          A.tris[3 * (size_t)i + 2] = e2;
+        }
+        tmn = make_float3(fmin_sel(fmin_sel(v0.x, v1.x), v2.x), fmin_sel(fmin_sel(v0.y, v1.y), v2.y), fmin_sel(fmin_sel(v0.z, v1.z), v2.z));
+        tmx = make_float3(fmax_sel(fmax_sel(v0.x, v1.x), v2.x), fmax_sel(fmax_sel(v0.y, v1.y), v2.y), fmax_sel(fmax_sel(v0.z, v1.z), v2.z));
       }
-      mn.x = fmin_sel(mn.x, fmin_sel(fmin_sel(v0.x, v1.x), v2.x));
-      mn.y = fmin_sel(mn.y, fmin_sel(fmin_sel(v0.y, v1.y), v2.y));
-      mn.z = fmin_sel(mn.z, fmin_sel(fmin_sel(v0.z, v1.z), v2.z));
-      mx.x = fmax_sel(mx.x, fmax_sel(fmax_sel(v0.x, v1.x), v2.x));
-      mx.y = fmax_sel(mx.y, fmax_sel(fmax_sel(v0.y, v1.y), v2.y));
-      mx.z = fmax_sel(mx.z, fmax_sel(fmax_sel(v0.z, v1.z), v2.z));
+      mn = make_float3(fmin_sel(mn.x, tmn.x), fmin_sel(mn.y, tmn.y), fmin_sel(mn.z, tmn.z));
+      mx = make_float3(fmax_sel(mx.x, tmx.x), fmax_sel(mx.y, tmx.y), fmax_sel(mx.z, tmx.z));
+      if (A.acc_groups) {
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+          tmn.x = fmin_sel(tmn.x, __shfl_xor_sync(0xffffffffu, tmn.x, o));
+          tmn.y = fmin_sel(tmn.y, __shfl_xor_sync(0xffffffffu, tmn.y, o));
+          tmn.z = fmin_sel(tmn.z, __shfl_xor_sync(0xffffffffu, tmn.z, o));
+          tmx.x = fmax_sel(tmx.x, __shfl_xor_sync(0xffffffffu, tmx.x, o));
+          tmx.y = fmax_sel(tmx.y, __shfl_xor_sync(0xffffffffu, tmx.y, o));
+          tmx.z = fmax_sel(tmx.z, __shfl_xor_sync(0xffffffffu, tmx.z, o));
+        }
+        if ((lane & 7u) == 0 && base + lane < cnt) {
+          pad_box(tmn, tmx);
+          const size_t gi = (size_t)gbase + ((base + lane) >> 3);
+          A.acc_groups[2 * gi] = make_float4(tmn.x, tmn.y, tmn.z, 0.0f);
+          A.acc_groups[2 * gi + 1] = make_float4(tmx.x, tmx.y, tmx.z, 0.0f);
+        }
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -538,6 +587,42 @@ __global__ __launch_bounds__(256) void k_leaves(LeafArgs A) {
   }
 }
 
+// Two-child traversal records, indexed by pre-order rank (internal node p
+// with left child c has rank (c - 1) / 2): both children's padded boxes and
+// references (rank for an internal child, ~leaf index for a leaf child).
+__global__ __launch_bounds__(256) void k_accel_nodes(const uint32_t* __restrict__ nodes, const uint32_t* __restrict__ hdr,
+                                                    const uint32_t* __restrict__ leaf_lambda, float4* __restrict__ tnodes,
+                                                    uint32_t* __restrict__ acc_hdr) {
+  const uint32_t node_count = hdr[2];
+  if (hdr[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const bool root_leaf = (nodes[0] & 1u) != 0;
+    acc_hdr[0] = root_leaf ? ~0u : 0u;  // root reference
+    acc_hdr[1] = hdr[0];                // leaf count
+    acc_hdr[2] = node_count;
+  }
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < node_count; p += gridDim.x * blockDim.x) {
+    const uint2 w = *(const uint2*)(nodes + 8 * (size_t)p);
+    if (w.x & 1u) continue;
+    const uint32_t rank = (w.y - 1u) >> 1;
+    float4 out[4];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const uint32_t c = w.y + side;
+      const uint32_t* cn = nodes + 8 * (size_t)c;
+      const uint32_t cw0 = cn[0], cw1 = cn[1];
+      float3 mn = make_float3(__uint_as_float(cn[2]), __uint_as_float(cn[3]), __uint_as_float(cn[4]));
+      float3 mx = make_float3(__uint_as_float(cn[5]), __uint_as_float(cn[6]), __uint_as_float(cn[7]));
+      pad_box(mn, mx);
+      const uint32_t ref = (cw0 & 1u) ? ~leaf_lambda[c] : ((cw1 - 1u) >> 1);
+      out[2 * side] = make_float4(mn.x, mn.y, mn.z, __uint_as_float(ref));
+      out[2 * side + 1] = make_float4(mx.x, mx.y, mx.z, 0.0f);
+    }
+    float4* dst = tnodes + 4 * (size_t)rank;
+    dst[0] = out[0]; dst[1] = out[1]; dst[2] = out[2]; dst[3] = out[3];
+  }
+}
+
 __global__ void k_write_info(const uint32_t* __restrict__ hdr, const uint32_t* __restrict__ err, rt_build_info* info) {
   if (threadIdx.x != 0) return;
   info->leaf_count = hdr[0];
@@ -568,10 +653,27 @@ struct BuildLayout {
   uint32_t* arrive;
   uint32_t* hdr;
   uint32_t* err;
+  uint32_t* leaf_lambda;
   uint4* faces_tmp;
 };
 
 constexpr uint32_t kHitParts = 296;
+
+// Traversal blob: header (256 B), internal-node records (64 B, <= N - 1),
+// leaf table (16 B, <= N), group boxes (32 B, <= N/8 + N).
+struct AccelLayout {
+  uint32_t* hdr;
+  float4* tnodes;
+  uint4* leaves;
+  float4* groups;
+};
+size_t carve_accel(Carve& c, AccelLayout& A, uint32_t n) {
+  A.hdr = c.take<uint32_t>(64);
+  A.tnodes = c.take<float4>(4 * (size_t)n);
+  A.leaves = c.take<uint4>(n);
+  A.groups = c.take<float4>(2 * ((size_t)n / 8 + n + 1));
+  return c.off + 256;
+}
 
 uint32_t morton_cap(uint32_t n, uint32_t D) {
   uint64_t a = (D >= 31) ? (1ull << 32) : ((1ull << (D + 1)) - 1);
@@ -601,6 +703,7 @@ size_t carve_build(Carve& c, BuildLayout& L, uint32_t n, uint32_t D, bool need_c
   L.arrive = c.take<uint32_t>(L.max_nodes);
   L.hdr = c.take<uint32_t>(16);
   L.err = c.take<uint32_t>(4);
+  L.leaf_lambda = c.take<uint32_t>(L.max_nodes);
   L.faces_tmp = need_faces_tmp ? c.take<uint4>(n) : nullptr;
   return c.off + 256;
 }
@@ -638,6 +741,14 @@ extern "C" rt_status rt_lbvh_scratch_bytes(uint32_t face_count, const rt_build_p
   BuildLayout L;
   *scratch_bytes = carve_build(c, L, face_count, q.tree_depth, true, true);
   if (max_nodes) *max_nodes = 2 * face_count - 1;
+  return RT_OK;
+}
+
+extern "C" rt_status rt_lbvh_accel_bytes(uint32_t face_count, size_t* bytes) {
+  if (!bytes || face_count == 0) return RT_ERR_INVALID_ARGUMENT;
+  Carve c(nullptr, 0);
+  AccelLayout A;
+  *bytes = carve_accel(c, A, face_count);
   return RT_OK;
 }
 
@@ -717,9 +828,24 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
     A.tris = complete ? (float4*)d->tris : nullptr;
     A.indices = d->indices; A.ml_lambda = L.ml_lambda; A.ml_rec = L.ml_rec; A.ml_rank = L.ml_rank; A.parent_id = L.parent_id;
     A.arrive = L.arrive; A.nodes = d->nodes; A.max_nodes = d->max_nodes; A.max_leaf = q.max_leaf; A.hdr = L.hdr; A.err = L.err;
+    AccelLayout AL{};
+    const bool accel = complete && d->accel && d->tris;
+    if (accel) {
+      Carve ca(d->accel, d->accel_bytes);
+      carve_accel(ca, AL, n);
+      if (!ca.ok()) return RT_ERR_SCRATCH_TOO_SMALL;
+    }
+    A.acc_leaves = accel ? AL.leaves : nullptr;
+    A.acc_groups = accel ? AL.groups : nullptr;
+    A.leaf_lambda = L.leaf_lambda;
     k_leaves<<<sms * 8, 256, 0, st>>>(A);
     note_launch();
     RT_CHECK_LAUNCH();
+    if (accel) {
+      k_accel_nodes<<<sms * 4, 256, 0, st>>>(d->nodes, L.hdr, L.leaf_lambda, AL.tnodes, AL.hdr);
+      note_launch();
+      RT_CHECK_LAUNCH();
+    }
   }
   if (in_place && cudaMemcpyAsync(d->faces_out, L.faces_tmp, (size_t)n * 16, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
     return RT_ERR_CUDA;

@@ -154,6 +154,122 @@ __global__ __launch_bounds__(128) void k_trace(TraceArgs A) {
   }
 }
 
+// ----------------------------------------------------------------------------
+// Traversal over the build's blob: two-child records (both children's padded
+// boxes tested together, the nearer child first, the farther pushed with its
+// entry distance so that it is dropped on pop once the best hit is closer),
+// then inside a leaf one padded box per 8 consecutive triangles. Same
+// conservative test and the same (t, position) rule as k_trace, so the hits
+// are identical; only the work differs.
+// Counters: visits = 32-byte box records read (a two-child record counts 2,
+// a group box 1, a leaf-table entry 1), tests = triangles tested.
+// ----------------------------------------------------------------------------
+struct AccelArgs {
+  const float4* tnodes;
+  const uint4* leaves;
+  const float4* groups;
+  const uint32_t* hdr;
+};
+
+__device__ __forceinline__ bool slab2(const float4& mn, const float4& mx, const float4& o, float ix, float iy, float iz, float tbest,
+                                      float& tn) {
+  const float t0x = (mn.x - o.x) * ix, t1x = (mx.x - o.x) * ix;
+  const float t0y = (mn.y - o.y) * iy, t1y = (mx.y - o.y) * iy;
+  const float t0z = (mn.z - o.z) * iz, t1z = (mx.z - o.z) * iz;
+  tn = fmax_sel(fmax_sel(fmin_sel(t0x, t1x), fmin_sel(t0y, t1y)), fmin_sel(t0z, t1z));
+  const float tf = fmin_sel(fmin_sel(fmax_sel(t0x, t1x), fmax_sel(t0y, t1y)), fmax_sel(t0z, t1z));
+  return tn <= tf && tf >= 0.0f && tn <= tbest * kCullSlack;
+}
+
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_trace_accel(TraceArgs A, AccelArgs C) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= A.ray_count) return;
+  const float4 o = ldg4(A.orig + r), d = ldg4(A.dir + r);
+  const float tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
+  int32_t best = -1;
+  float bt = tmax0, bu = 0.0f, bv = 0.0f;
+  uint32_t visits = 0, tests = 0;
+  if (tmax0 > 0.0f) {
+    const float ix = 1.0f / fix_dir(d.x), iy = 1.0f / fix_dir(d.y), iz = 1.0f / fix_dir(d.z);
+    const float zu = o.w * 0.0f, zv = d.w * 0.0f;
+    uint32_t st_ref[kStack];
+    float st_t[kStack];
+    int sp = 0;
+    uint32_t ref = __ldg(C.hdr);
+    for (;;) {
+      if (ref & 0x80000000u) {
+        // leaf
+        const uint4 L = __ldg(C.leaves + (~ref));
+        if (kCount) ++visits;
+        const uint32_t first = L.x, cnt = L.y, gbase = L.z;
+        for (uint32_t g = 0; g * 8 < cnt; ++g) {
+          const float4 gmn = ldg4(C.groups + 2 * ((size_t)gbase + g));
+          const float4 gmx = ldg4(C.groups + 2 * ((size_t)gbase + g) + 1);
+          if (kCount) ++visits;
+          float tg;
+          if (!slab2(gmn, gmx, o, ix, iy, iz, bt, tg)) continue;
+          const uint32_t kend = min(cnt, g * 8 + 8);
+          for (uint32_t k = g * 8; k < kend; ++k) {
+            const uint32_t pos = first + k;
+            const float4 v0 = ldg4(A.tris + 3 * (size_t)pos);
+            const float4 e1 = ldg4(A.tris + 3 * (size_t)pos + 1);
+            const float4 e2 = ldg4(A.tris + 3 * (size_t)pos + 2);
+            if (kCount) ++tests;
+            float t, u, v;
+            if (!mt_test(o, d, zu, zv, v0, e1, e2, t, u, v)) continue;
+            if (t < bt || (best >= 0 && t == bt && (int32_t)pos < best)) {
+              best = (int32_t)pos; bt = t; bu = u; bv = v;
+            }
+          }
+        }
+      } else {
+        const float4* tn = C.tnodes + 4 * (size_t)ref;
+        const float4 a0 = ldg4(tn), a1 = ldg4(tn + 1), b0 = ldg4(tn + 2), b1 = ldg4(tn + 3);
+        if (kCount) visits += 2;
+        float ta, tb;
+        const bool ha = slab2(a0, a1, o, ix, iy, iz, bt, ta);
+        const bool hb = slab2(b0, b1, o, ix, iy, iz, bt, tb);
+        const uint32_t ra = __float_as_uint(a0.w), rb = __float_as_uint(b0.w);
+        if (ha && hb) {
+          const bool a_first = ta <= tb;
+          if (sp < kStack) {
+            st_ref[sp] = a_first ? rb : ra;
+            st_t[sp] = a_first ? tb : ta;
+            ++sp;
+          } else if (A.err) {
+            atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
+          }
+          ref = a_first ? ra : rb;
+          continue;
+        }
+        if (ha) { ref = ra; continue; }
+        if (hb) { ref = rb; continue; }
+      }
+      // pop the next subtree whose entry is still within reach
+      bool found = false;
+      while (sp > 0) {
+        --sp;
+        if (st_t[sp] <= bt * kCullSlack) { ref = st_ref[sp]; found = true; break; }
+      }
+      if (!found) break;
+    }
+  }
+  if (best >= 0) {
+    A.hit_id[r] = A.id_mode == 1 ? (int32_t)__ldg(A.indices + best) : best;
+    A.hit_t[r] = bt;
+    A.hit_uv[r] = make_float2(bu, bv);
+  } else {
+    A.hit_id[r] = -1;
+    A.hit_t[r] = tmax0;
+    A.hit_uv[r] = make_float2(0.0f, 0.0f);
+  }
+  if (kCount) {
+    if (A.visits) A.visits[r] = visits;
+    if (A.tests) A.tests[r] = tests;
+  }
+}
+
 // kernels/CUDA_calcPrimaryRays.cu:20-32
 __global__ __launch_bounds__(256) void k_primary(float4 ro, float4 rd, float4 rx, float4 ry, uint32_t w, uint32_t h,
                                                  float4* __restrict__ orig, float4* __restrict__ dir) {
@@ -267,6 +383,22 @@ extern "C" rt_status rt_trace_closest(const rt_trace_desc* d, rt_stream stream) 
   const bool count = d->ray_visits || d->ray_tests;
   const uint32_t blocks = (d->ray_count + 127) / 128;
   cudaStream_t st = (cudaStream_t)stream;
+  if (d->accel) {
+    if (!d->tris) return RT_ERR_INVALID_ARGUMENT;
+    // blob layout of rt_lbvh_build: header (256 B), records, leaf table, group boxes
+    const size_t n = d->face_count_hint;
+    AccelArgs C;
+    Carve c((void*)d->accel, ~(size_t)0);
+    C.hdr = c.take<uint32_t>(64);
+    C.tnodes = c.take<float4>(4 * n);
+    C.leaves = c.take<uint4>(n);
+    C.groups = c.take<float4>(2 * (n / 8 + n + 1));
+    if (count) k_trace_accel<true><<<blocks, 128, 0, st>>>(A, C);
+    else k_trace_accel<false><<<blocks, 128, 0, st>>>(A, C);
+    note_launch();
+    RT_CHECK_LAUNCH();
+    return RT_OK;
+  }
   if (d->tris) {
     if (count) k_trace<true, true><<<blocks, 128, 0, st>>>(A);
     else k_trace<true, false><<<blocks, 128, 0, st>>>(A);

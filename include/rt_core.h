@@ -84,12 +84,21 @@ typedef struct rt_build_desc {
   rt_build_info* info;      /* device pointer, may be NULL */
   void* scratch;
   size_t scratch_bytes;
+  void* accel;              /* optional traversal blob (needs tris and tree_complete); NULL = not produced */
+  size_t accel_bytes;       /* >= rt_lbvh_accel_bytes */
 } rt_build_desc;
 
 /* Scratch bytes and the node-count bound for an N-face build.
  * Replaces the temporaries CUDA_buildMeshTreeLBVH cudaMalloc'd per call
  * (kernels/CUDA_buildMeshTreeLBVH.cu:462-471). */
 rt_status rt_lbvh_scratch_bytes(uint32_t face_count, const rt_build_params* params, size_t* scratch_bytes, uint32_t* max_nodes);
+
+/* Bytes of the optional traversal blob of an N-face build: two-child records
+ * of the internal nodes (both children's padded boxes, indexed by pre-order
+ * rank), the leaf table, and one padded box per 8 consecutive triangles of a
+ * leaf. Derived from the same tree; the nodes stay the reference's. No
+ * reference counterpart (the reference traverses bvnodes directly). */
+rt_status rt_lbvh_accel_bytes(uint32_t face_count, size_t* bytes);
 
 /* LBVH build: boxes, Morton codes, key+index sort, split lists, topology,
  * node boxes, face reorder and triangle pre-gather.
@@ -152,6 +161,8 @@ typedef struct rt_trace_desc {
   uint32_t* ray_visits;     /* optional out: nodes popped per ray */
   uint32_t* ray_tests;      /* optional out: triangles tested per ray */
   uint32_t* error_word;     /* optional device word: RT_DEVERR_* bits are OR-ed in */
+  const void* accel;        /* optional traversal blob from rt_lbvh_build (with tris): faster, same results */
+  uint32_t face_count_hint; /* the face count the blob was built for (required with accel) */
 } rt_trace_desc;
 
 /* Closest hit per ray: the minimum (t, position) over all triangles that the

@@ -168,8 +168,12 @@ def test_primary_rays_match_oracle(T, oracle, scene):
 
 def _check_trace(T, oracle, tree, ref, o, d, tmax=None, id_mode=0, use_tris=True, vertices=None, sel=None):
     from cudart_b200 import core
-    out = core.trace(tree, o, d, tmax=tmax, id_mode=id_mode, counters=True, use_tris=use_tris, vertices=vertices)
+    out = core.trace(tree, o, d, tmax=tmax, id_mode=id_mode, counters=True, use_tris=use_tris, vertices=vertices, use_accel=False)
+    fast = core.trace(tree, o, d, tmax=tmax, id_mode=id_mode, use_tris=use_tris, vertices=vertices, use_accel=True)
     T.cuda.synchronize()
+    # the traversal-blob path returns the same bits as the reference-node walk
+    assert T.equal(fast["id"], out["id"]) and T.equal(fast["t"], out["t"]) and T.equal(fast["uv"], out["uv"])
+    assert int(_host(fast["err"])[0]) == 0
     oo, dd = _host(o), _host(d)
     tm = None if tmax is None else _host(tmax)
     e = oracle.trace(ref["nodes"], ref["tris"], ref["indices"], oo, dd, tm, mode=0, id_mode=id_mode, counters=True)
