@@ -21,7 +21,7 @@ DEVERR_MORTON_CAPACITY = 0x4
 # every symbol include/rt_core.h declares
 EXPORTS = (
     "rt_lbvh_scratch_bytes", "rt_lbvh_accel_bytes", "rt_lbvh_build", "rt_mesh_boxes", "rt_reorder_faces", "rt_sort_scratch_bytes",
-    "rt_radix_sort_pairs", "rt_radix_sort_keys", "rt_camera_look_at", "rt_camera_basis", "rt_primary_rays",
+    "rt_radix_sort_pairs", "rt_radix_sort_pairs_static", "rt_radix_sort_keys", "rt_camera_look_at", "rt_camera_basis", "rt_primary_rays",
     "rt_trace_closest", "rt_bounce_rays", "rt_status_string", "rt_version", "rt_device_check", "rt_launch_count",
 )
 
@@ -77,6 +77,7 @@ def lib():
         L.rt_reorder_faces.argtypes = [_P, _P, _U32, _P, _P]
         L.rt_sort_scratch_bytes.argtypes = [_U32, C.POINTER(C.c_size_t)]
         L.rt_radix_sort_pairs.argtypes = [_P, _P, _U32, _U32, C.c_int, _P, C.c_size_t, _P]
+        L.rt_radix_sort_pairs_static.argtypes = [_P, _P, _U32, _U32, C.c_int, _P]
         L.rt_radix_sort_keys.argtypes = [_P, _U32, _U32, _P, C.c_size_t, _P]
         L.rt_camera_look_at.argtypes = [C.POINTER(Camera), C.POINTER(C.c_float)]
         L.rt_camera_basis.argtypes = [C.POINTER(Camera), _U32, _U32, C.POINTER(C.c_float)]

@@ -127,6 +127,21 @@ rt_status rt_radix_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t n, uint
  * CUDA_bitonicSort<uint> (kernels/CUDA_bitonicSort.cu:403). */
 rt_status rt_radix_sort_keys(uint32_t* keys, uint32_t n, uint32_t bit_depth, void* scratch, size_t scratch_bytes, rt_stream stream);
 
+/* Allocation-free variant of rt_radix_sort_pairs, for callers that cannot
+ * allocate device memory where they sort (a plug-in whose host application
+ * owns every device allocation; a frame loop that cannot afford cudaMalloc /
+ * cudaFree, which may synchronize the device). No counterpart in the
+ * reference. Same results as rt_radix_sort_pairs. Its scratch is a
+ * RT_STATIC_SORT_SCRATCH_BYTES array inside the library that every GPU using
+ * the library holds until the process exits; n above RT_STATIC_SORT_MAX_N is
+ * refused with RT_ERR_CAPACITY. The first call on a device looks up the
+ * array's device address (make it before any stream capture). All calls share
+ * the array: calls that overlap on the GPU race and must be serialized. */
+#define RT_STATIC_SORT_MAX_N (1u << 20)
+#define RT_STATIC_SORT_SCRATCH_BYTES ((8u << 20) + (272u << 10))
+rt_status rt_radix_sort_pairs_static(uint32_t* keys, uint32_t* values, uint32_t n, uint32_t bit_depth, int init_values,
+                                     rt_stream stream);
+
 /* Camera state of CUDACamera (CUDACamera.h:15-321) that ray generation reads. */
 typedef struct rt_camera {
   float center[3];
