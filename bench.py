@@ -40,13 +40,14 @@ L2_FLUSH_BYTES = 512 << 20  # > 126 MB L2
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--faces", type=int, default=1 << 20)
     ap.add_argument("--build16m", type=int, default=1, help="also time the LBVH build alone on a 2^24-face soup")
+    ap.add_argument("--batch", type=int, default=1, help="also time the batched workload (1024 meshes, CUDA graph)")
     return ap.parse_args()
 
 
@@ -70,7 +71,9 @@ def load_traffic(kernel: str):
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons (every 20 ms, from
+    before the timed region until after it); the summary keeps the samples
+    taken inside the timed window (or the nearest one when the window is short)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -78,39 +81,59 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
+        self.samples = []  # (monotonic time, sm_mhz, max_mhz, reason flags)
+        self.t0 = self.t1 = None
 
-    def __enter__(self):
-        try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except Exception:
-            self.proc = None
-        return self
-
-    def __exit__(self, *a):
-        self.out = ""
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.out, _ = self.proc.communicate(timeout=5)
-            except Exception:
-                self.proc.kill()
-
-    def summary(self):
-        rows = []
-        for line in (self.out or "").strip().splitlines():
+    def _reader(self):
+        for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
             try:
-                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                self.samples.append((time.monotonic(), float(parts[1]), float(parts[2]), parts[5:9]))
             except ValueError:
                 continue
-        if not rows:
+
+    def start(self):
+        import threading
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return self
+        self.thread = threading.Thread(target=self._reader, daemon=True)
+        self.thread.start()
+        deadline = time.monotonic() + 10.0
+        while not self.samples and time.monotonic() < deadline:
+            time.sleep(0.01)
+        return self
+
+    def __enter__(self):
+        self.t0 = time.monotonic()
+        return self
+
+    def __exit__(self, *a):
+        self.t1 = time.monotonic()
+        time.sleep(0.05)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples or self.t0 is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        rows = [r for r in self.samples if self.t0 <= r[0] <= self.t1]
+        if not rows:
+            rows = [min(self.samples, key=lambda r: abs(r[0] - self.t1))]
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
-        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+        reasons = sorted({names[i] for _, _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[1] for r in rows), "sm_max_mhz": max(r[2] for r in rows), "reasons": reasons,
                 "samples": len(rows)}
 
 
@@ -141,6 +164,10 @@ def run_ours(args, rank, world, local_rank):
     bounce = core.bounce_rays(tree.tris, rays[0], rays[1], hits1["id"], hits1["t"], SEED_BOUNCE)
     hits2 = core.trace(tree, bounce[0], bounce[1], tmax=bounce[2])
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    # autotune the traversal schedule on this workload's rays (untimed); results never depend on it
+    from cudart_b200 import tune
+    sched1, tim1 = tune.tune_trace(tree, rays[0], rays[1], image_width=W, key=f"soup{N}-primary", use_cache=False)
+    sched2, tim2 = tune.tune_trace(tree, bounce[0], bounce[1], tmax=bounce[2], image_width=W, key=f"soup{N}-bounce", use_cache=False)
 
     def step(ev):
         ev[0].record(stream)
@@ -148,11 +175,11 @@ def run_ours(args, rank, world, local_rank):
         ev[1].record(stream)
         core.primary_rays(camera, W, H, out=rays)
         ev[2].record(stream)
-        core.trace(tree, rays[0], rays[1], out=hits1)
+        core.trace(tree, rays[0], rays[1], out=hits1, schedule=sched1)
         ev[3].record(stream)
         core.bounce_rays(tree.tris, rays[0], rays[1], hits1["id"], hits1["t"], SEED_BOUNCE, out=bounce)
         ev[4].record(stream)
-        core.trace(tree, bounce[0], bounce[1], tmax=bounce[2], out=hits2)
+        core.trace(tree, bounce[0], bounce[1], tmax=bounce[2], out=hits2, schedule=sched2)
         ev[5].record(stream)
 
     def new_events():
@@ -185,7 +212,8 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     launches0 = _abi.lib().rt_launch_count()
     evs = []
-    with ClockSampler(local_rank) as clk:
+    sampler = ClockSampler(local_rank).start()
+    with sampler as clk:
         t_wall = time.perf_counter()
         for _ in range(args.steps):
             flush.zero_()  # L2 flush between timed steps (outside the event brackets)
@@ -235,7 +263,9 @@ def run_ours(args, rank, world, local_rank):
                   "leaf_count": info["leaf_count"], "real_depth": info["real_depth"]},
         "trace": {"ms": round(trace_ms / K, 4), "primary_ms": round(trace1_ms / K, 4), "bounce_ms": round(trace2_ms / K, 4),
                   "primary_hits": n_primary_hits, "mean_visits": round(vis / (2 * R), 3), "mean_tests": round(tst / (2 * R), 3),
-                  "counted_run_identical": bool(same)},
+                  "counted_run_identical": bool(same), "schedule_primary": sched1, "schedule_bounce": sched2,
+                  "tuning_ms_primary": {json.dumps(k, sort_keys=True): round(v, 4) for k, v in tim1},
+                  "tuning_ms_bounce": {json.dumps(k, sort_keys=True): round(v, 4) for k, v in tim2}},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
@@ -244,13 +274,18 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "wall_s_timed": round(t_wall, 3),
     }
-    if args.build16m:
+    if args.build16m or args.batch:
         del flush
+    if args.build16m:
         result["build_16m"] = build_only(24, args, dev, world)
+    if args.batch:
+        result["batch_c2"] = batched(args, dev, world)
     clocks = clk.summary()
-    result["clocks"] = {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]}
+    sampler.stop()
+    result["clocks"] = {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
+                        "samples": clocks["samples"]}
     if not args.no_e2e:
-        result["e2e"] = run_e2e(args, mesh, camera, W, H, dev, world)
+        result["e2e"] = run_e2e(args, mesh, camera, W, H, dev, world, sched1, sched2)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(mesh, cam, budget_s=12.0)
     return result
@@ -293,7 +328,96 @@ def build_only(log2n, args, dev, world):
             "node_count": info["node_count"], "reps": reps}
 
 
-def run_e2e(args, mesh, camera, W, H, dev, world):
+def batched(args, dev, world, count=1024):
+    """1024 independent meshes (face counts log-uniform in [64, 65536], terrain or
+    soup by coin flip), each with side x side rays (side log-uniform in
+    [64, 512]) from its bounding sphere aimed uniformly inward. One batched
+    build (all meshes) and one batched trace (all rays), captured together in a
+    CUDA graph and replayed; CUDA events around each replay."""
+    import math
+
+    import torch
+
+    from cudart_b200 import core, scenes
+
+    meshes = scenes.batch_meshes(count, seed=3)
+    verts, faces, fo, vo = scenes.concat_batch(meshes)
+    rng = np.random.default_rng(11)
+    sides = np.exp(rng.uniform(math.log(64), math.log(512), count)).astype(np.int64)
+    counts = sides * sides
+    ro = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    centers, radii = [], []
+    for m in meshes:
+        v = m.vertices[:, :3].astype(np.float64)
+        c = 0.5 * (v.min(0) + v.max(0))
+        centers.append(c)
+        radii.append(max(float(np.linalg.norm(v - c, axis=1).max()), 1e-6) * 1.01)
+    R = int(ro[-1])
+    del meshes
+    V = torch.from_numpy(verts).to(dev)
+    Fc = torch.from_numpy(faces.view(np.int32)).to(dev)
+    mesh_of_ray = torch.repeat_interleave(torch.arange(count, device=dev), torch.from_numpy(counts).to(dev))
+    cen = torch.tensor(np.array(centers), dtype=torch.float64, device=dev)[mesh_of_ray]
+    rad = torch.tensor(radii, dtype=torch.float64, device=dev)[mesh_of_ray].unsqueeze(1)
+    g = torch.Generator(device=dev).manual_seed(5)
+    p = torch.randn((R, 3), generator=g, device=dev, dtype=torch.float64)
+    p = p / p.norm(dim=1, keepdim=True)
+    q = torch.randn((R, 3), generator=g, device=dev, dtype=torch.float64)
+    q = q / q.norm(dim=1, keepdim=True) * torch.rand((R, 1), generator=g, device=dev, dtype=torch.float64).pow(1.0 / 3.0)
+    orig = torch.zeros((R, 4), dtype=torch.float32, device=dev)
+    dirs = torch.zeros((R, 4), dtype=torch.float32, device=dev)
+    orig[:, :3] = (cen + rad * p).float()
+    dirs[:, :3] = ((cen + rad * q) - (cen + rad * p)).float()
+    del p, q, cen, rad, mesh_of_ray
+    roff = torch.tensor(ro.astype(np.int32), device=dev)
+    tree = core.batch_build(V, Fc, fo, vo)
+    hits = core.batch_trace(tree, orig, dirs, roff)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    cap = torch.cuda.Stream()
+    cap.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(cap):
+        core.batch_build(V, Fc, fo, vo, out=tree)
+        core.batch_trace(tree, orig, dirs, roff, out=hits)
+        torch.cuda.synchronize()
+        with torch.cuda.graph(graph, stream=cap):
+            core.batch_build(V, Fc, fo, vo, out=tree)
+            core.batch_trace(tree, orig, dirs, roff, out=hits)
+    torch.cuda.current_stream().wait_stream(cap)
+    torch.cuda.synchronize()
+    reps = 3
+    for _ in range(2):
+        graph.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    graph_ms = e0.elapsed_time(e1) / reps
+    # build and trace separately (plain launches) for the split
+    b0, b1, t1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    b0.record()
+    core.batch_build(V, Fc, fo, vo, out=tree)
+    b1.record()
+    core.batch_trace(tree, orig, dirs, roff, out=hits)
+    t1.record()
+    torch.cuda.synchronize()
+    build_ms, trace_ms = b0.elapsed_time(b1), b1.elapsed_time(t1)
+    info = tree.info.cpu().numpy()
+    hit_frac = float((hits["id"] >= 0).float().mean().item())
+    N = int(fo[-1])
+    res = {"meshes": count, "faces": N, "rays": R, "graph_ms_per_step": round(graph_ms, 4),
+           "graph_mrays_s": round(world * R / (graph_ms * 1e-3) / 1e6, 2), "build_ms": round(build_ms, 4),
+           "build_mtri_s": round(world * N / (build_ms * 1e-3) / 1e6, 2), "trace_ms": round(trace_ms, 4),
+           "trace_mrays_s": round(world * R / (trace_ms * 1e-3) / 1e6, 2), "hit_fraction": round(hit_frac, 4),
+           "device_errors": int((info[:, 7] != 0).sum()), "graph": "build + trace captured in one CUDA graph"}
+    del graph
+    return res
+
+
+def run_e2e(args, mesh, camera, W, H, dev, world, sched1=None, sched2=None):
     """Same metric through the public API with host buffers: pinned host mesh ->
     device, build, rays, trace, bounce, trace, hits -> pinned host, every step."""
     import torch
@@ -322,9 +446,9 @@ def run_e2e(args, mesh, camera, W, H, dev, world):
         f.copy_(fh, non_blocking=True)
         core.build_lbvh(v, f, out=tree)
         core.primary_rays(camera, W, H, out=rays)
-        core.trace(tree, rays[0], rays[1], out=h1)
+        core.trace(tree, rays[0], rays[1], out=h1, schedule=sched1)
         core.bounce_rays(tree.tris, rays[0], rays[1], h1["id"], h1["t"], SEED_BOUNCE, out=b)
-        core.trace(tree, b[0], b[1], tmax=b[2], out=h2)
+        core.trace(tree, b[0], b[1], tmax=b[2], out=h2, schedule=sched2)
         for i, h in enumerate((h1, h2)):
             out_id[i].copy_(h["id"], non_blocking=True)
             out_t[i].copy_(h["t"], non_blocking=True)

@@ -12,17 +12,21 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librt_core.so")
 
 RT_OK = 0
+ABI_VERSION = 5  # RT_ABI_VERSION of include/rt_core.h that the structs below mirror
 STATUS_NAMES = {0: "RT_OK", 1: "RT_ERR_INVALID_ARGUMENT", 2: "RT_ERR_NO_DEVICE", 3: "RT_ERR_CUDA",
                 4: "RT_ERR_SCRATCH_TOO_SMALL", 5: "RT_ERR_CAPACITY", 6: "RT_ERR_UNSUPPORTED"}
 DEVERR_NODE_CAPACITY = 0x1
 DEVERR_STACK_OVERFLOW = 0x2
 DEVERR_MORTON_CAPACITY = 0x4
+TRACE_WHILE_WHILE = 0x1
+TRACE_COOP = 0x2
 
 # every symbol include/rt_core.h declares
 EXPORTS = (
-    "rt_lbvh_scratch_bytes", "rt_lbvh_accel_bytes", "rt_lbvh_build", "rt_mesh_boxes", "rt_reorder_faces", "rt_sort_scratch_bytes",
+    "rt_lbvh_scratch_bytes", "rt_lbvh_accel_bytes", "rt_lbvh_build", "rt_batch_sizes", "rt_batch_build", "rt_batch_trace", "rt_mesh_boxes", "rt_reorder_faces", "rt_sort_scratch_bytes",
     "rt_radix_sort_pairs", "rt_radix_sort_pairs_static", "rt_radix_sort_keys", "rt_camera_look_at", "rt_camera_basis", "rt_primary_rays",
-    "rt_trace_closest", "rt_bounce_rays", "rt_status_string", "rt_version", "rt_device_check", "rt_launch_count",
+    "rt_trace_closest", "rt_ray_order_scratch_bytes", "rt_ray_order", "rt_interpolate", "rt_bounce_rays", "rt_mesh_file_save", "rt_mesh_file_info", "rt_mesh_file_load", "rt_tree_file_save", "rt_tree_file_info",
+    "rt_tree_file_load", "rt_status_string", "rt_version", "rt_abi_version", "rt_device_check", "rt_launch_count",
 )
 
 _P = C.c_void_p
@@ -54,7 +58,39 @@ class BuildDesc(C.Structure):
 class TraceDesc(C.Structure):
     _fields_ = [("nodes", _P), ("tris", _P), ("vertices", _P), ("faces", _P), ("indices", _P), ("orig", _P), ("dir", _P),
                 ("tmax", _P), ("ray_count", _U32), ("id_mode", _U32), ("hit_id", _P), ("hit_t", _P), ("hit_uv", _P),
-                ("ray_visits", _P), ("ray_tests", _P), ("error_word", _P), ("accel", _P), ("face_count_hint", _U32)]
+                ("ray_visits", _P), ("ray_tests", _P), ("error_word", _P), ("accel", _P), ("face_count_hint", _U32),
+                ("image_width", _U32), ("work_counter", _P), ("persistent_blocks_per_sm", _U32), ("schedule", _U32),
+                ("ray_order", _P)]
+
+
+class InterpDesc(C.Structure):
+    _fields_ = [("hit_id", _P), ("hit_uv", _P), ("count", _U32), ("faces", _P), ("vertices", _P), ("normals", _P),
+                ("colors", _P), ("texcoords", _P), ("out_points", _P), ("out_normals", _P), ("out_colors", _P),
+                ("out_texcoords", _P), ("out_materials", _P)]
+
+
+class MeshFile(C.Structure):
+    _fields_ = [("hitbox", C.c_float * 8), ("has_hitbox", C.c_int32), ("vertex_count", _U32), ("normal_count", _U32),
+                ("color_count", _U32), ("texcoord_count", _U32), ("face_count", _U32), ("vertices", _P), ("normals", _P),
+                ("colors", _P), ("texcoords", _P), ("faces", _P)]
+
+
+class TreeFile(C.Structure):
+    _fields_ = [("node_count", _U32), ("index_count", _U32), ("box_count", _U32), ("nodes", _P), ("indices", _P), ("boxes", _P)]
+
+
+class BatchBuildDesc(C.Structure):
+    _fields_ = [("mesh_count", _U32), ("face_count", _U32), ("vertex_count", _U32), ("face_offsets", _P), ("vertex_offsets", _P),
+                ("vertices", _P), ("faces_in", _P), ("faces_out", _P), ("params", BuildParams), ("boxes", _P), ("indices", _P),
+                ("codes", _P), ("nodes", _P), ("tris", _P), ("accel", _P), ("accel_bytes", C.c_size_t), ("info", _P),
+                ("scratch", _P), ("scratch_bytes", C.c_size_t)]
+
+
+class BatchTraceDesc(C.Structure):
+    _fields_ = [("mesh_count", _U32), ("face_offsets", _P), ("ray_offsets", _P), ("accel", _P), ("tris", _P), ("indices", _P),
+                ("face_count", _U32), ("orig", _P), ("dir", _P), ("tmax", _P), ("ray_count", _U32), ("id_mode", _U32),
+                ("hit_id", _P), ("hit_t", _P), ("hit_uv", _P), ("ray_visits", _P), ("ray_tests", _P), ("error_word", _P),
+                ("schedule", _U32)]
 
 
 class Camera(C.Structure):
@@ -73,6 +109,9 @@ def lib():
         L.rt_lbvh_scratch_bytes.argtypes = [_U32, C.POINTER(BuildParams), C.POINTER(C.c_size_t), C.POINTER(_U32)]
         L.rt_lbvh_build.argtypes = [C.POINTER(BuildDesc), _P]
         L.rt_lbvh_accel_bytes.argtypes = [_U32, C.POINTER(C.c_size_t)]
+        L.rt_batch_sizes.argtypes = [_U32, _U32, C.POINTER(BuildParams), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+        L.rt_batch_build.argtypes = [C.POINTER(BatchBuildDesc), _P]
+        L.rt_batch_trace.argtypes = [C.POINTER(BatchTraceDesc), _P]
         L.rt_mesh_boxes.argtypes = [_P, _P, _U32, _P, _P, _P]
         L.rt_reorder_faces.argtypes = [_P, _P, _U32, _P, _P]
         L.rt_sort_scratch_bytes.argtypes = [_U32, C.POINTER(C.c_size_t)]
@@ -83,15 +122,25 @@ def lib():
         L.rt_camera_basis.argtypes = [C.POINTER(Camera), _U32, _U32, C.POINTER(C.c_float)]
         L.rt_primary_rays.argtypes = [C.POINTER(Camera), _U32, _U32, _P, _P, _P]
         L.rt_trace_closest.argtypes = [C.POINTER(TraceDesc), _P]
+        L.rt_interpolate.argtypes = [C.POINTER(InterpDesc), _P]
+        L.rt_ray_order_scratch_bytes.argtypes = [_U32, C.POINTER(C.c_size_t)]
+        L.rt_ray_order.argtypes = [_P, _P, _P, _U32, C.POINTER(C.c_float), _P, _P, C.c_size_t, _P]
         L.rt_bounce_rays.argtypes = [_P, _P, _P, _P, _P, _U32, C.c_uint64, _P, _P, _P, _P]
+        for fn, st in (("mesh", MeshFile), ("tree", TreeFile)):
+            getattr(L, f"rt_{fn}_file_save").argtypes = [C.c_char_p, C.c_int, C.POINTER(st)]
+            getattr(L, f"rt_{fn}_file_info").argtypes = [C.c_char_p, C.POINTER(st)]
+            getattr(L, f"rt_{fn}_file_load").argtypes = [C.c_char_p, C.POINTER(st)]
         L.rt_status_string.restype = C.c_char_p
         L.rt_status_string.argtypes = [C.c_int]
         L.rt_version.restype = _U32
         L.rt_device_check.restype = C.c_int
         L.rt_launch_count.restype = C.c_uint64
+        L.rt_abi_version.restype = _U32
         for name in EXPORTS:
-            if name not in ("rt_status_string", "rt_version", "rt_device_check", "rt_launch_count"):
+            if name not in ("rt_status_string", "rt_version", "rt_abi_version", "rt_device_check", "rt_launch_count"):
                 getattr(L, name).restype = C.c_int
+        if L.rt_abi_version() != ABI_VERSION:
+            raise RuntimeError(f"{LIB_PATH} has struct layout version {L.rt_abi_version()}, these bindings expect {ABI_VERSION}: rebuild")
         _lib = L
     return _lib
 

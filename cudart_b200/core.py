@@ -61,6 +61,22 @@ class _Scratch:
 
 
 _SCRATCH = _Scratch()
+_ORDER_SCRATCH = _Scratch()
+_COUNTERS = {}
+
+# Traversal schedule of the blob path (never changes the results). The
+# autotuner in cudart_b200/tune.py can replace it per device.
+DEFAULT_SCHEDULE = {"image_width": 0, "persistent": False, "blocks_per_sm": 8, "while_while": False}
+
+
+def _work_counter(device, stream=None) -> torch.Tensor:
+    s = torch.cuda.current_stream() if stream is None else stream
+    key = (torch.device(device).index or 0, s.cuda_stream)  # one counter per stream: concurrent traces do not share it
+    c = _COUNTERS.get(key)
+    if c is None:
+        c = torch.zeros(1, dtype=torch.int32, device=device)
+        _COUNTERS[key] = c
+    return c
 
 
 def device_check() -> bool:
@@ -159,7 +175,7 @@ def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_de
 
 def trace(tree: Tree, orig: torch.Tensor, dir: torch.Tensor, tmax: torch.Tensor | None = None, id_mode: int = 0,
           counters: bool = False, use_tris: bool = True, vertices: torch.Tensor | None = None, out: dict | None = None,
-          ray_count: int | None = None, use_accel: bool = True, stream=None) -> dict:
+          ray_count: int | None = None, use_accel: bool = True, schedule: dict | None = None, stream=None) -> dict:
     """Closest hit per ray. Returns dict(id=int32, t=float32, uv=float32 (R, 2), err=int32 (1,))."""
     _need_cuda(orig, "orig", _F32, 4)
     _need_cuda(dir, "dir", _F32, 4)
@@ -196,8 +212,44 @@ def trace(tree: Tree, orig: torch.Tensor, dir: torch.Tensor, tmax: torch.Tensor 
     if use_accel and use_tris and tree.accel is not None:
         d.accel = tree.accel.data_ptr()
         d.face_count_hint = tree.faces.shape[0]
+        sch = DEFAULT_SCHEDULE if schedule is None else schedule
+        d.image_width = int(sch.get("image_width", 0))
+        if sch.get("persistent", False):
+            d.work_counter = _work_counter(dev, stream).data_ptr()
+            d.persistent_blocks_per_sm = int(sch.get("blocks_per_sm", 8))
+        d.schedule = (_abi.TRACE_WHILE_WHILE if sch.get("while_while", False) else 0) | (_abi.TRACE_COOP if sch.get("coop", False) else 0)
+        if sch.get("sorted", False):
+            order = ray_order(orig, dir, tmax, tree_box(tree), ray_count=R, stream=stream)
+            out["_order"] = order  # keep it alive until the trace has run
+            d.ray_order = order.data_ptr()
     _abi.check("rt_trace_closest", _abi.lib().rt_trace_closest(C.byref(d), _stream(stream)))
     return out
+
+
+def tree_box(tree: Tree):
+    """Scene box for ray ordering (host floats), read once from the root node and cached on the tree."""
+    box = getattr(tree, "_box", None)
+    if box is None:
+        root = tree.nodes[0].cpu().view(torch.float32).tolist()
+        box = [root[2], root[3], root[4], root[5], root[6], root[7]]
+        if not all(abs(x) < 1e30 for x in box):  # inverted (flat-z quirk) or empty: fall back to the face boxes
+            b = tree.boxes.view(-1, 8)
+            box = b[:, :3].min(0).values.tolist() + b[:, 4:7].max(0).values.tolist()
+        tree._box = box
+    return box
+
+
+def ray_order(orig, dir, tmax, box, ray_count: int | None = None, stream=None) -> torch.Tensor:
+    """Permutation of the rays sorted by direction octant and origin Morton code (rt_ray_order)."""
+    R = orig.shape[0] if ray_count is None else ray_count
+    nb = C.c_size_t(0)
+    _abi.lib().rt_ray_order_scratch_bytes(R, C.byref(nb))
+    scratch = _ORDER_SCRATCH.get(nb.value, orig.device)
+    order = torch.empty(R, dtype=torch.int32, device=orig.device)
+    b = (C.c_float * 6)(*[float(x) for x in box])
+    _abi.check("rt_ray_order", _abi.lib().rt_ray_order(_p(orig), _p(dir), _p(tmax), R, b, _p(order), _p(scratch), scratch.numel(),
+                                                       _stream(stream)))
+    return order
 
 
 def make_camera(center, target=None, angle=None, fov=3.14159265359 * 0.5, ratio=4.0 / 3.0) -> _abi.Camera:
@@ -274,4 +326,175 @@ def mesh_boxes(vertices, faces, stream=None):
 def reorder_faces(faces, indices, stream=None):
     out = torch.empty_like(faces)
     _abi.check("rt_reorder_faces", _abi.lib().rt_reorder_faces(_p(faces), _p(indices), faces.shape[0], _p(out), _stream(stream)))
+    return out
+
+
+def interpolate(tree: Tree, vertices: torch.Tensor, hits: dict, normals=None, colors=None, texcoords=None,
+                outputs=("points", "normals", "colors", "texcoords", "materials"), stream=None) -> dict:
+    """CUDARaytracer::interpolateOutputSurfaces: per-ray hit point, normal, color,
+    texcoord and material from the trace's (position, u, v) (id_mode 0)."""
+    R = hits["id"].shape[0]
+    dev = vertices.device
+    shapes = {"points": (R, 4), "normals": (R, 4), "colors": (R, 4), "texcoords": (R, 2), "materials": (R,)}
+    out = {k: torch.empty(shapes[k], dtype=torch.int32 if k == "materials" else torch.float32, device=dev) for k in outputs}
+    d = _abi.InterpDesc()
+    d.hit_id = hits["id"].data_ptr()
+    d.hit_uv = hits["uv"].data_ptr()
+    d.count = R
+    d.faces = tree.faces.data_ptr()
+    d.vertices = vertices.data_ptr()
+    d.normals = normals.data_ptr() if normals is not None else None
+    d.colors = colors.data_ptr() if colors is not None else None
+    d.texcoords = texcoords.data_ptr() if texcoords is not None else None
+    for k in outputs:
+        setattr(d, "out_" + k, out[k].data_ptr())
+    _abi.check("rt_interpolate", _abi.lib().rt_interpolate(C.byref(d), _stream(stream)))
+    return out
+
+
+# ----------------------------------------------------------------------------
+# chunk files (CUDAMesh / CUDAMeshTree quickSave / quickLoad)
+# ----------------------------------------------------------------------------
+def mesh_save(path: str, vertices, faces, hitbox, normals=None, colors=None, texcoords=None, overwrite: bool = True):
+    m = _abi.MeshFile()
+    m.hitbox[:] = [float(x) for x in hitbox]
+    m.has_hitbox = 1
+    for name, t in (("vertices", vertices), ("normals", normals), ("colors", colors), ("texcoords", texcoords), ("faces", faces)):
+        if t is not None:
+            setattr(m, name, t.data_ptr())
+            setattr(m, {"vertices": "vertex_count", "normals": "normal_count", "colors": "color_count",
+                        "texcoords": "texcoord_count", "faces": "face_count"}[name], t.shape[0])
+    torch.cuda.synchronize()
+    _abi.check("rt_mesh_file_save", _abi.lib().rt_mesh_file_save(path.encode(), int(overwrite), C.byref(m)))
+
+
+def mesh_load(path: str, device="cuda") -> dict:
+    m = _abi.MeshFile()
+    _abi.check("rt_mesh_file_info", _abi.lib().rt_mesh_file_info(path.encode(), C.byref(m)))
+    out = {"hitbox": list(m.hitbox) if m.has_hitbox else None}
+    spec = (("vertices", "vertex_count", 4, torch.float32), ("normals", "normal_count", 4, torch.float32),
+            ("colors", "color_count", 4, torch.float32), ("texcoords", "texcoord_count", 2, torch.float32),
+            ("faces", "face_count", 4, torch.int32))
+    for name, cnt, cols, dt in spec:
+        n = getattr(m, cnt)
+        if n:
+            t = torch.empty((n, cols), dtype=dt, device=device)
+            setattr(m, name, t.data_ptr())
+            out[name] = t
+    _abi.check("rt_mesh_file_load", _abi.lib().rt_mesh_file_load(path.encode(), C.byref(m)))
+    return out
+
+
+def tree_save(path: str, tree: Tree, overwrite: bool = True):
+    t = _abi.TreeFile()
+    t.node_count = tree.node_count
+    t.index_count = tree.indices.shape[0]
+    t.box_count = tree.boxes.shape[0]
+    t.nodes, t.indices, t.boxes = tree.nodes.data_ptr(), tree.indices.data_ptr(), tree.boxes.data_ptr()
+    torch.cuda.synchronize()
+    _abi.check("rt_tree_file_save", _abi.lib().rt_tree_file_save(path.encode(), int(overwrite), C.byref(t)))
+
+
+def tree_load(path: str, device="cuda") -> dict:
+    t = _abi.TreeFile()
+    _abi.check("rt_tree_file_info", _abi.lib().rt_tree_file_info(path.encode(), C.byref(t)))
+    out = {}
+    for name, cnt, cols, dt in (("nodes", "node_count", 8, torch.int32), ("indices", "index_count", 1, torch.int32),
+                                ("boxes", "box_count", 8, torch.float32)):
+        n = getattr(t, cnt)
+        if n:
+            x = torch.empty((n, cols) if cols > 1 else (n,), dtype=dt, device=device)
+            setattr(t, name, x.data_ptr())
+            out[name] = x
+    _abi.check("rt_tree_file_load", _abi.lib().rt_tree_file_load(path.encode(), C.byref(t)))
+    return out
+
+
+# ----------------------------------------------------------------------------
+# batched meshes (one set of launches for all builds, one launch for all rays)
+# ----------------------------------------------------------------------------
+@dataclass
+class BatchTree:
+    face_offsets: torch.Tensor    # int32 (M + 1,) on the device
+    vertex_offsets: torch.Tensor  # int32 (M + 1,)
+    face_offsets_host: list
+    nodes: torch.Tensor           # int32 (2N - M, 8): mesh m's nodes start at 2 F_m - m
+    boxes: torch.Tensor
+    indices: torch.Tensor         # mesh-local face ids per position
+    codes: torch.Tensor
+    faces: torch.Tensor           # per mesh, Morton order
+    tris: torch.Tensor
+    accel: torch.Tensor
+    info: torch.Tensor            # int32 (M, 8)
+
+    @property
+    def mesh_count(self) -> int:
+        return self.face_offsets.shape[0] - 1
+
+    def mesh_nodes(self, m: int, node_count: int | None = None):
+        F = self.face_offsets_host[m]
+        nc = int(self.info[m, 0].item()) if node_count is None else node_count
+        base = 2 * F - m
+        return self.nodes[base: base + nc]
+
+
+def batch_build(vertices: torch.Tensor, faces: torch.Tensor, face_offsets: list, vertex_offsets: list, tree_depth: int = 12,
+                out: BatchTree | None = None, stream=None) -> BatchTree:
+    """Builds every mesh of a concatenated batch (faces index their own mesh's vertices from 0)."""
+    _need_cuda(vertices, "vertices", _F32, 4)
+    _need_cuda(faces, "faces", _I32, 4)
+    M = len(face_offsets) - 1
+    N = faces.shape[0]
+    dev = vertices.device
+    params = _abi.BuildParams(tree_depth, 1, 0, 0, 32)
+    sb, ab = C.c_size_t(0), C.c_size_t(0)
+    _abi.check("rt_batch_sizes", _abi.lib().rt_batch_sizes(M, N, C.byref(params), C.byref(sb), C.byref(ab)))
+    if out is None:
+        out = BatchTree(
+            face_offsets=torch.tensor(face_offsets, dtype=torch.int32, device=dev),
+            vertex_offsets=torch.tensor(vertex_offsets, dtype=torch.int32, device=dev),
+            face_offsets_host=list(face_offsets),
+            nodes=torch.empty((2 * N - M, 8), dtype=torch.int32, device=dev),
+            boxes=torch.empty((N, 8), dtype=torch.float32, device=dev),
+            indices=torch.empty(N, dtype=torch.int32, device=dev),
+            codes=torch.empty(N, dtype=torch.int32, device=dev),
+            faces=torch.empty((N, 4), dtype=torch.int32, device=dev),
+            tris=torch.empty((N, 12), dtype=torch.float32, device=dev),
+            accel=torch.empty(ab.value, dtype=torch.uint8, device=dev),
+            info=torch.zeros((M, 8), dtype=torch.int32, device=dev),
+        )
+    scratch = _SCRATCH.get(sb.value, dev)
+    d = _abi.BatchBuildDesc()
+    d.mesh_count, d.face_count, d.vertex_count = M, N, vertices.shape[0]
+    d.face_offsets, d.vertex_offsets = out.face_offsets.data_ptr(), out.vertex_offsets.data_ptr()
+    d.vertices, d.faces_in, d.faces_out = vertices.data_ptr(), faces.data_ptr(), out.faces.data_ptr()
+    d.params = params
+    d.boxes, d.indices, d.codes, d.nodes = out.boxes.data_ptr(), out.indices.data_ptr(), out.codes.data_ptr(), out.nodes.data_ptr()
+    d.tris, d.accel, d.accel_bytes = out.tris.data_ptr(), out.accel.data_ptr(), out.accel.numel()
+    d.info, d.scratch, d.scratch_bytes = out.info.data_ptr(), scratch.data_ptr(), scratch.numel()
+    _abi.check("rt_batch_build", _abi.lib().rt_batch_build(C.byref(d), _stream(stream)))
+    return out
+
+
+def batch_trace(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax=None, id_mode: int = 0, counters: bool = False,
+                while_while: bool = True, out: dict | None = None, stream=None) -> dict:
+    """Closest hits for the rays of all meshes (rays of mesh m: ray_offsets[m] .. ray_offsets[m+1])."""
+    R = orig.shape[0]
+    dev = orig.device
+    if out is None:
+        out = dict(id=torch.empty(R, dtype=torch.int32, device=dev), t=torch.empty(R, dtype=torch.float32, device=dev),
+                   uv=torch.empty((R, 2), dtype=torch.float32, device=dev), err=torch.zeros(1, dtype=torch.int32, device=dev))
+        if counters:
+            out["visits"] = torch.empty(R, dtype=torch.int32, device=dev)
+            out["tests"] = torch.empty(R, dtype=torch.int32, device=dev)
+    d = _abi.BatchTraceDesc()
+    d.mesh_count = tree.mesh_count
+    d.face_offsets, d.ray_offsets = tree.face_offsets.data_ptr(), ray_offsets.data_ptr()
+    d.accel, d.tris, d.indices, d.face_count = tree.accel.data_ptr(), tree.tris.data_ptr(), tree.indices.data_ptr(), tree.faces.shape[0]
+    d.orig, d.dir, d.tmax, d.ray_count, d.id_mode = orig.data_ptr(), dir.data_ptr(), _p(tmax), R, id_mode
+    d.hit_id, d.hit_t, d.hit_uv, d.error_word = out["id"].data_ptr(), out["t"].data_ptr(), out["uv"].data_ptr(), out["err"].data_ptr()
+    if "visits" in out:
+        d.ray_visits, d.ray_tests = out["visits"].data_ptr(), out["tests"].data_ptr()
+    d.schedule = _abi.TRACE_WHILE_WHILE if while_while else 0
+    _abi.check("rt_batch_trace", _abi.lib().rt_batch_trace(C.byref(d), _stream(stream)))
     return out

@@ -37,12 +37,11 @@
 // or after start(L) holding a value > a"; it sticks at start(L+1) exactly when
 // the first visit with a >= last(P_L) finds C[start(L+1)] > a. Both facts make
 // every visit of a level independent once that one visit is known.
-#include "rt_common.cuh"
+#include "rt_device.cuh"
 
 namespace rt {
 namespace {
 
-constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr int kTopoThreads = 1024;
 constexpr int kTopoWarps = kTopoThreads / 32;
 
@@ -103,30 +102,6 @@ __global__ void k_hitbox_final(const float4* __restrict__ partial, uint32_t part
 // ----------------------------------------------------------------------------
 // boxes + Morton + iota
 // ----------------------------------------------------------------------------
-// float -> uint with the saturating round-toward-zero rule of cvt.rzi.u32.f32.
-__device__ __forceinline__ uint32_t f2u_sat(float x) { return __float2uint_rz(x); }
-
-__device__ __forceinline__ uint32_t spread_code(uint32_t qx, uint32_t qy, uint32_t qz, int layout) {
-  uint32_t code = 0;
-  if (layout == 30) {
-#pragma unroll
-    for (int k = 0; k < 10; ++k) {
-      code |= ((qz >> k) & 1u) << (3 * k + 2);
-      code |= ((qy >> k) & 1u) << (3 * k + 3);
-      code |= ((qx >> k) & 1u) << (3 * k + 4);
-    }
-  } else {
-    // kernels/CUDA_buildMeshTreeLBVH.cu:138-169: bit 3k = y_k, 3k+1 = x_k, 3k+2 = z_k
-#pragma unroll
-    for (int k = 0; k < 11; ++k) {
-      code |= ((qy >> k) & 1u) << (3 * k + 0);
-      code |= ((qx >> k) & 1u) << (3 * k + 1);
-      if (k < 10) code |= ((qz >> k) & 1u) << (3 * k + 2);
-    }
-  }
-  return code;
-}
-
 // kernels/CUDA_calcMeshBoxes.cu:30-58 (boxes, iota) fused with
 // kernels/CUDA_buildMeshTreeLBVH.cu:115-173 (Morton code of the box centre).
 __global__ __launch_bounds__(256) void k_boxes_morton(const float4* __restrict__ verts, const uint4* __restrict__ faces, uint32_t n,
@@ -188,75 +163,11 @@ struct TopoArgs {
   uint32_t max_nodes;
   uint32_t* hdr;       // [16] header: 0 leaf_count, 1 morton_leaves, 2 node_count, 3 real_depth, 4 split_count,
                        //             5 overrun, 6 nondet, 7 past_end, 8 error
+  const uint32_t* level_start;  // optional [33] absolute starts of the level lists in C (batched build); else from lev_count
+  uint32_t pos_base;            // first position of this mesh (0 for a single mesh)
 };
 
-// Leaves of the median subtree of a range of s faces entered from a leaf
-// (s > max_leaf): recursive floor/ceil halving, a node of fewer than max_leaf
-// faces is a leaf (kernels/CUDA_buildMeshTreeLBVH.cu:314-339). The sizes at
-// depth j are floor(s/2^j) and floor(s/2^j)+1, the latter s mod 2^j times.
-__device__ __forceinline__ uint32_t median_leaves(uint32_t s, uint32_t maxl) {
-  if (s < maxl) return 1u;
-  uint32_t j0 = 0;
-  while ((s >> j0) >= maxl) ++j0;
-  uint32_t q0 = s >> j0;
-  uint32_t r = s & ((1u << j0) - 1u);
-  return (1u << j0) + ((q0 + 1u == maxl) ? r : 0u);
-}
-__device__ __forceinline__ uint32_t median_depth(uint32_t s, uint32_t maxl) {
-  if (s < maxl) return 0u;
-  uint32_t j0 = 0;
-  while ((s >> j0) >= maxl) ++j0;
-  uint32_t q0 = s >> j0;
-  uint32_t r = s & ((1u << j0) - 1u);
-  return j0 + ((q0 + 1u == maxl && r) ? 1u : 0u);
-}
-
-template <int NT>
-__device__ __forceinline__ uint32_t block_excl_scan_nt(uint32_t v, uint32_t* s_warp, uint32_t& total) {
-  constexpr int W = NT / 32;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) s_warp[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t w = lane < W ? s_warp[lane] : 0u;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += y;
-    }
-    if (lane < W) s_warp[lane] = w;
-  }
-  __syncthreads();
-  uint32_t prefix = warp ? s_warp[warp - 1] : 0u;
-  total = s_warp[W - 1];
-  __syncthreads();
-  return prefix + x - v;
-}
-
-// First index j >= start[L] of C with C[j] > a, scanning the level lists in
-// order (each is ascending). Returns S when none.
-__device__ uint32_t split_scan(const uint32_t* __restrict__ C, const uint32_t* s_start, uint32_t L, uint32_t a) {
-  for (uint32_t l = L; l < 32; ++l) {
-    uint32_t st = s_start[l], en = s_start[l + 1];
-    if (st < en && __ldg(C + en - 1) > a) {
-      uint32_t lo = st, hi = en - 1;
-      while (lo < hi) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(C + mid) > a) hi = mid; else lo = mid + 1;
-      }
-      return lo;
-    }
-  }
-  return s_start[32];
-}
-
-__global__ __launch_bounds__(kTopoThreads) void k_topo_morton(TopoArgs A) {
+__device__ __forceinline__ void topo_morton(const TopoArgs& A) {
   __shared__ uint32_t s_start[34];
   __shared__ uint32_t s_level_lo[34];
   __shared__ uint32_t s_warp[kTopoWarps];
@@ -264,11 +175,15 @@ __global__ __launch_bounds__(kTopoThreads) void k_topo_morton(TopoArgs A) {
   __shared__ uint32_t s_overrun, s_nondet, s_past, s_err, s_depth;
   const uint32_t tid = threadIdx.x;
   if (tid == 0) {
-    uint32_t acc = 0;
-    for (int l = 0; l < 33; ++l) { s_start[l] = acc; acc += (l < 32) ? A.lev_count[l] : 0u; }
+    if (A.level_start) {
+      for (int l = 0; l < 33; ++l) s_start[l] = A.level_start[l];
+    } else {
+      uint32_t acc = 0;
+      for (int l = 0; l < 33; ++l) { s_start[l] = acc; acc += (l < 32) ? A.lev_count[l] : 0u; }
+    }
     s_start[33] = s_start[32];
     s_overrun = s_nondet = s_past = s_err = s_depth = 0;
-    A.ra[0] = 0; A.rb[0] = A.n; A.parent[0] = kNone;
+    A.ra[0] = A.pos_base; A.rb[0] = A.pos_base + A.n; A.parent[0] = kNone;
   }
   __syncthreads();
   const uint32_t S = s_start[32];
@@ -401,13 +316,15 @@ __global__ __launch_bounds__(kTopoThreads) void k_topo_morton(TopoArgs A) {
     A.hdr[1] = A.mleaves[0];
     A.hdr[2] = 2 * leaves - 1;
     A.hdr[3] = s_depth;
-    A.hdr[4] = S;
+    A.hdr[4] = S - s_start[0];
     A.hdr[5] = s_overrun;
     A.hdr[6] = s_nondet;
     A.hdr[7] = s_past;
     A.hdr[8] = s_err | ((2 * leaves - 1 > A.max_nodes) ? (uint32_t)RT_DEVERR_NODE_CAPACITY : 0u);
   }
 }
+
+__global__ __launch_bounds__(kTopoThreads) void k_topo_morton(TopoArgs A) { topo_morton(A); }
 
 // ----------------------------------------------------------------------------
 // leaves: one warp per final leaf
@@ -432,34 +349,17 @@ struct LeafArgs {
   uint4* acc_leaves;
   float4* acc_groups;
   uint32_t* leaf_lambda;  // node id -> leaf order index
+  uint32_t pos_base;      // first position of this mesh (node records store positions relative to it)
+  uint32_t vert_base;     // first vertex of this mesh (faces index vertices relative to it)
+  uint32_t* local_indices; // optional: indices[i] - pos_base written here (batched build)
 };
 
 constexpr int kMaxMedianDepth = 40;
-constexpr float kAccelPad = 1.220703125e-4f;  // 2^-13 of the largest coordinate magnitude per axis
-
-// Box padded for the traversal's conservative slab test.
-__device__ __forceinline__ void pad_box(float3& mn, float3& mx) {
-  const float px = fmax_sel(fabsf(mn.x), fabsf(mx.x)) * kAccelPad;
-  const float py = fmax_sel(fabsf(mn.y), fabsf(mx.y)) * kAccelPad;
-  const float pz = fmax_sel(fabsf(mn.z), fabsf(mx.z)) * kAccelPad;
-  mn.x = mn.x - px; mn.y = mn.y - py; mn.z = mn.z - pz;
-  mx.x = mx.x + px; mx.y = mx.y + py; mx.z = mx.z + pz;
-}
-
-__device__ __forceinline__ void write_box(uint32_t* node, float3 mn, float3 mx) {
-  float* f = (float*)node;
-  __stcg(f + 2, mn.x); __stcg(f + 3, mn.y); __stcg(f + 4, mn.z);
-  __stcg(f + 5, mx.x); __stcg(f + 6, mx.y); __stcg(f + 7, mx.z);
-}
-
-__global__ __launch_bounds__(256) void k_leaves(LeafArgs A) {
+// One final leaf (leaf-order index g of its mesh), processed by one warp.
+__device__ __forceinline__ void leaf_body(const LeafArgs& A, const uint32_t g) {
   const uint32_t lane = lane_id();
-  const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t leaf_count = A.hdr[0];
   const uint32_t mleaf_count = A.hdr[1];
-  if (A.hdr[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) return;
-  for (uint32_t g = warp_global; g < leaf_count; g += nwarps) {
+  {
     uint32_t leaf_id = 0, first = 0, cnt = 0;
     // median path (ids and ranks from the median root down to the leaf's parent)
     uint32_t path_id[kMaxMedianDepth], path_rank[kMaxMedianDepth];
@@ -472,7 +372,7 @@ __global__ __launch_bounds__(256) void k_leaves(LeafArgs A) {
         if (A.ml_lambda[mid] <= g) lo = mid; else hi = mid - 1;
       }
       const uint4 rec = A.ml_rec[lo];
-      leaf_id = rec.x; first = rec.y; cnt = rec.z;
+      leaf_id = rec.x; first = rec.y; cnt = rec.z;  // first: absolute position
       if (rec.w & 0x80000000u) {
         uint32_t q = g - A.ml_lambda[lo];
         uint32_t rank = A.ml_rank[lo];
@@ -496,18 +396,20 @@ __global__ __launch_bounds__(256) void k_leaves(LeafArgs A) {
     cnt = __shfl_sync(0xffffffffu, cnt, 0);
 
     float3 mn = make_float3(kHuge, kHuge, kHuge), mx = make_float3(-kHuge, -kHuge, -kHuge);
-    const uint32_t gbase = (first >> 3) + g;  // leaf g's groups: disjoint across leaves, no scan needed
+    const uint32_t lfirst = first - A.pos_base;  // position inside the mesh
+    const uint32_t gbase = (lfirst >> 3) + g;      // leaf g's groups: disjoint across leaves, no scan needed
     if (A.acc_leaves && lane == 0) {
-      A.acc_leaves[g] = make_uint4(first, cnt, gbase, leaf_id);
+      A.acc_leaves[g] = make_uint4(lfirst, cnt, gbase, leaf_id);
       A.leaf_lambda[leaf_id] = g;
     }
     for (uint32_t base = 0; base < cnt; base += 32) {
       const uint32_t i = first + base + lane;
       float3 tmn = make_float3(kHuge, kHuge, kHuge), tmx = make_float3(-kHuge, -kHuge, -kHuge);
       if (base + lane < cnt) {
-        const uint32_t orig = __ldg(A.indices + i);
+        const uint32_t orig = A.indices[i];
         const uint4 f = ldg4(A.faces_in + orig);
-        const float4 v0 = ldg4(A.verts + f.x), v1 = ldg4(A.verts + f.y), v2 = ldg4(A.verts + f.z);
+        const float4 v0 = ldg4(A.verts + A.vert_base + f.x), v1 = ldg4(A.verts + A.vert_base + f.y), v2 = ldg4(A.verts + A.vert_base + f.z);
+        if (A.local_indices) A.local_indices[i] = orig - A.pos_base;
         if (A.faces_out) A.faces_out[i] = f;
         if (A.tris) {
           float4 e1 = make_float4(v1.x - v0.x, v1.y - v0.y, v1.z - v0.z, 0.0f);
@@ -549,9 +451,9 @@ __global__ __launch_bounds__(256) void k_leaves(LeafArgs A) {
       mx.z = fmax_sel(mx.z, __shfl_xor_sync(0xffffffffu, mx.z, o));
     }
     if (lane == 0) {
-      if (leaf_id >= A.max_nodes) { atomicOr(A.err, (uint32_t)RT_DEVERR_NODE_CAPACITY); continue; }
+      if (leaf_id >= A.max_nodes) { atomicOr(A.err, (uint32_t)RT_DEVERR_NODE_CAPACITY); return; }
       uint32_t* nd = A.nodes + 8 * (size_t)leaf_id;
-      *(uint2*)nd = make_uint2(1u | (cnt << 1), first);
+      *(uint2*)nd = make_uint2(1u | (cnt << 1), lfirst);
       write_box(nd, mn, mx);
       // propagate up: the second child to arrive merges the two boxes
       uint32_t cur = leaf_id;
@@ -587,6 +489,40 @@ __global__ __launch_bounds__(256) void k_leaves(LeafArgs A) {
   }
 }
 
+__global__ __launch_bounds__(256) void k_leaves(LeafArgs A) {
+  const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t leaf_count = A.hdr[0];
+  if (A.hdr[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) return;
+  for (uint32_t g = warp_global; g < leaf_count; g += nwarps) leaf_body(A, g);
+}
+
+// Two-child traversal records, indexed by pre-order rank (internal node p
+// with left child c has rank (c - 1) / 2): both children's padded boxes and
+// references (rank for an internal child, ~leaf index for a leaf child).
+// One internal node's two-child record.
+__device__ __forceinline__ void accel_node(const uint32_t* __restrict__ nodes, const uint32_t* __restrict__ leaf_lambda,
+                                           float4* __restrict__ tnodes, const uint32_t p) {
+  const uint2 w = *(const uint2*)(nodes + 8 * (size_t)p);
+  if (w.x & 1u) return;
+  const uint32_t rank = (w.y - 1u) >> 1;
+  float4 out[4];
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const uint32_t c = w.y + side;
+    const uint32_t* cn = nodes + 8 * (size_t)c;
+    const uint32_t cw0 = cn[0], cw1 = cn[1];
+    float3 mn = make_float3(__uint_as_float(cn[2]), __uint_as_float(cn[3]), __uint_as_float(cn[4]));
+    float3 mx = make_float3(__uint_as_float(cn[5]), __uint_as_float(cn[6]), __uint_as_float(cn[7]));
+    pad_box(mn, mx);
+    const uint32_t ref = (cw0 & 1u) ? ~leaf_lambda[c] : ((cw1 - 1u) >> 1);
+    out[2 * side] = make_float4(mn.x, mn.y, mn.z, __uint_as_float(ref));
+    out[2 * side + 1] = make_float4(mx.x, mx.y, mx.z, 0.0f);
+  }
+  float4* dst = tnodes + 4 * (size_t)rank;
+  dst[0] = out[0]; dst[1] = out[1]; dst[2] = out[2]; dst[3] = out[3];
+}
+
 // Two-child traversal records, indexed by pre-order rank (internal node p
 // with left child c has rank (c - 1) / 2): both children's padded boxes and
 // references (rank for an internal child, ~leaf index for a leaf child).
@@ -601,26 +537,8 @@ __global__ __launch_bounds__(256) void k_accel_nodes(const uint32_t* __restrict_
     acc_hdr[1] = hdr[0];                // leaf count
     acc_hdr[2] = node_count;
   }
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < node_count; p += gridDim.x * blockDim.x) {
-    const uint2 w = *(const uint2*)(nodes + 8 * (size_t)p);
-    if (w.x & 1u) continue;
-    const uint32_t rank = (w.y - 1u) >> 1;
-    float4 out[4];
-#pragma unroll
-    for (int side = 0; side < 2; ++side) {
-      const uint32_t c = w.y + side;
-      const uint32_t* cn = nodes + 8 * (size_t)c;
-      const uint32_t cw0 = cn[0], cw1 = cn[1];
-      float3 mn = make_float3(__uint_as_float(cn[2]), __uint_as_float(cn[3]), __uint_as_float(cn[4]));
-      float3 mx = make_float3(__uint_as_float(cn[5]), __uint_as_float(cn[6]), __uint_as_float(cn[7]));
-      pad_box(mn, mx);
-      const uint32_t ref = (cw0 & 1u) ? ~leaf_lambda[c] : ((cw1 - 1u) >> 1);
-      out[2 * side] = make_float4(mn.x, mn.y, mn.z, __uint_as_float(ref));
-      out[2 * side + 1] = make_float4(mx.x, mx.y, mx.z, 0.0f);
-    }
-    float4* dst = tnodes + 4 * (size_t)rank;
-    dst[0] = out[0]; dst[1] = out[1]; dst[2] = out[2]; dst[3] = out[3];
-  }
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < node_count; p += gridDim.x * blockDim.x)
+    accel_node(nodes, leaf_lambda, tnodes, p);
 }
 
 __global__ void k_write_info(const uint32_t* __restrict__ hdr, const uint32_t* __restrict__ err, rt_build_info* info) {
@@ -673,6 +591,13 @@ size_t carve_accel(Carve& c, AccelLayout& A, uint32_t n) {
   A.leaves = c.take<uint4>(n);
   A.groups = c.take<float4>(2 * ((size_t)n / 8 + n + 1));
   return c.off + 256;
+}
+
+__host__ __device__ uint32_t morton_cap_dev(uint32_t n, uint32_t D) {
+  uint64_t a = (D >= 31) ? (1ull << 32) : ((1ull << (D + 1)) - 1);
+  uint64_t b = 2ull * n + 1;
+  uint64_t c = a < b ? a : b;
+  return (uint32_t)(c + 2);
 }
 
 uint32_t morton_cap(uint32_t n, uint32_t D) {
@@ -813,6 +738,7 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
     A.rank = L.rank; A.lambda = L.lambda; A.ord = L.ord; A.id = L.id;
     A.ml_lambda = L.ml_lambda; A.ml_rec = L.ml_rec; A.ml_rank = L.ml_rank; A.parent_id = L.parent_id;
     A.nodes = d->nodes; A.max_nodes = d->max_nodes; A.hdr = L.hdr;
+    A.level_start = nullptr; A.pos_base = 0;
     k_topo_morton<<<1, kTopoThreads, 0, st>>>(A);
     note_launch();
     RT_CHECK_LAUNCH();
@@ -838,6 +764,9 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
     A.acc_leaves = accel ? AL.leaves : nullptr;
     A.acc_groups = accel ? AL.groups : nullptr;
     A.leaf_lambda = L.leaf_lambda;
+    A.pos_base = 0;
+    A.vert_base = 0;
+    A.local_indices = nullptr;
     k_leaves<<<sms * 8, 256, 0, st>>>(A);
     note_launch();
     RT_CHECK_LAUNCH();
@@ -885,6 +814,338 @@ extern "C" rt_status rt_reorder_faces(const uint32_t* faces_in, const uint32_t* 
   uint32_t blocks = (uint32_t)hmin<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 16);
   k_reorder<<<blocks, 256, 0, (cudaStream_t)st>>>((const uint4*)faces_in, indices, n, (uint4*)faces_out);
     note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+// ============================================================================
+// Batched build: M meshes, every stage in one set of launches.
+// ============================================================================
+namespace rt {
+namespace {
+
+
+struct BatchArgs {
+  uint32_t M, N;
+  const uint32_t* foff;
+  const uint32_t* voff;
+  const float4* verts;
+  const uint4* faces_in;
+  uint4* faces_out;
+  float4* boxes;
+  uint32_t* indices_out;
+  uint32_t* codes;
+  uint32_t* nodes;
+  float4* tris;
+  rt_build_params q;
+  // scratch
+  float4* hits;           // [2M]
+  uint32_t* idx;          // [N] global face index in sorted order
+  uint32_t* codes_raw;    // [N] codes before sorting
+  uint32_t* mkey;         // [N] mesh id per position
+  uint32_t* lev;          // [N] (mesh, level) keys
+  uint32_t* C;            // [N] split positions
+  uint32_t* hist;         // [M * 64 + 1]
+  uint32_t* level_start;  // [M * 64 + 1]
+  uint32_t *ra, *rb, *parent, *info, *child, *leaves, *mleaves, *rank, *lambda, *ord, *id;  // [2N + 3M]
+  uint32_t* ml_lambda;
+  uint4* ml_rec;
+  uint32_t* ml_rank;
+  uint32_t* parent_id;    // [2N - M]
+  uint32_t* arrive;       // [2N - M]
+  uint32_t* leaf_lambda;  // [2N - M]
+  uint32_t* hdr;          // [16 M]
+  uint32_t* leaf_base;    // [M + 1]
+  uint32_t* err;          // [4]
+  // traversal blob
+  uint32_t* acc_hdr;      // [64 M]
+  float4* tnodes;         // [4 N]
+  uint4* acc_leaves;      // [N]
+  float4* groups;         // [2 (N + N/8 + M + 1)]
+  rt_build_info* info_out;
+};
+
+__global__ __launch_bounds__(256) void k_batch_hitbox(BatchArgs B) {
+  const uint32_t m = blockIdx.x;
+  const uint32_t v0 = B.voff[m], v1 = B.voff[m + 1];
+  float4 mn = make_float4(kHuge, kHuge, kHuge, kHuge), mx = make_float4(-kHuge, -kHuge, -kHuge, -kHuge);
+  for (uint32_t i = v0 + threadIdx.x; i < v1; i += blockDim.x) {
+    const float4 p = ldg4(B.verts + i);
+    mn = f4min(mn, p);
+    mx = f4max(mx, p);
+  }
+  __shared__ float4 s_mn[256], s_mx[256];
+  s_mn[threadIdx.x] = mn;
+  s_mx[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      s_mn[threadIdx.x] = f4min(s_mn[threadIdx.x], s_mn[threadIdx.x + o]);
+      s_mx[threadIdx.x] = f4max(s_mx[threadIdx.x], s_mx[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { B.hits[2 * m] = s_mn[0]; B.hits[2 * m + 1] = s_mx[0]; }
+}
+
+__global__ __launch_bounds__(256) void k_batch_boxes_morton(BatchArgs B) {
+  const int layout = (int)B.q.morton_bits;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < B.N; k += gridDim.x * blockDim.x) {
+    const uint32_t m = find_seg(B.foff, B.M, k);
+    const float4 hmin = B.hits[2 * m], hmax = B.hits[2 * m + 1];
+    const float sx = (layout == 30 ? 1023.0f : 2047.0f) / (hmax.x - hmin.x);
+    const float sy = (layout == 30 ? 1023.0f : 2047.0f) / (hmax.y - hmin.y);
+    const float sz = 1023.0f / (hmax.z - hmin.z);
+    const uint32_t vb = __ldg(B.voff + m);
+    const uint4 f = ldg4(B.faces_in + k);
+    const float4 v0 = ldg4(B.verts + vb + f.x), v1 = ldg4(B.verts + vb + f.y), v2 = ldg4(B.verts + vb + f.z);
+    const float4 mn = f4min(f4min(v0, v1), v2);
+    const float4 mx = f4max(f4max(v0, v1), v2);
+    B.boxes[2 * (size_t)k] = mn;
+    B.boxes[2 * (size_t)k + 1] = mx;
+    B.idx[k] = k;
+    const float cx = 0.5f * (mn.x + mx.x), cy = 0.5f * (mn.y + mx.y), cz = 0.5f * (mn.z + mx.z);
+    const uint32_t code = spread_code(f2u_sat((cx - hmin.x) * sx), f2u_sat((cy - hmin.y) * sy), f2u_sat((cz - hmin.z) * sz), layout);
+    B.codes[k] = code;
+    B.codes_raw[k] = code;
+  }
+}
+
+__global__ __launch_bounds__(256) void k_batch_meshkey(BatchArgs B) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < B.N; i += gridDim.x * blockDim.x)
+    B.mkey[i] = find_seg(B.foff, B.M, B.idx[i]);
+}
+
+// After the (mesh, code) order is complete: codes per position, and the split
+// level key (mesh * 64 + level; 32 = no split, also across meshes) per pair.
+__global__ __launch_bounds__(256) void k_batch_levels(BatchArgs B) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < B.N; i += gridDim.x * blockDim.x) {
+    B.codes[i] = B.codes_raw[B.idx[i]];
+  }
+}
+__global__ __launch_bounds__(256) void k_batch_levels2(BatchArgs B) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i + 1 < B.N; i += gridDim.x * blockDim.x) {
+    const uint32_t m = B.mkey[i];
+    uint32_t lev = 32;
+    if (B.mkey[i + 1] == m) {
+      const uint32_t d = B.codes[i] ^ B.codes[i + 1];
+      if (d) lev = (uint32_t)__clz(d);
+    }
+    const uint32_t key = m * 64 + lev;
+    B.lev[i] = key;
+    B.C[i] = i + 1;
+    atomicAdd(B.hist + key, 1u);
+  }
+}
+
+// Exclusive scan of the (mesh, level) histogram: absolute start of each list in C.
+__global__ __launch_bounds__(1024) void k_batch_level_starts(BatchArgs B) {
+  __shared__ uint32_t s_warp[32];
+  const uint32_t total_keys = B.M * 64;
+  uint32_t running = 0;
+  for (uint32_t c = 0; c < total_keys; c += 1024) {
+    const uint32_t i = c + threadIdx.x;
+    const uint32_t v = i < total_keys ? B.hist[i] : 0u;
+    uint32_t tot;
+    const uint32_t ex = block_excl_scan_nt<1024>(v, s_warp, tot);
+    if (i < total_keys) B.level_start[i] = running + ex;
+    running += tot;
+  }
+  if (threadIdx.x == 0) B.level_start[total_keys] = running;
+}
+
+__global__ __launch_bounds__(kTopoThreads) void k_batch_topo(BatchArgs B) {
+  const uint32_t m = blockIdx.x;
+  const uint32_t F = B.foff[m], n = B.foff[m + 1] - F;
+  const uint32_t bb = bfs_base(F, m), nb = node_base(F, m);
+  TopoArgs A;
+  A.C = B.C; A.lev_count = nullptr; A.n = n; A.D = B.q.tree_depth; A.min_leaf = B.q.min_leaf; A.max_leaf = B.q.max_leaf;
+  A.complete = 1u; A.cap_m = morton_cap_dev(n, B.q.tree_depth);
+  A.ra = B.ra + bb; A.rb = B.rb + bb; A.parent = B.parent + bb; A.info = B.info + bb; A.child = B.child + bb;
+  A.leaves = B.leaves + bb; A.mleaves = B.mleaves + bb; A.rank = B.rank + bb; A.lambda = B.lambda + bb; A.ord = B.ord + bb;
+  A.id = B.id + bb; A.ml_lambda = B.ml_lambda + bb; A.ml_rec = B.ml_rec + bb; A.ml_rank = B.ml_rank + bb;
+  A.parent_id = B.parent_id + nb; A.nodes = B.nodes + 8 * (size_t)nb; A.max_nodes = 2 * n - 1; A.hdr = B.hdr + 16 * m;
+  A.level_start = B.level_start + 64 * m; A.pos_base = F;
+  topo_morton(A);
+}
+
+// Leaf-order bases per mesh (exclusive scan of the leaf counts) and the total.
+__global__ __launch_bounds__(1024) void k_batch_leaf_base(BatchArgs B) {
+  __shared__ uint32_t s_warp[32];
+  uint32_t running = 0;
+  for (uint32_t c = 0; c < B.M; c += 1024) {
+    const uint32_t i = c + threadIdx.x;
+    const uint32_t bad = i < B.M ? (B.hdr[16 * i + 8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) : 0u;
+    const uint32_t v = (i < B.M && !bad) ? B.hdr[16 * i] : 0u;
+    uint32_t tot;
+    const uint32_t ex = block_excl_scan_nt<1024>(v, s_warp, tot);
+    if (i < B.M) B.leaf_base[i] = running + ex;
+    running += tot;
+  }
+  if (threadIdx.x == 0) B.leaf_base[B.M] = running;
+}
+
+__global__ __launch_bounds__(256) void k_batch_leaves(BatchArgs B) {
+  const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t total = B.leaf_base[B.M];
+  for (uint32_t g = warp_global; g < total; g += nwarps) {
+    const uint32_t m = find_seg(B.leaf_base, B.M, g);
+    const uint32_t F = B.foff[m], n = B.foff[m + 1] - F;
+    const uint32_t bb = bfs_base(F, m), nb = node_base(F, m);
+    LeafArgs A;
+    A.verts = B.verts; A.faces_in = B.faces_in; A.faces_out = B.faces_out; A.tris = B.tris; A.indices = B.idx;
+    A.ml_lambda = B.ml_lambda + bb; A.ml_rec = B.ml_rec + bb; A.ml_rank = B.ml_rank + bb;
+    A.parent_id = B.parent_id + nb; A.arrive = B.arrive + nb; A.nodes = B.nodes + 8 * (size_t)nb; A.max_nodes = 2 * n - 1;
+    A.max_leaf = B.q.max_leaf; A.hdr = B.hdr + 16 * m; A.err = B.err;
+    A.acc_leaves = B.acc_leaves + F; A.acc_groups = B.groups + 2 * (size_t)group_base(F, m); A.leaf_lambda = B.leaf_lambda + nb;
+    A.pos_base = F; A.vert_base = B.voff[m]; A.local_indices = B.indices_out;
+    leaf_body(A, g - B.leaf_base[m]);
+  }
+}
+
+__global__ __launch_bounds__(256) void k_batch_accel_nodes(BatchArgs B) {
+  const uint32_t slots = 2 * B.N - B.M;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < slots; p += gridDim.x * blockDim.x) {
+    // mesh whose node range holds slot p: largest m with 2 F_m - m <= p
+    uint32_t lo = 0, hi = B.M - 1;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (node_base(__ldg(B.foff + mid), mid) <= p) lo = mid; else hi = mid - 1;
+    }
+    const uint32_t m = lo, F = B.foff[m], nb = node_base(F, m);
+    const uint32_t* h = B.hdr + 16 * m;
+    if (h[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) continue;
+    const uint32_t lp = p - nb;
+    if (lp >= h[2]) continue;
+    if (lp == 0) {
+      uint32_t* ah = B.acc_hdr + 64 * m;
+      ah[0] = (B.nodes[8 * (size_t)nb] & 1u) ? ~0u : 0u;
+      ah[1] = h[0];
+      ah[2] = h[2];
+    }
+    accel_node(B.nodes + 8 * (size_t)nb, B.leaf_lambda + nb, B.tnodes + 4 * (size_t)F, lp);
+  }
+}
+
+__global__ void k_batch_info(BatchArgs B) {
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < B.M; m += gridDim.x * blockDim.x) {
+    const uint32_t* h = B.hdr + 16 * m;
+    rt_build_info* o = B.info_out + m;
+    o->leaf_count = h[0]; o->node_count = h[2]; o->real_depth = h[3]; o->split_count = h[4];
+    o->overrun_visits = h[5]; o->nondet_reads = h[6]; o->past_end_reads = h[7]; o->error = h[8] | *B.err;
+  }
+}
+
+size_t carve_batch(Carve& c, BatchArgs& B, uint32_t M, uint32_t N) {
+  B.hits = c.take<float4>(2 * (size_t)M);
+  B.idx = c.take<uint32_t>(N);
+  B.codes_raw = c.take<uint32_t>(N);
+  B.mkey = c.take<uint32_t>(N);
+  B.lev = c.take<uint32_t>(N);
+  B.C = c.take<uint32_t>(N);
+  B.hist = c.take<uint32_t>((size_t)M * 64 + 1);
+  B.level_start = c.take<uint32_t>((size_t)M * 64 + 1);
+  const size_t bfs = 2 * (size_t)N + 3 * (size_t)M + 4;
+  uint32_t** arrs[] = {&B.ra, &B.rb, &B.parent, &B.info, &B.child, &B.leaves, &B.mleaves, &B.rank, &B.lambda, &B.ord, &B.id};
+  for (auto a : arrs) *a = c.take<uint32_t>(bfs);
+  B.ml_lambda = c.take<uint32_t>(bfs);
+  B.ml_rec = c.take<uint4>(bfs);
+  B.ml_rank = c.take<uint32_t>(bfs);
+  const size_t nodes = 2 * (size_t)N;
+  B.parent_id = c.take<uint32_t>(nodes);
+  B.arrive = c.take<uint32_t>(nodes);
+  B.leaf_lambda = c.take<uint32_t>(nodes);
+  B.hdr = c.take<uint32_t>(16 * (size_t)M);
+  B.leaf_base = c.take<uint32_t>((size_t)M + 1);
+  B.err = c.take<uint32_t>(4);
+  const size_t sort_bytes = radix_scratch_bytes(N);
+  c.take<char>(sort_bytes);
+  return c.off + 256;
+}
+
+size_t carve_batch_accel(Carve& c, BatchArgs& B, uint32_t M, uint32_t N) {
+  BatchAccel L;
+  const size_t bytes = carve_batch_accel_layout(c, L, M, N);
+  B.acc_hdr = L.hdr; B.tnodes = L.tnodes; B.acc_leaves = L.leaves; B.groups = L.groups;
+  return bytes;
+}
+
+}  // namespace
+}  // namespace rt
+
+extern "C" rt_status rt_batch_sizes(uint32_t M, uint32_t N, const rt_build_params* params, size_t* scratch_bytes, size_t* accel_bytes) {
+  if (M == 0 || N < M || !scratch_bytes) return RT_ERR_INVALID_ARGUMENT;
+  (void)params;
+  Carve c(nullptr, 0);
+  BatchArgs B;
+  *scratch_bytes = carve_batch(c, B, M, N);
+  if (accel_bytes) {
+    Carve a(nullptr, 0);
+    *accel_bytes = carve_batch_accel(a, B, M, N);
+  }
+  return RT_OK;
+}
+
+extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stream_) {
+  if (!d || d->mesh_count == 0 || d->face_count < d->mesh_count || !d->face_offsets || !d->vertex_offsets || !d->vertices ||
+      !d->faces_in || !d->faces_out || !d->boxes || !d->indices || !d->codes || !d->nodes || !d->tris || !d->accel || !d->info)
+    return RT_ERR_INVALID_ARGUMENT;
+  if (d->faces_out == d->faces_in) return RT_ERR_INVALID_ARGUMENT;
+  if (d->mesh_count > 65536u || d->face_count > 0x3FFFFFFFu) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  rt_build_params q = normalized(&d->params);
+  if (!q.tree_complete || (q.morton_bits != 32 && q.morton_bits != 30)) return RT_ERR_INVALID_ARGUMENT;
+  const uint32_t M = d->mesh_count, N = d->face_count;
+  Carve c(d->scratch, d->scratch_bytes);
+  BatchArgs B;
+  carve_batch(c, B, M, N);
+  if (!d->scratch || !c.ok()) return RT_ERR_SCRATCH_TOO_SMALL;
+  // the sort scratch is the last region
+  const size_t sort_bytes = radix_scratch_bytes(N);
+  void* sort_scratch = (char*)d->scratch + (c.off - sort_bytes - 0);
+  {
+    Carve a(d->accel, d->accel_bytes);
+    carve_batch_accel(a, B, M, N);
+    if (!a.ok()) return RT_ERR_SCRATCH_TOO_SMALL;
+  }
+  B.M = M; B.N = N; B.foff = d->face_offsets; B.voff = d->vertex_offsets; B.verts = (const float4*)d->vertices;
+  B.faces_in = (const uint4*)d->faces_in; B.faces_out = (uint4*)d->faces_out; B.boxes = (float4*)d->boxes;
+  B.indices_out = d->indices; B.codes = d->codes; B.nodes = d->nodes; B.tris = (float4*)d->tris; B.q = q; B.info_out = d->info;
+  cudaStream_t st = (cudaStream_t)stream_;
+  const int sms = sm_count();
+  const uint32_t fblocks = (uint32_t)hmin<uint64_t>((N + 255) / 256, (uint64_t)sms * 16);
+  k_batch_hitbox<<<M, 256, 0, st>>>(B);
+  k_batch_boxes_morton<<<fblocks, 256, 0, st>>>(B);
+  note_launch(2);
+  RT_CHECK_LAUNCH();
+  rt_status s = radix_sort_pairs(B.codes, B.idx, N, 0, 32, 0, sort_scratch, sort_bytes, st, nullptr);
+  if (s != RT_OK) return s;
+  k_batch_meshkey<<<fblocks, 256, 0, st>>>(B);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  s = radix_sort_pairs(B.mkey, B.idx, N, 0, 16, 0, sort_scratch, sort_bytes, st, nullptr);
+  if (s != RT_OK) return s;
+  if (cudaMemsetAsync(B.hist, 0, ((size_t)M * 64 + 1) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
+  k_batch_levels<<<fblocks, 256, 0, st>>>(B);
+  k_batch_levels2<<<fblocks, 256, 0, st>>>(B);
+  note_launch(2);
+  RT_CHECK_LAUNCH();
+  if (N > 1) {
+    s = radix_sort_pairs(B.lev, B.C, N - 1, 0, 24, 0, sort_scratch, sort_bytes, st, nullptr);
+    if (s != RT_OK) return s;
+  }
+  k_batch_level_starts<<<1, 1024, 0, st>>>(B);
+  if (cudaMemsetAsync(B.err, 0, 16, st) != cudaSuccess) return RT_ERR_CUDA;
+  k_batch_topo<<<M, kTopoThreads, 0, st>>>(B);
+  k_batch_leaf_base<<<1, 1024, 0, st>>>(B);
+  note_launch(3);
+  RT_CHECK_LAUNCH();
+  if (cudaMemsetAsync(B.arrive, 0, (2 * (size_t)N) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
+  k_batch_leaves<<<sms * 8, 256, 0, st>>>(B);
+  k_batch_accel_nodes<<<sms * 4, 256, 0, st>>>(B);
+  k_batch_info<<<(M + 255) / 256, 256, 0, st>>>(B);
+  note_launch(3);
   RT_CHECK_LAUNCH();
   return RT_OK;
 }

@@ -1,0 +1,205 @@
+// rt_device.cuh -- device helpers shared by the single-mesh and batched
+// build and traversal kernels (one definition of every pinned computation).
+#pragma once
+#include "rt_common.cuh"
+
+namespace rt {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+// float -> uint with the saturating round-toward-zero rule of cvt.rzi.u32.f32.
+__device__ __forceinline__ uint32_t f2u_sat(float x) { return __float2uint_rz(x); }
+
+__device__ __forceinline__ uint32_t spread_code(uint32_t qx, uint32_t qy, uint32_t qz, int layout) {
+  uint32_t code = 0;
+  if (layout == 30) {
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+      code |= ((qz >> k) & 1u) << (3 * k + 2);
+      code |= ((qy >> k) & 1u) << (3 * k + 3);
+      code |= ((qx >> k) & 1u) << (3 * k + 4);
+    }
+  } else {
+    // kernels/CUDA_buildMeshTreeLBVH.cu:138-169: bit 3k = y_k, 3k+1 = x_k, 3k+2 = z_k
+#pragma unroll
+    for (int k = 0; k < 11; ++k) {
+      code |= ((qy >> k) & 1u) << (3 * k + 0);
+      code |= ((qx >> k) & 1u) << (3 * k + 1);
+      if (k < 10) code |= ((qz >> k) & 1u) << (3 * k + 2);
+    }
+  }
+  return code;
+}
+
+// Leaves of the median subtree of a range of s faces entered from a leaf
+// (s > max_leaf): recursive floor/ceil halving, a node of fewer than max_leaf
+// faces is a leaf (kernels/CUDA_buildMeshTreeLBVH.cu:314-339). The sizes at
+// depth j are floor(s/2^j) and floor(s/2^j)+1, the latter s mod 2^j times.
+__device__ __forceinline__ uint32_t median_leaves(uint32_t s, uint32_t maxl) {
+  if (s < maxl) return 1u;
+  uint32_t j0 = 0;
+  while ((s >> j0) >= maxl) ++j0;
+  uint32_t q0 = s >> j0;
+  uint32_t r = s & ((1u << j0) - 1u);
+  return (1u << j0) + ((q0 + 1u == maxl) ? r : 0u);
+}
+__device__ __forceinline__ uint32_t median_depth(uint32_t s, uint32_t maxl) {
+  if (s < maxl) return 0u;
+  uint32_t j0 = 0;
+  while ((s >> j0) >= maxl) ++j0;
+  uint32_t q0 = s >> j0;
+  uint32_t r = s & ((1u << j0) - 1u);
+  return j0 + ((q0 + 1u == maxl && r) ? 1u : 0u);
+}
+
+template <int NT>
+__device__ __forceinline__ uint32_t block_excl_scan_nt(uint32_t v, uint32_t* s_warp, uint32_t& total) {
+  constexpr int W = NT / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < W ? s_warp[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < W) s_warp[lane] = w;
+  }
+  __syncthreads();
+  uint32_t prefix = warp ? s_warp[warp - 1] : 0u;
+  total = s_warp[W - 1];
+  __syncthreads();
+  return prefix + x - v;
+}
+
+// First index j >= start[L] of C with C[j] > a, scanning the level lists in
+// order (each is ascending). Returns S when none.
+__device__ __forceinline__ uint32_t split_scan(const uint32_t* __restrict__ C, const uint32_t* s_start, uint32_t L, uint32_t a) {
+  for (uint32_t l = L; l < 32; ++l) {
+    uint32_t st = s_start[l], en = s_start[l + 1];
+    if (st < en && __ldg(C + en - 1) > a) {
+      uint32_t lo = st, hi = en - 1;
+      while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(C + mid) > a) hi = mid; else lo = mid + 1;
+      }
+      return lo;
+    }
+  }
+  return s_start[32];
+}
+
+constexpr float kAccelPad = 1.220703125e-4f;  // 2^-13 of the largest coordinate magnitude per axis
+
+// Box padded for the traversal's conservative slab test.
+__device__ __forceinline__ void pad_box(float3& mn, float3& mx) {
+  const float px = fmax_sel(fabsf(mn.x), fabsf(mx.x)) * kAccelPad;
+  const float py = fmax_sel(fabsf(mn.y), fabsf(mx.y)) * kAccelPad;
+  const float pz = fmax_sel(fabsf(mn.z), fabsf(mx.z)) * kAccelPad;
+  mn.x = mn.x - px; mn.y = mn.y - py; mn.z = mn.z - pz;
+  mx.x = mx.x + px; mx.y = mx.y + py; mx.z = mx.z + pz;
+}
+
+__device__ __forceinline__ void write_box(uint32_t* node, float3 mn, float3 mx) {
+  float* f = (float*)node;
+  __stcg(f + 2, mn.x); __stcg(f + 3, mn.y); __stcg(f + 4, mn.z);
+  __stcg(f + 5, mx.x); __stcg(f + 6, mx.y); __stcg(f + 7, mx.z);
+}
+
+constexpr int kStack = 64;
+constexpr float kBoxPad = 1.220703125e-4f;      // 2^-13
+constexpr float kCullSlack = 1.0001220703125f;  // 1 + 2^-13
+
+__device__ __forceinline__ float fix_dir(float c) { return fabsf(c) < 1e-20f ? copysignf(1e-20f, c) : c; }
+
+// Moller-Trumbore of kernels/CUDA_raytraceMeshTree.cu:57-89; zu / zv are the
+// (ray.w * 0) products of the 4-wide dot products (they only fix the sign of a
+// zero sum).
+__device__ __forceinline__ bool mt_test(const float4& o, const float4& d, float zu, float zv, const float4& v0, const float4& e1,
+                                        const float4& e2, float& t, float& u, float& v) {
+  const float px = d.y * e2.z - d.z * e2.y;
+  const float py = d.z * e2.x - d.x * e2.z;
+  const float pz = d.x * e2.y - d.y * e2.x;
+  const float det = ((e1.x * px + e1.y * py) + e1.z * pz) + 0.0f;
+  if (det > -0.000001f && det < 0.000001f) return false;
+  const float inv = 1.0f / det;
+  const float tx = o.x - v0.x, ty = o.y - v0.y, tz = o.z - v0.z;
+  u = (((tx * px + ty * py) + tz * pz) + zu) * inv;
+  if (u < 0.0f || u > 1.0f) return false;
+  const float qx = ty * e1.z - tz * e1.y;
+  const float qy = tz * e1.x - tx * e1.z;
+  const float qz = tx * e1.y - ty * e1.x;
+  v = (((d.x * qx + d.y * qy) + d.z * qz) + zv) * inv;
+  if (v < 0.0f || u + v > 1.0f) return false;
+  t = (((e2.x * qx + e2.y * qy) + e2.z * qz) + 0.0f) * inv;
+  return t >= 0.0f;
+}
+
+__device__ __forceinline__ bool box_test(float bx0, float by0, float bz0, float bx1, float by1, float bz1, const float4& o,
+                                         float ix, float iy, float iz, float tbest) {
+  float px = fmax_sel(fabsf(bx0), fabsf(bx1)) * kBoxPad;
+  float py = fmax_sel(fabsf(by0), fabsf(by1)) * kBoxPad;
+  float pz = fmax_sel(fabsf(bz0), fabsf(bz1)) * kBoxPad;
+  float t0x = ((bx0 - px) - o.x) * ix, t1x = ((bx1 + px) - o.x) * ix;
+  float t0y = ((by0 - py) - o.y) * iy, t1y = ((by1 + py) - o.y) * iy;
+  float t0z = ((bz0 - pz) - o.z) * iz, t1z = ((bz1 + pz) - o.z) * iz;
+  float tn = fmax_sel(fmax_sel(fmin_sel(t0x, t1x), fmin_sel(t0y, t1y)), fmin_sel(t0z, t1z));
+  float tf = fmin_sel(fmin_sel(fmax_sel(t0x, t1x), fmax_sel(t0y, t1y)), fmax_sel(t0z, t1z));
+  return tn <= tf && tf >= 0.0f && tn <= tbest * kCullSlack;
+}
+
+__device__ __forceinline__ bool slab2(const float4& mn, const float4& mx, const float4& o, float ix, float iy, float iz, float tbest,
+                                      float& tn) {
+  const float t0x = (mn.x - o.x) * ix, t1x = (mx.x - o.x) * ix;
+  const float t0y = (mn.y - o.y) * iy, t1y = (mx.y - o.y) * iy;
+  const float t0z = (mn.z - o.z) * iz, t1z = (mx.z - o.z) * iz;
+  tn = fmax_sel(fmax_sel(fmin_sel(t0x, t1x), fmin_sel(t0y, t1y)), fmin_sel(t0z, t1z));
+  const float tf = fmin_sel(fmin_sel(fmax_sel(t0x, t1x), fmax_sel(t0y, t1y)), fmax_sel(t0z, t1z));
+  return tn <= tf && tf >= 0.0f && tn <= tbest * kCullSlack;
+}
+
+// ---------------------------------------------------------------------------
+// batched meshes
+// ---------------------------------------------------------------------------
+// Largest m in [0, M) with off[m] <= x (off ascending, off[0] = 0).
+__device__ __forceinline__ uint32_t find_seg(const uint32_t* __restrict__ off, uint32_t M, uint32_t x) {
+  uint32_t lo = 0, hi = M - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (__ldg(off + mid) <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Per-mesh bases inside the batched arrays, all derived from F_m (the mesh's
+// first face) and m: node records (capacity 2 n_m - 1), Morton-level arrays
+// (capacity 2 n_m + 3), group boxes (mesh m uses fewer than n_m + n_m / 8 + 1).
+__host__ __device__ __forceinline__ uint32_t node_base(uint32_t F, uint32_t m) { return 2 * F - m; }
+__host__ __device__ __forceinline__ uint32_t bfs_base(uint32_t F, uint32_t m) { return 2 * F + 3 * m; }
+__host__ __device__ __forceinline__ uint32_t group_base(uint32_t F, uint32_t m) { return F + F / 8 + m; }
+
+// Batched traversal blob: per-mesh headers (64 words), two-child records at
+// 4 F_m, leaf tables at F_m, group boxes at 2 group_base(F_m, m).
+struct BatchAccel {
+  uint32_t* hdr;
+  float4* tnodes;
+  uint4* leaves;
+  float4* groups;
+};
+inline size_t carve_batch_accel_layout(Carve& c, BatchAccel& L, uint32_t M, uint32_t N) {
+  L.hdr = c.take<uint32_t>(64 * (size_t)M);
+  L.tnodes = c.take<float4>(4 * (size_t)N);
+  L.leaves = c.take<uint4>(N);
+  L.groups = c.take<float4>(2 * ((size_t)N + N / 8 + M + 1));
+  return c.off + 256;
+}
+
+}  // namespace rt

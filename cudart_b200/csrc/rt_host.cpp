@@ -77,6 +77,7 @@ extern "C" const char* rt_status_string(rt_status s) {
 }
 
 extern "C" uint32_t rt_version(void) { return 100u; }
+extern "C" uint32_t rt_abi_version(void) { return RT_ABI_VERSION; }
 
 namespace {
 std::atomic<uint64_t> g_launches{0};

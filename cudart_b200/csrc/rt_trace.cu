@@ -13,14 +13,10 @@
 // loaded as two 128-bit read-only loads; triangles are read from the build's
 // position-ordered {v0, e1, e2} stream (48 bytes, three 128-bit loads), so a
 // leaf's triangles are contiguous.
-#include "rt_common.cuh"
+#include "rt_device.cuh"
 
 namespace rt {
 namespace {
-
-constexpr int kStack = 64;
-constexpr float kBoxPad = 1.220703125e-4f;      // 2^-13
-constexpr float kCullSlack = 1.0001220703125f;  // 1 + 2^-13
 
 struct TraceArgs {
   const uint4* nodes;
@@ -40,44 +36,6 @@ struct TraceArgs {
   uint32_t* tests;
   uint32_t* err;
 };
-
-__device__ __forceinline__ float fix_dir(float c) { return fabsf(c) < 1e-20f ? copysignf(1e-20f, c) : c; }
-
-// Moller-Trumbore of kernels/CUDA_raytraceMeshTree.cu:57-89; zu / zv are the
-// (ray.w * 0) products of the 4-wide dot products (they only fix the sign of a
-// zero sum).
-__device__ __forceinline__ bool mt_test(const float4& o, const float4& d, float zu, float zv, const float4& v0, const float4& e1,
-                                        const float4& e2, float& t, float& u, float& v) {
-  const float px = d.y * e2.z - d.z * e2.y;
-  const float py = d.z * e2.x - d.x * e2.z;
-  const float pz = d.x * e2.y - d.y * e2.x;
-  const float det = ((e1.x * px + e1.y * py) + e1.z * pz) + 0.0f;
-  if (det > -0.000001f && det < 0.000001f) return false;
-  const float inv = 1.0f / det;
-  const float tx = o.x - v0.x, ty = o.y - v0.y, tz = o.z - v0.z;
-  u = (((tx * px + ty * py) + tz * pz) + zu) * inv;
-  if (u < 0.0f || u > 1.0f) return false;
-  const float qx = ty * e1.z - tz * e1.y;
-  const float qy = tz * e1.x - tx * e1.z;
-  const float qz = tx * e1.y - ty * e1.x;
-  v = (((d.x * qx + d.y * qy) + d.z * qz) + zv) * inv;
-  if (v < 0.0f || u + v > 1.0f) return false;
-  t = (((e2.x * qx + e2.y * qy) + e2.z * qz) + 0.0f) * inv;
-  return t >= 0.0f;
-}
-
-__device__ __forceinline__ bool box_test(float bx0, float by0, float bz0, float bx1, float by1, float bz1, const float4& o,
-                                         float ix, float iy, float iz, float tbest) {
-  float px = fmax_sel(fabsf(bx0), fabsf(bx1)) * kBoxPad;
-  float py = fmax_sel(fabsf(by0), fabsf(by1)) * kBoxPad;
-  float pz = fmax_sel(fabsf(bz0), fabsf(bz1)) * kBoxPad;
-  float t0x = ((bx0 - px) - o.x) * ix, t1x = ((bx1 + px) - o.x) * ix;
-  float t0y = ((by0 - py) - o.y) * iy, t1y = ((by1 + py) - o.y) * iy;
-  float t0z = ((bz0 - pz) - o.z) * iz, t1z = ((bz1 + pz) - o.z) * iz;
-  float tn = fmax_sel(fmax_sel(fmin_sel(t0x, t1x), fmin_sel(t0y, t1y)), fmin_sel(t0z, t1z));
-  float tf = fmin_sel(fmin_sel(fmax_sel(t0x, t1x), fmax_sel(t0y, t1y)), fmax_sel(t0z, t1z));
-  return tn <= tf && tf >= 0.0f && tn <= tbest * kCullSlack;
-}
 
 template <bool kTris, bool kCount>
 __global__ __launch_bounds__(128) void k_trace(TraceArgs A) {
@@ -171,20 +129,11 @@ struct AccelArgs {
   const uint32_t* hdr;
 };
 
-__device__ __forceinline__ bool slab2(const float4& mn, const float4& mx, const float4& o, float ix, float iy, float iz, float tbest,
-                                      float& tn) {
-  const float t0x = (mn.x - o.x) * ix, t1x = (mx.x - o.x) * ix;
-  const float t0y = (mn.y - o.y) * iy, t1y = (mx.y - o.y) * iy;
-  const float t0z = (mn.z - o.z) * iz, t1z = (mx.z - o.z) * iz;
-  tn = fmax_sel(fmax_sel(fmin_sel(t0x, t1x), fmin_sel(t0y, t1y)), fmin_sel(t0z, t1z));
-  const float tf = fmin_sel(fmin_sel(fmax_sel(t0x, t1x), fmax_sel(t0y, t1y)), fmax_sel(t0z, t1z));
-  return tn <= tf && tf >= 0.0f && tn <= tbest * kCullSlack;
-}
-
-template <bool kCount>
-__global__ __launch_bounds__(128) void k_trace_accel(TraceArgs A, AccelArgs C) {
-  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= A.ray_count) return;
+// One ray through the blob. kWW: "while-while" schedule (descend internal
+// nodes until the ray holds a leaf, then test the leaf), which keeps the lanes
+// of a warp in the same phase more often than the "if-if" schedule.
+template <bool kCount, bool kWW>
+__device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArgs& A, const AccelArgs& C) {
   const float4 o = ldg4(A.orig + r), d = ldg4(A.dir + r);
   const float tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
   int32_t best = -1;
@@ -197,33 +146,10 @@ __global__ __launch_bounds__(128) void k_trace_accel(TraceArgs A, AccelArgs C) {
     float st_t[kStack];
     int sp = 0;
     uint32_t ref = __ldg(C.hdr);
-    for (;;) {
-      if (ref & 0x80000000u) {
-        // leaf
-        const uint4 L = __ldg(C.leaves + (~ref));
-        if (kCount) ++visits;
-        const uint32_t first = L.x, cnt = L.y, gbase = L.z;
-        for (uint32_t g = 0; g * 8 < cnt; ++g) {
-          const float4 gmn = ldg4(C.groups + 2 * ((size_t)gbase + g));
-          const float4 gmx = ldg4(C.groups + 2 * ((size_t)gbase + g) + 1);
-          if (kCount) ++visits;
-          float tg;
-          if (!slab2(gmn, gmx, o, ix, iy, iz, bt, tg)) continue;
-          const uint32_t kend = min(cnt, g * 8 + 8);
-          for (uint32_t k = g * 8; k < kend; ++k) {
-            const uint32_t pos = first + k;
-            const float4 v0 = ldg4(A.tris + 3 * (size_t)pos);
-            const float4 e1 = ldg4(A.tris + 3 * (size_t)pos + 1);
-            const float4 e2 = ldg4(A.tris + 3 * (size_t)pos + 2);
-            if (kCount) ++tests;
-            float t, u, v;
-            if (!mt_test(o, d, zu, zv, v0, e1, e2, t, u, v)) continue;
-            if (t < bt || (best >= 0 && t == bt && (int32_t)pos < best)) {
-              best = (int32_t)pos; bt = t; bu = u; bv = v;
-            }
-          }
-        }
-      } else {
+    bool alive = true;
+    while (alive) {
+      // descend internal nodes (kWW: until this ray holds a leaf)
+      while (!(ref & 0x80000000u)) {
         const float4* tn = C.tnodes + 4 * (size_t)ref;
         const float4 a0 = ldg4(tn), a1 = ldg4(tn + 1), b0 = ldg4(tn + 2), b1 = ldg4(tn + 3);
         if (kCount) visits += 2;
@@ -241,12 +167,46 @@ __global__ __launch_bounds__(128) void k_trace_accel(TraceArgs A, AccelArgs C) {
             atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
           }
           ref = a_first ? ra : rb;
-          continue;
+        } else if (ha) {
+          ref = ra;
+        } else if (hb) {
+          ref = rb;
+        } else {
+          bool found = false;
+          while (sp > 0) {
+            --sp;
+            if (st_t[sp] <= bt * kCullSlack) { ref = st_ref[sp]; found = true; break; }
+          }
+          if (!found) { alive = false; break; }
         }
-        if (ha) { ref = ra; continue; }
-        if (hb) { ref = rb; continue; }
+        if (!kWW && (ref & 0x80000000u)) break;
       }
-      // pop the next subtree whose entry is still within reach
+      if (!alive) break;
+      // leaf: group boxes, then the triangles of the groups that pass
+      const uint4 L = __ldg(C.leaves + (~ref));
+      if (kCount) ++visits;
+      const uint32_t first = L.x, cnt = L.y, gbase = L.z;
+      for (uint32_t g = 0; g * 8 < cnt; ++g) {
+        const float4 gmn = ldg4(C.groups + 2 * ((size_t)gbase + g));
+        const float4 gmx = ldg4(C.groups + 2 * ((size_t)gbase + g) + 1);
+        if (kCount) ++visits;
+        float tg;
+        if (!slab2(gmn, gmx, o, ix, iy, iz, bt, tg)) continue;
+        const uint32_t kend = min(cnt, g * 8 + 8);
+        for (uint32_t k = g * 8; k < kend; ++k) {
+          const uint32_t pos = first + k;
+          const float4 v0 = ldg4(A.tris + 3 * (size_t)pos);
+          const float4 e1 = ldg4(A.tris + 3 * (size_t)pos + 1);
+          const float4 e2 = ldg4(A.tris + 3 * (size_t)pos + 2);
+          if (kCount) ++tests;
+          float t, u, v;
+          if (!mt_test(o, d, zu, zv, v0, e1, e2, t, u, v)) continue;
+          if (t < bt || (best >= 0 && t == bt && (int32_t)pos < best)) {
+            best = (int32_t)pos; bt = t; bu = u; bv = v;
+          }
+        }
+      }
+      // next subtree whose entry is still within reach
       bool found = false;
       while (sp > 0) {
         --sp;
@@ -267,6 +227,325 @@ __global__ __launch_bounds__(128) void k_trace_accel(TraceArgs A, AccelArgs C) {
   if (kCount) {
     if (A.visits) A.visits[r] = visits;
     if (A.tests) A.tests[r] = tests;
+  }
+}
+
+// Warp-cooperative schedule. Each lane descends its own ray until it holds a
+// leaf (while-while); then every lane tests its own leaf's group boxes, and the
+// (ray, 8-triangle group) items of the whole warp are spread over the 32 lanes:
+// a lane tests one group against the ray of the item's owner (fetched by
+// shuffles) and merges its best hit into the owner's slot with a 64-bit
+// shared-memory atomicMin on (t bits, position), which is the same
+// (t, position) rule as the other schedules. The (u, v) of the current best
+// are written by the lane whose key is the minimum right after its merge.
+constexpr int kCoopWarps = 4;  // 128-thread CTAs
+
+template <bool kCount>
+__device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool valid, const TraceArgs& A, const AccelArgs& C,
+                                                unsigned long long* s_key, float2* s_uv) {
+  const uint32_t lane = lane_id();
+  float4 o = make_float4(0.f, 0.f, 0.f, 0.f), d = make_float4(0.f, 0.f, 1.f, 0.f);
+  float tmax0 = -1.0f;
+  if (valid) {
+    o = ldg4(A.orig + r);
+    d = ldg4(A.dir + r);
+    tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
+  }
+  int32_t best = -1;
+  float bt = tmax0, bu = 0.0f, bv = 0.0f;
+  uint32_t visits = 0, tests = 0;
+  const float ix = 1.0f / fix_dir(d.x), iy = 1.0f / fix_dir(d.y), iz = 1.0f / fix_dir(d.z);
+  const float zu = o.w * 0.0f, zv = d.w * 0.0f;
+  uint32_t st_ref[kStack];
+  float st_t[kStack];
+  int sp = 0;
+  uint32_t ref = __ldg(C.hdr);
+  bool alive = valid && tmax0 > 0.0f;
+  while (__any_sync(0xffffffffu, alive)) {
+    // 1. descend until this ray holds a leaf
+    bool has_leaf = false;
+    if (alive) {
+      while (!(ref & 0x80000000u)) {
+        const float4* tn = C.tnodes + 4 * (size_t)ref;
+        const float4 a0 = ldg4(tn), a1 = ldg4(tn + 1), b0 = ldg4(tn + 2), b1 = ldg4(tn + 3);
+        if (kCount) visits += 2;
+        float ta, tb;
+        const bool ha = slab2(a0, a1, o, ix, iy, iz, bt, ta);
+        const bool hb = slab2(b0, b1, o, ix, iy, iz, bt, tb);
+        const uint32_t ra = __float_as_uint(a0.w), rb = __float_as_uint(b0.w);
+        if (ha && hb) {
+          const bool a_first = ta <= tb;
+          if (sp < kStack) {
+            st_ref[sp] = a_first ? rb : ra;
+            st_t[sp] = a_first ? tb : ta;
+            ++sp;
+          } else if (A.err) {
+            atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
+          }
+          ref = a_first ? ra : rb;
+        } else if (ha) {
+          ref = ra;
+        } else if (hb) {
+          ref = rb;
+        } else {
+          bool found = false;
+          while (sp > 0) {
+            --sp;
+            if (st_t[sp] <= bt * kCullSlack) { ref = st_ref[sp]; found = true; break; }
+          }
+          if (!found) { alive = false; break; }
+        }
+      }
+      has_leaf = alive;
+    }
+    // 2. own leaf: group boxes -> mask of groups to test
+    uint32_t mask = 0, first = 0, cnt = 0;
+    if (has_leaf) {
+      const uint4 L = __ldg(C.leaves + (~ref));
+      if (kCount) ++visits;
+      first = L.x; cnt = L.y;
+      const uint32_t gbase = L.z;
+      const uint32_t ng = (cnt + 7) >> 3;
+      for (uint32_t g = 0; g < ng; ++g) {
+        const float4 gmn = ldg4(C.groups + 2 * ((size_t)gbase + g));
+        const float4 gmx = ldg4(C.groups + 2 * ((size_t)gbase + g) + 1);
+        if (kCount) ++visits;
+        float tg;
+        if (slab2(gmn, gmx, o, ix, iy, iz, bt, tg)) {
+          if (g < 32) mask |= 1u << g;
+        }
+      }
+      // leaves of more than 256 triangles (tree_complete = 0) keep the groups
+      // past 32 to this lane: they are tested below by the owner alone
+    }
+    // 3. spread the warp's (ray, group) items over the lanes
+    const uint32_t my_items = __popc(mask);
+    uint32_t incl = my_items;
+#pragma unroll
+    for (int k = 1; k < 32; k <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, k);
+      if (lane >= (uint32_t)k) incl += y;
+    }
+    const uint32_t excl = incl - my_items;
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    // (t bits, position) of the best hit so far; with no hit yet, (tmax bits, 0),
+    // which no accepted hit equals (t < tmax is required)
+    const unsigned long long key0 = ((unsigned long long)__float_as_uint(bt) << 32) | (uint32_t)(best >= 0 ? best : 0);
+    s_key[lane] = key0;
+    s_uv[lane] = make_float2(bu, bv);
+    __syncwarp();
+    for (uint32_t base = 0; base < total; base += 32) {
+      const uint32_t item = base + lane;
+      unsigned long long cand = ~0ull;
+      float cu = 0.f, cv = 0.f;
+      // owner: last lane whose exclusive offset is <= item
+      uint32_t lo = 0, hi = 31;
+#pragma unroll
+      for (int it = 0; it < 5; ++it) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        const uint32_t off_mid = __shfl_sync(0xffffffffu, excl, mid);
+        if (off_mid <= item) lo = mid; else hi = mid - 1;
+      }
+      const uint32_t owner = lo;
+      const float4 oo = make_float4(__shfl_sync(0xffffffffu, o.x, owner), __shfl_sync(0xffffffffu, o.y, owner),
+                                    __shfl_sync(0xffffffffu, o.z, owner), 0.0f);
+      const float4 od = make_float4(__shfl_sync(0xffffffffu, d.x, owner), __shfl_sync(0xffffffffu, d.y, owner),
+                                    __shfl_sync(0xffffffffu, d.z, owner), 0.0f);
+      const float ozu = __shfl_sync(0xffffffffu, zu, owner), ozv = __shfl_sync(0xffffffffu, zv, owner);
+      const uint32_t omask = __shfl_sync(0xffffffffu, mask, owner);
+      const uint32_t oexcl = __shfl_sync(0xffffffffu, excl, owner);
+      const uint32_t ofirst = __shfl_sync(0xffffffffu, first, owner);
+      const uint32_t ocnt = __shfl_sync(0xffffffffu, cnt, owner);
+      if (item < total) {
+        const uint32_t g = __fns(omask, 0, (int)(item - oexcl) + 1);
+        const uint32_t kend = min(ocnt, g * 8 + 8);
+        const unsigned long long cur = s_key[owner];
+        unsigned long long mine = ~0ull;
+        float mu = 0.f, mv = 0.f;
+        for (uint32_t k = g * 8; k < kend; ++k) {
+          const uint32_t pos = ofirst + k;
+          const float4 v0 = ldg4(A.tris + 3 * (size_t)pos);
+          const float4 e1 = ldg4(A.tris + 3 * (size_t)pos + 1);
+          const float4 e2 = ldg4(A.tris + 3 * (size_t)pos + 2);
+          if (kCount) ++tests;
+          float t, u, v;
+          if (!mt_test(oo, od, ozu, ozv, v0, e1, e2, t, u, v)) continue;
+          const unsigned long long key = ((unsigned long long)__float_as_uint(t) << 32) | pos;
+          if (key < mine) { mine = key; mu = u; mv = v; }
+        }
+        if (mine < cur) atomicMin(s_key + owner, mine);
+        cand = mine;
+        cu = mu; cv = mv;
+      }
+      __syncwarp();
+      // (u, v) of the owner's minimum, written by the one lane holding that key
+      if (item < total && cand != ~0ull && s_key[owner] == cand) s_uv[owner] = make_float2(cu, cv);
+      __syncwarp();
+    }
+    // 4. read back the merged best and move on
+    if (has_leaf) {
+      const unsigned long long k = s_key[lane];
+      if (k < key0) {
+        bt = __uint_as_float((uint32_t)(k >> 32));
+        best = (int32_t)(k & 0xFFFFFFFFu);
+        const float2 uv = s_uv[lane];
+        bu = uv.x; bv = uv.y;
+      }
+      // groups beyond the first 32 (leaves of more than 256 triangles): this lane alone
+      for (uint32_t g = 32; g * 8 < cnt; ++g) {
+        const uint32_t gbase = __ldg(C.leaves + (~ref)).z;
+        const float4 gmn = ldg4(C.groups + 2 * ((size_t)gbase + g));
+        const float4 gmx = ldg4(C.groups + 2 * ((size_t)gbase + g) + 1);
+        float tg;
+        if (!slab2(gmn, gmx, o, ix, iy, iz, bt, tg)) continue;
+        const uint32_t kend = min(cnt, g * 8 + 8);
+        for (uint32_t kk = g * 8; kk < kend; ++kk) {
+          const uint32_t pos = first + kk;
+          const float4 v0 = ldg4(A.tris + 3 * (size_t)pos);
+          const float4 e1 = ldg4(A.tris + 3 * (size_t)pos + 1);
+          const float4 e2 = ldg4(A.tris + 3 * (size_t)pos + 2);
+          if (kCount) ++tests;
+          float t, u, v;
+          if (!mt_test(o, d, zu, zv, v0, e1, e2, t, u, v)) continue;
+          if (t < bt || (best >= 0 && t == bt && (int32_t)pos < best)) { best = (int32_t)pos; bt = t; bu = u; bv = v; }
+        }
+      }
+      bool found = false;
+      while (sp > 0) {
+        --sp;
+        if (st_t[sp] <= bt * kCullSlack) { ref = st_ref[sp]; found = true; break; }
+      }
+      if (!found) alive = false;
+    }
+    __syncwarp();
+  }
+  if (!valid) return;
+  if (best >= 0) {
+    A.hit_id[r] = A.id_mode == 1 ? (int32_t)__ldg(A.indices + best) : best;
+    A.hit_t[r] = bt;
+    A.hit_uv[r] = make_float2(bu, bv);
+  } else {
+    A.hit_id[r] = -1;
+    A.hit_t[r] = tmax0;
+    A.hit_uv[r] = make_float2(0.0f, 0.0f);
+  }
+  if (kCount) {
+    if (A.visits) A.visits[r] = visits;
+    if (A.tests) A.tests[r] = tests;
+  }
+}
+
+// Slot -> ray. With an image width, slots walk 8x4 pixel tiles of the
+// row-major image (a warp traces one tile); otherwise slots are ray indices.
+struct SlotMap {
+  uint32_t width, height, tiles_x, slots;
+  const uint32_t* order;  // optional slot -> ray permutation (rt_ray_order)
+  __device__ __forceinline__ bool ray_of(uint32_t s, uint32_t& r) const {
+    if (order) { r = __ldg(order + s); return s < slots; }
+    if (!width) { r = s; return s < slots; }
+    const uint32_t tile = s >> 5, w = s & 31u;
+    const uint32_t x = (tile % tiles_x) * 8 + (w & 7u), y = (tile / tiles_x) * 4 + (w >> 3);
+    r = y * width + x;
+    return x < width && y < height;
+  }
+};
+
+template <bool kCount, bool kWW>
+__global__ __launch_bounds__(128) void k_trace_accel(TraceArgs A, AccelArgs C, SlotMap M) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t r;
+  if (s < M.slots && M.ray_of(s, r)) trace_ray_accel<kCount, kWW>(r, A, C);
+}
+
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_trace_coop(TraceArgs A, AccelArgs C, SlotMap M) {
+  __shared__ unsigned long long s_key[kCoopWarps][32];
+  __shared__ float2 s_uv[kCoopWarps][32];
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t r = 0;
+  const bool valid = s < M.slots && M.ray_of(s, r);
+  const uint32_t w = threadIdx.x >> 5;
+  trace_warp_coop<kCount>(r, valid, A, C, s_key[w], s_uv[w]);
+}
+
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_trace_coop_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter) {
+  __shared__ unsigned long long s_key[kCoopWarps][32];
+  __shared__ float2 s_uv[kCoopWarps][32];
+  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= M.slots) break;
+    uint32_t r = 0;
+    const uint32_t s = base + lane;
+    const bool valid = s < M.slots && M.ray_of(s, r);
+    trace_warp_coop<kCount>(r, valid, A, C, s_key[w], s_uv[w]);
+  }
+}
+
+// Persistent warps: each warp takes 32 slots at a time from a global counter
+// until the slots run out (the counter is zeroed before the launch).
+template <bool kCount, bool kWW>
+__global__ __launch_bounds__(128) void k_trace_accel_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter) {
+  const uint32_t lane = lane_id();
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= M.slots) break;
+    uint32_t r;
+    const uint32_t s = base + lane;
+    if (s < M.slots && M.ray_of(s, r)) trace_ray_accel<kCount, kWW>(r, A, C);
+  }
+}
+
+// Batched traversal: one launch for the rays of all meshes of rt_batch_build;
+// each ray finds its mesh by binary search over ray_offsets and traverses that
+// mesh's part of the blob with the single-mesh per-ray code.
+struct BatchTraceArgs {
+  uint32_t M;
+  const uint32_t* foff;
+  const uint32_t* roff;
+  BatchAccel acc;
+};
+
+template <bool kCount, bool kWW>
+__global__ __launch_bounds__(128) void k_batch_trace(TraceArgs A, BatchTraceArgs B) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= A.ray_count) return;
+  const uint32_t m = find_seg(B.roff, B.M, r);
+  const uint32_t F = __ldg(B.foff + m);
+  AccelArgs C;
+  C.hdr = B.acc.hdr + 64 * (size_t)m;
+  C.tnodes = B.acc.tnodes + 4 * (size_t)F;
+  C.leaves = B.acc.leaves + F;
+  C.groups = B.acc.groups + 2 * (size_t)group_base(F, m);
+  TraceArgs Am = A;
+  Am.tris = A.tris + 3 * (size_t)F;
+  Am.indices = A.indices + F;
+  trace_ray_accel<kCount, kWW>(r, Am, C);
+}
+
+// Sort key of a ray: direction octant (3 bits) above a 29-bit Morton code of
+// its origin in the given box; inactive rays (tmax <= 0) sort last.
+__global__ __launch_bounds__(256) void k_ray_keys(const float4* __restrict__ orig, const float4* __restrict__ dir,
+                                                 const float* __restrict__ tmax, uint32_t count, float3 lo, float3 scale,
+                                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < count; r += gridDim.x * blockDim.x) {
+    idx[r] = r;
+    if (tmax && !(__ldg(tmax + r) > 0.0f)) { keys[r] = 0xFFFFFFFFu; continue; }
+    const float4 o = ldg4(orig + r), d = ldg4(dir + r);
+    const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+    uint32_t q[3];
+    const float c[3] = {(o.x - lo.x) * scale.x, (o.y - lo.y) * scale.y, (o.z - lo.z) * scale.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) q[a] = min(__float2uint_rz(fmaxf(c[a], 0.0f)), 511u);
+    uint32_t m = 0;
+#pragma unroll
+    for (int b = 0; b < 9; ++b) m |= ((q[0] >> b) & 1u) << (3 * b + 2) | ((q[1] >> b) & 1u) << (3 * b + 1) | ((q[2] >> b) & 1u) << (3 * b);
+    keys[r] = (oct << 27) | m;  // 3 + 27 bits
   }
 }
 
@@ -393,8 +672,45 @@ extern "C" rt_status rt_trace_closest(const rt_trace_desc* d, rt_stream stream) 
     C.tnodes = c.take<float4>(4 * n);
     C.leaves = c.take<uint4>(n);
     C.groups = c.take<float4>(2 * (n / 8 + n + 1));
-    if (count) k_trace_accel<true><<<blocks, 128, 0, st>>>(A, C);
-    else k_trace_accel<false><<<blocks, 128, 0, st>>>(A, C);
+    SlotMap M;
+    M.order = d->ray_order;
+    const uint32_t R = d->ray_count;
+    if (d->ray_order) {
+      M.width = 0; M.height = 0; M.tiles_x = 0; M.slots = R;
+    } else if (d->image_width && R % d->image_width == 0) {
+      M.width = d->image_width;
+      M.height = R / d->image_width;
+      M.tiles_x = (M.width + 7) / 8;
+      M.slots = M.tiles_x * ((M.height + 3) / 4) * 32;
+    } else {
+      M.width = 0; M.height = 0; M.tiles_x = 0; M.slots = R;
+    }
+    const bool ww = (d->schedule & RT_TRACE_WHILE_WHILE) != 0;
+    if (d->schedule & RT_TRACE_COOP) {
+      if (d->work_counter) {
+        if (cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
+        const uint32_t pblocks = (uint32_t)sms() * (d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u);
+        if (count) k_trace_coop_persistent<true><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter);
+        else k_trace_coop_persistent<false><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter);
+      } else {
+        const uint32_t sblocks = (M.slots + 127) / 128;
+        if (count) k_trace_coop<true><<<sblocks, 128, 0, st>>>(A, C, M);
+        else k_trace_coop<false><<<sblocks, 128, 0, st>>>(A, C, M);
+      }
+    } else if (d->work_counter) {
+      if (cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
+      const uint32_t pblocks = (uint32_t)sms() * (d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u);
+#define RT_LAUNCH_P(CNT, WW) k_trace_accel_persistent<CNT, WW><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter)
+      if (count) { if (ww) RT_LAUNCH_P(true, true); else RT_LAUNCH_P(true, false); }
+      else { if (ww) RT_LAUNCH_P(false, true); else RT_LAUNCH_P(false, false); }
+#undef RT_LAUNCH_P
+    } else {
+      const uint32_t sblocks = (M.slots + 127) / 128;
+#define RT_LAUNCH_S(CNT, WW) k_trace_accel<CNT, WW><<<sblocks, 128, 0, st>>>(A, C, M)
+      if (count) { if (ww) RT_LAUNCH_S(true, true); else RT_LAUNCH_S(true, false); }
+      else { if (ww) RT_LAUNCH_S(false, true); else RT_LAUNCH_S(false, false); }
+#undef RT_LAUNCH_S
+    }
     note_launch();
     RT_CHECK_LAUNCH();
     return RT_OK;
@@ -409,6 +725,36 @@ extern "C" rt_status rt_trace_closest(const rt_trace_desc* d, rt_stream stream) 
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
+}
+
+extern "C" rt_status rt_ray_order_scratch_bytes(uint32_t count, size_t* bytes) {
+  if (!bytes) return RT_ERR_INVALID_ARGUMENT;
+  Carve c(nullptr, 0);
+  c.take<uint32_t>(count);
+  *bytes = c.off + radix_scratch_bytes(count) + 512;
+  return RT_OK;
+}
+
+extern "C" rt_status rt_ray_order(const float* orig, const float* dir, const float* tmax, uint32_t count, const float box[6],
+                                  uint32_t* order, void* scratch, size_t scratch_bytes, rt_stream stream) {
+  if (!orig || !dir || !order || !box) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  if (count == 0) return RT_OK;
+  size_t need = 0;
+  rt_ray_order_scratch_bytes(count, &need);
+  if (!scratch || scratch_bytes < need) return RT_ERR_SCRATCH_TOO_SMALL;
+  Carve c(scratch, scratch_bytes);
+  uint32_t* keys = c.take<uint32_t>(count);
+  void* sort_scratch = c.take<char>(radix_scratch_bytes(count));
+  const float3 lo = make_float3(box[0], box[1], box[2]);
+  const float3 sc = make_float3(511.0f / fmaxf(box[3] - box[0], 1e-30f), 511.0f / fmaxf(box[4] - box[1], 1e-30f),
+                                511.0f / fmaxf(box[5] - box[2], 1e-30f));
+  const uint32_t blocks = (uint32_t)hmin<size_t>((count + 255) / 256, (size_t)sms() * 16);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_ray_keys<<<blocks, 256, 0, st>>>((const float4*)orig, (const float4*)dir, tmax, count, lo, sc, keys, order);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return radix_sort_pairs(keys, order, count, 0, 32, 0, sort_scratch, radix_scratch_bytes(count), st, nullptr);
 }
 
 extern "C" rt_status rt_primary_rays(const rt_camera* cam, uint32_t w, uint32_t h, float* orig, float* dir, rt_stream stream) {
@@ -435,6 +781,32 @@ extern "C" rt_status rt_bounce_rays(const float* tris, const float* orig, const 
   const uint32_t blocks = (uint32_t)hmin<size_t>((count + 255) / 256, (size_t)sms() * 16);
   k_bounce<<<blocks, 256, 0, (cudaStream_t)stream>>>((const float4*)tris, (const float4*)orig, (const float4*)dir, hit_pos, hit_t, count,
                                                      seed, (float4*)orig_out, (float4*)dir_out, tmax_out);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_batch_trace(const rt_batch_trace_desc* d, rt_stream stream) {
+  if (!d || d->mesh_count == 0 || !d->face_offsets || !d->ray_offsets || !d->accel || !d->tris || !d->orig || !d->dir ||
+      !d->hit_id || !d->hit_t || !d->hit_uv || d->face_count < d->mesh_count)
+    return RT_ERR_INVALID_ARGUMENT;
+  if (d->id_mode == 1 && !d->indices) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  if (d->ray_count == 0) return RT_OK;
+  TraceArgs A = {};
+  A.tris = (const float4*)d->tris; A.indices = d->indices; A.orig = (const float4*)d->orig; A.dir = (const float4*)d->dir;
+  A.tmax = d->tmax; A.ray_count = d->ray_count; A.id_mode = d->id_mode; A.hit_id = d->hit_id; A.hit_t = d->hit_t;
+  A.hit_uv = (float2*)d->hit_uv; A.visits = d->ray_visits; A.tests = d->ray_tests; A.err = d->error_word;
+  BatchTraceArgs B;
+  B.M = d->mesh_count; B.foff = d->face_offsets; B.roff = d->ray_offsets;
+  Carve c((void*)d->accel, ~(size_t)0);
+  carve_batch_accel_layout(c, B.acc, d->mesh_count, d->face_count);
+  const bool count = d->ray_visits || d->ray_tests;
+  const bool ww = (d->schedule & RT_TRACE_WHILE_WHILE) != 0;
+  const uint32_t blocks = (d->ray_count + 127) / 128;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (count) { if (ww) k_batch_trace<true, true><<<blocks, 128, 0, st>>>(A, B); else k_batch_trace<true, false><<<blocks, 128, 0, st>>>(A, B); }
+  else { if (ww) k_batch_trace<false, true><<<blocks, 128, 0, st>>>(A, B); else k_batch_trace<false, false><<<blocks, 128, 0, st>>>(A, B); }
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;

@@ -122,3 +122,52 @@ def soup_1m_scene(width: int = 1920, height: int = 1080, seed: int = 1, n: int =
     sigma 0.01); 1920 x 1080 primary rays from (0.5, 0.5, -0.4) looking at the
     cube's centre, so that the cube fills the frame, plus one diffuse bounce per hit."""
     return soup(n, seed), Camera((0.5, 0.5, -0.4), (0.5, 0.5, 0.5), FOV_60, width, height)
+
+
+def batch_meshes(count: int = 1024, seed: int = 3, min_faces: int = 64, max_faces: int = 65536):
+    """Independent meshes with face counts log-uniform in [min_faces, max_faces],
+    each a terrain (side chosen so that 2 (s-1)^2 is near the count) or a soup
+    by a fair coin. Returns the list of meshes."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(min_faces), math.log(max_faces)))))
+        if rng.random() < 0.5:
+            side = max(2, int(round(math.sqrt(n / 2.0))) + 1)
+            out.append(terrain(side, seed=int(rng.integers(1 << 30))))
+        else:
+            out.append(soup(n, seed=int(rng.integers(1 << 30))))
+    return out
+
+
+def concat_batch(meshes):
+    """Concatenation for the batched build: faces keep indices local to their mesh."""
+    fo, vo = [0], [0]
+    for m in meshes:
+        fo.append(fo[-1] + m.face_count)
+        vo.append(vo[-1] + m.vertex_count)
+    verts = np.concatenate([m.vertices for m in meshes])
+    faces = np.concatenate([m.faces for m in meshes])
+    return verts, faces, fo, vo
+
+
+def sphere_rays(mesh: Mesh, side: int, seed: int):
+    """side x side rays with origins uniform on the mesh's bounding sphere, each
+    aimed at a uniform point inside the sphere (float32 float4 origin, direction)."""
+    rng = np.random.default_rng(seed)
+    v = mesh.vertices[:, :3].astype(np.float64)
+    c = 0.5 * (v.min(0) + v.max(0))
+    r = max(float(np.linalg.norm(v - c, axis=1).max()), 1e-6) * 1.01
+    R = side * side
+    p = rng.normal(size=(R, 3))
+    p /= np.linalg.norm(p, axis=1, keepdims=True)
+    q = rng.normal(size=(R, 3))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    q *= rng.uniform(size=(R, 1)) ** (1.0 / 3.0)
+    o = c + r * p
+    d = (c + r * q) - o
+    orig = np.zeros((R, 4), np.float32)
+    dirs = np.zeros((R, 4), np.float32)
+    orig[:, :3] = o
+    dirs[:, :3] = d
+    return orig, dirs

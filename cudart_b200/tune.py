@@ -1,0 +1,85 @@
+"""Autotuner for the traversal schedule.
+
+The blob traversal has knobs that change its speed and never its results:
+the ray-to-thread mapping (linear, 8x4 pixel tiles of a row-major image, or
+an order sorted by direction octant and origin Morton code, whose cost is
+part of the timed trace),
+warp-cooperative leaf tests (the warp's lanes share the triangle tests of all
+its rays' leaves), static one-ray-per-thread launches or persistent warps that fetch rays from a
+counter (and how many 128-thread CTAs per SM), and the if-if or while-while
+leaf schedule. ``tune_trace`` times every combination on the caller's own
+rays with CUDA events and returns the fastest; the choice is cached per GPU
+name and workload key in a JSON file (``CUDART_B200_TUNE_CACHE``, default
+``~/.cache/cudart_b200/tune.json``).
+"""
+from __future__ import annotations
+
+import itertools
+import json
+import os
+
+import torch
+
+from . import core
+
+CACHE = os.environ.get("CUDART_B200_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "cudart_b200", "tune.json"))
+
+
+def candidates(image_width: int):
+    widths = [0, image_width] if image_width else [0]
+    out = []
+    for w, ww in itertools.product(widths, (False, True)):
+        out.append({"image_width": w, "persistent": False, "blocks_per_sm": 0, "while_while": ww, "sorted": False})
+        for bps in (8, 16):
+            out.append({"image_width": w, "persistent": True, "blocks_per_sm": bps, "while_while": ww, "sorted": False})
+    for ww, (p, bps) in itertools.product((False, True), ((False, 0), (True, 16))):
+        out.append({"image_width": 0, "persistent": p, "blocks_per_sm": bps, "while_while": ww, "sorted": True})
+    # warp-cooperative leaf tests (always while-while)
+    for w, srt, (p, bps) in itertools.product(widths, (False, True), ((False, 0), (True, 8), (True, 16))):
+        if srt and w:
+            continue
+        out.append({"image_width": w, "persistent": p, "blocks_per_sm": bps, "while_while": True, "sorted": srt, "coop": True})
+    return out
+
+
+def _load():
+    try:
+        with open(CACHE) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def _store(d):
+    try:
+        os.makedirs(os.path.dirname(CACHE), exist_ok=True)
+        with open(CACHE, "w") as f:
+            json.dump(d, f, indent=1)
+    except OSError:
+        pass
+
+
+def tune_trace(tree, orig, dir, tmax=None, image_width: int = 0, key: str = "default", reps: int = 3, use_cache: bool = True):
+    """Returns (best_schedule, timings) where timings is a list of (schedule, ms)."""
+    gpu = torch.cuda.get_device_name(orig.device)
+    cache = _load() if use_cache else {}
+    ck = f"{gpu}|{key}"
+    if ck in cache:
+        return cache[ck]["best"], cache[ck]["timings"]
+    out = core.trace(tree, orig, dir, tmax=tmax)
+    stream = torch.cuda.current_stream()
+    timings = []
+    for sch in candidates(image_width):
+        core.trace(tree, orig, dir, tmax=tmax, out=out, schedule=sch)  # warm
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            core.trace(tree, orig, dir, tmax=tmax, out=out, schedule=sch)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        timings.append((sch, e0.elapsed_time(e1) / reps))
+    best = min(timings, key=lambda x: x[1])[0]
+    if use_cache:
+        cache[ck] = {"best": best, "timings": timings}
+        _store(cache)
+    return best, timings

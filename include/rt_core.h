@@ -32,6 +32,11 @@ extern "C" {
 
 typedef struct CUstream_st* rt_stream; /* a cudaStream_t; NULL = legacy default stream */
 
+/* Layout version of the structs below. A caller compiled against this header
+ * must check rt_abi_version() == RT_ABI_VERSION before passing any struct:
+ * a library built from a different header reads different field offsets. */
+#define RT_ABI_VERSION 5u
+
 typedef enum rt_status {
   RT_OK = 0,
   RT_ERR_INVALID_ARGUMENT = 1,
@@ -106,6 +111,69 @@ rt_status rt_lbvh_accel_bytes(uint32_t face_count, size_t* bytes);
  * called by CUDAMeshTree::buildMeshTreeLBVH (CUDAMeshTree.cpp:88-91). */
 rt_status rt_lbvh_build(const rt_build_desc* desc, rt_stream stream);
 
+/* Batched build of M meshes in one set of launches (no per-mesh host work).
+ * Faces and vertices of all meshes are concatenated; face_offsets[m] and
+ * vertex_offsets[m] (DEVICE arrays of M + 1 entries) delimit mesh m, and its
+ * faces index its own vertices from 0. Every per-mesh output equals what
+ * rt_lbvh_build gives for that mesh alone (same bits), stored at fixed
+ * offsets derived from F_m = face_offsets[m]:
+ *   faces_out, boxes, codes, tris, indices  at position F_m (indices hold mesh-local face ids),
+ *   nodes                                   at node 2 F_m - m (capacity 2 n_m - 1),
+ *   info                                    at entry m,
+ *   accel                                   the batched traversal blob (rt_batch_trace).
+ * The hit box of each mesh is the min/max of its vertices. No reference
+ * counterpart (the reference builds one mesh per call). */
+typedef struct rt_batch_build_desc {
+  uint32_t mesh_count;
+  uint32_t face_count;            /* total */
+  uint32_t vertex_count;          /* total */
+  const uint32_t* face_offsets;   /* DEVICE [mesh_count + 1] */
+  const uint32_t* vertex_offsets; /* DEVICE [mesh_count + 1] */
+  const float* vertices;
+  const uint32_t* faces_in;
+  uint32_t* faces_out;            /* must not alias faces_in */
+  rt_build_params params;         /* tree_complete must be 1 */
+  float* boxes;
+  uint32_t* indices;
+  uint32_t* codes;
+  uint32_t* nodes;                /* >= 2 * face_count - mesh_count records */
+  float* tris;
+  void* accel;
+  size_t accel_bytes;
+  rt_build_info* info;            /* DEVICE [mesh_count] */
+  void* scratch;
+  size_t scratch_bytes;
+} rt_batch_build_desc;
+rt_status rt_batch_sizes(uint32_t mesh_count, uint32_t face_count, const rt_build_params* params, size_t* scratch_bytes,
+                         size_t* accel_bytes);
+rt_status rt_batch_build(const rt_batch_build_desc* desc, rt_stream stream);
+
+/* One traversal launch for the rays of all meshes of a batched build: the rays
+ * of mesh m are ray_offsets[m] .. ray_offsets[m+1] (DEVICE, M + 1 entries).
+ * Hit ids are positions (id_mode 0) or face ids (id_mode 1) inside the mesh. */
+typedef struct rt_batch_trace_desc {
+  uint32_t mesh_count;
+  const uint32_t* face_offsets;   /* DEVICE [mesh_count + 1], as given to rt_batch_build */
+  const uint32_t* ray_offsets;    /* DEVICE [mesh_count + 1] */
+  const void* accel;              /* from rt_batch_build */
+  const float* tris;
+  const uint32_t* indices;
+  uint32_t face_count;            /* total, as given to rt_batch_build */
+  const float* orig;
+  const float* dir;
+  const float* tmax;              /* optional */
+  uint32_t ray_count;
+  uint32_t id_mode;
+  int32_t* hit_id;
+  float* hit_t;
+  float* hit_uv;
+  uint32_t* ray_visits;
+  uint32_t* ray_tests;
+  uint32_t* error_word;
+  uint32_t schedule;              /* RT_TRACE_WHILE_WHILE */
+} rt_batch_trace_desc;
+rt_status rt_batch_trace(const rt_batch_trace_desc* desc, rt_stream stream);
+
 /* Per-face boxes and indices[k] = k.
  * Replaces CUDA_calcMeshBoxes (kernels/CUDA_calcMeshBoxes.cu:65-104). */
 rt_status rt_mesh_boxes(const float* vertices, const uint32_t* faces, uint32_t face_count, float* boxes, uint32_t* indices, rt_stream stream);
@@ -178,7 +246,24 @@ typedef struct rt_trace_desc {
   uint32_t* error_word;     /* optional device word: RT_DEVERR_* bits are OR-ed in */
   const void* accel;        /* optional traversal blob from rt_lbvh_build (with tris): faster, same results */
   uint32_t face_count_hint; /* the face count the blob was built for (required with accel) */
+  /* schedule of the blob traversal (results never depend on it): */
+  uint32_t image_width;     /* > 0 and dividing ray_count: rays are a row-major image; a warp takes an 8x4 pixel tile */
+  uint32_t* work_counter;   /* optional device word: persistent warps fetch rays through it (the call zeroes it) */
+  uint32_t persistent_blocks_per_sm; /* with work_counter: CTAs of 128 threads per SM (0 = 8) */
+  uint32_t schedule;        /* RT_TRACE_* bits */
+  const uint32_t* ray_order; /* optional permutation from rt_ray_order: threads take rays in this order */
 } rt_trace_desc;
+
+#define RT_TRACE_WHILE_WHILE 0x1u /* descend until a leaf is held, then test it (else: interleaved) */
+#define RT_TRACE_COOP 0x2u        /* the warp's lanes share the triangle tests of all its rays' leaves */
+
+/* A tracing order for incoherent rays: ray indices sorted by direction octant,
+ * then by the Morton code of the origin inside box (min xyz, max xyz, HOST);
+ * rays with tmax <= 0 go last. Feed it to rt_trace_desc.ray_order (results
+ * stay in each ray's own slot). No reference counterpart. */
+rt_status rt_ray_order_scratch_bytes(uint32_t count, size_t* scratch_bytes);
+rt_status rt_ray_order(const float* orig, const float* dir, const float* tmax, uint32_t count, const float box[6], uint32_t* order,
+                       void* scratch, size_t scratch_bytes, rt_stream stream);
 
 /* Closest hit per ray: the minimum (t, position) over all triangles that the
  * Moller-Trumbore test of kernels/CUDA_raytraceMeshTree.cu:57-89 accepts with
@@ -186,14 +271,70 @@ typedef struct rt_trace_desc {
  * called by CUDARaytracer::raytraceMeshTree (CUDARaytracer.cpp:130-135). */
 rt_status rt_trace_closest(const rt_trace_desc* desc, rt_stream stream);
 
+typedef struct rt_interp_desc {
+  const int32_t* hit_id;   /* from rt_trace_closest with id_mode 0 (face positions); < 0 = miss */
+  const float* hit_uv;     /* float2 per ray */
+  uint32_t count;          /* rays */
+  const uint32_t* faces;   /* uint4 faces indexed by hit_id (the build's reordered faces) */
+  const float* vertices;   /* float4 per vertex */
+  const float* normals;    /* optional float4 per vertex (CUDAMesh::getNormalsArray); NULL = face normal */
+  const float* colors;     /* optional float4 per vertex; NULL = white */
+  const float* texcoords;  /* optional float2 per vertex; NULL = (u, v) */
+  float* out_points;       /* optional outputs, one per ray: float4 */
+  float* out_normals;      /* float4 */
+  float* out_colors;       /* float4 */
+  float* out_texcoords;    /* float2 */
+  uint32_t* out_materials; /* face.w */
+} rt_interp_desc;
+
+/* Hit point, normal, color, texcoord and material per ray from (face, u, v).
+ * Replaces CUDA_interpolateData (kernels/CUDA_interpolateData.cu:216-256),
+ * called by CUDARaytracer::interpolateOutputSurfaces (CUDARaytracer.cpp:144-162).
+ * Misses write zeros. */
+rt_status rt_interpolate(const rt_interp_desc* desc, rt_stream stream);
+
 /* One cosine-weighted diffuse bounce per hit (PCG32 stream = ray index);
  * misses give an inactive ray with tmax = -1. Workload generation for the
  * incoherent scene; no reference counterpart. */
 rt_status rt_bounce_rays(const float* tris, const float* orig, const float* dir, const int32_t* hit_pos, const float* hit_t,
                          uint32_t ray_count, uint64_t seed, float* orig_out, float* dir_out, float* tmax_out, rt_stream stream);
 
+/* Mesh and tree chunk files (HOST calls; arrays may be device or host memory).
+ * Same bytes as CUDAMesh::quickSave / CUDAMeshTree::quickSave with
+ * overwrite = true (CUDAMesh.cpp:253-400, CUDAMeshTree.cpp:194-289); readers
+ * follow CUDAMesh::quickLoad / CUDAMeshTree::quickLoad (CUDAMesh.cpp:134-251,
+ * CUDAMeshTree.cpp:114-192) but require stored counts EQUAL to the buffers'
+ * (the reference's tree loader inverts that check), and appending
+ * (overwrite = 0) writes whole chunks (the reference's append mode corrupts
+ * the chunk lengths). A NULL array pointer skips that chunk; *_info fills the
+ * counts (and the hit box) so that the caller can size the buffers. */
+typedef struct rt_mesh_file {
+  float hitbox[8];
+  int32_t has_hitbox;
+  uint32_t vertex_count, normal_count, color_count, texcoord_count, face_count;
+  float* vertices;   /* float4 */
+  float* normals;    /* float4 */
+  float* colors;     /* float4 */
+  float* texcoords;  /* float2 */
+  uint32_t* faces;   /* uint4 */
+} rt_mesh_file;
+typedef struct rt_tree_file {
+  uint32_t node_count, index_count, box_count;
+  uint32_t* nodes;    /* bvnode */
+  uint32_t* indices;  /* uint */
+  float* boxes;       /* aabox */
+} rt_tree_file;
+rt_status rt_mesh_file_save(const char* path, int overwrite, const rt_mesh_file* mesh);
+rt_status rt_mesh_file_info(const char* path, rt_mesh_file* mesh);
+rt_status rt_mesh_file_load(const char* path, rt_mesh_file* mesh);
+rt_status rt_tree_file_save(const char* path, int overwrite, const rt_tree_file* tree);
+rt_status rt_tree_file_info(const char* path, rt_tree_file* tree);
+rt_status rt_tree_file_load(const char* path, rt_tree_file* tree);
+
 const char* rt_status_string(rt_status status);
 uint32_t rt_version(void);
+/* RT_ABI_VERSION of the header the library was built with. */
+uint32_t rt_abi_version(void);
 /* RT_OK when a CUDA device is usable, RT_ERR_NO_DEVICE otherwise. */
 rt_status rt_device_check(void);
 /* Kernels this library has launched in this process (to count the kernels of a timed region). */

@@ -53,6 +53,7 @@ def lib():
         L.or_primary_rays.argtypes = [_P, C.c_int, C.c_int, _P, _P]
         L.or_lbvh_build.argtypes = [_P, _U32, _P, _U32, _P, _U32, C.c_int, C.c_int, _P, _P, _P, _P, _U32, _P, _P, _P]
         L.or_build_topology.argtypes = [_P, _U32, _U32, C.c_int, _U32, _U32, _P, _U32, _P]
+        L.or_interpolate.argtypes = [_P, _P, C.c_long, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]
         _lib = L
     return _lib
 
@@ -71,6 +72,7 @@ def ref():
         R.ref_reorder_faces.argtypes = [_P, _P, _U32, _P]
         R.ref_trace.argtypes = [_P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P]
         R.ref_camera_rays.argtypes = [_P, _P, C.c_float, C.c_float, C.c_int, C.c_int, _P, _P, _P, _P]
+        R.ref_interpolate.argtypes = [_P, _P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]
         _ref = R
     return _ref
 
@@ -195,6 +197,16 @@ def bounce_rays(tris, orig, dir, hit_pos, hit_t, seed):
     return o, d, dep
 
 
+def interpolate(hit_id, hit_uv, faces, vertices, normals=None, colors=None, texcoords=None):
+    R = len(hit_id)
+    out = dict(points=np.zeros((R, 4), np.float32), normals=np.zeros((R, 4), np.float32), colors=np.zeros((R, 4), np.float32),
+               texcoords=np.zeros((R, 2), np.float32), materials=np.zeros(R, np.uint32))
+    lib().or_interpolate(_ptr(hit_id), _ptr(hit_uv), C.c_long(R), _ptr(faces), _ptr(vertices), _ptr(normals), _ptr(colors),
+                         _ptr(texcoords), _ptr(out["points"]), _ptr(out["normals"]), _ptr(out["colors"]), _ptr(out["texcoords"]),
+                         _ptr(out["materials"]))
+    return out
+
+
 def max_threads() -> int:
     return int(lib().or_max_threads())
 
@@ -247,3 +259,14 @@ def ref_camera_rays(cam):
     ref().ref_camera_rays(_ptr(np.asarray(cam.center, np.float32)), _ptr(np.asarray(cam.target, np.float32)), C.c_float(cam.fov),
                           C.c_float(cam.ratio), C.c_int(cam.width), C.c_int(cam.height), _ptr(ang), _ptr(basis), _ptr(o), _ptr(d))
     return o, d, basis, ang
+
+
+def ref_interpolate(hit_id, hit_uv, width, height, faces, vertices, normals=None, colors=None, texcoords=None):
+    """The reference kernel_interpolateData run per pixel (ids must be valid face positions)."""
+    R = width * height
+    out = dict(points=np.zeros((R, 4), np.float32), normals=np.zeros((R, 4), np.float32), colors=np.zeros((R, 4), np.float32),
+               texcoords=np.zeros((R, 2), np.float32), materials=np.zeros(R, np.uint32))
+    ref().ref_interpolate(_ptr(hit_id), _ptr(hit_uv), C.c_int(width), C.c_int(height), _ptr(faces), _ptr(vertices), _ptr(normals),
+                          _ptr(colors), _ptr(texcoords), _ptr(out["points"]), _ptr(out["normals"]), _ptr(out["colors"]),
+                          _ptr(out["texcoords"]), _ptr(out["materials"]))
+    return out

@@ -12,7 +12,8 @@
 # preceded by a #line directive, so diagnostics point at the reference file.
 #
 # Output: oracle/_ref/libref_cudart.so exporting ref_mesh_boxes, ref_lbvh_build,
-# ref_reorder_faces, ref_trace, ref_camera_rays. TEST INFRASTRUCTURE ONLY.
+# ref_reorder_faces, ref_trace, ref_camera_rays, ref_interpolate, ref_mesh_quick_save,
+# ref_mesh_quick_load, ref_tree_quick_save. TEST INFRASTRUCTURE ONLY.
 #
 # Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
 set -euo pipefail
@@ -100,6 +101,30 @@ P=kernels/CUDA_calcPrimaryRays.cu
   echo "}"
 } | build_tu ref_rays
 
-g++ -shared -fPIC -o "$OUT/libref_cudart.so" "$OUT"/ref_lbvh.o "$OUT"/ref_boxes.o "$OUT"/ref_reorder.o "$OUT"/ref_trace.o "$OUT"/ref_rays.o
+I=kernels/CUDA_interpolateData.cu
+{
+  cat "$SHIM/prelude.hpp"
+  echo "namespace tu_interp {"
+  rng "$I" 23 31      # textures
+  rng "$I" 37 39      # block sizes
+  rng "$I" 45 138     # kernel_interpolateData
+  cat "$SHIM/interp_epilogue.hpp"
+  echo "}"
+} | build_tu ref_interp
+
+{
+  cat "$SHIM/prelude.hpp"
+  echo "#include <stdio.h>"
+  echo "namespace tu_file {"
+  cat "$SHIM/mesh_shim.hpp"
+  echo "namespace renderkit {"
+  rng CUDAMesh.cpp 134 400       # CUDAMesh::quickLoad, CUDAMesh::quickSave
+  rng CUDAMeshTree.cpp 194 289   # CUDAMeshTree::quickSave
+  echo "}"
+  cat "$SHIM/file_epilogue.hpp"
+  echo "}"
+} | build_tu ref_file
+
+g++ -shared -fPIC -o "$OUT/libref_cudart.so" "$OUT"/ref_lbvh.o "$OUT"/ref_boxes.o "$OUT"/ref_reorder.o "$OUT"/ref_trace.o "$OUT"/ref_rays.o "$OUT"/ref_interp.o "$OUT"/ref_file.o
 rm -f "$OUT"/*.o
 echo "built $OUT/libref_cudart.so"

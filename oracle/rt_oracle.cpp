@@ -658,6 +658,52 @@ OR_API void or_bounce_rays(const float* tris, const float* orig, const float* di
   }
 }
 
+// ---------------------------------------------------------------------------
+// Attribute interpolation, kernels/CUDA_interpolateData.cu:45-138: weights
+// (1 - u - v, u, v), sums left to right, normalize with 1/sqrtf (the reference's
+// device rsqrtf is an approximate instruction). A miss (id < 0) gives zeros.
+// outputs: points/normals/colors float4, texcoords float2, materials u32; NULL = skip.
+// ---------------------------------------------------------------------------
+OR_API void or_interpolate(const int32_t* hit_id, const float* hit_uv, long count, const u32* faces, const float* vertices,
+                           const float* normals, const float* colors, const float* texcoords,
+                           float* out_points, float* out_normals, float* out_colors, float* out_texcoords, u32* out_materials) {
+  const U4* f = (const U4*)faces; const F4* v = (const F4*)vertices;
+  const F4* nrm = (const F4*)normals; const F4* col = (const F4*)colors;
+#pragma omp parallel for schedule(static)
+  for (long l = 0; l < count; ++l) {
+    int32_t id = hit_id[l];
+    if (id < 0) {
+      F4 z = {0, 0, 0, 0};
+      if (out_points) ((F4*)out_points)[l] = z;
+      if (out_normals) ((F4*)out_normals)[l] = z;
+      if (out_colors) ((F4*)out_colors)[l] = z;
+      if (out_texcoords) { out_texcoords[2 * l] = 0; out_texcoords[2 * l + 1] = 0; }
+      if (out_materials) out_materials[l] = 0;
+      continue;
+    }
+    float u = hit_uv[2 * l], w = hit_uv[2 * l + 1];
+    U4 face = f[id];
+    F4 v0 = v[face.x], v1 = v[face.y], v2 = v[face.z];
+    float w0 = 1 - u - w;
+    auto lerp = [&](F4 a, F4 b, F4 c) { return f4add(f4add(f4scale(a, w0), f4scale(b, u)), f4scale(c, w)); };
+    if (out_points) ((F4*)out_points)[l] = lerp(v0, v1, v2);
+    if (out_normals) {
+      F4 n = nrm ? normalize4(lerp(nrm[face.x], nrm[face.y], nrm[face.z])) : normalize4(cross4(f4sub(v1, v0), f4sub(v2, v0)));
+      ((F4*)out_normals)[l] = n;
+    }
+    if (out_colors) ((F4*)out_colors)[l] = col ? lerp(col[face.x], col[face.y], col[face.z]) : F4{1.0f, 1.0f, 1.0f, 1.0f};
+    if (out_texcoords) {
+      if (texcoords) {
+        const float* t0 = texcoords + 2 * (size_t)face.x; const float* t1 = texcoords + 2 * (size_t)face.y;
+        const float* t2 = texcoords + 2 * (size_t)face.z;
+        out_texcoords[2 * l] = t0[0] * w0 + t1[0] * u + t2[0] * w;
+        out_texcoords[2 * l + 1] = t0[1] * w0 + t1[1] * u + t2[1] * w;
+      } else { out_texcoords[2 * l] = u; out_texcoords[2 * l + 1] = w; }
+    }
+    if (out_materials) out_materials[l] = face.w;
+  }
+}
+
 OR_API int or_max_threads() {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -272,3 +272,94 @@ def test_soup_1m_full_size(T, oracle):
                       np.ascontiguousarray(et[sel]))
     assert np.array_equal(_host(out2["id"])[sel], e2["id"])
     assert np.array_equal(_u32(_host(out2["t"])[sel]), _u32(e2["t"]))
+
+
+def test_trace_schedules_identical(T, oracle):
+    """Every traversal schedule of the blob path returns the same bits."""
+    from cudart_b200 import core, tune
+    mesh = scenes.soup(100000, seed=31)
+    v, f, tree, ref = _check_build(T, oracle, mesh)
+    cam = scenes.Camera((0.5, 0.5, -0.4), (0.5, 0.5, 0.5), scenes.FOV_60, 200, 120)
+    o, d = _rays(T, cam)
+    base = core.trace(tree, o, d, use_accel=False)
+    bo, bd, bt = core.bounce_rays(tree.tris, o, d, base["id"], base["t"], 5)
+    base2 = core.trace(tree, bo, bd, tmax=bt, use_accel=False)
+    for sch in tune.candidates(cam.width):
+        out = core.trace(tree, o, d, schedule=sch)
+        out2 = core.trace(tree, bo, bd, tmax=bt, schedule=sch)
+        T.cuda.synchronize()
+        assert int(_host(out["err"])[0]) == 0, sch
+        for a, b in ((out, base), (out2, base2)):
+            assert T.equal(a["id"], b["id"]) and T.equal(a["t"], b["t"]) and T.equal(a["uv"], b["uv"]), sch
+
+
+@pytest.mark.parametrize("attrs", [False, True])
+def test_interpolate_matches_oracle(T, oracle, attrs):
+    from cudart_b200 import core
+    mesh, cam = scenes.terrain_small_scene(256, 160)
+    v, f, tree, ref = _check_build(T, oracle, mesh)
+    o, d = _rays(T, cam)
+    hits = core.trace(tree, o, d)
+    rng = np.random.default_rng(2)
+    V = mesh.vertex_count
+    nrm = rng.normal(size=(V, 4)).astype(np.float32) if attrs else None
+    col = rng.uniform(size=(V, 4)).astype(np.float32) if attrs else None
+    tex = rng.uniform(size=(V, 2)).astype(np.float32) if attrs else None
+    out = core.interpolate(tree, v, hits, *(None if a is None else _dev(T, a) for a in (nrm, col, tex)))
+    T.cuda.synchronize()
+    e = oracle.interpolate(_host(hits["id"]), _host(hits["uv"]), ref["faces"], mesh.vertices, nrm, col, tex)
+    for k in ("points", "normals", "colors", "texcoords", "materials"):
+        assert np.array_equal(_u32(_host(out[k])), _u32(e[k])), k
+
+
+def test_file_round_trip_device(T, oracle, tmp_path):
+    """quickSave/quickLoad-format files from and into device buffers."""
+    from cudart_b200 import core
+    mesh = scenes.soup(20000, seed=51)
+    v, f, tree, ref = _check_build(T, oracle, mesh)
+    hb = oracle.hitbox(mesh.vertices)
+    path = str(tmp_path / "scene.bin")
+    core.mesh_save(path, v, f, hb)
+    core.tree_save(path, tree, overwrite=False)
+    m = core.mesh_load(path)
+    t = core.tree_load(path)
+    assert np.array_equal(np.array(m["hitbox"], np.float32), hb)
+    assert T.equal(m["vertices"], v) and T.equal(m["faces"], f)
+    nc = tree.node_count
+    assert T.equal(t["nodes"], tree.nodes[:nc]) and T.equal(t["indices"], tree.indices) and T.equal(t["boxes"], tree.boxes)
+
+
+def test_batch_build_and_trace_match_single_mesh(T, oracle):
+    """Every mesh of a batched build equals its single-mesh build bit for bit,
+    and one batched trace launch equals the per-mesh traces."""
+    from cudart_b200 import core
+    meshes = [scenes.soup(1, seed=1), scenes.soup(17, seed=2), scenes.terrain(9, 3), scenes.soup(224, seed=4),
+              scenes.soup(5000, seed=5), scenes.terrain(64, 6), scenes.soup(33000, seed=7), scenes.soup(2, seed=8)]
+    verts, faces, fo, vo = scenes.concat_batch(meshes)
+    bt = core.batch_build(_dev(T, verts), _dev(T, faces.view(np.int32)), fo, vo)
+    rays = [scenes.sphere_rays(m, 24 + 8 * i, seed=100 + i) for i, m in enumerate(meshes)]
+    ro = [0]
+    for o, _ in rays:
+        ro.append(ro[-1] + len(o))
+    O = _dev(T, np.concatenate([o for o, _ in rays]))
+    D = _dev(T, np.concatenate([d for _, d in rays]))
+    hits = core.batch_trace(bt, O, D, T.tensor(ro, dtype=T.int32, device="cuda"))
+    T.cuda.synchronize()
+    info = _host(bt.info)
+    assert np.all(info[:, 7] == 0), info
+    for m, mesh in enumerate(meshes):
+        v, f, tree = _build(T, mesh)
+        nc = tree.node_count
+        assert int(info[m, 0]) == nc
+        F0, F1 = fo[m], fo[m + 1]
+        assert T.equal(bt.mesh_nodes(m, nc), tree.nodes[:nc]), m
+        assert T.equal(bt.indices[F0:F1], tree.indices), m
+        assert T.equal(bt.codes[F0:F1], tree.codes), m
+        assert T.equal(bt.faces[F0:F1], tree.faces), m
+        assert T.equal(bt.tris[F0:F1], tree.tris), m
+        assert T.equal(bt.boxes[F0:F1], tree.boxes), m
+        single = core.trace(tree, _dev(T, rays[m][0]), _dev(T, rays[m][1]))
+        T.cuda.synchronize()
+        sl = slice(ro[m], ro[m + 1])
+        assert T.equal(hits["id"][sl], single["id"]) and T.equal(hits["t"][sl], single["t"]) and T.equal(hits["uv"][sl], single["uv"]), m
+    assert int(_host(hits["err"])[0]) == 0

@@ -76,3 +76,26 @@ def test_degenerate_inputs(oracle):
     v = m.vertices.copy()
     v[1::3] = v[0::3]  # collinear / degenerate triangles (two equal vertices)
     _check(oracle, scenes.Mesh(v, m.faces), CAM)
+
+
+def test_interpolation_matches_reference(oracle):
+    """kernels/CUDA_interpolateData.cu:45-138 (compiled from the reference) vs the
+    oracle, with and without per-vertex normals / colors / texcoords."""
+    mesh, cam = scenes.terrain_small_scene(96, 64)
+    res = oracle.lbvh_build(mesh.vertices, mesh.faces)
+    o, d, _, _ = oracle.primary_rays(cam)
+    tr = oracle.trace(res["nodes"], res["tris"], res["indices"], o, d)
+    hit = tr["id"] >= 0
+    assert hit.any()
+    ids = np.where(hit, tr["id"], 0).astype(np.int32)  # the reference reads some face on a miss; compare hits only
+    rng = np.random.default_rng(1)
+    V = mesh.vertex_count
+    normals = rng.normal(size=(V, 4)).astype(np.float32)
+    normals[:, 3] = 0
+    colors = rng.uniform(size=(V, 4)).astype(np.float32)
+    texc = rng.uniform(size=(V, 2)).astype(np.float32)
+    for attrs in ((None, None, None), (normals, colors, texc)):
+        e = oracle.interpolate(ids, tr["uv"], res["faces"], mesh.vertices, *attrs)
+        r = oracle.ref_interpolate(ids.view(np.uint32), tr["uv"], cam.width, cam.height, res["faces"], mesh.vertices, *attrs)
+        for k in ("points", "normals", "colors", "texcoords", "materials"):
+            assert np.array_equal(_u32(e[k][hit]), _u32(r[k][hit])), k
