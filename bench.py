@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--faces", type=int, default=1 << 20)
     ap.add_argument("--build16m", type=int, default=1, help="also time the LBVH build alone on a 2^24-face soup")
     ap.add_argument("--batch", type=int, default=1, help="also time the batched workload (1024 meshes, CUDA graph)")
+    ap.add_argument("--learned", type=int, default=1, help="also train and time the learned subtree proposal (4M-triangle scene)")
+    ap.add_argument("--learned-scale", type=float, default=1.0, help="triangle-count scale of the learned-proposal scene")
     return ap.parse_args()
 
 
@@ -280,6 +282,8 @@ def run_ours(args, rank, world, local_rank):
         result["build_16m"] = build_only(24, args, dev, world)
     if args.batch:
         result["batch_c2"] = batched(args, dev, world)
+    if args.learned:
+        result["nn_proposal_c3"] = learned(args, dev, world)
     clocks = clk.summary()
     sampler.stop()
     result["clocks"] = {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
@@ -415,6 +419,113 @@ def batched(args, dev, world, count=1024):
            "device_errors": int((info[:, 7] != 0).sum()), "graph": "build + trace captured in one CUDA graph"}
     del graph
     return res
+
+
+def learned(args, dev, world, train_rays=16 << 20, eval_rays=8 << 20, batch=8192, lr=2e-3):
+    """Learned subtree proposal: 4,022,242-triangle terrain + soup scene, tree
+    cut at depth 12 (4096 slots). Training set: 16M rays (origins uniform in the
+    scene box grown 1.5x, directions uniform on the sphere) labelled by the plain
+    traversal; rays that miss are left out. One epoch of Adam (batch 8192,
+    cosine learning rate) on the GPU through the project's GEMM / softmax / Adam
+    kernels. Evaluation: 8M fresh rays traced plain and with the proposal (MLP
+    inference + seeded traversal); hits compared bit for bit. The "oracle" line
+    seeds every ray with its true slot: the most any proposal can save."""
+    import math
+
+    import torch
+
+    from cudart_b200 import core, proposal, scenes, tune
+
+    scale = args.learned_scale
+    mesh = scenes.learned_scene(scale)
+    box = scenes.scene_box(mesh, 1.5)
+    V = torch.from_numpy(mesh.vertices).to(dev)
+    Fc = torch.from_numpy(mesh.faces.view(np.int32)).to(dev)
+    N = mesh.face_count
+    del mesh
+    tree = core.build_lbvh(V, Fc)
+    slots = proposal.subtree_slots(tree, proposal.DEPTH)
+    to, td = scenes.box_rays_torch(int(train_rays * scale) if scale < 1 else train_rays, box, seed=1, device=dev)
+    eo, ed = scenes.box_rays_torch(int(eval_rays * scale) if scale < 1 else eval_rays, box, seed=2, device=dev)
+    sched, _ = tune.tune_trace(tree, eo, ed, key=f"learned{N}", use_cache=False)
+    lab_hits = core.trace(tree, to, td, schedule=sched)
+    labels = proposal.hit_labels(lab_hits["id"], slots["pos_label"])
+    keep = labels >= 0
+    to, td, tl = to[keep].contiguous(), td[keep].contiguous(), labels[keep].contiguous()
+    del lab_hits, labels, keep
+    n_train = (to.shape[0] // batch) * batch
+    steps = n_train // batch
+    net = proposal.ProposalNet(seed=0, device=dev)
+    g = torch.Generator(device=dev).manual_seed(3)
+    perm = torch.randperm(to.shape[0], device=dev, generator=g)[:n_train]
+    to, td, tl = to[perm].contiguous(), td[perm].contiguous(), tl[perm].contiguous()
+    del perm
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    first_loss = None
+    for st in range(steps):
+        sl = slice(st * batch, (st + 1) * batch)
+        cur = lr * 0.5 * (1.0 + math.cos(math.pi * st / steps))
+        loss = net.train_step(to[sl], td[sl], tl[sl], box, lr=cur)
+        if st == 0:
+            first_loss = loss
+    ev1.record()
+    torch.cuda.synchronize()
+    train_ms = ev0.elapsed_time(ev1)
+    last_loss = loss.item()
+    flop_fwd = 2.0 * (144 * 128 + 2 * 128 * 128 + 128 * 4096)
+    del to, td, tl
+
+    R = eo.shape[0]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    plain = core.trace(tree, eo, ed, counters=True, schedule=sched)
+    prop = net.propose(eo, ed, box)
+    seeded = proposal.trace_seeded(tree, eo, ed, prop, slots, counters=True, in_proposal=True, schedule=sched)
+    oracle_prop = proposal.hit_labels(plain["id"], slots["pos_label"])
+    best = proposal.trace_seeded(tree, eo, ed, oracle_prop, slots, counters=True, schedule=sched)
+    torch.cuda.synchronize()
+    exact = (torch.equal(plain["id"], seeded["id"]) and torch.equal(plain["t"].view(torch.int32), seeded["t"].view(torch.int32))
+             and torch.equal(plain["uv"].view(torch.int32), seeded["uv"].view(torch.int32)))
+    hit = plain["id"] >= 0
+    acc = float(seeded["in_proposal"][hit].float().mean().item())
+    vp, tp = plain["visits"].sum().item(), plain["tests"].sum().item()
+
+    def timed(fn, reps=3):
+        out = []
+        for _ in range(reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            out.append(a.elapsed_time(b))
+        return min(out)
+
+    hits_p = core.trace(tree, eo, ed, schedule=sched)
+    hits_s = proposal.trace_seeded(tree, eo, ed, prop, slots, schedule=sched)
+    ms_plain = timed(lambda: core.trace(tree, eo, ed, schedule=sched, out=hits_p))
+    ms_mlp = timed(lambda: net.propose(eo, ed, box, out=prop))
+    ms_seeded = timed(lambda: proposal.trace_seeded(tree, eo, ed, prop, slots, schedule=sched, out=hits_s))
+    ms_oracle = timed(lambda: proposal.trace_seeded(tree, eo, ed, oracle_prop, slots, schedule=sched, out=hits_s))
+    ms_nn = ms_mlp + ms_seeded
+    del flush
+    return {"faces": N, "train_rays": train_rays, "train_hits": n_train, "train_steps": steps, "batch": batch,
+            "train_ms": round(train_ms, 2), "train_ms_per_step": round(train_ms / max(steps, 1), 4),
+            "train_tflops": round(3 * flop_fwd * n_train / (train_ms * 1e-3) / 1e12, 1),
+            "loss_first": round(float(first_loss.item()), 4), "loss_last": round(last_loss, 4),
+            "eval_rays": R, "hit_fraction": round(float(hit.float().mean().item()), 4), "schedule": sched,
+            "bit_exact": bool(exact), "proposal_accuracy": round(acc, 4),
+            "plain_ms": round(ms_plain, 4), "plain_mrays_s": round(world * R / (ms_plain * 1e-3) / 1e6, 2),
+            "mlp_ms": round(ms_mlp, 4), "mlp_tflops": round(flop_fwd * R / (ms_mlp * 1e-3) / 1e12, 1),
+            "seeded_ms": round(ms_seeded, 4), "nn_mrays_s": round(world * R / (ms_nn * 1e-3) / 1e6, 2),
+            "nn_over_plain": round(ms_plain / ms_nn, 4), "seeded_only_over_plain": round(ms_plain / ms_seeded, 4),
+            "visits_ratio": round(seeded["visits"].sum().item() / vp, 4), "tests_ratio": round(seeded["tests"].sum().item() / tp, 4),
+            "oracle_proposal": {"ms": round(ms_oracle, 4), "over_plain": round(ms_plain / ms_oracle, 4),
+                                "visits_ratio": round(best["visits"].sum().item() / vp, 4),
+                                "tests_ratio": round(best["tests"].sum().item() / tp, 4)},
+            "mean_visits_plain": round(vp / R, 3), "mean_tests_plain": round(tp / R, 3)}
 
 
 def run_e2e(args, mesh, camera, W, H, dev, world, sched1=None, sched2=None):

@@ -1,4 +1,5 @@
-"""ctypes declarations of the C ABI in include/rt_core.h (librt_core.so).
+"""ctypes declarations of the C ABI in include/rt_core.h and include/rt_propose.h
+(librt_core.so).
 
 Loading fails loudly when the shared library is missing: there is no CPU
 fallback for any compute entry point.
@@ -18,6 +19,8 @@ STATUS_NAMES = {0: "RT_OK", 1: "RT_ERR_INVALID_ARGUMENT", 2: "RT_ERR_NO_DEVICE",
 DEVERR_NODE_CAPACITY = 0x1
 DEVERR_STACK_OVERFLOW = 0x2
 DEVERR_MORTON_CAPACITY = 0x4
+DEVERR_WAIT_TIMEOUT = 0x8
+PROPOSE_ABI_VERSION = 1  # RT_PROPOSE_ABI_VERSION of include/rt_propose.h
 TRACE_WHILE_WHILE = 0x1
 TRACE_COOP = 0x2
 
@@ -27,6 +30,11 @@ EXPORTS = (
     "rt_radix_sort_pairs", "rt_radix_sort_pairs_static", "rt_radix_sort_keys", "rt_camera_look_at", "rt_camera_basis", "rt_primary_rays",
     "rt_trace_closest", "rt_ray_order_scratch_bytes", "rt_ray_order", "rt_interpolate", "rt_bounce_rays", "rt_mesh_file_save", "rt_mesh_file_info", "rt_mesh_file_load", "rt_tree_file_save", "rt_tree_file_info",
     "rt_tree_file_load", "rt_status_string", "rt_version", "rt_abi_version", "rt_device_check", "rt_launch_count",
+)
+# every symbol include/rt_propose.h declares
+PROPOSE_EXPORTS = (
+    "rt_propose_abi_version", "rt_gemm_bf16", "rt_gemm_argmax_bf16", "rt_ray_features", "rt_softmax_xent", "rt_transpose_bf16",
+    "rt_colsum_bf16", "rt_adam_step", "rt_subtree_slots", "rt_hit_labels", "rt_trace_closest_seeded",
 )
 
 _P = C.c_void_p
@@ -93,6 +101,37 @@ class BatchTraceDesc(C.Structure):
                 ("schedule", _U32)]
 
 
+class GemmDesc(C.Structure):
+    _fields_ = [("a", _P), ("lda", _U32), ("b", _P), ("ldb", _U32), ("m", _U32), ("n", _U32), ("k", _U32), ("alpha", C.c_float),
+                ("bias", _P), ("relu", _U32), ("mask", _P), ("ldmask", _U32), ("c_f32", _P), ("ldc_f32", _U32), ("c_bf16", _P),
+                ("ldc_bf16", _U32), ("ct_bf16", _P), ("ldct", _U32), ("error_word", _P)]
+
+
+class GemmArgmaxDesc(C.Structure):
+    _fields_ = [("a", _P), ("lda", _U32), ("b", _P), ("ldb", _U32), ("m", _U32), ("n", _U32), ("k", _U32), ("bias", _P),
+                ("min_margin", C.c_float), ("out_index", _P), ("out_value", _P), ("out_margin", _P), ("error_word", _P)]
+
+
+class FeatureDesc(C.Structure):
+    _fields_ = [("orig", _P), ("dir", _P), ("count", _U32), ("box_lo", C.c_float * 3), ("box_hi", C.c_float * 3), ("out", _P),
+                ("ld_out", _U32), ("out_t", _P), ("ld_out_t", _U32)]
+
+
+class AdamDesc(C.Structure):
+    _fields_ = [("param", _P), ("grad", _P), ("m", _P), ("v", _P), ("rows", _U32), ("cols", _U32), ("lr", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float), ("step", _U32), ("out_bf16", _P), ("ld_bf16", _U32),
+                ("out_bf16_t", _P), ("ld_bf16_t", _U32)]
+
+
+class SlotDesc(C.Structure):
+    _fields_ = [("nodes", _P), ("accel", _P), ("face_count", _U32), ("depth", _U32), ("slot_ref", _P), ("slot_box", _P),
+                ("pos_label", _P), ("slot_first", _P), ("slot_count", _P)]
+
+
+class SeedDesc(C.Structure):
+    _fields_ = [("proposal", _P), ("slot_ref", _P), ("slot_box", _P), ("slot_count", _U32), ("in_proposal", _P)]
+
+
 class Camera(C.Structure):
     _fields_ = [("center", C.c_float * 3), ("angle", C.c_float * 3), ("fov", C.c_float), ("ratio", C.c_float)]
 
@@ -130,6 +169,19 @@ def lib():
             getattr(L, f"rt_{fn}_file_save").argtypes = [C.c_char_p, C.c_int, C.POINTER(st)]
             getattr(L, f"rt_{fn}_file_info").argtypes = [C.c_char_p, C.POINTER(st)]
             getattr(L, f"rt_{fn}_file_load").argtypes = [C.c_char_p, C.POINTER(st)]
+        L.rt_gemm_bf16.argtypes = [C.POINTER(GemmDesc), _P]
+        L.rt_gemm_argmax_bf16.argtypes = [C.POINTER(GemmArgmaxDesc), _P]
+        L.rt_ray_features.argtypes = [C.POINTER(FeatureDesc), _P]
+        L.rt_softmax_xent.argtypes = [_P, _U32, _U32, _P, C.c_float, _P, _P, _P]
+        L.rt_transpose_bf16.argtypes = [_P, _U32, _U32, _U32, _P, _U32, _P]
+        L.rt_colsum_bf16.argtypes = [_P, _U32, _U32, _U32, _P, _P]
+        L.rt_adam_step.argtypes = [C.POINTER(AdamDesc), _P]
+        L.rt_subtree_slots.argtypes = [C.POINTER(SlotDesc), _P]
+        L.rt_hit_labels.argtypes = [_P, _U32, _P, _P, _P]
+        L.rt_trace_closest_seeded.argtypes = [C.POINTER(TraceDesc), C.POINTER(SeedDesc), _P]
+        for name in PROPOSE_EXPORTS[1:]:
+            getattr(L, name).restype = C.c_int
+        L.rt_propose_abi_version.restype = _U32
         L.rt_status_string.restype = C.c_char_p
         L.rt_status_string.argtypes = [C.c_int]
         L.rt_version.restype = _U32
@@ -141,6 +193,8 @@ def lib():
                 getattr(L, name).restype = C.c_int
         if L.rt_abi_version() != ABI_VERSION:
             raise RuntimeError(f"{LIB_PATH} has struct layout version {L.rt_abi_version()}, these bindings expect {ABI_VERSION}: rebuild")
+        if L.rt_propose_abi_version() != PROPOSE_ABI_VERSION:
+            raise RuntimeError(f"{LIB_PATH} has proposal struct version {L.rt_propose_abi_version()}, expected {PROPOSE_ABI_VERSION}: rebuild")
         _lib = L
     return _lib
 

@@ -177,6 +177,15 @@ def trace(tree: Tree, orig: torch.Tensor, dir: torch.Tensor, tmax: torch.Tensor 
           counters: bool = False, use_tris: bool = True, vertices: torch.Tensor | None = None, out: dict | None = None,
           ray_count: int | None = None, use_accel: bool = True, schedule: dict | None = None, stream=None) -> dict:
     """Closest hit per ray. Returns dict(id=int32, t=float32, uv=float32 (R, 2), err=int32 (1,))."""
+    d, out = trace_desc(tree, orig, dir, tmax, id_mode, counters, use_tris, vertices, out, ray_count, use_accel, schedule, stream)
+    _abi.check("rt_trace_closest", _abi.lib().rt_trace_closest(C.byref(d), _stream(stream)))
+    return out
+
+
+def trace_desc(tree: Tree, orig, dir, tmax=None, id_mode: int = 0, counters: bool = False, use_tris: bool = True, vertices=None,
+               out: dict | None = None, ray_count: int | None = None, use_accel: bool = True, schedule: dict | None = None,
+               stream=None):
+    """The rt_trace_desc of a trace call and its output tensors (shared by trace and the seeded trace)."""
     _need_cuda(orig, "orig", _F32, 4)
     _need_cuda(dir, "dir", _F32, 4)
     R = orig.shape[0] if ray_count is None else ray_count
@@ -222,8 +231,7 @@ def trace(tree: Tree, orig: torch.Tensor, dir: torch.Tensor, tmax: torch.Tensor 
             order = ray_order(orig, dir, tmax, tree_box(tree), ray_count=R, stream=stream)
             out["_order"] = order  # keep it alive until the trace has run
             d.ray_order = order.data_ptr()
-    _abi.check("rt_trace_closest", _abi.lib().rt_trace_closest(C.byref(d), _stream(stream)))
-    return out
+    return d, out
 
 
 def tree_box(tree: Tree):

@@ -1,0 +1,659 @@
+// rt_mlp.cu -- tensor-core kernels of the learned subtree proposal.
+//
+// The proposal network maps a ray (origin, direction) to one of 2^depth BVH
+// subtrees: 6 inputs -> 12-frequency sin/cos encoding (144 features, padded
+// with zeros to 192) -> 3 hidden layers of 128 (ReLU) -> 4096 logits. Weights
+// are BF16 in [out][in] layout (K-major for the tensor cores), accumulation is
+// FP32 in tensor memory, biases and the optimizer state are FP32.
+//
+// Kernels:
+//   k_gemm_tc         C = alpha * A B^T (+ bias, ReLU, ReLU' mask) with FP32 /
+//                     BF16 / transposed-BF16 outputs; one 128 x BN tile per CTA;
+//                     TMA loads through a 4-stage ring, one thread issues
+//                     tcgen05.mma, the accumulator lives in TMEM.
+//   k_gemm_argmax_tc  one CTA owns 128 rows and sweeps all N columns in tiles
+//                     of 256 with two TMEM accumulators (MMA of tile t+1
+//                     overlaps the argmax epilogue of tile t); the logits never
+//                     reach HBM.
+//   k_ray_features, k_softmax_xent, k_transpose_bf16, k_colsum_bf16, k_adam.
+// The reference has no learned component; none of this replaces reference code.
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "../../include/rt_propose.h"
+#include "rt_tc.cuh"
+
+namespace rt {
+namespace {
+using namespace tc;
+
+constexpr uint32_t kBM = 128, kBK = 64, kStages = 4;
+constexpr uint32_t kTileA = kBM * kBK * 2;  // 16 KB per A stage
+
+int num_sms() {
+  int dev = 0, n = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n;
+}
+
+struct GemmEpi {
+  float alpha;
+  const float* bias;
+  uint32_t relu;
+  const __nv_bfloat16* mask;
+  uint32_t ldmask;
+  float* c32;
+  uint32_t ldc32;
+  __nv_bfloat16* c16;
+  uint32_t ldc16;
+  __nv_bfloat16* ct16;
+  uint32_t ldct;
+};
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *(const uint32_t*)&h;
+}
+
+__device__ __forceinline__ void epilogue16(const GemmEpi& E, uint32_t row, uint32_t col, float (&v)[16]) {
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    float x = v[i] * E.alpha;
+    if (E.bias) x += __ldg(E.bias + col + i);
+    if (E.relu) x = fmaxf(x, 0.0f);
+    v[i] = x;
+  }
+  if (E.mask) {
+    const uint4* mp = (const uint4*)(E.mask + (size_t)row * E.ldmask + col);
+    const uint4 m0 = __ldg(mp), m1 = __ldg(mp + 1);
+    const uint32_t w[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      // a BF16 value is > 0 when its sign bit is clear and it is not +0 (ReLU outputs hold no NaN)
+      const uint32_t lo = w[i] & 0xFFFFu, hi = w[i] >> 16;
+      if (!(lo != 0u && !(lo & 0x8000u))) v[2 * i] = 0.0f;
+      if (!(hi != 0u && !(hi & 0x8000u))) v[2 * i + 1] = 0.0f;
+    }
+  }
+  if (E.c32) {
+    float4* p = (float4*)(E.c32 + (size_t)row * E.ldc32 + col);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) p[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+  }
+  if (E.c16) {
+    uint4* p = (uint4*)(E.c16 + (size_t)row * E.ldc16 + col);
+    p[0] = make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
+    p[1] = make_uint4(pack_bf16(v[8], v[9]), pack_bf16(v[10], v[11]), pack_bf16(v[12], v[13]), pack_bf16(v[14], v[15]));
+  }
+  if (E.ct16) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) E.ct16[(size_t)(col + i) * E.ldct + row] = __float2bfloat16_rn(v[i]);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Generic GEMM: grid (n / bn, m / 128), 128 threads. Warp 0 lane 0 loads
+// (TMA), warp 1 lane 0 issues the MMAs, then all four warps drain TMEM.
+// ----------------------------------------------------------------------------
+__global__ void __launch_bounds__(128, 1)
+    k_gemm_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmEpi E, uint32_t bn,
+              uint32_t tmem_cols, uint32_t num_k, uint32_t* err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const uint32_t tile_b = bn * 128u;
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + kStages * kTileA;
+  uint64_t* full = (uint64_t*)(sB + kStages * tile_b);
+  uint64_t* empty = full + kStages;
+  uint64_t* done = empty + kStages;
+  uint32_t* tmem_slot = (uint32_t*)(done + 1);
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < kStages; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    mbar_init(done, 1);
+    fence_mbar_init();
+    prefetch_tmap(&ta);
+    prefetch_tmap(&tb);
+  }
+  __syncwarp();
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, tmem_cols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int32_t m0 = (int32_t)(blockIdx.y * kBM), n0 = (int32_t)(blockIdx.x * bn);
+
+  if (warp == 0 && lane == 0) {
+    for (uint32_t kc = 0; kc < num_k; ++kc) {
+      const uint32_t s = kc % kStages;
+      if (kc >= kStages && !mbar_wait(empty + s, ((kc / kStages) - 1u) & 1u, err)) break;
+      mbar_arrive_expect_tx(full + s, kTileA + tile_b);
+      tma_load_2d(sA + s * kTileA, &ta, (int32_t)(kc * kBK), m0, full + s);
+      tma_load_2d(sB + s * tile_b, &tb, (int32_t)(kc * kBK), n0, full + s);
+    }
+  } else if (warp == 1 && lane == 0) {
+    const uint32_t idesc = idesc_bf16_f32(kBM, bn);
+    for (uint32_t kc = 0; kc < num_k; ++kc) {
+      const uint32_t s = kc % kStages;
+      if (!mbar_wait(full + s, (kc / kStages) & 1u, err)) break;
+      tc_fence_after();
+      const uint32_t a = smem_u32(sA + s * kTileA), b = smem_u32(sB + s * tile_b);
+#pragma unroll
+      for (uint32_t kk = 0; kk < kBK / 16; ++kk)
+        mma_bf16(tmem, desc_sw128(a + kk * 32u), desc_sw128(b + kk * 32u), idesc, (kc | kk) != 0u);
+      mma_commit(empty + s);
+    }
+    mma_commit(done);  // arrives once every MMA issued above has completed
+  }
+  __syncwarp();
+
+  // warp-uniform, so that tcgen05.ld (.sync.aligned) runs on whole warps
+  const bool ok = __all_sync(0xffffffffu, mbar_wait(done, 0, err));
+  tc_fence_after();
+  if (ok) {
+    const uint32_t row = (uint32_t)m0 + warp * 32u + lane;
+    const uint32_t tl = tmem + ((warp * 32u) << 16);
+    for (uint32_t c = 0; c < bn; c += 16) {
+      float v[16];
+      tmem_ld16(tl + c, v);
+      epilogue16(E, row, (uint32_t)n0 + c, v);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, tmem_cols);
+}
+
+// ----------------------------------------------------------------------------
+// Row argmax of A B^T + bias: grid m / 128, 320 threads. Warps 0-7 drain TMEM
+// (warp w reads lanes 32 (w % 4) .. + 31 and the column half w / 4 of each
+// tile), warp 8 loads, warp 9 issues MMAs. A (128 rows x k, k <= 256) stays in
+// shared memory; B tiles of 256 rows x 64 stream through the ring;
+// accumulators alternate between TMEM columns [0, 256) and [256, 512). Each
+// thread keeps four independent (max, index, runner-up) chains (columns
+// i % 4) so that the compare chain does not serialize the epilogue.
+// ----------------------------------------------------------------------------
+constexpr uint32_t kArgBN = 256;
+constexpr uint32_t kArgTileB = kArgBN * 128u;  // 32 KB
+constexpr uint32_t kArgMaxN = 4096;
+constexpr uint32_t kArgThreads = 320;
+
+struct Top2 {
+  float best, second;
+  int32_t idx;
+};
+// Merge two partial results: the larger maximum wins (the lower index on equal
+// maxima); the runner-up is the larger of the winner's runner-up and the
+// loser's maximum.
+__device__ __forceinline__ Top2 top2_merge(Top2 a, Top2 b) {
+  const bool b_wins = b.best > a.best || (b.best == a.best && b.idx >= 0 && (a.idx < 0 || b.idx < a.idx));
+  Top2 r;
+  if (b_wins) {
+    r.best = b.best; r.idx = b.idx; r.second = fmaxf(b.second, a.best);
+  } else {
+    r.best = a.best; r.idx = a.idx; r.second = fmaxf(a.second, b.best);
+  }
+  return r;
+}
+
+__global__ void __launch_bounds__(kArgThreads, 1)
+    k_gemm_argmax_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, const float* __restrict__ bias,
+                     uint32_t n, uint32_t num_k, float min_margin, int32_t* __restrict__ out_idx, float* __restrict__ out_val,
+                     float* __restrict__ out_margin, uint32_t* err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* sA = smem;                        // num_k x 16 KB
+  uint8_t* sB = smem + num_k * kTileA;       // kStages x 32 KB
+  float* s_bias = (float*)(sB + kStages * kArgTileB);  // n floats
+  Top2* s_half = (Top2*)(s_bias + n);                  // 128 partial results of the upper column half
+  uint64_t* full = (uint64_t*)(s_half + kBM);
+  uint64_t* empty = full + kStages;
+  uint64_t* a_full = empty + kStages;
+  uint64_t* acc_full = a_full + 1;   // [2]
+  uint64_t* acc_empty = acc_full + 2;  // [2]
+  uint32_t* tmem_slot = (uint32_t*)(acc_empty + 2);
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  for (uint32_t j = threadIdx.x; j < n; j += kArgThreads) s_bias[j] = bias ? bias[j] : 0.0f;
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < kStages; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    mbar_init(a_full, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(acc_full + b, 1);
+      mbar_init(acc_empty + b, 256);
+    }
+    fence_mbar_init();
+    prefetch_tmap(&ta);
+    prefetch_tmap(&tb);
+  }
+  __syncwarp();
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int32_t m0 = (int32_t)(blockIdx.x * kBM);
+  const uint32_t ntiles = n / kArgBN;
+  Top2 res = {-INFINITY, -INFINITY, -1};
+  bool ok = true;
+
+  if (warp == 8) {
+    if (lane == 0) {
+      mbar_arrive_expect_tx(a_full, num_k * kTileA);
+      for (uint32_t kc = 0; kc < num_k; ++kc) tma_load_2d(sA + kc * kTileA, &ta, (int32_t)(kc * kBK), m0, a_full);
+      const uint32_t total = ntiles * num_k;
+      for (uint32_t g = 0; g < total; ++g) {
+        const uint32_t s = g % kStages;
+        if (g >= kStages && !mbar_wait(empty + s, ((g / kStages) - 1u) & 1u, err)) break;
+        const uint32_t t = g / num_k, kc = g % num_k;
+        mbar_arrive_expect_tx(full + s, kArgTileB);
+        tma_load_2d(sB + s * kArgTileB, &tb, (int32_t)(kc * kBK), (int32_t)(t * kArgBN), full + s);
+      }
+    }
+  } else if (warp == 9) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16_f32(kBM, kArgBN);
+      bool mok = mbar_wait(a_full, 0, err);
+      uint32_t g = 0;
+      for (uint32_t t = 0; mok && t < ntiles; ++t) {
+        const uint32_t buf = t & 1u;
+        if (t >= 2 && !mbar_wait(acc_empty + buf, ((t >> 1) - 1u) & 1u, err)) break;
+        tc_fence_after();
+        const uint32_t d = tmem + buf * kArgBN;
+        for (uint32_t kc = 0; kc < num_k; ++kc, ++g) {
+          const uint32_t s = g % kStages;
+          if (!mbar_wait(full + s, (g / kStages) & 1u, err)) { mok = false; break; }
+          tc_fence_after();
+          const uint32_t a = smem_u32(sA + kc * kTileA), b = smem_u32(sB + s * kArgTileB);
+#pragma unroll
+          for (uint32_t kk = 0; kk < kBK / 16; ++kk)
+            mma_bf16(d, desc_sw128(a + kk * 32u), desc_sw128(b + kk * 32u), idesc, (kc | kk) != 0u);
+          mma_commit(empty + s);
+        }
+        mma_commit(acc_full + buf);
+      }
+    }
+  } else {
+    // epilogue warps 0-7: lane quarter warp % 4, column half warp / 4
+    const uint32_t q = warp & 3u, half = warp >> 2;
+    float bk[4], sk[4];
+    int32_t ik[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { bk[k] = -INFINITY; sk[k] = -INFINITY; ik[k] = -1; }
+    for (uint32_t t = 0; t < ntiles; ++t) {
+      const uint32_t buf = t & 1u;
+      ok = __all_sync(0xffffffffu, ok && mbar_wait(acc_full + buf, (t >> 1) & 1u, err));
+      tc_fence_after();
+      if (ok) {
+        const uint32_t c0 = half * (kArgBN / 2);
+        const uint32_t tl = tmem + ((q * 32u) << 16) + buf * kArgBN + c0;
+        for (uint32_t c = 0; c < kArgBN / 2; c += 16) {
+          float v[16];
+          tmem_ld16(tl + c, v);
+          const uint32_t col = t * kArgBN + c0 + c;
+          const float4* bp = (const float4*)(s_bias + col);
+#pragma unroll
+          for (int i4 = 0; i4 < 4; ++i4) {
+            const float4 b4 = bp[i4];
+            const float bb[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const float x = v[4 * i4 + k] + bb[k];
+              sk[k] = fmaxf(sk[k], fminf(x, bk[k]));
+              if (x > bk[k]) { bk[k] = x; ik[k] = (int32_t)(col + 4 * i4 + k); }
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(acc_empty + buf);
+    }
+    res = Top2{bk[0], sk[0], ik[0]};
+#pragma unroll
+    for (int k = 1; k < 4; ++k) res = top2_merge(res, Top2{bk[k], sk[k], ik[k]});
+    if (half == 1) s_half[q * 32u + lane] = res;
+  }
+  __syncthreads();
+  if (warp < 4) {
+    const uint32_t r = warp * 32u + lane;
+    res = top2_merge(res, s_half[r]);
+    const uint32_t row = (uint32_t)m0 + r;
+    const float margin = res.best - res.second;
+    out_idx[row] = (ok && margin >= min_margin) ? res.idx : -1;
+    if (out_val) out_val[row] = res.best;
+    if (out_margin) out_margin[row] = margin;
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 512);
+}
+
+// ----------------------------------------------------------------------------
+// Small kernels
+// ----------------------------------------------------------------------------
+// Features of one ray: u = ((o - c) * s, d / |d|); f[24 i + 2 j] = sin(pi 2^j u_i),
+// f[24 i + 2 j + 1] = cos(pi 2^j u_i) for j < 12; columns 144..191 are zero
+// (rows hold ld >= 192 elements). Eight threads per ray: thread i < 6 encodes input i (48 bytes), threads 6
+// and 7 write the zero padding, so a warp stores 4 whole 384-byte rows.
+__global__ __launch_bounds__(256) void k_ray_features(const float4* __restrict__ orig, const float4* __restrict__ dir, uint32_t count,
+                                                      float3 c, float3 s, __nv_bfloat16* __restrict__ out, uint32_t ld,
+                                                      __nv_bfloat16* __restrict__ out_t, uint32_t ld_t) {
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t r = gid >> 3, i = gid & 7u;
+  if (r >= count) return;
+  uint32_t w[12];
+  if (i < 6) {
+    float x;
+    if (i < 3) {
+      const float4 o = __ldg(orig + r);
+      x = i == 0 ? (o.x - c.x) * s.x : (i == 1 ? (o.y - c.y) * s.y : (o.z - c.z) * s.z);
+    } else {
+      const float4 d = __ldg(dir + r);
+      const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+      const float inv = len > 0.0f ? 1.0f / len : 0.0f;
+      x = (i == 3 ? d.x : (i == 4 ? d.y : d.z)) * inv;
+    }
+#pragma unroll
+    for (int j = 0; j < 12; ++j) {
+      float sv, cv;
+      sincospif(x, &sv, &cv);
+      w[j] = pack_bf16(sv, cv);
+      x *= 2.0f;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 12; ++j) w[j] = 0u;
+  }
+  if (out) {
+    uint4* p = (uint4*)(out + (size_t)r * ld + 24u * i);
+    p[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    p[1] = make_uint4(w[4], w[5], w[6], w[7]);
+    p[2] = make_uint4(w[8], w[9], w[10], w[11]);
+  }
+  if (out_t) {
+#pragma unroll
+    for (int j = 0; j < 12; ++j) {
+      const uint32_t f = 24u * i + 2u * j;
+      out_t[(size_t)f * ld_t + r] = __ushort_as_bfloat16((unsigned short)(w[j] & 0xFFFFu));
+      out_t[(size_t)(f + 1) * ld_t + r] = __ushort_as_bfloat16((unsigned short)(w[j] >> 16));
+    }
+  }
+}
+
+// One warp per row: grad = (softmax(logits) - onehot(label)) * scale (BF16),
+// loss_sum += logsumexp - logit[label]. Rows with label < 0 get zero gradient.
+__global__ __launch_bounds__(256) void k_softmax_xent(const float* __restrict__ logits, uint32_t rows, uint32_t cols,
+                                                      const int32_t* __restrict__ labels, float scale,
+                                                      __nv_bfloat16* __restrict__ grad, float* __restrict__ loss_sum) {
+  const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t lane = threadIdx.x & 31u;
+  if (row >= rows) return;
+  const float* x = logits + (size_t)row * cols;
+  __nv_bfloat16* g = grad + (size_t)row * cols;
+  const int32_t lab = labels[row];
+  if (lab < 0 || lab >= (int32_t)cols) {
+    for (uint32_t j = lane * 2; j < cols; j += 64) *(uint32_t*)(g + j) = 0u;
+    return;
+  }
+  float mx = -INFINITY;
+  for (uint32_t j = lane * 4; j < cols; j += 128) {
+    const float4 v = *(const float4*)(x + j);
+    mx = fmaxf(mx, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+  }
+  for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  float sum = 0.0f;
+  for (uint32_t j = lane * 4; j < cols; j += 128) {
+    const float4 v = *(const float4*)(x + j);
+    sum += __expf(v.x - mx) + __expf(v.y - mx) + __expf(v.z - mx) + __expf(v.w - mx);
+  }
+  for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  const float inv = 1.0f / sum;
+  for (uint32_t j = lane * 4; j < cols; j += 128) {
+    const float4 v = *(const float4*)(x + j);
+    float p0 = __expf(v.x - mx) * inv, p1 = __expf(v.y - mx) * inv, p2 = __expf(v.z - mx) * inv, p3 = __expf(v.w - mx) * inv;
+    if ((int32_t)j == lab) p0 -= 1.0f;
+    if ((int32_t)j + 1 == lab) p1 -= 1.0f;
+    if ((int32_t)j + 2 == lab) p2 -= 1.0f;
+    if ((int32_t)j + 3 == lab) p3 -= 1.0f;
+    *(uint2*)(g + j) = make_uint2(pack_bf16(p0 * scale, p1 * scale), pack_bf16(p2 * scale, p3 * scale));
+  }
+  if (lane == 0 && loss_sum) atomicAdd(loss_sum, (logf(sum) + mx - x[lab]) * scale);
+}
+
+// out[c][r] = in[r][c], 32 x 32 tiles through shared memory.
+__global__ __launch_bounds__(256) void k_transpose_bf16(const __nv_bfloat16* __restrict__ in, uint32_t rows, uint32_t cols, uint32_t ld_in,
+                                                        __nv_bfloat16* __restrict__ out, uint32_t ld_out) {
+  __shared__ __nv_bfloat16 tile[32][33];
+  const uint32_t c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (uint32_t y = threadIdx.y; y < 32; y += blockDim.y) {
+    const uint32_t r = r0 + y, c = c0 + threadIdx.x;
+    if (r < rows && c < cols) tile[y][threadIdx.x] = in[(size_t)r * ld_in + c];
+  }
+  __syncthreads();
+  for (uint32_t y = threadIdx.y; y < 32; y += blockDim.y) {
+    const uint32_t c = c0 + y, r = r0 + threadIdx.x;
+    if (r < rows && c < cols) out[(size_t)c * ld_out + r] = tile[threadIdx.x][y];
+  }
+}
+
+// out[c] += sum over a chunk of rows of in[r][c] (FP32 accumulation).
+__global__ __launch_bounds__(256) void k_colsum_bf16(const __nv_bfloat16* __restrict__ in, uint32_t rows, uint32_t cols, uint32_t ld,
+                                                     uint32_t rows_per_block, float* __restrict__ out) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  const uint32_t r0 = blockIdx.y * rows_per_block;
+  const uint32_t r1 = min(rows, r0 + rows_per_block);
+  float s = 0.0f;
+  for (uint32_t r = r0; r < r1; ++r) s += __bfloat162float(in[(size_t)r * ld + c]);
+  atomicAdd(out + c, s);
+}
+
+// Adam (bias-corrected) on FP32 parameters [rows][cols]; refreshes the BF16
+// copies [rows][ld16] and transposed [cols][ld16t] when given.
+__global__ __launch_bounds__(256) void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                                              float* __restrict__ v, uint32_t rows, uint32_t cols, float lr, float b1, float b2,
+                                              float eps, float c1, float c2, __nv_bfloat16* __restrict__ out16, uint32_t ld16,
+                                              __nv_bfloat16* __restrict__ out16t, uint32_t ld16t) {
+  const size_t total = (size_t)rows * cols;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float pi = p[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+    p[i] = pi;
+    const uint32_t r = (uint32_t)(i / cols), c = (uint32_t)(i % cols);
+    if (out16) out16[(size_t)r * ld16 + c] = __float2bfloat16_rn(pi);
+    if (out16t) out16t[(size_t)c * ld16t + r] = __float2bfloat16_rn(pi);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Host side
+// ----------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// BF16 matrix [rows][ld] (K-major, k valid columns) as boxes of 64 x box_rows
+// with the 128-byte swizzle.
+bool make_map(CUtensorMap* map, const void* base, uint32_t k, uint32_t rows, uint32_t ld, uint32_t box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {k, rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 2u};
+  cuuint32_t box[2] = {kBK, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+uint32_t pick_bn(uint32_t n) {
+  for (uint32_t bn = 256; bn >= 16; bn -= 16)
+    if (n % bn == 0) return bn;
+  return 0;
+}
+
+uint32_t pow2_cols(uint32_t n) {
+  uint32_t c = 32;
+  while (c < n) c <<= 1;
+  return c;
+}
+
+size_t gemm_smem(uint32_t bn) { return 1024 + kStages * (kTileA + (size_t)bn * 128u) + 256; }
+size_t argmax_smem(uint32_t num_k, uint32_t n) {
+  return 1024 + num_k * (size_t)kTileA + kStages * (size_t)kArgTileB + (size_t)n * 4 + kBM * sizeof(Top2) + 256;
+}
+
+}  // namespace
+}  // namespace rt
+
+using namespace rt;
+
+extern "C" uint32_t rt_propose_abi_version(void) { return RT_PROPOSE_ABI_VERSION; }
+
+extern "C" rt_status rt_gemm_bf16(const rt_gemm_desc* d, rt_stream stream) {
+  if (!d || !d->a || !d->b) return RT_ERR_INVALID_ARGUMENT;
+  if (d->m == 0 || d->n == 0 || d->k == 0) return RT_ERR_INVALID_ARGUMENT;
+  if (d->m % kBM || d->k % kBK || d->n % 16) return RT_ERR_INVALID_ARGUMENT;
+  if (d->lda < d->k || d->ldb < d->k || d->lda % 8 || d->ldb % 8) return RT_ERR_INVALID_ARGUMENT;
+  if (!aligned16(d->a) || !aligned16(d->b)) return RT_ERR_INVALID_ARGUMENT;
+  if (d->c_f32 && (d->ldc_f32 < d->n || d->ldc_f32 % 4 || !aligned16(d->c_f32))) return RT_ERR_INVALID_ARGUMENT;
+  if (d->c_bf16 && (d->ldc_bf16 < d->n || d->ldc_bf16 % 8 || !aligned16(d->c_bf16))) return RT_ERR_INVALID_ARGUMENT;
+  if (d->mask && (d->ldmask < d->n || d->ldmask % 8 || !aligned16(d->mask))) return RT_ERR_INVALID_ARGUMENT;
+  if (d->ct_bf16 && d->ldct < d->m) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  const uint32_t bn = pick_bn(d->n);
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, d->a, d->k, d->m, d->lda, kBM) || !make_map(&tb, d->b, d->k, d->n, d->ldb, bn)) return RT_ERR_UNSUPPORTED;
+  GemmEpi E;
+  E.alpha = d->alpha; E.bias = d->bias; E.relu = d->relu; E.mask = (const __nv_bfloat16*)d->mask; E.ldmask = d->ldmask;
+  E.c32 = d->c_f32; E.ldc32 = d->ldc_f32; E.c16 = (__nv_bfloat16*)d->c_bf16; E.ldc16 = d->ldc_bf16;
+  E.ct16 = (__nv_bfloat16*)d->ct_bf16; E.ldct = d->ldct;
+  const size_t smem = gemm_smem(bn);
+  static std::once_flag once;
+  std::call_once(once, [] { cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem(256)); });
+  dim3 grid(d->n / bn, d->m / kBM);
+  k_gemm_tc<<<grid, 128, smem, (cudaStream_t)stream>>>(ta, tb, E, bn, pow2_cols(bn), d->k / kBK, d->error_word);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_gemm_argmax_bf16(const rt_gemm_argmax_desc* d, rt_stream stream) {
+  if (!d || !d->a || !d->b || !d->out_index) return RT_ERR_INVALID_ARGUMENT;
+  if (d->m == 0 || d->m % kBM || d->n == 0 || d->n % kArgBN || d->n > kArgMaxN || d->k == 0 || d->k % kBK || d->k > 256)
+    return RT_ERR_INVALID_ARGUMENT;
+  if (d->lda < d->k || d->ldb < d->k || d->lda % 8 || d->ldb % 8 || !aligned16(d->a) || !aligned16(d->b))
+    return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, d->a, d->k, d->m, d->lda, kBM) || !make_map(&tb, d->b, d->k, d->n, d->ldb, kArgBN)) return RT_ERR_UNSUPPORTED;
+  const uint32_t num_k = d->k / kBK;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaFuncSetAttribute(k_gemm_argmax_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)argmax_smem(4, kArgMaxN));
+  });
+  k_gemm_argmax_tc<<<d->m / kBM, kArgThreads, argmax_smem(num_k, d->n), (cudaStream_t)stream>>>(ta, tb, d->bias, d->n, num_k, d->min_margin,
+                                                                                  d->out_index, d->out_value, d->out_margin, d->error_word);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_ray_features(const rt_feature_desc* d, rt_stream stream) {
+  if (!d || !d->orig || !d->dir || (!d->out && !d->out_t)) return RT_ERR_INVALID_ARGUMENT;
+  if (d->out && (d->ld_out < 192 || d->ld_out % 8 || !aligned16(d->out))) return RT_ERR_INVALID_ARGUMENT;
+  if (d->out_t && d->ld_out_t < d->count) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  if (d->count == 0) return RT_OK;
+  const float3 c = make_float3(0.5f * (d->box_lo[0] + d->box_hi[0]), 0.5f * (d->box_lo[1] + d->box_hi[1]), 0.5f * (d->box_lo[2] + d->box_hi[2]));
+  const float3 s = make_float3(2.0f / (d->box_hi[0] - d->box_lo[0]), 2.0f / (d->box_hi[1] - d->box_lo[1]), 2.0f / (d->box_hi[2] - d->box_lo[2]));
+  k_ray_features<<<(uint32_t)(((size_t)d->count * 8 + 255) / 256), 256, 0, (cudaStream_t)stream>>>((const float4*)d->orig, (const float4*)d->dir, d->count, c, s,
+                                                                           (__nv_bfloat16*)d->out, d->ld_out, (__nv_bfloat16*)d->out_t,
+                                                                           d->ld_out_t);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_softmax_xent(const float* logits, uint32_t rows, uint32_t cols, const int32_t* labels, float scale, void* grad_bf16,
+                                     float* loss_sum, rt_stream stream) {
+  if (!logits || !labels || !grad_bf16 || cols == 0 || cols % 128) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  if (rows == 0) return RT_OK;
+  k_softmax_xent<<<(rows + 7) / 8, 256, 0, (cudaStream_t)stream>>>(logits, rows, cols, labels, scale, (__nv_bfloat16*)grad_bf16, loss_sum);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_transpose_bf16(const void* in, uint32_t rows, uint32_t cols, uint32_t ld_in, void* out, uint32_t ld_out,
+                                       rt_stream stream) {
+  if (!in || !out || ld_in < cols || ld_out < rows) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  if (rows == 0 || cols == 0) return RT_OK;
+  dim3 grid((cols + 31) / 32, (rows + 31) / 32);
+  k_transpose_bf16<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)in, rows, cols, ld_in, (__nv_bfloat16*)out, ld_out);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_colsum_bf16(const void* in, uint32_t rows, uint32_t cols, uint32_t ld, float* out, rt_stream stream) {
+  if (!in || !out || ld < cols) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemsetAsync(out, 0, (size_t)cols * 4, st) != cudaSuccess) return RT_ERR_CUDA;
+  if (rows == 0 || cols == 0) return RT_OK;
+  const uint32_t rpb = 256;
+  dim3 grid((cols + 255) / 256, (rows + rpb - 1) / rpb);
+  k_colsum_bf16<<<grid, 256, 0, st>>>((const __nv_bfloat16*)in, rows, cols, ld, rpb, out);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_adam_step(const rt_adam_desc* d, rt_stream stream) {
+  if (!d || !d->param || !d->grad || !d->m || !d->v || d->step == 0) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  const size_t total = (size_t)d->rows * d->cols;
+  if (total == 0) return RT_OK;
+  const float c1 = 1.0f / (1.0f - powf(d->beta1, (float)d->step));
+  const float c2 = 1.0f / (1.0f - powf(d->beta2, (float)d->step));
+  const uint32_t blocks = (uint32_t)hmin<size_t>((total + 255) / 256, (size_t)num_sms() * 8);
+  k_adam<<<blocks, 256, 0, (cudaStream_t)stream>>>(d->param, d->grad, d->m, d->v, d->rows, d->cols, d->lr, d->beta1, d->beta2, d->eps, c1,
+                                                    c2, (__nv_bfloat16*)d->out_bf16, d->ld_bf16, (__nv_bfloat16*)d->out_bf16_t,
+                                                    d->ld_bf16_t);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}

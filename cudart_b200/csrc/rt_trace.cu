@@ -14,6 +14,7 @@
 // position-ordered {v0, e1, e2} stream (48 bytes, three 128-bit loads), so a
 // leaf's triangles are contiguous.
 #include "rt_device.cuh"
+#include "../../include/rt_propose.h"
 
 namespace rt {
 namespace {
@@ -132,21 +133,84 @@ struct AccelArgs {
 // One ray through the blob. kWW: "while-while" schedule (descend internal
 // nodes until the ray holds a leaf, then test the leaf), which keeps the lanes
 // of a warp in the same phase more often than the "if-if" schedule.
-template <bool kCount, bool kWW>
-__device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArgs& A, const AccelArgs& C) {
+// Proposal seeding (rt_trace_closest_seeded): the ray first walks the subtree
+// `slot_ref[proposal[r]]` (phase 0), then the whole tree with that subtree cut
+// out (phase 1), keeping the best hit of phase 0 as its starting best. Phase 0
+// finds the exact minimum (t, position) of the subtree, so skipping it in
+// phase 1 loses nothing and the final hit is the same as a plain walk's.
+struct SeedArgs {
+  const int32_t* proposal;
+  const int32_t* slot_ref;
+  const float4* slot_box;
+  uint32_t slot_count;
+  int32_t* in_prop;
+};
+constexpr uint32_t kNoSkip = 0x7FFFFFFFu;  // never a record index or a leaf reference
+
+// A slot reference is walked only when it names a record or leaf of this blob
+// (hdr[1] = leaf count; a tree of L leaves has L - 1 two-child records).
+__device__ __forceinline__ bool seed_ref_ok(uint32_t q, const AccelArgs& C) {
+  const uint32_t leaves = __ldg(C.hdr + 1);
+  return (q & 0x80000000u) ? (~q < leaves) : (q + 1u < leaves);
+}
+
+// Where a seeded walk starts. With a valid proposal: the proposed subtree
+// (phase 0) and that subtree cut out of phase 1. When the ray misses the slot's
+// padded box (the same conservative test as every node box), nothing in the
+// subtree can be hit, so phase 0 is skipped and the subtree is still cut out.
+// Returns false when nothing is left to walk.
+template <bool kCount>
+__device__ __forceinline__ bool seed_start(uint32_t r, const SeedArgs& S, const AccelArgs& C, const float4& o, float ix, float iy,
+                                           float iz, float bt, uint32_t root, uint32_t& ref, uint32_t& skip, uint32_t& phase,
+                                           uint32_t& visits) {
+  const int32_t p = __ldg(S.proposal + r);
+  if (p < 0 || (uint32_t)p >= S.slot_count) return true;
+  const uint32_t q = (uint32_t)__ldg(S.slot_ref + p);
+  if (!seed_ref_ok(q, C)) return true;
+  skip = q;
+  if (S.slot_box) {
+    if (kCount) ++visits;
+    float tb;
+    if (!slab2(ldg4(S.slot_box + 2 * p), ldg4(S.slot_box + 2 * p + 1), o, ix, iy, iz, bt, tb)) return root != skip;
+  }
+  ref = q;
+  phase = 0;
+  return true;
+}
+
+template <bool kCount, bool kWW, bool kSeed = false>
+__device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArgs& A, const AccelArgs& C,
+                                                const SeedArgs& S = SeedArgs{}) {
   const float4 o = ldg4(A.orig + r), d = ldg4(A.dir + r);
   const float tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
   int32_t best = -1;
   float bt = tmax0, bu = 0.0f, bv = 0.0f;
   uint32_t visits = 0, tests = 0;
+  uint32_t phase = 1, best_phase = 1;
   if (tmax0 > 0.0f) {
     const float ix = 1.0f / fix_dir(d.x), iy = 1.0f / fix_dir(d.y), iz = 1.0f / fix_dir(d.z);
     const float zu = o.w * 0.0f, zv = d.w * 0.0f;
     uint32_t st_ref[kStack];
     float st_t[kStack];
     int sp = 0;
-    uint32_t ref = __ldg(C.hdr);
+    const uint32_t root = __ldg(C.hdr);
+    uint32_t ref = root, skip = kNoSkip;
     bool alive = true;
+    if (kSeed) alive = seed_start<kCount>(r, S, C, o, ix, iy, iz, bt, root, ref, skip, phase, visits);
+    // next reference to walk: the nearest stacked subtree still within reach,
+    // else (phase 0) the root of phase 1; false when the walk is over
+    auto next = [&]() -> bool {
+      while (sp > 0) {
+        --sp;
+        if (st_t[sp] <= bt * kCullSlack) { ref = st_ref[sp]; return true; }
+      }
+      if (kSeed && phase == 0) {
+        phase = 1;
+        ref = root;
+        return root != skip;
+      }
+      return false;
+    };
     while (alive) {
       // descend internal nodes (kWW: until this ray holds a leaf)
       while (!(ref & 0x80000000u)) {
@@ -154,9 +218,13 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
         const float4 a0 = ldg4(tn), a1 = ldg4(tn + 1), b0 = ldg4(tn + 2), b1 = ldg4(tn + 3);
         if (kCount) visits += 2;
         float ta, tb;
-        const bool ha = slab2(a0, a1, o, ix, iy, iz, bt, ta);
-        const bool hb = slab2(b0, b1, o, ix, iy, iz, bt, tb);
+        bool ha = slab2(a0, a1, o, ix, iy, iz, bt, ta);
+        bool hb = slab2(b0, b1, o, ix, iy, iz, bt, tb);
         const uint32_t ra = __float_as_uint(a0.w), rb = __float_as_uint(b0.w);
+        if (kSeed && phase) {
+          if (ra == skip) ha = false;
+          if (rb == skip) hb = false;
+        }
         if (ha && hb) {
           const bool a_first = ta <= tb;
           if (sp < kStack) {
@@ -171,13 +239,9 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
           ref = ra;
         } else if (hb) {
           ref = rb;
-        } else {
-          bool found = false;
-          while (sp > 0) {
-            --sp;
-            if (st_t[sp] <= bt * kCullSlack) { ref = st_ref[sp]; found = true; break; }
-          }
-          if (!found) { alive = false; break; }
+        } else if (!next()) {
+          alive = false;
+          break;
         }
         if (!kWW && (ref & 0x80000000u)) break;
       }
@@ -203,16 +267,12 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
           if (!mt_test(o, d, zu, zv, v0, e1, e2, t, u, v)) continue;
           if (t < bt || (best >= 0 && t == bt && (int32_t)pos < best)) {
             best = (int32_t)pos; bt = t; bu = u; bv = v;
+            best_phase = phase;
           }
         }
       }
       // next subtree whose entry is still within reach
-      bool found = false;
-      while (sp > 0) {
-        --sp;
-        if (st_t[sp] <= bt * kCullSlack) { ref = st_ref[sp]; found = true; break; }
-      }
-      if (!found) break;
+      if (!next()) break;
     }
   }
   if (best >= 0) {
@@ -224,6 +284,7 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
     A.hit_t[r] = tmax0;
     A.hit_uv[r] = make_float2(0.0f, 0.0f);
   }
+  if (kSeed && S.in_prop) S.in_prop[r] = (best >= 0 && best_phase == 0) ? 1 : 0;
   if (kCount) {
     if (A.visits) A.visits[r] = visits;
     if (A.tests) A.tests[r] = tests;
@@ -240,9 +301,9 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
 // are written by the lane whose key is the minimum right after its merge.
 constexpr int kCoopWarps = 4;  // 128-thread CTAs
 
-template <bool kCount>
+template <bool kCount, bool kSeed = false>
 __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool valid, const TraceArgs& A, const AccelArgs& C,
-                                                unsigned long long* s_key, float2* s_uv) {
+                                                unsigned long long* s_key, float2* s_uv, const SeedArgs& S = SeedArgs{}) {
   const uint32_t lane = lane_id();
   float4 o = make_float4(0.f, 0.f, 0.f, 0.f), d = make_float4(0.f, 0.f, 1.f, 0.f);
   float tmax0 = -1.0f;
@@ -259,8 +320,24 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
   uint32_t st_ref[kStack];
   float st_t[kStack];
   int sp = 0;
-  uint32_t ref = __ldg(C.hdr);
-  bool alive = valid && tmax0 > 0.0f;
+  const uint32_t root = __ldg(C.hdr);
+  uint32_t ref = root, skip = kNoSkip;
+  uint32_t phase = 1, best_phase = 1;
+  bool go = true;
+  if (kSeed && valid && tmax0 > 0.0f) go = seed_start<kCount>(r, S, C, o, ix, iy, iz, bt, root, ref, skip, phase, visits);
+  auto next = [&]() -> bool {
+    while (sp > 0) {
+      --sp;
+      if (st_t[sp] <= bt * kCullSlack) { ref = st_ref[sp]; return true; }
+    }
+    if (kSeed && phase == 0) {
+      phase = 1;
+      ref = root;
+      return root != skip;
+    }
+    return false;
+  };
+  bool alive = valid && tmax0 > 0.0f && go;
   while (__any_sync(0xffffffffu, alive)) {
     // 1. descend until this ray holds a leaf
     bool has_leaf = false;
@@ -270,9 +347,13 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
         const float4 a0 = ldg4(tn), a1 = ldg4(tn + 1), b0 = ldg4(tn + 2), b1 = ldg4(tn + 3);
         if (kCount) visits += 2;
         float ta, tb;
-        const bool ha = slab2(a0, a1, o, ix, iy, iz, bt, ta);
-        const bool hb = slab2(b0, b1, o, ix, iy, iz, bt, tb);
+        bool ha = slab2(a0, a1, o, ix, iy, iz, bt, ta);
+        bool hb = slab2(b0, b1, o, ix, iy, iz, bt, tb);
         const uint32_t ra = __float_as_uint(a0.w), rb = __float_as_uint(b0.w);
+        if (kSeed && phase) {
+          if (ra == skip) ha = false;
+          if (rb == skip) hb = false;
+        }
         if (ha && hb) {
           const bool a_first = ta <= tb;
           if (sp < kStack) {
@@ -287,13 +368,9 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
           ref = ra;
         } else if (hb) {
           ref = rb;
-        } else {
-          bool found = false;
-          while (sp > 0) {
-            --sp;
-            if (st_t[sp] <= bt * kCullSlack) { ref = st_ref[sp]; found = true; break; }
-          }
-          if (!found) { alive = false; break; }
+        } else if (!next()) {
+          alive = false;
+          break;
         }
       }
       has_leaf = alive;
@@ -390,6 +467,7 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
         best = (int32_t)(k & 0xFFFFFFFFu);
         const float2 uv = s_uv[lane];
         bu = uv.x; bv = uv.y;
+        best_phase = phase;
       }
       // groups beyond the first 32 (leaves of more than 256 triangles): this lane alone
       for (uint32_t g = 32; g * 8 < cnt; ++g) {
@@ -407,19 +485,18 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
           if (kCount) ++tests;
           float t, u, v;
           if (!mt_test(o, d, zu, zv, v0, e1, e2, t, u, v)) continue;
-          if (t < bt || (best >= 0 && t == bt && (int32_t)pos < best)) { best = (int32_t)pos; bt = t; bu = u; bv = v; }
+          if (t < bt || (best >= 0 && t == bt && (int32_t)pos < best)) {
+            best = (int32_t)pos; bt = t; bu = u; bv = v;
+            best_phase = phase;
+          }
         }
       }
-      bool found = false;
-      while (sp > 0) {
-        --sp;
-        if (st_t[sp] <= bt * kCullSlack) { ref = st_ref[sp]; found = true; break; }
-      }
-      if (!found) alive = false;
+      if (!next()) alive = false;
     }
     __syncwarp();
   }
   if (!valid) return;
+  if (kSeed && S.in_prop) S.in_prop[r] = (best >= 0 && best_phase == 0) ? 1 : 0;
   if (best >= 0) {
     A.hit_id[r] = A.id_mode == 1 ? (int32_t)__ldg(A.indices + best) : best;
     A.hit_t[r] = bt;
@@ -450,26 +527,26 @@ struct SlotMap {
   }
 };
 
-template <bool kCount, bool kWW>
-__global__ __launch_bounds__(128) void k_trace_accel(TraceArgs A, AccelArgs C, SlotMap M) {
+template <bool kCount, bool kWW, bool kSeed>
+__global__ __launch_bounds__(128) void k_trace_accel(TraceArgs A, AccelArgs C, SlotMap M, SeedArgs S) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t r;
-  if (s < M.slots && M.ray_of(s, r)) trace_ray_accel<kCount, kWW>(r, A, C);
+  if (s < M.slots && M.ray_of(s, r)) trace_ray_accel<kCount, kWW, kSeed>(r, A, C, S);
 }
 
-template <bool kCount>
-__global__ __launch_bounds__(128) void k_trace_coop(TraceArgs A, AccelArgs C, SlotMap M) {
+template <bool kCount, bool kSeed>
+__global__ __launch_bounds__(128) void k_trace_coop(TraceArgs A, AccelArgs C, SlotMap M, SeedArgs S) {
   __shared__ unsigned long long s_key[kCoopWarps][32];
   __shared__ float2 s_uv[kCoopWarps][32];
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t r = 0;
   const bool valid = s < M.slots && M.ray_of(s, r);
   const uint32_t w = threadIdx.x >> 5;
-  trace_warp_coop<kCount>(r, valid, A, C, s_key[w], s_uv[w]);
+  trace_warp_coop<kCount, kSeed>(r, valid, A, C, s_key[w], s_uv[w], S);
 }
 
-template <bool kCount>
-__global__ __launch_bounds__(128) void k_trace_coop_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter) {
+template <bool kCount, bool kSeed>
+__global__ __launch_bounds__(128) void k_trace_coop_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter, SeedArgs S) {
   __shared__ unsigned long long s_key[kCoopWarps][32];
   __shared__ float2 s_uv[kCoopWarps][32];
   const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
@@ -481,14 +558,14 @@ __global__ __launch_bounds__(128) void k_trace_coop_persistent(TraceArgs A, Acce
     uint32_t r = 0;
     const uint32_t s = base + lane;
     const bool valid = s < M.slots && M.ray_of(s, r);
-    trace_warp_coop<kCount>(r, valid, A, C, s_key[w], s_uv[w]);
+    trace_warp_coop<kCount, kSeed>(r, valid, A, C, s_key[w], s_uv[w], S);
   }
 }
 
 // Persistent warps: each warp takes 32 slots at a time from a global counter
 // until the slots run out (the counter is zeroed before the launch).
-template <bool kCount, bool kWW>
-__global__ __launch_bounds__(128) void k_trace_accel_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter) {
+template <bool kCount, bool kWW, bool kSeed>
+__global__ __launch_bounds__(128) void k_trace_accel_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter, SeedArgs S) {
   const uint32_t lane = lane_id();
   for (;;) {
     uint32_t base = 0;
@@ -497,7 +574,7 @@ __global__ __launch_bounds__(128) void k_trace_accel_persistent(TraceArgs A, Acc
     if (base >= M.slots) break;
     uint32_t r;
     const uint32_t s = base + lane;
-    if (s < M.slots && M.ray_of(s, r)) trace_ray_accel<kCount, kWW>(r, A, C);
+    if (s < M.slots && M.ray_of(s, r)) trace_ray_accel<kCount, kWW, kSeed>(r, A, C, S);
   }
 }
 
@@ -648,72 +725,86 @@ extern "C" rt_status rt_device_check(void) {
   return state ? RT_OK : RT_ERR_NO_DEVICE;
 }
 
-extern "C" rt_status rt_trace_closest(const rt_trace_desc* d, rt_stream stream) {
+namespace {
+
+// Blob traversal launch for every schedule of rt_trace_desc.
+template <bool kSeed>
+rt_status launch_accel(const rt_trace_desc* d, const TraceArgs& A, const SeedArgs& S, cudaStream_t st) {
+  const bool count = d->ray_visits || d->ray_tests;
+  // blob layout of rt_lbvh_build: header (256 B), records, leaf table, group boxes
+  const size_t n = d->face_count_hint;
+  AccelArgs C;
+  Carve c((void*)d->accel, ~(size_t)0);
+  C.hdr = c.take<uint32_t>(64);
+  C.tnodes = c.take<float4>(4 * n);
+  C.leaves = c.take<uint4>(n);
+  C.groups = c.take<float4>(2 * (n / 8 + n + 1));
+  SlotMap M;
+  M.order = d->ray_order;
+  const uint32_t R = d->ray_count;
+  if (d->ray_order) {
+    M.width = 0; M.height = 0; M.tiles_x = 0; M.slots = R;
+  } else if (d->image_width && R % d->image_width == 0) {
+    M.width = d->image_width;
+    M.height = R / d->image_width;
+    M.tiles_x = (M.width + 7) / 8;
+    M.slots = M.tiles_x * ((M.height + 3) / 4) * 32;
+  } else {
+    M.width = 0; M.height = 0; M.tiles_x = 0; M.slots = R;
+  }
+  const bool ww = (d->schedule & RT_TRACE_WHILE_WHILE) != 0;
+  const uint32_t pblocks = (uint32_t)sms() * (d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u);
+  const uint32_t sblocks = (M.slots + 127) / 128;
+  if (d->work_counter && cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
+  if (d->schedule & RT_TRACE_COOP) {
+    if (d->work_counter) {
+      if (count) k_trace_coop_persistent<true, kSeed><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter, S);
+      else k_trace_coop_persistent<false, kSeed><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter, S);
+    } else {
+      if (count) k_trace_coop<true, kSeed><<<sblocks, 128, 0, st>>>(A, C, M, S);
+      else k_trace_coop<false, kSeed><<<sblocks, 128, 0, st>>>(A, C, M, S);
+    }
+  } else if (d->work_counter) {
+#define RT_LAUNCH_P(CNT, WW) k_trace_accel_persistent<CNT, WW, kSeed><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter, S)
+    if (count) { if (ww) RT_LAUNCH_P(true, true); else RT_LAUNCH_P(true, false); }
+    else { if (ww) RT_LAUNCH_P(false, true); else RT_LAUNCH_P(false, false); }
+#undef RT_LAUNCH_P
+  } else {
+#define RT_LAUNCH_S(CNT, WW) k_trace_accel<CNT, WW, kSeed><<<sblocks, 128, 0, st>>>(A, C, M, S)
+    if (count) { if (ww) RT_LAUNCH_S(true, true); else RT_LAUNCH_S(true, false); }
+    else { if (ww) RT_LAUNCH_S(false, true); else RT_LAUNCH_S(false, false); }
+#undef RT_LAUNCH_S
+  }
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+rt_status trace_args(const rt_trace_desc* d, TraceArgs& A) {
   if (!d || !d->nodes || !d->orig || !d->dir || !d->hit_id || !d->hit_t || !d->hit_uv) return RT_ERR_INVALID_ARGUMENT;
   if (!d->tris && (!d->vertices || !d->faces)) return RT_ERR_INVALID_ARGUMENT;
   if (d->id_mode == 1 && !d->indices) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
-  if (d->ray_count == 0) return RT_OK;
-  TraceArgs A;
   A.nodes = (const uint4*)d->nodes; A.tris = (const float4*)d->tris; A.verts = (const float4*)d->vertices;
   A.faces = (const uint4*)d->faces; A.indices = d->indices; A.orig = (const float4*)d->orig; A.dir = (const float4*)d->dir;
   A.tmax = d->tmax; A.ray_count = d->ray_count; A.id_mode = d->id_mode; A.hit_id = d->hit_id; A.hit_t = d->hit_t;
   A.hit_uv = (float2*)d->hit_uv; A.visits = d->ray_visits; A.tests = d->ray_tests; A.err = d->error_word;
+  return RT_OK;
+}
+
+}  // namespace
+
+extern "C" rt_status rt_trace_closest(const rt_trace_desc* d, rt_stream stream) {
+  TraceArgs A;
+  const rt_status s = trace_args(d, A);
+  if (s != RT_OK) return s;
+  if (d->ray_count == 0) return RT_OK;
   const bool count = d->ray_visits || d->ray_tests;
   const uint32_t blocks = (d->ray_count + 127) / 128;
   cudaStream_t st = (cudaStream_t)stream;
   if (d->accel) {
     if (!d->tris) return RT_ERR_INVALID_ARGUMENT;
-    // blob layout of rt_lbvh_build: header (256 B), records, leaf table, group boxes
-    const size_t n = d->face_count_hint;
-    AccelArgs C;
-    Carve c((void*)d->accel, ~(size_t)0);
-    C.hdr = c.take<uint32_t>(64);
-    C.tnodes = c.take<float4>(4 * n);
-    C.leaves = c.take<uint4>(n);
-    C.groups = c.take<float4>(2 * (n / 8 + n + 1));
-    SlotMap M;
-    M.order = d->ray_order;
-    const uint32_t R = d->ray_count;
-    if (d->ray_order) {
-      M.width = 0; M.height = 0; M.tiles_x = 0; M.slots = R;
-    } else if (d->image_width && R % d->image_width == 0) {
-      M.width = d->image_width;
-      M.height = R / d->image_width;
-      M.tiles_x = (M.width + 7) / 8;
-      M.slots = M.tiles_x * ((M.height + 3) / 4) * 32;
-    } else {
-      M.width = 0; M.height = 0; M.tiles_x = 0; M.slots = R;
-    }
-    const bool ww = (d->schedule & RT_TRACE_WHILE_WHILE) != 0;
-    if (d->schedule & RT_TRACE_COOP) {
-      if (d->work_counter) {
-        if (cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
-        const uint32_t pblocks = (uint32_t)sms() * (d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u);
-        if (count) k_trace_coop_persistent<true><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter);
-        else k_trace_coop_persistent<false><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter);
-      } else {
-        const uint32_t sblocks = (M.slots + 127) / 128;
-        if (count) k_trace_coop<true><<<sblocks, 128, 0, st>>>(A, C, M);
-        else k_trace_coop<false><<<sblocks, 128, 0, st>>>(A, C, M);
-      }
-    } else if (d->work_counter) {
-      if (cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
-      const uint32_t pblocks = (uint32_t)sms() * (d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u);
-#define RT_LAUNCH_P(CNT, WW) k_trace_accel_persistent<CNT, WW><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter)
-      if (count) { if (ww) RT_LAUNCH_P(true, true); else RT_LAUNCH_P(true, false); }
-      else { if (ww) RT_LAUNCH_P(false, true); else RT_LAUNCH_P(false, false); }
-#undef RT_LAUNCH_P
-    } else {
-      const uint32_t sblocks = (M.slots + 127) / 128;
-#define RT_LAUNCH_S(CNT, WW) k_trace_accel<CNT, WW><<<sblocks, 128, 0, st>>>(A, C, M)
-      if (count) { if (ww) RT_LAUNCH_S(true, true); else RT_LAUNCH_S(true, false); }
-      else { if (ww) RT_LAUNCH_S(false, true); else RT_LAUNCH_S(false, false); }
-#undef RT_LAUNCH_S
-    }
-    note_launch();
-    RT_CHECK_LAUNCH();
-    return RT_OK;
+    return launch_accel<false>(d, A, SeedArgs{}, st);
   }
   if (d->tris) {
     if (count) k_trace<true, true><<<blocks, 128, 0, st>>>(A);
@@ -725,6 +816,18 @@ extern "C" rt_status rt_trace_closest(const rt_trace_desc* d, rt_stream stream) 
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
+}
+
+extern "C" rt_status rt_trace_closest_seeded(const rt_trace_desc* d, const rt_seed_desc* sd, rt_stream stream) {
+  TraceArgs A;
+  const rt_status s = trace_args(d, A);
+  if (s != RT_OK) return s;
+  if (!sd || !sd->proposal || !sd->slot_ref || !d->accel || !d->tris) return RT_ERR_INVALID_ARGUMENT;
+  if (d->ray_count == 0) return RT_OK;
+  SeedArgs S;
+  S.proposal = sd->proposal; S.slot_ref = sd->slot_ref; S.slot_box = (const float4*)sd->slot_box; S.slot_count = sd->slot_count;
+  S.in_prop = sd->in_proposal;
+  return launch_accel<true>(d, A, S, (cudaStream_t)stream);
 }
 
 extern "C" rt_status rt_ray_order_scratch_bytes(uint32_t count, size_t* bytes) {

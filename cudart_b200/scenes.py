@@ -151,6 +151,42 @@ def concat_batch(meshes):
     return verts, faces, fo, vo
 
 
+def learned_scene(scale: float = 1.0, seed: int = 4):
+    """Terrain + soup for the learned proposal: a 512 x 512 height field (522,242
+    triangles) with 3,500,000 soup triangles (vertex noise sigma 0.01) whose
+    centroids are uniform in the 2 x 0.5 x 2 box x, z in [-1, 1], y in [0.45, 0.95]
+    above it (the terrain spans y in [-0.4, 0.4]). `scale` shrinks both triangle
+    counts (grid side ~ 512 sqrt(scale)) for smaller test cases."""
+    side = max(8, int(round(511 * math.sqrt(scale)))) + 1
+    t = terrain(side, seed)
+    s = soup(max(1, int(round(3_500_000 * scale))), seed + 1, lo=(-1.0, 0.45, -1.0), hi=(1.0, 0.95, 1.0))
+    return concat(t, s)
+
+
+def scene_box(mesh: Mesh, factor: float = 1.5):
+    """The mesh's bounding box grown by `factor` about its centre (lo xyz, hi xyz)."""
+    v = mesh.vertices[:, :3].astype(np.float64)
+    lo, hi = v.min(0), v.max(0)
+    c, h = 0.5 * (lo + hi), 0.5 * (hi - lo) * factor
+    return tuple(float(x) for x in np.concatenate([c - h, c + h]))
+
+
+def box_rays_torch(count: int, box, seed: int, device="cuda"):
+    """`count` rays with origins uniform in `box` and directions uniform on the
+    unit sphere (float4, w = 0), drawn on the device from a seeded generator."""
+    import torch
+
+    g = torch.Generator(device=device).manual_seed(seed)
+    lo = torch.tensor(box[:3], dtype=torch.float32, device=device)
+    hi = torch.tensor(box[3:], dtype=torch.float32, device=device)
+    o = torch.zeros((count, 4), dtype=torch.float32, device=device)
+    d = torch.zeros((count, 4), dtype=torch.float32, device=device)
+    o[:, :3] = lo + (hi - lo) * torch.rand((count, 3), generator=g, device=device)
+    v = torch.randn((count, 3), generator=g, device=device)
+    d[:, :3] = v / v.norm(dim=1, keepdim=True).clamp(min=1e-30)
+    return o, d
+
+
 def sphere_rays(mesh: Mesh, side: int, seed: int):
     """side x side rays with origins uniform on the mesh's bounding sphere, each
     aimed at a uniform point inside the sphere (float32 float4 origin, direction)."""

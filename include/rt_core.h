@@ -51,6 +51,7 @@ typedef enum rt_status {
 #define RT_DEVERR_NODE_CAPACITY 0x1u  /* more nodes than max_nodes */
 #define RT_DEVERR_STACK_OVERFLOW 0x2u /* traversal stack exhausted (result of that ray may be wrong) */
 #define RT_DEVERR_MORTON_CAPACITY 0x4u
+#define RT_DEVERR_WAIT_TIMEOUT 0x8u    /* a bounded wait inside a kernel ran out (2 s); that kernel's output is invalid */
 
 typedef struct rt_build_params {
   uint32_t tree_depth;    /* Morton levels; reference default 12 (CUDAMeshTree.h:118); 1..32 */

@@ -1,0 +1,155 @@
+/* rt_propose.h -- C ABI of the learned subtree proposal (sm_100a).
+ *
+ * No reference counterpart: gatouillatpy/cudart has no learned component.
+ * These entry points add a proposal in front of rt_trace_closest: a small MLP
+ * maps each ray to one BVH subtree (a "slot" of the tree cut at a fixed depth),
+ * the traversal tests that subtree first and starts the full traversal with the
+ * hit it found as its best so far. The full traversal still runs, so the hit
+ * (id, t, u, v) is bit-identical to rt_trace_closest's; only the work changes.
+ *
+ * Network: 6 inputs (origin scaled to [-1, 1] over a box, unit direction) ->
+ * sin/cos(pi 2^j u), j < 12 (144 features, zero-padded to 192) -> 3 x 128 ReLU
+ * -> 2^depth logits. BF16 weights [out][in], FP32 biases, FP32 accumulation on
+ * the tensor cores (tcgen05, TMA, tensor memory).
+ */
+#ifndef RT_PROPOSE_H
+#define RT_PROPOSE_H
+
+#include "rt_core.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RT_PROPOSE_ABI_VERSION 1u
+uint32_t rt_propose_abi_version(void);
+
+/* C = alpha * A * B^T (+ bias[n]) (ReLU) (* (mask > 0)), on the tensor cores.
+ * A: BF16 [m][lda], B: BF16 [n][ldb], both K-major. m % 128 == 0, k % 64 == 0,
+ * n % 16 == 0; lda, ldb multiples of 8; pointers 16-byte aligned. Outputs (any
+ * subset): FP32 [m][ldc_f32], BF16 [m][ldc_bf16], BF16 transposed [n][ldct]. */
+typedef struct rt_gemm_desc {
+  const void* a;
+  uint32_t lda;
+  const void* b;
+  uint32_t ldb;
+  uint32_t m, n, k;
+  float alpha;
+  const float* bias;
+  uint32_t relu;
+  const void* mask; /* BF16 [m][ldmask] or NULL: outputs where mask <= 0 are zeroed (ReLU backward) */
+  uint32_t ldmask;
+  float* c_f32;
+  uint32_t ldc_f32;
+  void* c_bf16;
+  uint32_t ldc_bf16;
+  void* ct_bf16;
+  uint32_t ldct;
+  uint32_t* error_word; /* optional: RT_DEVERR_WAIT_TIMEOUT */
+} rt_gemm_desc;
+rt_status rt_gemm_bf16(const rt_gemm_desc* d, rt_stream stream);
+
+/* out_index[i] = argmax_j (A B^T + bias)[i][j] (lowest j among equal maxima),
+ * out_value[i] = that maximum, out_margin[i] = maximum - second largest value;
+ * out_index[i] = -1 when the margin is below min_margin. The m x n logits are
+ * never stored. m % 128 == 0, n % 256 == 0, n <= 4096, k % 64 == 0, k <= 256. */
+typedef struct rt_gemm_argmax_desc {
+  const void* a;
+  uint32_t lda;
+  const void* b;
+  uint32_t ldb;
+  uint32_t m, n, k;
+  const float* bias;
+  float min_margin;
+  int32_t* out_index;
+  float* out_value;  /* optional */
+  float* out_margin; /* optional */
+  uint32_t* error_word;
+} rt_gemm_argmax_desc;
+rt_status rt_gemm_argmax_bf16(const rt_gemm_argmax_desc* d, rt_stream stream);
+
+/* Ray features: u = ((o - c) * 2 / (hi - lo), d / |d|), c = (lo + hi) / 2;
+ * f[24 i + 2 j] = sin(pi 2^j u_i), f[24 i + 2 j + 1] = cos(pi 2^j u_i), j < 12;
+ * columns 144 .. 191 are zero. out: BF16 [count][ld_out] (ld_out >= 192, a
+ * multiple of 8; 16-byte aligned); out_t: BF16 [192][ld_out_t] (rows 144..191
+ * zero). */
+typedef struct rt_feature_desc {
+  const float* orig; /* float4 per ray */
+  const float* dir;  /* float4 per ray */
+  uint32_t count;
+  float box_lo[3], box_hi[3];
+  void* out;
+  uint32_t ld_out;
+  void* out_t;
+  uint32_t ld_out_t;
+} rt_feature_desc;
+rt_status rt_ray_features(const rt_feature_desc* d, rt_stream stream);
+
+/* grad[r][j] = (softmax(logits[r])_j - [j == labels[r]]) * scale (BF16), rows
+ * with a label outside [0, cols) get 0; *loss_sum += scale * (logsumexp - logit[label]).
+ * cols % 128 == 0. */
+rt_status rt_softmax_xent(const float* logits, uint32_t rows, uint32_t cols, const int32_t* labels, float scale, void* grad_bf16,
+                          float* loss_sum, rt_stream stream);
+/* out[c][r] = in[r][c] (BF16). */
+rt_status rt_transpose_bf16(const void* in, uint32_t rows, uint32_t cols, uint32_t ld_in, void* out, uint32_t ld_out, rt_stream stream);
+/* out[c] = sum_r in[r][c] (BF16 in, FP32 out; out is overwritten). */
+rt_status rt_colsum_bf16(const void* in, uint32_t rows, uint32_t cols, uint32_t ld, float* out, rt_stream stream);
+
+/* One Adam step (bias-corrected, step >= 1) on FP32 parameters [rows][cols];
+ * refreshes BF16 copies [rows][ld_bf16] and [cols][ld_bf16_t] when given. */
+typedef struct rt_adam_desc {
+  float* param;
+  const float* grad;
+  float* m;
+  float* v;
+  uint32_t rows, cols;
+  float lr, beta1, beta2, eps;
+  uint32_t step;
+  void* out_bf16;
+  uint32_t ld_bf16;
+  void* out_bf16_t;
+  uint32_t ld_bf16_t;
+} rt_adam_desc;
+rt_status rt_adam_step(const rt_adam_desc* d, rt_stream stream);
+
+/* Slots of a built tree cut at `depth` (1..16): slot s follows the bits of s
+ * (most significant first, 0 = left child) from the root for `depth` levels
+ * or until a leaf. slot_ref[s] = traversal-blob reference of the node reached
+ * (int32 bits of the blob's child reference). A slot is the "first" slot of
+ * its node when the bits below the node's depth are zero; pos_label[p] = the
+ * first slot of the node holding face position p. */
+typedef struct rt_slot_desc {
+  const uint32_t* nodes; /* bvnode array of rt_lbvh_build */
+  const void* accel;     /* traversal blob of the same build */
+  uint32_t face_count;
+  uint32_t depth;
+  int32_t* slot_ref;  /* [2^depth] */
+  float* slot_box;    /* [2^depth][8], optional: padded box of the slot's node (min xyz, 0, max xyz, 0) */
+  int32_t* pos_label; /* [face_count], optional */
+  uint32_t* slot_first; /* [2^depth], optional: first face position of the slot's node (first slots), else 0 */
+  uint32_t* slot_count; /* [2^depth], optional: face count of the slot's node (first slots), else 0 */
+} rt_slot_desc;
+rt_status rt_subtree_slots(const rt_slot_desc* d, rt_stream stream);
+
+/* labels[r] = pos_label[hit_pos[r]] for hits (hit_pos >= 0), -1 for misses. */
+rt_status rt_hit_labels(const int32_t* hit_pos, uint32_t count, const int32_t* pos_label, int32_t* labels, rt_stream stream);
+
+/* rt_trace_closest (blob path, d->accel and d->tris required) where ray r first
+ * walks the subtree slot_ref[proposal[r]] (proposal[r] < 0 or >= slot_count:
+ * none), then the whole tree minus that subtree, starting from the best hit the
+ * first walk found. With slot_box, a ray that misses the proposed node's box
+ * skips the first walk (one box read). Outputs are bit-identical to
+ * rt_trace_closest's. */
+typedef struct rt_seed_desc {
+  const int32_t* proposal;
+  const int32_t* slot_ref;
+  const float* slot_box; /* optional, rt_slot_desc.slot_box of the same tree */
+  uint32_t slot_count;
+  int32_t* in_proposal; /* optional [ray_count]: 1 when the final hit lies in the proposed subtree */
+} rt_seed_desc;
+rt_status rt_trace_closest_seeded(const rt_trace_desc* d, const rt_seed_desc* s, rt_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RT_PROPOSE_H */

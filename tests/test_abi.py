@@ -26,6 +26,11 @@ def test_header_declarations_are_exported():
     for name in declared:
         assert hasattr(lib, name), name
     assert set(declared) <= set(_abi.EXPORTS)
+    proposal = _declared("rt_propose.h")
+    assert len(proposal) >= 10
+    for name in proposal:
+        assert hasattr(lib, name), name
+    assert set(proposal) == set(_abi.PROPOSE_EXPORTS)
 
 
 def test_status_strings_and_version():
