@@ -54,6 +54,8 @@ def lib():
         L.or_lbvh_build.argtypes = [_P, _U32, _P, _U32, _P, _U32, C.c_int, C.c_int, _P, _P, _P, _P, _U32, _P, _P, _P]
         L.or_build_topology.argtypes = [_P, _U32, _U32, C.c_int, _U32, _U32, _P, _U32, _P]
         L.or_interpolate.argtypes = [_P, _P, C.c_long, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.or_sah_build.restype = C.c_int
+        L.or_sah_build.argtypes = [_P, _P, _P, _U32, _P, _U32, _P, _U32, _P, _P]
         _lib = L
     return _lib
 
@@ -73,6 +75,8 @@ def ref():
         R.ref_trace.argtypes = [_P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P]
         R.ref_camera_rays.argtypes = [_P, _P, C.c_float, C.c_float, C.c_int, C.c_int, _P, _P, _P, _P]
         R.ref_interpolate.argtypes = [_P, _P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        R.ref_sah_build.restype = C.c_int
+        R.ref_sah_build.argtypes = [_P, _P, _P, _U32, _P, _U32, _P, _U32, _P]
         _ref = R
     return _ref
 
@@ -137,6 +141,42 @@ def lbvh_build(vertices, faces, hit=None, tree_depth=12, tree_complete=True, lay
                              _U32(cap), _ptr(faces_out), _ptr(tris), _ptr(info))
     return dict(boxes=boxes, indices=idx, codes=codes, nodes=nodes[:nc].copy(), faces=faces_out, tris=tris,
                 info=dict(zip(INFO_KEYS, (int(x) for x in info))))
+
+
+def sah_build(vertices, faces, hit=None, hybrid_depth=None):
+    """Full oracle SAH build (CUDAMeshTree::buildMeshTreeSAH) or, with
+    hybrid_depth, the Hybrid build (LBVH of that depth without leaf splitting
+    or reorder, then SAH on every leaf). Returns dict with boxes, indices,
+    nodes, faces (reordered), tris, no_split (leaves made because no bin
+    boundary splits a node of >= 224 faces)."""
+    n = len(faces)
+    if hit is None:
+        hit = np.zeros(8, np.float32)
+        lib().or_hitbox(_ptr(vertices), _U32(len(vertices)), _ptr(hit))
+    hit = np.ascontiguousarray(hit, np.float32)
+    cap = 2 * n + 64
+    if hybrid_depth is None:
+        boxes = np.zeros((n, 8), np.float32)
+        idx = np.zeros(n, np.uint32)
+        lib().or_mesh_boxes(_ptr(vertices), _ptr(faces), _U32(n), _ptr(boxes), _ptr(idx))
+        nodes_in, nc_in = None, 0
+    else:
+        lb = lbvh_build(vertices, faces, hit, tree_depth=hybrid_depth, tree_complete=False)
+        boxes, idx = lb["boxes"], lb["indices"].copy()
+        nodes_in, nc_in = np.ascontiguousarray(lb["nodes"]), lb["info"]["node_count"]
+        cap += nc_in
+    nodes = np.zeros((cap, 8), np.float32)
+    nc = np.zeros(1, np.uint32)
+    stats = np.zeros(4, np.uint32)
+    rc = lib().or_sah_build(_ptr(boxes), _ptr(hit), _ptr(idx), _U32(n), _ptr(nodes_in), _U32(nc_in), _ptr(nodes), _U32(cap),
+                            _ptr(nc), _ptr(stats))
+    if rc != 0:
+        raise RuntimeError(f"or_sah_build failed ({rc})")
+    faces_out = np.zeros_like(faces)
+    lib().or_reorder_faces(_ptr(faces), _ptr(idx), _U32(n), _ptr(faces_out))
+    tris = np.zeros((n, 12), np.float32)
+    lib().or_pack_tris(_ptr(vertices), _ptr(faces_out), _U32(n), _ptr(tris))
+    return dict(boxes=boxes, indices=idx, nodes=nodes[: int(nc[0])].copy(), faces=faces_out, tris=tris, no_split=int(stats[0]))
 
 
 def camera_look_at(center, target):
@@ -232,6 +272,24 @@ def ref_lbvh_build(boxes, hit, tree_depth=12, tree_complete=True):
     nc = ref().ref_lbvh_build(_ptr(boxes), _U32(n), _ptr(hit), _U32(tree_depth), C.c_int(int(tree_complete)),
                               _ptr(codes), _ptr(idx), _ptr(nodes), _U32(cap), _ptr(info))
     return dict(codes=codes, indices=idx, nodes=nodes[:nc].copy(), real_depth=int(info[1]), split_count=int(info[2]))
+
+
+def ref_sah_build(boxes, root_box, indices, nodes_in=None, capacity=None):
+    """The reference's SAH kernels (emulated blocks, serial order) on face boxes
+    and an index order; nodes_in refines an existing tree's leaves (Hybrid).
+    Returns (status, nodes, indices): status 0 ok, 1 stack overflow, 2 node
+    capacity exceeded (the reference does not terminate)."""
+    n = len(boxes)
+    idx = np.ascontiguousarray(indices, np.uint32).copy()
+    nc_in = 0 if nodes_in is None else len(nodes_in)
+    cap = capacity or (2 * n + 64 + nc_in)
+    nodes = np.zeros((cap, 8), np.float32)
+    nc = np.zeros(1, np.uint32)
+    root = np.ascontiguousarray(root_box, np.float32)
+    st = ref().ref_sah_build(_ptr(np.ascontiguousarray(boxes, np.float32)), _ptr(root), _ptr(idx), _U32(n),
+                             _ptr(None if nodes_in is None else np.ascontiguousarray(nodes_in, np.float32)), _U32(nc_in),
+                             _ptr(nodes), _U32(cap), _ptr(nc))
+    return int(st), nodes[: min(int(nc[0]), cap)].copy(), idx
 
 
 def ref_reorder_faces(faces, indices):

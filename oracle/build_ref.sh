@@ -13,7 +13,7 @@
 #
 # Output: oracle/_ref/libref_cudart.so exporting ref_mesh_boxes, ref_lbvh_build,
 # ref_reorder_faces, ref_trace, ref_camera_rays, ref_interpolate, ref_mesh_quick_save,
-# ref_mesh_quick_load, ref_tree_quick_save. TEST INFRASTRUCTURE ONLY.
+# ref_mesh_quick_load, ref_tree_quick_save, ref_sah_build. TEST INFRASTRUCTURE ONLY.
 #
 # Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
 set -euo pipefail
@@ -32,9 +32,29 @@ rng() { echo "#line $2 \"$1\""; sed -n "$2,$3p" "$REF/$1"; }
 
 CXXFLAGS=(-O2 -ffp-contract=off -fno-strict-aliasing -w -shared -fPIC -std=c++17)
 
-build_tu() {  # build_tu NAME  (reads the TU from stdin)
-  g++ "${CXXFLAGS[@]}" -x c++ - -c -o "$OUT/$1.o"
+build_tu() {  # build_tu NAME [extra flags]  (reads the TU from stdin)
+  local name="$1"; shift
+  g++ "${CXXFLAGS[@]}" "$@" -x c++ - -c -o "$OUT/$name.o"
 }
+
+S=kernels/CUDA_buildMeshTreeSAH.cu
+{
+  echo "#define SHIM_THREADED 1"
+  cat "$SHIM/prelude.hpp"
+  cat "$SHIM/sah_shim.hpp"
+  echo "namespace renderkit {"
+  rng CUDABin.h 15 113   # bvbin
+  echo "}"
+  echo "namespace tu_sah {"
+  rng "$S" 31 40      # item
+  rng "$S" 46 56      # BLOCK_SIZE, SM_BIN_COUNT, STACK_SIZE, costs, leaf sizes
+  rng "$S" 62 67      # __device__ mutex, stack, sp, node_count
+  rng "$S" 73 73      # texture tex_boxes
+  rng "$S" 79 159     # stack_push_global, stack_push, stack_pop, make_node, make_leaf
+  rng "$S" 224 666    # kernel_buildMeshTree, kernel_initStack
+  cat "$SHIM/sah_epilogue.hpp"
+  echo "}"
+} | build_tu ref_sah
 
 L=kernels/CUDA_buildMeshTreeLBVH.cu
 {
@@ -125,6 +145,6 @@ I=kernels/CUDA_interpolateData.cu
   echo "}"
 } | build_tu ref_file
 
-g++ -shared -fPIC -o "$OUT/libref_cudart.so" "$OUT"/ref_lbvh.o "$OUT"/ref_boxes.o "$OUT"/ref_reorder.o "$OUT"/ref_trace.o "$OUT"/ref_rays.o "$OUT"/ref_interp.o "$OUT"/ref_file.o
+g++ -shared -fPIC -o "$OUT/libref_cudart.so" "$OUT"/ref_lbvh.o "$OUT"/ref_boxes.o "$OUT"/ref_reorder.o "$OUT"/ref_trace.o "$OUT"/ref_rays.o "$OUT"/ref_interp.o "$OUT"/ref_file.o "$OUT"/ref_sah.o -lpthread
 rm -f "$OUT"/*.o
 echo "built $OUT/libref_cudart.so"

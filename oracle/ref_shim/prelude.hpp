@@ -48,7 +48,14 @@ typedef unsigned int uint;
 #define CUDART_NORM_HUGE_F 3.402823466e+38f
 
 struct ShimDim3 { unsigned x, y, z; };
+#ifdef SHIM_THREADED
+// kernels with __syncthreads run their 32 threads as real host threads
+// (sah_shim.hpp); each has its own threadIdx
+static ShimDim3 blockIdx, blockDim;
+static thread_local ShimDim3 threadIdx;
+#else
 static ShimDim3 blockIdx, blockDim, threadIdx;
+#endif
 
 enum cudaTextureReadMode { cudaReadModeElementType = 0 };
 template <typename T, int dim, int mode>
@@ -100,6 +107,13 @@ static inline float3 normalize(float3 v) { float inv_len = rsqrtf(dot(v, v)); re
 static inline float3 fminf(float3 a, float3 b) { return make_float3(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)); }
 static inline float3 fmaxf(float3 a, float3 b) { return make_float3(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)); }
 
+// Mixed float4 / float3 min and max: the float4 keeps its w (types/_cuda_float4.h),
+// the float3 result drops the other's w (types/_cuda_float3.h).
+static inline float4 fminf(float4 a, float3 b) { return make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), a.w); }
+static inline float4 fmaxf(float4 a, float3 b) { return make_float4(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z), a.w); }
+static inline float3 fminf(float3 a, float4 b) { return make_float3(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)); }
+static inline float3 fmaxf(float3 a, float4 b) { return make_float3(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)); }
+
 namespace renderkit {
 // bvnode: same members and bit layout as CUDANode.h:20-50.
 struct __attribute__((aligned(16))) bvnode {
@@ -124,10 +138,18 @@ static inline void getChildren(const bvnode& b, const float4& dir, int& near_id,
 // aabox: CUDABox.h:17-148 (the members used by the extracted kernels).
 struct __attribute__((aligned(16))) aabox {
   float4 min, max;
+  float getArea() const {
+    float4 v = max - min;
+    return 2.f * (v.x * v.y + v.x * v.z + v.y * v.z);
+  }
   void reset() { min = make_float4(+CUDART_NORM_HUGE_F); max = make_float4(-CUDART_NORM_HUGE_F); }
   void reset(const float4& v) { min = v; max = v; }
+  void reset(const float4& a, const float4& b) { min = a; max = b; }
+  void reset(const float3& a, const float3& b) { min = make_float4(a); max = make_float4(b); }
+  void merge(const aabox& b) { min = fminf(min, b.min); max = fmaxf(max, b.max); }
   void merge(const float4& v) { min = fminf(min, v); max = fmaxf(max, v); }
   void merge(const float4& a, const float4& b) { min = fminf(min, a); max = fmaxf(max, b); }
+  void merge(const float3& a, const float3& b) { min = fminf(min, a); max = fmaxf(max, b); }
 };
 }  // namespace renderkit
 using namespace renderkit;

@@ -392,6 +392,196 @@ OR_API u32 or_lbvh_build(const float* vertices, u32 vertex_count, const u32* fac
 }
 
 // ---------------------------------------------------------------------------
+// SAH / Hybrid build (kernels/CUDA_buildMeshTreeSAH.cu:224-789,
+// CUDAMeshTree.cpp:93-103). The reference keeps a global stack of work items
+// (node id, node box, face range); each launch runs one 32-thread block per
+// stacked item and every block pops one item, bins its faces' centroids on the
+// longest axis of their bounds into 32 bins, and either writes a leaf or
+// allocates two child ids with atomicAdd and pushes (right, left). Executed
+// serially (one block at a time), pops are depth first, left child first, so a
+// node is split in pre-order and the k-th split of a subtree whose root was
+// popped when the node counter stood at B gets children B + 2k, B + 2k + 1.
+// That serial order is the contract here (the GPU's concurrent blocks number
+// nodes in a racy order). One departure: a node of >= 224 faces for which no
+// bin boundary separates two non-empty sides (every centroid in one bin, or a
+// degenerate parent box) becomes a leaf; the reference never terminates there.
+// Arithmetic as written (no contraction); device fminf / fmaxf = C's.
+// ---------------------------------------------------------------------------
+namespace sah {
+const int kBins = 32;                      // SM_BIN_COUNT, :48
+const float kTriCost = 0.125f;             // TRI_RAY_COST, :52
+const float kBoxCost = 1.0f;               // BOX_RAY_COST, :53
+const u32 kMinLeaf = 16, kMaxLeaf = 224;   // :55-56
+
+struct Item { F4 mn, mx; u32 node, first, bound; };
+struct Bin { float bmin[3], bmax[3]; int count, lcount, rcount; float larea, rarea; };
+
+static inline F4 f4fmin(F4 a, F4 b) { return {fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), fminf(a.w, b.w)}; }
+static inline F4 f4fmax(F4 a, F4 b) { return {fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w)}; }
+// aabox::getArea (CUDABox.h:35-45)
+static inline float area(F4 mn, F4 mx) {
+  const F4 v = f4sub(mx, mn);
+  return 2.f * (v.x * v.y + v.x * v.z + v.y * v.z);
+}
+// (int) of a float inside a kernel: round toward zero, saturating, NaN -> 0
+static inline int f2i_rz_sat(float x) {
+  if (x != x) return 0;
+  if (x >= 2147483648.0f) return 2147483647;
+  if (x <= -2147483648.0f) return (int)0x80000000u;
+  return (int)x;
+}
+static inline float comp(F4 v, int axis) { return axis == 0 ? v.x : (axis == 1 ? v.y : v.z); }
+
+static void write_leaf(Node* nodes, u32 id, F4 mn, F4 mx, u32 first, u32 count) {
+  Node& o = nodes[id];
+  o.w0 = 1u | (count << 1);
+  o.w1 = first;
+  o.bmin[0] = mn.x; o.bmin[1] = mn.y; o.bmin[2] = mn.z;
+  o.bmax[0] = mx.x; o.bmax[1] = mx.y; o.bmax[2] = mx.z;
+}
+static void write_node(Node* nodes, u32 id, F4 mn, F4 mx, int axis, u32 child) {
+  Node& o = nodes[id];
+  o.w0 = (u32)axis << 1;
+  o.w1 = child;
+  o.bmin[0] = mn.x; o.bmin[1] = mn.y; o.bmin[2] = mn.z;
+  o.bmax[0] = mx.x; o.bmax[1] = mx.y; o.bmax[2] = mx.z;
+}
+}  // namespace sah
+
+// boxes: aabox per original face; indices: face ids in position order (in/out);
+// nodes_in / node_count_in: an existing tree whose leaves are refined (Hybrid),
+// or node_count_in = 0 for a full SAH build from root_box. Returns 0 or 2 when
+// the node capacity would be exceeded. stats[0] = leaves made because no bin
+// boundary splits a node of >= 224 faces.
+OR_API int or_sah_build(const float* boxes_f, const float* root_box, u32* indices, u32 n, const float* nodes_in, u32 node_count_in,
+                        float* nodes_out, u32 capacity, u32* node_count_out, u32* stats) {
+  using namespace sah;
+  const Box* boxes = (const Box*)boxes_f;
+  Node* nodes = (Node*)nodes_out;
+  std::vector<Item> stack;
+  std::vector<u32> tmp(n);
+  u32 node_count = 0, no_split = 0;
+  if (node_count_in == 0) {
+    Item it;
+    memcpy(&it.mn, root_box, 16);
+    memcpy(&it.mx, root_box + 4, 16);
+    it.node = 0; it.first = 0; it.bound = n;
+    stack.push_back(it);
+    node_count = 1;
+  } else {
+    if (node_count_in > capacity) return 2;
+    memcpy(nodes, nodes_in, (size_t)node_count_in * sizeof(Node));
+    node_count = node_count_in;
+    for (u32 k = 0; k < node_count_in; ++k) {  // kernel_initStack (:647-666), threads in order
+      const Node& b = nodes[k];
+      if (!(b.w0 & 1u)) continue;
+      Item it;
+      it.mn = {b.bmin[0], b.bmin[1], b.bmin[2], 0.0f};
+      it.mx = {b.bmax[0], b.bmax[1], b.bmax[2], 0.0f};
+      it.node = k; it.first = b.w1; it.bound = b.w1 + (b.w0 >> 1);
+      stack.push_back(it);
+    }
+  }
+  while (!stack.empty()) {
+    const Item it = stack.back();
+    stack.pop_back();
+    const u32 cnt = it.bound - it.first;
+    if (cnt <= kMinLeaf) { write_leaf(nodes, it.node, it.mn, it.mx, it.first, cnt); continue; }
+    // centroid bounds and the longest axis (:275-345)
+    F4 cmn = {kHuge, kHuge, kHuge, kHuge}, cmx = {-kHuge, -kHuge, -kHuge, -kHuge};
+    for (u32 l = it.first; l < it.bound; ++l) {
+      const Box& b = boxes[indices[l]];
+      const F4 c = f4scale(f4add(b.mn, b.mx), 0.5f);
+      cmn = f4fmin(cmn, c);
+      cmx = f4fmax(cmx, c);
+    }
+    const F4 ext = f4sub(cmx, cmn);
+    int axis;
+    if (ext.x > ext.y) axis = ext.x > ext.z ? 0 : 2;
+    else axis = ext.y > ext.z ? 1 : 2;
+    const float scale = (float)(kBins - 1) / comp(ext, axis);
+    const float bmin = comp(cmn, axis);
+    // binning (:356-409)
+    Bin bins[kBins];
+    for (int m = 0; m < kBins; ++m) {
+      for (int k = 0; k < 3; ++k) { bins[m].bmin[k] = kHuge; bins[m].bmax[k] = -kHuge; }
+      bins[m].count = bins[m].lcount = bins[m].rcount = 0;
+      bins[m].larea = bins[m].rarea = 0.f;
+    }
+    std::vector<unsigned char> bin_of(cnt);
+    for (u32 l = it.first; l < it.bound; ++l) {
+      const Box& b = boxes[indices[l]];
+      const F4 c = f4scale(f4add(b.mn, b.mx), 0.5f);
+      int m = f2i_rz_sat((comp(c, axis) - bmin) * scale);
+      if (m < 0) m = 0;
+      else if (m >= kBins - 1) m = kBins - 1;
+      bin_of[l - it.first] = (unsigned char)m;
+      Bin& q = bins[m];
+      q.bmin[0] = fminf(q.bmin[0], b.mn.x); q.bmin[1] = fminf(q.bmin[1], b.mn.y); q.bmin[2] = fminf(q.bmin[2], b.mn.z);
+      q.bmax[0] = fmaxf(q.bmax[0], b.mx.x); q.bmax[1] = fmaxf(q.bmax[1], b.mx.y); q.bmax[2] = fmaxf(q.bmax[2], b.mx.z);
+      q.count++;
+    }
+    // sweeps and the cost of every boundary (:423-474, bvbin::getSAH CUDABin.h:104-111)
+    F4 lmn = {kHuge, kHuge, kHuge, kHuge}, lmx = {-kHuge, -kHuge, -kHuge, -kHuge};
+    int lcount = 0;
+    for (int m = 0; m < kBins - 1; ++m) {
+      lcount += bins[m].count;
+      lmn = {fminf(lmn.x, bins[m].bmin[0]), fminf(lmn.y, bins[m].bmin[1]), fminf(lmn.z, bins[m].bmin[2]), lmn.w};
+      lmx = {fmaxf(lmx.x, bins[m].bmax[0]), fmaxf(lmx.y, bins[m].bmax[1]), fmaxf(lmx.z, bins[m].bmax[2]), lmx.w};
+      bins[m].larea += area(lmn, lmx);
+      bins[m].lcount += lcount;
+    }
+    const float parent_area = area(it.mn, it.mx);
+    float t_min = kHuge;
+    int m_min = -1;
+    F4 rmn = {kHuge, kHuge, kHuge, kHuge}, rmx = {-kHuge, -kHuge, -kHuge, -kHuge};
+    int rcount = 0;
+    for (int m = kBins - 1; m > 0; --m) {
+      rcount += bins[m].count;
+      rmn = {fminf(rmn.x, bins[m].bmin[0]), fminf(rmn.y, bins[m].bmin[1]), fminf(rmn.z, bins[m].bmin[2]), rmn.w};
+      rmx = {fmaxf(rmx.x, bins[m].bmax[0]), fmaxf(rmx.y, bins[m].bmax[1]), fmaxf(rmx.z, bins[m].bmax[2]), rmx.w};
+      Bin& q = bins[m - 1];
+      q.rarea += area(rmn, rmx);
+      q.rcount += rcount;
+      const float t = kBoxCost * 2.f + kTriCost * ((q.larea / parent_area) * q.lcount + (q.rarea / parent_area) * q.rcount);
+      if (t < t_min) { t_min = t; m_min = m - 1; }
+    }
+    // leaf by cost (:479-496); no usable boundary -> leaf (departure, see above)
+    if ((cnt < kMaxLeaf && t_min > (float)(cnt + 1) * kTriCost) || m_min < 0) {
+      if (m_min < 0 && cnt >= kMaxLeaf) ++no_split;
+      write_leaf(nodes, it.node, it.mn, it.mx, it.first, cnt);
+      continue;
+    }
+    // child boxes and the stable partition (:498-613)
+    F4 a_mn = {kHuge, kHuge, kHuge, kHuge}, a_mx = {-kHuge, -kHuge, -kHuge, -kHuge};
+    F4 b_mn = a_mn, b_mx = a_mx;
+    u32 nl = 0;
+    for (int m = 0; m < kBins; ++m) {
+      F4& mn = m <= m_min ? a_mn : b_mn;
+      F4& mx = m <= m_min ? a_mx : b_mx;
+      mn = {fminf(mn.x, bins[m].bmin[0]), fminf(mn.y, bins[m].bmin[1]), fminf(mn.z, bins[m].bmin[2]), mn.w};
+      mx = {fmaxf(mx.x, bins[m].bmax[0]), fmaxf(mx.y, bins[m].bmax[1]), fmaxf(mx.z, bins[m].bmax[2]), mx.w};
+      if (m <= m_min) nl += (u32)bins[m].count;
+    }
+    u32 li = it.first, ri = it.first + nl;
+    for (u32 l = it.first; l < it.bound; ++l) {
+      if (bin_of[l - it.first] <= m_min) tmp[li++] = indices[l];
+      else tmp[ri++] = indices[l];
+    }
+    memcpy(indices + it.first, tmp.data() + it.first, (size_t)cnt * 4);
+    if (node_count + 2 > capacity) return 2;
+    const u32 c = node_count;
+    node_count += 2;
+    write_node(nodes, it.node, it.mn, it.mx, axis, c);
+    stack.push_back(Item{b_mn, b_mx, c + 1, it.first + nl, it.bound});
+    stack.push_back(Item{a_mn, a_mx, c, it.first, it.first + nl});
+  }
+  *node_count_out = node_count;
+  if (stats) stats[0] = no_split;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
 // Camera and primary rays.
 // lookAt / angleFromDir: CUDACamera.cpp:126-132, 70-88 (float3 normalize uses the
 // host rsqrtf = 1/sqrtf). Basis and per-pixel directions:

@@ -12,8 +12,15 @@ reference's own functions, compiled from its sources by oracle/build_ref.sh
   soup_small.npz  soups of N in {1, 16, 17, 224, 225, 513, 5000} triangles:
                   nodes and indices per N.
   flatz.npz       a flat z = 0.5 plane (the node-box quirk).
+  sah.npz         the reference's SAH kernels (kernels/CUDA_buildMeshTreeSAH.cu,
+                  emulated blocks in serial order): nodes and indices of a full
+                  SAH build of a 64 x 64 terrain and of a 5000-triangle soup, and
+                  of the Hybrid build (LBVH depth 4, then SAH) of the terrain.
+                  Internal nodes keep only bits 0-2 of their first word (the
+                  reference leaves the rest unset).
 
-Run:  python tests/golden/make_golden.py   (needs /root/reference and a built oracle/_ref)
+Run:  python tests/golden/make_golden.py [sah]   (needs /root/reference and a built oracle/_ref;
+      "sah" writes sah.npz only)
 """
 import hashlib
 import os
@@ -70,6 +77,30 @@ def main():
     print("golden fixtures written to", HERE)
 
 
+def _mask_internal(nodes):
+    w = nodes.view(np.uint32).copy()
+    internal = (w[:, 0] & 1) == 0
+    w[internal, 0] &= 7
+    return w
+
+
+def sah_fixtures():
+    out = {}
+    cases = {"terrain": (scenes.terrain(64, 2), None), "soup": (scenes.soup(5000, 4), None), "hybrid": (scenes.terrain(64, 2), 4)}
+    for name, (m, depth) in cases.items():
+        hit = O.hitbox(m.vertices)
+        boxes, idx = O.ref_mesh_boxes(m.vertices, m.faces)
+        if depth is None:
+            st, nodes, ridx = O.ref_sah_build(boxes, hit, idx)
+        else:
+            lb = O.ref_lbvh_build(boxes, hit, tree_depth=depth, tree_complete=False)
+            st, nodes, ridx = O.ref_sah_build(boxes, hit, lb["indices"], nodes_in=lb["nodes"])
+        assert st == 0
+        out[f"nodes_{name}"] = _mask_internal(nodes)
+        out[f"indices_{name}"] = ridx
+    np.savez_compressed(os.path.join(HERE, "sah.npz"), **out)
+
+
 def flat_z_mesh():
     m = scenes.terrain(32, 3)
     v = m.vertices.copy()
@@ -79,4 +110,9 @@ def flat_z_mesh():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "sah":
+        sah_fixtures()
+        print("sah.npz written to", HERE)
+    else:
+        main()
+        sah_fixtures()
