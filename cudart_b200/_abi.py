@@ -31,6 +31,8 @@ EXPORTS = (
     "rt_trace_closest", "rt_ray_order_scratch_bytes", "rt_ray_order", "rt_interpolate", "rt_bounce_rays", "rt_mesh_file_save", "rt_mesh_file_info", "rt_mesh_file_load", "rt_tree_file_save", "rt_tree_file_info",
     "rt_tree_file_load", "rt_status_string", "rt_version", "rt_abi_version", "rt_device_check", "rt_launch_count",
 )
+# every symbol include/rt_sah.h declares
+SAH_EXPORTS = ("rt_sah_sizes", "rt_sah_build")
 # every symbol include/rt_propose.h declares
 PROPOSE_EXPORTS = (
     "rt_propose_abi_version", "rt_gemm_bf16", "rt_gemm_argmax_bf16", "rt_ray_features", "rt_softmax_xent", "rt_transpose_bf16",
@@ -101,6 +103,12 @@ class BatchTraceDesc(C.Structure):
                 ("schedule", _U32)]
 
 
+class SahDesc(C.Structure):
+    _fields_ = [("vertices", _P), ("vertex_count", _U32), ("face_count", _U32), ("faces_in", _P), ("faces_out", _P), ("hitbox", _P),
+                ("lbvh_depth", _U32), ("boxes", _P), ("indices", _P), ("nodes", _P), ("max_nodes", _U32), ("tris", _P), ("accel", _P),
+                ("accel_bytes", C.c_size_t), ("info", _P), ("scratch", _P), ("scratch_bytes", C.c_size_t)]
+
+
 class GemmDesc(C.Structure):
     _fields_ = [("a", _P), ("lda", _U32), ("b", _P), ("ldb", _U32), ("m", _U32), ("n", _U32), ("k", _U32), ("alpha", C.c_float),
                 ("bias", _P), ("relu", _U32), ("mask", _P), ("ldmask", _U32), ("c_f32", _P), ("ldc_f32", _U32), ("c_bf16", _P),
@@ -169,6 +177,10 @@ def lib():
             getattr(L, f"rt_{fn}_file_save").argtypes = [C.c_char_p, C.c_int, C.POINTER(st)]
             getattr(L, f"rt_{fn}_file_info").argtypes = [C.c_char_p, C.POINTER(st)]
             getattr(L, f"rt_{fn}_file_load").argtypes = [C.c_char_p, C.POINTER(st)]
+        L.rt_sah_sizes.argtypes = [_U32, _U32, C.POINTER(C.c_size_t), C.POINTER(_U32)]
+        L.rt_sah_build.argtypes = [C.POINTER(SahDesc), _P]
+        for name in SAH_EXPORTS:
+            getattr(L, name).restype = C.c_int
         L.rt_gemm_bf16.argtypes = [C.POINTER(GemmDesc), _P]
         L.rt_gemm_argmax_bf16.argtypes = [C.POINTER(GemmArgmaxDesc), _P]
         L.rt_ray_features.argtypes = [C.POINTER(FeatureDesc), _P]

@@ -173,6 +173,53 @@ def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_de
     return out
 
 
+def sah_sizes(face_count: int, lbvh_depth: int = 0):
+    nb = C.c_size_t(0)
+    mx = C.c_uint32(0)
+    _abi.check("rt_sah_sizes", _abi.lib().rt_sah_sizes(face_count, lbvh_depth, C.byref(nb), C.byref(mx)))
+    return nb.value, mx.value
+
+
+def build_sah(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, lbvh_depth: int = 0, accel: bool = True,
+              out: Tree | None = None, stream=None) -> Tree:
+    """SAH build (CUDAMeshTree::buildMeshTreeSAH) or, with lbvh_depth > 0, the
+    Hybrid build (buildMeshTreeHybrid(lbvh_depth)). Same Tree layout as
+    build_lbvh; `codes` is left unwritten."""
+    _need_cuda(vertices, "vertices", _F32, 4)
+    _need_cuda(faces, "faces", _I32, 4)
+    n = faces.shape[0]
+    dev = vertices.device
+    nbytes, max_nodes = sah_sizes(n, lbvh_depth)
+    if out is None:
+        out = Tree(
+            nodes=torch.empty((max_nodes, 8), dtype=torch.int32, device=dev),
+            boxes=torch.empty((n, 8), dtype=torch.float32, device=dev),
+            indices=torch.empty(n, dtype=torch.int32, device=dev),
+            codes=torch.zeros(n, dtype=torch.int32, device=dev),
+            faces=torch.empty((n, 4), dtype=torch.int32, device=dev),
+            tris=torch.empty((n, 12), dtype=torch.float32, device=dev),
+            info=torch.zeros(8, dtype=torch.int32, device=dev),
+            accel=torch.empty(accel_bytes(n), dtype=torch.uint8, device=dev) if accel else None,
+        )
+    scratch = _SCRATCH.get(nbytes, dev)
+    hb = None
+    if hitbox is not None:
+        hb = (C.c_float * 8)(*[float(x) for x in hitbox])
+    d = _abi.SahDesc()
+    d.vertices, d.vertex_count, d.face_count = vertices.data_ptr(), vertices.shape[0], n
+    d.faces_in, d.faces_out = faces.data_ptr(), out.faces.data_ptr()
+    d.hitbox = C.cast(hb, C.c_void_p).value if hb is not None else None
+    d.lbvh_depth = lbvh_depth
+    d.boxes, d.indices, d.nodes, d.max_nodes = out.boxes.data_ptr(), out.indices.data_ptr(), out.nodes.data_ptr(), out.nodes.shape[0]
+    d.tris = out.tris.data_ptr()
+    if out.accel is not None:
+        d.accel, d.accel_bytes = out.accel.data_ptr(), out.accel.numel()
+    d.info = out.info.data_ptr()
+    d.scratch, d.scratch_bytes = scratch.data_ptr(), scratch.numel()
+    _abi.check("rt_sah_build", _abi.lib().rt_sah_build(C.byref(d), _stream(stream)))
+    return out
+
+
 def trace(tree: Tree, orig: torch.Tensor, dir: torch.Tensor, tmax: torch.Tensor | None = None, id_mode: int = 0,
           counters: bool = False, use_tris: bool = True, vertices: torch.Tensor | None = None, out: dict | None = None,
           ray_count: int | None = None, use_accel: bool = True, schedule: dict | None = None, stream=None) -> dict:

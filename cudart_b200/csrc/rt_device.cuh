@@ -114,6 +114,48 @@ __device__ __forceinline__ void write_box(uint32_t* node, float3 mn, float3 mx) 
   __stcg(f + 5, mx.x); __stcg(f + 6, mx.y); __stcg(f + 7, mx.z);
 }
 
+// Two-child traversal records, indexed by pre-order rank (internal node p
+// with left child c has rank (c - 1) / 2): both children's padded boxes and
+// references (rank for an internal child, ~leaf index for a leaf child).
+// One internal node's two-child record.
+__device__ __forceinline__ void accel_node(const uint32_t* __restrict__ nodes, const uint32_t* __restrict__ leaf_lambda,
+                                           float4* __restrict__ tnodes, const uint32_t p) {
+  const uint2 w = *(const uint2*)(nodes + 8 * (size_t)p);
+  if (w.x & 1u) return;
+  const uint32_t rank = (w.y - 1u) >> 1;
+  float4 out[4];
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const uint32_t c = w.y + side;
+    const uint32_t* cn = nodes + 8 * (size_t)c;
+    const uint32_t cw0 = cn[0], cw1 = cn[1];
+    float3 mn = make_float3(__uint_as_float(cn[2]), __uint_as_float(cn[3]), __uint_as_float(cn[4]));
+    float3 mx = make_float3(__uint_as_float(cn[5]), __uint_as_float(cn[6]), __uint_as_float(cn[7]));
+    pad_box(mn, mx);
+    const uint32_t ref = (cw0 & 1u) ? ~leaf_lambda[c] : ((cw1 - 1u) >> 1);
+    out[2 * side] = make_float4(mn.x, mn.y, mn.z, __uint_as_float(ref));
+    out[2 * side + 1] = make_float4(mx.x, mx.y, mx.z, 0.0f);
+  }
+  float4* dst = tnodes + 4 * (size_t)rank;
+  dst[0] = out[0]; dst[1] = out[1]; dst[2] = out[2]; dst[3] = out[3];
+}
+
+// Traversal blob: header (256 B), internal-node records (64 B, <= N - 1),
+// leaf table (16 B, <= N), group boxes (32 B, <= N/8 + N).
+struct AccelLayout {
+  uint32_t* hdr;
+  float4* tnodes;
+  uint4* leaves;
+  float4* groups;
+};
+inline size_t carve_accel(Carve& c, AccelLayout& A, uint32_t n) {
+  A.hdr = c.take<uint32_t>(64);
+  A.tnodes = c.take<float4>(4 * (size_t)n);
+  A.leaves = c.take<uint4>(n);
+  A.groups = c.take<float4>(2 * ((size_t)n / 8 + n + 1));
+  return c.off + 256;
+}
+
 constexpr int kStack = 64;
 constexpr float kBoxPad = 1.220703125e-4f;      // 2^-13
 constexpr float kCullSlack = 1.0001220703125f;  // 1 + 2^-13

@@ -405,7 +405,7 @@ OR_API u32 or_lbvh_build(const float* vertices, u32 vertex_count, const u32* fac
 // nodes in a racy order). One departure: a node of >= 224 faces for which no
 // bin boundary separates two non-empty sides (every centroid in one bin, or a
 // degenerate parent box) becomes a leaf; the reference never terminates there.
-// Arithmetic as written (no contraction); device fminf / fmaxf = C's.
+// Arithmetic as written (no contraction); box min / max as omin / omax below.
 // ---------------------------------------------------------------------------
 namespace sah {
 const int kBins = 32;                      // SM_BIN_COUNT, :48
@@ -416,8 +416,14 @@ const u32 kMinLeaf = 16, kMaxLeaf = 224;   // :55-56
 struct Item { F4 mn, mx; u32 node, first, bound; };
 struct Bin { float bmin[3], bmax[3]; int count, lcount, rcount; float larea, rarea; };
 
-static inline F4 f4fmin(F4 a, F4 b) { return {fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), fminf(a.w, b.w)}; }
-static inline F4 f4fmax(F4 a, F4 b) { return {fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w)}; }
+// min / max in the order of the floats' bit patterns read as sign-magnitude
+// (-0 < +0; the reference's fminf leaves that tie unspecified), as the GPU's
+// ordered-key atomics compute them
+static inline u32 ordkey(float f) { u32 u; memcpy(&u, &f, 4); return (u & 0x80000000u) ? ~u : (u | 0x80000000u); }
+static inline float omin(float a, float b) { return ordkey(b) < ordkey(a) ? b : a; }
+static inline float omax(float a, float b) { return ordkey(b) > ordkey(a) ? b : a; }
+static inline F4 f4fmin(F4 a, F4 b) { return {omin(a.x, b.x), omin(a.y, b.y), omin(a.z, b.z), omin(a.w, b.w)}; }
+static inline F4 f4fmax(F4 a, F4 b) { return {omax(a.x, b.x), omax(a.y, b.y), omax(a.z, b.z), omax(a.w, b.w)}; }
 // aabox::getArea (CUDABox.h:35-45)
 static inline float area(F4 mn, F4 mx) {
   const F4 v = f4sub(mx, mn);
@@ -517,8 +523,8 @@ OR_API int or_sah_build(const float* boxes_f, const float* root_box, u32* indice
       else if (m >= kBins - 1) m = kBins - 1;
       bin_of[l - it.first] = (unsigned char)m;
       Bin& q = bins[m];
-      q.bmin[0] = fminf(q.bmin[0], b.mn.x); q.bmin[1] = fminf(q.bmin[1], b.mn.y); q.bmin[2] = fminf(q.bmin[2], b.mn.z);
-      q.bmax[0] = fmaxf(q.bmax[0], b.mx.x); q.bmax[1] = fmaxf(q.bmax[1], b.mx.y); q.bmax[2] = fmaxf(q.bmax[2], b.mx.z);
+      q.bmin[0] = omin(q.bmin[0], b.mn.x); q.bmin[1] = omin(q.bmin[1], b.mn.y); q.bmin[2] = omin(q.bmin[2], b.mn.z);
+      q.bmax[0] = omax(q.bmax[0], b.mx.x); q.bmax[1] = omax(q.bmax[1], b.mx.y); q.bmax[2] = omax(q.bmax[2], b.mx.z);
       q.count++;
     }
     // sweeps and the cost of every boundary (:423-474, bvbin::getSAH CUDABin.h:104-111)
@@ -526,8 +532,8 @@ OR_API int or_sah_build(const float* boxes_f, const float* root_box, u32* indice
     int lcount = 0;
     for (int m = 0; m < kBins - 1; ++m) {
       lcount += bins[m].count;
-      lmn = {fminf(lmn.x, bins[m].bmin[0]), fminf(lmn.y, bins[m].bmin[1]), fminf(lmn.z, bins[m].bmin[2]), lmn.w};
-      lmx = {fmaxf(lmx.x, bins[m].bmax[0]), fmaxf(lmx.y, bins[m].bmax[1]), fmaxf(lmx.z, bins[m].bmax[2]), lmx.w};
+      lmn = {omin(lmn.x, bins[m].bmin[0]), omin(lmn.y, bins[m].bmin[1]), omin(lmn.z, bins[m].bmin[2]), lmn.w};
+      lmx = {omax(lmx.x, bins[m].bmax[0]), omax(lmx.y, bins[m].bmax[1]), omax(lmx.z, bins[m].bmax[2]), lmx.w};
       bins[m].larea += area(lmn, lmx);
       bins[m].lcount += lcount;
     }
@@ -538,8 +544,8 @@ OR_API int or_sah_build(const float* boxes_f, const float* root_box, u32* indice
     int rcount = 0;
     for (int m = kBins - 1; m > 0; --m) {
       rcount += bins[m].count;
-      rmn = {fminf(rmn.x, bins[m].bmin[0]), fminf(rmn.y, bins[m].bmin[1]), fminf(rmn.z, bins[m].bmin[2]), rmn.w};
-      rmx = {fmaxf(rmx.x, bins[m].bmax[0]), fmaxf(rmx.y, bins[m].bmax[1]), fmaxf(rmx.z, bins[m].bmax[2]), rmx.w};
+      rmn = {omin(rmn.x, bins[m].bmin[0]), omin(rmn.y, bins[m].bmin[1]), omin(rmn.z, bins[m].bmin[2]), rmn.w};
+      rmx = {omax(rmx.x, bins[m].bmax[0]), omax(rmx.y, bins[m].bmax[1]), omax(rmx.z, bins[m].bmax[2]), rmx.w};
       Bin& q = bins[m - 1];
       q.rarea += area(rmn, rmx);
       q.rcount += rcount;
@@ -559,8 +565,8 @@ OR_API int or_sah_build(const float* boxes_f, const float* root_box, u32* indice
     for (int m = 0; m < kBins; ++m) {
       F4& mn = m <= m_min ? a_mn : b_mn;
       F4& mx = m <= m_min ? a_mx : b_mx;
-      mn = {fminf(mn.x, bins[m].bmin[0]), fminf(mn.y, bins[m].bmin[1]), fminf(mn.z, bins[m].bmin[2]), mn.w};
-      mx = {fmaxf(mx.x, bins[m].bmax[0]), fmaxf(mx.y, bins[m].bmax[1]), fmaxf(mx.z, bins[m].bmax[2]), mx.w};
+      mn = {omin(mn.x, bins[m].bmin[0]), omin(mn.y, bins[m].bmin[1]), omin(mn.z, bins[m].bmin[2]), mn.w};
+      mx = {omax(mx.x, bins[m].bmax[0]), omax(mx.y, bins[m].bmax[1]), omax(mx.z, bins[m].bmax[2]), mx.w};
       if (m <= m_min) nl += (u32)bins[m].count;
     }
     u32 li = it.first, ri = it.first + nl;

@@ -31,6 +31,10 @@ def test_header_declarations_are_exported():
     for name in proposal:
         assert hasattr(lib, name), name
     assert set(proposal) == set(_abi.PROPOSE_EXPORTS)
+    sah = _declared("rt_sah.h")
+    assert set(sah) == set(_abi.SAH_EXPORTS)
+    for name in sah:
+        assert hasattr(lib, name), name
 
 
 def test_status_strings_and_version():
