@@ -185,8 +185,8 @@ __device__ Decision decide(const Bins& B, float3 pmn, float3 pmx, uint32_t count
 struct LevelArgs {
   SNode* table;
   uint32_t* table_count;  // [0] entries, [1] big entries of the next level, [2] no-split leaves
-  uint32_t* big_next;     // table indices of the next level's big nodes
-  const uint32_t* big_cur;
+  uint2* big_next;        // (table index, faces) of the next level's big nodes
+  const uint32_t* big_cur;  // table indices of this level's big nodes handled one CTA each
   uint32_t level_begin, level_end;
   const uint32_t* idx_in;
   const Item* box_in;
@@ -223,8 +223,8 @@ __device__ __forceinline__ void write_split(const LevelArgs& A, uint32_t e, cons
   R.id = kNone;
   A.table[c] = L;
   A.table[c + 1] = R;
-  if (L.count > kBigNode) A.big_next[atomicAdd(A.table_count + 1, 1u)] = c;
-  if (R.count > kBigNode) A.big_next[atomicAdd(A.table_count + 1, 1u)] = c + 1;
+  if (L.count > kBigNode) A.big_next[atomicAdd(A.table_count + 1, 1u)] = make_uint2(c, L.count);
+  if (R.count > kBigNode) A.big_next[atomicAdd(A.table_count + 1, 1u)] = make_uint2(c + 1, R.count);
   A.table[e].child = c;
   A.table[e].info = (nd.info & 1u) | ((uint32_t)sp.axis << 2);  // keep the right-child bit
   child_out = c;
@@ -387,6 +387,159 @@ __global__ __launch_bounds__(kCta) void k_sah_big(LevelArgs A, uint32_t count_bi
   }
 }
 
+// ---------------------------------------------------------------- huge nodes
+// Nodes of more than kHugeNode faces are cut into tiles of kTile faces that
+// separate CTAs process: bounds and bins meet in global order-key atomics, one
+// warp per node decides, a scan over the tiles' left counts places every
+// tile, and each tile scatters its faces stably (per-thread slices + a block
+// scan), so the result equals the single-owner kernels'.
+constexpr uint32_t kHugeNode = 32768;
+constexpr uint32_t kTile = 8192;
+
+struct HugeArgs {
+  const uint32_t* node;   // [H] table index of huge node h
+  const uint32_t* tnode;  // [tiles] huge slot of tile t
+  const uint32_t* tstart; // [tiles] first face (position) of tile t
+  const uint32_t* tfirst; // [H] first tile of node h
+  uint32_t* keys;         // [H][8] centroid bounds as order keys (min xyz, max xyz)
+  Bins* bins;             // [H]
+  Decision* dec;          // [H]
+  Split* split;           // [H]
+  uint32_t* child;        // [H] first child table index, kNone when a leaf
+  uint32_t* tleft;        // [tiles] left faces per tile, then its exclusive scan
+  uint32_t H, tiles;
+};
+
+__global__ __launch_bounds__(256) void k_huge_reset(HugeArgs G) {
+  const uint32_t h = blockIdx.x;
+  if (h >= G.H) return;
+  if (threadIdx.x < 3) { G.keys[8 * h + threadIdx.x] = 0xFFFFFFFFu; G.keys[8 * h + 3 + threadIdx.x] = 0u; }
+  if (threadIdx.x < kBins) bins_reset(G.bins[h], (int)threadIdx.x);
+}
+
+__global__ __launch_bounds__(kCta) void k_huge_bounds(LevelArgs A, HugeArgs G) {
+  const uint32_t t = blockIdx.x;
+  const uint32_t h = G.tnode[t];
+  const SNode nd = A.table[G.node[h]];
+  const uint32_t ts = G.tstart[t], te = min(nd.first + nd.count, ts + kTile);
+  uint32_t k[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
+  for (uint32_t p = ts + threadIdx.x; p < te; p += kCta) {
+    const Item it = load_item(A.box_in + p);
+    const uint32_t cx = okey(0.5f * (it.mn.x + it.mx.x)), cy = okey(0.5f * (it.mn.y + it.mx.y)), cz = okey(0.5f * (it.mn.z + it.mx.z));
+    k[0] = min(k[0], cx); k[1] = min(k[1], cy); k[2] = min(k[2], cz);
+    k[3] = max(k[3], cx); k[4] = max(k[4], cy); k[5] = max(k[5], cz);
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      k[c] = min(k[c], __shfl_xor_sync(0xffffffffu, k[c], o));
+      k[3 + c] = max(k[3 + c], __shfl_xor_sync(0xffffffffu, k[3 + c], o));
+    }
+  }
+  if ((threadIdx.x & 31u) == 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { atomicMin(G.keys + 8 * h + c, k[c]); atomicMax(G.keys + 8 * h + 3 + c, k[3 + c]); }
+  }
+}
+
+__device__ __forceinline__ Split huge_split(const HugeArgs& G, uint32_t h) {
+  const uint32_t* k = G.keys + 8 * h;
+  return make_split(make_float3(ofloat(k[0]), ofloat(k[1]), ofloat(k[2])), make_float3(ofloat(k[3]), ofloat(k[4]), ofloat(k[5])));
+}
+
+__global__ __launch_bounds__(kCta) void k_huge_bins(LevelArgs A, HugeArgs G) {
+  __shared__ Bins B;
+  const uint32_t t = blockIdx.x;
+  const uint32_t h = G.tnode[t];
+  const SNode nd = A.table[G.node[h]];
+  const uint32_t ts = G.tstart[t], te = min(nd.first + nd.count, ts + kTile);
+  const Split sp = huge_split(G, h);
+  if (threadIdx.x < kBins) bins_reset(B, (int)threadIdx.x);
+  __syncthreads();
+  for (uint32_t p = ts + threadIdx.x; p < te; p += kCta) {
+    const Item it = load_item(A.box_in + p);
+    bins_add(B, bin_of(center_on(it, sp.axis), sp), it);
+  }
+  __syncthreads();
+  if (threadIdx.x < kBins) {
+    const int m = (int)threadIdx.x;
+    if (B.cnt[m]) {
+      Bins& g = G.bins[h];
+      atomicAdd(&g.cnt[m], B.cnt[m]);
+      for (int c = 0; c < 3; ++c) { atomicMin(&g.mn[c][m], B.mn[c][m]); atomicMax(&g.mx[c][m], B.mx[c][m]); }
+    }
+  }
+}
+
+// one warp per huge node
+__global__ __launch_bounds__(32) void k_huge_decide(LevelArgs A, HugeArgs G) {
+  const uint32_t h = blockIdx.x;
+  const uint32_t e = G.node[h];
+  const SNode nd = A.table[e];
+  const Split sp = huge_split(G, h);
+  const Decision d = decide(G.bins[h], make_float3(nd.mn.x, nd.mn.y, nd.mn.z), make_float3(nd.mx.x, nd.mx.y, nd.mx.z), nd.count);
+  if (threadIdx.x == 0) {
+    uint32_t c = kNone;
+    if (d.m_min >= 0) {
+      write_split(A, e, nd, sp, d, c);
+    } else {
+      A.table[e].info = (nd.info & 1u) | 2u;
+      atomicAdd(A.table_count + 2, 1u);
+    }
+    G.dec[h] = d;
+    G.split[h] = sp;
+    G.child[h] = c;
+  }
+}
+
+__global__ __launch_bounds__(kCta) void k_huge_count(LevelArgs A, HugeArgs G) {
+  __shared__ uint32_t s_w[kCta / 32];
+  const uint32_t t = blockIdx.x;
+  const uint32_t h = G.tnode[t];
+  const SNode nd = A.table[G.node[h]];
+  const uint32_t ts = G.tstart[t], te = min(nd.first + nd.count, ts + kTile);
+  const Decision& d = G.dec[h];
+  const Split sp = G.split[h];
+  uint32_t n = 0;
+  if (d.m_min >= 0)
+    for (uint32_t p = ts + threadIdx.x; p < te; p += kCta) n += bin_of(center_on(load_item(A.box_in + p), sp.axis), sp) <= d.m_min ? 1u : 0u;
+  uint32_t total;
+  block_excl_scan_nt<kCta>(n, s_w, total);
+  if (threadIdx.x == 0) G.tleft[t] = total;
+}
+
+__global__ __launch_bounds__(kCta) void k_huge_scatter(LevelArgs A, HugeArgs G) {
+  __shared__ uint32_t s_w[kCta / 32];
+  const uint32_t t = blockIdx.x;
+  const uint32_t h = G.tnode[t];
+  const SNode nd = A.table[G.node[h]];
+  const uint32_t ts = G.tstart[t], te = min(nd.first + nd.count, ts + kTile);
+  const Decision d = G.dec[h];
+  if (d.m_min < 0) {  // a leaf: its faces are final
+    for (uint32_t p = ts + threadIdx.x; p < te; p += kCta) A.final_idx[p] = A.idx_in[p];
+    return;
+  }
+  if (G.child[h] == kNone) return;
+  const Split sp = G.split[h];
+  const uint32_t left_before = G.tleft[t] - G.tleft[G.tfirst[h]];  // left faces in the node's earlier tiles
+  const uint32_t S = (te - ts + kCta - 1) / kCta;
+  const uint32_t a = min(te, ts + threadIdx.x * S), b = min(te, a + S);
+  uint32_t my_left = 0;
+  for (uint32_t p = a; p < b; ++p) my_left += bin_of(center_on(load_item(A.box_in + p), sp.axis), sp) <= d.m_min ? 1u : 0u;
+  uint32_t total;
+  const uint32_t lpre = block_excl_scan_nt<kCta>(my_left, s_w, total);
+  uint32_t lo = nd.first + left_before + lpre;
+  uint32_t ro = nd.first + d.nl + ((ts - nd.first) - left_before) + ((a - ts) - lpre);
+  for (uint32_t p = a; p < b; ++p) {
+    const Item it = load_item(A.box_in + p);
+    const uint32_t id = A.idx_in[p];
+    const uint32_t dst = bin_of(center_on(it, sp.axis), sp) <= d.m_min ? lo++ : ro++;
+    A.idx_out[dst] = id;
+    A.box_out[dst] = it;
+  }
+}
+
 // ---------------------------------------------------------------- setup
 // SAH: positions start as the faces in order, the root's box is the mesh box.
 __global__ __launch_bounds__(256) void k_sah_init(const float4* __restrict__ boxes, uint32_t n, const float* __restrict__ hit,
@@ -453,7 +606,7 @@ __global__ __launch_bounds__(256) void k_hyb_leaf_flags(const uint32_t* __restri
     flags_rev[m - 1 - k] = nodes[8 * (size_t)k] & 1u;
 }
 __global__ __launch_bounds__(256) void k_hyb_roots(const uint32_t* __restrict__ nodes, uint32_t m, const uint32_t* __restrict__ order_rev,
-                                                   SNode* table, uint32_t* big, uint32_t* counts) {
+                                                   SNode* table, uint2* big, uint32_t* counts) {
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
     const uint32_t* w = nodes + 8 * (size_t)k;
     if (!(w[0] & 1u)) continue;
@@ -463,7 +616,7 @@ __global__ __launch_bounds__(256) void k_hyb_roots(const uint32_t* __restrict__ 
     r.mx = make_float4(__uint_as_float(w[5]), __uint_as_float(w[6]), __uint_as_float(w[7]), 0.0f);
     r.first = w[1]; r.count = w[0] >> 1; r.parent = kNone; r.info = 0; r.child = kNone; r.sub = j; r.internal = 0; r.id = k;
     table[j] = r;
-    if (r.count > kBigNode) big[atomicAdd(counts + 1, 1u)] = j;
+    if (r.count > kBigNode) big[atomicAdd(counts + 1, 1u)] = make_uint2(j, r.count);
   }
 }
 
@@ -654,7 +807,13 @@ int sm_count() {
 }
 
 struct SahLayout {
-  uint32_t *idx_a, *idx_b, *big_a, *big_b, *counts, *rank, *base, *marks, *sums, *scalars, *keys, *err, *leaf_lambda;
+  uint32_t *idx_a, *idx_b, *big_list, *counts, *rank, *base, *marks, *sums, *scalars, *keys, *err, *leaf_lambda;
+  uint2 *big_a, *big_b;
+  uint32_t *h_node, *h_tnode, *h_tstart, *h_tfirst, *h_keys, *h_child, *h_tleft, *h_sums;
+  Bins* h_bins;
+  Decision* h_dec;
+  Split* h_split;
+  uint32_t h_cap, t_cap;
   Item *box_a, *box_b;
   SNode* table;
   rt_build_info* lb_info;
@@ -671,8 +830,22 @@ size_t carve_sah(Carve& c, SahLayout& L, uint32_t n, uint32_t lbvh_depth, uint32
   L.idx_b = c.take<uint32_t>(n);
   L.box_a = c.take<Item>(n);
   L.box_b = c.take<Item>(n);
-  L.big_a = c.take<uint32_t>(n / kBigNode + 2);
-  L.big_b = c.take<uint32_t>(n / kBigNode + 2);
+  L.big_a = c.take<uint2>(n / kBigNode + 2);
+  L.big_b = c.take<uint2>(n / kBigNode + 2);
+  L.big_list = c.take<uint32_t>(n / kBigNode + 2);
+  L.h_cap = n / kHugeNode + 2;
+  L.t_cap = n / kTile + L.h_cap + 2;
+  L.h_node = c.take<uint32_t>(L.h_cap);
+  L.h_tfirst = c.take<uint32_t>(L.h_cap);
+  L.h_keys = c.take<uint32_t>(8 * (size_t)L.h_cap);
+  L.h_child = c.take<uint32_t>(L.h_cap);
+  L.h_bins = c.take<Bins>(L.h_cap);
+  L.h_dec = c.take<Decision>(L.h_cap);
+  L.h_split = c.take<Split>(L.h_cap);
+  L.h_tnode = c.take<uint32_t>(L.t_cap);
+  L.h_tstart = c.take<uint32_t>(L.t_cap);
+  L.h_tleft = c.take<uint32_t>(L.t_cap + 1);
+  L.h_sums = c.take<uint32_t>(L.t_cap / 1024 + 2);
   L.counts = c.take<uint32_t>(8);
   L.table = c.take<SNode>(L.table_cap);
   L.rank = c.take<uint32_t>(L.table_cap);
@@ -768,8 +941,8 @@ extern "C" rt_status rt_sah_build(const rt_sah_desc* d, rt_stream stream) {
     k_sah_init<<<grid, 256, 0, st>>>((const float4*)d->boxes, n, hit, L.idx_a, L.box_a, L.table, L.counts);
     note_launch();
     if (n > kBigNode) {
-      const uint32_t zero = 0;
-      if (cudaMemcpyAsync(L.big_a, &zero, 4, cudaMemcpyHostToDevice, st) != cudaSuccess) return RT_ERR_CUDA;
+      const uint2 root = make_uint2(0u, n);
+      if (cudaMemcpyAsync(L.big_a, &root, 8, cudaMemcpyHostToDevice, st) != cudaSuccess) return RT_ERR_CUDA;
     }
   } else {
     rt_build_desc b = {};
@@ -799,27 +972,80 @@ extern "C" rt_status rt_sah_build(const rt_sah_desc* d, rt_stream stream) {
 
   // levels
   std::vector<uint32_t> level_start;
-  uint32_t begin = 0, end = roots, big = 0;
+  uint32_t begin = 0, end = roots;
   uint32_t host_counts[3];
   if (cudaMemcpyAsync(host_counts, L.counts, 12, cudaMemcpyDeviceToHost, st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
     return RT_ERR_CUDA;
-  big = host_counts[1];
+  uint32_t nbig = host_counts[1];
   uint32_t* idx_in = L.idx_a;
   uint32_t* idx_out = L.idx_b;
   Item* box_in = L.box_a;
   Item* box_out = L.box_b;
-  uint32_t* big_cur = L.big_a;
-  uint32_t* big_next = L.big_b;
+  uint2* big_cur = L.big_a;
+  uint2* big_next = L.big_b;
+  std::vector<uint2> bigs;
+  std::vector<uint32_t> regular, h_node, h_tfirst, t_node, t_start;
   while (begin < end) {
     level_start.push_back(begin);
+    // this level's big nodes: a CTA each, or tiles of several CTAs when huge
+    bigs.resize(nbig);
+    regular.clear(); h_node.clear(); h_tfirst.clear(); t_node.clear(); t_start.clear();
+    if (nbig) {
+      if (cudaMemcpyAsync(bigs.data(), big_cur, (size_t)nbig * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          cudaStreamSynchronize(st) != cudaSuccess)
+        return RT_ERR_CUDA;
+    }
+    std::vector<SNode> firsts;  // first position of each huge node, read below
+    for (const uint2& bg : bigs) {
+      if (bg.y > kHugeNode && h_node.size() < L.h_cap) h_node.push_back(bg.x);
+      else regular.push_back(bg.x);
+    }
+    const uint32_t H = (uint32_t)h_node.size();
+    if (H) {
+      firsts.resize(H);
+      for (uint32_t h = 0; h < H; ++h)
+        if (cudaMemcpyAsync(&firsts[h], L.table + h_node[h], sizeof(SNode), cudaMemcpyDeviceToHost, st) != cudaSuccess) return RT_ERR_CUDA;
+      if (cudaStreamSynchronize(st) != cudaSuccess) return RT_ERR_CUDA;
+      for (uint32_t h = 0; h < H; ++h) {
+        h_tfirst.push_back((uint32_t)t_node.size());
+        for (uint32_t o = 0; o < firsts[h].count; o += kTile) {
+          t_node.push_back(h);
+          t_start.push_back(firsts[h].first + o);
+        }
+      }
+    }
+    const uint32_t tiles = (uint32_t)t_node.size();
+    if (tiles > L.t_cap) return RT_ERR_CAPACITY;
     const uint32_t zero = 0;
     if (cudaMemcpyAsync(L.counts + 1, &zero, 4, cudaMemcpyHostToDevice, st) != cudaSuccess) return RT_ERR_CUDA;
+    if (!regular.empty() &&
+        cudaMemcpyAsync(L.big_list, regular.data(), regular.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return RT_ERR_CUDA;
     LevelArgs A;
-    A.table = L.table; A.table_count = L.counts; A.big_next = big_next; A.big_cur = big_cur; A.level_begin = begin; A.level_end = end;
+    A.table = L.table; A.table_count = L.counts; A.big_next = big_next; A.big_cur = L.big_list; A.level_begin = begin; A.level_end = end;
     A.idx_in = idx_in; A.box_in = box_in; A.idx_out = idx_out; A.box_out = box_out; A.final_idx = d->indices; A.err = L.err;
     A.table_cap = L.table_cap;
-    if (big) {
-      k_sah_big<<<big, kCta, 0, st>>>(A, big);
+    if (H) {
+      if (cudaMemcpyAsync(L.h_node, h_node.data(), H * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+          cudaMemcpyAsync(L.h_tfirst, h_tfirst.data(), H * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+          cudaMemcpyAsync(L.h_tnode, t_node.data(), tiles * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+          cudaMemcpyAsync(L.h_tstart, t_start.data(), tiles * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return RT_ERR_CUDA;
+      HugeArgs G;
+      G.node = L.h_node; G.tnode = L.h_tnode; G.tstart = L.h_tstart; G.tfirst = L.h_tfirst; G.keys = L.h_keys; G.bins = L.h_bins;
+      G.dec = L.h_dec; G.split = L.h_split; G.child = L.h_child; G.tleft = L.h_tleft; G.H = H; G.tiles = tiles;
+      k_huge_reset<<<H, 64, 0, st>>>(G);
+      k_huge_bounds<<<tiles, kCta, 0, st>>>(A, G);
+      k_huge_bins<<<tiles, kCta, 0, st>>>(A, G);
+      k_huge_decide<<<H, 32, 0, st>>>(A, G);
+      k_huge_count<<<tiles, kCta, 0, st>>>(A, G);
+      note_launch(5);
+      excl_scan(L.h_tleft, tiles, L.h_sums, nullptr, st);
+      k_huge_scatter<<<tiles, kCta, 0, st>>>(A, G);
+      note_launch();
+    }
+    if (!regular.empty()) {
+      k_sah_big<<<(uint32_t)regular.size(), kCta, 0, st>>>(A, (uint32_t)regular.size());
       note_launch();
     }
     k_sah_small<<<(end - begin + 7) / 8, kCta, 0, st>>>(A);
@@ -829,7 +1055,7 @@ extern "C" rt_status rt_sah_build(const rt_sah_desc* d, rt_stream stream) {
       return RT_ERR_CUDA;
     begin = end;
     end = host_counts[0] < L.table_cap ? host_counts[0] : L.table_cap;
-    big = host_counts[1];
+    nbig = host_counts[1];
     std::swap(idx_in, idx_out);
     std::swap(box_in, box_out);
     std::swap(big_cur, big_next);
