@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--build16m", type=int, default=1, help="also time the LBVH build alone on a 2^24-face soup")
     ap.add_argument("--batch", type=int, default=1, help="also time the batched workload (1024 meshes, CUDA graph)")
     ap.add_argument("--learned", type=int, default=1, help="also train and time the learned subtree proposal (4M-triangle scene)")
+    ap.add_argument("--sah", type=int, default=1, help="also time the SAH and Hybrid builds and tracing through their trees")
     ap.add_argument("--learned-scale", type=float, default=1.0, help="triangle-count scale of the learned-proposal scene")
     return ap.parse_args()
 
@@ -282,6 +283,8 @@ def run_ours(args, rank, world, local_rank):
         result["build_16m"] = build_only(24, args, dev, world)
     if args.batch:
         result["batch_c2"] = batched(args, dev, world)
+    if args.sah:
+        result["sah"] = sah_leg(args, dev, world, mesh, camera, W, H, tree)
     if args.learned:
         result["nn_proposal_c3"] = learned(args, dev, world)
     clocks = clk.summary()
@@ -419,6 +422,59 @@ def batched(args, dev, world, count=1024):
            "device_errors": int((info[:, 7] != 0).sum()), "graph": "build + trace captured in one CUDA graph"}
     del graph
     return res
+
+
+def sah_leg(args, dev, world, mesh, camera, W, H, lbvh_tree):
+    """SAH and Hybrid (LBVH depth 12, then SAH) builds of the 2^20-face soup
+    (CUDA events, L2 flushed), and the primary + bounce trace through each tree
+    with its own tuned schedule, beside the LBVH tree's."""
+    import torch
+
+    from cudart_b200 import core, tune
+
+    v = torch.from_numpy(mesh.vertices).to(dev)
+    f = torch.from_numpy(mesh.faces.view(np.int32)).to(dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    o, d = core.primary_rays(camera, W, H)
+    base_hits = core.trace(lbvh_tree, o, d)
+    b = core.bounce_rays(lbvh_tree.tris, o, d, base_hits["id"], base_hits["t"], SEED_BOUNCE)
+    R = o.shape[0]
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    out = {"faces": int(f.shape[0])}
+    trees = {"lbvh": lbvh_tree}
+    sah = core.build_sah(v, f)
+    hyb = core.build_sah(v, f, lbvh_depth=12)
+    out["sah_build_ms"] = round(timed(lambda: core.build_sah(v, f, out=sah)), 4)
+    out["hybrid12_build_ms"] = round(timed(lambda: core.build_sah(v, f, lbvh_depth=12, out=hyb)), 4)
+    out["lbvh_build_ms"] = round(timed(lambda: core.build_lbvh(v, f, out=lbvh_tree)), 4)
+    out["sah_levels"] = sah.info_host()["real_depth"]
+    trees["sah"], trees["hybrid12"] = sah, hyb
+    for name, tr in trees.items():
+        s1, _ = tune.tune_trace(tr, o, d, image_width=W, key=f"sah-{name}-p", use_cache=False)
+        s2, _ = tune.tune_trace(tr, b[0], b[1], tmax=b[2], key=f"sah-{name}-b", use_cache=False)
+        tp = timed(lambda: core.trace(tr, o, d, schedule=s1))
+        tb = timed(lambda: core.trace(tr, b[0], b[1], tmax=b[2], schedule=s2))
+        cnt = core.trace(tr, o, d, counters=True)
+        out[name] = {"nodes": tr.node_count, "primary_ms": round(tp, 4), "bounce_ms": round(tb, 4),
+                     "mrays_s": round(world * 2 * R / ((tp + tb) * 1e-3) / 1e6, 2),
+                     "primary_visits_per_ray": round(cnt["visits"].float().mean().item(), 2),
+                     "primary_tests_per_ray": round(cnt["tests"].float().mean().item(), 2)}
+    del flush
+    return out
 
 
 def learned(args, dev, world, train_rays=16 << 20, eval_rays=8 << 20, batch=8192, lr=2e-3):
