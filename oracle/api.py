@@ -54,6 +54,8 @@ def lib():
         L.or_lbvh_build.argtypes = [_P, _U32, _P, _U32, _P, _U32, C.c_int, C.c_int, _P, _P, _P, _P, _U32, _P, _P, _P]
         L.or_build_topology.argtypes = [_P, _U32, _U32, C.c_int, _U32, _U32, _P, _U32, _P]
         L.or_interpolate.argtypes = [_P, _P, C.c_long, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.or_raster_matrix.argtypes = [_P, _P, _P, C.c_float, C.c_float, _P]
+        L.or_rasterize.argtypes = [_P, _P, _U32, _P, C.c_int, C.c_int, _P, _P, _P]
         L.or_sah_build.restype = C.c_int
         L.or_sah_build.argtypes = [_P, _P, _P, _U32, _P, _U32, _P, _U32, _P, _P]
         _lib = L
@@ -75,6 +77,8 @@ def ref():
         R.ref_trace.argtypes = [_P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P]
         R.ref_camera_rays.argtypes = [_P, _P, C.c_float, C.c_float, C.c_int, C.c_int, _P, _P, _P, _P]
         R.ref_interpolate.argtypes = [_P, _P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        R.ref_raster_matrix.argtypes = [_P, _P, _P, C.c_float, C.c_float, _P]
+        R.ref_rasterize.argtypes = [_P, _P, C.c_int, _P, C.c_int, C.c_int, _P, _P, _P]
         R.ref_sah_build.restype = C.c_int
         R.ref_sah_build.argtypes = [_P, _P, _P, _U32, _P, _U32, _P, _U32, _P]
         _ref = R
@@ -177,6 +181,51 @@ def sah_build(vertices, faces, hit=None, hybrid_depth=None):
     tris = np.zeros((n, 12), np.float32)
     lib().or_pack_tris(_ptr(vertices), _ptr(faces_out), _U32(n), _ptr(tris))
     return dict(boxes=boxes, indices=idx, nodes=nodes[: int(nc[0])].copy(), faces=faces_out, tris=tris, no_split=int(stats[0]))
+
+
+def look_dir(center, target):
+    """CUDACamera::lookAt's direction: (target - center) * (1 / sqrtf(|.|^2)) in float32."""
+    c = np.asarray(center, np.float32)
+    t = np.asarray(target, np.float32)
+    d = (t - c).astype(np.float32)
+    inv = np.float32(1.0) / np.float32(np.sqrt(np.float32(d[0] * d[0] + d[1] * d[1] + d[2] * d[2])))
+    return (d * inv).astype(np.float32)
+
+
+def raster_matrix(center, dir3, angle, fov, ratio):
+    out = np.zeros(16, np.float32)
+    lib().or_raster_matrix(_ptr(np.asarray(center, np.float32)), _ptr(np.asarray(dir3, np.float32)), _ptr(np.asarray(angle, np.float32)),
+                           C.c_float(fov), C.c_float(ratio), _ptr(out))
+    return out
+
+
+def rasterize(vertices, faces, matrix, width, height, faces_id=None, coords=None, depths=None):
+    """Oracle rasteriser; buffers start as CUDABuffer::clearOutputSurfaces leaves them
+    (id 0, uv 0, depth +HUGE) unless given. Returns (faces_id, coords, depths)."""
+    P = width * height
+    fid = np.zeros(P, np.uint32) if faces_id is None else faces_id.copy()
+    uv = np.zeros((P, 2), np.float32) if coords is None else coords.copy()
+    dep = np.full(P, HUGE, np.float32) if depths is None else depths.copy()
+    lib().or_rasterize(_ptr(vertices), _ptr(faces), _U32(len(faces)), _ptr(np.asarray(matrix, np.float32)), C.c_int(width),
+                       C.c_int(height), _ptr(fid), _ptr(uv), _ptr(dep))
+    return fid, uv, dep
+
+
+def ref_raster_matrix(center, dir3, angle, fov, ratio):
+    out = np.zeros(16, np.float32)
+    ref().ref_raster_matrix(_ptr(np.asarray(center, np.float32)), _ptr(np.asarray(dir3, np.float32)), _ptr(np.asarray(angle, np.float32)),
+                            C.c_float(fov), C.c_float(ratio), _ptr(out))
+    return out
+
+
+def ref_rasterize(vertices, faces, matrix, width, height):
+    P = width * height
+    fid = np.zeros(P, np.uint32)
+    uv = np.zeros((P, 2), np.float32)
+    dep = np.full(P, HUGE, np.float32)
+    ref().ref_rasterize(_ptr(vertices), _ptr(faces), C.c_int(len(faces)), _ptr(np.asarray(matrix, np.float32)), C.c_int(width),
+                        C.c_int(height), _ptr(fid), _ptr(uv), _ptr(dep))
+    return fid, uv, dep
 
 
 def camera_look_at(center, target):

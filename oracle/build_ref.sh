@@ -13,7 +13,8 @@
 #
 # Output: oracle/_ref/libref_cudart.so exporting ref_mesh_boxes, ref_lbvh_build,
 # ref_reorder_faces, ref_trace, ref_camera_rays, ref_interpolate, ref_mesh_quick_save,
-# ref_mesh_quick_load, ref_tree_quick_save, ref_sah_build. TEST INFRASTRUCTURE ONLY.
+# ref_mesh_quick_load, ref_tree_quick_save, ref_sah_build, ref_raster_matrix,
+# ref_rasterize. TEST INFRASTRUCTURE ONLY.
 #
 # Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
 set -euo pipefail
@@ -55,6 +56,33 @@ S=kernels/CUDA_buildMeshTreeSAH.cu
   cat "$SHIM/sah_epilogue.hpp"
   echo "}"
 } | build_tu ref_sah
+
+Z=kernels/CUDA_rasterizeMeshTree.cu
+{
+  echo "#define SHIM_THREADED 1"
+  cat "$SHIM/prelude.hpp"
+  cat "$SHIM/sah_shim.hpp"
+  cat "$SHIM/raster_shim.hpp"
+  echo "namespace tu_raster {"
+  rng types/_cuda_float4.h 135 140      # operator/=(float4, float): multiply by the reciprocal
+  rng types/_cuda_float4.h 210 227      # cross(float4, float4, float4)
+  rng types/_cuda_float4x4.h 11 140     # float4x4, determinant, transpose, inverse
+  rng types/_cuda_float4x4.h 142 167    # matrixMultiply
+  rng types/_cuda_float4x4.h 183 198    # matrixTransform (both forms)
+  rng types/_cuda_float4x4.h 323 350    # matrixRotationAxis
+  rng types/_cuda_float4x4.h 398 426    # matrixPerspectiveFov, matrixLookAt
+  echo "namespace renderkit {"
+  echo "class CUDACamera { public: float3 center, dir, angle; float fov, ratio, zNearPlane, zFarPlane;"
+  echo "  float4x4 matView, matProj, matInvView, matInvProj; bool dirty; void update(); };"
+  rng CUDACamera.cpp 245 266            # CUDACamera::update
+  echo "}"
+  rng "$Z" 23 25      # textures
+  rng "$Z" 31 41      # EPSILON, CACHE_SIZE, block shape
+  rng "$Z" 47 71      # intersectRectRect, intersectTriPoint
+  rng "$Z" 77 225     # kernel_rasterizeMeshTree
+  cat "$SHIM/raster_epilogue.hpp"
+  echo "}"
+} | build_tu ref_raster
 
 L=kernels/CUDA_buildMeshTreeLBVH.cu
 {
@@ -145,6 +173,6 @@ I=kernels/CUDA_interpolateData.cu
   echo "}"
 } | build_tu ref_file
 
-g++ -shared -fPIC -o "$OUT/libref_cudart.so" "$OUT"/ref_lbvh.o "$OUT"/ref_boxes.o "$OUT"/ref_reorder.o "$OUT"/ref_trace.o "$OUT"/ref_rays.o "$OUT"/ref_interp.o "$OUT"/ref_file.o "$OUT"/ref_sah.o -lpthread
+g++ -shared -fPIC -o "$OUT/libref_cudart.so" "$OUT"/ref_lbvh.o "$OUT"/ref_boxes.o "$OUT"/ref_reorder.o "$OUT"/ref_trace.o "$OUT"/ref_rays.o "$OUT"/ref_interp.o "$OUT"/ref_file.o "$OUT"/ref_sah.o "$OUT"/ref_raster.o -lpthread
 rm -f "$OUT"/*.o
 echo "built $OUT/libref_cudart.so"

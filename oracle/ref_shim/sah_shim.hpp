@@ -1,5 +1,6 @@
-// sah_shim.hpp -- thread emulation for the reference's SAH build kernel, whose
-// 32 threads per block cooperate through __syncthreads and __shared__ data.
+// sah_shim.hpp -- thread emulation for the reference's SAH build and raster
+// kernels, whose 32 threads per block cooperate through __syncthreads and
+// __shared__ data.
 // Each emulated block runs on 32 host threads (a persistent pool) that meet at
 // a barrier for every __syncthreads; blocks run one after another, which is
 // the serial execution of the reference's launches (the block that pops the
@@ -12,6 +13,10 @@
 #include <vector>
 
 #define __builtin_align__(a) __attribute__((aligned(a)))
+
+// internal linkage: every checker TU that includes this file gets its own
+// pool and barrier (inline members would otherwise merge across TUs)
+namespace {
 
 struct ShimBarrier {
   std::mutex m;
@@ -50,17 +55,18 @@ static inline int atomicSub(int* p, int v) {
 }
 
 // 32 persistent host threads that run one block of a kernel per round.
+// Thread t gets threadIdx (t % block_x, t / block_x).
 struct ShimBlockPool {
   static const int kThreads = 32;
   ShimBarrier start{kThreads + 1}, done{kThreads + 1}, sync{kThreads};
   std::function<void()> body;
   bool quit = false;
   std::vector<std::thread> workers;
-  ShimBlockPool() {
+  explicit ShimBlockPool(int block_x = kThreads) {
     g_block_sync = &sync;
     for (int t = 0; t < kThreads; ++t)
-      workers.emplace_back([this, t] {
-        threadIdx.x = (unsigned)t; threadIdx.y = 0; threadIdx.z = 0;
+      workers.emplace_back([this, t, block_x] {
+        threadIdx.x = (unsigned)(t % block_x); threadIdx.y = (unsigned)(t / block_x); threadIdx.z = 0;
         for (;;) {
           start.wait();
           if (quit) return;
@@ -81,3 +87,4 @@ struct ShimBlockPool {
     g_block_sync = nullptr;
   }
 };
+}  // namespace

@@ -588,6 +588,153 @@ OR_API int or_sah_build(const float* boxes_f, const float* root_box, u32* indice
 }
 
 // ---------------------------------------------------------------------------
+// Rasteriser (kernels/CUDA_rasterizeMeshTree.cu:47-225, camera matrices of
+// CUDACamera::update, CUDACamera.cpp:245-266, types/_cuda_float4x4.h).
+// Per pixel the faces are tested in face order and the first face with the
+// smallest depth t > 0 wins (strict <). The pixel point is the pixel's corner
+// (x * 2 / width - 1, 1 - y * 2 / height); a face is tested on the 8 x 4 pixel
+// zones of its screen rectangle (start rounded down to an even zone). Face id
+// out = the face's index (the reference writes the first index of the face's
+// 192-face cache block, see the callers).
+// ---------------------------------------------------------------------------
+namespace raster {
+struct M4 { F4 r0, r1, r2, r3; };
+static inline F4 row(const M4& m, int i) { return i == 0 ? m.r0 : (i == 1 ? m.r1 : (i == 2 ? m.r2 : m.r3)); }
+static M4 transpose(const M4& m) {
+  M4 r;
+  r.r0 = {m.r0.x, m.r1.x, m.r2.x, m.r3.x};
+  r.r1 = {m.r0.y, m.r1.y, m.r2.y, m.r3.y};
+  r.r2 = {m.r0.z, m.r1.z, m.r2.z, m.r3.z};
+  r.r3 = {m.r0.w, m.r1.w, m.r2.w, m.r3.w};
+  return r;
+}
+// r_ij = dot(a_i, column j of b)  (matrixMultiply)
+static M4 multiply(const M4& a, const M4& b) {
+  const M4 t = transpose(b);
+  M4 r;
+  F4* rr[4] = {&r.r0, &r.r1, &r.r2, &r.r3};
+  for (int i = 0; i < 4; ++i) {
+    const F4 ai = row(a, i);
+    *rr[i] = {dot4(ai, t.r0), dot4(ai, t.r1), dot4(ai, t.r2), dot4(ai, t.r3)};
+  }
+  return r;
+}
+static F4 transform(const M4& m, F4 v) { return {dot4(m.r0, v), dot4(m.r1, v), dot4(m.r2, v), dot4(m.r3, v)}; }
+// (int) inside a kernel: toward zero, saturating, NaN -> 0
+static inline int f2i(float x) {
+  if (x != x) return 0;
+  if (x >= 2147483648.0f) return 2147483647;
+  if (x <= -2147483648.0f) return (int)0x80000000u;
+  return (int)x;
+}
+}  // namespace raster
+
+// transpose(view * proj) for a camera at center3 looking along dir3 (the
+// normalized lookAt direction), roll angle3[2], fov / ratio; near 1.0, far 1999.999.
+OR_API void or_raster_matrix(const float* center3, const float* dir3, const float* angle3, float fov, float ratio, float* out16) {
+  using namespace raster;
+  const float cx = center3[0], cy = center3[1], cz = center3[2];
+  const float dx = dir3[0], dy = dir3[1], dz = dir3[2];
+  // target = center + 4999.999 dir; normal = (dir.x, 0, dir.y) (CUDACamera.cpp:247-248)
+  const float tx = cx + dx * 4999.999f, ty = cy + dy * 4999.999f, tz = cz + dz * 4999.999f;
+  float nx = dx, ny = 0.0f, nz = dy;
+  const float ninv = 1.0f / sqrtf(nx * nx + ny * ny + nz * nz);
+  nx = nx * ninv; ny = ny * ninv; nz = nz * ninv;
+  // matrixRotationAxis(normal, angle.z) (types/_cuda_float4x4.h:323-350)
+  const float u = cosf(angle3[2]), v = sinf(angle3[2]), w = 1.0f - u;
+  M4 up_m;
+  up_m.r0 = {w * nx * nx + u, w * nx * ny - v * nz, w * nx * nz + v * ny, 0.0f};
+  up_m.r1 = {w * ny * nx + v * nz, w * ny * ny + u, w * ny * nz - v * nx, 0.0f};
+  up_m.r2 = {w * nz * nx - v * ny, w * nz * ny + v * nx, w * nz * nz + u, 0.0f};
+  up_m.r3 = {0.0f, 0.0f, 0.0f, 1.0f};
+  const F4 eye = {cx, cy, cz, 0.0f}, at = {tx, ty, tz, 0.0f};
+  const F4 up = transform(up_m, {0.0f, 1.0f, 0.0f, 1.0f});
+  // matrixLookAt (:412-426)
+  const F4 za = normalize4(f4sub(at, eye));
+  const F4 xa = normalize4(cross4(up, za));
+  const F4 ya = cross4(za, xa);
+  const float xf = -dot4(xa, eye), yf = -dot4(ya, eye), zf = -dot4(za, eye);
+  M4 view;
+  view.r0 = {xa.x, ya.x, za.x, 0.0f};
+  view.r1 = {xa.y, ya.y, za.y, 0.0f};
+  view.r2 = {xa.z, ya.z, za.z, 0.0f};
+  view.r3 = {xf, yf, zf, 1.0f};
+  // matrixPerspectiveFov (:398-410)
+  const float z_near = 1.000f, z_far = 1999.999f;
+  const float ys = 1.0f / tanf(fov * 0.5f);
+  const float xs = ys / ratio;
+  const float zfac = z_far / (z_far - z_near);
+  const float wfac = -z_near * zfac;
+  M4 proj;
+  proj.r0 = {xs, 0.0f, 0.0f, 0.0f};
+  proj.r1 = {0.0f, ys, 0.0f, 0.0f};
+  proj.r2 = {0.0f, 0.0f, zfac, 1.0f};
+  proj.r3 = {0.0f, 0.0f, wfac, 0.0f};
+  const M4 m = transpose(multiply(view, proj));
+  memcpy(out16, &m, 64);
+}
+
+// faces_id / coords / depths are read (the caller clears them) and updated.
+OR_API void or_rasterize(const float* vertices, const u32* faces, u32 face_count, const float* matrix16, int width, int height,
+                         u32* faces_id, float* coords, float* depths) {
+  using namespace raster;
+  M4 m;
+  memcpy(&m, matrix16, 64);
+  const F4* vtx = (const F4*)vertices;
+  const U4* fc = (const U4*)faces;
+  const int zcx = 1 + (width - 1) / 8, zcy = 1 + (height - 1) / 4;
+  const float zsx = 0.5f * (float)zcx, zsy = 0.5f * (float)zcy;
+  const float eps = 0.000001f;
+  for (u32 f = 0; f < face_count; ++f) {
+    F4 p[3];
+    F4 mn = {kHuge, kHuge, kHuge, kHuge}, mx = {-kHuge, -kHuge, -kHuge, -kHuge};
+    const u32 vid[3] = {fc[f].x, fc[f].y, fc[f].z};
+    for (int k = 0; k < 3; ++k) {
+      F4 vi = vtx[vid[k]];
+      vi.w = 1.0f;
+      F4 vo = transform(m, vi);
+      const float inv = 1.0f / fabsf(vo.w);  // operator/= multiplies by the reciprocal
+      vo = f4scale(vo, inv);
+      vo.w = 0.0f;
+      p[k] = vo;
+      mn = {fminf(mn.x, vo.x), fminf(mn.y, vo.y), fminf(mn.z, vo.z), fminf(mn.w, vo.w)};
+      mx = {fmaxf(mx.x, vo.x), fmaxf(mx.y, vo.y), fmaxf(mx.z, vo.z), fmaxf(mx.w, vo.w)};
+    }
+    if (!(mn.x < 1.0f && mx.x > -1.0f && mn.y < 1.0f && mx.y > -1.0f)) continue;
+    int x0 = f2i(zsx * (mn.x + 1.0f)); x0 = (x0 > 0 ? x0 : 0) / 2 * 2;
+    int y0 = f2i(zsy * (1.0f - mx.y)); y0 = (y0 > 0 ? y0 : 0) / 2 * 2;
+    int x1 = f2i(zsx * (mx.x + 1.0f)); x1 = x1 < zcx - 1 ? x1 : zcx - 1;
+    int y1 = f2i(zsy * (1.0f - mn.y)); y1 = y1 < zcy - 1 ? y1 : zcy - 1;
+    const F4 a = p[0], b = p[1], c = p[2];
+    for (int j = y0; j <= y1; ++j)
+      for (int i = x0; i <= x1; ++i)
+        for (int ty = 0; ty < 4; ++ty)
+          for (int tx = 0; tx < 8; ++tx) {
+            const int x = i * 8 + tx, y = j * 4 + ty;
+            const float px = (float)x * 2.0f / (float)width - 1.0f;
+            const float py = 1.0f - (float)y * 2.0f / (float)height;
+            // intersectTriPoint (:52-71)
+            const float det = (b.x - a.x) * (c.y - a.y) - (c.x - a.x) * (b.y - a.y);
+            if (det > -eps && det < eps) continue;
+            const float inv_det = 1.0f / det;
+            const float uu = ((c.x - px) * (a.y - py) - (a.x - px) * (c.y - py)) * inv_det;
+            if (uu < 0.0f || uu > 1.0f) continue;
+            const float vv = ((a.x - px) * (b.y - py) - (b.x - px) * (a.y - py)) * inv_det;
+            if (vv < 0.0f || uu + vv > 1.0f) continue;
+            const float t = (1.0f - uu - vv) * a.z + uu * b.z + vv * c.z;
+            if (x < 0 || x >= width || y < 0 || y >= height) continue;
+            const long l = (long)y * width + x;
+            if (t > 0 && t < depths[l]) {
+              faces_id[l] = f;
+              coords[2 * l] = uu;
+              coords[2 * l + 1] = vv;
+              depths[l] = t;
+            }
+          }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Camera and primary rays.
 // lookAt / angleFromDir: CUDACamera.cpp:126-132, 70-88 (float3 normalize uses the
 // host rsqrtf = 1/sqrtf). Basis and per-pixel directions:
