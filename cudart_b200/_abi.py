@@ -33,6 +33,8 @@ EXPORTS = (
 )
 # every symbol include/rt_sah.h declares
 SAH_EXPORTS = ("rt_sah_sizes", "rt_sah_build")
+# every symbol include/rt_raster.h declares
+RASTER_EXPORTS = ("rt_raster_matrix", "rt_raster_scratch_bytes", "rt_rasterize")
 # every symbol include/rt_propose.h declares
 PROPOSE_EXPORTS = (
     "rt_propose_abi_version", "rt_gemm_bf16", "rt_gemm_argmax_bf16", "rt_ray_features", "rt_softmax_xent", "rt_transpose_bf16",
@@ -109,6 +111,12 @@ class SahDesc(C.Structure):
                 ("accel_bytes", C.c_size_t), ("info", _P), ("scratch", _P), ("scratch_bytes", C.c_size_t)]
 
 
+class RasterDesc(C.Structure):
+    _fields_ = [("vertices", _P), ("vertex_count", _U32), ("faces", _P), ("face_count", _U32), ("matrix", C.c_float * 16),
+                ("width", _U32), ("height", _U32), ("id_mode", _U32), ("face_id", _P), ("uv", _P), ("depth", _P), ("pair_capacity", _U32),
+                ("scratch", _P), ("scratch_bytes", C.c_size_t), ("error_word", _P)]
+
+
 class GemmDesc(C.Structure):
     _fields_ = [("a", _P), ("lda", _U32), ("b", _P), ("ldb", _U32), ("m", _U32), ("n", _U32), ("k", _U32), ("alpha", C.c_float),
                 ("bias", _P), ("relu", _U32), ("mask", _P), ("ldmask", _U32), ("c_f32", _P), ("ldc_f32", _U32), ("c_bf16", _P),
@@ -180,6 +188,11 @@ def lib():
         L.rt_sah_sizes.argtypes = [_U32, _U32, C.POINTER(C.c_size_t), C.POINTER(_U32)]
         L.rt_sah_build.argtypes = [C.POINTER(SahDesc), _P]
         for name in SAH_EXPORTS:
+            getattr(L, name).restype = C.c_int
+        L.rt_raster_matrix.argtypes = [C.POINTER(Camera), C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.rt_raster_scratch_bytes.argtypes = [_U32, _U32, _U32, _U32, C.POINTER(C.c_size_t)]
+        L.rt_rasterize.argtypes = [C.POINTER(RasterDesc), _P]
+        for name in RASTER_EXPORTS:
             getattr(L, name).restype = C.c_int
         L.rt_gemm_bf16.argtypes = [C.POINTER(GemmDesc), _P]
         L.rt_gemm_argmax_bf16.argtypes = [C.POINTER(GemmArgmaxDesc), _P]

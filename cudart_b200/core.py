@@ -220,6 +220,41 @@ def build_sah(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, lbvh_dep
     return out
 
 
+def raster_matrix(cam: _abi.Camera, target) -> list:
+    """transpose(view * proj) of CUDACamera::update for a camera looking at `target`."""
+    t = (C.c_float * 3)(*[float(x) for x in target])
+    m = (C.c_float * 16)()
+    _abi.check("rt_raster_matrix", _abi.lib().rt_raster_matrix(C.byref(cam), t, m))
+    return list(m)
+
+
+def rasterize(vertices: torch.Tensor, faces: torch.Tensor, matrix, width: int, height: int, id_mode: int = 0, out: dict | None = None,
+              pair_capacity: int = 0, stream=None) -> dict:
+    """CUDARaytracer::rasterizeMeshTree into the surfaces of `out` (created cleared as
+    CUDABuffer::clearOutputSurfaces leaves them: id 0, uv 0, depth +HUGE)."""
+    _need_cuda(vertices, "vertices", _F32, 4)
+    _need_cuda(faces, "faces", _I32, 4)
+    P = width * height
+    dev = vertices.device
+    if out is None:
+        out = dict(id=torch.zeros(P, dtype=torch.int32, device=dev), uv=torch.zeros((P, 2), dtype=torch.float32, device=dev),
+                   depth=torch.full((P,), HUGE, dtype=torch.float32, device=dev), err=torch.zeros(1, dtype=torch.int32, device=dev))
+    nb = C.c_size_t(0)
+    _abi.check("rt_raster_scratch_bytes", _abi.lib().rt_raster_scratch_bytes(faces.shape[0], width, height, pair_capacity, C.byref(nb)))
+    scratch = _SCRATCH.get(nb.value, dev)
+    d = _abi.RasterDesc()
+    d.vertices, d.vertex_count, d.faces, d.face_count = vertices.data_ptr(), vertices.shape[0], faces.data_ptr(), faces.shape[0]
+    for i in range(16):
+        d.matrix[i] = float(matrix[i])
+    d.width, d.height, d.id_mode, d.pair_capacity = width, height, id_mode, pair_capacity
+    d.face_id, d.uv, d.depth = out["id"].data_ptr(), out["uv"].data_ptr(), out["depth"].data_ptr()
+    d.scratch, d.scratch_bytes = scratch.data_ptr(), scratch.numel()
+    if "err" in out:
+        d.error_word = out["err"].data_ptr()
+    _abi.check("rt_rasterize", _abi.lib().rt_rasterize(C.byref(d), _stream(stream)))
+    return out
+
+
 def trace(tree: Tree, orig: torch.Tensor, dir: torch.Tensor, tmax: torch.Tensor | None = None, id_mode: int = 0,
           counters: bool = False, use_tris: bool = True, vertices: torch.Tensor | None = None, out: dict | None = None,
           ray_count: int | None = None, use_accel: bool = True, schedule: dict | None = None, stream=None) -> dict:

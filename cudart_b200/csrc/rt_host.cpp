@@ -8,6 +8,7 @@
 #include <string.h>
 
 #include "../../include/rt_core.h"
+#include "../../include/rt_raster.h"
 
 namespace {
 
@@ -60,6 +61,46 @@ extern "C" rt_status rt_camera_basis(const rt_camera* cam, uint32_t width, uint3
   memcpy(basis + 4, &rayDir, 16);
   memcpy(basis + 8, &rayX, 16);
   memcpy(basis + 12, &rayY, 16);
+  return RT_OK;
+}
+
+// transpose(view * proj) of CUDACamera::update (CUDACamera.cpp:245-266) with the
+// float4x4 helpers of types/_cuda_float4x4.h (rotation about an axis :323-350,
+// perspective :398-410, lookAt :412-426, multiply :142-167): 4-wide dot
+// products summed left to right, normalize = v * (1 / sqrtf(dot(v, v))).
+extern "C" rt_status rt_raster_matrix(const rt_camera* cam, const float target[3], float m[16]) {
+  if (!cam || !target || !m) return RT_ERR_INVALID_ARGUMENT;
+  // CUDACamera::lookAt / angleFromDir: dir = normalize(target - center)
+  float dx = target[0] - cam->center[0], dy = target[1] - cam->center[1], dz = target[2] - cam->center[2];
+  const float dinv = 1.0f / sqrtf(dx * dx + dy * dy + dz * dz);
+  dx = dx * dinv; dy = dy * dinv; dz = dz * dinv;
+  const V4 eye = {cam->center[0], cam->center[1], cam->center[2], 0.0f};
+  const V4 at = {cam->center[0] + dx * 4999.999f, cam->center[1] + dy * 4999.999f, cam->center[2] + dz * 4999.999f, 0.0f};
+  float nx = dx, ny = 0.0f, nz = dy;  // the reference's roll axis (dir.x, 0, dir.y)
+  const float ninv = 1.0f / sqrtf(nx * nx + ny * ny + nz * nz);
+  nx = nx * ninv; ny = ny * ninv; nz = nz * ninv;
+  const float u = cosf(cam->angle[2]), v = sinf(cam->angle[2]), w = 1.0f - u;
+  const V4 r0 = {w * nx * nx + u, w * nx * ny - v * nz, w * nx * nz + v * ny, 0.0f};
+  const V4 r1 = {w * ny * nx + v * nz, w * ny * ny + u, w * ny * nz - v * nx, 0.0f};
+  const V4 r2 = {w * nz * nx - v * ny, w * nz * ny + v * nx, w * nz * nz + u, 0.0f};
+  const V4 r3 = {0.0f, 0.0f, 0.0f, 1.0f};
+  const V4 up0 = {0.0f, 1.0f, 0.0f, 1.0f};
+  const V4 up = {dot(r0, up0), dot(r1, up0), dot(r2, up0), dot(r3, up0)};
+  const V4 za = normalize({at.x - eye.x, at.y - eye.y, at.z - eye.z, at.w - eye.w});
+  const V4 xa = normalize(cross(up, za));
+  const V4 ya = cross(za, xa);
+  const V4 view[4] = {{xa.x, ya.x, za.x, 0.0f}, {xa.y, ya.y, za.y, 0.0f}, {xa.z, ya.z, za.z, 0.0f},
+                      {-dot(xa, eye), -dot(ya, eye), -dot(za, eye), 1.0f}};
+  const float zn = 1.000f, zf = 1999.999f;  // CUDACamera.cpp:34-35
+  const float ys = 1.0f / tanf(cam->fov * 0.5f);
+  const float xs = ys / cam->ratio;
+  const float zfac = zf / (zf - zn);
+  const float wfac = -zn * zfac;
+  // columns of proj (rows of its transpose)
+  const V4 pc[4] = {{xs, 0.0f, 0.0f, 0.0f}, {0.0f, ys, 0.0f, 0.0f}, {0.0f, 0.0f, zfac, wfac}, {0.0f, 0.0f, 1.0f, 0.0f}};
+  // (view * proj)_ij = dot(view_i, proj column j); the kernel's matrix is its transpose
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) m[4 * j + i] = dot(view[i], pc[j]);
   return RT_OK;
 }
 

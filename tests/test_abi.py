@@ -31,6 +31,10 @@ def test_header_declarations_are_exported():
     for name in proposal:
         assert hasattr(lib, name), name
     assert set(proposal) == set(_abi.PROPOSE_EXPORTS)
+    raster = _declared("rt_raster.h")
+    assert set(raster) == set(_abi.RASTER_EXPORTS)
+    for name in raster:
+        assert hasattr(lib, name), name
     sah = _declared("rt_sah.h")
     assert set(sah) == set(_abi.SAH_EXPORTS)
     for name in sah:

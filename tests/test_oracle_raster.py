@@ -71,3 +71,18 @@ def test_raster_depth_order(oracle):
     dup = np.array(near + near, np.uint32)
     fid, _, dep = oracle.rasterize(v, dup, m, 64, 64)
     assert set(np.unique(fid[dep != oracle.HUGE])) <= {0, 1}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_host_raster_matrix_matches_oracle(oracle, case):
+    """rt_raster_matrix (host code of the C ABI, no device needed) equals the oracle bit for bit."""
+    from cudart_b200 import core
+    mesh, center, target, w, h = CASES[case]()
+    fov = float(np.float32(np.pi / 3))
+    ratio = float(np.float32(w) / np.float32(h))
+    roll = 0.3 if case == "terrain_roll" else 0.0
+    d, angle = _camera(oracle, center, target, fov, ratio, roll=roll)
+    cam = core.make_camera(center, target, fov=fov, ratio=ratio)
+    cam.angle[2] = roll
+    m = np.array(core.raster_matrix(cam, target), np.float32)
+    assert np.array_equal(m.view(np.uint32), oracle.raster_matrix(center, d, angle, fov, ratio).view(np.uint32))
