@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=1, help="also time the batched workload (1024 meshes, CUDA graph)")
     ap.add_argument("--learned", type=int, default=1, help="also train and time the learned subtree proposal (4M-triangle scene)")
     ap.add_argument("--sah", type=int, default=1, help="also time the SAH and Hybrid builds and tracing through their trees")
+    ap.add_argument("--raster", type=int, default=1, help="also time the rasteriser on the same frame")
     ap.add_argument("--learned-scale", type=float, default=1.0, help="triangle-count scale of the learned-proposal scene")
     return ap.parse_args()
 
@@ -285,6 +286,8 @@ def run_ours(args, rank, world, local_rank):
         result["batch_c2"] = batched(args, dev, world)
     if args.sah:
         result["sah"] = sah_leg(args, dev, world, mesh, camera, W, H, tree)
+    if args.raster:
+        result["raster"] = raster_leg(dev, world, cam, tree, v, W, H)
     if args.learned:
         result["nn_proposal_c3"] = learned(args, dev, world)
     clocks = clk.summary()
@@ -422,6 +425,57 @@ def batched(args, dev, world, count=1024):
            "device_errors": int((info[:, 7] != 0).sum()), "graph": "build + trace captured in one CUDA graph"}
     del graph
     return res
+
+
+def raster_leg(dev, world, cam, tree, verts, W, H):
+    """The rasteriser on the same 2^20-face soup (faces in the build's position
+    order) and a W x H frame, beside the primary-ray trace of the same view.
+    The camera is moved off the z axis: the reference's view matrix is NaN for
+    a camera looking exactly along z. CUDA events, L2 flushed, surfaces cleared
+    (as CUDABuffer::clearOutputSurfaces) before each run."""
+    import torch
+
+    from cudart_b200 import core
+
+    center = (cam.center[0] + 0.05, cam.center[1] + 0.1, cam.center[2])
+    camera = core.make_camera(center, cam.target, fov=cam.fov, ratio=cam.ratio)
+    m = core.raster_matrix(camera, cam.target)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    P = W * H
+    out = dict(id=torch.zeros(P, dtype=torch.int32, device=dev), uv=torch.zeros((P, 2), dtype=torch.float32, device=dev),
+               depth=torch.full((P,), 3.402823466e38, dtype=torch.float32, device=dev), err=torch.zeros(1, dtype=torch.int32, device=dev))
+    faces = tree.faces
+    ms = []
+    for rep in range(6):
+        out["id"].zero_()
+        out["uv"].zero_()
+        out["depth"].fill_(3.402823466e38)
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        core.rasterize(verts, faces, m, W, H, out=out)
+        e1.record()
+        torch.cuda.synchronize()
+        if rep:
+            ms.append(e0.elapsed_time(e1))
+    o, d = core.primary_rays(camera, W, H)
+    core.trace(tree, o, d)
+    torch.cuda.synchronize()
+    tms = []
+    for rep in range(4):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        core.trace(tree, o, d)
+        e1.record()
+        torch.cuda.synchronize()
+        tms.append(e0.elapsed_time(e1))
+    r = statistics.median(ms)
+    covered = float((out["depth"] < 3.4e38).float().mean().item())
+    del flush
+    return {"width": W, "height": H, "faces": int(faces.shape[0]), "raster_ms": round(r, 4),
+            "raster_mpix_s": round(world * W * H / (r * 1e-3) / 1e6, 2), "covered_fraction": round(covered, 4),
+            "trace_primary_ms_same_view": round(statistics.median(tms), 4), "device_errors": int(out["err"].item())}
 
 
 def sah_leg(args, dev, world, mesh, camera, W, H, lbvh_tree):

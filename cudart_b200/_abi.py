@@ -34,7 +34,7 @@ EXPORTS = (
 # every symbol include/rt_sah.h declares
 SAH_EXPORTS = ("rt_sah_sizes", "rt_sah_build")
 # every symbol include/rt_raster.h declares
-RASTER_EXPORTS = ("rt_raster_matrix", "rt_raster_scratch_bytes", "rt_rasterize")
+RASTER_EXPORTS = ("rt_camera_view_dir", "rt_raster_matrix", "rt_raster_scratch_bytes", "rt_rasterize")
 # every symbol include/rt_propose.h declares
 PROPOSE_EXPORTS = (
     "rt_propose_abi_version", "rt_gemm_bf16", "rt_gemm_argmax_bf16", "rt_ray_features", "rt_softmax_xent", "rt_transpose_bf16",
@@ -190,6 +190,7 @@ def lib():
         for name in SAH_EXPORTS:
             getattr(L, name).restype = C.c_int
         L.rt_raster_matrix.argtypes = [C.POINTER(Camera), C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.rt_camera_view_dir.argtypes = [C.POINTER(Camera), C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.rt_raster_scratch_bytes.argtypes = [_U32, _U32, _U32, _U32, C.POINTER(C.c_size_t)]
         L.rt_rasterize.argtypes = [C.POINTER(RasterDesc), _P]
         for name in RASTER_EXPORTS:

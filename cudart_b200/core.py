@@ -221,10 +221,12 @@ def build_sah(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, lbvh_dep
 
 
 def raster_matrix(cam: _abi.Camera, target) -> list:
-    """transpose(view * proj) of CUDACamera::update for a camera looking at `target`."""
+    """transpose(view * proj) of CUDACamera::update for a camera that looked at `target`."""
     t = (C.c_float * 3)(*[float(x) for x in target])
+    d = (C.c_float * 3)()
+    _abi.check("rt_camera_view_dir", _abi.lib().rt_camera_view_dir(C.byref(cam), t, d))
     m = (C.c_float * 16)()
-    _abi.check("rt_raster_matrix", _abi.lib().rt_raster_matrix(C.byref(cam), t, m))
+    _abi.check("rt_raster_matrix", _abi.lib().rt_raster_matrix(C.byref(cam), d, m))
     return list(m)
 
 

@@ -68,12 +68,17 @@ extern "C" rt_status rt_camera_basis(const rt_camera* cam, uint32_t width, uint3
 // float4x4 helpers of types/_cuda_float4x4.h (rotation about an axis :323-350,
 // perspective :398-410, lookAt :412-426, multiply :142-167): 4-wide dot
 // products summed left to right, normalize = v * (1 / sqrtf(dot(v, v))).
-extern "C" rt_status rt_raster_matrix(const rt_camera* cam, const float target[3], float m[16]) {
-  if (!cam || !target || !m) return RT_ERR_INVALID_ARGUMENT;
-  // CUDACamera::lookAt / angleFromDir: dir = normalize(target - center)
-  float dx = target[0] - cam->center[0], dy = target[1] - cam->center[1], dz = target[2] - cam->center[2];
-  const float dinv = 1.0f / sqrtf(dx * dx + dy * dy + dz * dz);
-  dx = dx * dinv; dy = dy * dinv; dz = dz * dinv;
+extern "C" rt_status rt_camera_view_dir(const rt_camera* cam, const float target[3], float dir[3]) {
+  if (!cam || !target || !dir) return RT_ERR_INVALID_ARGUMENT;
+  const float dx = target[0] - cam->center[0], dy = target[1] - cam->center[1], dz = target[2] - cam->center[2];
+  const float inv = 1.0f / sqrtf(dx * dx + dy * dy + dz * dz);
+  dir[0] = dx * inv; dir[1] = dy * inv; dir[2] = dz * inv;
+  return RT_OK;
+}
+
+extern "C" rt_status rt_raster_matrix(const rt_camera* cam, const float dir[3], float m[16]) {
+  if (!cam || !dir || !m) return RT_ERR_INVALID_ARGUMENT;
+  const float dx = dir[0], dy = dir[1], dz = dir[2];
   const V4 eye = {cam->center[0], cam->center[1], cam->center[2], 0.0f};
   const V4 at = {cam->center[0] + dx * 4999.999f, cam->center[1] + dy * 4999.999f, cam->center[2] + dz * 4999.999f, 0.0f};
   float nx = dx, ny = 0.0f, nz = dy;  // the reference's roll axis (dir.x, 0, dir.y)

@@ -4,15 +4,17 @@
 // Same class and method names, argument meanings and defaults as the
 // reference (namespace renderkit):
 //   CUDAMesh           CUDAMesh.h:20-155       (device vertices/faces + hit box)
-//   CUDAMeshTree       CUDAMeshTree.h:22-164   (nodes, boxes, indices; buildMeshTreeLBVH)
+//   CUDAMeshTree       CUDAMeshTree.h:22-164   (nodes, boxes, indices; buildMeshTreeLBVH,
+//                                               buildMeshTreeSAH, buildMeshTreeHybrid)
 //   CUDACamera         CUDACamera.h:15-321     (center, angles, fov, ratio; lookAt)
 //   CUDABuffer         CUDABuffer.h:17-206     (ray in/out surfaces; clearOutputSurfaces)
 //   CUDARaytracer      CUDARaytracer.h:58-209  (headless: setBuffer/setCamera,
-//                                               calcPrimaryRays, raytraceMeshTree)
+//                                               calcPrimaryRays, raytraceMeshTree,
+//                                               rasterizeMeshTree)
 // and the free functions the reference's kernels export (CUDA_radixSortGeneral,
 // CUDA_radixSort, CUDA_bubbleSort512, CUDA_bitonicSort, CUDA_bitonicSortGeneral,
 // CUDA_calcMeshBoxes, CUDA_reorderMeshFaces, CUDA_buildMeshTreeLBVH,
-// CUDA_calcPrimaryRays, CUDA_raytraceMeshTree).
+// CUDA_calcPrimaryRays, CUDA_raytraceMeshTree, CUDA_rasterizeMeshTree).
 //
 // Error behaviour follows the reference's _assert (CUDACommon.h:123-133): a
 // failing call prints the file, line and message and exits, except that this
@@ -20,17 +22,23 @@
 // as the reference's did (cudaThreadSynchronize after each launch).
 // Differences: faces_id of a miss is 0xFFFFFFFF instead of an uninitialised
 // value; the LBVH build keeps the pre-gathered triangle stream and traversal
-// blob on the tree so that raytraceMeshTree uses the fast traversal.
+// blob on the tree so that raytraceMeshTree uses the fast traversal; the
+// rasteriser writes each pixel's face index (the reference writes the first
+// index of the face's 192-face block); buildMeshTreeSAH always builds from the
+// mesh (the reference refines the leaves of a tree that already has nodes).
 #pragma once
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
 
 #include "../rt_core.h"
+#include "../rt_raster.h"
+#include "../rt_sah.h"
 
 namespace renderkit {
 
@@ -121,6 +129,10 @@ class CUDAMeshTree {
 
   // CUDAMeshTree.cpp:88-91 -> CUDA_buildMeshTreeLBVH(mesh, this, true, tree_depth)
   void buildMeshTreeLBVH(uint tree_depth = 12);
+  // CUDAMeshTree.cpp:93-96 -> CUDA_buildMeshTreeSAH(mesh, this)
+  void buildMeshTreeSAH();
+  // CUDAMeshTree.cpp:98-103: LBVH of lbvh_tree_depth levels without leaf splitting, then SAH in every leaf
+  void buildMeshTreeHybrid(uint lbvh_tree_depth = 12);
 
   void updateNodes(bvnode* nodes_buffer, uint node_count) {  // CUDAMeshTree.cpp:105-112
     delete nodes;
@@ -134,6 +146,7 @@ class CUDAMeshTree {
 
  private:
   friend void CUDA_buildMeshTreeLBVH(CUDAMesh*, CUDAMeshTree*, bool, uint);
+  friend void rk_build_sah(CUDAMesh*, CUDAMeshTree*, uint);
   CUDAMesh* mesh;
   CUDAArray<bvnode>* nodes = nullptr;
   CUDAArray<aabox>* boxes = nullptr;
@@ -188,6 +201,55 @@ inline void CUDA_buildMeshTreeLBVH(CUDAMesh* mesh, CUDAMeshTree* tree, bool tree
 
 inline void CUDAMeshTree::buildMeshTreeLBVH(uint tree_depth) { CUDA_buildMeshTreeLBVH(mesh, this, true, tree_depth); }
 
+// SAH (lbvh_depth 0) or Hybrid build through rt_sah_build; faces reordered in
+// the mesh as the reference's CUDA_reorderMeshFaces call leaves them (:777-784).
+inline void rk_build_sah(CUDAMesh* mesh, CUDAMeshTree* tree, uint lbvh_depth) {
+  rk_check_abi();
+  const uint n = mesh->getFaceCount();
+  size_t scratch_bytes = 0, accel_bytes = 0;
+  uint32_t max_nodes = 0;
+  RK_OK(rt_sah_sizes(n, lbvh_depth, &scratch_bytes, &max_nodes));
+  RK_OK(rt_lbvh_accel_bytes(n, &accel_bytes));
+  CUDAArray<unsigned char> scratch(scratch_bytes);
+  CUDAArray<bvnode> nodes_buffer(max_nodes);
+  CUDAArray<uint4> faces_out(n);
+  CUDAArray<rt_build_info> info(1);
+  delete tree->tris; tree->tris = new CUDAArray<float4>(3 * (size_t)n);
+  delete tree->accel; tree->accel = new CUDAArray<unsigned char>(accel_bytes);
+  aabox hb = mesh->getHitbox();
+  rt_sah_desc d = {};
+  d.vertices = (const float*)mesh->getVerticesArray()->getPointer();
+  d.vertex_count = mesh->getVertexCount();
+  d.face_count = n;
+  d.faces_in = (const uint32_t*)mesh->getFacesArray()->getPointer();
+  d.faces_out = (uint32_t*)faces_out.getPointer();
+  d.hitbox = (const float*)&hb;
+  d.lbvh_depth = lbvh_depth;
+  d.boxes = (float*)tree->boxes->getPointer();
+  d.indices = tree->indices->getPointer();
+  d.nodes = (uint32_t*)nodes_buffer.getPointer();
+  d.max_nodes = max_nodes;
+  d.tris = (float*)tree->tris->getPointer();
+  d.accel = tree->accel->getPointer();
+  d.accel_bytes = accel_bytes;
+  d.info = info.getPointer();
+  d.scratch = scratch.getPointer();
+  d.scratch_bytes = scratch_bytes;
+  RK_OK(rt_sah_build(&d, nullptr));
+  rt_build_info h;
+  info.copyDataToHost(&h);
+  RK_CHECK(h.error == 0, "CUDA_buildMeshTreeSAH() : device error");
+  RK_CHECK(cudaMemcpy(mesh->getFacesArray()->getPointer(), faces_out.getPointer(), (size_t)n * 16, cudaMemcpyDeviceToDevice) == cudaSuccess,
+           "CUDA_buildMeshTreeSAH() : face reorder");
+  tree->real_depth = h.real_depth;
+  tree->updateNodes(nodes_buffer.getPointer(), h.node_count);
+}
+
+// kernels/CUDA_buildMeshTreeSAH.cu:672
+inline void CUDA_buildMeshTreeSAH(CUDAMesh* mesh, CUDAMeshTree* tree) { rk_build_sah(mesh, tree, 0); }
+inline void CUDAMeshTree::buildMeshTreeSAH() { rk_build_sah(mesh, this, 0); }
+inline void CUDAMeshTree::buildMeshTreeHybrid(uint lbvh_tree_depth) { rk_build_sah(mesh, this, lbvh_tree_depth); }
+
 // ---------------------------------------------------------------------------
 class CUDACamera {
  public:
@@ -199,9 +261,18 @@ class CUDACamera {
   }
   void setCenter(float x, float y, float z) { cam_.center[0] = x; cam_.center[1] = y; cam_.center[2] = z; }
   float3 getCenter() const { return make_float3(cam_.center[0], cam_.center[1], cam_.center[2]); }
-  void setAngle(float x, float y, float z) { cam_.angle[0] = x; cam_.angle[1] = y; cam_.angle[2] = z; }
+  void setAngle(float x, float y, float z) {  // CUDACamera.cpp:108-115
+    cam_.angle[0] = x; cam_.angle[1] = y; cam_.angle[2] = z;
+    dirFromAngle();
+  }
   float3 getAngle() const { return make_float3(cam_.angle[0], cam_.angle[1], cam_.angle[2]); }
-  void lookAt(float x, float y, float z) { float t[3] = {x, y, z}; RK_OK(rt_camera_look_at(&cam_, t)); }
+  void lookAt(float x, float y, float z) {  // CUDACamera.cpp:126-132
+    float t[3] = {x, y, z};
+    RK_OK(rt_camera_view_dir(&cam_, t, dir_));
+    RK_OK(rt_camera_look_at(&cam_, t));
+  }
+  float3 getDir() const { return make_float3(dir_[0], dir_[1], dir_[2]); }
+  const float* dirPtr() const { return dir_; }
   void setFOV(float fov) { cam_.fov = fov; }
   float getFOV() const { return cam_.fov; }
   void setRatio(float ratio) { cam_.ratio = ratio; }
@@ -213,7 +284,20 @@ class CUDACamera {
   const rt_camera* raw() const { return &cam_; }
 
  private:
+  // CUDACamera.cpp:55-68: wrap / clamp the angles, dir = normalize(cos p cos y, sin y, sin p cos y)
+  void dirFromAngle() {
+    const float pi = 3.14159265359f;
+    float* a = cam_.angle;
+    if (a[0] < 0.0f) a[0] += pi * 2.0f;
+    if (a[0] > pi * 2.0f) a[0] -= pi * 2.0f;
+    if (a[1] < -pi * 0.5f + 0.001f) a[1] = -pi * 0.5f + 0.001f;
+    if (a[1] > pi * 0.5f - 0.001f) a[1] = pi * 0.5f - 0.001f;
+    const float dx = cosf(a[0]) * cosf(a[1]), dy = sinf(a[1]), dz = sinf(a[0]) * cosf(a[1]);
+    const float inv = 1.0f / sqrtf(dx * dx + dy * dy + dz * dz);
+    dir_[0] = dx * inv; dir_[1] = dy * inv; dir_[2] = dz * inv;
+  }
   rt_camera cam_;
+  float dir_[3] = {0.0f, 0.0f, 1.0f};  // CUDACamera.cpp:45-47
 };
 
 // ---------------------------------------------------------------------------
@@ -277,6 +361,32 @@ inline void CUDA_raytraceMeshTree(CUDABuffer* buffer, CUDAMesh* mesh, CUDAMeshTr
   RK_CHECK(cudaDeviceSynchronize() == cudaSuccess, "CUDA_raytraceMeshTree() : Unable to execute CUDA kernel.");
 }
 
+// kernels/CUDA_rasterizeMeshTree.cu:255. faces_id is the face's index in the
+// mesh's (current) face order.
+inline void CUDA_rasterizeMeshTree(CUDABuffer* buffer, CUDACamera* camera, CUDAMesh* mesh, CUDAMeshTree* tree) {
+  rk_check_abi();
+  (void)tree;
+  rt_raster_desc d = {};
+  RK_OK(rt_raster_matrix(camera->raw(), camera->dirPtr(), d.matrix));
+  d.vertices = (const float*)mesh->getVerticesArray()->getPointer();
+  d.vertex_count = mesh->getVertexCount();
+  d.faces = (const uint32_t*)mesh->getFacesArray()->getPointer();
+  d.face_count = mesh->getFaceCount();
+  d.width = (uint32_t)buffer->getWidth();
+  d.height = (uint32_t)buffer->getHeight();
+  d.id_mode = 0;
+  d.face_id = (int32_t*)buffer->out_faces_id.getPointer();
+  d.uv = (float*)buffer->out_coords.getPointer();
+  d.depth = buffer->out_depths.getPointer();
+  size_t bytes = 0;
+  RK_OK(rt_raster_scratch_bytes(d.face_count, d.width, d.height, 0, &bytes));
+  CUDAArray<unsigned char> scratch(bytes);
+  d.scratch = scratch.getPointer();
+  d.scratch_bytes = bytes;
+  RK_OK(rt_rasterize(&d, nullptr));
+  RK_CHECK(cudaDeviceSynchronize() == cudaSuccess, "CUDA_rasterizeMeshTree() : Unable to execute CUDA kernel.");
+}
+
 class CUDARaytracer {
  public:
   void setBuffer(CUDABuffer* buffer) { current_buffer = buffer; }
@@ -287,6 +397,10 @@ class CUDARaytracer {
   void raytraceMeshTree(CUDAMesh* mesh, CUDAMeshTree* tree, bool coherency = true) {  // CUDARaytracer.cpp:130-135
     if (mesh->getVertexCount() == 0) return;
     CUDA_raytraceMeshTree(current_buffer, mesh, tree, coherency);
+  }
+  void rasterizeMeshTree(CUDAMesh* mesh, CUDAMeshTree* tree) {  // CUDARaytracer.cpp:137-142
+    if (mesh->getVertexCount() == 0) return;
+    CUDA_rasterizeMeshTree(current_buffer, current_camera, mesh, tree);
   }
 
  private:

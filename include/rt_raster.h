@@ -21,12 +21,16 @@
 extern "C" {
 #endif
 
+/* HOST. The camera's view direction after CUDACamera::lookAt(target)
+ * (CUDACamera.cpp:126-132, angleFromDir :70-72): (target - center) * (1 / sqrtf(|.|^2)). */
+rt_status rt_camera_view_dir(const rt_camera* camera, const float target[3], float dir[3]);
 /* HOST. transpose(view * proj) as CUDACamera::update (CUDACamera.cpp:245-266)
- * builds it for a camera at camera->center looking at `target` (CUDACamera::
- * lookAt's normalized direction), roll camera->angle[2], camera->fov /
- * ratio, near plane 1.0, far plane 1999.999. A camera looking exactly along z
- * gets a NaN matrix, as in the reference (its roll axis (dir.x, 0, dir.y) is zero). */
-rt_status rt_raster_matrix(const rt_camera* camera, const float target[3], float matrix[16]);
+ * builds it for a camera at camera->center with view direction `dir`
+ * (CUDACamera::dir: rt_camera_view_dir after a lookAt), roll camera->angle[2],
+ * camera->fov / ratio, near plane 1.0, far plane 1999.999. A camera looking
+ * exactly along z gets a NaN matrix, as in the reference (its roll axis
+ * (dir.x, 0, dir.y) is zero). */
+rt_status rt_raster_matrix(const rt_camera* camera, const float dir[3], float matrix[16]);
 
 typedef struct rt_raster_desc {
   const float* vertices; /* float4 per vertex */

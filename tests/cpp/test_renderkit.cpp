@@ -2,13 +2,16 @@
 // the way the reference's samples drive CUDAMeshTree / CUDARaytracer
 // (samples/02_how_to_use_the_raytracer.cpp:67-85,178-194) and its sorter
 // (samples/09_how_to_use_a_sorter.cpp): build, camera lookAt, primary rays,
-// trace, radix sort. Reads a scene file, writes the results for
-// tests/test_gpu_renderkit.py to compare with the CPU oracle.
+// trace, radix sort; then SAH and Hybrid builds of fresh copies of the mesh and
+// the rasteriser on the LBVH-ordered mesh. Reads a scene file, writes the
+// results for tests/test_gpu_renderkit.py to compare with the CPU oracle.
 //
 // in : u32 V, N, W, H, tree_depth, K; f32 center[3], target[3], fov, ratio, hitbox[8];
 //      float4 vertices[V]; uint4 faces[N]; u32 keys[K]
 // out: u32 node_count, real_depth; bvnode nodes[node_count]; uint4 faces[N] (reordered);
-//      u32 faces_id[W*H]; f32 depths[W*H]; float2 coords[W*H]; u32 keys[K]; u32 indices[K]
+//      u32 faces_id[W*H]; f32 depths[W*H]; float2 coords[W*H]; u32 keys[K]; u32 indices[K];
+//      then for SAH and Hybrid(8): u32 node_count; bvnode nodes[]; uint4 faces[N];
+//      then the raster surfaces: u32 faces_id[W*H]; f32 depths[W*H]; float2 coords[W*H]
 #include <cstdio>
 #include <vector>
 
@@ -38,6 +41,7 @@ int main(int argc, char** argv) {
   aabox hitbox;
   hitbox.min = make_float4(hb[0], hb[1], hb[2], hb[3]);
   hitbox.max = make_float4(hb[4], hb[5], hb[6], hb[7]);
+  const std::vector<uint4> faces0 = faces;
   CUDAMesh mesh(verts.data(), V, faces.data(), N, hitbox);
   CUDAMeshTree tree(&mesh);
   tree.buildMeshTreeLBVH(depth);
@@ -80,6 +84,26 @@ int main(int argc, char** argv) {
   wr(out, nodes.data(), nc); wr(out, faces.data(), N);
   wr(out, ids.data(), R); wr(out, depths.data(), R); wr(out, coords.data(), R);
   wr(out, sk.data(), K); wr(out, si.data(), K);
+
+  for (int hybrid = 0; hybrid < 2; ++hybrid) {
+    CUDAMesh m2(verts.data(), V, faces0.data(), N, hitbox);
+    CUDAMeshTree t2(&m2);
+    if (hybrid) t2.buildMeshTreeHybrid(8);
+    else t2.buildMeshTreeSAH();
+    const uint32_t n2 = t2.getNodeCount();
+    std::vector<bvnode> nodes2(n2);
+    std::vector<uint4> faces2(N);
+    t2.getNodesArray()->copyDataToHost(nodes2.data());
+    m2.getFacesArray()->copyDataToHost(faces2.data());
+    wr(out, &n2, 1); wr(out, nodes2.data(), n2); wr(out, faces2.data(), N);
+  }
+
+  buffer.clearOutputSurfaces();
+  raytracer.rasterizeMeshTree(&mesh, &tree);
+  buffer.out_faces_id.copyDataToHost(ids.data());
+  buffer.out_depths.copyDataToHost(depths.data());
+  buffer.out_coords.copyDataToHost(coords.data());
+  wr(out, ids.data(), R); wr(out, depths.data(), R); wr(out, coords.data(), R);
   fclose(out);
   std::printf("renderkit ok: %u faces, %u nodes, depth %u\n", N, nc, rd_);
   return 0;

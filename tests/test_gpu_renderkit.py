@@ -67,3 +67,23 @@ def test_renderkit_dropin(oracle, tmp_path, scene):
     assert np.array_equal(coords.view(np.uint32), e["uv"].view(np.uint32))
     ek, ev = oracle.sort_pairs(keys, None, 32, init_vals=True)
     assert np.array_equal(sk, ek) and np.array_equal(si, ev)
+
+    for depth in (None, 8):  # buildMeshTreeSAH, buildMeshTreeHybrid(8)
+        n2 = int(take(np.uint32, 1)[0])
+        nodes2 = take(np.uint32, 8 * n2).reshape(n2, 8)
+        faces2 = take(np.uint32, 4 * mesh.face_count).reshape(-1, 4)
+        o2 = oracle.sah_build(mesh.vertices, mesh.faces, hit, hybrid_depth=depth)
+        assert np.array_equal(nodes2, o2["nodes"].view(np.uint32))
+        assert np.array_equal(faces2, o2["faces"])
+
+    rid, rdep = take(np.uint32, R), take(np.float32, R)
+    ruv = take(np.float32, 2 * R).reshape(R, 2)
+    ang = oracle.camera_look_at(cam.center, cam.target)
+    m = oracle.raster_matrix(cam.center, oracle.look_dir(cam.center, cam.target), np.array([ang[0], ang[1], 0], np.float32),
+                             cam.fov, cam.ratio)
+    fo, uo, do = oracle.rasterize(mesh.vertices, ref["faces"], m, cam.width, cam.height)
+    assert np.array_equal(rdep.view(np.uint32), do.view(np.uint32))
+    assert np.array_equal(ruv.view(np.uint32), uo.view(np.uint32))
+    assert np.array_equal(rid, fo)
+    if scene == "terrain":
+        assert (do != oracle.HUGE).mean() > 0.1
