@@ -1,0 +1,108 @@
+"""Small, self-contained workloads for profiling one kernel at a time (the
+commands recorded in profiles/*.md run these).
+
+    python -m cudart_b200.profile_cases <case>
+
+Each case builds its inputs, runs the operation once untimed (warm-up), then
+once more; a profiler capturing the last launch of the named kernel sees a
+steady-state launch. Cases (kernel of interest in brackets):
+
+  trace_primary  2^20-face soup, 1920x1080 primary rays, tuned tile schedule   [k_trace_accel]
+  trace_bounce   the same scene's diffuse bounces, cooperative schedule          [k_trace_coop]
+  mlp_propose    proposal network inference on 2^18 rays (4096 slots)            [k_gemm_argmax_tc, k_gemm_tc]
+  mlp_train      one training step, batch 8192                                   [k_gemm_tc, k_softmax_xent]
+  sah_build      SAH build of the 2^20-face soup                                 [k_sah_small, k_huge_bins, k_sah_big]
+  raster         rasteriser, 2^20-face soup, 1920x1080                           [k_raster_zones, k_raster_emit]
+"""
+from __future__ import annotations
+
+import sys
+
+import numpy as np
+import torch
+
+
+def _soup_scene():
+    from . import core, scenes
+    mesh, cam = scenes.soup_1m_scene()
+    v = torch.from_numpy(mesh.vertices).cuda()
+    f = torch.from_numpy(mesh.faces.view(np.int32)).cuda()
+    return mesh, cam, v, f, core.build_lbvh(v, f)
+
+
+def trace_primary():
+    from . import core
+    mesh, cam, v, f, tree = _soup_scene()
+    c = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
+    o, d = core.primary_rays(c, cam.width, cam.height)
+    sch = dict(image_width=cam.width, while_while=True)
+    for _ in range(2):
+        core.trace(tree, o, d, schedule=sch)
+    torch.cuda.synchronize()
+
+
+def trace_bounce():
+    from . import core
+    mesh, cam, v, f, tree = _soup_scene()
+    c = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
+    o, d = core.primary_rays(c, cam.width, cam.height)
+    h = core.trace(tree, o, d)
+    b = core.bounce_rays(tree.tris, o, d, h["id"], h["t"], 1234)
+    for _ in range(2):
+        core.trace(tree, b[0], b[1], tmax=b[2], schedule=dict(coop=True, sorted=True))
+    torch.cuda.synchronize()
+
+
+def mlp_propose():
+    from . import proposal, scenes
+    box = (-1.5, -0.6, -1.5, 1.5, 1.4, 1.5)
+    o, d = scenes.box_rays_torch(1 << 18, box, seed=1)
+    net = proposal.ProposalNet(seed=0)
+    for _ in range(2):
+        net.propose(o, d, box)
+    torch.cuda.synchronize()
+
+
+def mlp_train():
+    from . import proposal, scenes
+    box = (-1.5, -0.6, -1.5, 1.5, 1.4, 1.5)
+    B = 8192
+    o, d = scenes.box_rays_torch(B, box, seed=1)
+    labels = torch.randint(0, 4096, (B,), dtype=torch.int32, device="cuda", generator=torch.Generator(device="cuda").manual_seed(2))
+    net = proposal.ProposalNet(seed=0)
+    for _ in range(2):
+        net.train_step(o, d, labels, box)
+    torch.cuda.synchronize()
+
+
+def sah_build():
+    from . import core, scenes
+    mesh = scenes.soup(1 << 20, 1)
+    v = torch.from_numpy(mesh.vertices).cuda()
+    f = torch.from_numpy(mesh.faces.view(np.int32)).cuda()
+    t = core.build_sah(v, f)
+    core.build_sah(v, f, out=t)
+    torch.cuda.synchronize()
+
+
+def raster():
+    from . import core, scenes
+    mesh, cam = scenes.soup_1m_scene()
+    v = torch.from_numpy(mesh.vertices).cuda()
+    f = torch.from_numpy(mesh.faces.view(np.int32)).cuda()
+    c = core.make_camera((cam.center[0] + 0.05, cam.center[1] + 0.1, cam.center[2]), cam.target, fov=cam.fov, ratio=cam.ratio)
+    m = core.raster_matrix(c, cam.target)
+    for _ in range(2):
+        core.rasterize(v, f, m, cam.width, cam.height)
+    torch.cuda.synchronize()
+
+
+CASES = {"trace_primary": trace_primary, "trace_bounce": trace_bounce, "mlp_propose": mlp_propose, "mlp_train": mlp_train,
+         "sah_build": sah_build, "raster": raster}
+
+if __name__ == "__main__":
+    if len(sys.argv) != 2 or sys.argv[1] not in CASES:
+        raise SystemExit("usage: python -m cudart_b200.profile_cases {" + ",".join(CASES) + "}")
+    torch.cuda.set_device(0)
+    CASES[sys.argv[1]]()
+    print("ok", sys.argv[1])
