@@ -23,6 +23,7 @@ DEVERR_WAIT_TIMEOUT = 0x8
 PROPOSE_ABI_VERSION = 1  # RT_PROPOSE_ABI_VERSION of include/rt_propose.h
 TRACE_WHILE_WHILE = 0x1
 TRACE_COOP = 0x2
+TRACE_WIDE = 0x4
 
 # every symbol include/rt_core.h declares
 EXPORTS = (

@@ -730,6 +730,8 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
     RT_CHECK_LAUNCH();
     if (accel) {
       k_accel_nodes<<<sms * 4, 256, 0, st>>>(d->nodes, L.hdr, L.leaf_lambda, AL.tnodes, AL.hdr);
+      k_wide_nodes<<<sms * 4, 256, 0, st>>>(AL.tnodes, AL.hdr, AL.wide);
+      note_launch();
       note_launch();
       RT_CHECK_LAUNCH();
     }

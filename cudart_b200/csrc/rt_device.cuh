@@ -142,18 +142,69 @@ __device__ __forceinline__ void accel_node(const uint32_t* __restrict__ nodes, c
 
 // Traversal blob: header (256 B), internal-node records (64 B, <= N - 1),
 // leaf table (16 B, <= N), group boxes (32 B, <= N/8 + N).
+// Single-mesh blobs also hold 4-wide records (128 B, <= N - 1), see wide_node.
 struct AccelLayout {
   uint32_t* hdr;
   float4* tnodes;
   uint4* leaves;
   float4* groups;
+  float4* wide;
 };
 inline size_t carve_accel(Carve& c, AccelLayout& A, uint32_t n) {
   A.hdr = c.take<uint32_t>(64);
   A.tnodes = c.take<float4>(4 * (size_t)n);
   A.leaves = c.take<uint4>(n);
   A.groups = c.take<float4>(2 * ((size_t)n / 8 + n + 1));
+  A.wide = c.take<float4>(8 * (size_t)n);
   return c.off + 256;
+}
+
+// 4-wide record of binary record r: r's two children, each internal child
+// replaced by that child's two children (their padded boxes come from the
+// child's own record). Layout (8 x float4): min x / y / z of the 4 children,
+// max x / y / z, child references (as in the two-child records; kNoChild for an
+// unused slot), and one spare. Every record gets one; a walk that starts at
+// the root only reaches those of even depth.
+constexpr uint32_t kNoChild = 0x7FFFFFFEu;
+__device__ __forceinline__ void wide_node(const float4* __restrict__ tnodes, float4* __restrict__ wide, uint32_t r) {
+  const float4* rec = tnodes + 4 * (size_t)r;
+  float mnx[4] = {0.f, 0.f, 0.f, 0.f}, mny[4] = {0.f, 0.f, 0.f, 0.f}, mnz[4] = {0.f, 0.f, 0.f, 0.f};
+  float mxx[4] = {0.f, 0.f, 0.f, 0.f}, mxy[4] = {0.f, 0.f, 0.f, 0.f}, mxz[4] = {0.f, 0.f, 0.f, 0.f};
+  uint32_t ref[4] = {kNoChild, kNoChild, kNoChild, kNoChild};
+  int k = 0;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const float4 a0 = rec[2 * side], a1 = rec[2 * side + 1];
+    const uint32_t c = __float_as_uint(a0.w);
+    if (c & 0x80000000u) {
+      mnx[k] = a0.x; mny[k] = a0.y; mnz[k] = a0.z; mxx[k] = a1.x; mxy[k] = a1.y; mxz[k] = a1.z; ref[k] = c;
+      ++k;
+    } else {
+      const float4* cr = tnodes + 4 * (size_t)c;
+#pragma unroll
+      for (int s2 = 0; s2 < 2; ++s2) {
+        const float4 b0 = cr[2 * s2], b1 = cr[2 * s2 + 1];
+        mnx[k] = b0.x; mny[k] = b0.y; mnz[k] = b0.z; mxx[k] = b1.x; mxy[k] = b1.y; mxz[k] = b1.z; ref[k] = __float_as_uint(b0.w);
+        ++k;
+      }
+    }
+  }
+  float4* w = wide + 8 * (size_t)r;
+  w[0] = make_float4(mnx[0], mnx[1], mnx[2], mnx[3]);
+  w[1] = make_float4(mny[0], mny[1], mny[2], mny[3]);
+  w[2] = make_float4(mnz[0], mnz[1], mnz[2], mnz[3]);
+  w[3] = make_float4(mxx[0], mxx[1], mxx[2], mxx[3]);
+  w[4] = make_float4(mxy[0], mxy[1], mxy[2], mxy[3]);
+  w[5] = make_float4(mxz[0], mxz[1], mxz[2], mxz[3]);
+  w[6] = make_float4(__uint_as_float(ref[0]), __uint_as_float(ref[1]), __uint_as_float(ref[2]), __uint_as_float(ref[3]));
+  w[7] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+// All records of a blob whose header holds the leaf count (hdr[1]).
+static __global__ __launch_bounds__(256) void k_wide_nodes(const float4* __restrict__ tnodes, const uint32_t* __restrict__ acc_hdr,
+                                                    float4* __restrict__ wide) {
+  const uint32_t leaves = acc_hdr[1];
+  const uint32_t records = leaves ? leaves - 1 : 0;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < records; r += gridDim.x * blockDim.x) wide_node(tnodes, wide, r);
 }
 
 constexpr int kStack = 64;
@@ -206,6 +257,38 @@ __device__ __forceinline__ bool slab2(const float4& mn, const float4& mx, const 
   tn = fmax_sel(fmax_sel(fmin_sel(t0x, t1x), fmin_sel(t0y, t1y)), fmin_sel(t0z, t1z));
   const float tf = fmin_sel(fmin_sel(fmax_sel(t0x, t1x), fmax_sel(t0y, t1y)), fmax_sel(t0z, t1z));
   return tn <= tf && tf >= 0.0f && tn <= tbest * kCullSlack;
+}
+
+// One 4-wide record against a ray: entry distance of every child the ray
+// enters within reach (+inf otherwise), children sorted nearest first
+// (5-comparator network), references alongside.
+__device__ __forceinline__ float f4c(const float4& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
+__device__ __forceinline__ uint32_t u4c(const uint4& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
+__device__ __forceinline__ void cswap_tr(float (&t)[4], uint32_t (&r)[4], int a, int b) {
+  if (t[b] < t[a]) {
+    const float tt = t[a]; t[a] = t[b]; t[b] = tt;
+    const uint32_t rr = r[a]; r[a] = r[b]; r[b] = rr;
+  }
+}
+__device__ __forceinline__ void wide_test(const float4* __restrict__ wn, const float4& o, float ix, float iy, float iz, float tbest,
+                                          uint32_t skip, float (&t)[4], uint32_t (&r)[4]) {
+  const float4 w0 = ldg4(wn), w1 = ldg4(wn + 1), w2 = ldg4(wn + 2), w3 = ldg4(wn + 3), w4 = ldg4(wn + 4), w5 = ldg4(wn + 5);
+  const uint4 wr = ldg4((const uint4*)(wn + 6));
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t rk = u4c(wr, k);
+    float tn;
+    const bool h = rk != kNoChild && rk != skip &&
+                   slab2(make_float4(f4c(w0, k), f4c(w1, k), f4c(w2, k), 0.0f), make_float4(f4c(w3, k), f4c(w4, k), f4c(w5, k), 0.0f), o,
+                         ix, iy, iz, tbest, tn);
+    t[k] = h ? tn : INFINITY;
+    r[k] = rk;
+  }
+  cswap_tr(t, r, 0, 1);
+  cswap_tr(t, r, 2, 3);
+  cswap_tr(t, r, 0, 2);
+  cswap_tr(t, r, 1, 3);
+  cswap_tr(t, r, 1, 2);
 }
 
 // ---------------------------------------------------------------------------

@@ -1105,6 +1105,8 @@ extern "C" rt_status rt_sah_build(const rt_sah_desc* d, rt_stream stream) {
     k_sah_accel<<<(uint32_t)hmin<uint64_t>((node_count + 255) / 256, (uint64_t)sms * 8), 256, 0, st>>>(d->nodes, node_count, leaf_total,
                                                                                                         L.leaf_lambda, AL.tnodes, AL.hdr);
     note_launch();
+    k_wide_nodes<<<(uint32_t)hmin<uint64_t>((node_count + 255) / 256, (uint64_t)sms * 8), 256, 0, st>>>(AL.tnodes, AL.hdr, AL.wide);
+    note_launch();
   }
   k_sah_info<<<1, 1, 0, st>>>(d->info, node_count, L.scalars + 5, levels, L.err, L.counts);
   note_launch();

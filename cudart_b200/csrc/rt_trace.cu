@@ -128,6 +128,7 @@ struct AccelArgs {
   const uint4* leaves;
   const float4* groups;
   const uint32_t* hdr;
+  const float4* wide;  // 4-wide records (single-mesh blobs)
 };
 
 // One ray through the blob. kWW: "while-while" schedule (descend internal
@@ -178,7 +179,7 @@ __device__ __forceinline__ bool seed_start(uint32_t r, const SeedArgs& S, const 
   return true;
 }
 
-template <bool kCount, bool kWW, bool kSeed = false>
+template <bool kCount, bool kWW, bool kSeed = false, bool kWide = false>
 __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArgs& A, const AccelArgs& C,
                                                 const SeedArgs& S = SeedArgs{}) {
   const float4 o = ldg4(A.orig + r), d = ldg4(A.dir + r);
@@ -214,6 +215,33 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
     while (alive) {
       // descend internal nodes (kWW: until this ray holds a leaf)
       while (!(ref & 0x80000000u)) {
+        if constexpr (kWide) {
+          // 4-wide record: up to four children tested at once, nearest first
+          float wt[4];
+          uint32_t wr[4];
+          wide_test(C.wide + 8 * (size_t)ref, o, ix, iy, iz, bt, (kSeed && phase) ? skip : kNoSkip, wt, wr);
+          if (kCount) visits += 4;
+          if (wt[0] == INFINITY) {
+            if (!next()) {
+              alive = false;
+              break;
+            }
+          } else {
+#pragma unroll
+            for (int k = 3; k >= 1; --k) {
+              if (wt[k] != INFINITY) {
+                if (sp < kStack) {
+                  st_ref[sp] = wr[k];
+                  st_t[sp] = wt[k];
+                  ++sp;
+                } else if (A.err) {
+                  atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
+                }
+              }
+            }
+            ref = wr[0];
+          }
+        } else {
         const float4* tn = C.tnodes + 4 * (size_t)ref;
         const float4 a0 = ldg4(tn), a1 = ldg4(tn + 1), b0 = ldg4(tn + 2), b1 = ldg4(tn + 3);
         if (kCount) visits += 2;
@@ -242,6 +270,7 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
         } else if (!next()) {
           alive = false;
           break;
+        }
         }
         if (!kWW && (ref & 0x80000000u)) break;
       }
@@ -301,7 +330,7 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
 // are written by the lane whose key is the minimum right after its merge.
 constexpr int kCoopWarps = 4;  // 128-thread CTAs
 
-template <bool kCount, bool kSeed = false>
+template <bool kCount, bool kSeed = false, bool kWide = false>
 __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool valid, const TraceArgs& A, const AccelArgs& C,
                                                 unsigned long long* s_key, float2* s_uv, const SeedArgs& S = SeedArgs{}) {
   const uint32_t lane = lane_id();
@@ -343,6 +372,33 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
     bool has_leaf = false;
     if (alive) {
       while (!(ref & 0x80000000u)) {
+        if constexpr (kWide) {
+          // 4-wide record: up to four children tested at once, nearest first
+          float wt[4];
+          uint32_t wr[4];
+          wide_test(C.wide + 8 * (size_t)ref, o, ix, iy, iz, bt, (kSeed && phase) ? skip : kNoSkip, wt, wr);
+          if (kCount) visits += 4;
+          if (wt[0] == INFINITY) {
+            if (!next()) {
+              alive = false;
+              break;
+            }
+          } else {
+#pragma unroll
+            for (int k = 3; k >= 1; --k) {
+              if (wt[k] != INFINITY) {
+                if (sp < kStack) {
+                  st_ref[sp] = wr[k];
+                  st_t[sp] = wt[k];
+                  ++sp;
+                } else if (A.err) {
+                  atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
+                }
+              }
+            }
+            ref = wr[0];
+          }
+        } else {
         const float4* tn = C.tnodes + 4 * (size_t)ref;
         const float4 a0 = ldg4(tn), a1 = ldg4(tn + 1), b0 = ldg4(tn + 2), b1 = ldg4(tn + 3);
         if (kCount) visits += 2;
@@ -371,6 +427,7 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
         } else if (!next()) {
           alive = false;
           break;
+        }
         }
       }
       has_leaf = alive;
@@ -527,14 +584,14 @@ struct SlotMap {
   }
 };
 
-template <bool kCount, bool kWW, bool kSeed>
+template <bool kCount, bool kWW, bool kSeed, bool kWide>
 __global__ __launch_bounds__(128) void k_trace_accel(TraceArgs A, AccelArgs C, SlotMap M, SeedArgs S) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t r;
-  if (s < M.slots && M.ray_of(s, r)) trace_ray_accel<kCount, kWW, kSeed>(r, A, C, S);
+  if (s < M.slots && M.ray_of(s, r)) trace_ray_accel<kCount, kWW, kSeed, kWide>(r, A, C, S);
 }
 
-template <bool kCount, bool kSeed>
+template <bool kCount, bool kSeed, bool kWide>
 __global__ __launch_bounds__(128) void k_trace_coop(TraceArgs A, AccelArgs C, SlotMap M, SeedArgs S) {
   __shared__ unsigned long long s_key[kCoopWarps][32];
   __shared__ float2 s_uv[kCoopWarps][32];
@@ -542,10 +599,10 @@ __global__ __launch_bounds__(128) void k_trace_coop(TraceArgs A, AccelArgs C, Sl
   uint32_t r = 0;
   const bool valid = s < M.slots && M.ray_of(s, r);
   const uint32_t w = threadIdx.x >> 5;
-  trace_warp_coop<kCount, kSeed>(r, valid, A, C, s_key[w], s_uv[w], S);
+  trace_warp_coop<kCount, kSeed, kWide>(r, valid, A, C, s_key[w], s_uv[w], S);
 }
 
-template <bool kCount, bool kSeed>
+template <bool kCount, bool kSeed, bool kWide>
 __global__ __launch_bounds__(128) void k_trace_coop_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter, SeedArgs S) {
   __shared__ unsigned long long s_key[kCoopWarps][32];
   __shared__ float2 s_uv[kCoopWarps][32];
@@ -558,13 +615,13 @@ __global__ __launch_bounds__(128) void k_trace_coop_persistent(TraceArgs A, Acce
     uint32_t r = 0;
     const uint32_t s = base + lane;
     const bool valid = s < M.slots && M.ray_of(s, r);
-    trace_warp_coop<kCount, kSeed>(r, valid, A, C, s_key[w], s_uv[w], S);
+    trace_warp_coop<kCount, kSeed, kWide>(r, valid, A, C, s_key[w], s_uv[w], S);
   }
 }
 
 // Persistent warps: each warp takes 32 slots at a time from a global counter
 // until the slots run out (the counter is zeroed before the launch).
-template <bool kCount, bool kWW, bool kSeed>
+template <bool kCount, bool kWW, bool kSeed, bool kWide>
 __global__ __launch_bounds__(128) void k_trace_accel_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter, SeedArgs S) {
   const uint32_t lane = lane_id();
   for (;;) {
@@ -574,7 +631,7 @@ __global__ __launch_bounds__(128) void k_trace_accel_persistent(TraceArgs A, Acc
     if (base >= M.slots) break;
     uint32_t r;
     const uint32_t s = base + lane;
-    if (s < M.slots && M.ray_of(s, r)) trace_ray_accel<kCount, kWW, kSeed>(r, A, C, S);
+    if (s < M.slots && M.ray_of(s, r)) trace_ray_accel<kCount, kWW, kSeed, kWide>(r, A, C, S);
   }
 }
 
@@ -728,17 +785,18 @@ extern "C" rt_status rt_device_check(void) {
 namespace {
 
 // Blob traversal launch for every schedule of rt_trace_desc.
-template <bool kSeed>
-rt_status launch_accel(const rt_trace_desc* d, const TraceArgs& A, const SeedArgs& S, cudaStream_t st) {
+template <bool kSeed, bool kWide>
+rt_status launch_accel_w(const rt_trace_desc* d, const TraceArgs& A, const SeedArgs& S, cudaStream_t st) {
   const bool count = d->ray_visits || d->ray_tests;
-  // blob layout of rt_lbvh_build: header (256 B), records, leaf table, group boxes
+  // blob layout of rt_lbvh_build / rt_sah_build
   const size_t n = d->face_count_hint;
   AccelArgs C;
-  Carve c((void*)d->accel, ~(size_t)0);
-  C.hdr = c.take<uint32_t>(64);
-  C.tnodes = c.take<float4>(4 * n);
-  C.leaves = c.take<uint4>(n);
-  C.groups = c.take<float4>(2 * (n / 8 + n + 1));
+  {
+    Carve c((void*)d->accel, ~(size_t)0);
+    AccelLayout AL;
+    carve_accel(c, AL, (uint32_t)n);
+    C.hdr = AL.hdr; C.tnodes = AL.tnodes; C.leaves = AL.leaves; C.groups = AL.groups; C.wide = AL.wide;
+  }
   SlotMap M;
   M.order = d->ray_order;
   const uint32_t R = d->ray_count;
@@ -758,19 +816,19 @@ rt_status launch_accel(const rt_trace_desc* d, const TraceArgs& A, const SeedArg
   if (d->work_counter && cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
   if (d->schedule & RT_TRACE_COOP) {
     if (d->work_counter) {
-      if (count) k_trace_coop_persistent<true, kSeed><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter, S);
-      else k_trace_coop_persistent<false, kSeed><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter, S);
+      if (count) k_trace_coop_persistent<true, kSeed, kWide><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter, S);
+      else k_trace_coop_persistent<false, kSeed, kWide><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter, S);
     } else {
-      if (count) k_trace_coop<true, kSeed><<<sblocks, 128, 0, st>>>(A, C, M, S);
-      else k_trace_coop<false, kSeed><<<sblocks, 128, 0, st>>>(A, C, M, S);
+      if (count) k_trace_coop<true, kSeed, kWide><<<sblocks, 128, 0, st>>>(A, C, M, S);
+      else k_trace_coop<false, kSeed, kWide><<<sblocks, 128, 0, st>>>(A, C, M, S);
     }
   } else if (d->work_counter) {
-#define RT_LAUNCH_P(CNT, WW) k_trace_accel_persistent<CNT, WW, kSeed><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter, S)
+#define RT_LAUNCH_P(CNT, WW) k_trace_accel_persistent<CNT, WW, kSeed, kWide><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter, S)
     if (count) { if (ww) RT_LAUNCH_P(true, true); else RT_LAUNCH_P(true, false); }
     else { if (ww) RT_LAUNCH_P(false, true); else RT_LAUNCH_P(false, false); }
 #undef RT_LAUNCH_P
   } else {
-#define RT_LAUNCH_S(CNT, WW) k_trace_accel<CNT, WW, kSeed><<<sblocks, 128, 0, st>>>(A, C, M, S)
+#define RT_LAUNCH_S(CNT, WW) k_trace_accel<CNT, WW, kSeed, kWide><<<sblocks, 128, 0, st>>>(A, C, M, S)
     if (count) { if (ww) RT_LAUNCH_S(true, true); else RT_LAUNCH_S(true, false); }
     else { if (ww) RT_LAUNCH_S(false, true); else RT_LAUNCH_S(false, false); }
 #undef RT_LAUNCH_S
@@ -778,6 +836,12 @@ rt_status launch_accel(const rt_trace_desc* d, const TraceArgs& A, const SeedArg
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
+}
+
+template <bool kSeed>
+rt_status launch_accel(const rt_trace_desc* d, const TraceArgs& A, const SeedArgs& S, cudaStream_t st) {
+  if (d->schedule & RT_TRACE_WIDE) return launch_accel_w<kSeed, true>(d, A, S, st);
+  return launch_accel_w<kSeed, false>(d, A, S, st);
 }
 
 rt_status trace_args(const rt_trace_desc* d, TraceArgs& A) {

@@ -39,6 +39,8 @@ def candidates(image_width: int):
         if srt and w:
             continue
         out.append({"image_width": w, "persistent": p, "blocks_per_sm": bps, "while_while": True, "sorted": srt, "coop": True})
+    # every schedule again with the 4-wide records
+    out += [dict(c, wide=True) for c in out]
     return out
 
 

@@ -257,6 +257,7 @@ typedef struct rt_trace_desc {
 
 #define RT_TRACE_WHILE_WHILE 0x1u /* descend until a leaf is held, then test it (else: interleaved) */
 #define RT_TRACE_COOP 0x2u        /* the warp's lanes share the triangle tests of all its rays' leaves */
+#define RT_TRACE_WIDE 0x4u /* descend through the blob's 4-wide records (single-mesh builds) */
 
 /* A tracing order for incoherent rays: ray indices sorted by direction octant,
  * then by the Morton code of the origin inside box (min xyz, max xyz, HOST);

@@ -205,7 +205,7 @@ def _seeded_equal(tree, o, d, prop, sl, schedule):
 
 
 SCHEDULES = [dict(), dict(while_while=True), dict(coop=True), dict(coop=True, sorted=True), dict(persistent=True, while_while=True),
-             dict(coop=True, persistent=True)]
+             dict(coop=True, persistent=True), dict(wide=True, while_while=True), dict(wide=True, coop=True, sorted=True)]
 
 
 @pytest.mark.parametrize("schedule", SCHEDULES)

@@ -77,7 +77,7 @@ def test_trace_through_sah_tree(depth):
     c = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
     o, d = core.primary_rays(c, cam.width, cam.height)
     want = core.trace(lb, o, d, id_mode=1)
-    for sch in (dict(), dict(coop=True), dict(image_width=cam.width, while_while=True)):
+    for sch in (dict(), dict(coop=True), dict(image_width=cam.width, while_while=True), dict(wide=True, coop=True)):
         got = core.trace(t, o, d, id_mode=1, schedule=sch)
         torch.cuda.synchronize()
         assert int(got["err"].item()) == 0
