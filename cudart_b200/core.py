@@ -110,8 +110,8 @@ class Tree:
         return self.nodes[: self.node_count].cpu()
 
 
-def lbvh_scratch_bytes(face_count: int, tree_depth=12, tree_complete=True, morton_bits=32):
-    params = _abi.BuildParams(tree_depth, int(tree_complete), 0, 0, morton_bits)
+def lbvh_scratch_bytes(face_count: int, tree_depth=12, tree_complete=True, morton_bits=32, min_leaf=0, max_leaf=0):
+    params = _abi.BuildParams(tree_depth, int(tree_complete), min_leaf, max_leaf, morton_bits)
     nb = C.c_size_t(0)
     mx = C.c_uint32(0)
     _abi.check("rt_lbvh_scratch_bytes", _abi.lib().rt_lbvh_scratch_bytes(face_count, C.byref(params), C.byref(nb), C.byref(mx)))
@@ -125,7 +125,8 @@ def accel_bytes(face_count: int) -> int:
 
 
 def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_depth: int = 12, tree_complete: bool = True,
-               morton_bits: int = 32, out: Tree | None = None, accel: bool = True, stream=None) -> Tree:
+               morton_bits: int = 32, out: Tree | None = None, accel: bool = True, min_leaf: int = 0, max_leaf: int = 0,
+               stream=None) -> Tree:
     """LBVH build of a mesh given as float4 vertices (V, 4) and uint4 faces (N, 4).
     hitbox: host sequence of 8 floats (min xyzw, max xyzw) or None for the
     vertices' min/max."""
@@ -133,7 +134,7 @@ def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_de
     _need_cuda(faces, "faces", _I32, 4)
     n = faces.shape[0]
     dev = vertices.device
-    nbytes, max_nodes = lbvh_scratch_bytes(n, tree_depth, tree_complete, morton_bits)
+    nbytes, max_nodes = lbvh_scratch_bytes(n, tree_depth, tree_complete, morton_bits, min_leaf, max_leaf)
     if out is None:
         out = Tree(
             nodes=torch.empty((max_nodes, 8), dtype=torch.int32, device=dev),
@@ -156,7 +157,7 @@ def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_de
     d.faces_in = faces.data_ptr()
     d.faces_out = out.faces.data_ptr()
     d.hitbox = C.cast(hb, C.c_void_p).value if hb is not None else None
-    d.params = _abi.BuildParams(tree_depth, int(tree_complete), 0, 0, morton_bits)
+    d.params = _abi.BuildParams(tree_depth, int(tree_complete), min_leaf, max_leaf, morton_bits)
     d.boxes = out.boxes.data_ptr()
     d.indices = out.indices.data_ptr()
     d.codes = out.codes.data_ptr()

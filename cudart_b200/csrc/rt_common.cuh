@@ -64,6 +64,10 @@ inline rt_status cuda_status(cudaError_t e) { return e == cudaSuccess ? RT_OK : 
 // rt_launch_count() so that a caller can count the kernels inside a timed region.
 void note_launch(uint32_t kernels = 1);
 
+// Exclusive scan of n words in place (rt_scan.cu); `sums` holds >= n / 1024 + 2
+// words; `total` (device, optional) receives the sum of all n words.
+void excl_scan(uint32_t* v, uint32_t n, uint32_t* sums, uint32_t* total, cudaStream_t st);
+
 // Radix sort internals shared by the build (rt_sort.cu).
 size_t radix_scratch_bytes(uint32_t n);
 rt_status radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t begin_bit, uint32_t end_bit, int init_vals,

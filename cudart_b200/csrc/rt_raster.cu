@@ -158,47 +158,6 @@ __global__ __launch_bounds__(256) void k_raster_zones(const float4* __restrict__
   }
 }
 
-// Exclusive scan of n words in place (block sums in `sums`, >= n / 1024 + 2 words).
-__global__ __launch_bounds__(256) void k_rs_blocks(uint32_t* v, uint32_t n, uint32_t* sums) {
-  __shared__ uint32_t s_w[8];
-  const uint32_t base = blockIdx.x * 1024u + threadIdx.x * 4u;
-  uint32_t a[4], t = 0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) { a[k] = base + k < n ? v[base + k] : 0u; t += a[k]; }
-  uint32_t total;
-  uint32_t ex = block_excl_scan_nt<256>(t, s_w, total);
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (base + k < n) v[base + k] = ex;
-    ex += a[k];
-  }
-  if (threadIdx.x == 0) sums[blockIdx.x] = total;
-}
-__global__ __launch_bounds__(1024) void k_rs_sums(uint32_t* sums, uint32_t nb) {
-  __shared__ uint32_t s_w[32];
-  __shared__ uint32_t s_carry;
-  if (threadIdx.x == 0) s_carry = 0;
-  __syncthreads();
-  for (uint32_t b0 = 0; b0 < nb; b0 += 1024) {
-    const uint32_t i = b0 + threadIdx.x;
-    const uint32_t x = i < nb ? sums[i] : 0u;
-    uint32_t total;
-    const uint32_t ex = block_excl_scan_nt<1024>(x, s_w, total);
-    const uint32_t carry = s_carry;
-    if (i < nb) sums[i] = carry + ex;
-    __syncthreads();
-    if (threadIdx.x == 0) s_carry = carry + total;
-    __syncthreads();
-  }
-}
-__global__ __launch_bounds__(256) void k_rs_add(uint32_t* v, uint32_t n, const uint32_t* sums) {
-  const uint32_t add = sums[blockIdx.x];
-  const uint32_t base = blockIdx.x * 1024u + threadIdx.x * 4u;
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-    if (base + k < n) v[base + k] += add;
-}
-
 int sm_count_r() {
   int dev = 0, n = 148;
   cudaGetDevice(&dev);
@@ -300,13 +259,10 @@ extern "C" rt_status rt_rasterize(const rt_raster_desc* d, rt_stream stream) {
     if (P == 0) continue;
     const uint32_t m = f1 - f0;
     if (cudaMemcpyAsync(L.off, L.cnt + f0, (size_t)m * 4, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return RT_ERR_CUDA;
-    const uint32_t sb = (m + 1023) / 1024;
-    k_rs_blocks<<<sb, 256, 0, st>>>(L.off, m, L.sums);
-    k_rs_sums<<<1, 1024, 0, st>>>(L.sums, sb);
-    k_rs_add<<<sb, 256, 0, st>>>(L.off, m, L.sums);
+    excl_scan(L.off, m, L.sums, nullptr, st);
     k_raster_emit<<<(uint32_t)hmin<uint64_t>((m + 255) / 256, (uint64_t)sms * 8), 256, 0, st>>>(L.rect, L.cnt, L.off, f0, f1, Z.zcx, L.keys,
                                                                                               L.vals);
-    note_launch(4);
+    note_launch();
     RT_CHECK_LAUNCH();
     uint32_t bits = 1;
     while (bits < 32 && (1ull << bits) < nz) ++bits;
