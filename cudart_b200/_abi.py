@@ -20,7 +20,7 @@ DEVERR_NODE_CAPACITY = 0x1
 DEVERR_STACK_OVERFLOW = 0x2
 DEVERR_MORTON_CAPACITY = 0x4
 DEVERR_WAIT_TIMEOUT = 0x8
-PROPOSE_ABI_VERSION = 1  # RT_PROPOSE_ABI_VERSION of include/rt_propose.h
+PROPOSE_ABI_VERSION = 2  # RT_PROPOSE_ABI_VERSION of include/rt_propose.h
 TRACE_WHILE_WHILE = 0x1
 TRACE_COOP = 0x2
 TRACE_WIDE = 0x4
@@ -39,7 +39,8 @@ RASTER_EXPORTS = ("rt_camera_view_dir", "rt_raster_matrix", "rt_raster_scratch_b
 # every symbol include/rt_propose.h declares
 PROPOSE_EXPORTS = (
     "rt_propose_abi_version", "rt_gemm_bf16", "rt_gemm_argmax_bf16", "rt_ray_features", "rt_softmax_xent", "rt_transpose_bf16",
-    "rt_colsum_bf16", "rt_adam_step", "rt_subtree_slots", "rt_hit_labels", "rt_trace_closest_seeded",
+    "rt_colsum_bf16", "rt_adam_step", "rt_subtree_slots", "rt_hit_labels", "rt_trace_closest_seeded", "rt_transpose_bf16_grouped",
+    "rt_colsum_bf16_grouped", "rt_gather_batch", "rt_batch_subtree_slots", "rt_batch_hit_labels", "rt_batch_trace_seeded",
 )
 
 _P = C.c_void_p
@@ -121,23 +122,24 @@ class RasterDesc(C.Structure):
 class GemmDesc(C.Structure):
     _fields_ = [("a", _P), ("lda", _U32), ("b", _P), ("ldb", _U32), ("m", _U32), ("n", _U32), ("k", _U32), ("alpha", C.c_float),
                 ("bias", _P), ("relu", _U32), ("mask", _P), ("ldmask", _U32), ("c_f32", _P), ("ldc_f32", _U32), ("c_bf16", _P),
-                ("ldc_bf16", _U32), ("ct_bf16", _P), ("ldct", _U32), ("error_word", _P)]
+                ("ldc_bf16", _U32), ("ct_bf16", _P), ("ldct", _U32), ("error_word", _P), ("groups", _U32)]
 
 
 class GemmArgmaxDesc(C.Structure):
     _fields_ = [("a", _P), ("lda", _U32), ("b", _P), ("ldb", _U32), ("m", _U32), ("n", _U32), ("k", _U32), ("bias", _P),
-                ("min_margin", C.c_float), ("out_index", _P), ("out_value", _P), ("out_margin", _P), ("error_word", _P)]
+                ("min_margin", C.c_float), ("out_index", _P), ("out_value", _P), ("out_margin", _P), ("error_word", _P),
+                ("groups", _U32)]
 
 
 class FeatureDesc(C.Structure):
     _fields_ = [("orig", _P), ("dir", _P), ("count", _U32), ("box_lo", C.c_float * 3), ("box_hi", C.c_float * 3), ("out", _P),
-                ("ld_out", _U32), ("out_t", _P), ("ld_out_t", _U32)]
+                ("ld_out", _U32), ("out_t", _P), ("ld_out_t", _U32), ("group_rows", _U32)]
 
 
 class AdamDesc(C.Structure):
     _fields_ = [("param", _P), ("grad", _P), ("m", _P), ("v", _P), ("rows", _U32), ("cols", _U32), ("lr", C.c_float),
                 ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float), ("step", _U32), ("out_bf16", _P), ("ld_bf16", _U32),
-                ("out_bf16_t", _P), ("ld_bf16_t", _U32)]
+                ("out_bf16_t", _P), ("ld_bf16_t", _U32), ("groups", _U32)]
 
 
 class SlotDesc(C.Structure):
@@ -147,6 +149,16 @@ class SlotDesc(C.Structure):
 
 class SeedDesc(C.Structure):
     _fields_ = [("proposal", _P), ("slot_ref", _P), ("slot_box", _P), ("slot_count", _U32), ("in_proposal", _P)]
+
+
+class BatchGatherDesc(C.Structure):
+    _fields_ = [("orig", _P), ("dir", _P), ("labels", _P), ("groups", _U32), ("group_stride", _U32), ("offset", _U32),
+                ("batch", _U32), ("out_orig", _P), ("out_dir", _P), ("out_labels", _P)]
+
+
+class BatchSlotDesc(C.Structure):
+    _fields_ = [("mesh_count", _U32), ("face_offsets", _P), ("nodes", _P), ("accel", _P), ("face_count", _U32), ("depth", _U32),
+                ("slot_ref", _P), ("slot_box", _P), ("pos_label", _P), ("slot_first", _P), ("slot_count", _P)]
 
 
 class Camera(C.Structure):
@@ -206,6 +218,12 @@ def lib():
         L.rt_subtree_slots.argtypes = [C.POINTER(SlotDesc), _P]
         L.rt_hit_labels.argtypes = [_P, _U32, _P, _P, _P]
         L.rt_trace_closest_seeded.argtypes = [C.POINTER(TraceDesc), C.POINTER(SeedDesc), _P]
+        L.rt_transpose_bf16_grouped.argtypes = [_P, _U32, _U32, _U32, _U32, _P, _U32, _P]
+        L.rt_colsum_bf16_grouped.argtypes = [_P, _U32, _U32, _U32, _U32, _P, _P]
+        L.rt_gather_batch.argtypes = [C.POINTER(BatchGatherDesc), _P]
+        L.rt_batch_subtree_slots.argtypes = [C.POINTER(BatchSlotDesc), _P]
+        L.rt_batch_hit_labels.argtypes = [_P, _U32, _U32, _P, _P, _P, _P, _P]
+        L.rt_batch_trace_seeded.argtypes = [C.POINTER(BatchTraceDesc), C.POINTER(SeedDesc), _P]
         for name in PROPOSE_EXPORTS[1:]:
             getattr(L, name).restype = C.c_int
         L.rt_propose_abi_version.restype = _U32

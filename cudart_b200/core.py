@@ -573,6 +573,14 @@ def batch_build(vertices: torch.Tensor, faces: torch.Tensor, face_offsets: list,
 def batch_trace(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax=None, id_mode: int = 0, counters: bool = False,
                 while_while: bool = True, out: dict | None = None, stream=None) -> dict:
     """Closest hits for the rays of all meshes (rays of mesh m: ray_offsets[m] .. ray_offsets[m+1])."""
+    d, out = batch_trace_desc(tree, orig, dir, ray_offsets, tmax, id_mode, counters, while_while, out)
+    _abi.check("rt_batch_trace", _abi.lib().rt_batch_trace(C.byref(d), _stream(stream)))
+    return out
+
+
+def batch_trace_desc(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax=None, id_mode: int = 0, counters: bool = False,
+                     while_while: bool = True, out: dict | None = None):
+    """The rt_batch_trace_desc of batch_trace and its output tensors."""
     R = orig.shape[0]
     dev = orig.device
     if out is None:
@@ -590,5 +598,4 @@ def batch_trace(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax=None
     if "visits" in out:
         d.ray_visits, d.ray_tests = out["visits"].data_ptr(), out["tests"].data_ptr()
     d.schedule = _abi.TRACE_WHILE_WHILE if while_while else 0
-    _abi.check("rt_batch_trace", _abi.lib().rt_batch_trace(C.byref(d), _stream(stream)))
-    return out
+    return d, out

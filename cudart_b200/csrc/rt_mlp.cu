@@ -51,6 +51,7 @@ struct GemmEpi {
   uint32_t ldc16;
   __nv_bfloat16* ct16;
   uint32_t ldct;
+  uint32_t gm, gn;  // rows and columns of one group's product
 };
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
@@ -58,11 +59,13 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   return *(const uint32_t*)&h;
 }
 
-__device__ __forceinline__ void epilogue16(const GemmEpi& E, uint32_t row, uint32_t col, float (&v)[16]) {
+// row: stacked row of A / C; col: column inside group g's product.
+__device__ __forceinline__ void epilogue16(const GemmEpi& E, uint32_t g, uint32_t row, uint32_t col, float (&v)[16]) {
+  const float* bias = E.bias ? E.bias + (size_t)g * E.gn : nullptr;
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
     float x = v[i] * E.alpha;
-    if (E.bias) x += __ldg(E.bias + col + i);
+    if (bias) x += __ldg(bias + col + i);
     if (E.relu) x = fmaxf(x, 0.0f);
     v[i] = x;
   }
@@ -89,13 +92,14 @@ __device__ __forceinline__ void epilogue16(const GemmEpi& E, uint32_t row, uint3
     p[1] = make_uint4(pack_bf16(v[8], v[9]), pack_bf16(v[10], v[11]), pack_bf16(v[12], v[13]), pack_bf16(v[14], v[15]));
   }
   if (E.ct16) {
+    __nv_bfloat16* ct = E.ct16 + (size_t)g * E.gn * E.ldct + (row - g * E.gm);
 #pragma unroll
-    for (int i = 0; i < 16; ++i) E.ct16[(size_t)(col + i) * E.ldct + row] = __float2bfloat16_rn(v[i]);
+    for (int i = 0; i < 16; ++i) ct[(size_t)(col + i) * E.ldct] = __float2bfloat16_rn(v[i]);
   }
 }
 
 // ----------------------------------------------------------------------------
-// Generic GEMM: grid (n / bn, m / 128), 128 threads. Warp 0 lane 0 loads
+// Generic GEMM: grid (n / bn, m / 128, groups), 128 threads. Warp 0 lane 0 loads
 // (TMA), warp 1 lane 0 issues the MMAs, then all four warps drain TMEM.
 // ----------------------------------------------------------------------------
 __global__ void __launch_bounds__(128, 1)
@@ -130,15 +134,17 @@ __global__ void __launch_bounds__(128, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int32_t m0 = (int32_t)(blockIdx.y * kBM), n0 = (int32_t)(blockIdx.x * bn);
+  const uint32_t g = blockIdx.z;
+  const int32_t m0 = (int32_t)(g * E.gm + blockIdx.y * kBM), n0 = (int32_t)(blockIdx.x * bn);
 
   if (warp == 0 && lane == 0) {
+    const int32_t b0 = (int32_t)(g * E.gn) + n0;
     for (uint32_t kc = 0; kc < num_k; ++kc) {
       const uint32_t s = kc % kStages;
       if (kc >= kStages && !mbar_wait(empty + s, ((kc / kStages) - 1u) & 1u, err)) break;
       mbar_arrive_expect_tx(full + s, kTileA + tile_b);
       tma_load_2d(sA + s * kTileA, &ta, (int32_t)(kc * kBK), m0, full + s);
-      tma_load_2d(sB + s * tile_b, &tb, (int32_t)(kc * kBK), n0, full + s);
+      tma_load_2d(sB + s * tile_b, &tb, (int32_t)(kc * kBK), b0, full + s);
     }
   } else if (warp == 1 && lane == 0) {
     const uint32_t idesc = idesc_bf16_f32(kBM, bn);
@@ -165,7 +171,7 @@ __global__ void __launch_bounds__(128, 1)
     for (uint32_t c = 0; c < bn; c += 16) {
       float v[16];
       tmem_ld16(tl + c, v);
-      epilogue16(E, row, (uint32_t)n0 + c, v);
+      epilogue16(E, g, row, (uint32_t)n0 + c, v);
     }
   }
   tc_fence_before();
@@ -174,7 +180,7 @@ __global__ void __launch_bounds__(128, 1)
 }
 
 // ----------------------------------------------------------------------------
-// Row argmax of A B^T + bias: grid m / 128, 320 threads. Warps 0-7 drain TMEM
+// Row argmax of A B^T + bias: grid (m / 128, groups), 320 threads. Warps 0-7 drain TMEM
 // (warp w reads lanes 32 (w % 4) .. + 31 and the column half w / 4 of each
 // tile), warp 8 loads, warp 9 issues MMAs. A (128 rows x k, k <= 256) stays in
 // shared memory; B tiles of 256 rows x 64 stream through the ring;
@@ -207,8 +213,8 @@ __device__ __forceinline__ Top2 top2_merge(Top2 a, Top2 b) {
 
 __global__ void __launch_bounds__(kArgThreads, 1)
     k_gemm_argmax_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, const float* __restrict__ bias,
-                     uint32_t n, uint32_t num_k, float min_margin, int32_t* __restrict__ out_idx, float* __restrict__ out_val,
-                     float* __restrict__ out_margin, uint32_t* err) {
+                     uint32_t n, uint32_t gm, uint32_t num_k, float min_margin, int32_t* __restrict__ out_idx,
+                     float* __restrict__ out_val, float* __restrict__ out_margin, uint32_t* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* sA = smem;                        // num_k x 16 KB
@@ -222,7 +228,8 @@ __global__ void __launch_bounds__(kArgThreads, 1)
   uint64_t* acc_empty = acc_full + 2;  // [2]
   uint32_t* tmem_slot = (uint32_t*)(acc_empty + 2);
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  for (uint32_t j = threadIdx.x; j < n; j += kArgThreads) s_bias[j] = bias ? bias[j] : 0.0f;
+  const uint32_t grp = blockIdx.y;
+  for (uint32_t j = threadIdx.x; j < n; j += kArgThreads) s_bias[j] = bias ? bias[(size_t)grp * n + j] : 0.0f;
   if (threadIdx.x == 0) {
     for (uint32_t s = 0; s < kStages; ++s) {
       mbar_init(full + s, 1);
@@ -246,7 +253,7 @@ __global__ void __launch_bounds__(kArgThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int32_t m0 = (int32_t)(blockIdx.x * kBM);
+  const int32_t m0 = (int32_t)(grp * gm + blockIdx.x * kBM);
   const uint32_t ntiles = n / kArgBN;
   Top2 res = {-INFINITY, -INFINITY, -1};
   bool ok = true;
@@ -261,7 +268,7 @@ __global__ void __launch_bounds__(kArgThreads, 1)
         if (g >= kStages && !mbar_wait(empty + s, ((g / kStages) - 1u) & 1u, err)) break;
         const uint32_t t = g / num_k, kc = g % num_k;
         mbar_arrive_expect_tx(full + s, kArgTileB);
-        tma_load_2d(sB + s * kArgTileB, &tb, (int32_t)(kc * kBK), (int32_t)(t * kArgBN), full + s);
+        tma_load_2d(sB + s * kArgTileB, &tb, (int32_t)(kc * kBK), (int32_t)(grp * n + t * kArgBN), full + s);
       }
     }
   } else if (warp == 9) {
@@ -349,9 +356,10 @@ __global__ void __launch_bounds__(kArgThreads, 1)
 // f[24 i + 2 j + 1] = cos(pi 2^j u_i) for j < 12; columns 144..191 are zero
 // (rows hold ld >= 192 elements). Eight threads per ray: thread i < 6 encodes input i (48 bytes), threads 6
 // and 7 write the zero padding, so a warp stores 4 whole 384-byte rows.
+// out_t: one [192][group_rows] transpose per group of group_rows rays.
 __global__ __launch_bounds__(256) void k_ray_features(const float4* __restrict__ orig, const float4* __restrict__ dir, uint32_t count,
                                                       float3 c, float3 s, __nv_bfloat16* __restrict__ out, uint32_t ld,
-                                                      __nv_bfloat16* __restrict__ out_t, uint32_t ld_t) {
+                                                      __nv_bfloat16* __restrict__ out_t, uint32_t ld_t, uint32_t group_rows) {
   const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t r = gid >> 3, i = gid & 7u;
   if (r >= count) return;
@@ -385,11 +393,13 @@ __global__ __launch_bounds__(256) void k_ray_features(const float4* __restrict__
     p[2] = make_uint4(w[8], w[9], w[10], w[11]);
   }
   if (out_t) {
+    const uint32_t g = r / group_rows;
+    __nv_bfloat16* ot = out_t + (size_t)g * 192u * ld_t + (r - g * group_rows);
 #pragma unroll
     for (int j = 0; j < 12; ++j) {
       const uint32_t f = 24u * i + 2u * j;
-      out_t[(size_t)f * ld_t + r] = __ushort_as_bfloat16((unsigned short)(w[j] & 0xFFFFu));
-      out_t[(size_t)(f + 1) * ld_t + r] = __ushort_as_bfloat16((unsigned short)(w[j] >> 16));
+      ot[(size_t)f * ld_t] = __ushort_as_bfloat16((unsigned short)(w[j] & 0xFFFFu));
+      ot[(size_t)(f + 1) * ld_t] = __ushort_as_bfloat16((unsigned short)(w[j] >> 16));
     }
   }
 }
@@ -434,11 +444,13 @@ __global__ __launch_bounds__(256) void k_softmax_xent(const float* __restrict__ 
   if (lane == 0 && loss_sum) atomicAdd(loss_sum, (logf(sum) + mx - x[lab]) * scale);
 }
 
-// out[c][r] = in[r][c], 32 x 32 tiles through shared memory.
+// out[c][r] = in[r][c], 32 x 32 tiles through shared memory; blockIdx.z = group.
 __global__ __launch_bounds__(256) void k_transpose_bf16(const __nv_bfloat16* __restrict__ in, uint32_t rows, uint32_t cols, uint32_t ld_in,
                                                         __nv_bfloat16* __restrict__ out, uint32_t ld_out) {
   __shared__ __nv_bfloat16 tile[32][33];
   const uint32_t c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  in += (size_t)blockIdx.z * rows * ld_in;
+  out += (size_t)blockIdx.z * cols * ld_out;
   for (uint32_t y = threadIdx.y; y < 32; y += blockDim.y) {
     const uint32_t r = r0 + y, c = c0 + threadIdx.x;
     if (r < rows && c < cols) tile[y][threadIdx.x] = in[(size_t)r * ld_in + c];
@@ -450,24 +462,49 @@ __global__ __launch_bounds__(256) void k_transpose_bf16(const __nv_bfloat16* __r
   }
 }
 
-// out[c] += sum over a chunk of rows of in[r][c] (FP32 accumulation).
+// out[g cols + c] = sum of in[g rows + r][c] over r < rows, FP32, in a fixed
+// order: block (32, 8) per 32 columns of one group (blockIdx.y); thread y sums
+// rows y, y + 8, ... and the eight partial sums are added in order y = 0..7.
 __global__ __launch_bounds__(256) void k_colsum_bf16(const __nv_bfloat16* __restrict__ in, uint32_t rows, uint32_t cols, uint32_t ld,
-                                                     uint32_t rows_per_block, float* __restrict__ out) {
-  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= cols) return;
-  const uint32_t r0 = blockIdx.y * rows_per_block;
-  const uint32_t r1 = min(rows, r0 + rows_per_block);
+                                                     float* __restrict__ out) {
+  __shared__ float part[8][33];
+  const uint32_t c = blockIdx.x * 32 + threadIdx.x, g = blockIdx.y;
+  const __nv_bfloat16* p = in + (size_t)g * rows * ld + c;
   float s = 0.0f;
-  for (uint32_t r = r0; r < r1; ++r) s += __bfloat162float(in[(size_t)r * ld + c]);
-  atomicAdd(out + c, s);
+  if (c < cols)
+    for (uint32_t r = threadIdx.y; r < rows; r += 8) s += __bfloat162float(p[(size_t)r * ld]);
+  part[threadIdx.y][threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.y == 0 && c < cols) {
+    float t = part[0][threadIdx.x];
+#pragma unroll
+    for (int y = 1; y < 8; ++y) t += part[y][threadIdx.x];
+    out[(size_t)g * cols + c] = t;
+  }
+}
+
+// Row g batch + b <- row g stride + (offset + b) % stride.
+__global__ __launch_bounds__(256) void k_gather_batch(const float4* __restrict__ orig, const float4* __restrict__ dir,
+                                                      const int32_t* __restrict__ labels, uint32_t groups, uint32_t stride,
+                                                      uint32_t offset, uint32_t batch, float4* __restrict__ oo, float4* __restrict__ od,
+                                                      int32_t* __restrict__ ol) {
+  const size_t total = (size_t)groups * batch;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t g = (uint32_t)(i / batch), b = (uint32_t)(i - (size_t)g * batch);
+    const size_t src = (size_t)g * stride + (uint32_t)(((uint64_t)offset + b) % stride);
+    oo[i] = __ldg(orig + src);
+    od[i] = __ldg(dir + src);
+    if (labels) ol[i] = __ldg(labels + src);
+  }
 }
 
 // Adam (bias-corrected) on FP32 parameters [rows][cols]; refreshes the BF16
-// copies [rows][ld16] and transposed [cols][ld16t] when given.
+// copies [rows][ld16] and transposed [cols][ld16t] when given (with groups of
+// group_rows rows: one transpose per group, group q in rows q cols ..).
 __global__ __launch_bounds__(256) void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
                                               float* __restrict__ v, uint32_t rows, uint32_t cols, float lr, float b1, float b2,
                                               float eps, float c1, float c2, __nv_bfloat16* __restrict__ out16, uint32_t ld16,
-                                              __nv_bfloat16* __restrict__ out16t, uint32_t ld16t) {
+                                              __nv_bfloat16* __restrict__ out16t, uint32_t ld16t, uint32_t group_rows) {
   const size_t total = (size_t)rows * cols;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const float gi = g[i];
@@ -479,7 +516,10 @@ __global__ __launch_bounds__(256) void k_adam(float* __restrict__ p, const float
     p[i] = pi;
     const uint32_t r = (uint32_t)(i / cols), c = (uint32_t)(i % cols);
     if (out16) out16[(size_t)r * ld16 + c] = __float2bfloat16_rn(pi);
-    if (out16t) out16t[(size_t)c * ld16t + r] = __float2bfloat16_rn(pi);
+    if (out16t) {
+      const uint32_t q = r / group_rows;
+      out16t[((size_t)q * cols + c) * ld16t + (r - q * group_rows)] = __float2bfloat16_rn(pi);
+    }
   }
 }
 
@@ -550,18 +590,21 @@ extern "C" rt_status rt_gemm_bf16(const rt_gemm_desc* d, rt_stream stream) {
   if (d->c_bf16 && (d->ldc_bf16 < d->n || d->ldc_bf16 % 8 || !aligned16(d->c_bf16))) return RT_ERR_INVALID_ARGUMENT;
   if (d->mask && (d->ldmask < d->n || d->ldmask % 8 || !aligned16(d->mask))) return RT_ERR_INVALID_ARGUMENT;
   if (d->ct_bf16 && d->ldct < d->m) return RT_ERR_INVALID_ARGUMENT;
+  const uint32_t G = d->groups ? d->groups : 1u;
+  if (G > 65535u || (uint64_t)G * d->m > 0x7FFFFFFFull || (uint64_t)G * d->n > 0x7FFFFFFFull) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   const uint32_t bn = pick_bn(d->n);
   CUtensorMap ta, tb;
-  if (!make_map(&ta, d->a, d->k, d->m, d->lda, kBM) || !make_map(&tb, d->b, d->k, d->n, d->ldb, bn)) return RT_ERR_UNSUPPORTED;
+  if (!make_map(&ta, d->a, d->k, G * d->m, d->lda, kBM) || !make_map(&tb, d->b, d->k, G * d->n, d->ldb, bn)) return RT_ERR_UNSUPPORTED;
   GemmEpi E;
   E.alpha = d->alpha; E.bias = d->bias; E.relu = d->relu; E.mask = (const __nv_bfloat16*)d->mask; E.ldmask = d->ldmask;
   E.c32 = d->c_f32; E.ldc32 = d->ldc_f32; E.c16 = (__nv_bfloat16*)d->c_bf16; E.ldc16 = d->ldc_bf16;
   E.ct16 = (__nv_bfloat16*)d->ct_bf16; E.ldct = d->ldct;
+  E.gm = d->m; E.gn = d->n;
   const size_t smem = gemm_smem(bn);
   static std::once_flag once;
   std::call_once(once, [] { cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem(256)); });
-  dim3 grid(d->n / bn, d->m / kBM);
+  dim3 grid(d->n / bn, d->m / kBM, G);
   k_gemm_tc<<<grid, 128, smem, (cudaStream_t)stream>>>(ta, tb, E, bn, pow2_cols(bn), d->k / kBK, d->error_word);
   note_launch();
   RT_CHECK_LAUNCH();
@@ -574,16 +617,18 @@ extern "C" rt_status rt_gemm_argmax_bf16(const rt_gemm_argmax_desc* d, rt_stream
     return RT_ERR_INVALID_ARGUMENT;
   if (d->lda < d->k || d->ldb < d->k || d->lda % 8 || d->ldb % 8 || !aligned16(d->a) || !aligned16(d->b))
     return RT_ERR_INVALID_ARGUMENT;
+  const uint32_t G = d->groups ? d->groups : 1u;
+  if (G > 65535u || (uint64_t)G * d->m > 0x7FFFFFFFull || (uint64_t)G * d->n > 0x7FFFFFFFull) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   CUtensorMap ta, tb;
-  if (!make_map(&ta, d->a, d->k, d->m, d->lda, kBM) || !make_map(&tb, d->b, d->k, d->n, d->ldb, kArgBN)) return RT_ERR_UNSUPPORTED;
+  if (!make_map(&ta, d->a, d->k, G * d->m, d->lda, kBM) || !make_map(&tb, d->b, d->k, G * d->n, d->ldb, kArgBN)) return RT_ERR_UNSUPPORTED;
   const uint32_t num_k = d->k / kBK;
   static std::once_flag once;
   std::call_once(once, [] {
     cudaFuncSetAttribute(k_gemm_argmax_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)argmax_smem(4, kArgMaxN));
   });
-  k_gemm_argmax_tc<<<d->m / kBM, kArgThreads, argmax_smem(num_k, d->n), (cudaStream_t)stream>>>(ta, tb, d->bias, d->n, num_k, d->min_margin,
-                                                                                  d->out_index, d->out_value, d->out_margin, d->error_word);
+  k_gemm_argmax_tc<<<dim3(d->m / kBM, G), kArgThreads, argmax_smem(num_k, d->n), (cudaStream_t)stream>>>(
+      ta, tb, d->bias, d->n, d->m, num_k, d->min_margin, d->out_index, d->out_value, d->out_margin, d->error_word);
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
@@ -592,14 +637,16 @@ extern "C" rt_status rt_gemm_argmax_bf16(const rt_gemm_argmax_desc* d, rt_stream
 extern "C" rt_status rt_ray_features(const rt_feature_desc* d, rt_stream stream) {
   if (!d || !d->orig || !d->dir || (!d->out && !d->out_t)) return RT_ERR_INVALID_ARGUMENT;
   if (d->out && (d->ld_out < 192 || d->ld_out % 8 || !aligned16(d->out))) return RT_ERR_INVALID_ARGUMENT;
-  if (d->out_t && d->ld_out_t < d->count) return RT_ERR_INVALID_ARGUMENT;
+  const uint32_t gr = d->group_rows ? d->group_rows : d->count;
+  if (d->group_rows && d->count % d->group_rows) return RT_ERR_INVALID_ARGUMENT;
+  if (d->out_t && d->ld_out_t < gr) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   if (d->count == 0) return RT_OK;
   const float3 c = make_float3(0.5f * (d->box_lo[0] + d->box_hi[0]), 0.5f * (d->box_lo[1] + d->box_hi[1]), 0.5f * (d->box_lo[2] + d->box_hi[2]));
   const float3 s = make_float3(2.0f / (d->box_hi[0] - d->box_lo[0]), 2.0f / (d->box_hi[1] - d->box_lo[1]), 2.0f / (d->box_hi[2] - d->box_lo[2]));
   k_ray_features<<<(uint32_t)(((size_t)d->count * 8 + 255) / 256), 256, 0, (cudaStream_t)stream>>>((const float4*)d->orig, (const float4*)d->dir, d->count, c, s,
                                                                            (__nv_bfloat16*)d->out, d->ld_out, (__nv_bfloat16*)d->out_t,
-                                                                           d->ld_out_t);
+                                                                           d->ld_out_t, gr);
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
@@ -616,27 +663,48 @@ extern "C" rt_status rt_softmax_xent(const float* logits, uint32_t rows, uint32_
   return RT_OK;
 }
 
-extern "C" rt_status rt_transpose_bf16(const void* in, uint32_t rows, uint32_t cols, uint32_t ld_in, void* out, uint32_t ld_out,
-                                       rt_stream stream) {
-  if (!in || !out || ld_in < cols || ld_out < rows) return RT_ERR_INVALID_ARGUMENT;
+extern "C" rt_status rt_transpose_bf16_grouped(const void* in, uint32_t groups, uint32_t rows, uint32_t cols, uint32_t ld_in, void* out,
+                                               uint32_t ld_out, rt_stream stream) {
+  if (!in || !out || ld_in < cols || ld_out < rows || groups == 0 || groups > 65535u) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   if (rows == 0 || cols == 0) return RT_OK;
-  dim3 grid((cols + 31) / 32, (rows + 31) / 32);
+  dim3 grid((cols + 31) / 32, (rows + 31) / 32, groups);
   k_transpose_bf16<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)in, rows, cols, ld_in, (__nv_bfloat16*)out, ld_out);
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
 }
 
-extern "C" rt_status rt_colsum_bf16(const void* in, uint32_t rows, uint32_t cols, uint32_t ld, float* out, rt_stream stream) {
-  if (!in || !out || ld < cols) return RT_ERR_INVALID_ARGUMENT;
+extern "C" rt_status rt_transpose_bf16(const void* in, uint32_t rows, uint32_t cols, uint32_t ld_in, void* out, uint32_t ld_out,
+                                       rt_stream stream) {
+  return rt_transpose_bf16_grouped(in, 1, rows, cols, ld_in, out, ld_out, stream);
+}
+
+extern "C" rt_status rt_colsum_bf16_grouped(const void* in, uint32_t groups, uint32_t rows, uint32_t cols, uint32_t ld, float* out,
+                                            rt_stream stream) {
+  if (!in || !out || ld < cols || groups == 0 || groups > 65535u) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
-  cudaStream_t st = (cudaStream_t)stream;
-  if (cudaMemsetAsync(out, 0, (size_t)cols * 4, st) != cudaSuccess) return RT_ERR_CUDA;
-  if (rows == 0 || cols == 0) return RT_OK;
-  const uint32_t rpb = 256;
-  dim3 grid((cols + 255) / 256, (rows + rpb - 1) / rpb);
-  k_colsum_bf16<<<grid, 256, 0, st>>>((const __nv_bfloat16*)in, rows, cols, ld, rpb, out);
+  if (cols == 0) return RT_OK;
+  k_colsum_bf16<<<dim3((cols + 31) / 32, groups), dim3(32, 8), 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)in, rows, cols, ld, out);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_colsum_bf16(const void* in, uint32_t rows, uint32_t cols, uint32_t ld, float* out, rt_stream stream) {
+  return rt_colsum_bf16_grouped(in, 1, rows, cols, ld, out, stream);
+}
+
+extern "C" rt_status rt_gather_batch(const rt_batch_gather_desc* d, rt_stream stream) {
+  if (!d || !d->orig || !d->dir || !d->out_orig || !d->out_dir || (d->labels && !d->out_labels) || d->group_stride == 0)
+    return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  const size_t total = (size_t)d->groups * d->batch;
+  if (total == 0) return RT_OK;
+  const uint32_t blocks = (uint32_t)hmin<size_t>((total + 255) / 256, (size_t)num_sms() * 8);
+  k_gather_batch<<<blocks, 256, 0, (cudaStream_t)stream>>>((const float4*)d->orig, (const float4*)d->dir, d->labels, d->groups,
+                                                           d->group_stride, d->offset, d->batch, (float4*)d->out_orig,
+                                                           (float4*)d->out_dir, d->out_labels);
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
@@ -644,6 +712,8 @@ extern "C" rt_status rt_colsum_bf16(const void* in, uint32_t rows, uint32_t cols
 
 extern "C" rt_status rt_adam_step(const rt_adam_desc* d, rt_stream stream) {
   if (!d || !d->param || !d->grad || !d->m || !d->v || d->step == 0) return RT_ERR_INVALID_ARGUMENT;
+  const uint32_t G = d->groups ? d->groups : 1u;
+  if (d->rows % G) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   const size_t total = (size_t)d->rows * d->cols;
   if (total == 0) return RT_OK;
@@ -652,7 +722,7 @@ extern "C" rt_status rt_adam_step(const rt_adam_desc* d, rt_stream stream) {
   const uint32_t blocks = (uint32_t)hmin<size_t>((total + 255) / 256, (size_t)num_sms() * 8);
   k_adam<<<blocks, 256, 0, (cudaStream_t)stream>>>(d->param, d->grad, d->m, d->v, d->rows, d->cols, d->lr, d->beta1, d->beta2, d->eps, c1,
                                                     c2, (__nv_bfloat16*)d->out_bf16, d->ld_bf16, (__nv_bfloat16*)d->out_bf16_t,
-                                                    d->ld_bf16_t);
+                                                    d->ld_bf16_t, G > 1 ? d->rows / G : (d->rows ? d->rows : 1u));
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;

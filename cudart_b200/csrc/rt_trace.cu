@@ -645,8 +645,9 @@ struct BatchTraceArgs {
   BatchAccel acc;
 };
 
-template <bool kCount, bool kWW>
-__global__ __launch_bounds__(128) void k_batch_trace(TraceArgs A, BatchTraceArgs B) {
+// Seeded: the slot tables of mesh m start at m slot_count entries.
+template <bool kCount, bool kWW, bool kSeed>
+__global__ __launch_bounds__(128) void k_batch_trace(TraceArgs A, BatchTraceArgs B, SeedArgs S) {
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= A.ray_count) return;
   const uint32_t m = find_seg(B.roff, B.M, r);
@@ -659,7 +660,14 @@ __global__ __launch_bounds__(128) void k_batch_trace(TraceArgs A, BatchTraceArgs
   TraceArgs Am = A;
   Am.tris = A.tris + 3 * (size_t)F;
   Am.indices = A.indices + F;
-  trace_ray_accel<kCount, kWW>(r, Am, C);
+  if constexpr (kSeed) {
+    SeedArgs Sm = S;
+    Sm.slot_ref = S.slot_ref + (size_t)m * S.slot_count;
+    if (S.slot_box) Sm.slot_box = S.slot_box + 2 * (size_t)m * S.slot_count;
+    trace_ray_accel<kCount, kWW, true>(r, Am, C, Sm);
+  } else {
+    trace_ray_accel<kCount, kWW>(r, Am, C);
+  }
 }
 
 // Sort key of a ray: direction octant (3 bits) above a 29-bit Morton code of
@@ -953,13 +961,9 @@ extern "C" rt_status rt_bounce_rays(const float* tris, const float* orig, const 
   return RT_OK;
 }
 
-extern "C" rt_status rt_batch_trace(const rt_batch_trace_desc* d, rt_stream stream) {
-  if (!d || d->mesh_count == 0 || !d->face_offsets || !d->ray_offsets || !d->accel || !d->tris || !d->orig || !d->dir ||
-      !d->hit_id || !d->hit_t || !d->hit_uv || d->face_count < d->mesh_count)
-    return RT_ERR_INVALID_ARGUMENT;
-  if (d->id_mode == 1 && !d->indices) return RT_ERR_INVALID_ARGUMENT;
-  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
-  if (d->ray_count == 0) return RT_OK;
+namespace {
+template <bool kSeed>
+rt_status batch_launch(const rt_batch_trace_desc* d, const SeedArgs& S, cudaStream_t st) {
   TraceArgs A = {};
   A.tris = (const float4*)d->tris; A.indices = d->indices; A.orig = (const float4*)d->orig; A.dir = (const float4*)d->dir;
   A.tmax = d->tmax; A.ray_count = d->ray_count; A.id_mode = d->id_mode; A.hit_id = d->hit_id; A.hit_t = d->hit_t;
@@ -971,10 +975,41 @@ extern "C" rt_status rt_batch_trace(const rt_batch_trace_desc* d, rt_stream stre
   const bool count = d->ray_visits || d->ray_tests;
   const bool ww = (d->schedule & RT_TRACE_WHILE_WHILE) != 0;
   const uint32_t blocks = (d->ray_count + 127) / 128;
-  cudaStream_t st = (cudaStream_t)stream;
-  if (count) { if (ww) k_batch_trace<true, true><<<blocks, 128, 0, st>>>(A, B); else k_batch_trace<true, false><<<blocks, 128, 0, st>>>(A, B); }
-  else { if (ww) k_batch_trace<false, true><<<blocks, 128, 0, st>>>(A, B); else k_batch_trace<false, false><<<blocks, 128, 0, st>>>(A, B); }
+  if (count) {
+    if (ww) k_batch_trace<true, true, kSeed><<<blocks, 128, 0, st>>>(A, B, S);
+    else k_batch_trace<true, false, kSeed><<<blocks, 128, 0, st>>>(A, B, S);
+  } else {
+    if (ww) k_batch_trace<false, true, kSeed><<<blocks, 128, 0, st>>>(A, B, S);
+    else k_batch_trace<false, false, kSeed><<<blocks, 128, 0, st>>>(A, B, S);
+  }
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
+}
+
+rt_status batch_check(const rt_batch_trace_desc* d) {
+  if (!d || d->mesh_count == 0 || !d->face_offsets || !d->ray_offsets || !d->accel || !d->tris || !d->orig || !d->dir ||
+      !d->hit_id || !d->hit_t || !d->hit_uv || d->face_count < d->mesh_count)
+    return RT_ERR_INVALID_ARGUMENT;
+  if (d->id_mode == 1 && !d->indices) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  return RT_OK;
+}
+}  // namespace
+
+extern "C" rt_status rt_batch_trace(const rt_batch_trace_desc* d, rt_stream stream) {
+  const rt_status s = batch_check(d);
+  if (s != RT_OK || d->ray_count == 0) return s;
+  return batch_launch<false>(d, SeedArgs{}, (cudaStream_t)stream);
+}
+
+extern "C" rt_status rt_batch_trace_seeded(const rt_batch_trace_desc* d, const rt_seed_desc* sd, rt_stream stream) {
+  const rt_status s = batch_check(d);
+  if (s != RT_OK) return s;
+  if (!sd || !sd->proposal || !sd->slot_ref) return RT_ERR_INVALID_ARGUMENT;
+  if (d->ray_count == 0) return RT_OK;
+  SeedArgs S;
+  S.proposal = sd->proposal; S.slot_ref = sd->slot_ref; S.slot_box = (const float4*)sd->slot_box; S.slot_count = sd->slot_count;
+  S.in_prop = sd->in_proposal;
+  return batch_launch<true>(d, S, (cudaStream_t)stream);
 }

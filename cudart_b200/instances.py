@@ -1,0 +1,141 @@
+"""Many deformed instances of one scene, rebuilt and traced every frame, each
+with its own proposal network fine-tuned on the previous frame's hits.
+
+Per frame: every instance's vertices move by fresh N(0, sigma^2) noise; one
+batched LBVH build makes all instance trees (rt_batch_build); each instance's
+primary rays (one pinhole camera per instance) and one diffuse bounce per hit
+are traced two ways over all instances at once:
+
+  plain   rt_batch_trace for the primaries, rt_bounce_rays, rt_batch_trace
+          for the bounces;
+  learned the grouped MLP (one network per instance, the same launches for
+          all) proposes a depth-12 slot of the instance's tree per ray, and
+          rt_batch_trace_seeded walks it first. Hits are bit-identical to the
+          plain ones, so the bounces are the same rays.
+
+The plain hits label the frame's rays (the slot holding the hit, per
+instance); the next frame fine-tunes every instance's network on them with
+`steps` grouped Adam steps of `batch` rays per instance, alternating between
+primary and bounce rays.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import core, proposal, scenes
+
+
+class InstancedFrames:
+    def __init__(self, count: int, scale: float, width: int, height: int, device="cuda", seed: int = 7, depth: int = proposal.DEPTH,
+                 batch: int = 1024, steps: int = 200, lr: float = 1e-3, sigma: float = 0.002, net_seed: int = 0):
+        if (width * height) % 128:
+            raise ValueError("width * height must be a multiple of 128 (one grouped GEMM tile of rays)")
+        self.count, self.width, self.height = count, width, height
+        self.dev = torch.device(device)
+        self.seed, self.depth, self.batch, self.steps, self.lr, self.sigma = seed, depth, batch, steps, lr, sigma
+        base = scenes.learned_scene(scale)
+        self.base_faces = base.face_count
+        self.base_v = torch.from_numpy(base.vertices).to(self.dev)
+        f = torch.from_numpy(base.faces.view(np.int32)).to(self.dev)
+        self.faces = f.repeat(count, 1).contiguous()
+        N, V = base.face_count, base.vertex_count
+        self.face_offsets = [i * N for i in range(count + 1)]
+        self.vertex_offsets = [i * V for i in range(count + 1)]
+        self.cams = scenes.instance_cameras(count, width, height)
+        R = width * height
+        self.rays_per_instance = R
+        self.orig = torch.empty((count * R, 4), dtype=torch.float32, device=self.dev)
+        self.dir = torch.empty((count * R, 4), dtype=torch.float32, device=self.dev)
+        for i, c in enumerate(self.cams):
+            cam = core.make_camera(c.center, c.target, fov=c.fov, ratio=c.ratio)
+            core.primary_rays(cam, width, height, out=(self.orig[i * R:(i + 1) * R], self.dir[i * R:(i + 1) * R]))
+        self.ray_offsets = torch.tensor([i * R for i in range(count + 1)], dtype=torch.int32, device=self.dev)
+        self.ray_face_base = torch.repeat_interleave(torch.tensor(self.face_offsets[:-1], dtype=torch.int32, device=self.dev),
+                                                     torch.full((count,), R, dtype=torch.int64, device=self.dev))
+        pts = np.concatenate([base.vertices[:, :3], np.array([c.center for c in self.cams], np.float32)])
+        lo, hi = pts.min(0).astype(np.float64), pts.max(0).astype(np.float64)
+        mid, half = 0.5 * (lo + hi), 0.55 * (hi - lo)
+        self.box = tuple(float(x) for x in np.concatenate([mid - half, mid + half]))
+        self.nets = proposal.ProposalGroup(count, 1 << depth, device=self.dev, seed=net_seed)
+        self.verts = None
+        self.tree = None
+        self.slots = None
+        self.frame_index = -1
+        self.prev = None  # (bounce orig, bounce dir, primary labels, bounce labels) of the previous frame
+
+    @property
+    def face_count(self) -> int:
+        return self.faces.shape[0]
+
+    @property
+    def ray_count(self) -> int:
+        return self.orig.shape[0]
+
+    # ------------------------------------------------------------ frame steps
+    def displace(self, frame: int):
+        self.frame_index = frame
+        self.verts = scenes.displace_instances(self.base_v, self.count, frame, self.seed, self.sigma, out=self.verts)
+
+    def build(self):
+        self.tree = core.batch_build(self.verts, self.faces, self.face_offsets, self.vertex_offsets, out=self.tree)
+        return self.tree
+
+    def make_slots(self):
+        self.slots = proposal.batch_subtree_slots(self.tree, self.depth)
+        return self.slots
+
+    def bounce(self, hits, out=None):
+        gpos = torch.where(hits["id"] >= 0, hits["id"] + self.ray_face_base, hits["id"])
+        return core.bounce_rays(self.tree.tris, self.orig, self.dir, gpos, hits["t"], 1000 + self.frame_index, out=out)
+
+    def trace_plain(self, out=None):
+        """Primary hits, bounce rays and bounce hits through rt_batch_trace."""
+        out = out or {}
+        h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, out=out.get("h1"))
+        b = self.bounce(h1, out=out.get("b"))
+        h2 = core.batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], out=out.get("h2"))
+        return dict(h1=h1, b=b, h2=h2)
+
+    def trace_learned(self, out=None, in_proposal: bool = False):
+        """The same through the grouped proposal and rt_batch_trace_seeded."""
+        out = out or {}
+        R = self.rays_per_instance
+        p1 = self.nets.propose(self.orig, self.dir, self.box, R, out=out.get("p1"))
+        h1 = proposal.batch_trace_seeded(self.tree, self.orig, self.dir, self.ray_offsets, p1, self.slots, in_proposal=in_proposal,
+                                         out=out.get("h1"))
+        b = self.bounce(h1, out=out.get("b"))
+        p2 = self.nets.propose(b[0], b[1], self.box, R, out=out.get("p2"))
+        h2 = proposal.batch_trace_seeded(self.tree, b[0], b[1], self.ray_offsets, p2, self.slots, tmax=b[2], in_proposal=in_proposal,
+                                         out=out.get("h2"))
+        return dict(p1=p1, h1=h1, b=b, p2=p2, h2=h2)
+
+    def labels(self, plain):
+        """Per-instance slot labels of the frame's primary and bounce rays (-1 for misses)."""
+        l1 = proposal.batch_hit_labels(self.tree, plain["h1"]["id"], self.ray_offsets, self.slots["pos_label"])
+        l2 = proposal.batch_hit_labels(self.tree, plain["h2"]["id"], self.ray_offsets, self.slots["pos_label"])
+        return l1, l2
+
+    def remember(self, plain):
+        """Keep this frame's rays and labels for the next frame's fine-tuning."""
+        l1, l2 = self.labels(plain)
+        b = plain["b"]
+        self.prev = (b[0].clone(), b[1].clone(), l1, l2)
+
+    def fine_tune(self, steps: int | None = None):
+        """Grouped Adam steps on the previous frame's labelled rays: even steps
+        take primary rays, odd steps bounce rays, each a window of `batch` rays
+        per instance advancing by `batch` every second step."""
+        if self.prev is None:
+            return None
+        steps = self.steps if steps is None else steps
+        bo, bd, l1, l2 = self.prev
+        net, B, R = self.nets, self.batch, self.rays_per_instance
+        ws = net._workspace(B, True)
+        gb = (ws["bo"], ws["bd"], ws["bl"])
+        loss = None
+        for j in range(steps):
+            o, d, lab = (self.orig, self.dir, l1) if j % 2 == 0 else (bo, bd, l2)
+            proposal.gather_batch(o, d, lab, self.count, R, (j // 2) * B, B, gb)
+            loss = net.train_step(gb[0], gb[1], gb[2], self.box, B, lr=self.lr)
+        return loss

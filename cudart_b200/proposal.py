@@ -41,13 +41,18 @@ def _bf16(shape, device):
 
 
 def gemm(a: torch.Tensor, b: torch.Tensor, bias=None, relu=False, mask=None, alpha=1.0, out_f32=None, out_bf16=None, out_t=None,
-         err=None, stream=None):
-    """C = alpha * a @ b.T (+ bias) (ReLU) (* (mask > 0)); a: bf16 (m, k), b: bf16 (n, k)."""
-    m, k = a.shape
-    n = b.shape[0]
+         err=None, groups: int = 1, stream=None):
+    """C = alpha * a @ b.T (+ bias) (ReLU) (* (mask > 0)); a: bf16 (m, k), b: bf16 (n, k).
+    groups > 1: a holds `groups` stacked (m, k) blocks and b stacked (n, k)
+    blocks; block g of C is a_g @ b_g.T (out_t: stacked (n, m) transposes)."""
+    m, k = a.shape[0] // groups, a.shape[1]
+    n = b.shape[0] // groups
     if b.shape[1] != k:
         raise ValueError("inner dimensions differ")
+    if a.shape[0] % groups or b.shape[0] % groups:
+        raise ValueError("rows are not a multiple of groups")
     d = _abi.GemmDesc()
+    d.groups = groups
     d.a, d.lda, d.b, d.ldb = a.data_ptr(), a.stride(0), b.data_ptr(), b.stride(0)
     d.m, d.n, d.k, d.alpha = m, n, k, alpha
     d.bias = bias.data_ptr() if bias is not None else None
@@ -66,14 +71,15 @@ def gemm(a: torch.Tensor, b: torch.Tensor, bias=None, relu=False, mask=None, alp
 
 
 def gemm_argmax(a: torch.Tensor, b: torch.Tensor, bias=None, out_index=None, out_value=None, out_margin=None, min_margin=0.0,
-                err=None, stream=None):
+                err=None, groups: int = 1, stream=None):
     """Row argmax of a @ b.T + bias without storing the logits (-1 where the
-    top-1 / top-2 margin is below min_margin)."""
-    m, k = a.shape
-    n = b.shape[0]
+    top-1 / top-2 margin is below min_margin); grouped as in gemm()."""
+    m, k = a.shape[0] // groups, a.shape[1]
+    n = b.shape[0] // groups
     if out_index is None:
-        out_index = torch.empty(m, dtype=torch.int32, device=a.device)
+        out_index = torch.empty(a.shape[0], dtype=torch.int32, device=a.device)
     d = _abi.GemmArgmaxDesc()
+    d.groups = groups
     d.a, d.lda, d.b, d.ldb = a.data_ptr(), a.stride(0), b.data_ptr(), b.stride(0)
     d.m, d.n, d.k = m, n, k
     d.bias = bias.data_ptr() if bias is not None else None
@@ -87,10 +93,12 @@ def gemm_argmax(a: torch.Tensor, b: torch.Tensor, bias=None, out_index=None, out
     return out_index
 
 
-def ray_features(orig, dir, box, out=None, out_t=None, count=None, stream=None):
-    """bf16 features (count, 192) and/or their transpose (192, count); box = (lo xyz, hi xyz)."""
+def ray_features(orig, dir, box, out=None, out_t=None, count=None, group_rows: int = 0, stream=None):
+    """bf16 features (count, 192) and/or their transpose (192, count); box = (lo xyz, hi xyz).
+    group_rows > 0: out_t holds one (192, group_rows) transpose per group of rays."""
     R = orig.shape[0] if count is None else count
     d = _abi.FeatureDesc()
+    d.group_rows = group_rows
     d.orig, d.dir, d.count = orig.data_ptr(), dir.data_ptr(), R
     for i in range(3):
         d.box_lo[i] = float(box[i])
@@ -109,6 +117,30 @@ def transpose(x: torch.Tensor, out: torch.Tensor, stream=None):
 
 def colsum(x: torch.Tensor, out: torch.Tensor, stream=None):
     _check("rt_colsum_bf16", _abi.lib().rt_colsum_bf16(_p(x), x.shape[0], x.shape[1], x.stride(0), _p(out), _stream(stream)))
+
+
+def transpose_grouped(x: torch.Tensor, groups: int, out: torch.Tensor, stream=None):
+    """x: `groups` stacked (r, c) blocks -> out: stacked (c, r) transposes."""
+    r = x.shape[0] // groups
+    _check("rt_transpose_bf16_grouped", _abi.lib().rt_transpose_bf16_grouped(_p(x), groups, r, x.shape[1], x.stride(0), _p(out),
+                                                                              out.stride(0), _stream(stream)))
+
+
+def colsum_grouped(x: torch.Tensor, groups: int, out: torch.Tensor, stream=None):
+    """Column sums of each of `groups` stacked blocks: out (groups * cols,)."""
+    r = x.shape[0] // groups
+    _check("rt_colsum_bf16_grouped", _abi.lib().rt_colsum_bf16_grouped(_p(x), groups, r, x.shape[1], x.stride(0), _p(out),
+                                                                        _stream(stream)))
+
+
+def gather_batch(orig, dir, labels, groups: int, group_stride: int, offset: int, batch: int, out: tuple, stream=None):
+    """Rows g * batch + b <- g * group_stride + (offset + b) % group_stride."""
+    d = _abi.BatchGatherDesc()
+    d.orig, d.dir, d.labels = orig.data_ptr(), dir.data_ptr(), _p(labels)
+    d.groups, d.group_stride, d.offset, d.batch = groups, group_stride, offset % group_stride, batch
+    d.out_orig, d.out_dir, d.out_labels = out[0].data_ptr(), out[1].data_ptr(), _p(out[2])
+    _check("rt_gather_batch", _abi.lib().rt_gather_batch(C.byref(d), _stream(stream)))
+    return out
 
 
 class ProposalNet:
@@ -250,6 +282,155 @@ class ProposalNet:
         return out
 
 
+class ProposalGroup:
+    """`groups` independent proposal networks (one per mesh of a batched
+    build) trained and run in the same launches: every weight, bias and
+    activation stacks the groups along its rows, and group g's numbers equal,
+    bit for bit, a ProposalNet holding group g's weights fed group g's rays."""
+
+    def __init__(self, groups: int, classes: int = 1 << DEPTH, device="cuda", seed: int = 0, init: "ProposalNet | None" = None):
+        self.groups, self.classes = groups, classes
+        self.device = torch.device(device)
+        base = init if init is not None else ProposalNet(classes, device=self.device, seed=seed)
+        G = groups
+        self.W = [w.repeat(G, 1).contiguous() for w in base.W]
+        self.b = [b.repeat(G).contiguous() for b in base.b]
+        self.W16 = [w.to(torch.bfloat16).contiguous() for w in self.W]
+        self.W16t = [self._stacked_t(w) for w in self.W]
+        self.params = [t for pair in zip(self.W, self.b) for t in pair]
+        self.m = [torch.zeros_like(t) for t in self.params]
+        self.v = [torch.zeros_like(t) for t in self.params]
+        self.grads = [torch.zeros_like(t) for t in self.params]
+        self.step_count = 0
+        self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._ws = {}
+
+    def _stacked_t(self, w):
+        G = self.groups
+        out_f, in_f = w.shape[0] // G, w.shape[1]
+        return w.view(G, out_f, in_f).transpose(1, 2).reshape(G * in_f, out_f).to(torch.bfloat16).contiguous()
+
+    def net(self, g: int) -> ProposalNet:
+        """Group g's weights as a stand-alone ProposalNet (FP32 master copies)."""
+        n = ProposalNet(self.classes, device=self.device)
+        for i in range(4):
+            rows = n.W[i].shape[0]
+            n.W[i].copy_(self.W[i][g * rows:(g + 1) * rows])
+            n.b[i].copy_(self.b[i][g * rows:(g + 1) * rows])
+            n.W16[i].copy_(self.W16[i][g * rows:(g + 1) * rows])
+            cols = n.W[i].shape[1]
+            n.W16t[i].copy_(self.W16t[i][g * cols:(g + 1) * cols])
+        return n
+
+    def _workspace(self, B: int, train: bool):
+        key = (B, train)
+        ws = self._ws.get(key)
+        if ws is None:
+            G, dev, K = self.groups, self.device, self.classes
+            R = G * B
+            ws = dict(X=_bf16((R, FEATURES_PAD), dev), H1=_bf16((R, HIDDEN), dev), H2=_bf16((R, HIDDEN), dev), H3=_bf16((R, HIDDEN), dev))
+            if train:
+                ws.update(XT=_bf16((G * FEATURES_PAD, B), dev), H1T=_bf16((G * HIDDEN, B), dev), H2T=_bf16((G * HIDDEN, B), dev),
+                          H3T=_bf16((G * HIDDEN, B), dev), L=torch.empty((R, K), dtype=torch.float32, device=dev),
+                          G=_bf16((R, K), dev), GT=_bf16((G * K, B), dev), D3=_bf16((R, HIDDEN), dev),
+                          D3T=_bf16((G * HIDDEN, B), dev), D2=_bf16((R, HIDDEN), dev), D2T=_bf16((G * HIDDEN, B), dev),
+                          D1=_bf16((R, HIDDEN), dev), D1T=_bf16((G * HIDDEN, B), dev),
+                          loss=torch.zeros(1, dtype=torch.float32, device=dev),
+                          bo=torch.empty((R, 4), dtype=torch.float32, device=dev), bd=torch.empty((R, 4), dtype=torch.float32, device=dev),
+                          bl=torch.empty(R, dtype=torch.int32, device=dev))
+            self._ws[key] = ws
+        return ws
+
+    def forward_backward(self, orig, dir, labels, box, batch: int, stream=None):
+        """Gradients of each group's mean cross-entropy over its `batch` rays
+        (rows g * batch ..; labels outside [0, classes) are left out); returns
+        the sum over groups of the group losses."""
+        G, B = self.groups, batch
+        if B % 128 or orig.shape[0] != G * B:
+            raise ValueError("need groups * batch rays with batch % 128 == 0")
+        ws = self._workspace(B, True)
+        W16, W16t, b, err = self.W16, self.W16t, self.b, self.err
+        kw = dict(err=err, groups=G, stream=stream)
+        ray_features(orig, dir, box, out=ws["X"], out_t=ws["XT"], group_rows=B, stream=stream)
+        gemm(ws["X"], W16[0], bias=b[0], relu=True, out_bf16=ws["H1"], out_t=ws["H1T"], **kw)
+        gemm(ws["H1"], W16[1], bias=b[1], relu=True, out_bf16=ws["H2"], out_t=ws["H2T"], **kw)
+        gemm(ws["H2"], W16[2], bias=b[2], relu=True, out_bf16=ws["H3"], out_t=ws["H3T"], **kw)
+        gemm(ws["H3"], W16[3], bias=b[3], out_f32=ws["L"], **kw)
+        ws["loss"].zero_()
+        _check("rt_softmax_xent", _abi.lib().rt_softmax_xent(_p(ws["L"]), G * B, self.classes, _p(labels), 1.0 / B, _p(ws["G"]),
+                                                              _p(ws["loss"]), _stream(stream)))
+        transpose_grouped(ws["G"], G, ws["GT"], stream=stream)
+        gW, gb = self.grads[0::2], self.grads[1::2]
+        gemm(ws["GT"], ws["H3T"], out_f32=gW[3], **kw)
+        colsum_grouped(ws["G"], G, gb[3], stream=stream)
+        gemm(ws["G"], W16t[3], mask=ws["H3"], out_bf16=ws["D3"], out_t=ws["D3T"], **kw)
+        gemm(ws["D3T"], ws["H2T"], out_f32=gW[2], **kw)
+        colsum_grouped(ws["D3"], G, gb[2], stream=stream)
+        gemm(ws["D3"], W16t[2], mask=ws["H2"], out_bf16=ws["D2"], out_t=ws["D2T"], **kw)
+        gemm(ws["D2T"], ws["H1T"], out_f32=gW[1], **kw)
+        colsum_grouped(ws["D2"], G, gb[1], stream=stream)
+        gemm(ws["D2"], W16t[1], mask=ws["H1"], out_bf16=ws["D1"], out_t=ws["D1T"], **kw)
+        gemm(ws["D1T"], ws["XT"], out_f32=gW[0], **kw)
+        colsum_grouped(ws["D1"], G, gb[0], stream=stream)
+        return ws["loss"]
+
+    def adam(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, stream=None):
+        self.step_count += 1
+        for i, (p, g, m, v) in enumerate(zip(self.params, self.grads, self.m, self.v)):
+            d = _abi.AdamDesc()
+            d.param, d.grad, d.m, d.v = p.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr()
+            if p.dim() == 2:
+                d.rows, d.cols = p.shape
+                d.groups = self.groups
+                w16, w16t = self.W16[i // 2], self.W16t[i // 2]
+                d.out_bf16, d.ld_bf16 = w16.data_ptr(), w16.stride(0)
+                d.out_bf16_t, d.ld_bf16_t = w16t.data_ptr(), w16t.stride(0)
+            else:
+                d.rows, d.cols = 1, p.shape[0]
+            d.lr, d.beta1, d.beta2, d.eps, d.step = lr, beta1, beta2, eps, self.step_count
+            _check("rt_adam_step", _abi.lib().rt_adam_step(C.byref(d), _stream(stream)))
+
+    def train_step(self, orig, dir, labels, box, batch: int, lr=1e-3, stream=None):
+        loss = self.forward_backward(orig, dir, labels, box, batch, stream=stream)
+        self.adam(lr=lr, stream=stream)
+        return loss
+
+    def fine_tune(self, orig, dir, labels, box, group_rays: int, steps: int, batch: int, lr=1e-3, offset: int = 0, stream=None):
+        """`steps` Adam steps; step j trains group g on its rays
+        g * group_rays + (offset + j * batch + b) % group_rays, b < batch."""
+        ws = self._workspace(batch, True)
+        out = (ws["bo"], ws["bd"], ws["bl"])
+        loss = None
+        for j in range(steps):
+            gather_batch(orig, dir, labels, self.groups, group_rays, offset + j * batch, batch, out, stream=stream)
+            loss = self.train_step(out[0], out[1], out[2], box, batch, lr=lr, stream=stream)
+        return loss
+
+    def propose(self, orig, dir, box, group_rays: int, out=None, min_margin: float = 0.0, chunk_rows: int = 1 << 22, stream=None):
+        """Slot proposal per ray; group g's rays are rows g * group_rays ..
+        (group_rays % 128 == 0), scored by group g's network."""
+        G = self.groups
+        if group_rays % 128 or orig.shape[0] != G * group_rays:
+            raise ValueError("need groups * group_rays rays with group_rays % 128 == 0")
+        if out is None:
+            out = torch.empty(G * group_rays, dtype=torch.int32, device=orig.device)
+        cg = max(1, min(G, chunk_rows // group_rays))
+        ws = self._workspace(cg * group_rays, False)
+        for g0 in range(0, G, cg):
+            g1 = min(G, g0 + cg)
+            ng, r0, r1 = g1 - g0, g0 * group_rays, g1 * group_rays
+            X, H1, H2, H3 = (ws[k][:r1 - r0] for k in ("X", "H1", "H2", "H3"))
+            ray_features(orig[r0:r1], dir[r0:r1], box, out=X, stream=stream)
+            wv = [w[g0 * (w.shape[0] // G): g1 * (w.shape[0] // G)] for w in self.W16]
+            bv = [b[g0 * (b.shape[0] // G): g1 * (b.shape[0] // G)] for b in self.b]
+            kw = dict(err=self.err, groups=ng, stream=stream)
+            gemm(X, wv[0], bias=bv[0], relu=True, out_bf16=H1, **kw)
+            gemm(H1, wv[1], bias=bv[1], relu=True, out_bf16=H2, **kw)
+            gemm(H2, wv[2], bias=bv[2], relu=True, out_bf16=H3, **kw)
+            gemm_argmax(H3, wv[3], bias=bv[3], out_index=out[r0:r1], min_margin=min_margin, **kw)
+        return out
+
+
 # ----------------------------------------------------------------- tree side
 def subtree_slots(tree: Tree, depth: int = DEPTH, stream=None) -> dict:
     """Slot table of a built tree: slot_ref (2^depth blob references), pos_label
@@ -292,4 +473,46 @@ def trace_seeded(tree: Tree, orig, dir, proposal, slots: dict, tmax=None, id_mod
         out["in_proposal"] = torch.empty(orig.shape[0], dtype=torch.int32, device=orig.device)
         s.in_proposal = out["in_proposal"].data_ptr()
     _check("rt_trace_closest_seeded", _abi.lib().rt_trace_closest_seeded(C.byref(d), C.byref(s), _stream(stream)))
+    return out
+
+
+# ----------------------------------------------------------- batched meshes
+def batch_subtree_slots(tree, depth: int = DEPTH, stream=None) -> dict:
+    """Per-mesh slot tables of a core.batch_build tree: slot_ref (M, 2^depth),
+    slot_box (M, 2^depth, 8), pos_label (global face position -> mesh-local slot)."""
+    M, N = tree.mesh_count, tree.faces.shape[0]
+    dev = tree.faces.device
+    S = 1 << depth
+    out = dict(slot_ref=torch.empty((M, S), dtype=torch.int32, device=dev), slot_box=torch.empty((M, S, 8), dtype=torch.float32, device=dev),
+               pos_label=torch.empty(N, dtype=torch.int32, device=dev))
+    d = _abi.BatchSlotDesc()
+    d.mesh_count, d.face_offsets, d.nodes, d.accel = M, tree.face_offsets.data_ptr(), tree.nodes.data_ptr(), tree.accel.data_ptr()
+    d.face_count, d.depth = N, depth
+    d.slot_ref, d.slot_box, d.pos_label = out["slot_ref"].data_ptr(), out["slot_box"].data_ptr(), out["pos_label"].data_ptr()
+    _check("rt_batch_subtree_slots", _abi.lib().rt_batch_subtree_slots(C.byref(d), _stream(stream)))
+    return out
+
+
+def batch_hit_labels(tree, hit_pos, ray_offsets, pos_label, out=None, stream=None):
+    if out is None:
+        out = torch.empty_like(hit_pos)
+    _check("rt_batch_hit_labels", _abi.lib().rt_batch_hit_labels(_p(hit_pos), hit_pos.shape[0], tree.mesh_count, _p(ray_offsets),
+                                                                  _p(tree.face_offsets), _p(pos_label), _p(out), _stream(stream)))
+    return out
+
+
+def batch_trace_seeded(tree, orig, dir, ray_offsets, proposal, slots: dict, tmax=None, id_mode: int = 0, counters: bool = False,
+                       in_proposal: bool = False, while_while: bool = True, box_test: bool = True, out: dict | None = None,
+                       stream=None) -> dict:
+    """core.batch_trace with each ray's proposed subtree (of its own mesh) walked first; same outputs, bit for bit."""
+    from .core import batch_trace_desc
+    d, out = batch_trace_desc(tree, orig, dir, ray_offsets, tmax, id_mode, counters, while_while, out)
+    s = _abi.SeedDesc()
+    s.proposal, s.slot_ref, s.slot_count = proposal.data_ptr(), slots["slot_ref"].data_ptr(), slots["slot_ref"].shape[1]
+    if box_test:
+        s.slot_box = slots["slot_box"].data_ptr()
+    if in_proposal:
+        out["in_proposal"] = torch.empty(orig.shape[0], dtype=torch.int32, device=orig.device)
+        s.in_proposal = out["in_proposal"].data_ptr()
+    _check("rt_batch_trace_seeded", _abi.lib().rt_batch_trace_seeded(C.byref(d), C.byref(s), _stream(stream)))
     return out

@@ -163,6 +163,32 @@ def learned_scene(scale: float = 1.0, seed: int = 4):
     return concat(t, s)
 
 
+def instance_cameras(count: int, width: int, height: int, radius: float = 2.4, y: float = 1.3, target=(0.0, 0.2, 0.0)):
+    """One pinhole camera per instance of the instanced learned scene, on a
+    ring of `radius` around the scene at height y, each looking at `target`."""
+    cams = []
+    for i in range(count):
+        a = 2.0 * math.pi * (i + 0.5) / count
+        cams.append(Camera((radius * math.cos(a), y, radius * math.sin(a)), tuple(target), FOV_60, width, height))
+    return cams
+
+
+def displace_instances(base_vertices, count: int, frame: int, seed: int = 7, sigma: float = 0.002, out=None):
+    """`count` copies of a device vertex array (float4), each vertex moved by
+    N(0, sigma^2) per axis, drawn on the device from a generator seeded by
+    (seed, frame): instance i is rows i V .. (i + 1) V of the result."""
+    import torch
+
+    V = base_vertices.shape[0]
+    dev = base_vertices.device
+    g = torch.Generator(device=dev).manual_seed(seed * 1_000_003 + frame)
+    if out is None:
+        out = torch.empty((count * V, 4), dtype=torch.float32, device=dev)
+    out.view(count, V, 4).copy_(base_vertices.unsqueeze(0).expand(count, V, 4))
+    out[:, :3] += sigma * torch.randn((count * V, 3), generator=g, device=dev)
+    return out
+
+
 def scene_box(mesh: Mesh, factor: float = 1.5):
     """The mesh's bounding box grown by `factor` about its centre (lo xyz, hi xyz)."""
     v = mesh.vertices[:, :3].astype(np.float64)

@@ -11,6 +11,12 @@
  * sin/cos(pi 2^j u), j < 12 (144 features, zero-padded to 192) -> 3 x 128 ReLU
  * -> 2^depth logits. BF16 weights [out][in], FP32 biases, FP32 accumulation on
  * the tensor cores (tcgen05, TMA, tensor memory).
+ *
+ * Groups: several independent networks (one per mesh of a batched build) run
+ * in the same launches. A grouped operand stacks the groups' matrices along
+ * its rows (group g's rows follow group g - 1's); every group has the same
+ * shape. Group g's results equal, bit for bit, an ungrouped call on group g's
+ * rows alone.
  */
 #ifndef RT_PROPOSE_H
 #define RT_PROPOSE_H
@@ -21,13 +27,17 @@
 extern "C" {
 #endif
 
-#define RT_PROPOSE_ABI_VERSION 1u
+#define RT_PROPOSE_ABI_VERSION 2u
 uint32_t rt_propose_abi_version(void);
 
 /* C = alpha * A * B^T (+ bias[n]) (ReLU) (* (mask > 0)), on the tensor cores.
  * A: BF16 [m][lda], B: BF16 [n][ldb], both K-major. m % 128 == 0, k % 64 == 0,
  * n % 16 == 0; lda, ldb multiples of 8; pointers 16-byte aligned. Outputs (any
- * subset): FP32 [m][ldc_f32], BF16 [m][ldc_bf16], BF16 transposed [n][ldct]. */
+ * subset): FP32 [m][ldc_f32], BF16 [m][ldc_bf16], BF16 transposed [n][ldct].
+ * groups > 1: C_g = A_g B_g^T for g < groups with A [groups m][lda],
+ * B [groups n][ldb], bias [groups n], mask and C [groups m][.], and C^T
+ * [groups n][ldct] (group g's transpose in rows g n .. g n + n - 1, columns
+ * 0 .. m - 1). */
 typedef struct rt_gemm_desc {
   const void* a;
   uint32_t lda;
@@ -46,13 +56,16 @@ typedef struct rt_gemm_desc {
   void* ct_bf16;
   uint32_t ldct;
   uint32_t* error_word; /* optional: RT_DEVERR_WAIT_TIMEOUT */
+  uint32_t groups;      /* 0 or 1: one product */
 } rt_gemm_desc;
 rt_status rt_gemm_bf16(const rt_gemm_desc* d, rt_stream stream);
 
 /* out_index[i] = argmax_j (A B^T + bias)[i][j] (lowest j among equal maxima),
  * out_value[i] = that maximum, out_margin[i] = maximum - second largest value;
  * out_index[i] = -1 when the margin is below min_margin. The m x n logits are
- * never stored. m % 128 == 0, n % 256 == 0, n <= 4096, k % 64 == 0, k <= 256. */
+ * never stored. m % 128 == 0, n % 256 == 0, n <= 4096, k % 64 == 0, k <= 256.
+ * groups > 1: A [groups m], B [groups n], bias [groups n], outputs [groups m];
+ * a row of group g is scored against group g's n rows of B (indices 0 .. n - 1). */
 typedef struct rt_gemm_argmax_desc {
   const void* a;
   uint32_t lda;
@@ -65,6 +78,7 @@ typedef struct rt_gemm_argmax_desc {
   float* out_value;  /* optional */
   float* out_margin; /* optional */
   uint32_t* error_word;
+  uint32_t groups; /* 0 or 1: one product */
 } rt_gemm_argmax_desc;
 rt_status rt_gemm_argmax_bf16(const rt_gemm_argmax_desc* d, rt_stream stream);
 
@@ -72,7 +86,9 @@ rt_status rt_gemm_argmax_bf16(const rt_gemm_argmax_desc* d, rt_stream stream);
  * f[24 i + 2 j] = sin(pi 2^j u_i), f[24 i + 2 j + 1] = cos(pi 2^j u_i), j < 12;
  * columns 144 .. 191 are zero. out: BF16 [count][ld_out] (ld_out >= 192, a
  * multiple of 8; 16-byte aligned); out_t: BF16 [192][ld_out_t] (rows 144..191
- * zero). */
+ * zero). group_rows > 0 (count % group_rows == 0): out_t holds one transpose
+ * per group of group_rows rays, group g in rows 192 g .. 192 g + 191, columns
+ * 0 .. group_rows - 1 (ld_out_t >= group_rows). */
 typedef struct rt_feature_desc {
   const float* orig; /* float4 per ray */
   const float* dir;  /* float4 per ray */
@@ -82,6 +98,7 @@ typedef struct rt_feature_desc {
   uint32_t ld_out;
   void* out_t;
   uint32_t ld_out_t;
+  uint32_t group_rows; /* 0: one group of count rays */
 } rt_feature_desc;
 rt_status rt_ray_features(const rt_feature_desc* d, rt_stream stream);
 
@@ -92,8 +109,30 @@ rt_status rt_softmax_xent(const float* logits, uint32_t rows, uint32_t cols, con
                           float* loss_sum, rt_stream stream);
 /* out[c][r] = in[r][c] (BF16). */
 rt_status rt_transpose_bf16(const void* in, uint32_t rows, uint32_t cols, uint32_t ld_in, void* out, uint32_t ld_out, rt_stream stream);
-/* out[c] = sum_r in[r][c] (BF16 in, FP32 out; out is overwritten). */
+/* out[c] = sum_r in[r][c] (BF16 in, FP32 out; out is overwritten; the
+ * summation order is fixed, so the result is deterministic). */
 rt_status rt_colsum_bf16(const void* in, uint32_t rows, uint32_t cols, uint32_t ld, float* out, rt_stream stream);
+/* Grouped forms: group g's input rows are g rows .. g rows + rows - 1; its
+ * output rows (transpose) are g cols .. g cols + cols - 1, and its column sums
+ * out[g cols + c]. */
+rt_status rt_transpose_bf16_grouped(const void* in, uint32_t groups, uint32_t rows, uint32_t cols, uint32_t ld_in, void* out,
+                                    uint32_t ld_out, rt_stream stream);
+rt_status rt_colsum_bf16_grouped(const void* in, uint32_t groups, uint32_t rows, uint32_t cols, uint32_t ld, float* out,
+                                 rt_stream stream);
+
+/* Training batch of grouped networks: row g batch + b of the outputs is input
+ * row g group_stride + (offset + b) % group_stride (origin, direction, label),
+ * so that each group trains on a window of its own rays. */
+typedef struct rt_batch_gather_desc {
+  const float* orig; /* float4 per ray */
+  const float* dir;
+  const int32_t* labels;
+  uint32_t groups, group_stride, offset, batch;
+  float* out_orig;
+  float* out_dir;
+  int32_t* out_labels;
+} rt_batch_gather_desc;
+rt_status rt_gather_batch(const rt_batch_gather_desc* d, rt_stream stream);
 
 /* One Adam step (bias-corrected, step >= 1) on FP32 parameters [rows][cols];
  * refreshes BF16 copies [rows][ld_bf16] and [cols][ld_bf16_t] when given. */
@@ -109,6 +148,7 @@ typedef struct rt_adam_desc {
   uint32_t ld_bf16;
   void* out_bf16_t;
   uint32_t ld_bf16_t;
+  uint32_t groups; /* > 1: rows hold groups stacked matrices; out_bf16_t holds their transposes stacked (group g in rows g cols ..) */
 } rt_adam_desc;
 rt_status rt_adam_step(const rt_adam_desc* d, rt_stream stream);
 
@@ -148,6 +188,36 @@ typedef struct rt_seed_desc {
   int32_t* in_proposal; /* optional [ray_count]: 1 when the final hit lies in the proposed subtree */
 } rt_seed_desc;
 rt_status rt_trace_closest_seeded(const rt_trace_desc* d, const rt_seed_desc* s, rt_stream stream);
+
+/* Batched forms over the trees of rt_batch_build (mesh m: faces
+ * face_offsets[m] .. face_offsets[m + 1], rays ray_offsets[m] .. ray_offsets[m + 1]).
+ * Slot tables are per mesh: slot_ref [mesh_count][2^depth], slot_box
+ * [mesh_count][2^depth][8], slot_first / slot_count likewise; pos_label is
+ * indexed by the global face position and holds mesh-local slots. */
+typedef struct rt_batch_slot_desc {
+  uint32_t mesh_count;
+  const uint32_t* face_offsets; /* DEVICE [mesh_count + 1] */
+  const uint32_t* nodes;        /* of rt_batch_build */
+  const void* accel;            /* of rt_batch_build */
+  uint32_t face_count;          /* total */
+  uint32_t depth;
+  int32_t* slot_ref;
+  float* slot_box;   /* optional */
+  int32_t* pos_label; /* optional [face_count] */
+  uint32_t* slot_first; /* optional */
+  uint32_t* slot_count; /* optional */
+} rt_batch_slot_desc;
+rt_status rt_batch_subtree_slots(const rt_batch_slot_desc* d, rt_stream stream);
+
+/* labels[r] = pos_label[face_offsets[m] + hit_pos[r]] for the rays r of mesh m
+ * that hit (mesh-local positions, as rt_batch_trace writes them), -1 for misses. */
+rt_status rt_batch_hit_labels(const int32_t* hit_pos, uint32_t ray_count, uint32_t mesh_count, const uint32_t* ray_offsets,
+                              const uint32_t* face_offsets, const int32_t* pos_label, int32_t* labels, rt_stream stream);
+
+/* rt_batch_trace where ray r of mesh m first walks the subtree
+ * slot_ref[m slot_count + proposal[r]] (s->slot_ref, s->slot_box per mesh as
+ * above); outputs bit-identical to rt_batch_trace's. */
+rt_status rt_batch_trace_seeded(const rt_batch_trace_desc* d, const rt_seed_desc* s, rt_stream stream);
 
 #ifdef __cplusplus
 }

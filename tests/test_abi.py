@@ -86,3 +86,48 @@ def test_camera_host_math_matches_oracle(oracle, scene):
     basis = np.array(core.camera_basis(c, cam.width, cam.height), np.float32)
     ob = oracle.camera_basis(cam.center, ang, cam.fov, cam.ratio, cam.width, cam.height)
     assert np.array_equal(basis.view(np.uint32), ob.view(np.uint32))
+
+
+_STRUCTS = {  # C typedef -> ctypes mirror in cudart_b200._abi
+    "rt_build_params": "BuildParams", "rt_build_info": "BuildInfo", "rt_build_desc": "BuildDesc", "rt_trace_desc": "TraceDesc",
+    "rt_interp_desc": "InterpDesc", "rt_mesh_file": "MeshFile", "rt_tree_file": "TreeFile", "rt_batch_build_desc": "BatchBuildDesc",
+    "rt_batch_trace_desc": "BatchTraceDesc", "rt_sah_desc": "SahDesc", "rt_raster_desc": "RasterDesc", "rt_gemm_desc": "GemmDesc",
+    "rt_gemm_argmax_desc": "GemmArgmaxDesc", "rt_feature_desc": "FeatureDesc", "rt_adam_desc": "AdamDesc", "rt_slot_desc": "SlotDesc",
+    "rt_seed_desc": "SeedDesc", "rt_batch_gather_desc": "BatchGatherDesc", "rt_batch_slot_desc": "BatchSlotDesc", "rt_camera": "Camera",
+}
+
+
+def test_struct_layouts_match_headers(tmp_path):
+    """Every ctypes mirror has the C struct's size and each field's offset
+    (a C probe compiled with gcc against include/*.h prints them)."""
+    import shutil
+    import subprocess
+
+    from cudart_b200 import _abi
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "rt_core.h"', '#include "rt_sah.h"', '#include "rt_raster.h"',
+             '#include "rt_propose.h"', "int main(void) {"]
+    for cname, pyname in _STRUCTS.items():
+        st = getattr(_abi, pyname)
+        lines.append(f'  printf("{pyname} size %zu\\n", sizeof({cname}));')
+        for f in st._fields_:
+            lines.append(f'  printf("{pyname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "probe"
+    inc = os.path.join(ROOT, "include")
+    r = subprocess.run(["gcc", "-std=c11", "-I", inc, str(src), "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {}
+    for ln in out:
+        if ln:
+            py, field, val = ln.split()
+            got[(py, field)] = int(val)
+    for pyname in _STRUCTS.values():
+        st = getattr(_abi, pyname)
+        assert got[(pyname, "size")] == C.sizeof(st), pyname
+        for f in st._fields_:
+            assert got[(pyname, f[0])] == getattr(st, f[0]).offset, (pyname, f[0])
