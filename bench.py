@@ -52,6 +52,11 @@ def parse():
     ap.add_argument("--sah", type=int, default=1, help="also time the SAH and Hybrid builds and tracing through their trees")
     ap.add_argument("--raster", type=int, default=1, help="also time the rasteriser on the same frame")
     ap.add_argument("--learned-scale", type=float, default=1.0, help="triangle-count scale of the learned-proposal scene")
+    ap.add_argument("--instanced", type=int, default=1,
+                    help="also time the instanced workload: 64 deformed copies of the learned scene rebuilt every frame, "
+                         "per-instance networks fine-tuned on the previous frame")
+    ap.add_argument("--instanced-frames", type=int, default=16)
+    ap.add_argument("--instanced-count", type=int, default=64)
     return ap.parse_args()
 
 
@@ -290,6 +295,8 @@ def run_ours(args, rank, world, local_rank):
         result["raster"] = raster_leg(dev, world, cam, tree, v, W, H)
     if args.learned:
         result["nn_proposal_c3"] = learned(args, dev, world)
+    if args.instanced:
+        result["instanced_c4"] = instanced(args, dev, world)
     clocks = clk.summary()
     sampler.stop()
     result["clocks"] = {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
@@ -636,6 +643,84 @@ def learned(args, dev, world, train_rays=16 << 20, eval_rays=8 << 20, batch=8192
                                 "visits_ratio": round(best["visits"].sum().item() / vp, 4),
                                 "tests_ratio": round(best["tests"].sum().item() / tp, 4)},
             "mean_visits_plain": round(vp / R, 3), "mean_tests_plain": round(tp / R, 3)}
+
+
+def instanced(args, dev, world, scale=1 / 16, width=960, height=540, steps=200, batch=1024, lr=1e-3):
+    """Instanced frames: `count` (64) copies of the learned scene at 1/16 size
+    (251,518 triangles each, 16.1M per frame), every vertex moved by fresh
+    N(0, 0.002^2) noise each frame and all copies rebuilt by one batched LBVH
+    build. Each copy renders a 480 x 270 tile of a 3840 x 2160 frame at 4
+    samples per pixel (its own camera at 960 x 540: a regular 2 x 2 sub-pixel
+    grid), plus one diffuse bounce per hit. Each copy has its own proposal
+    network, fine-tuned every frame for `steps` grouped Adam steps of `batch`
+    rays on the previous frame's plain-traversal labels. Per frame, timed on
+    the device: the build, the fine-tuning, the plain traversal (primaries +
+    bounces) and the learned one (grouped MLP proposals + seeded traversal),
+    side by side; hits compared bit for bit every frame."""
+    import torch
+
+    from cudart_b200.instances import InstancedFrames
+
+    count, frames = args.instanced_count, args.instanced_frames
+    w = InstancedFrames(count, scale, width, height, device=dev, batch=batch, steps=steps, lr=lr)
+    # frame 0 (untimed): labels for frame 1, workspaces, first launches
+    w.displace(0)
+    w.build()
+    w.make_slots()
+    plain = w.trace_plain()
+    learned = w.trace_learned()
+    w.remember(plain)
+    w.fine_tune(steps=2)
+    torch.cuda.synchronize()
+    R = w.ray_count
+    ev = []
+    mism = torch.zeros(1, dtype=torch.int64, device=dev)
+    active = torch.zeros(1, dtype=torch.int64, device=dev)
+    inprop = torch.zeros(2, dtype=torch.int64, device=dev)
+    loss0 = loss1 = None
+    for f in range(1, frames + 1):
+        w.displace(f)  # the frame's input (untimed)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+        e[0].record()
+        w.build()
+        w.make_slots()
+        e[1].record()
+        loss = w.fine_tune()
+        e[2].record()
+        w.trace_plain(out=plain)
+        e[3].record()
+        w.trace_learned(out=learned, in_proposal=True)
+        e[4].record()
+        for k in ("h1", "h2"):
+            mism += (plain[k]["id"] != learned[k]["id"]).sum() + (plain[k]["t"].view(torch.int32) != learned[k]["t"].view(torch.int32)).sum()
+            mism += (plain[k]["uv"].view(torch.int32) != learned[k]["uv"].view(torch.int32)).sum()
+            hit = plain[k]["id"] >= 0
+            inprop[0] += (learned[k]["in_proposal"].bool() & hit).sum()
+            inprop[1] += hit.sum()
+        active += (plain["b"][2] > 0).sum()
+        if f == 1:
+            loss0 = loss.clone() / count
+        loss1 = loss.clone() / count
+        w.remember(plain)
+        e[5].record()
+        ev.append(e)
+    torch.cuda.synchronize()
+    build_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
+    tune_ms = sum(e[1].elapsed_time(e[2]) for e in ev)
+    plain_ms = sum(e[2].elapsed_time(e[3]) for e in ev)
+    nn_ms = sum(e[3].elapsed_time(e[4]) for e in ev)
+    rays = frames * R + int(active.item())  # primaries + active bounces
+    F = w.face_count
+    return {"instances": count, "faces_per_frame": F, "frames": frames, "tile": [width // 2, height // 2], "spp": 4,
+            "primary_rays_per_frame": R, "rays_timed": rays, "finetune_steps_per_frame": steps, "batch_per_instance": batch,
+            "build_ms_per_frame": round(build_ms / frames, 3), "build_mtri_s": round(world * F * frames / (build_ms * 1e-3) / 1e6, 1),
+            "finetune_ms_per_frame": round(tune_ms / frames, 3),
+            "plain_ms_per_frame": round(plain_ms / frames, 3), "plain_mrays_s": round(world * rays / (plain_ms * 1e-3) / 1e6, 2),
+            "nn_ms_per_frame": round(nn_ms / frames, 3), "nn_mrays_s": round(world * rays / (nn_ms * 1e-3) / 1e6, 2),
+            "nn_over_plain": round(plain_ms / nn_ms, 4), "bit_exact": int(mism.item()) == 0,
+            "proposal_accuracy": round(int(inprop[0].item()) / max(1, int(inprop[1].item())), 4),
+            "loss_first_frame": round(float(loss0.item()), 4), "loss_last_frame": round(float(loss1.item()), 4),
+            "frame_ms": round(sum(e[0].elapsed_time(e[4]) for e in ev) / frames, 3)}
 
 
 def run_e2e(args, mesh, camera, W, H, dev, world, sched1=None, sched2=None):

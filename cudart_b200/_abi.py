@@ -41,6 +41,7 @@ PROPOSE_EXPORTS = (
     "rt_propose_abi_version", "rt_gemm_bf16", "rt_gemm_argmax_bf16", "rt_ray_features", "rt_softmax_xent", "rt_transpose_bf16",
     "rt_colsum_bf16", "rt_adam_step", "rt_subtree_slots", "rt_hit_labels", "rt_trace_closest_seeded", "rt_transpose_bf16_grouped",
     "rt_colsum_bf16_grouped", "rt_gather_batch", "rt_batch_subtree_slots", "rt_batch_hit_labels", "rt_batch_trace_seeded",
+    "rt_group_select",
 )
 
 _P = C.c_void_p
@@ -153,7 +154,8 @@ class SeedDesc(C.Structure):
 
 class BatchGatherDesc(C.Structure):
     _fields_ = [("orig", _P), ("dir", _P), ("labels", _P), ("groups", _U32), ("group_stride", _U32), ("offset", _U32),
-                ("batch", _U32), ("out_orig", _P), ("out_dir", _P), ("out_labels", _P)]
+                ("batch", _U32), ("out_orig", _P), ("out_dir", _P), ("out_labels", _P), ("index", _P), ("index_count", _P),
+                ("hop", _U32)]
 
 
 class BatchSlotDesc(C.Structure):
@@ -221,6 +223,7 @@ def lib():
         L.rt_transpose_bf16_grouped.argtypes = [_P, _U32, _U32, _U32, _U32, _P, _U32, _P]
         L.rt_colsum_bf16_grouped.argtypes = [_P, _U32, _U32, _U32, _U32, _P, _P]
         L.rt_gather_batch.argtypes = [C.POINTER(BatchGatherDesc), _P]
+        L.rt_group_select.argtypes = [_P, _U32, _U32, _P, _P, _P]
         L.rt_batch_subtree_slots.argtypes = [C.POINTER(BatchSlotDesc), _P]
         L.rt_batch_hit_labels.argtypes = [_P, _U32, _U32, _P, _P, _P, _P, _P]
         L.rt_batch_trace_seeded.argtypes = [C.POINTER(BatchTraceDesc), C.POINTER(SeedDesc), _P]

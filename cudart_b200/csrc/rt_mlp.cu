@@ -483,19 +483,57 @@ __global__ __launch_bounds__(256) void k_colsum_bf16(const __nv_bfloat16* __rest
   }
 }
 
-// Row g batch + b <- row g stride + (offset + b) % stride.
+// Row g batch + b <- row g stride + q, q from a strided walk of the group's
+// rows (or of its index list).
 __global__ __launch_bounds__(256) void k_gather_batch(const float4* __restrict__ orig, const float4* __restrict__ dir,
                                                       const int32_t* __restrict__ labels, uint32_t groups, uint32_t stride,
-                                                      uint32_t offset, uint32_t batch, float4* __restrict__ oo, float4* __restrict__ od,
-                                                      int32_t* __restrict__ ol) {
+                                                      uint32_t offset, uint32_t batch, uint32_t hop, const uint32_t* __restrict__ index,
+                                                      const uint32_t* __restrict__ index_count, float4* __restrict__ oo,
+                                                      float4* __restrict__ od, int32_t* __restrict__ ol) {
   const size_t total = (size_t)groups * batch;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const uint32_t g = (uint32_t)(i / batch), b = (uint32_t)(i - (size_t)g * batch);
-    const size_t src = (size_t)g * stride + (uint32_t)(((uint64_t)offset + b) % stride);
+    const uint32_t n = index ? __ldg(index_count + g) : stride;
+    if (n == 0) {
+      oo[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      od[i] = make_float4(0.f, 0.f, 1.f, 0.f);
+      if (ol) ol[i] = -1;
+      continue;
+    }
+    const uint32_t k = (uint32_t)((((uint64_t)offset + b) * hop) % n);
+    const size_t src = (size_t)g * stride + (index ? __ldg(index + (size_t)g * stride + k) : k);
     oo[i] = __ldg(orig + src);
     od[i] = __ldg(dir + src);
     if (labels) ol[i] = __ldg(labels + src);
   }
+}
+
+// One CTA per group: stable compaction of the rows with a label >= 0.
+__global__ __launch_bounds__(1024) void k_group_select(const int32_t* __restrict__ labels, uint32_t stride, uint32_t* __restrict__ index,
+                                                       uint32_t* __restrict__ count) {
+  __shared__ uint32_t s_w[32];
+  const uint32_t g = blockIdx.x;
+  const int32_t* lab = labels + (size_t)g * stride;
+  uint32_t* idx = index + (size_t)g * stride;
+  uint32_t base = 0;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  for (uint32_t c = 0; c < stride; c += 1024) {
+    const uint32_t r = c + threadIdx.x;
+    const bool keep = r < stride && __ldg(lab + r) >= 0;
+    const uint32_t bal = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) s_w[warp] = __popc(bal);
+    __syncthreads();
+    uint32_t before = 0, tot = 0;
+    for (uint32_t w = 0; w < 32; ++w) {
+      const uint32_t x = s_w[w];
+      before += w < warp ? x : 0u;
+      tot += x;
+    }
+    if (keep) idx[base + before + __popc(bal & ((1u << lane) - 1u))] = r;
+    base += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) count[g] = base;
 }
 
 // Adam (bias-corrected) on FP32 parameters [rows][cols]; refreshes the BF16
@@ -696,15 +734,26 @@ extern "C" rt_status rt_colsum_bf16(const void* in, uint32_t rows, uint32_t cols
 }
 
 extern "C" rt_status rt_gather_batch(const rt_batch_gather_desc* d, rt_stream stream) {
-  if (!d || !d->orig || !d->dir || !d->out_orig || !d->out_dir || (d->labels && !d->out_labels) || d->group_stride == 0)
+  if (!d || !d->orig || !d->dir || !d->out_orig || !d->out_dir || (d->labels && !d->out_labels) || d->group_stride == 0 ||
+      (d->index && !d->index_count))
     return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   const size_t total = (size_t)d->groups * d->batch;
   if (total == 0) return RT_OK;
   const uint32_t blocks = (uint32_t)hmin<size_t>((total + 255) / 256, (size_t)num_sms() * 8);
   k_gather_batch<<<blocks, 256, 0, (cudaStream_t)stream>>>((const float4*)d->orig, (const float4*)d->dir, d->labels, d->groups,
-                                                           d->group_stride, d->offset, d->batch, (float4*)d->out_orig,
-                                                           (float4*)d->out_dir, d->out_labels);
+                                                           d->group_stride, d->offset, d->batch, d->hop ? d->hop : 1u, d->index,
+                                                           d->index_count, (float4*)d->out_orig, (float4*)d->out_dir, d->out_labels);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_group_select(const int32_t* labels, uint32_t groups, uint32_t group_stride, uint32_t* index, uint32_t* count,
+                                     rt_stream stream) {
+  if (!labels || !index || !count || groups == 0 || groups > 0x7FFFFFFFu) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  k_group_select<<<groups, 1024, 0, (cudaStream_t)stream>>>(labels, group_stride, index, count);
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;

@@ -26,6 +26,9 @@ import torch
 from . import core, proposal, scenes
 
 
+HOP = 7919  # a prime: consecutive samples of a batch lie far apart in the list of hits
+
+
 class InstancedFrames:
     def __init__(self, count: int, scale: float, width: int, height: int, device="cuda", seed: int = 7, depth: int = proposal.DEPTH,
                  batch: int = 1024, steps: int = 200, lr: float = 1e-3, sigma: float = 0.002, net_seed: int = 0):
@@ -117,25 +120,29 @@ class InstancedFrames:
         return l1, l2
 
     def remember(self, plain):
-        """Keep this frame's rays and labels for the next frame's fine-tuning."""
+        """Keep this frame's rays, labels and per-instance lists of the rays
+        that hit, for the next frame's fine-tuning."""
         l1, l2 = self.labels(plain)
         b = plain["b"]
-        self.prev = (b[0].clone(), b[1].clone(), l1, l2)
+        s1 = proposal.group_select(l1, self.count, self.rays_per_instance)
+        s2 = proposal.group_select(l2, self.count, self.rays_per_instance)
+        self.prev = (b[0].clone(), b[1].clone(), l1, l2, s1, s2)
 
     def fine_tune(self, steps: int | None = None):
-        """Grouped Adam steps on the previous frame's labelled rays: even steps
-        take primary rays, odd steps bounce rays, each a window of `batch` rays
-        per instance advancing by `batch` every second step."""
+        """Grouped Adam steps on the previous frame's rays that hit: even steps
+        take primary rays, odd steps bounce rays; each instance walks its list
+        of hits with a stride of HOP entries, so that a batch spreads over the
+        whole image."""
         if self.prev is None:
             return None
         steps = self.steps if steps is None else steps
-        bo, bd, l1, l2 = self.prev
+        bo, bd, l1, l2, s1, s2 = self.prev
         net, B, R = self.nets, self.batch, self.rays_per_instance
         ws = net._workspace(B, True)
         gb = (ws["bo"], ws["bd"], ws["bl"])
         loss = None
         for j in range(steps):
-            o, d, lab = (self.orig, self.dir, l1) if j % 2 == 0 else (bo, bd, l2)
-            proposal.gather_batch(o, d, lab, self.count, R, (j // 2) * B, B, gb)
+            o, d, lab, sel = (self.orig, self.dir, l1, s1) if j % 2 == 0 else (bo, bd, l2, s2)
+            proposal.gather_batch(o, d, lab, self.count, R, (j // 2) * B, B, gb, index=sel[0], count=sel[1], hop=HOP)
             loss = net.train_step(gb[0], gb[1], gb[2], self.box, B, lr=self.lr)
         return loss

@@ -133,14 +133,28 @@ def colsum_grouped(x: torch.Tensor, groups: int, out: torch.Tensor, stream=None)
                                                                         _stream(stream)))
 
 
-def gather_batch(orig, dir, labels, groups: int, group_stride: int, offset: int, batch: int, out: tuple, stream=None):
-    """Rows g * batch + b <- g * group_stride + (offset + b) % group_stride."""
+def gather_batch(orig, dir, labels, groups: int, group_stride: int, offset: int, batch: int, out: tuple, index=None, count=None,
+                 hop: int = 1, stream=None):
+    """Rows g * batch + b <- g * group_stride + q: q = k, or index[g][k] with an
+    index list (group_select), for k = ((offset + b) * hop) mod n_g."""
     d = _abi.BatchGatherDesc()
     d.orig, d.dir, d.labels = orig.data_ptr(), dir.data_ptr(), _p(labels)
-    d.groups, d.group_stride, d.offset, d.batch = groups, group_stride, offset % group_stride, batch
+    d.groups, d.group_stride, d.offset, d.batch = groups, group_stride, offset % (1 << 32), batch
     d.out_orig, d.out_dir, d.out_labels = out[0].data_ptr(), out[1].data_ptr(), _p(out[2])
+    d.index, d.index_count, d.hop = _p(index), _p(count), hop
     _check("rt_gather_batch", _abi.lib().rt_gather_batch(C.byref(d), _stream(stream)))
     return out
+
+
+def group_select(labels, groups: int, group_stride: int, index=None, count=None, stream=None):
+    """Per group, the rows (ascending) whose label is >= 0, and how many."""
+    dev = labels.device
+    if index is None:
+        index = torch.empty(groups * group_stride, dtype=torch.int32, device=dev)
+    if count is None:
+        count = torch.empty(groups, dtype=torch.int32, device=dev)
+    _check("rt_group_select", _abi.lib().rt_group_select(_p(labels), groups, group_stride, _p(index), _p(count), _stream(stream)))
+    return index, count
 
 
 class ProposalNet:
@@ -323,11 +337,12 @@ class ProposalGroup:
         return n
 
     def _workspace(self, B: int, train: bool):
+        """Training: B rays per group (G B rows); inference: B rows in all."""
         key = (B, train)
         ws = self._ws.get(key)
         if ws is None:
             G, dev, K = self.groups, self.device, self.classes
-            R = G * B
+            R = G * B if train else B
             ws = dict(X=_bf16((R, FEATURES_PAD), dev), H1=_bf16((R, HIDDEN), dev), H2=_bf16((R, HIDDEN), dev), H3=_bf16((R, HIDDEN), dev))
             if train:
                 ws.update(XT=_bf16((G * FEATURES_PAD, B), dev), H1T=_bf16((G * HIDDEN, B), dev), H2T=_bf16((G * HIDDEN, B), dev),

@@ -120,9 +120,12 @@ rt_status rt_transpose_bf16_grouped(const void* in, uint32_t groups, uint32_t ro
 rt_status rt_colsum_bf16_grouped(const void* in, uint32_t groups, uint32_t rows, uint32_t cols, uint32_t ld, float* out,
                                  rt_stream stream);
 
-/* Training batch of grouped networks: row g batch + b of the outputs is input
- * row g group_stride + (offset + b) % group_stride (origin, direction, label),
- * so that each group trains on a window of its own rays. */
+/* Training batch of grouped networks. Row g batch + b of the outputs (origin,
+ * direction, label) is input row g group_stride + q with
+ *   k = ((offset + b) * hop) mod n_g  (hop 0 counts as 1),
+ *   q = index[g group_stride + k], n_g = index_count[g]  with an index list,
+ *   q = k, n_g = group_stride                            without;
+ * a group whose list is empty gives zero rays labelled -1. */
 typedef struct rt_batch_gather_desc {
   const float* orig; /* float4 per ray */
   const float* dir;
@@ -131,8 +134,16 @@ typedef struct rt_batch_gather_desc {
   float* out_orig;
   float* out_dir;
   int32_t* out_labels;
+  const uint32_t* index;       /* optional [groups][group_stride] (rt_group_select) */
+  const uint32_t* index_count; /* [groups], with index */
+  uint32_t hop;
 } rt_batch_gather_desc;
 rt_status rt_gather_batch(const rt_batch_gather_desc* d, rt_stream stream);
+
+/* Per group g: index[g group_stride + k] = the k-th row r (ascending) with
+ * labels[g group_stride + r] >= 0; count[g] = how many. */
+rt_status rt_group_select(const int32_t* labels, uint32_t groups, uint32_t group_stride, uint32_t* index, uint32_t* count,
+                          rt_stream stream);
 
 /* One Adam step (bias-corrected, step >= 1) on FP32 parameters [rows][cols];
  * refreshes BF16 copies [rows][ld_bf16] and [cols][ld_bf16_t] when given. */
