@@ -41,7 +41,7 @@ PROPOSE_EXPORTS = (
     "rt_propose_abi_version", "rt_gemm_bf16", "rt_gemm_argmax_bf16", "rt_ray_features", "rt_softmax_xent", "rt_transpose_bf16",
     "rt_colsum_bf16", "rt_adam_step", "rt_subtree_slots", "rt_hit_labels", "rt_trace_closest_seeded", "rt_transpose_bf16_grouped",
     "rt_colsum_bf16_grouped", "rt_gather_batch", "rt_batch_subtree_slots", "rt_batch_hit_labels", "rt_batch_trace_seeded",
-    "rt_group_select",
+    "rt_group_select", "rt_mlp_propose", "rt_gemm_xent_bf16",
 )
 
 _P = C.c_void_p
@@ -158,6 +158,19 @@ class BatchGatherDesc(C.Structure):
                 ("hop", _U32)]
 
 
+class GemmXentDesc(C.Structure):
+    _fields_ = [("a", _P), ("lda", _U32), ("b", _P), ("ldb", _U32), ("m", _U32), ("n", _U32), ("k", _U32), ("bias", _P), ("labels", _P),
+                ("scale", C.c_float), ("g", _P), ("ldg", _U32), ("gt", _P), ("ldgt", _U32), ("loss_sum", _P), ("error_word", _P),
+                ("groups", _U32)]
+
+
+class MlpProposeDesc(C.Structure):
+    _fields_ = [("orig", _P), ("dir", _P), ("count", _U32), ("box_lo", C.c_float * 3), ("box_hi", C.c_float * 3), ("w1", _P), ("w2", _P),
+                ("w3", _P), ("w4", _P), ("b1", _P), ("b2", _P), ("b3", _P), ("b4", _P), ("n", _U32), ("groups", _U32),
+                ("group_rows", _U32), ("min_margin", C.c_float), ("out_index", _P), ("out_value", _P), ("out_margin", _P),
+                ("error_word", _P)]
+
+
 class BatchSlotDesc(C.Structure):
     _fields_ = [("mesh_count", _U32), ("face_offsets", _P), ("nodes", _P), ("accel", _P), ("face_count", _U32), ("depth", _U32),
                 ("slot_ref", _P), ("slot_box", _P), ("pos_label", _P), ("slot_first", _P), ("slot_count", _P)]
@@ -224,6 +237,8 @@ def lib():
         L.rt_colsum_bf16_grouped.argtypes = [_P, _U32, _U32, _U32, _U32, _P, _P]
         L.rt_gather_batch.argtypes = [C.POINTER(BatchGatherDesc), _P]
         L.rt_group_select.argtypes = [_P, _U32, _U32, _P, _P, _P]
+        L.rt_mlp_propose.argtypes = [C.POINTER(MlpProposeDesc), _P]
+        L.rt_gemm_xent_bf16.argtypes = [C.POINTER(GemmXentDesc), _P]
         L.rt_batch_subtree_slots.argtypes = [C.POINTER(BatchSlotDesc), _P]
         L.rt_batch_hit_labels.argtypes = [_P, _U32, _U32, _P, _P, _P, _P, _P]
         L.rt_batch_trace_seeded.argtypes = [C.POINTER(BatchTraceDesc), C.POINTER(SeedDesc), _P]

@@ -350,8 +350,226 @@ __global__ void __launch_bounds__(kArgThreads, 1)
 }
 
 // ----------------------------------------------------------------------------
+// Logits + softmax cross-entropy gradient: grid (m / 128, groups), 320 threads,
+// the layout of k_gemm_argmax_tc. The logits of a 128-row block are computed
+// twice, never stored: pass 1 keeps each row's running max and sum of
+// exponentials (per half of the columns, merged through shared memory); pass
+// 2 writes g = (softmax - onehot(label)) * scale in BF16, row-major and
+// transposed, and adds the row's loss scale * (log sum - logit[label]).
+// Rows whose label is outside [0, n) get g = 0 and no loss.
+// ----------------------------------------------------------------------------
+struct XentArgs {
+  const float* bias;
+  const int32_t* labels;
+  uint32_t n, gm;
+  float scale;
+  __nv_bfloat16* g;
+  uint32_t ldg;
+  __nv_bfloat16* gt;
+  uint32_t ldgt;
+  float* loss_sum;
+  uint32_t* err;
+};
+
+size_t xent_smem(uint32_t num_k, uint32_t n) {
+  return 1024 + num_k * (size_t)kTileA + kStages * (size_t)kArgTileB + (size_t)n * 4 + kBM * 16 + 16 * 8 + 64;
+}
+
+__global__ void __launch_bounds__(kArgThreads, 1)
+    k_gemm_xent_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, XentArgs X, uint32_t num_k) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + num_k * kTileA;
+  float* s_bias = (float*)(sB + kStages * kArgTileB);
+  float4* s_x = (float4*)(s_bias + X.n);  // per row: (max, sum, logit[label], -) of a column half
+  uint64_t* full = (uint64_t*)(s_x + kBM);
+  uint64_t* empty = full + kStages;
+  uint64_t* a_full = empty + kStages;
+  uint64_t* acc_full = a_full + 1;     // [2]
+  uint64_t* acc_empty = acc_full + 2;  // [2]
+  uint64_t* xch_a = acc_empty + 2;
+  uint64_t* xch_b = xch_a + 1;
+  uint32_t* tmem_slot = (uint32_t*)(xch_b + 1);
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t grp = blockIdx.y, n = X.n;
+  for (uint32_t j = threadIdx.x; j < n; j += kArgThreads) s_bias[j] = X.bias ? X.bias[(size_t)grp * n + j] : 0.0f;
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < kStages; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    mbar_init(a_full, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(acc_full + b, 1);
+      mbar_init(acc_empty + b, 256);
+    }
+    mbar_init(xch_a, 128);
+    mbar_init(xch_b, 128);
+    fence_mbar_init();
+    prefetch_tmap(&ta);
+    prefetch_tmap(&tb);
+  }
+  __syncwarp();
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int32_t m0 = (int32_t)(grp * X.gm + blockIdx.x * kBM);
+  const uint32_t ntiles = n / kArgBN, total_tiles = 2 * ntiles;
+
+  if (warp == 8) {
+    if (lane == 0) {
+      mbar_arrive_expect_tx(a_full, num_k * kTileA);
+      for (uint32_t kc = 0; kc < num_k; ++kc) tma_load_2d(sA + kc * kTileA, &ta, (int32_t)(kc * kBK), m0, a_full);
+      const uint32_t total = total_tiles * num_k;
+      uint32_t q = 0;
+      for (; q < total; ++q) {
+        const uint32_t s = q % kStages;
+        if (q >= kStages && !mbar_wait(empty + s, ((q / kStages) - 1u) & 1u, X.err)) break;
+        const uint32_t t = (q / num_k) % ntiles, kc = q % num_k;
+        mbar_arrive_expect_tx(full + s, kArgTileB);
+        tma_load_2d(sB + s * kArgTileB, &tb, (int32_t)(kc * kBK), (int32_t)(grp * n + t * kArgBN), full + s);
+      }
+      // the latest load of each stage (and A) has landed before the CTA may exit
+      mbar_wait(a_full, 0, X.err);
+      for (uint32_t j = q > kStages ? q - kStages : 0u; j < q; ++j) mbar_wait(full + j % kStages, (j / kStages) & 1u, X.err);
+    }
+  } else if (warp == 9) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16_f32(kBM, kArgBN);
+      bool mok = mbar_wait(a_full, 0, X.err);
+      uint32_t q = 0;
+      for (uint32_t t = 0; mok && t < total_tiles; ++t) {
+        const uint32_t buf = t & 1u;
+        if (t >= 2 && !mbar_wait(acc_empty + buf, ((t >> 1) - 1u) & 1u, X.err)) break;
+        tc_fence_after();
+        const uint32_t d = tmem + buf * kArgBN;
+        for (uint32_t kc = 0; kc < num_k; ++kc, ++q) {
+          const uint32_t s = q % kStages;
+          if (!mbar_wait(full + s, (q / kStages) & 1u, X.err)) { mok = false; break; }
+          tc_fence_after();
+          const uint32_t a = smem_u32(sA + kc * kTileA), b = smem_u32(sB + s * kArgTileB);
+#pragma unroll
+          for (uint32_t kk = 0; kk < kBK / 16; ++kk)
+            mma_bf16(d, desc_sw128(a + kk * 32u), desc_sw128(b + kk * 32u), idesc, (kc | kk) != 0u);
+          mma_commit(empty + s);
+        }
+        if (mok) mma_commit(acc_full + buf);
+      }
+    }
+  } else {
+    const uint32_t qw = warp & 3u, half = warp >> 2;
+    const uint32_t trow = qw * 32u + lane, row = (uint32_t)m0 + trow, rowl = blockIdx.x * kBM + trow;
+    const int32_t lab = X.labels[row];
+    const bool valid = lab >= 0 && lab < (int32_t)n;
+    const uint32_t c0 = half * (kArgBN / 2);
+    float mx = -INFINITY, sum = 0.0f, xl = 0.0f, inv = 0.0f;
+    bool ok = true;
+    for (uint32_t t2 = 0; t2 < total_tiles; ++t2) {
+      const uint32_t buf = t2 & 1u, pass = t2 / ntiles, t = t2 - pass * ntiles;
+      if (t2 == ntiles && ok) {
+        // merge the two column halves of each row: half 1 -> shared -> half 0 -> shared -> half 1
+        if (half == 1) {
+          s_x[trow] = make_float4(mx, sum, xl, 0.0f);
+          mbar_arrive(xch_a);
+          ok = __all_sync(0xffffffffu, mbar_wait(xch_b, 0, X.err));
+          const float4 w = s_x[trow];
+          mx = w.x; sum = w.y;
+        } else {
+          ok = __all_sync(0xffffffffu, mbar_wait(xch_a, 0, X.err));
+          const float4 w = s_x[trow];
+          const float m2 = fmaxf(mx, w.x);
+          sum = sum * __expf(mx - m2) + w.y * __expf(w.x - m2);
+          mx = m2;
+          xl += w.z;  // exactly one half saw the label's column; the other holds 0
+          s_x[trow] = make_float4(mx, sum, 0.0f, 0.0f);
+          mbar_arrive(xch_b);
+          if (valid && X.loss_sum) atomicAdd(X.loss_sum, (logf(sum) + mx - xl) * X.scale);
+        }
+        inv = 1.0f / sum;
+      }
+      ok = ok && __all_sync(0xffffffffu, mbar_wait(acc_full + buf, (t2 >> 1) & 1u, X.err));
+      tc_fence_after();
+      if (ok) {
+        const uint32_t tl = tmem + ((qw * 32u) << 16) + buf * kArgBN + c0;
+        for (uint32_t c = 0; c < kArgBN / 2; c += 16) {
+          float v[16];
+          tmem_ld16(tl + c, v);
+          const uint32_t col = t * kArgBN + c0 + c;
+#pragma unroll
+          for (int i = 0; i < 16; ++i) v[i] += s_bias[col + i];
+          if (pass == 0) {
+            float cm = v[0];
+#pragma unroll
+            for (int i = 1; i < 16; ++i) cm = fmaxf(cm, v[i]);
+            if (cm > mx) {
+              sum *= __expf(mx - cm);
+              mx = cm;
+            }
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              sum += __expf(v[i] - mx);
+              if ((int32_t)(col + i) == lab) xl = v[i];
+            }
+          } else {
+            uint32_t w[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              float p0 = __expf(v[2 * i] - mx) * inv, p1 = __expf(v[2 * i + 1] - mx) * inv;
+              if ((int32_t)(col + 2 * i) == lab) p0 -= 1.0f;
+              if ((int32_t)(col + 2 * i + 1) == lab) p1 -= 1.0f;
+              w[i] = valid ? pack_bf16(p0 * X.scale, p1 * X.scale) : 0u;
+            }
+            uint4* gp = (uint4*)(X.g + (size_t)row * X.ldg + col);
+            gp[0] = make_uint4(w[0], w[1], w[2], w[3]);
+            gp[1] = make_uint4(w[4], w[5], w[6], w[7]);
+            __nv_bfloat16* gt = X.gt + ((size_t)grp * n + col) * X.ldgt + rowl;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              gt[(size_t)(2 * i) * X.ldgt] = __ushort_as_bfloat16((unsigned short)(w[i] & 0xFFFFu));
+              gt[(size_t)(2 * i + 1) * X.ldgt] = __ushort_as_bfloat16((unsigned short)(w[i] >> 16));
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(acc_empty + buf);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 512);
+}
+
+// ----------------------------------------------------------------------------
 // Small kernels
 // ----------------------------------------------------------------------------
+// The six network inputs of a ray: the origin scaled to [-1, 1] over the box
+// (component i < 3), the unit direction (component i < 3 of dir_input).
+__device__ __forceinline__ float origin_input(const float4& o, float3 c, float3 s, uint32_t i) {
+  return i == 0 ? (o.x - c.x) * s.x : (i == 1 ? (o.y - c.y) * s.y : (o.z - c.z) * s.z);
+}
+__device__ __forceinline__ float dir_input(const float4& d, uint32_t i) {
+  const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+  const float inv = len > 0.0f ? 1.0f / len : 0.0f;
+  return (i == 0 ? d.x : (i == 1 ? d.y : d.z)) * inv;
+}
+// w[j] = BF16 pair (sin(pi 2^j x), cos(pi 2^j x)), j < 12.
+__device__ __forceinline__ void encode12(float x, uint32_t (&w)[12]) {
+#pragma unroll
+  for (int j = 0; j < 12; ++j) {
+    float sv, cv;
+    sincospif(x, &sv, &cv);
+    w[j] = pack_bf16(sv, cv);
+    x *= 2.0f;
+  }
+}
+
 // Features of one ray: u = ((o - c) * s, d / |d|); f[24 i + 2 j] = sin(pi 2^j u_i),
 // f[24 i + 2 j + 1] = cos(pi 2^j u_i) for j < 12; columns 144..191 are zero
 // (rows hold ld >= 192 elements). Eight threads per ray: thread i < 6 encodes input i (48 bytes), threads 6
@@ -365,23 +583,7 @@ __global__ __launch_bounds__(256) void k_ray_features(const float4* __restrict__
   if (r >= count) return;
   uint32_t w[12];
   if (i < 6) {
-    float x;
-    if (i < 3) {
-      const float4 o = __ldg(orig + r);
-      x = i == 0 ? (o.x - c.x) * s.x : (i == 1 ? (o.y - c.y) * s.y : (o.z - c.z) * s.z);
-    } else {
-      const float4 d = __ldg(dir + r);
-      const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-      const float inv = len > 0.0f ? 1.0f / len : 0.0f;
-      x = (i == 3 ? d.x : (i == 4 ? d.y : d.z)) * inv;
-    }
-#pragma unroll
-    for (int j = 0; j < 12; ++j) {
-      float sv, cv;
-      sincospif(x, &sv, &cv);
-      w[j] = pack_bf16(sv, cv);
-      x *= 2.0f;
-    }
+    encode12(i < 3 ? origin_input(__ldg(orig + r), c, s, i) : dir_input(__ldg(dir + r), i - 3), w);
   } else {
 #pragma unroll
     for (int j = 0; j < 12; ++j) w[j] = 0u;
@@ -562,6 +764,297 @@ __global__ __launch_bounds__(256) void k_adam(float* __restrict__ p, const float
 }
 
 // ----------------------------------------------------------------------------
+// Fused proposal: features -> 3 x (128, ReLU) -> argmax over n logits for a
+// tile of 128 rays per step, persistent over tiles (grid <= SM count).
+// Warps 0-7 compute (features into shared memory, the hidden layers' bias +
+// ReLU from TMEM back into shared memory as the next layer's A operand, the
+// running top-2 over the logits), warp 8 streams every weight tile through a
+// 3-stage ring with TMA (W1..W3 as 128 x 64 tiles, W4 as 256 x 64), warp 9
+// issues the MMAs. Activations never leave the SM. Shared memory: A (48 KB:
+// X, then H2), B (32 KB: H1, then H3), ring 3 x 32 KB. TMEM: the hidden
+// layers use columns [0, 128); the logits alternate [0, 256) / [256, 512).
+// Every wait is bounded; one that runs out raises the shared abort flag, and
+// every role leaves its tile loop at its next wait.
+// ----------------------------------------------------------------------------
+constexpr uint32_t kFuseThreads = 320;
+constexpr uint32_t kFuseStages = 3;
+constexpr uint32_t kFuseStage = 32768;
+
+struct FuseArgs {
+  const float4* orig;
+  const float4* dir;
+  uint32_t count;
+  float3 c, s;
+  const float* b1;
+  const float* b2;
+  const float* b3;
+  const float* b4;
+  uint32_t n, group_rows, tiles;
+  float min_margin;
+  int32_t* out_idx;
+  float* out_val;
+  float* out_margin;
+  uint32_t* err;
+};
+
+size_t fuse_smem() {
+  return 1024 + 5 * (size_t)kTileA + kFuseStages * (size_t)kFuseStage + kBM * sizeof(Top2) + 16 * 8 + 64;
+}
+
+__global__ void __launch_bounds__(kFuseThreads, 1)
+    k_mlp_propose_tc(const __grid_constant__ CUtensorMap t1, const __grid_constant__ CUtensorMap t2,
+                     const __grid_constant__ CUtensorMap t3, const __grid_constant__ CUtensorMap t4, FuseArgs P) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* sA = smem;                   // 3 atoms of 128 x 64 BF16
+  uint8_t* sB = sA + 3 * kTileA;        // 2 atoms
+  uint8_t* sR = sB + 2 * kTileA;        // ring
+  Top2* s_half = (Top2*)(sR + kFuseStages * kFuseStage);
+  uint64_t* full = (uint64_t*)(s_half + kBM);
+  uint64_t* empty = full + kFuseStages;
+  uint64_t* x_ready = empty + kFuseStages;
+  uint64_t* h_ready = x_ready + 1;
+  uint64_t* lay_done = h_ready + 1;
+  uint64_t* acc_full = lay_done + 1;   // [2]
+  uint64_t* acc_empty = acc_full + 2;  // [2]
+  uint64_t* half_ready = acc_empty + 2;
+  uint64_t* half_free = half_ready + 1;
+  uint64_t* done = half_free + 1;
+  uint32_t* tmem_slot = (uint32_t*)(done + 1);
+  volatile uint32_t* s_abort = tmem_slot + 1;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  if (threadIdx.x == 0) {
+    for (uint32_t q = 0; q < kFuseStages; ++q) {
+      mbar_init(full + q, 1);
+      mbar_init(empty + q, 1);
+    }
+    mbar_init(x_ready, 256);
+    mbar_init(h_ready, 256);
+    mbar_init(lay_done, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(acc_full + b, 1);
+      mbar_init(acc_empty + b, 256);
+    }
+    mbar_init(half_ready, 128);
+    mbar_init(half_free, 128);
+    mbar_init(done, 1);
+    *s_abort = 0u;
+    fence_mbar_init();
+    prefetch_tmap(&t1);
+    prefetch_tmap(&t2);
+    prefetch_tmap(&t3);
+    prefetch_tmap(&t4);
+  }
+  // features 144 .. 191 (atom 2, columns 16 .. 63) stay zero: no tile writes them
+  for (uint32_t i = threadIdx.x; i < kTileA / 16; i += kFuseThreads) ((uint4*)(sA + 2 * kTileA))[i] = make_uint4(0u, 0u, 0u, 0u);
+  fence_proxy_async();
+  __syncwarp();
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t ntiles = P.n / kArgBN;
+  // bounded wait that also honours (and raises) the abort flag
+  auto wait = [&](uint64_t* bar, uint32_t parity) -> bool {
+    if (*s_abort) return false;
+    if (mbar_wait(bar, parity, P.err)) return true;
+    *s_abort = 1u;
+    return false;
+  };
+
+  if (warp == 8) {
+    if (lane == 0) {
+      uint32_t q = 0;
+      bool ok = true;
+      auto load = [&](const CUtensorMap* m, int32_t x, int32_t y, uint32_t bytes) -> bool {
+        const uint32_t st = q % kFuseStages;
+        if (q >= kFuseStages && !wait(empty + st, ((q / kFuseStages) - 1u) & 1u)) return false;
+        mbar_arrive_expect_tx(full + st, bytes);
+        tma_load_2d(sR + st * kFuseStage, m, x, y, full + st);
+        ++q;
+        return true;
+      };
+      for (uint32_t tile = blockIdx.x; ok && tile < P.tiles; tile += gridDim.x) {
+        const uint32_t g = tile * kBM / P.group_rows;
+        for (uint32_t kc = 0; ok && kc < 3; ++kc) ok = load(&t1, (int32_t)(kc * kBK), (int32_t)(g * kBM), kTileA);
+        for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = load(&t2, (int32_t)(kc * kBK), (int32_t)(g * kBM), kTileA);
+        for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = load(&t3, (int32_t)(kc * kBK), (int32_t)(g * kBM), kTileA);
+        for (uint32_t t = 0; ok && t < ntiles; ++t)
+          for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = load(&t4, (int32_t)(kc * kBK), (int32_t)(g * P.n + t * kArgBN), kArgTileB);
+      }
+      // the last load of each stage has landed before the CTA may exit
+      for (uint32_t j = q > kFuseStages ? q - kFuseStages : 0u; j < q; ++j) mbar_wait(full + j % kFuseStages, (j / kFuseStages) & 1u, P.err);
+    }
+  } else if (warp == 9) {
+    if (lane == 0) {
+      const uint32_t id_h = idesc_bf16_f32(kBM, 128), id_l = idesc_bf16_f32(kBM, kArgBN);
+      uint32_t q = 0, xr = 0, hr = 0, n4 = 0;
+      bool ok = true;
+      // one 64-wide K chunk: A atom at a_atom, B from the next ring stage
+      auto chunk = [&](uint32_t d, const uint8_t* a_atom, uint32_t idesc, bool first) -> bool {
+        const uint32_t st = q % kFuseStages;
+        if (!wait(full + st, (q / kFuseStages) & 1u)) return false;
+        tc_fence_after();
+        const uint32_t a = smem_u32(a_atom), b = smem_u32(sR + st * kFuseStage);
+#pragma unroll
+        for (uint32_t kk = 0; kk < kBK / 16; ++kk) mma_bf16(d, desc_sw128(a + kk * 32u), desc_sw128(b + kk * 32u), idesc, (!first || kk) ? 1u : 0u);
+        mma_commit(empty + st);
+        ++q;
+        return true;
+      };
+      for (uint32_t tile = blockIdx.x; ok && tile < P.tiles; tile += gridDim.x) {
+        ok = wait(x_ready, xr++ & 1u);
+        tc_fence_after();
+        for (uint32_t kc = 0; ok && kc < 3; ++kc) ok = chunk(tmem, sA + kc * kTileA, id_h, kc == 0);
+        if (!ok) break;
+        mma_commit(lay_done);
+        ok = wait(h_ready, hr++ & 1u);
+        tc_fence_after();
+        for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = chunk(tmem, sB + kc * kTileA, id_h, kc == 0);
+        if (!ok) break;
+        mma_commit(lay_done);
+        ok = wait(h_ready, hr++ & 1u);
+        tc_fence_after();
+        for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = chunk(tmem, sA + kc * kTileA, id_h, kc == 0);
+        if (!ok) break;
+        mma_commit(lay_done);
+        ok = wait(h_ready, hr++ & 1u);
+        tc_fence_after();
+        for (uint32_t t = 0; ok && t < ntiles; ++t, ++n4) {
+          const uint32_t buf = n4 & 1u;
+          if (n4 >= 2 && !(ok = wait(acc_empty + buf, ((n4 >> 1) - 1u) & 1u))) break;
+          tc_fence_after();
+          for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = chunk(tmem + buf * kArgBN, sB + kc * kTileA, id_l, kc == 0);
+          if (ok) mma_commit(acc_full + buf);
+        }
+      }
+      mma_commit(done);  // arrives when every MMA issued above has completed
+      mbar_wait(done, 0, P.err);
+    }
+  } else {
+    // compute warps 0-7: lane quarter warp % 4 of TMEM, column half warp / 4
+    const uint32_t qw = warp & 3u, half = warp >> 2, tid = threadIdx.x;
+    const uint32_t trow = qw * 32u + lane;  // TMEM lane = tile row of this thread
+    uint32_t ld = 0, n4 = 0, hf = 0;
+    bool ok = true;
+    for (uint32_t tile = blockIdx.x; ok && tile < P.tiles; tile += gridDim.x) {
+      const uint32_t row0 = tile * kBM, g = row0 / P.group_rows;
+      {  // features of ray r = tid % 128: inputs 0-2 (origin) or 3-5 (direction)
+        const uint32_t r = tid & 127u, part = tid >> 7, row = row0 + r;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (row < P.count) v = __ldg((part ? P.dir : P.orig) + row);
+#pragma unroll
+        for (uint32_t i = 0; i < 3; ++i) {
+          uint32_t w[12];
+          encode12(part ? dir_input(v, i) : origin_input(v, P.c, P.s, i), w);
+          const uint32_t f0 = 24u * (3u * part + i);
+#pragma unroll
+          for (uint32_t j = 0; j < 12; ++j) {
+            const uint32_t f = f0 + 2u * j;
+            *(uint32_t*)(sA + (f >> 6) * kTileA + sw128_offset(r, f & 63u)) = w[j];
+          }
+        }
+      }
+      fence_proxy_async();
+      mbar_arrive(x_ready);
+      // hidden layers: bias + ReLU of TMEM columns [64 half, 64 half + 64) into the next A operand
+      for (uint32_t L = 0; L < 3; ++L) {
+        ok = __all_sync(0xffffffffu, wait(lay_done, ld++ & 1u));
+        tc_fence_after();
+        if (!ok) break;
+        uint8_t* dst = L == 1 ? sA : sB;
+        const float* bias = (L == 0 ? P.b1 : (L == 1 ? P.b2 : P.b3)) + (size_t)g * 128u;
+        const uint32_t tl = tmem + ((qw * 32u) << 16) + half * 64u;
+#pragma unroll
+        for (uint32_t c = 0; c < 64; c += 16) {
+          float v[16];
+          tmem_ld16(tl + c, v);
+          const uint32_t col = half * 64u + c;
+          uint32_t w[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const float a = fmaxf(v[2 * i] + __ldg(bias + col + 2 * i), 0.0f);
+            const float b = fmaxf(v[2 * i + 1] + __ldg(bias + col + 2 * i + 1), 0.0f);
+            w[i] = pack_bf16(a, b);
+          }
+          uint8_t* atom = dst + half * kTileA;  // col / 64 == half
+          *(uint4*)(atom + sw128_offset(trow, c)) = make_uint4(w[0], w[1], w[2], w[3]);
+          *(uint4*)(atom + sw128_offset(trow, c + 8u)) = make_uint4(w[4], w[5], w[6], w[7]);
+        }
+        fence_proxy_async();
+        tc_fence_before();
+        mbar_arrive(h_ready);
+      }
+      if (!ok) break;
+      // logits of group g: running top-2 over four interleaved column chains
+      float bk[4], sk[4];
+      int32_t ik[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { bk[k] = -INFINITY; sk[k] = -INFINITY; ik[k] = -1; }
+      const float* b4 = P.b4 + (size_t)g * P.n;
+      for (uint32_t t = 0; t < ntiles; ++t, ++n4) {
+        const uint32_t buf = n4 & 1u;
+        ok = ok && __all_sync(0xffffffffu, wait(acc_full + buf, (n4 >> 1) & 1u));
+        tc_fence_after();
+        if (ok) {
+          const uint32_t c0 = half * (kArgBN / 2);
+          const uint32_t tl = tmem + ((qw * 32u) << 16) + buf * kArgBN + c0;
+          for (uint32_t c = 0; c < kArgBN / 2; c += 16) {
+            float v[16];
+            tmem_ld16(tl + c, v);
+            const uint32_t col = t * kArgBN + c0 + c;
+            const float4* bp = (const float4*)(b4 + col);
+#pragma unroll
+            for (int i4 = 0; i4 < 4; ++i4) {
+              const float4 b = __ldg(bp + i4);
+              const float bb[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                const float x = v[4 * i4 + k] + bb[k];
+                sk[k] = fmaxf(sk[k], fminf(x, bk[k]));
+                if (x > bk[k]) { bk[k] = x; ik[k] = (int32_t)(col + 4 * i4 + k); }
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(acc_empty + buf);
+      }
+      if (!ok) break;
+      Top2 res = Top2{bk[0], sk[0], ik[0]};
+#pragma unroll
+      for (int k = 1; k < 4; ++k) res = top2_merge(res, Top2{bk[k], sk[k], ik[k]});
+      if (half == 1) {
+        if (hf > 0) ok = __all_sync(0xffffffffu, wait(half_free, (hf - 1u) & 1u));
+        if (!ok) break;
+        s_half[trow] = res;
+        mbar_arrive(half_ready);
+      } else {
+        ok = __all_sync(0xffffffffu, wait(half_ready, hf & 1u));
+        if (!ok) break;
+        res = top2_merge(res, s_half[trow]);
+        mbar_arrive(half_free);
+        const uint32_t row = row0 + trow;
+        if (row < P.count) {
+          const float margin = res.best - res.second;
+          P.out_idx[row] = margin >= P.min_margin ? res.idx : -1;
+          if (P.out_val) P.out_val[row] = res.best;
+          if (P.out_margin) P.out_margin[row] = margin;
+        }
+      }
+      ++hf;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 512);
+}
+
+// ----------------------------------------------------------------------------
 // Host side
 // ----------------------------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -667,6 +1160,65 @@ extern "C" rt_status rt_gemm_argmax_bf16(const rt_gemm_argmax_desc* d, rt_stream
   });
   k_gemm_argmax_tc<<<dim3(d->m / kBM, G), kArgThreads, argmax_smem(num_k, d->n), (cudaStream_t)stream>>>(
       ta, tb, d->bias, d->n, d->m, num_k, d->min_margin, d->out_index, d->out_value, d->out_margin, d->error_word);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_gemm_xent_bf16(const rt_gemm_xent_desc* d, rt_stream stream) {
+  if (!d || !d->a || !d->b || !d->labels || !d->g || !d->gt) return RT_ERR_INVALID_ARGUMENT;
+  if (d->m == 0 || d->m % kBM || d->n == 0 || d->n % kArgBN || d->n > kArgMaxN || d->k == 0 || d->k % kBK || d->k > 256)
+    return RT_ERR_INVALID_ARGUMENT;
+  if (d->lda < d->k || d->ldb < d->k || d->lda % 8 || d->ldb % 8 || !aligned16(d->a) || !aligned16(d->b))
+    return RT_ERR_INVALID_ARGUMENT;
+  if (d->ldg < d->n || d->ldg % 8 || !aligned16(d->g) || d->ldgt < d->m) return RT_ERR_INVALID_ARGUMENT;
+  const uint32_t G = d->groups ? d->groups : 1u;
+  if (G > 65535u || (uint64_t)G * d->m > 0x7FFFFFFFull || (uint64_t)G * d->n > 0x7FFFFFFFull) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, d->a, d->k, G * d->m, d->lda, kBM) || !make_map(&tb, d->b, d->k, G * d->n, d->ldb, kArgBN)) return RT_ERR_UNSUPPORTED;
+  XentArgs X;
+  X.bias = d->bias; X.labels = d->labels; X.n = d->n; X.gm = d->m; X.scale = d->scale;
+  X.g = (__nv_bfloat16*)d->g; X.ldg = d->ldg; X.gt = (__nv_bfloat16*)d->gt; X.ldgt = d->ldgt; X.loss_sum = d->loss_sum;
+  X.err = d->error_word;
+  const uint32_t num_k = d->k / kBK;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaFuncSetAttribute(k_gemm_xent_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xent_smem(4, kArgMaxN));
+  });
+  k_gemm_xent_tc<<<dim3(d->m / kBM, G), kArgThreads, xent_smem(num_k, d->n), (cudaStream_t)stream>>>(ta, tb, X, num_k);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_mlp_propose(const rt_mlp_propose_desc* d, rt_stream stream) {
+  if (!d || !d->orig || !d->dir || !d->w1 || !d->w2 || !d->w3 || !d->w4 || !d->b1 || !d->b2 || !d->b3 || !d->b4 || !d->out_index)
+    return RT_ERR_INVALID_ARGUMENT;
+  if (d->n == 0 || d->n % kArgBN || d->n > kArgMaxN) return RT_ERR_INVALID_ARGUMENT;
+  const uint32_t G = d->groups ? d->groups : 1u;
+  if (G > 1 && (d->group_rows == 0 || d->group_rows % kBM || (uint64_t)G * d->group_rows != d->count)) return RT_ERR_INVALID_ARGUMENT;
+  if ((uint64_t)G * d->n > 0x7FFFFFFFull || !aligned16(d->w1) || !aligned16(d->w2) || !aligned16(d->w3) || !aligned16(d->w4) ||
+      !aligned16(d->b4))
+    return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  if (d->count == 0) return RT_OK;
+  CUtensorMap t1, t2, t3, t4;
+  if (!make_map(&t1, d->w1, 192, G * kBM, 192, kBM) || !make_map(&t2, d->w2, 128, G * kBM, 128, kBM) ||
+      !make_map(&t3, d->w3, 128, G * kBM, 128, kBM) || !make_map(&t4, d->w4, 128, G * d->n, 128, kArgBN))
+    return RT_ERR_UNSUPPORTED;
+  FuseArgs P;
+  P.orig = (const float4*)d->orig; P.dir = (const float4*)d->dir; P.count = d->count;
+  P.c = make_float3(0.5f * (d->box_lo[0] + d->box_hi[0]), 0.5f * (d->box_lo[1] + d->box_hi[1]), 0.5f * (d->box_lo[2] + d->box_hi[2]));
+  P.s = make_float3(2.0f / (d->box_hi[0] - d->box_lo[0]), 2.0f / (d->box_hi[1] - d->box_lo[1]), 2.0f / (d->box_hi[2] - d->box_lo[2]));
+  P.b1 = d->b1; P.b2 = d->b2; P.b3 = d->b3; P.b4 = d->b4; P.n = d->n;
+  P.tiles = (d->count + kBM - 1) / kBM;
+  P.group_rows = G > 1 ? d->group_rows : P.tiles * kBM;
+  P.min_margin = d->min_margin; P.out_idx = d->out_index; P.out_val = d->out_value; P.out_margin = d->out_margin; P.err = d->error_word;
+  static std::once_flag once;
+  std::call_once(once, [] { cudaFuncSetAttribute(k_mlp_propose_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fuse_smem()); });
+  const uint32_t grid = (uint32_t)hmin<uint32_t>(P.tiles, (uint32_t)num_sms());
+  k_mlp_propose_tc<<<grid, kFuseThreads, fuse_smem(), (cudaStream_t)stream>>>(t1, t2, t3, t4, P);
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;

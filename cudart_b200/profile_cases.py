@@ -13,6 +13,8 @@ steady-state launch. Cases (kernel of interest in brackets):
   mlp_train      one training step, batch 8192                                   [k_gemm_tc, k_softmax_xent]
   sah_build      SAH build of the 2^20-face soup                                 [k_sah_small, k_huge_bins, k_sah_big]
   raster         rasteriser, 2^20-face soup, 1920x1080                           [k_raster_zones, k_raster_emit]
+  mlp_grouped    64 grouped networks: 3 training steps of 1024 rays each,        [k_gemm_tc, k_softmax_xent, ...]
+                 then proposals for 64 x 518,400 rays
 """
 from __future__ import annotations
 
@@ -97,8 +99,23 @@ def raster():
     torch.cuda.synchronize()
 
 
+def mlp_grouped():
+    from . import proposal, scenes
+    box = (-1.5, -0.6, -1.5, 1.5, 1.4, 1.5)
+    G, B, R = 64, 1024, 518400
+    o, d = scenes.box_rays_torch(G * B, box, seed=1)
+    labels = torch.randint(0, 4096, (G * B,), dtype=torch.int32, device="cuda", generator=torch.Generator(device="cuda").manual_seed(2))
+    net = proposal.ProposalGroup(G, seed=0)
+    for _ in range(3):
+        net.train_step(o, d, labels, box, B)
+    po, pd = scenes.box_rays_torch(G * R, box, seed=3)
+    for _ in range(2):
+        net.propose(po, pd, box, R)
+    torch.cuda.synchronize()
+
+
 CASES = {"trace_primary": trace_primary, "trace_bounce": trace_bounce, "mlp_propose": mlp_propose, "mlp_train": mlp_train,
-         "sah_build": sah_build, "raster": raster}
+         "sah_build": sah_build, "raster": raster, "mlp_grouped": mlp_grouped}
 
 if __name__ == "__main__":
     if len(sys.argv) != 2 or sys.argv[1] not in CASES:

@@ -93,6 +93,43 @@ def gemm_argmax(a: torch.Tensor, b: torch.Tensor, bias=None, out_index=None, out
     return out_index
 
 
+def gemm_xent(a: torch.Tensor, b: torch.Tensor, bias, labels, scale: float, g: torch.Tensor, gt: torch.Tensor, loss=None, err=None,
+              groups: int = 1, stream=None):
+    """Softmax cross-entropy gradient of a @ b.T + bias (logits never stored):
+    g = (softmax - onehot(labels)) * scale in BF16 and its (grouped) transpose gt;
+    loss += scale * sum of the rows' cross-entropies."""
+    m, k = a.shape[0] // groups, a.shape[1]
+    n = b.shape[0] // groups
+    d = _abi.GemmXentDesc()
+    d.a, d.lda, d.b, d.ldb = a.data_ptr(), a.stride(0), b.data_ptr(), b.stride(0)
+    d.m, d.n, d.k, d.bias, d.labels, d.scale = m, n, k, _p(bias), labels.data_ptr(), float(scale)
+    d.g, d.ldg, d.gt, d.ldgt = g.data_ptr(), g.stride(0), gt.data_ptr(), gt.stride(0)
+    d.loss_sum, d.error_word, d.groups = _p(loss), _p(err), groups
+    _check("rt_gemm_xent_bf16", _abi.lib().rt_gemm_xent_bf16(C.byref(d), _stream(stream)))
+
+
+def mlp_propose(orig, dir, box, W16, b, out=None, groups: int = 1, group_rows: int = 0, min_margin: float = 0.0, margin=None,
+                value=None, err=None, count=None, stream=None):
+    """Fused proposal (rt_mlp_propose): features, hidden layers and argmax in
+    one launch. W16 / b: the four BF16 weight matrices and FP32 biases (grouped:
+    stacked along rows)."""
+    R = orig.shape[0] if count is None else count
+    if out is None:
+        out = torch.empty(R, dtype=torch.int32, device=orig.device)
+    d = _abi.MlpProposeDesc()
+    d.orig, d.dir, d.count = orig.data_ptr(), dir.data_ptr(), R
+    for i in range(3):
+        d.box_lo[i] = float(box[i])
+        d.box_hi[i] = float(box[3 + i])
+    d.w1, d.w2, d.w3, d.w4 = (w.data_ptr() for w in W16)
+    d.b1, d.b2, d.b3, d.b4 = (x.data_ptr() for x in b)
+    d.n = W16[3].shape[0] // groups
+    d.groups, d.group_rows, d.min_margin = groups, group_rows, float(min_margin)
+    d.out_index, d.out_value, d.out_margin, d.error_word = out.data_ptr(), _p(value), _p(margin), _p(err)
+    _check("rt_mlp_propose", _abi.lib().rt_mlp_propose(C.byref(d), _stream(stream)))
+    return out
+
+
 def ray_features(orig, dir, box, out=None, out_t=None, count=None, group_rows: int = 0, stream=None):
     """bf16 features (count, 192) and/or their transpose (192, count); box = (lo xyz, hi xyz).
     group_rows > 0: out_t holds one (192, group_rows) transpose per group of rays."""
@@ -195,8 +232,7 @@ class ProposalNet:
             ws = dict(X=_bf16((B, FEATURES_PAD), dev), H1=_bf16((B, HIDDEN), dev), H2=_bf16((B, HIDDEN), dev), H3=_bf16((B, HIDDEN), dev))
             if train:
                 ws.update(XT=_bf16((FEATURES_PAD, B), dev), H1T=_bf16((HIDDEN, B), dev), H2T=_bf16((HIDDEN, B), dev),
-                          H3T=_bf16((HIDDEN, B), dev), L=torch.empty((B, self.classes), dtype=torch.float32, device=dev),
-                          G=_bf16((B, self.classes), dev), GT=_bf16((self.classes, B), dev), D3=_bf16((B, HIDDEN), dev),
+                          H3T=_bf16((HIDDEN, B), dev), G=_bf16((B, self.classes), dev), GT=_bf16((self.classes, B), dev), D3=_bf16((B, HIDDEN), dev),
                           D3T=_bf16((HIDDEN, B), dev), D2=_bf16((B, HIDDEN), dev), D2T=_bf16((HIDDEN, B), dev),
                           D1=_bf16((B, HIDDEN), dev), D1T=_bf16((HIDDEN, B), dev),
                           loss=torch.zeros(1, dtype=torch.float32, device=dev))
@@ -217,11 +253,8 @@ class ProposalNet:
         gemm(ws["X"], W16[0], bias=b[0], relu=True, out_bf16=ws["H1"], out_t=ws["H1T"], err=err, stream=stream)
         gemm(ws["H1"], W16[1], bias=b[1], relu=True, out_bf16=ws["H2"], out_t=ws["H2T"], err=err, stream=stream)
         gemm(ws["H2"], W16[2], bias=b[2], relu=True, out_bf16=ws["H3"], out_t=ws["H3T"], err=err, stream=stream)
-        gemm(ws["H3"], W16[3], bias=b[3], out_f32=ws["L"], err=err, stream=stream)
         ws["loss"].zero_()
-        _check("rt_softmax_xent", _abi.lib().rt_softmax_xent(_p(ws["L"]), B, self.classes, _p(labels), 1.0 / B, _p(ws["G"]),
-                                                              _p(ws["loss"]), _stream(stream)))
-        transpose(ws["G"], ws["GT"], stream=stream)
+        gemm_xent(ws["H3"], W16[3], b[3], labels, 1.0 / B, ws["G"], ws["GT"], loss=ws["loss"], err=err, stream=stream)
         gW = self.grads[0::2]
         gb = self.grads[1::2]
         # layer 4
@@ -262,12 +295,18 @@ class ProposalNet:
         return loss
 
     # ------------------------------------------------------------- inference
-    def propose(self, orig, dir, box, out=None, min_margin: float = 0.0, margin=None, chunk: int = 1 << 20, stream=None):
+    def propose(self, orig, dir, box, out=None, min_margin: float = 0.0, margin=None, chunk: int = 1 << 20, fused: bool = True,
+                stream=None):
         """int32 slot proposal per ray: the argmax of the logits, or -1 (no
-        proposal) where its margin over the runner-up is below min_margin."""
+        proposal) where its margin over the runner-up is below min_margin.
+        fused: one rt_mlp_propose launch; otherwise features, three GEMMs and
+        the argmax GEMM as separate launches (the same bits)."""
         R = orig.shape[0]
         if out is None:
             out = torch.empty(R, dtype=torch.int32, device=orig.device)
+        if fused:
+            return mlp_propose(orig, dir, box, self.W16, self.b, out=out, min_margin=min_margin, margin=margin, err=self.err,
+                               stream=stream)
         c = min(chunk, ((R + 127) // 128) * 128)
         ws = self._workspace(c, False)
         for s in range(0, R, c):
@@ -346,8 +385,7 @@ class ProposalGroup:
             ws = dict(X=_bf16((R, FEATURES_PAD), dev), H1=_bf16((R, HIDDEN), dev), H2=_bf16((R, HIDDEN), dev), H3=_bf16((R, HIDDEN), dev))
             if train:
                 ws.update(XT=_bf16((G * FEATURES_PAD, B), dev), H1T=_bf16((G * HIDDEN, B), dev), H2T=_bf16((G * HIDDEN, B), dev),
-                          H3T=_bf16((G * HIDDEN, B), dev), L=torch.empty((R, K), dtype=torch.float32, device=dev),
-                          G=_bf16((R, K), dev), GT=_bf16((G * K, B), dev), D3=_bf16((R, HIDDEN), dev),
+                          H3T=_bf16((G * HIDDEN, B), dev), G=_bf16((R, K), dev), GT=_bf16((G * K, B), dev), D3=_bf16((R, HIDDEN), dev),
                           D3T=_bf16((G * HIDDEN, B), dev), D2=_bf16((R, HIDDEN), dev), D2T=_bf16((G * HIDDEN, B), dev),
                           D1=_bf16((R, HIDDEN), dev), D1T=_bf16((G * HIDDEN, B), dev),
                           loss=torch.zeros(1, dtype=torch.float32, device=dev),
@@ -370,11 +408,8 @@ class ProposalGroup:
         gemm(ws["X"], W16[0], bias=b[0], relu=True, out_bf16=ws["H1"], out_t=ws["H1T"], **kw)
         gemm(ws["H1"], W16[1], bias=b[1], relu=True, out_bf16=ws["H2"], out_t=ws["H2T"], **kw)
         gemm(ws["H2"], W16[2], bias=b[2], relu=True, out_bf16=ws["H3"], out_t=ws["H3T"], **kw)
-        gemm(ws["H3"], W16[3], bias=b[3], out_f32=ws["L"], **kw)
         ws["loss"].zero_()
-        _check("rt_softmax_xent", _abi.lib().rt_softmax_xent(_p(ws["L"]), G * B, self.classes, _p(labels), 1.0 / B, _p(ws["G"]),
-                                                              _p(ws["loss"]), _stream(stream)))
-        transpose_grouped(ws["G"], G, ws["GT"], stream=stream)
+        gemm_xent(ws["H3"], W16[3], b[3], labels, 1.0 / B, ws["G"], ws["GT"], loss=ws["loss"], **kw)
         gW, gb = self.grads[0::2], self.grads[1::2]
         gemm(ws["GT"], ws["H3T"], out_f32=gW[3], **kw)
         colsum_grouped(ws["G"], G, gb[3], stream=stream)
@@ -421,7 +456,8 @@ class ProposalGroup:
             loss = self.train_step(out[0], out[1], out[2], box, batch, lr=lr, stream=stream)
         return loss
 
-    def propose(self, orig, dir, box, group_rays: int, out=None, min_margin: float = 0.0, chunk_rows: int = 1 << 22, stream=None):
+    def propose(self, orig, dir, box, group_rays: int, out=None, min_margin: float = 0.0, chunk_rows: int = 1 << 22, fused: bool = True,
+                margin=None, stream=None):
         """Slot proposal per ray; group g's rays are rows g * group_rays ..
         (group_rays % 128 == 0), scored by group g's network."""
         G = self.groups
@@ -429,6 +465,9 @@ class ProposalGroup:
             raise ValueError("need groups * group_rays rays with group_rays % 128 == 0")
         if out is None:
             out = torch.empty(G * group_rays, dtype=torch.int32, device=orig.device)
+        if fused:
+            return mlp_propose(orig, dir, box, self.W16, self.b, out=out, groups=G, group_rows=group_rays, min_margin=min_margin,
+                               margin=margin, err=self.err, stream=stream)
         cg = max(1, min(G, chunk_rows // group_rays))
         ws = self._workspace(cg * group_rays, False)
         for g0 in range(0, G, cg):

@@ -82,6 +82,62 @@ typedef struct rt_gemm_argmax_desc {
 } rt_gemm_argmax_desc;
 rt_status rt_gemm_argmax_bf16(const rt_gemm_argmax_desc* d, rt_stream stream);
 
+/* The whole proposal network in one launch: features, three hidden layers
+ * and the argmax over n logits for each ray, bit-identical to rt_ray_features
+ * + 3 x rt_gemm_bf16 (bias, ReLU, BF16 outputs) + rt_gemm_argmax_bf16, with no
+ * activation written to memory. Weights BF16, rows contiguous: w1 [groups 128][192],
+ * w2, w3 [groups 128][128], w4 [groups n][128]; biases FP32 [groups 128] (b1..b3),
+ * [groups n] (b4). n % 256 == 0, n <= 4096. groups > 1: ray r belongs to group
+ * r / group_rows (group_rows % 128 == 0, count == groups * group_rows). */
+typedef struct rt_mlp_propose_desc {
+  const float* orig; /* float4 per ray */
+  const float* dir;
+  uint32_t count;
+  float box_lo[3], box_hi[3];
+  const void* w1;
+  const void* w2;
+  const void* w3;
+  const void* w4;
+  const float* b1;
+  const float* b2;
+  const float* b3;
+  const float* b4;
+  uint32_t n;
+  uint32_t groups, group_rows;
+  float min_margin;
+  int32_t* out_index;
+  float* out_value;  /* optional */
+  float* out_margin; /* optional */
+  uint32_t* error_word;
+} rt_mlp_propose_desc;
+rt_status rt_mlp_propose(const rt_mlp_propose_desc* d, rt_stream stream);
+
+/* Softmax cross-entropy gradient of the logits A B^T + bias without storing
+ * them: g[r][j] = (softmax(row r)_j - [j == labels[r]]) * scale in BF16, written
+ * row-major (g, [m][ldg]) and transposed (gt, [n][ldgt]); *loss_sum +=
+ * scale * (logsumexp(row r) - logit[labels[r]]). Rows whose label is outside
+ * [0, n) get g = 0 and add no loss. m % 128 == 0, n % 256 == 0, n <= 4096,
+ * k % 64 == 0, k <= 256, ldg % 8 == 0. groups > 1 as for rt_gemm_argmax_bf16;
+ * group q's transpose fills rows q n .. q n + n - 1 of gt, columns 0 .. m - 1. */
+typedef struct rt_gemm_xent_desc {
+  const void* a;
+  uint32_t lda;
+  const void* b;
+  uint32_t ldb;
+  uint32_t m, n, k;
+  const float* bias;
+  const int32_t* labels;
+  float scale;
+  void* g;
+  uint32_t ldg;
+  void* gt;
+  uint32_t ldgt;
+  float* loss_sum; /* optional, accumulated */
+  uint32_t* error_word;
+  uint32_t groups;
+} rt_gemm_xent_desc;
+rt_status rt_gemm_xent_bf16(const rt_gemm_xent_desc* d, rt_stream stream);
+
 /* Ray features: u = ((o - c) * 2 / (hi - lo), d / |d|), c = (lo + hi) / 2;
  * f[24 i + 2 j] = sin(pi 2^j u_i), f[24 i + 2 j + 1] = cos(pi 2^j u_i), j < 12;
  * columns 144 .. 191 are zero. out: BF16 [count][ld_out] (ld_out >= 192, a

@@ -94,6 +94,7 @@ _STRUCTS = {  # C typedef -> ctypes mirror in cudart_b200._abi
     "rt_batch_trace_desc": "BatchTraceDesc", "rt_sah_desc": "SahDesc", "rt_raster_desc": "RasterDesc", "rt_gemm_desc": "GemmDesc",
     "rt_gemm_argmax_desc": "GemmArgmaxDesc", "rt_feature_desc": "FeatureDesc", "rt_adam_desc": "AdamDesc", "rt_slot_desc": "SlotDesc",
     "rt_seed_desc": "SeedDesc", "rt_batch_gather_desc": "BatchGatherDesc", "rt_batch_slot_desc": "BatchSlotDesc", "rt_camera": "Camera",
+    "rt_mlp_propose_desc": "MlpProposeDesc", "rt_gemm_xent_desc": "GemmXentDesc",
 }
 
 

@@ -100,6 +100,23 @@ def test_grouped_features_transpose_and_small_kernels():
     assert torch.equal(ol, lab[src]) and torch.equal(oo, oq[src]) and torch.equal(od, dq[src])
 
 
+@pytest.mark.parametrize("G,R", [(3, 256), (5, 1280)])
+def test_grouped_fused_propose_matches_layered(G, R):
+    from cudart_b200 import proposal, scenes
+    box = (-1.5, -0.6, -1.5, 1.5, 1.4, 1.5)
+    grp = proposal.ProposalGroup(G, seed=2)
+    to, td = scenes.box_rays_torch(G * 256, box, seed=40)
+    lab = torch.randint(0, 4096, (G * 256,), dtype=torch.int32, device="cuda", generator=torch.Generator(device="cuda").manual_seed(6))
+    for _ in range(2):
+        grp.train_step(to, td, lab, box, 256, lr=3e-3)
+    o, d = scenes.box_rays_torch(G * R, box, seed=41)
+    a = grp.propose(o, d, box, R, fused=True)
+    b = grp.propose(o, d, box, R, fused=False)
+    torch.cuda.synchronize()
+    assert int(grp.err.item()) == 0
+    assert torch.equal(a, b)
+
+
 def test_group_select_and_index_gather():
     from cudart_b200 import proposal
     G, S = 3, 5000

@@ -285,3 +285,66 @@ def test_training_gains_over_untrained():
     assert acc_o == 1.0
     assert t_o <= 1.0 and v_o <= 1.02
     assert v1 <= 1.10 and t1 <= 1.10
+
+
+@pytest.mark.parametrize("R,margin", [(1000, 0.0), (4096, 0.5), (128 * 150 + 17, 0.0)])
+def test_fused_propose_matches_layered(R, margin):
+    """rt_mlp_propose (one launch, activations on chip) returns the bits of the
+    layer-by-layer path: features, three GEMMs, argmax GEMM."""
+    from cudart_b200 import proposal as P
+    box = (-1.5, -0.6, -1.5, 1.5, 1.4, 1.5)
+    o, d = _rays(R, 17, box)
+    o, d = torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda()
+    net = P.ProposalNet(seed=3)
+    lab = torch.randint(0, 4096, (1024,), dtype=torch.int32, device="cuda", generator=torch.Generator(device="cuda").manual_seed(5))
+    to, td = _rays(1024, 18, box)
+    for _ in range(3):  # move the weights off their initial values
+        net.train_step(torch.from_numpy(to).cuda(), torch.from_numpy(td).cuda(), lab, box, lr=3e-3)
+    m1, m2 = torch.empty(R, device="cuda"), torch.empty(R, device="cuda")
+    if margin > 0:  # as a quantile of this network's margins, so that both outcomes occur
+        net.propose(o, d, box, margin=m1)
+        margin = float(m1.quantile(margin).item())
+    a = net.propose(o, d, box, min_margin=margin, margin=m1, fused=True)
+    b = net.propose(o, d, box, min_margin=margin, margin=m2, fused=False)
+    torch.cuda.synchronize()
+    assert int(net.err.item()) == 0
+    assert torch.equal(a, b)
+    assert torch.equal(m1.view(torch.int32), m2.view(torch.int32))
+    if margin > 0:
+        assert (a == -1).any() and (a >= 0).any()
+
+
+@pytest.mark.parametrize("n,groups", [(1024, 1), (4096, 1), (512, 3)])
+def test_gemm_xent_matches_torch(n, groups):
+    """Fused logits + softmax cross-entropy gradient against torch in FP32 on
+    the same logits (the kernel's FP32 GEMM output): |g - g_ref| <= 2^-8 |scale|
+    (one BF16 rounding of values <= 1), the transpose exact, the loss within 1e-4."""
+    from cudart_b200 import proposal as P
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    m, k = 256, 128
+    a = _bf16(torch.randn(groups * m, k, device="cuda", generator=gen))
+    b = _bf16(torch.randn(groups * n, k, device="cuda", generator=gen) * 0.3)
+    bias = torch.randn(groups * n, device="cuda", generator=gen)
+    labels = torch.randint(-1, n + 2, (groups * m,), dtype=torch.int32, device="cuda", generator=gen)
+    scale = 1.0 / m
+    g = torch.empty(groups * m, n, dtype=torch.bfloat16, device="cuda")
+    gt = torch.empty(groups * n, m, dtype=torch.bfloat16, device="cuda")
+    loss = torch.zeros(1, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    P.gemm_xent(a, b, bias, labels, scale, g, gt, loss=loss, err=err, groups=groups)
+    logits = torch.empty(groups * m, n, device="cuda")
+    P.gemm(a, b, bias=bias, out_f32=logits, groups=groups)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    valid = (labels >= 0) & (labels < n)
+    p = torch.softmax(logits.double(), dim=1)
+    onehot = torch.zeros_like(p)
+    onehot[valid, labels[valid].long()] = 1.0
+    ref = ((p - onehot) * scale).float()
+    ref[~valid] = 0.0
+    assert (g.float() - ref).abs().max().item() <= scale * 2.0 ** -8
+    for q in range(groups):
+        assert torch.equal(gt[q * n:(q + 1) * n].view(torch.int16), g[q * m:(q + 1) * m].T.contiguous().view(torch.int16))
+    lse = torch.logsumexp(logits.double(), dim=1)
+    want = ((lse - logits.double().gather(1, labels.clamp(0, n - 1).long()[:, None])[:, 0])[valid] * scale).sum().item()
+    assert abs(loss.item() - want) <= 1e-4 * max(1.0, abs(want))
