@@ -738,6 +738,18 @@ __global__ __launch_bounds__(1024) void k_group_select(const int32_t* __restrict
   if (threadIdx.x == 0) count[g] = base;
 }
 
+__device__ __forceinline__ float adam_update(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                                             float* __restrict__ v, size_t i, float lr, float b1, float b2, float eps, float c1, float c2) {
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float pi = p[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+  p[i] = pi;
+  return pi;
+}
+
 // Adam (bias-corrected) on FP32 parameters [rows][cols]; refreshes the BF16
 // copies [rows][ld16] and transposed [cols][ld16t] when given (with groups of
 // group_rows rows: one transpose per group, group q in rows q cols ..).
@@ -747,18 +759,41 @@ __global__ __launch_bounds__(256) void k_adam(float* __restrict__ p, const float
                                               __nv_bfloat16* __restrict__ out16t, uint32_t ld16t, uint32_t group_rows) {
   const size_t total = (size_t)rows * cols;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const float gi = g[i];
-    const float mi = b1 * m[i] + (1.0f - b1) * gi;
-    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
-    m[i] = mi;
-    v[i] = vi;
-    const float pi = p[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
-    p[i] = pi;
+    const float pi = adam_update(p, g, m, v, i, lr, b1, b2, eps, c1, c2);
     const uint32_t r = (uint32_t)(i / cols), c = (uint32_t)(i % cols);
     if (out16) out16[(size_t)r * ld16 + c] = __float2bfloat16_rn(pi);
     if (out16t) {
       const uint32_t q = r / group_rows;
       out16t[((size_t)q * cols + c) * ld16t + (r - q * group_rows)] = __float2bfloat16_rn(pi);
+    }
+  }
+}
+
+// The same update over 32 x 32 tiles (block 32 x 8), with the BF16 transpose
+// staged through shared memory so that both copies are written coalesced.
+__global__ __launch_bounds__(256) void k_adam_t(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                                                float* __restrict__ v, uint32_t rows, uint32_t cols, float lr, float b1, float b2,
+                                                float eps, float c1, float c2, __nv_bfloat16* __restrict__ out16, uint32_t ld16,
+                                                __nv_bfloat16* __restrict__ out16t, uint32_t ld16t, uint32_t group_rows) {
+  __shared__ __nv_bfloat16 tile[32][34];
+  const uint32_t c0 = blockIdx.x * 32, r0 = blockIdx.y * 32, tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+  for (uint32_t k = 0; k < 4; ++k) {
+    const uint32_t r = r0 + ty + 8 * k, c = c0 + tx;
+    if (r < rows && c < cols) {
+      const float pi = adam_update(p, g, m, v, (size_t)r * cols + c, lr, b1, b2, eps, c1, c2);
+      const __nv_bfloat16 h = __float2bfloat16_rn(pi);
+      if (out16) out16[(size_t)r * ld16 + c] = h;
+      tile[ty + 8 * k][tx] = h;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (uint32_t k = 0; k < 4; ++k) {
+    const uint32_t c = c0 + ty + 8 * k, r = r0 + tx;
+    if (r < rows && c < cols) {
+      const uint32_t q = r / group_rows;
+      out16t[((size_t)q * cols + c) * ld16t + (r - q * group_rows)] = tile[tx][ty + 8 * k];
     }
   }
 }
@@ -1320,10 +1355,16 @@ extern "C" rt_status rt_adam_step(const rt_adam_desc* d, rt_stream stream) {
   if (total == 0) return RT_OK;
   const float c1 = 1.0f / (1.0f - powf(d->beta1, (float)d->step));
   const float c2 = 1.0f / (1.0f - powf(d->beta2, (float)d->step));
-  const uint32_t blocks = (uint32_t)hmin<size_t>((total + 255) / 256, (size_t)num_sms() * 8);
-  k_adam<<<blocks, 256, 0, (cudaStream_t)stream>>>(d->param, d->grad, d->m, d->v, d->rows, d->cols, d->lr, d->beta1, d->beta2, d->eps, c1,
-                                                    c2, (__nv_bfloat16*)d->out_bf16, d->ld_bf16, (__nv_bfloat16*)d->out_bf16_t,
-                                                    d->ld_bf16_t, G > 1 ? d->rows / G : (d->rows ? d->rows : 1u));
+  const uint32_t gr = G > 1 ? d->rows / G : (d->rows ? d->rows : 1u);
+  if (d->out_bf16_t) {
+    k_adam_t<<<dim3((d->cols + 31) / 32, (d->rows + 31) / 32), dim3(32, 8), 0, (cudaStream_t)stream>>>(
+        d->param, d->grad, d->m, d->v, d->rows, d->cols, d->lr, d->beta1, d->beta2, d->eps, c1, c2, (__nv_bfloat16*)d->out_bf16,
+        d->ld_bf16, (__nv_bfloat16*)d->out_bf16_t, d->ld_bf16_t, gr);
+  } else {
+    const uint32_t blocks = (uint32_t)hmin<size_t>((total + 255) / 256, (size_t)num_sms() * 8);
+    k_adam<<<blocks, 256, 0, (cudaStream_t)stream>>>(d->param, d->grad, d->m, d->v, d->rows, d->cols, d->lr, d->beta1, d->beta2, d->eps,
+                                                      c1, c2, (__nv_bfloat16*)d->out_bf16, d->ld_bf16, nullptr, 0, gr);
+  }
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
