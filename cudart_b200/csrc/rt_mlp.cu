@@ -801,19 +801,24 @@ __global__ __launch_bounds__(256) void k_adam_t(float* __restrict__ p, const flo
 // ----------------------------------------------------------------------------
 // Fused proposal: features -> 3 x (128, ReLU) -> argmax over n logits for a
 // tile of 128 rays per step, persistent over tiles (grid <= SM count).
-// Warps 0-7 compute (features into shared memory, the hidden layers' bias +
-// ReLU from TMEM back into shared memory as the next layer's A operand, the
-// running top-2 over the logits), warp 8 streams every weight tile through a
-// 3-stage ring with TMA (W1..W3 as 128 x 64 tiles, W4 as 256 x 64), warp 9
-// issues the MMAs. Activations never leave the SM. Shared memory: A (48 KB:
-// X, then H2), B (32 KB: H1, then H3), ring 3 x 32 KB. TMEM: the hidden
-// layers use columns [0, 128); the logits alternate [0, 256) / [256, 512).
-// Every wait is bounded; one that runs out raises the shared abort flag, and
-// every role leaves its tile loop at its next wait.
+// Warps 0-15 compute: warp w serves TMEM lane quarter w % 4 and column quarter
+// w / 4 (features into shared memory; the hidden layers' bias + ReLU from TMEM
+// back into shared memory as the next layer's A operand; a running top-2 over
+// its quarter of the logits, merged per row through shared memory). Warp 16
+// streams the weight tiles through a 3-stage TMA ring (W1..W3 as 128 x 64, W4
+// as 256 x 64) and the tile's biases into one of two shared buffers with bulk
+// copies; warp 17 issues the MMAs. Activations never leave the SM. Shared
+// memory: A (48 KB: X, then H2), B (32 KB: H1, then H3), ring 3 x 32 KB, bias
+// 2 x (n + 384) floats. TMEM: the hidden layers use columns [0, 128); the
+// logits alternate [0, 256) / [256, 512). Every wait is bounded; one that runs
+// out raises the shared abort flag, and every role leaves its tile loop at its
+// next wait.
 // ----------------------------------------------------------------------------
-constexpr uint32_t kFuseThreads = 320;
+constexpr uint32_t kFuseCompute = 512;
+constexpr uint32_t kFuseThreads = kFuseCompute + 64;
 constexpr uint32_t kFuseStages = 3;
 constexpr uint32_t kFuseStage = 32768;
+constexpr uint32_t kFuseBias = kArgMaxN + 384;  // floats per bias buffer: b4 [n], b1, b2, b3 [128] at kArgMaxN
 
 struct FuseArgs {
   const float4* orig;
@@ -833,9 +838,13 @@ struct FuseArgs {
 };
 
 size_t fuse_smem() {
-  return 1024 + 5 * (size_t)kTileA + kFuseStages * (size_t)kFuseStage + kBM * sizeof(Top2) + 16 * 8 + 64;
+  return 1024 + 5 * (size_t)kTileA + kFuseStages * (size_t)kFuseStage + 2 * (size_t)kFuseBias * 4 + 3 * kBM * sizeof(Top2) + 24 * 8 +
+         64;
 }
 
+// kTop2: also track each row's runner-up (for a margin); without it the logit
+// sweep keeps only the maximum and its index (the same index either way).
+template <bool kTop2>
 __global__ void __launch_bounds__(kFuseThreads, 1)
     k_mlp_propose_tc(const __grid_constant__ CUtensorMap t1, const __grid_constant__ CUtensorMap t2,
                      const __grid_constant__ CUtensorMap t3, const __grid_constant__ CUtensorMap t4, FuseArgs P) {
@@ -844,17 +853,20 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
   uint8_t* sA = smem;                   // 3 atoms of 128 x 64 BF16
   uint8_t* sB = sA + 3 * kTileA;        // 2 atoms
   uint8_t* sR = sB + 2 * kTileA;        // ring
-  Top2* s_half = (Top2*)(sR + kFuseStages * kFuseStage);
-  uint64_t* full = (uint64_t*)(s_half + kBM);
+  float* s_bias = (float*)(sR + kFuseStages * kFuseStage);  // [2][kFuseBias]
+  Top2* s_part = (Top2*)(s_bias + 2 * kFuseBias);           // [3][128]: column quarters 1..3
+  uint64_t* full = (uint64_t*)(s_part + 3 * kBM);
   uint64_t* empty = full + kFuseStages;
   uint64_t* x_ready = empty + kFuseStages;
   uint64_t* h_ready = x_ready + 1;
   uint64_t* lay_done = h_ready + 1;
   uint64_t* acc_full = lay_done + 1;   // [2]
   uint64_t* acc_empty = acc_full + 2;  // [2]
-  uint64_t* half_ready = acc_empty + 2;
-  uint64_t* half_free = half_ready + 1;
-  uint64_t* done = half_free + 1;
+  uint64_t* part_ready = acc_empty + 2;
+  uint64_t* part_free = part_ready + 1;
+  uint64_t* bias_full = part_free + 1;    // [2]
+  uint64_t* bias_empty = bias_full + 2;   // [2]
+  uint64_t* done = bias_empty + 2;
   uint32_t* tmem_slot = (uint32_t*)(done + 1);
   volatile uint32_t* s_abort = tmem_slot + 1;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -863,15 +875,17 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
       mbar_init(full + q, 1);
       mbar_init(empty + q, 1);
     }
-    mbar_init(x_ready, 256);
-    mbar_init(h_ready, 256);
+    mbar_init(x_ready, kFuseCompute);
+    mbar_init(h_ready, kFuseCompute);
     mbar_init(lay_done, 1);
     for (int b = 0; b < 2; ++b) {
       mbar_init(acc_full + b, 1);
-      mbar_init(acc_empty + b, 256);
+      mbar_init(acc_empty + b, kFuseCompute);
+      mbar_init(bias_full + b, 1);
+      mbar_init(bias_empty + b, kFuseCompute);
     }
-    mbar_init(half_ready, 128);
-    mbar_init(half_free, 128);
+    mbar_init(part_ready, 3 * kBM);
+    mbar_init(part_free, kBM);
     mbar_init(done, 1);
     *s_abort = 0u;
     fence_mbar_init();
@@ -901,9 +915,9 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
     return false;
   };
 
-  if (warp == 8) {
+  if (warp == 16) {
     if (lane == 0) {
-      uint32_t q = 0;
+      uint32_t q = 0, k = 0;
       bool ok = true;
       auto load = [&](const CUtensorMap* m, int32_t x, int32_t y, uint32_t bytes) -> bool {
         const uint32_t st = q % kFuseStages;
@@ -913,18 +927,26 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
         ++q;
         return true;
       };
-      for (uint32_t tile = blockIdx.x; ok && tile < P.tiles; tile += gridDim.x) {
-        const uint32_t g = tile * kBM / P.group_rows;
+      for (uint32_t tile = blockIdx.x; ok && tile < P.tiles; tile += gridDim.x, ++k) {
+        const uint32_t g = tile * kBM / P.group_rows, bb = k & 1u;
+        if (k >= 2 && !(ok = wait(bias_empty + bb, ((k >> 1) - 1u) & 1u))) break;
+        float* sb = s_bias + bb * kFuseBias;
+        mbar_arrive_expect_tx(bias_full + bb, P.n * 4u + 3u * 512u);
+        bulk_load(sb, P.b4 + (size_t)g * P.n, P.n * 4u, bias_full + bb);
+        bulk_load(sb + kArgMaxN, P.b1 + (size_t)g * 128u, 512u, bias_full + bb);
+        bulk_load(sb + kArgMaxN + 128, P.b2 + (size_t)g * 128u, 512u, bias_full + bb);
+        bulk_load(sb + kArgMaxN + 256, P.b3 + (size_t)g * 128u, 512u, bias_full + bb);
         for (uint32_t kc = 0; ok && kc < 3; ++kc) ok = load(&t1, (int32_t)(kc * kBK), (int32_t)(g * kBM), kTileA);
         for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = load(&t2, (int32_t)(kc * kBK), (int32_t)(g * kBM), kTileA);
         for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = load(&t3, (int32_t)(kc * kBK), (int32_t)(g * kBM), kTileA);
         for (uint32_t t = 0; ok && t < ntiles; ++t)
           for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = load(&t4, (int32_t)(kc * kBK), (int32_t)(g * P.n + t * kArgBN), kArgTileB);
       }
-      // the last load of each stage has landed before the CTA may exit
+      // the last copy into each stage / bias buffer has landed before the CTA may exit
       for (uint32_t j = q > kFuseStages ? q - kFuseStages : 0u; j < q; ++j) mbar_wait(full + j % kFuseStages, (j / kFuseStages) & 1u, P.err);
+      for (uint32_t j = k > 2 ? k - 2 : 0u; j < k; ++j) mbar_wait(bias_full + (j & 1u), (j >> 1) & 1u, P.err);
     }
-  } else if (warp == 9) {
+  } else if (warp == 17) {
     if (lane == 0) {
       const uint32_t id_h = idesc_bf16_f32(kBM, 128), id_l = idesc_bf16_f32(kBM, kArgBN);
       uint32_t q = 0, xr = 0, hr = 0, n4 = 0;
@@ -971,87 +993,90 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
       mbar_wait(done, 0, P.err);
     }
   } else {
-    // compute warps 0-7: lane quarter warp % 4 of TMEM, column half warp / 4
-    const uint32_t qw = warp & 3u, half = warp >> 2, tid = threadIdx.x;
+    // compute warps 0-15: TMEM lane quarter warp % 4, column quarter warp / 4
+    const uint32_t qw = warp & 3u, cq = warp >> 2, tid = threadIdx.x;
     const uint32_t trow = qw * 32u + lane;  // TMEM lane = tile row of this thread
-    uint32_t ld = 0, n4 = 0, hf = 0;
+    uint32_t ld = 0, n4 = 0, k = 0;
     bool ok = true;
-    for (uint32_t tile = blockIdx.x; ok && tile < P.tiles; tile += gridDim.x) {
-      const uint32_t row0 = tile * kBM, g = row0 / P.group_rows;
-      {  // features of ray r = tid % 128: inputs 0-2 (origin) or 3-5 (direction)
-        const uint32_t r = tid & 127u, part = tid >> 7, row = row0 + r;
+    for (uint32_t tile = blockIdx.x; ok && tile < P.tiles; tile += gridDim.x, ++k) {
+      const uint32_t row0 = tile * kBM, bb = k & 1u;
+      // features: (ray r, input i) pairs p = 128 i + r, i < 6
+      for (uint32_t p = tid; p < 6u * kBM; p += kFuseCompute) {
+        const uint32_t r = p & 127u, i = p >> 7, row = row0 + r;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (row < P.count) v = __ldg((part ? P.dir : P.orig) + row);
+        if (row < P.count) v = __ldg((i < 3 ? P.orig : P.dir) + row);
+        uint32_t w[12];
+        encode12(i < 3 ? origin_input(v, P.c, P.s, i) : dir_input(v, i - 3), w);
+        const uint32_t f0 = 24u * i;
 #pragma unroll
-        for (uint32_t i = 0; i < 3; ++i) {
-          uint32_t w[12];
-          encode12(part ? dir_input(v, i) : origin_input(v, P.c, P.s, i), w);
-          const uint32_t f0 = 24u * (3u * part + i);
-#pragma unroll
-          for (uint32_t j = 0; j < 12; ++j) {
-            const uint32_t f = f0 + 2u * j;
-            *(uint32_t*)(sA + (f >> 6) * kTileA + sw128_offset(r, f & 63u)) = w[j];
-          }
+        for (uint32_t j = 0; j < 12; ++j) {
+          const uint32_t f = f0 + 2u * j;
+          *(uint32_t*)(sA + (f >> 6) * kTileA + sw128_offset(r, f & 63u)) = w[j];
         }
       }
       fence_proxy_async();
       mbar_arrive(x_ready);
-      // hidden layers: bias + ReLU of TMEM columns [64 half, 64 half + 64) into the next A operand
+      ok = __all_sync(0xffffffffu, wait(bias_full + bb, (k >> 1) & 1u));
+      if (!ok) break;
+      const float* sb = s_bias + bb * kFuseBias;
+      // hidden layers: bias + ReLU of TMEM columns [32 cq, 32 cq + 32) into the next A operand
       for (uint32_t L = 0; L < 3; ++L) {
         ok = __all_sync(0xffffffffu, wait(lay_done, ld++ & 1u));
         tc_fence_after();
         if (!ok) break;
-        uint8_t* dst = L == 1 ? sA : sB;
-        const float* bias = (L == 0 ? P.b1 : (L == 1 ? P.b2 : P.b3)) + (size_t)g * 128u;
-        const uint32_t tl = tmem + ((qw * 32u) << 16) + half * 64u;
+        uint8_t* atom = (L == 1 ? sA : sB) + (cq >> 1) * kTileA;
+        const float* bias = sb + kArgMaxN + L * 128u;
+        const uint32_t tl = tmem + ((qw * 32u) << 16) + cq * 32u;
 #pragma unroll
-        for (uint32_t c = 0; c < 64; c += 16) {
+        for (uint32_t c = 0; c < 32; c += 16) {
           float v[16];
           tmem_ld16(tl + c, v);
-          const uint32_t col = half * 64u + c;
+          const uint32_t col = cq * 32u + c, kin = col & 63u;
           uint32_t w[8];
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
-            const float a = fmaxf(v[2 * i] + __ldg(bias + col + 2 * i), 0.0f);
-            const float b = fmaxf(v[2 * i + 1] + __ldg(bias + col + 2 * i + 1), 0.0f);
+            const float a = fmaxf(v[2 * i] + bias[col + 2 * i], 0.0f);
+            const float b = fmaxf(v[2 * i + 1] + bias[col + 2 * i + 1], 0.0f);
             w[i] = pack_bf16(a, b);
           }
-          uint8_t* atom = dst + half * kTileA;  // col / 64 == half
-          *(uint4*)(atom + sw128_offset(trow, c)) = make_uint4(w[0], w[1], w[2], w[3]);
-          *(uint4*)(atom + sw128_offset(trow, c + 8u)) = make_uint4(w[4], w[5], w[6], w[7]);
+          *(uint4*)(atom + sw128_offset(trow, kin)) = make_uint4(w[0], w[1], w[2], w[3]);
+          *(uint4*)(atom + sw128_offset(trow, kin + 8u)) = make_uint4(w[4], w[5], w[6], w[7]);
         }
         fence_proxy_async();
         tc_fence_before();
         mbar_arrive(h_ready);
       }
       if (!ok) break;
-      // logits of group g: running top-2 over four interleaved column chains
+      // logits: running maximum (and runner-up) over four interleaved column
+      // chains of this quarter; chain j holds columns = j (mod 4), and ik[j]
+      // keeps the winner's column minus j
       float bk[4], sk[4];
       int32_t ik[4];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) { bk[k] = -INFINITY; sk[k] = -INFINITY; ik[k] = -1; }
-      const float* b4 = P.b4 + (size_t)g * P.n;
+      for (int j = 0; j < 4; ++j) { bk[j] = -INFINITY; sk[j] = -INFINITY; ik[j] = -1 - j; }
       for (uint32_t t = 0; t < ntiles; ++t, ++n4) {
         const uint32_t buf = n4 & 1u;
         ok = ok && __all_sync(0xffffffffu, wait(acc_full + buf, (n4 >> 1) & 1u));
         tc_fence_after();
         if (ok) {
-          const uint32_t c0 = half * (kArgBN / 2);
+          const uint32_t c0 = cq * (kArgBN / 4);
           const uint32_t tl = tmem + ((qw * 32u) << 16) + buf * kArgBN + c0;
-          for (uint32_t c = 0; c < kArgBN / 2; c += 16) {
+#pragma unroll
+          for (uint32_t c = 0; c < kArgBN / 4; c += 16) {
             float v[16];
             tmem_ld16(tl + c, v);
             const uint32_t col = t * kArgBN + c0 + c;
-            const float4* bp = (const float4*)(b4 + col);
+            const float4* bp = (const float4*)(sb + col);
 #pragma unroll
             for (int i4 = 0; i4 < 4; ++i4) {
-              const float4 b = __ldg(bp + i4);
-              const float bb[4] = {b.x, b.y, b.z, b.w};
+              const float4 b = bp[i4];
+              const float bv[4] = {b.x, b.y, b.z, b.w};
+              const int32_t base = (int32_t)(col + 4 * i4);
 #pragma unroll
-              for (int k = 0; k < 4; ++k) {
-                const float x = v[4 * i4 + k] + bb[k];
-                sk[k] = fmaxf(sk[k], fminf(x, bk[k]));
-                if (x > bk[k]) { bk[k] = x; ik[k] = (int32_t)(col + 4 * i4 + k); }
+              for (int j = 0; j < 4; ++j) {
+                const float x = v[4 * i4 + j] + bv[j];
+                if (kTop2) sk[j] = fmaxf(sk[j], fminf(x, bk[j]));
+                if (x > bk[j]) { bk[j] = x; ik[j] = base; }
               }
             }
           }
@@ -1059,20 +1084,22 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
         tc_fence_before();
         mbar_arrive(acc_empty + buf);
       }
+      mbar_arrive(bias_empty + bb);
       if (!ok) break;
       Top2 res = Top2{bk[0], sk[0], ik[0]};
 #pragma unroll
-      for (int k = 1; k < 4; ++k) res = top2_merge(res, Top2{bk[k], sk[k], ik[k]});
-      if (half == 1) {
-        if (hf > 0) ok = __all_sync(0xffffffffu, wait(half_free, (hf - 1u) & 1u));
+      for (int j = 1; j < 4; ++j) res = top2_merge(res, Top2{bk[j], sk[j], ik[j] + j});
+      if (cq > 0) {
+        if (k > 0) ok = __all_sync(0xffffffffu, wait(part_free, (k - 1u) & 1u));
         if (!ok) break;
-        s_half[trow] = res;
-        mbar_arrive(half_ready);
+        s_part[(cq - 1u) * kBM + trow] = res;
+        mbar_arrive(part_ready);
       } else {
-        ok = __all_sync(0xffffffffu, wait(half_ready, hf & 1u));
+        ok = __all_sync(0xffffffffu, wait(part_ready, k & 1u));
         if (!ok) break;
-        res = top2_merge(res, s_half[trow]);
-        mbar_arrive(half_free);
+#pragma unroll
+        for (uint32_t j = 0; j < 3; ++j) res = top2_merge(res, s_part[j * kBM + trow]);
+        mbar_arrive(part_free);
         const uint32_t row = row0 + trow;
         if (row < P.count) {
           const float margin = res.best - res.second;
@@ -1081,7 +1108,6 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
           if (P.out_margin) P.out_margin[row] = margin;
         }
       }
-      ++hf;
     }
   }
   tc_fence_before();
@@ -1234,7 +1260,7 @@ extern "C" rt_status rt_mlp_propose(const rt_mlp_propose_desc* d, rt_stream stre
   const uint32_t G = d->groups ? d->groups : 1u;
   if (G > 1 && (d->group_rows == 0 || d->group_rows % kBM || (uint64_t)G * d->group_rows != d->count)) return RT_ERR_INVALID_ARGUMENT;
   if ((uint64_t)G * d->n > 0x7FFFFFFFull || !aligned16(d->w1) || !aligned16(d->w2) || !aligned16(d->w3) || !aligned16(d->w4) ||
-      !aligned16(d->b4))
+      !aligned16(d->b1) || !aligned16(d->b2) || !aligned16(d->b3) || !aligned16(d->b4))
     return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   if (d->count == 0) return RT_OK;
@@ -1251,9 +1277,15 @@ extern "C" rt_status rt_mlp_propose(const rt_mlp_propose_desc* d, rt_stream stre
   P.group_rows = G > 1 ? d->group_rows : P.tiles * kBM;
   P.min_margin = d->min_margin; P.out_idx = d->out_index; P.out_val = d->out_value; P.out_margin = d->out_margin; P.err = d->error_word;
   static std::once_flag once;
-  std::call_once(once, [] { cudaFuncSetAttribute(k_mlp_propose_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fuse_smem()); });
+  std::call_once(once, [] {
+    cudaFuncSetAttribute(k_mlp_propose_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fuse_smem());
+    cudaFuncSetAttribute(k_mlp_propose_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fuse_smem());
+  });
   const uint32_t grid = (uint32_t)hmin<uint32_t>(P.tiles, (uint32_t)num_sms());
-  k_mlp_propose_tc<<<grid, kFuseThreads, fuse_smem(), (cudaStream_t)stream>>>(t1, t2, t3, t4, P);
+  if (d->out_margin || d->min_margin > 0.0f)
+    k_mlp_propose_tc<true><<<grid, kFuseThreads, fuse_smem(), (cudaStream_t)stream>>>(t1, t2, t3, t4, P);
+  else
+    k_mlp_propose_tc<false><<<grid, kFuseThreads, fuse_smem(), (cudaStream_t)stream>>>(t1, t2, t3, t4, P);
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;

@@ -87,7 +87,7 @@ rt_status rt_gemm_argmax_bf16(const rt_gemm_argmax_desc* d, rt_stream stream);
  * + 3 x rt_gemm_bf16 (bias, ReLU, BF16 outputs) + rt_gemm_argmax_bf16, with no
  * activation written to memory. Weights BF16, rows contiguous: w1 [groups 128][192],
  * w2, w3 [groups 128][128], w4 [groups n][128]; biases FP32 [groups 128] (b1..b3),
- * [groups n] (b4). n % 256 == 0, n <= 4096. groups > 1: ray r belongs to group
+ * [groups n] (b4); all pointers 16-byte aligned. n % 256 == 0, n <= 4096. groups > 1: ray r belongs to group
  * r / group_rows (group_rows % 128 == 0, count == groups * group_rows). */
 typedef struct rt_mlp_propose_desc {
   const float* orig; /* float4 per ray */
