@@ -139,13 +139,16 @@ __global__ void __launch_bounds__(128, 1)
 
   if (warp == 0 && lane == 0) {
     const int32_t b0 = (int32_t)(g * E.gn) + n0;
-    for (uint32_t kc = 0; kc < num_k; ++kc) {
+    uint32_t kc = 0;
+    for (; kc < num_k; ++kc) {
       const uint32_t s = kc % kStages;
       if (kc >= kStages && !mbar_wait(empty + s, ((kc / kStages) - 1u) & 1u, err)) break;
       mbar_arrive_expect_tx(full + s, kTileA + tile_b);
       tma_load_2d(sA + s * kTileA, &ta, (int32_t)(kc * kBK), m0, full + s);
       tma_load_2d(sB + s * tile_b, &tb, (int32_t)(kc * kBK), b0, full + s);
     }
+    // the latest load of each stage has landed before the CTA may exit
+    for (uint32_t j = kc > kStages ? kc - kStages : 0u; j < kc; ++j) mbar_wait(full + j % kStages, (j / kStages) & 1u, err);
   } else if (warp == 1 && lane == 0) {
     const uint32_t idesc = idesc_bf16_f32(kBM, bn);
     for (uint32_t kc = 0; kc < num_k; ++kc) {
@@ -226,7 +229,8 @@ __global__ void __launch_bounds__(kArgThreads, 1)
   uint64_t* a_full = empty + kStages;
   uint64_t* acc_full = a_full + 1;   // [2]
   uint64_t* acc_empty = acc_full + 2;  // [2]
-  uint32_t* tmem_slot = (uint32_t*)(acc_empty + 2);
+  uint64_t* mdone = acc_empty + 2;
+  uint32_t* tmem_slot = (uint32_t*)(mdone + 1);
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t grp = blockIdx.y;
   for (uint32_t j = threadIdx.x; j < n; j += kArgThreads) s_bias[j] = bias ? bias[(size_t)grp * n + j] : 0.0f;
@@ -240,6 +244,7 @@ __global__ void __launch_bounds__(kArgThreads, 1)
       mbar_init(acc_full + b, 1);
       mbar_init(acc_empty + b, 256);
     }
+    mbar_init(mdone, 1);
     fence_mbar_init();
     prefetch_tmap(&ta);
     prefetch_tmap(&tb);
@@ -263,13 +268,17 @@ __global__ void __launch_bounds__(kArgThreads, 1)
       mbar_arrive_expect_tx(a_full, num_k * kTileA);
       for (uint32_t kc = 0; kc < num_k; ++kc) tma_load_2d(sA + kc * kTileA, &ta, (int32_t)(kc * kBK), m0, a_full);
       const uint32_t total = ntiles * num_k;
-      for (uint32_t g = 0; g < total; ++g) {
+      uint32_t g = 0;
+      for (; g < total; ++g) {
         const uint32_t s = g % kStages;
         if (g >= kStages && !mbar_wait(empty + s, ((g / kStages) - 1u) & 1u, err)) break;
         const uint32_t t = g / num_k, kc = g % num_k;
         mbar_arrive_expect_tx(full + s, kArgTileB);
         tma_load_2d(sB + s * kArgTileB, &tb, (int32_t)(kc * kBK), (int32_t)(grp * n + t * kArgBN), full + s);
       }
+      // the A block and the latest load of each stage have landed before the CTA may exit
+      mbar_wait(a_full, 0, err);
+      for (uint32_t j = g > kStages ? g - kStages : 0u; j < g; ++j) mbar_wait(full + j % kStages, (j / kStages) & 1u, err);
     }
   } else if (warp == 9) {
     if (lane == 0) {
@@ -293,6 +302,8 @@ __global__ void __launch_bounds__(kArgThreads, 1)
         }
         mma_commit(acc_full + buf);
       }
+      mma_commit(mdone);  // every MMA issued above has completed before TMEM is released
+      mbar_wait(mdone, 0, err);
     }
   } else {
     // epilogue warps 0-7: lane quarter warp % 4, column half warp / 4
@@ -390,7 +401,8 @@ __global__ void __launch_bounds__(kArgThreads, 1)
   uint64_t* acc_empty = acc_full + 2;  // [2]
   uint64_t* xch_a = acc_empty + 2;
   uint64_t* xch_b = xch_a + 1;
-  uint32_t* tmem_slot = (uint32_t*)(xch_b + 1);
+  uint64_t* mdone = xch_b + 1;
+  uint32_t* tmem_slot = (uint32_t*)(mdone + 1);
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t grp = blockIdx.y, n = X.n;
   for (uint32_t j = threadIdx.x; j < n; j += kArgThreads) s_bias[j] = X.bias ? X.bias[(size_t)grp * n + j] : 0.0f;
@@ -406,6 +418,7 @@ __global__ void __launch_bounds__(kArgThreads, 1)
     }
     mbar_init(xch_a, 128);
     mbar_init(xch_b, 128);
+    mbar_init(mdone, 1);
     fence_mbar_init();
     prefetch_tmap(&ta);
     prefetch_tmap(&tb);
@@ -461,6 +474,8 @@ __global__ void __launch_bounds__(kArgThreads, 1)
         }
         if (mok) mma_commit(acc_full + buf);
       }
+      mma_commit(mdone);  // every MMA issued above has completed before TMEM is released
+      mbar_wait(mdone, 0, X.err);
     }
   } else {
     const uint32_t qw = warp & 3u, half = warp >> 2;
