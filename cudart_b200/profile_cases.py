@@ -9,8 +9,8 @@ steady-state launch. Cases (kernel of interest in brackets):
 
   trace_primary  2^20-face soup, 1920x1080 primary rays, tuned tile schedule   [k_trace_accel]
   trace_bounce   the same scene's diffuse bounces, cooperative schedule          [k_trace_coop]
-  mlp_propose    proposal network inference on 2^18 rays (4096 slots)            [k_gemm_argmax_tc, k_gemm_tc]
-  mlp_train      one training step, batch 8192                                   [k_gemm_tc, k_softmax_xent]
+  mlp_propose    proposal network inference on 2^18 rays (4096 slots)            [k_mlp_propose_tc]
+  mlp_train      one training step, batch 8192                                   [k_gemm_xent_tc, k_gemm_tc]
   sah_build      SAH build of the 2^20-face soup                                 [k_sah_small, k_huge_bins, k_sah_big]
   raster         rasteriser, 2^20-face soup, 1920x1080                           [k_raster_zones, k_raster_emit]
   mlp_grouped    64 grouped networks: 3 training steps of 1024 rays each,        [k_gemm_tc, k_softmax_xent, ...]
