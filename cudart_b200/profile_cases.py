@@ -37,7 +37,7 @@ def trace_primary():
     mesh, cam, v, f, tree = _soup_scene()
     c = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
     o, d = core.primary_rays(c, cam.width, cam.height)
-    sch = dict(image_width=cam.width, while_while=True)
+    sch = dict(image_width=cam.width, while_while=True, wide=True)  # the schedule the tuner picks for these rays
     for _ in range(2):
         core.trace(tree, o, d, schedule=sch)
     torch.cuda.synchronize()
@@ -51,7 +51,8 @@ def trace_bounce():
     h = core.trace(tree, o, d)
     b = core.bounce_rays(tree.tris, o, d, h["id"], h["t"], 1234)
     for _ in range(2):
-        core.trace(tree, b[0], b[1], tmax=b[2], schedule=dict(coop=True, sorted=True))
+        core.trace(tree, b[0], b[1], tmax=b[2], schedule=dict(persistent=True, blocks_per_sm=16, while_while=True, sorted=True,
+                                                              coop=True, wide=True))  # the tuner's pick for these rays
     torch.cuda.synchronize()
 
 
