@@ -213,7 +213,7 @@ def run_ours(args, rank, world, local_rank):
     same = torch.equal(cnt1["id"], hits1["id"]) and torch.equal(cnt2["id"], hits2["id"])
     # algorithmic bytes: 32 B ray in + 16 B hit out per ray slot, 32 B per box record read, 48 B per triangle tested
     primary_bytes = 48 * R + 32 * vis1 + 48 * tst1
-    trace_bytes = 48 * (R + R) + 32 * vis + 48 * tst
+    bounce_bytes = 48 * R + 32 * (vis - vis1) + 48 * (tst - tst1)
 
     if world > 1:
         import torch.distributed as dist
@@ -247,10 +247,24 @@ def run_ours(args, rank, world, local_rank):
     value = world * rays_per_step * K / (trace_ms * 1e-3) / 1e6
     build_mtri = world * N * K / (build_ms * 1e-3) / 1e6
     peak, peak_kind = load_peaks()
-    launch_ms = trace1_ms / K  # primary-ray launch, per launch (this rank)
-    achieved = primary_bytes / (launch_ms * 1e-3) / 1e9  # GB/s of one GPU primary-ray launch
-    kernel_name = "k_trace_accel" if getattr(tree, "accel", None) is not None else "k_trace"
-    traffic = load_traffic(kernel_name)
+    # roofline of the dominant kernel: the bounce launch (54% of a step's GPU time in the launch list of
+    # `python -m cudart_b200.profile_cases bench_step`), and of the primary launch beside it
+    def trace_kernel(sch):
+        if getattr(tree, "accel", None) is None:
+            return "k_trace"
+        if sch.get("coop"):
+            return "k_trace_coop_persistent" if sch.get("persistent") else "k_trace_coop"
+        return "k_trace_accel_persistent" if sch.get("persistent") else "k_trace_accel"
+
+    def roofline(bytes_, ms, kernel, what):
+        achieved = bytes_ / (ms * 1e-3) / 1e9  # GB/s of one GPU's launch
+        traffic = load_traffic(kernel)
+        return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "peak_kind": peak_kind, "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
+                "kernel": f"{kernel} ({what}, {R} ray slots)", "algorithmic_bytes_per_launch": bytes_, "launch_ms": round(ms, 4)}
+
+    roof_bounce = roofline(bounce_bytes, trace2_ms / K, trace_kernel(sched2), "bounce-ray launch")
+    roof_primary = roofline(primary_bytes, trace1_ms / K, trace_kernel(sched1), "primary-ray launch")
 
     result = {
         "metric": METRIC,
@@ -275,11 +289,8 @@ def run_ours(args, rank, world, local_rank):
                   "counted_run_identical": bool(same), "schedule_primary": sched1, "schedule_bounce": sched2,
                   "tuning_ms_primary": {json.dumps(k, sort_keys=True): round(v, 4) for k, v in tim1},
                   "tuning_ms_bounce": {json.dumps(k, sort_keys=True): round(v, 4) for k, v in tim2}},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
-                     "kernel": f"{kernel_name} (primary-ray launch, {R} rays)",
-                     "algorithmic_bytes_per_launch": primary_bytes, "launch_ms": round(launch_ms, 4)},
+        "roofline": roof_bounce,
+        "roofline_primary": roof_primary,
         "gpu_launches": int(launches),
         "wall_s_timed": round(t_wall, 3),
     }

@@ -7,6 +7,7 @@ Each case builds its inputs, runs the operation once untimed (warm-up), then
 once more; a profiler capturing the last launch of the named kernel sees a
 steady-state launch. Cases (kernel of interest in brackets):
 
+  bench_step     three steps of the main workload (build, primary, bounce)     [launch list]
   trace_primary  2^20-face soup, 1920x1080 primary rays, tuned tile schedule   [k_trace_accel]
   trace_bounce   the same scene's diffuse bounces, cooperative schedule          [k_trace_coop]
   mlp_propose    proposal network inference on 2^18 rays (4096 slots)            [k_mlp_propose_tc]
@@ -53,6 +54,24 @@ def trace_bounce():
     for _ in range(2):
         core.trace(tree, b[0], b[1], tmax=b[2], schedule=dict(persistent=True, blocks_per_sm=16, while_while=True, sorted=True,
                                                               coop=True, wide=True))  # the tuner's pick for these rays
+    torch.cuda.synchronize()
+
+
+def bench_step():
+    """Three steps of the main workload with the schedules the tuner picks for
+    it: build, primary rays, trace, bounce rays, trace (no tuning launches)."""
+    from . import core
+    mesh, cam, v, f, tree = _soup_scene()
+    c = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
+    W, H = cam.width, cam.height
+    s1 = dict(image_width=W, while_while=True, wide=True)
+    s2 = dict(persistent=True, blocks_per_sm=16, while_while=True, sorted=True, coop=True, wide=True)
+    for _ in range(3):
+        core.build_lbvh(v, f, out=tree)
+        o, d = core.primary_rays(c, W, H)
+        h = core.trace(tree, o, d, schedule=s1)
+        b = core.bounce_rays(tree.tris, o, d, h["id"], h["t"], 1234)
+        core.trace(tree, b[0], b[1], tmax=b[2], schedule=s2)
     torch.cuda.synchronize()
 
 
@@ -115,7 +134,7 @@ def mlp_grouped():
     torch.cuda.synchronize()
 
 
-CASES = {"trace_primary": trace_primary, "trace_bounce": trace_bounce, "mlp_propose": mlp_propose, "mlp_train": mlp_train,
+CASES = {"bench_step": bench_step, "trace_primary": trace_primary, "trace_bounce": trace_bounce, "mlp_propose": mlp_propose, "mlp_train": mlp_train,
          "sah_build": sah_build, "raster": raster, "mlp_grouped": mlp_grouped}
 
 if __name__ == "__main__":
