@@ -449,6 +449,12 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
           if (g < 32) mask |= 1u << g;
         }
       }
+      // the triangles of these groups are tested below, by whichever lanes: count them for this ray
+      if (kCount)
+        for (uint32_t mm = mask; mm; mm &= mm - 1u) {
+          const uint32_t g = __ffs(mm) - 1u;
+          tests += min(cnt, g * 8u + 8u) - g * 8u;
+        }
       // leaves of more than 256 triangles (tree_complete = 0) keep the groups
       // past 32 to this lane: they are tested below by the owner alone
     }
@@ -501,7 +507,6 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
           const float4 v0 = ldg4(A.tris + 3 * (size_t)pos);
           const float4 e1 = ldg4(A.tris + 3 * (size_t)pos + 1);
           const float4 e2 = ldg4(A.tris + 3 * (size_t)pos + 2);
-          if (kCount) ++tests;
           float t, u, v;
           if (!mt_test(oo, od, ozu, ozv, v0, e1, e2, t, u, v)) continue;
           const unsigned long long key = ((unsigned long long)__float_as_uint(t) << 32) | pos;

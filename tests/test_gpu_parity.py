@@ -293,6 +293,29 @@ def test_trace_schedules_identical(T, oracle):
             assert T.equal(a["id"], b["id"]) and T.equal(a["t"], b["t"]) and T.equal(a["uv"], b["uv"]), sch
 
 
+@pytest.mark.parametrize("wide", [False, True])
+def test_coop_counters_follow_the_ray(T, oracle, wide):
+    """The cooperative schedules count each ray's own box reads and triangle
+    tests, whichever lanes ran them: persistent warps (with and without ray
+    sorting, so other warp compositions) give every ray the counts of the
+    one-launch-slot-per-ray schedule."""
+    from cudart_b200 import core
+    mesh = scenes.soup(60000, seed=32)
+    v, f, tree, ref = _check_build(T, oracle, mesh)
+    cam = scenes.Camera((0.5, 0.5, -0.4), (0.5, 0.5, 0.5), scenes.FOV_60, 160, 96)
+    o, d = _rays(T, cam)
+    h = core.trace(tree, o, d)
+    bo, bd, bt = core.bounce_rays(tree.tris, o, d, h["id"], h["t"], 9)
+    base = core.trace(tree, bo, bd, tmax=bt, counters=True, schedule=dict(coop=True, wide=wide))
+    for sch in (dict(coop=True, persistent=True, blocks_per_sm=2, wide=wide),
+                dict(coop=True, persistent=True, blocks_per_sm=8, sorted=True, while_while=True, wide=wide)):
+        out = core.trace(tree, bo, bd, tmax=bt, counters=True, schedule=sch)
+        T.cuda.synchronize()
+        assert T.equal(out["id"], base["id"]) and T.equal(out["t"], base["t"]), sch
+        assert T.equal(out["visits"], base["visits"]) and T.equal(out["tests"], base["tests"]), sch
+    assert int(base["tests"].sum()) > 0
+
+
 @pytest.mark.parametrize("attrs", [False, True])
 def test_interpolate_matches_oracle(T, oracle, attrs):
     from cudart_b200 import core
