@@ -168,7 +168,7 @@ class MlpProposeDesc(C.Structure):
     _fields_ = [("orig", _P), ("dir", _P), ("count", _U32), ("box_lo", C.c_float * 3), ("box_hi", C.c_float * 3), ("w1", _P), ("w2", _P),
                 ("w3", _P), ("w4", _P), ("b1", _P), ("b2", _P), ("b3", _P), ("b4", _P), ("n", _U32), ("groups", _U32),
                 ("group_rows", _U32), ("min_margin", C.c_float), ("out_index", _P), ("out_value", _P), ("out_margin", _P),
-                ("error_word", _P)]
+                ("error_word", _P), ("tmax", _P)]
 
 
 class BatchSlotDesc(C.Structure):

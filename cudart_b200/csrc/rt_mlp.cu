@@ -850,7 +850,20 @@ struct FuseArgs {
   float* out_val;
   float* out_margin;
   uint32_t* err;
+  const float* tmax;  // optional: rays with tmax <= 0 get -1; all-inactive tiles are skipped
 };
+
+// Whether any ray of the tile starting at row0 is active (tmax > 0), computed
+// by a whole warp; every role of the CTA reaches the same answer.
+__device__ __forceinline__ bool tile_active(const FuseArgs& P, uint32_t row0) {
+  if (!P.tmax) return true;
+  bool any = false;
+  for (uint32_t i = lane_id(); i < kBM; i += 32) {
+    const uint32_t row = row0 + i;
+    any |= row < P.count && __ldg(P.tmax + row) > 0.0f;
+  }
+  return __any_sync(0xffffffffu, any);
+}
 
 size_t fuse_smem() {
   return 1024 + 5 * (size_t)kTileA + kFuseStages * (size_t)kFuseStage + 2 * (size_t)kFuseBias * 4 + 3 * kBM * sizeof(Top2) + 24 * 8 +
@@ -931,7 +944,7 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
   };
 
   if (warp == 16) {
-    if (lane == 0) {
+    {
       uint32_t q = 0, k = 0;
       bool ok = true;
       auto load = [&](const CUtensorMap* m, int32_t x, int32_t y, uint32_t bytes) -> bool {
@@ -942,26 +955,40 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
         ++q;
         return true;
       };
-      for (uint32_t tile = blockIdx.x; ok && tile < P.tiles; tile += gridDim.x, ++k) {
-        const uint32_t g = tile * kBM / P.group_rows, bb = k & 1u;
-        if (k >= 2 && !(ok = wait(bias_empty + bb, ((k >> 1) - 1u) & 1u))) break;
-        float* sb = s_bias + bb * kFuseBias;
-        mbar_arrive_expect_tx(bias_full + bb, P.n * 4u + 3u * 512u);
-        bulk_load(sb, P.b4 + (size_t)g * P.n, P.n * 4u, bias_full + bb);
-        bulk_load(sb + kArgMaxN, P.b1 + (size_t)g * 128u, 512u, bias_full + bb);
-        bulk_load(sb + kArgMaxN + 128, P.b2 + (size_t)g * 128u, 512u, bias_full + bb);
-        bulk_load(sb + kArgMaxN + 256, P.b3 + (size_t)g * 128u, 512u, bias_full + bb);
-        for (uint32_t kc = 0; ok && kc < 3; ++kc) ok = load(&t1, (int32_t)(kc * kBK), (int32_t)(g * kBM), kTileA);
-        for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = load(&t2, (int32_t)(kc * kBK), (int32_t)(g * kBM), kTileA);
-        for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = load(&t3, (int32_t)(kc * kBK), (int32_t)(g * kBM), kTileA);
-        for (uint32_t t = 0; ok && t < ntiles; ++t)
-          for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = load(&t4, (int32_t)(kc * kBK), (int32_t)(g * P.n + t * kArgBN), kArgTileB);
+      // lane 0 issues the copies; the whole warp only decides which tiles are active
+      for (uint32_t tile = blockIdx.x; ok && tile < P.tiles; tile += gridDim.x) {
+        if (!tile_active(P, tile * kBM)) continue;
+        bool issued = false;  // the tile's bias copy went out (k counts those)
+        if (lane == 0 && k >= 2) ok = wait(bias_empty + (k & 1u), ((k >> 1) - 1u) & 1u);
+        if (lane == 0 && ok) {
+          const uint32_t g = tile * kBM / P.group_rows, bb = k & 1u;
+          float* sb = s_bias + bb * kFuseBias;
+          issued = true;
+          mbar_arrive_expect_tx(bias_full + bb, P.n * 4u + 3u * 512u);
+          bulk_load(sb, P.b4 + (size_t)g * P.n, P.n * 4u, bias_full + bb);
+          bulk_load(sb + kArgMaxN, P.b1 + (size_t)g * 128u, 512u, bias_full + bb);
+          bulk_load(sb + kArgMaxN + 128, P.b2 + (size_t)g * 128u, 512u, bias_full + bb);
+          bulk_load(sb + kArgMaxN + 256, P.b3 + (size_t)g * 128u, 512u, bias_full + bb);
+          for (uint32_t kc = 0; ok && kc < 3; ++kc) ok = load(&t1, (int32_t)(kc * kBK), (int32_t)(g * kBM), kTileA);
+          for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = load(&t2, (int32_t)(kc * kBK), (int32_t)(g * kBM), kTileA);
+          for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = load(&t3, (int32_t)(kc * kBK), (int32_t)(g * kBM), kTileA);
+          for (uint32_t t = 0; ok && t < ntiles; ++t)
+            for (uint32_t kc = 0; ok && kc < 2; ++kc) ok = load(&t4, (int32_t)(kc * kBK), (int32_t)(g * P.n + t * kArgBN), kArgTileB);
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (__shfl_sync(0xffffffffu, issued, 0)) ++k;
       }
       // the last copy into each stage / bias buffer has landed before the CTA may exit
-      for (uint32_t j = q > kFuseStages ? q - kFuseStages : 0u; j < q; ++j) mbar_wait(full + j % kFuseStages, (j / kFuseStages) & 1u, P.err);
-      for (uint32_t j = k > 2 ? k - 2 : 0u; j < k; ++j) mbar_wait(bias_full + (j & 1u), (j >> 1) & 1u, P.err);
+      if (lane == 0) {
+        for (uint32_t j = q > kFuseStages ? q - kFuseStages : 0u; j < q; ++j)
+          mbar_wait(full + j % kFuseStages, (j / kFuseStages) & 1u, P.err);
+        for (uint32_t j = k > 2 ? k - 2 : 0u; j < k; ++j) mbar_wait(bias_full + (j & 1u), (j >> 1) & 1u, P.err);
+      }
     }
   } else if (warp == 17) {
+    // lane 0 issues the MMAs of this CTA's active tiles (every tile takes the same MMA sequence)
+    uint32_t nact = 0;
+    for (uint32_t tile = blockIdx.x; tile < P.tiles; tile += gridDim.x) nact += tile_active(P, tile * kBM) ? 1u : 0u;
     if (lane == 0) {
       const uint32_t id_h = idesc_bf16_f32(kBM, 128), id_l = idesc_bf16_f32(kBM, kArgBN);
       uint32_t q = 0, xr = 0, hr = 0, n4 = 0;
@@ -978,7 +1005,7 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
         ++q;
         return true;
       };
-      for (uint32_t tile = blockIdx.x; ok && tile < P.tiles; tile += gridDim.x) {
+      for (uint32_t it = 0; ok && it < nact; ++it) {
         ok = wait(x_ready, xr++ & 1u);
         tc_fence_after();
         for (uint32_t kc = 0; ok && kc < 3; ++kc) ok = chunk(tmem, sA + kc * kTileA, id_h, kc == 0);
@@ -1013,8 +1040,16 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
     const uint32_t trow = qw * 32u + lane;  // TMEM lane = tile row of this thread
     uint32_t ld = 0, n4 = 0, k = 0;
     bool ok = true;
-    for (uint32_t tile = blockIdx.x; ok && tile < P.tiles; tile += gridDim.x, ++k) {
+    for (uint32_t tile = blockIdx.x; ok && tile < P.tiles; tile += gridDim.x) {
       const uint32_t row0 = tile * kBM, bb = k & 1u;
+      if (!tile_active(P, row0)) {  // no ray of the tile is active: no proposal
+        if (cq == 0 && row0 + trow < P.count) {
+          P.out_idx[row0 + trow] = -1;
+          if (P.out_val) P.out_val[row0 + trow] = -INFINITY;
+          if (P.out_margin) P.out_margin[row0 + trow] = 0.0f;
+        }
+        continue;
+      }
       // features: (ray r, input i) pairs p = 128 i + r, i < 6
       for (uint32_t p = tid; p < 6u * kBM; p += kFuseCompute) {
         const uint32_t r = p & 127u, i = p >> 7, row = row0 + r;
@@ -1118,11 +1153,13 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
         const uint32_t row = row0 + trow;
         if (row < P.count) {
           const float margin = res.best - res.second;
-          P.out_idx[row] = margin >= P.min_margin ? res.idx : -1;
+          const bool active = !P.tmax || __ldg(P.tmax + row) > 0.0f;
+          P.out_idx[row] = (active && margin >= P.min_margin) ? res.idx : -1;
           if (P.out_val) P.out_val[row] = res.best;
           if (P.out_margin) P.out_margin[row] = margin;
         }
       }
+      ++k;
     }
   }
   tc_fence_before();
@@ -1291,6 +1328,7 @@ extern "C" rt_status rt_mlp_propose(const rt_mlp_propose_desc* d, rt_stream stre
   P.tiles = (d->count + kBM - 1) / kBM;
   P.group_rows = G > 1 ? d->group_rows : P.tiles * kBM;
   P.min_margin = d->min_margin; P.out_idx = d->out_index; P.out_val = d->out_value; P.out_margin = d->out_margin; P.err = d->error_word;
+  P.tmax = d->tmax;
   static std::once_flag once;
   std::call_once(once, [] {
     cudaFuncSetAttribute(k_mlp_propose_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fuse_smem());

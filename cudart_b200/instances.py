@@ -108,7 +108,7 @@ class InstancedFrames:
         h1 = proposal.batch_trace_seeded(self.tree, self.orig, self.dir, self.ray_offsets, p1, self.slots, in_proposal=in_proposal,
                                          out=out.get("h1"))
         b = self.bounce(h1, out=out.get("b"))
-        p2 = self.nets.propose(b[0], b[1], self.box, R, out=out.get("p2"))
+        p2 = self.nets.propose(b[0], b[1], self.box, R, out=out.get("p2"), tmax=b[2])  # bounces of misses are inactive
         h2 = proposal.batch_trace_seeded(self.tree, b[0], b[1], self.ray_offsets, p2, self.slots, tmax=b[2], in_proposal=in_proposal,
                                          out=out.get("h2"))
         return dict(p1=p1, h1=h1, b=b, p2=p2, h2=h2)

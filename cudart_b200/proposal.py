@@ -109,10 +109,11 @@ def gemm_xent(a: torch.Tensor, b: torch.Tensor, bias, labels, scale: float, g: t
 
 
 def mlp_propose(orig, dir, box, W16, b, out=None, groups: int = 1, group_rows: int = 0, min_margin: float = 0.0, margin=None,
-                value=None, err=None, count=None, stream=None):
+                value=None, err=None, count=None, tmax=None, stream=None):
     """Fused proposal (rt_mlp_propose): features, hidden layers and argmax in
     one launch. W16 / b: the four BF16 weight matrices and FP32 biases (grouped:
-    stacked along rows)."""
+    stacked along rows). tmax: rays with tmax <= 0 get -1 (tiles of 128 such
+    rays cost nothing)."""
     R = orig.shape[0] if count is None else count
     if out is None:
         out = torch.empty(R, dtype=torch.int32, device=orig.device)
@@ -126,6 +127,7 @@ def mlp_propose(orig, dir, box, W16, b, out=None, groups: int = 1, group_rows: i
     d.n = W16[3].shape[0] // groups
     d.groups, d.group_rows, d.min_margin = groups, group_rows, float(min_margin)
     d.out_index, d.out_value, d.out_margin, d.error_word = out.data_ptr(), _p(value), _p(margin), _p(err)
+    d.tmax = _p(tmax)
     _check("rt_mlp_propose", _abi.lib().rt_mlp_propose(C.byref(d), _stream(stream)))
     return out
 
@@ -457,9 +459,10 @@ class ProposalGroup:
         return loss
 
     def propose(self, orig, dir, box, group_rays: int, out=None, min_margin: float = 0.0, chunk_rows: int = 1 << 22, fused: bool = True,
-                margin=None, stream=None):
+                margin=None, tmax=None, stream=None):
         """Slot proposal per ray; group g's rays are rows g * group_rays ..
-        (group_rays % 128 == 0), scored by group g's network."""
+        (group_rays % 128 == 0), scored by group g's network; rays with
+        tmax <= 0 (when given) get -1."""
         G = self.groups
         if group_rays % 128 or orig.shape[0] != G * group_rays:
             raise ValueError("need groups * group_rays rays with group_rays % 128 == 0")
@@ -467,7 +470,7 @@ class ProposalGroup:
             out = torch.empty(G * group_rays, dtype=torch.int32, device=orig.device)
         if fused:
             return mlp_propose(orig, dir, box, self.W16, self.b, out=out, groups=G, group_rows=group_rays, min_margin=min_margin,
-                               margin=margin, err=self.err, stream=stream)
+                               margin=margin, err=self.err, tmax=tmax, stream=stream)
         cg = max(1, min(G, chunk_rows // group_rays))
         ws = self._workspace(cg * group_rays, False)
         for g0 in range(0, G, cg):
@@ -482,6 +485,8 @@ class ProposalGroup:
             gemm(H1, wv[1], bias=bv[1], relu=True, out_bf16=H2, **kw)
             gemm(H2, wv[2], bias=bv[2], relu=True, out_bf16=H3, **kw)
             gemm_argmax(H3, wv[3], bias=bv[3], out_index=out[r0:r1], min_margin=min_margin, **kw)
+        if tmax is not None:
+            out.masked_fill_(~(tmax > 0), -1)
         return out
 
 

@@ -88,7 +88,9 @@ rt_status rt_gemm_argmax_bf16(const rt_gemm_argmax_desc* d, rt_stream stream);
  * activation written to memory. Weights BF16, rows contiguous: w1 [groups 128][192],
  * w2, w3 [groups 128][128], w4 [groups n][128]; biases FP32 [groups 128] (b1..b3),
  * [groups n] (b4); all pointers 16-byte aligned. n % 256 == 0, n <= 4096. groups > 1: ray r belongs to group
- * r / group_rows (group_rows % 128 == 0, count == groups * group_rows). */
+ * r / group_rows (group_rows % 128 == 0, count == groups * group_rows).
+ * tmax (optional): rays with tmax <= 0 (inactive: a bounce of a ray that
+ * missed) get -1, and a tile of 128 rays that are all inactive costs no MMA. */
 typedef struct rt_mlp_propose_desc {
   const float* orig; /* float4 per ray */
   const float* dir;
@@ -109,6 +111,7 @@ typedef struct rt_mlp_propose_desc {
   float* out_value;  /* optional */
   float* out_margin; /* optional */
   uint32_t* error_word;
+  const float* tmax; /* optional */
 } rt_mlp_propose_desc;
 rt_status rt_mlp_propose(const rt_mlp_propose_desc* d, rt_stream stream);
 

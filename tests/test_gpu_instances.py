@@ -117,6 +117,28 @@ def test_grouped_fused_propose_matches_layered(G, R):
     assert torch.equal(a, b)
 
 
+def test_fused_propose_skips_inactive_rays():
+    """With tmax, inactive rays (tmax <= 0) get -1 and whole inactive tiles are
+    skipped; every active ray keeps the layered path's proposal."""
+    from cudart_b200 import proposal, scenes
+    box = (-1.5, -0.6, -1.5, 1.5, 1.4, 1.5)
+    G, R = 3, 1024
+    grp = proposal.ProposalGroup(G, seed=4)
+    o, d = scenes.box_rays_torch(G * R, box, seed=43)
+    g = torch.Generator(device="cuda").manual_seed(8)
+    tmax = torch.where(torch.rand(G * R, device="cuda", generator=g) < 0.5, 1e30, -1.0).float()
+    tmax[200:700] = -1.0             # tiles 2..4 of group 0 wholly inactive (rows 256..639)
+    tmax[R + 128: R + 256] = 0.0     # one inactive tile of group 1
+    tmax[2 * R:] = 1.0               # group 2 all active
+    a = grp.propose(o, d, box, R, tmax=tmax, fused=True)
+    b = grp.propose(o, d, box, R, fused=False)
+    torch.cuda.synchronize()
+    active = tmax > 0
+    assert torch.equal(a[active], b[active])
+    assert bool((a[~active] == -1).all())
+    assert int(grp.err.item()) == 0
+
+
 def test_group_select_and_index_gather():
     from cudart_b200 import proposal
     G, S = 3, 5000
