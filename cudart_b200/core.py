@@ -171,6 +171,8 @@ def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_de
         d.accel = out.accel.data_ptr()
         d.accel_bytes = out.accel.numel()
     _abi.check("rt_lbvh_build", _abi.lib().rt_lbvh_build(C.byref(d), _stream(stream)))
+    if hitbox is not None:  # the scene box for ray ordering, known on the host: no device read later
+        out._box = [float(hitbox[i]) for i in (0, 1, 2, 4, 5, 6)]
     return out
 
 
@@ -321,7 +323,10 @@ def trace_desc(tree: Tree, orig, dir, tmax=None, id_mode: int = 0, counters: boo
 
 
 def tree_box(tree: Tree):
-    """Scene box for ray ordering (host floats), read once from the root node and cached on the tree."""
+    """Scene box for ray ordering (host floats): the hitbox given to build_lbvh,
+    else read once from the root node and cached on the tree. A Tree rebuilt
+    in place from other geometry without a hitbox keeps the first box; the
+    order only affects speed, never the hits."""
     box = getattr(tree, "_box", None)
     if box is None:
         root = tree.nodes[0].cpu().view(torch.float32).tolist()
