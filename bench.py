@@ -399,18 +399,20 @@ def batched(args, dev, world, count=1024):
     del p, q, cen, rad, mesh_of_ray
     roff = torch.tensor(ro.astype(np.int32), device=dev)
     tree = core.batch_build(V, Fc, fo, vo)
-    hits = core.batch_trace(tree, orig, dirs, roff)
+    from cudart_b200 import tune
+    sched, tim = tune.tune_batch_trace(tree, orig, dirs, roff, key=f"batch{count}", use_cache=False)  # untimed
+    hits = core.batch_trace(tree, orig, dirs, roff, schedule=sched)
     torch.cuda.synchronize()
     graph = torch.cuda.CUDAGraph()
     cap = torch.cuda.Stream()
     cap.wait_stream(torch.cuda.current_stream())
     with torch.cuda.stream(cap):
         core.batch_build(V, Fc, fo, vo, out=tree)
-        core.batch_trace(tree, orig, dirs, roff, out=hits)
+        core.batch_trace(tree, orig, dirs, roff, out=hits, schedule=sched)
         torch.cuda.synchronize()
         with torch.cuda.graph(graph, stream=cap):
             core.batch_build(V, Fc, fo, vo, out=tree)
-            core.batch_trace(tree, orig, dirs, roff, out=hits)
+            core.batch_trace(tree, orig, dirs, roff, out=hits, schedule=sched)
     torch.cuda.current_stream().wait_stream(cap)
     torch.cuda.synchronize()
     reps = 3
@@ -429,14 +431,15 @@ def batched(args, dev, world, count=1024):
     b0.record()
     core.batch_build(V, Fc, fo, vo, out=tree)
     b1.record()
-    core.batch_trace(tree, orig, dirs, roff, out=hits)
+    core.batch_trace(tree, orig, dirs, roff, out=hits, schedule=sched)
     t1.record()
     torch.cuda.synchronize()
     build_ms, trace_ms = b0.elapsed_time(b1), b1.elapsed_time(t1)
     info = tree.info.cpu().numpy()
     hit_frac = float((hits["id"] >= 0).float().mean().item())
     N = int(fo[-1])
-    res = {"meshes": count, "faces": N, "rays": R, "graph_ms_per_step": round(graph_ms, 4),
+    res = {"meshes": count, "faces": N, "rays": R, "schedule": sched,
+           "tuning_ms": {json.dumps(k, sort_keys=True): round(v, 3) for k, v in tim}, "graph_ms_per_step": round(graph_ms, 4),
            "graph_mrays_s": round(world * R / (graph_ms * 1e-3) / 1e6, 2), "build_ms": round(build_ms, 4),
            "build_mtri_s": round(world * N / (build_ms * 1e-3) / 1e6, 2), "trace_ms": round(trace_ms, 4),
            "trace_mrays_s": round(world * R / (trace_ms * 1e-3) / 1e6, 2), "hit_fraction": round(hit_frac, 4),
@@ -678,6 +681,7 @@ def instanced(args, dev, world, scale=1 / 16, width=960, height=540, steps=200, 
     w.displace(0)
     w.build()
     w.make_slots()
+    sched, _ = w.tune()
     plain = w.trace_plain()
     learned = w.trace_learned()
     w.remember(plain)
@@ -722,7 +726,7 @@ def instanced(args, dev, world, scale=1 / 16, width=960, height=540, steps=200, 
     nn_ms = sum(e[3].elapsed_time(e[4]) for e in ev)
     rays = frames * R + int(active.item())  # primaries + active bounces
     F = w.face_count
-    return {"instances": count, "faces_per_frame": F, "frames": frames, "tile": [width // 2, height // 2], "spp": 4,
+    return {"instances": count, "faces_per_frame": F, "frames": frames, "tile": [width // 2, height // 2], "spp": 4, "schedule": sched,
             "primary_rays_per_frame": R, "rays_timed": rays, "finetune_steps_per_frame": steps, "batch_per_instance": batch,
             "build_ms_per_frame": round(build_ms / frames, 3), "build_mtri_s": round(world * F * frames / (build_ms * 1e-3) / 1e6, 1),
             "finetune_ms_per_frame": round(tune_ms / frames, 3),

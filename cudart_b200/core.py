@@ -576,15 +576,17 @@ def batch_build(vertices: torch.Tensor, faces: torch.Tensor, face_offsets: list,
 
 
 def batch_trace(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax=None, id_mode: int = 0, counters: bool = False,
-                while_while: bool = True, out: dict | None = None, stream=None) -> dict:
-    """Closest hits for the rays of all meshes (rays of mesh m: ray_offsets[m] .. ray_offsets[m+1])."""
-    d, out = batch_trace_desc(tree, orig, dir, ray_offsets, tmax, id_mode, counters, while_while, out)
+                while_while: bool = True, out: dict | None = None, schedule: dict | None = None, stream=None) -> dict:
+    """Closest hits for the rays of all meshes (rays of mesh m: ray_offsets[m] .. ray_offsets[m+1]).
+    schedule (results never depend on it): while_while, wide (4-wide records),
+    persistent + blocks_per_sm (warps fetching 32 rays at a time)."""
+    d, out = batch_trace_desc(tree, orig, dir, ray_offsets, tmax, id_mode, counters, while_while, out, schedule)
     _abi.check("rt_batch_trace", _abi.lib().rt_batch_trace(C.byref(d), _stream(stream)))
     return out
 
 
 def batch_trace_desc(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax=None, id_mode: int = 0, counters: bool = False,
-                     while_while: bool = True, out: dict | None = None):
+                     while_while: bool = True, out: dict | None = None, schedule: dict | None = None):
     """The rt_batch_trace_desc of batch_trace and its output tensors."""
     R = orig.shape[0]
     dev = orig.device
@@ -602,5 +604,12 @@ def batch_trace_desc(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax
     d.hit_id, d.hit_t, d.hit_uv, d.error_word = out["id"].data_ptr(), out["t"].data_ptr(), out["uv"].data_ptr(), out["err"].data_ptr()
     if "visits" in out:
         d.ray_visits, d.ray_tests = out["visits"].data_ptr(), out["tests"].data_ptr()
-    d.schedule = _abi.TRACE_WHILE_WHILE if while_while else 0
+    sch = dict(while_while=while_while) if schedule is None else schedule
+    d.schedule = ((_abi.TRACE_WHILE_WHILE if sch.get("while_while", False) else 0)
+                  | (_abi.TRACE_WIDE if sch.get("wide", False) else 0))
+    if sch.get("persistent", False):
+        if "_counter" not in out:
+            out["_counter"] = torch.zeros(1, dtype=torch.int32, device=dev)
+        d.work_counter = out["_counter"].data_ptr()
+        d.persistent_blocks_per_sm = int(sch.get("blocks_per_sm", 8))
     return d, out

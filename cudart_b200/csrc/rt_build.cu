@@ -822,6 +822,7 @@ struct BatchArgs {
   float4* tnodes;         // [4 N]
   uint4* acc_leaves;      // [N]
   float4* groups;         // [2 (N + N/8 + M + 1)]
+  float4* wide;           // [8 N]
   rt_build_info* info_out;
 };
 
@@ -988,6 +989,19 @@ __global__ __launch_bounds__(256) void k_batch_accel_nodes(BatchArgs B) {
   }
 }
 
+// 4-wide records of every mesh (after all two-child records exist).
+__global__ __launch_bounds__(256) void k_batch_wide_nodes(BatchArgs B) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < B.N; p += gridDim.x * blockDim.x) {
+    const uint32_t m = find_seg(B.foff, B.M, p);
+    const uint32_t F = __ldg(B.foff + m);
+    const uint32_t* h = B.hdr + 16 * m;
+    if (h[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) continue;
+    const uint32_t leaves = B.acc_hdr[64 * (size_t)m + 1];
+    const uint32_t lp = p - F;
+    if (lp + 1 < leaves) wide_node(B.tnodes + 4 * (size_t)F, B.wide + 8 * (size_t)F, lp);
+  }
+}
+
 __global__ void k_batch_info(BatchArgs B) {
   for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < B.M; m += gridDim.x * blockDim.x) {
     const uint32_t* h = B.hdr + 16 * m;
@@ -1027,7 +1041,7 @@ size_t carve_batch(Carve& c, BatchArgs& B, uint32_t M, uint32_t N) {
 size_t carve_batch_accel(Carve& c, BatchArgs& B, uint32_t M, uint32_t N) {
   BatchAccel L;
   const size_t bytes = carve_batch_accel_layout(c, L, M, N);
-  B.acc_hdr = L.hdr; B.tnodes = L.tnodes; B.acc_leaves = L.leaves; B.groups = L.groups;
+  B.acc_hdr = L.hdr; B.tnodes = L.tnodes; B.acc_leaves = L.leaves; B.groups = L.groups; B.wide = L.wide;
   return bytes;
 }
 
@@ -1104,8 +1118,9 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   if (cudaMemsetAsync(B.arrive, 0, (2 * (size_t)N) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   k_batch_leaves<<<sms * 8, 256, 0, st>>>(B);
   k_batch_accel_nodes<<<sms * 4, 256, 0, st>>>(B);
+  k_batch_wide_nodes<<<sms * 4, 256, 0, st>>>(B);
   k_batch_info<<<(M + 255) / 256, 256, 0, st>>>(B);
-  note_launch(3);
+  note_launch(4);
   RT_CHECK_LAUNCH();
   return RT_OK;
 }

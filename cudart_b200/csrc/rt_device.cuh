@@ -313,17 +313,21 @@ __host__ __device__ __forceinline__ uint32_t group_base(uint32_t F, uint32_t m) 
 
 // Batched traversal blob: per-mesh headers (64 words), two-child records at
 // 4 F_m, leaf tables at F_m, group boxes at 2 group_base(F_m, m).
+// Mesh m (F = faces before it) owns header words 64 m .., two-child records
+// 4 F .., leaves F .., group boxes 2 group_base(F, m) .. and 4-wide records 8 F ..
 struct BatchAccel {
   uint32_t* hdr;
   float4* tnodes;
   uint4* leaves;
   float4* groups;
+  float4* wide;
 };
 inline size_t carve_batch_accel_layout(Carve& c, BatchAccel& L, uint32_t M, uint32_t N) {
   L.hdr = c.take<uint32_t>(64 * (size_t)M);
   L.tnodes = c.take<float4>(4 * (size_t)N);
   L.leaves = c.take<uint4>(N);
   L.groups = c.take<float4>(2 * ((size_t)N + N / 8 + M + 1));
+  L.wide = c.take<float4>(8 * (size_t)N);
   return c.off + 256;
 }
 

@@ -651,10 +651,8 @@ struct BatchTraceArgs {
 };
 
 // Seeded: the slot tables of mesh m start at m slot_count entries.
-template <bool kCount, bool kWW, bool kSeed>
-__global__ __launch_bounds__(128) void k_batch_trace(TraceArgs A, BatchTraceArgs B, SeedArgs S) {
-  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= A.ray_count) return;
+template <bool kCount, bool kWW, bool kSeed, bool kWide>
+__device__ __forceinline__ void batch_trace_ray(uint32_t r, const TraceArgs& A, const BatchTraceArgs& B, const SeedArgs& S) {
   const uint32_t m = find_seg(B.roff, B.M, r);
   const uint32_t F = __ldg(B.foff + m);
   AccelArgs C;
@@ -662,6 +660,7 @@ __global__ __launch_bounds__(128) void k_batch_trace(TraceArgs A, BatchTraceArgs
   C.tnodes = B.acc.tnodes + 4 * (size_t)F;
   C.leaves = B.acc.leaves + F;
   C.groups = B.acc.groups + 2 * (size_t)group_base(F, m);
+  C.wide = B.acc.wide + 8 * (size_t)F;
   TraceArgs Am = A;
   Am.tris = A.tris + 3 * (size_t)F;
   Am.indices = A.indices + F;
@@ -669,9 +668,29 @@ __global__ __launch_bounds__(128) void k_batch_trace(TraceArgs A, BatchTraceArgs
     SeedArgs Sm = S;
     Sm.slot_ref = S.slot_ref + (size_t)m * S.slot_count;
     if (S.slot_box) Sm.slot_box = S.slot_box + 2 * (size_t)m * S.slot_count;
-    trace_ray_accel<kCount, kWW, true>(r, Am, C, Sm);
+    trace_ray_accel<kCount, kWW, true, kWide>(r, Am, C, Sm);
   } else {
-    trace_ray_accel<kCount, kWW>(r, Am, C);
+    trace_ray_accel<kCount, kWW, false, kWide>(r, Am, C);
+  }
+}
+
+template <bool kCount, bool kWW, bool kSeed, bool kWide>
+__global__ __launch_bounds__(128) void k_batch_trace(TraceArgs A, BatchTraceArgs B, SeedArgs S) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < A.ray_count) batch_trace_ray<kCount, kWW, kSeed, kWide>(r, A, B, S);
+}
+
+// Persistent warps over the batched rays: 32 rays at a time from a global counter.
+template <bool kCount, bool kWW, bool kSeed, bool kWide>
+__global__ __launch_bounds__(128) void k_batch_trace_persistent(TraceArgs A, BatchTraceArgs B, SeedArgs S, uint32_t* counter) {
+  const uint32_t lane = lane_id();
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= A.ray_count) break;
+    const uint32_t r = base + lane;
+    if (r < A.ray_count) batch_trace_ray<kCount, kWW, kSeed, kWide>(r, A, B, S);
   }
 }
 
@@ -967,6 +986,35 @@ extern "C" rt_status rt_bounce_rays(const float* tris, const float* orig, const 
 }
 
 namespace {
+template <bool kSeed, bool kWide>
+rt_status batch_launch_w(const rt_batch_trace_desc* d, const TraceArgs& A, const BatchTraceArgs& B, const SeedArgs& S, cudaStream_t st,
+                         bool count, bool ww) {
+  if (d->work_counter) {
+    if (cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
+    const uint32_t per_sm = d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u;
+    const uint32_t blocks = (uint32_t)hmin<uint64_t>((uint64_t)sms() * per_sm, (d->ray_count + 127) / 128);
+    if (count) {
+      if (ww) k_batch_trace_persistent<true, true, kSeed, kWide><<<blocks, 128, 0, st>>>(A, B, S, d->work_counter);
+      else k_batch_trace_persistent<true, false, kSeed, kWide><<<blocks, 128, 0, st>>>(A, B, S, d->work_counter);
+    } else {
+      if (ww) k_batch_trace_persistent<false, true, kSeed, kWide><<<blocks, 128, 0, st>>>(A, B, S, d->work_counter);
+      else k_batch_trace_persistent<false, false, kSeed, kWide><<<blocks, 128, 0, st>>>(A, B, S, d->work_counter);
+    }
+  } else {
+    const uint32_t blocks = (d->ray_count + 127) / 128;
+    if (count) {
+      if (ww) k_batch_trace<true, true, kSeed, kWide><<<blocks, 128, 0, st>>>(A, B, S);
+      else k_batch_trace<true, false, kSeed, kWide><<<blocks, 128, 0, st>>>(A, B, S);
+    } else {
+      if (ww) k_batch_trace<false, true, kSeed, kWide><<<blocks, 128, 0, st>>>(A, B, S);
+      else k_batch_trace<false, false, kSeed, kWide><<<blocks, 128, 0, st>>>(A, B, S);
+    }
+  }
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
 template <bool kSeed>
 rt_status batch_launch(const rt_batch_trace_desc* d, const SeedArgs& S, cudaStream_t st) {
   TraceArgs A = {};
@@ -979,17 +1027,8 @@ rt_status batch_launch(const rt_batch_trace_desc* d, const SeedArgs& S, cudaStre
   carve_batch_accel_layout(c, B.acc, d->mesh_count, d->face_count);
   const bool count = d->ray_visits || d->ray_tests;
   const bool ww = (d->schedule & RT_TRACE_WHILE_WHILE) != 0;
-  const uint32_t blocks = (d->ray_count + 127) / 128;
-  if (count) {
-    if (ww) k_batch_trace<true, true, kSeed><<<blocks, 128, 0, st>>>(A, B, S);
-    else k_batch_trace<true, false, kSeed><<<blocks, 128, 0, st>>>(A, B, S);
-  } else {
-    if (ww) k_batch_trace<false, true, kSeed><<<blocks, 128, 0, st>>>(A, B, S);
-    else k_batch_trace<false, false, kSeed><<<blocks, 128, 0, st>>>(A, B, S);
-  }
-  note_launch();
-  RT_CHECK_LAUNCH();
-  return RT_OK;
+  if (d->schedule & RT_TRACE_WIDE) return batch_launch_w<kSeed, true>(d, A, B, S, st, count, ww);
+  return batch_launch_w<kSeed, false>(d, A, B, S, st, count, ww);
 }
 
 rt_status batch_check(const rt_batch_trace_desc* d) {

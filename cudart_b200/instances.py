@@ -65,6 +65,7 @@ class InstancedFrames:
         self.tree = None
         self.slots = None
         self.frame_index = -1
+        self.schedule = None  # batched traversal schedule (tune() picks one); results never depend on it
         self.prev = None  # (bounce orig, bounce dir, primary labels, bounce labels) of the previous frame
 
     @property
@@ -92,12 +93,18 @@ class InstancedFrames:
         gpos = torch.where(hits["id"] >= 0, hits["id"] + self.ray_face_base, hits["id"])
         return core.bounce_rays(self.tree.tris, self.orig, self.dir, gpos, hits["t"], 1000 + self.frame_index, out=out)
 
+    def tune(self):
+        """Pick the batched traversal schedule on this frame's primary rays (untimed)."""
+        from . import tune
+        self.schedule, timings = tune.tune_batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, use_cache=False)
+        return self.schedule, timings
+
     def trace_plain(self, out=None):
         """Primary hits, bounce rays and bounce hits through rt_batch_trace."""
         out = out or {}
-        h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, out=out.get("h1"))
+        h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, out=out.get("h1"), schedule=self.schedule)
         b = self.bounce(h1, out=out.get("b"))
-        h2 = core.batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], out=out.get("h2"))
+        h2 = core.batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], out=out.get("h2"), schedule=self.schedule)
         return dict(h1=h1, b=b, h2=h2)
 
     def trace_learned(self, out=None, in_proposal: bool = False):
@@ -106,11 +113,11 @@ class InstancedFrames:
         R = self.rays_per_instance
         p1 = self.nets.propose(self.orig, self.dir, self.box, R, out=out.get("p1"))
         h1 = proposal.batch_trace_seeded(self.tree, self.orig, self.dir, self.ray_offsets, p1, self.slots, in_proposal=in_proposal,
-                                         out=out.get("h1"))
+                                         out=out.get("h1"), schedule=self.schedule)
         b = self.bounce(h1, out=out.get("b"))
         p2 = self.nets.propose(b[0], b[1], self.box, R, out=out.get("p2"), tmax=b[2])  # bounces of misses are inactive
         h2 = proposal.batch_trace_seeded(self.tree, b[0], b[1], self.ray_offsets, p2, self.slots, tmax=b[2], in_proposal=in_proposal,
-                                         out=out.get("h2"))
+                                         out=out.get("h2"), schedule=self.schedule)
         return dict(p1=p1, h1=h1, b=b, p2=p2, h2=h2)
 
     def labels(self, plain):

@@ -85,3 +85,39 @@ def tune_trace(tree, orig, dir, tmax=None, image_width: int = 0, key: str = "def
         cache[ck] = {"best": best, "timings": timings}
         _store(cache)
     return best, timings
+
+
+def batch_candidates():
+    """Schedules of the batched traversal (rt_batch_trace)."""
+    out = []
+    for ww, wide in itertools.product((False, True), (False, True)):
+        out.append({"while_while": ww, "wide": wide, "persistent": False, "blocks_per_sm": 0})
+        for bps in (8, 16):
+            out.append({"while_while": ww, "wide": wide, "persistent": True, "blocks_per_sm": bps})
+    return out
+
+
+def tune_batch_trace(tree, orig, dir, ray_offsets, tmax=None, key: str = "batch", reps: int = 2, use_cache: bool = True):
+    """tune_trace for core.batch_trace: (best_schedule, [(schedule, ms), ...])."""
+    gpu = torch.cuda.get_device_name(orig.device)
+    cache = _load() if use_cache else {}
+    ck = f"{gpu}|{key}"
+    if ck in cache:
+        return cache[ck]["best"], cache[ck]["timings"]
+    out = core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax)
+    stream = torch.cuda.current_stream()
+    timings = []
+    for sch in batch_candidates():
+        core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax, out=out, schedule=sch)  # warm
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax, out=out, schedule=sch)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        timings.append((sch, e0.elapsed_time(e1) / reps))
+    best = min(timings, key=lambda x: x[1])[0]
+    if use_cache:
+        cache[ck] = {"best": best, "timings": timings}
+        _store(cache)
+    return best, timings

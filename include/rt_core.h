@@ -35,7 +35,7 @@ typedef struct CUstream_st* rt_stream; /* a cudaStream_t; NULL = legacy default 
 /* Layout version of the structs below. A caller compiled against this header
  * must check rt_abi_version() == RT_ABI_VERSION before passing any struct:
  * a library built from a different header reads different field offsets. */
-#define RT_ABI_VERSION 5u
+#define RT_ABI_VERSION 6u
 
 typedef enum rt_status {
   RT_OK = 0,
@@ -171,7 +171,9 @@ typedef struct rt_batch_trace_desc {
   uint32_t* ray_visits;
   uint32_t* ray_tests;
   uint32_t* error_word;
-  uint32_t schedule;              /* RT_TRACE_WHILE_WHILE */
+  uint32_t schedule;              /* RT_TRACE_WHILE_WHILE, RT_TRACE_WIDE */
+  uint32_t* work_counter;         /* optional device word: persistent warps fetch rays through it (the call zeroes it) */
+  uint32_t persistent_blocks_per_sm; /* with work_counter: CTAs of 128 threads per SM (0 = 8) */
 } rt_batch_trace_desc;
 rt_status rt_batch_trace(const rt_batch_trace_desc* desc, rt_stream stream);
 
@@ -257,7 +259,7 @@ typedef struct rt_trace_desc {
 
 #define RT_TRACE_WHILE_WHILE 0x1u /* descend until a leaf is held, then test it (else: interleaved) */
 #define RT_TRACE_COOP 0x2u        /* the warp's lanes share the triangle tests of all its rays' leaves */
-#define RT_TRACE_WIDE 0x4u /* descend through the blob's 4-wide records (single-mesh builds) */
+#define RT_TRACE_WIDE 0x4u /* descend through the blob's 4-wide records */
 
 /* A tracing order for incoherent rays: ray indices sorted by direction octant,
  * then by the Morton code of the origin inside box (min xyz, max xyz, HOST);

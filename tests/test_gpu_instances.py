@@ -231,9 +231,11 @@ def test_batch_seeded_trace_is_bit_exact():
     g = torch.Generator(device="cuda").manual_seed(1)
     R = o.shape[0]
     rnd = torch.randint(-2, 4200, (R,), dtype=torch.int32, device="cuda", generator=g)  # includes none and out of range
+    sch_wide = dict(while_while=True, wide=True, persistent=True, blocks_per_sm=4)
     for prop in (labels, rnd):
-        for box_test in (True, False):
-            s = proposal.batch_trace_seeded(bt, o, d, roff, prop, slots, counters=True, in_proposal=True, box_test=box_test)
+        for box_test, sch in ((True, None), (False, None), (True, sch_wide)):
+            s = proposal.batch_trace_seeded(bt, o, d, roff, prop, slots, counters=True, in_proposal=True, box_test=box_test,
+                                            schedule=sch)
             torch.cuda.synchronize()
             assert int(s["err"].item()) == 0
             assert torch.equal(s["id"], plain["id"])

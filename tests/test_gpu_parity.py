@@ -386,3 +386,11 @@ def test_batch_build_and_trace_match_single_mesh(T, oracle):
         sl = slice(ro[m], ro[m + 1])
         assert T.equal(hits["id"][sl], single["id"]) and T.equal(hits["t"][sl], single["t"]) and T.equal(hits["uv"][sl], single["uv"]), m
     assert int(_host(hits["err"])[0]) == 0
+    # every schedule of the batched traversal (4-wide records, persistent warps) returns the same bits
+    from cudart_b200 import tune
+    roff = T.tensor(ro, dtype=T.int32, device="cuda")
+    for sch in tune.batch_candidates():
+        h = core.batch_trace(bt, O, D, roff, schedule=sch)
+        T.cuda.synchronize()
+        assert int(_host(h["err"])[0]) == 0, sch
+        assert T.equal(h["id"], hits["id"]) and T.equal(h["t"], hits["t"]) and T.equal(h["uv"], hits["uv"]), sch
