@@ -60,6 +60,32 @@ def parse():
     return ap.parse_args()
 
 
+def capture_graphs(stages):
+    """One CUDA graph per callable (each run once eagerly first, on a side stream).
+    Returns the graphs and the number of this library's kernel launches they hold."""
+    import torch
+
+    from cudart_b200 import _abi
+
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    graphs = []
+    with torch.cuda.stream(side):
+        for fn in stages:
+            fn()
+        torch.cuda.synchronize()
+        n0 = _abi.lib().rt_launch_count()
+        for fn in stages:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=side):
+                fn()
+            graphs.append(g)
+        kernels = _abi.lib().rt_launch_count() - n0
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    return graphs, int(kernels)
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -178,18 +204,20 @@ def run_ours(args, rank, world, local_rank):
     sched1, tim1 = tune.tune_trace(tree, rays[0], rays[1], image_width=W, key=f"soup{N}-primary", use_cache=False)
     sched2, tim2 = tune.tune_trace(tree, bounce[0], bounce[1], tmax=bounce[2], image_width=W, key=f"soup{N}-bounce", use_cache=False)
 
+    # each stage of a step is captured once as a CUDA graph and replayed (one launch per stage), with the
+    # timing events recorded between the replays
+    stages = [lambda: core.build_lbvh(v, f, out=tree),
+              lambda: core.primary_rays(camera, W, H, out=rays),
+              lambda: core.trace(tree, rays[0], rays[1], out=hits1, schedule=sched1),
+              lambda: core.bounce_rays(tree.tris, rays[0], rays[1], hits1["id"], hits1["t"], SEED_BOUNCE, out=bounce),
+              lambda: core.trace(tree, bounce[0], bounce[1], tmax=bounce[2], out=hits2, schedule=sched2)]
+    graphs, kernels_per_step = capture_graphs(stages)
+
     def step(ev):
         ev[0].record(stream)
-        core.build_lbvh(v, f, out=tree)
-        ev[1].record(stream)
-        core.primary_rays(camera, W, H, out=rays)
-        ev[2].record(stream)
-        core.trace(tree, rays[0], rays[1], out=hits1, schedule=sched1)
-        ev[3].record(stream)
-        core.bounce_rays(tree.tris, rays[0], rays[1], hits1["id"], hits1["t"], SEED_BOUNCE, out=bounce)
-        ev[4].record(stream)
-        core.trace(tree, bounce[0], bounce[1], tmax=bounce[2], out=hits2, schedule=sched2)
-        ev[5].record(stream)
+        for i, g in enumerate(graphs):
+            g.replay()
+            ev[i + 1].record(stream)
 
     def new_events():
         return [torch.cuda.Event(enable_timing=True) for _ in range(6)]
@@ -231,7 +259,9 @@ def run_ours(args, rank, world, local_rank):
             evs.append(ev)
         torch.cuda.synchronize()
         t_wall = time.perf_counter() - t_wall
-    launches = _abi.lib().rt_launch_count() - launches0
+    # the kernels run inside graph replays, so the library's launch counter does not see them: count the
+    # kernels each step's graphs hold
+    launches = kernels_per_step * args.steps + (_abi.lib().rt_launch_count() - launches0)
     build_ms = sum(e[0].elapsed_time(e[1]) for e in evs)
     trace1_ms = sum(e[2].elapsed_time(e[3]) for e in evs)
     trace2_ms = sum(e[4].elapsed_time(e[5]) for e in evs)
@@ -292,6 +322,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roof_bounce,
         "roofline_primary": roof_primary,
         "gpu_launches": int(launches),
+        "graphs": f"each step = 5 CUDA graph replays (build, primary rays, trace, bounce rays, trace) holding {kernels_per_step} kernels",
         "wall_s_timed": round(t_wall, 3),
     }
     if args.build16m or args.batch:
@@ -320,7 +351,8 @@ def run_ours(args, rank, world, local_rank):
 
 
 def build_only(log2n, args, dev, world):
-    """LBVH build alone on a 2^log2n-face soup (the 16M-face build target), CUDA events, L2 flushed between builds."""
+    """LBVH build alone on a 2^log2n-face soup (the 16M-face build target), replayed from a CUDA graph, CUDA
+    events, L2 flushed between builds."""
     import torch
 
     from cudart_b200 import core, scenes
@@ -332,8 +364,9 @@ def build_only(log2n, args, dev, world):
     tree = core.build_lbvh(v, f)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream()
+    (graph,), _ = capture_graphs([lambda: core.build_lbvh(v, f, out=tree)])
     for _ in range(2):
-        core.build_lbvh(v, f, out=tree)
+        graph.replay()
     torch.cuda.synchronize()
     ms = 0.0
     reps = max(3, min(args.steps, 10))
@@ -341,7 +374,7 @@ def build_only(log2n, args, dev, world):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        core.build_lbvh(v, f, out=tree)
+        graph.replay()
         e1.record(stream)
         torch.cuda.synchronize()
         ms += e0.elapsed_time(e1)
@@ -744,8 +777,9 @@ def run_e2e(args, mesh, camera, W, H, dev, world, sched1=None, sched2=None):
     traces the primary rays and the bounces, and copies all hits back to pinned
     host memory. The copies run on two copy streams (one per direction) with
     the device mesh and hits double-buffered, so that step k+1's upload and
-    step k-1's download overlap step k's kernels; the timed region holds every
-    step's copies and kernels."""
+    step k-1's download overlap step k's kernels, which are replayed from a
+    CUDA graph per buffer set; the timed region holds every step's copies and
+    kernels."""
     import torch
 
     from cudart_b200 import core
@@ -768,26 +802,30 @@ def run_e2e(args, mesh, camera, W, H, dev, world, sched1=None, sched2=None):
     h1 = [core.trace(tree, rays[0], rays[1]) for _ in range(2)]
     b = core.bounce_rays(tree.tris, rays[0], rays[1], h1[0]["id"], h1[0]["t"], SEED_BOUNCE)
     h2 = [core.trace(tree, b[0], b[1], tmax=b[2]) for _ in range(2)]
-    ev = {k: [torch.cuda.Event(), torch.cuda.Event()] for k in ("uploaded", "built", "traced", "downloaded")}
+    ev = {k: [torch.cuda.Event(), torch.cuda.Event()] for k in ("uploaded", "traced", "downloaded")}
+
+    def compute(s):  # build, primary rays, trace, bounces, trace of buffer set s
+        core.build_lbvh(v[s], f[s], out=tree)
+        core.primary_rays(camera, W, H, out=rays)
+        core.trace(tree, rays[0], rays[1], out=h1[s], schedule=sched1)
+        core.bounce_rays(tree.tris, rays[0], rays[1], h1[s]["id"], h1[s]["t"], SEED_BOUNCE, out=b)
+        core.trace(tree, b[0], b[1], tmax=b[2], out=h2[s], schedule=sched2)
+
+    graphs, _ = capture_graphs([lambda: compute(0), lambda: compute(1)])  # one replay per step
     torch.cuda.synchronize()
 
     def step(k):
         s = k % 2
         if k >= 2:
-            up.wait_event(ev["built"][s])  # step k-2's build is done with this mesh buffer
+            up.wait_event(ev["traced"][s])  # step k-2's kernels are done with this mesh buffer
         with torch.cuda.stream(up):
             v[s].copy_(vh, non_blocking=True)
             f[s].copy_(fh, non_blocking=True)
         ev["uploaded"][s].record(up)
         comp.wait_event(ev["uploaded"][s])
-        core.build_lbvh(v[s], f[s], out=tree)
-        ev["built"][s].record(comp)
-        core.primary_rays(camera, W, H, out=rays)
         if k >= 2:
             comp.wait_event(ev["downloaded"][s])  # step k-2's hits have reached the host
-        core.trace(tree, rays[0], rays[1], out=h1[s], schedule=sched1)
-        core.bounce_rays(tree.tris, rays[0], rays[1], h1[s]["id"], h1[s]["t"], SEED_BOUNCE, out=b)
-        core.trace(tree, b[0], b[1], tmax=b[2], out=h2[s], schedule=sched2)
+        graphs[s].replay()
         ev["traced"][s].record(comp)
         down.wait_event(ev["traced"][s])
         with torch.cuda.stream(down):
@@ -821,7 +859,8 @@ def run_e2e(args, mesh, camera, W, H, dev, world, sched1=None, sched2=None):
     d2h = (out_id[0].numel() + out_t[0].numel() + out_uv[0].numel()) * 4
     return {"value": round(world * rays_per_step * args.steps / (ms * 1e-3) / 1e6, 3), "unit": "Mrays/s",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": round(ms / args.steps, 4),
-            "pipeline": "upload and download on two copy streams, double-buffered, overlapping the neighbouring steps' kernels"}
+            "pipeline": "upload and download on two copy streams, double-buffered, overlapping the neighbouring steps' kernels; "
+                        "each step's kernels replayed from a CUDA graph"}
 
 
 # ----------------------------------------------------------------------------
