@@ -597,7 +597,7 @@ __global__ __launch_bounds__(128) void k_trace_accel(TraceArgs A, AccelArgs C, S
 }
 
 template <bool kCount, bool kSeed, bool kWide>
-__global__ __launch_bounds__(128) void k_trace_coop(TraceArgs A, AccelArgs C, SlotMap M, SeedArgs S) {
+__global__ __launch_bounds__(128, kSeed ? 6 : 0) void k_trace_coop(TraceArgs A, AccelArgs C, SlotMap M, SeedArgs S) {
   __shared__ unsigned long long s_key[kCoopWarps][32];
   __shared__ float2 s_uv[kCoopWarps][32];
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -608,7 +608,8 @@ __global__ __launch_bounds__(128) void k_trace_coop(TraceArgs A, AccelArgs C, Sl
 }
 
 template <bool kCount, bool kSeed, bool kWide>
-__global__ __launch_bounds__(128) void k_trace_coop_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter, SeedArgs S) {
+__global__ __launch_bounds__(128, kSeed ? 6 : 0) void k_trace_coop_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter,
+                                                                          SeedArgs S) {
   __shared__ unsigned long long s_key[kCoopWarps][32];
   __shared__ float2 s_uv[kCoopWarps][32];
   const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
