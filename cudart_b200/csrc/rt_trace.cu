@@ -608,7 +608,7 @@ __global__ __launch_bounds__(128, kSeed ? 6 : 0) void k_trace_coop(TraceArgs A, 
 }
 
 template <bool kCount, bool kSeed, bool kWide>
-__global__ __launch_bounds__(128, kSeed ? 6 : 0) void k_trace_coop_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter,
+__global__ __launch_bounds__(128, kSeed ? 6 : (kCount ? 0 : 7)) void k_trace_coop_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter,
                                                                           SeedArgs S) {
   __shared__ unsigned long long s_key[kCoopWarps][32];
   __shared__ float2 s_uv[kCoopWarps][32];
