@@ -399,7 +399,8 @@ class ProposalGroup:
     def forward_backward(self, orig, dir, labels, box, batch: int, stream=None):
         """Gradients of each group's mean cross-entropy over its `batch` rays
         (rows g * batch ..; labels outside [0, classes) are left out); returns
-        the sum over groups of the group losses."""
+        the sum over groups of the group losses (a workspace tensor: the next
+        step overwrites it)."""
         G, B = self.groups, batch
         if B % 128 or orig.shape[0] != G * B:
             raise ValueError("need groups * batch rays with batch % 128 == 0")
