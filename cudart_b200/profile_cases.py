@@ -8,6 +8,7 @@ once more; a profiler capturing the last launch of the named kernel sees a
 steady-state launch. Cases (kernel of interest in brackets):
 
   bench_step     three steps of the main workload (build, primary, bounce)     [launch list]
+  build_16m      LBVH build of a 2^24-face soup, twice                            [k_radix_scatter, k_leaves, k_boxes_morton]
   trace_primary  2^20-face soup, 1920x1080 primary rays, tuned tile schedule   [k_trace_accel]
   trace_bounce   the same scene's diffuse bounces, cooperative schedule          [k_trace_coop]
   mlp_propose    proposal network inference on 2^18 rays (4096 slots)            [k_mlp_propose_tc]
@@ -75,6 +76,17 @@ def bench_step():
     torch.cuda.synchronize()
 
 
+def build_16m():
+    from . import core, scenes
+    mesh = scenes.soup(1 << 24, seed=7)
+    v = torch.from_numpy(mesh.vertices).cuda()
+    f = torch.from_numpy(mesh.faces.view(np.int32)).cuda()
+    del mesh
+    t = core.build_lbvh(v, f)
+    core.build_lbvh(v, f, out=t)
+    torch.cuda.synchronize()
+
+
 def mlp_propose():
     from . import proposal, scenes
     box = (-1.5, -0.6, -1.5, 1.5, 1.4, 1.5)
@@ -134,7 +146,7 @@ def mlp_grouped():
     torch.cuda.synchronize()
 
 
-CASES = {"bench_step": bench_step, "trace_primary": trace_primary, "trace_bounce": trace_bounce, "mlp_propose": mlp_propose, "mlp_train": mlp_train,
+CASES = {"bench_step": bench_step, "build_16m": build_16m, "trace_primary": trace_primary, "trace_bounce": trace_bounce, "mlp_propose": mlp_propose, "mlp_train": mlp_train,
          "sah_build": sah_build, "raster": raster, "mlp_grouped": mlp_grouped}
 
 if __name__ == "__main__":
