@@ -335,9 +335,12 @@ inline void CUDA_calcPrimaryRays(CUDABuffer* buffer, CUDACamera* camera) {
 
 // kernels/CUDA_raytraceMeshTree.cu:434. Depths are read as the initial tmax and
 // written in place; faces_id is the position in the (reordered) mesh faces.
+// coherency (the reference's choice between its packet and per-ray kernels)
+// picks the traversal schedule here: 8 x 4 pixel tiles for coherent primary
+// rays, one ray per thread otherwise; both descend while-while through the
+// 4-wide records. The closest hits do not depend on the schedule.
 inline void CUDA_raytraceMeshTree(CUDABuffer* buffer, CUDAMesh* mesh, CUDAMeshTree* tree, bool coherency = true) {
   rk_check_abi();
-  (void)coherency;  // one traversal serves both of the reference's kernels (same closest hits)
   rt_trace_desc d = {};
   d.nodes = (const uint32_t*)tree->getNodesArray()->getPointer();
   if (tree->tris) {
@@ -357,6 +360,10 @@ inline void CUDA_raytraceMeshTree(CUDABuffer* buffer, CUDAMesh* mesh, CUDAMeshTr
   d.hit_uv = (float*)buffer->out_coords.getPointer();
   d.ray_count = (uint32_t)((size_t)buffer->getWidth() * buffer->getHeight());
   d.id_mode = 0;
+  if (d.accel) {
+    d.schedule = RT_TRACE_WHILE_WHILE | RT_TRACE_WIDE;
+    if (coherency) d.image_width = buffer->getWidth();
+  }
   RK_OK(rt_trace_closest(&d, nullptr));
   RK_CHECK(cudaDeviceSynchronize() == cudaSuccess, "CUDA_raytraceMeshTree() : Unable to execute CUDA kernel.");
 }
