@@ -87,3 +87,16 @@ def test_renderkit_dropin(oracle, tmp_path, scene):
     assert np.array_equal(rid, fo)
     if scene == "terrain":
         assert (do != oracle.HUGE).mean() > 0.1
+
+
+def test_learned_proposal_from_cpp():
+    """tests/cpp/test_learned.cpp: C++ host code trains the proposal network
+    through the C ABI (features, tensor-core GEMMs, fused cross-entropy, Adam),
+    proposes a slot per ray with rt_mlp_propose and traces with
+    rt_trace_closest_seeded; the hits equal rt_trace_closest's bit for bit."""
+    import __graft_entry__
+    __graft_entry__.build_cpp_tests()
+    exe = os.path.join(ROOT, "tests", "cpp", "_build", "test_learned")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "differing hits 0" in r.stdout, r.stdout
