@@ -579,7 +579,8 @@ def batch_trace(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax=None
                 while_while: bool = True, out: dict | None = None, schedule: dict | None = None, stream=None) -> dict:
     """Closest hits for the rays of all meshes (rays of mesh m: ray_offsets[m] .. ray_offsets[m+1]).
     schedule (results never depend on it): while_while, wide (4-wide records),
-    persistent + blocks_per_sm (warps fetching 32 rays at a time)."""
+    persistent + blocks_per_sm (warps fetching 32 rays at a time), coop
+    (warp-cooperative leaf tests; always persistent)."""
     d, out = batch_trace_desc(tree, orig, dir, ray_offsets, tmax, id_mode, counters, while_while, out, schedule)
     _abi.check("rt_batch_trace", _abi.lib().rt_batch_trace(C.byref(d), _stream(stream)))
     return out
@@ -606,8 +607,9 @@ def batch_trace_desc(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax
         d.ray_visits, d.ray_tests = out["visits"].data_ptr(), out["tests"].data_ptr()
     sch = dict(while_while=while_while) if schedule is None else schedule
     d.schedule = ((_abi.TRACE_WHILE_WHILE if sch.get("while_while", False) else 0)
-                  | (_abi.TRACE_WIDE if sch.get("wide", False) else 0))
-    if sch.get("persistent", False):
+                  | (_abi.TRACE_WIDE if sch.get("wide", False) else 0)
+                  | (_abi.TRACE_COOP if sch.get("coop", False) else 0))
+    if sch.get("persistent", False) or sch.get("coop", False):
         if "_counter" not in out:
             out["_counter"] = torch.zeros(1, dtype=torch.int32, device=dev)
         d.work_counter = out["_counter"].data_ptr()

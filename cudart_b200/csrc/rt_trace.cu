@@ -128,7 +128,7 @@ struct AccelArgs {
   const uint4* leaves;
   const float4* groups;
   const uint32_t* hdr;
-  const float4* wide;  // 4-wide records (single-mesh blobs)
+  const float4* wide;  // 4-wide records
 };
 
 // One ray through the blob. kWW: "while-while" schedule (descend internal
@@ -496,6 +496,8 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
       const uint32_t oexcl = __shfl_sync(0xffffffffu, excl, owner);
       const uint32_t ofirst = __shfl_sync(0xffffffffu, first, owner);
       const uint32_t ocnt = __shfl_sync(0xffffffffu, cnt, owner);
+      // the owner's triangle stream (lanes of a batched launch may trace different meshes)
+      const float4* otris = (const float4*)__shfl_sync(0xffffffffu, (unsigned long long)A.tris, owner);
       if (item < total) {
         const uint32_t g = __fns(omask, 0, (int)(item - oexcl) + 1);
         const uint32_t kend = min(ocnt, g * 8 + 8);
@@ -504,9 +506,9 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
         float mu = 0.f, mv = 0.f;
         for (uint32_t k = g * 8; k < kend; ++k) {
           const uint32_t pos = ofirst + k;
-          const float4 v0 = ldg4(A.tris + 3 * (size_t)pos);
-          const float4 e1 = ldg4(A.tris + 3 * (size_t)pos + 1);
-          const float4 e2 = ldg4(A.tris + 3 * (size_t)pos + 2);
+          const float4 v0 = ldg4(otris + 3 * (size_t)pos);
+          const float4 e1 = ldg4(otris + 3 * (size_t)pos + 1);
+          const float4 e2 = ldg4(otris + 3 * (size_t)pos + 2);
           float t, u, v;
           if (!mt_test(oo, od, ozu, ozv, v0, e1, e2, t, u, v)) continue;
           const unsigned long long key = ((unsigned long long)__float_as_uint(t) << 32) | pos;
@@ -679,6 +681,56 @@ template <bool kCount, bool kWW, bool kSeed, bool kWide>
 __global__ __launch_bounds__(128) void k_batch_trace(TraceArgs A, BatchTraceArgs B, SeedArgs S) {
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r < A.ray_count) batch_trace_ray<kCount, kWW, kSeed, kWide>(r, A, B, S);
+}
+
+// The per-ray arguments of batched ray r: its mesh's part of the blob, triangle
+// stream and indices, and (seeded) slot tables.
+template <bool kSeed>
+__device__ __forceinline__ void batch_ray_args(uint32_t r, const TraceArgs& A, const BatchTraceArgs& B, const SeedArgs& S, TraceArgs& Am,
+                                               AccelArgs& C, SeedArgs& Sm) {
+  const uint32_t m = find_seg(B.roff, B.M, r);
+  const uint32_t F = __ldg(B.foff + m);
+  C.hdr = B.acc.hdr + 64 * (size_t)m;
+  C.tnodes = B.acc.tnodes + 4 * (size_t)F;
+  C.leaves = B.acc.leaves + F;
+  C.groups = B.acc.groups + 2 * (size_t)group_base(F, m);
+  C.wide = B.acc.wide + 8 * (size_t)F;
+  Am = A;
+  Am.tris = A.tris + 3 * (size_t)F;
+  Am.indices = A.indices + F;
+  Sm = S;
+  if (kSeed) {
+    Sm.slot_ref = S.slot_ref + (size_t)m * S.slot_count;
+    if (S.slot_box) Sm.slot_box = S.slot_box + 2 * (size_t)m * S.slot_count;
+  }
+}
+
+// Warp-cooperative leaf tests over batched rays (persistent warps, 32 rays at a
+// time): each lane walks its own mesh; a lane testing another lane's leaf reads
+// that lane's triangle stream.
+template <bool kCount, bool kSeed, bool kWide>
+__global__ __launch_bounds__(128, kSeed ? 6 : (kCount ? 0 : 7)) void k_batch_trace_coop(TraceArgs A, BatchTraceArgs B, SeedArgs S,
+                                                                                      uint32_t* counter) {
+  __shared__ unsigned long long s_key[kCoopWarps][32];
+  __shared__ float2 s_uv[kCoopWarps][32];
+  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= A.ray_count) break;
+    const uint32_t r = base + lane;
+    const bool valid = r < A.ray_count;
+    TraceArgs Am = A;
+    AccelArgs C = {};
+    SeedArgs Sm = S;
+    if (valid) {
+      batch_ray_args<kSeed>(r, A, B, S, Am, C, Sm);
+    } else {  // idle lanes read mesh 0's header only
+      C.hdr = B.acc.hdr; C.tnodes = B.acc.tnodes; C.leaves = B.acc.leaves; C.groups = B.acc.groups; C.wide = B.acc.wide;
+    }
+    trace_warp_coop<kCount, kSeed, kWide>(r, valid, Am, C, s_key[w], s_uv[w], Sm);
+  }
 }
 
 // Persistent warps over the batched rays: 32 rays at a time from a global counter.
@@ -990,7 +1042,13 @@ namespace {
 template <bool kSeed, bool kWide>
 rt_status batch_launch_w(const rt_batch_trace_desc* d, const TraceArgs& A, const BatchTraceArgs& B, const SeedArgs& S, cudaStream_t st,
                          bool count, bool ww) {
-  if (d->work_counter) {
+  if (d->work_counter && (d->schedule & RT_TRACE_COOP)) {
+    if (cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
+    const uint32_t per_sm = d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u;
+    const uint32_t blocks = (uint32_t)hmin<uint64_t>((uint64_t)sms() * per_sm, (d->ray_count + 127) / 128);
+    if (count) k_batch_trace_coop<true, kSeed, kWide><<<blocks, 128, 0, st>>>(A, B, S, d->work_counter);
+    else k_batch_trace_coop<false, kSeed, kWide><<<blocks, 128, 0, st>>>(A, B, S, d->work_counter);
+  } else if (d->work_counter) {
     if (cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
     const uint32_t per_sm = d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u;
     const uint32_t blocks = (uint32_t)hmin<uint64_t>((uint64_t)sms() * per_sm, (d->ray_count + 127) / 128);

@@ -94,6 +94,9 @@ def batch_candidates():
         out.append({"while_while": ww, "wide": wide, "persistent": False, "blocks_per_sm": 0})
         for bps in (8, 16):
             out.append({"while_while": ww, "wide": wide, "persistent": True, "blocks_per_sm": bps})
+    # warp-cooperative leaf tests (persistent, while-while)
+    for wide, bps in itertools.product((False, True), (8, 16)):
+        out.append({"while_while": True, "wide": wide, "persistent": True, "blocks_per_sm": bps, "coop": True})
     return out
 
 

@@ -171,7 +171,7 @@ typedef struct rt_batch_trace_desc {
   uint32_t* ray_visits;
   uint32_t* ray_tests;
   uint32_t* error_word;
-  uint32_t schedule;              /* RT_TRACE_WHILE_WHILE, RT_TRACE_WIDE */
+  uint32_t schedule;              /* RT_TRACE_WHILE_WHILE, RT_TRACE_WIDE, RT_TRACE_COOP (with work_counter) */
   uint32_t* work_counter;         /* optional device word: persistent warps fetch rays through it (the call zeroes it) */
   uint32_t persistent_blocks_per_sm; /* with work_counter: CTAs of 128 threads per SM (0 = 8) */
 } rt_batch_trace_desc;

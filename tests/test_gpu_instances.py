@@ -232,8 +232,9 @@ def test_batch_seeded_trace_is_bit_exact():
     R = o.shape[0]
     rnd = torch.randint(-2, 4200, (R,), dtype=torch.int32, device="cuda", generator=g)  # includes none and out of range
     sch_wide = dict(while_while=True, wide=True, persistent=True, blocks_per_sm=4)
+    sch_coop = dict(while_while=True, wide=True, persistent=True, blocks_per_sm=4, coop=True)
     for prop in (labels, rnd):
-        for box_test, sch in ((True, None), (False, None), (True, sch_wide)):
+        for box_test, sch in ((True, None), (False, None), (True, sch_wide), (True, sch_coop)):
             s = proposal.batch_trace_seeded(bt, o, d, roff, prop, slots, counters=True, in_proposal=True, box_test=box_test,
                                             schedule=sch)
             torch.cuda.synchronize()
