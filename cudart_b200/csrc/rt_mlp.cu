@@ -361,13 +361,16 @@ __global__ void __launch_bounds__(kArgThreads, 1)
 }
 
 // ----------------------------------------------------------------------------
-// Logits + softmax cross-entropy gradient: grid (m / 128, groups), 320 threads,
-// the layout of k_gemm_argmax_tc. The logits of a 128-row block are computed
-// twice, never stored: pass 1 keeps each row's running max and sum of
-// exponentials (per half of the columns, merged through shared memory); pass
-// 2 writes g = (softmax - onehot(label)) * scale in BF16, row-major and
-// transposed, and adds the row's loss scale * (log sum - logit[label]).
-// Rows whose label is outside [0, n) get g = 0 and no loss.
+// Logits + softmax cross-entropy gradient: grid (m / 128, groups), 576 threads:
+// warps 0-15 drain TMEM (warp w: lane quarter w % 4, column quarter w / 4 of
+// each 256-wide logit tile), warp 16 loads, warp 17 issues the MMAs. The
+// logits of a 128-row block are computed twice, never stored: pass 1 keeps
+// each row's running max and sum of exponentials (per column quarter, merged
+// in a fixed order through shared memory); pass 2 writes g = (softmax -
+// onehot(label)) * scale in BF16, row-major and transposed, and adds the row's
+// loss scale * (log sum - logit[label]). Rows whose label is outside [0, n)
+// get g = 0 and no loss.
+constexpr uint32_t kXentThreads = 576;
 // ----------------------------------------------------------------------------
 struct XentArgs {
   const float* bias;
@@ -383,18 +386,18 @@ struct XentArgs {
 };
 
 size_t xent_smem(uint32_t num_k, uint32_t n) {
-  return 1024 + num_k * (size_t)kTileA + kStages * (size_t)kArgTileB + (size_t)n * 4 + kBM * 16 + 16 * 8 + 64;
+  return 1024 + num_k * (size_t)kTileA + kStages * (size_t)kArgTileB + (size_t)n * 4 + 3 * kBM * 16 + 16 * 8 + 64;
 }
 
-__global__ void __launch_bounds__(kArgThreads, 1)
+__global__ void __launch_bounds__(kXentThreads, 1)
     k_gemm_xent_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, XentArgs X, uint32_t num_k) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* sA = smem;
   uint8_t* sB = smem + num_k * kTileA;
   float* s_bias = (float*)(sB + kStages * kArgTileB);
-  float4* s_x = (float4*)(s_bias + X.n);  // per row: (max, sum, logit[label], -) of a column half
-  uint64_t* full = (uint64_t*)(s_x + kBM);
+  float4* s_x = (float4*)(s_bias + X.n);  // [3][128]: (max, sum, logit[label], -) of column quarters 1..3
+  uint64_t* full = (uint64_t*)(s_x + 3 * kBM);
   uint64_t* empty = full + kStages;
   uint64_t* a_full = empty + kStages;
   uint64_t* acc_full = a_full + 1;     // [2]
@@ -405,7 +408,7 @@ __global__ void __launch_bounds__(kArgThreads, 1)
   uint32_t* tmem_slot = (uint32_t*)(mdone + 1);
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t grp = blockIdx.y, n = X.n;
-  for (uint32_t j = threadIdx.x; j < n; j += kArgThreads) s_bias[j] = X.bias ? X.bias[(size_t)grp * n + j] : 0.0f;
+  for (uint32_t j = threadIdx.x; j < n; j += kXentThreads) s_bias[j] = X.bias ? X.bias[(size_t)grp * n + j] : 0.0f;
   if (threadIdx.x == 0) {
     for (uint32_t s = 0; s < kStages; ++s) {
       mbar_init(full + s, 1);
@@ -414,9 +417,9 @@ __global__ void __launch_bounds__(kArgThreads, 1)
     mbar_init(a_full, 1);
     for (int b = 0; b < 2; ++b) {
       mbar_init(acc_full + b, 1);
-      mbar_init(acc_empty + b, 256);
+      mbar_init(acc_empty + b, 512);
     }
-    mbar_init(xch_a, 128);
+    mbar_init(xch_a, 3 * 128);
     mbar_init(xch_b, 128);
     mbar_init(mdone, 1);
     fence_mbar_init();
@@ -435,7 +438,7 @@ __global__ void __launch_bounds__(kArgThreads, 1)
   const int32_t m0 = (int32_t)(grp * X.gm + blockIdx.x * kBM);
   const uint32_t ntiles = n / kArgBN, total_tiles = 2 * ntiles;
 
-  if (warp == 8) {
+  if (warp == 16) {
     if (lane == 0) {
       mbar_arrive_expect_tx(a_full, num_k * kTileA);
       for (uint32_t kc = 0; kc < num_k; ++kc) tma_load_2d(sA + kc * kTileA, &ta, (int32_t)(kc * kBK), m0, a_full);
@@ -452,7 +455,7 @@ __global__ void __launch_bounds__(kArgThreads, 1)
       mbar_wait(a_full, 0, X.err);
       for (uint32_t j = q > kStages ? q - kStages : 0u; j < q; ++j) mbar_wait(full + j % kStages, (j / kStages) & 1u, X.err);
     }
-  } else if (warp == 9) {
+  } else if (warp == 17) {
     if (lane == 0) {
       const uint32_t idesc = idesc_bf16_f32(kBM, kArgBN);
       bool mok = mbar_wait(a_full, 0, X.err);
@@ -478,30 +481,34 @@ __global__ void __launch_bounds__(kArgThreads, 1)
       mbar_wait(mdone, 0, X.err);
     }
   } else {
-    const uint32_t qw = warp & 3u, half = warp >> 2;
+    const uint32_t qw = warp & 3u, cq = warp >> 2;
     const uint32_t trow = qw * 32u + lane, row = (uint32_t)m0 + trow, rowl = blockIdx.x * kBM + trow;
     const int32_t lab = X.labels[row];
     const bool valid = lab >= 0 && lab < (int32_t)n;
-    const uint32_t c0 = half * (kArgBN / 2);
+    const uint32_t c0 = cq * (kArgBN / 4);
     float mx = -INFINITY, sum = 0.0f, xl = 0.0f, inv = 0.0f;
     bool ok = true;
     for (uint32_t t2 = 0; t2 < total_tiles; ++t2) {
       const uint32_t buf = t2 & 1u, pass = t2 / ntiles, t = t2 - pass * ntiles;
       if (t2 == ntiles && ok) {
-        // merge the two column halves of each row: half 1 -> shared -> half 0 -> shared -> half 1
-        if (half == 1) {
-          s_x[trow] = make_float4(mx, sum, xl, 0.0f);
+        // merge the four column quarters of each row (quarter 0 merges 1, 2, 3 in that order) and share the result
+        if (cq > 0) {
+          s_x[(cq - 1u) * kBM + trow] = make_float4(mx, sum, xl, 0.0f);
           mbar_arrive(xch_a);
           ok = __all_sync(0xffffffffu, mbar_wait(xch_b, 0, X.err));
           const float4 w = s_x[trow];
           mx = w.x; sum = w.y;
         } else {
           ok = __all_sync(0xffffffffu, mbar_wait(xch_a, 0, X.err));
-          const float4 w = s_x[trow];
-          const float m2 = fmaxf(mx, w.x);
-          sum = sum * __expf(mx - m2) + w.y * __expf(w.x - m2);
-          mx = m2;
-          xl += w.z;  // exactly one half saw the label's column; the other holds 0
+#pragma unroll
+          for (uint32_t j = 0; j < 3; ++j) {
+            const float4 w = s_x[j * kBM + trow];
+            const float m2 = fmaxf(mx, w.x);
+            sum = sum * __expf(mx - m2) + w.y * __expf(w.x - m2);
+            mx = m2;
+            xl += w.z;  // exactly one quarter saw the label's column; the others hold 0
+          }
+          // every partial has been read above: slot 0 now carries the merged row
           s_x[trow] = make_float4(mx, sum, 0.0f, 0.0f);
           mbar_arrive(xch_b);
           if (valid && X.loss_sum) atomicAdd(X.loss_sum, (logf(sum) + mx - xl) * X.scale);
@@ -512,7 +519,7 @@ __global__ void __launch_bounds__(kArgThreads, 1)
       tc_fence_after();
       if (ok) {
         const uint32_t tl = tmem + ((qw * 32u) << 16) + buf * kArgBN + c0;
-        for (uint32_t c = 0; c < kArgBN / 2; c += 16) {
+        for (uint32_t c = 0; c < kArgBN / 4; c += 16) {
           float v[16];
           tmem_ld16(tl + c, v);
           const uint32_t col = t * kArgBN + c0 + c;
@@ -1299,7 +1306,7 @@ extern "C" rt_status rt_gemm_xent_bf16(const rt_gemm_xent_desc* d, rt_stream str
   std::call_once(once, [] {
     cudaFuncSetAttribute(k_gemm_xent_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xent_smem(4, kArgMaxN));
   });
-  k_gemm_xent_tc<<<dim3(d->m / kBM, G), kArgThreads, xent_smem(num_k, d->n), (cudaStream_t)stream>>>(ta, tb, X, num_k);
+  k_gemm_xent_tc<<<dim3(d->m / kBM, G), kXentThreads, xent_smem(num_k, d->n), (cudaStream_t)stream>>>(ta, tb, X, num_k);
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
