@@ -52,7 +52,15 @@ struct GemmEpi {
   __nv_bfloat16* ct16;
   uint32_t ldct;
   uint32_t gm, gn;  // rows and columns of one group's product
+  uint32_t c32_v8, c16_v8;  // the output's 16-column pieces are 32-byte aligned: 256-bit stores
 };
+
+// One 32-byte store (256-bit, sm_100); p must be 32-byte aligned.
+__device__ __forceinline__ void st_global_v8(void* p, const uint32_t (&w)[8]) {
+  asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]),
+               "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7])
+               : "memory");
+}
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -82,14 +90,30 @@ __device__ __forceinline__ void epilogue16(const GemmEpi& E, uint32_t g, uint32_
     }
   }
   if (E.c32) {
-    float4* p = (float4*)(E.c32 + (size_t)row * E.ldc32 + col);
+    float* p = E.c32 + (size_t)row * E.ldc32 + col;
+    if (E.c32_v8) {
+      uint32_t a[8], b[8];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) p[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+      for (int i = 0; i < 8; ++i) { a[i] = __float_as_uint(v[i]); b[i] = __float_as_uint(v[8 + i]); }
+      st_global_v8(p, a);
+      st_global_v8(p + 8, b);
+    } else {
+      float4* q = (float4*)p;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) q[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+    }
   }
   if (E.c16) {
-    uint4* p = (uint4*)(E.c16 + (size_t)row * E.ldc16 + col);
-    p[0] = make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
-    p[1] = make_uint4(pack_bf16(v[8], v[9]), pack_bf16(v[10], v[11]), pack_bf16(v[12], v[13]), pack_bf16(v[14], v[15]));
+    const uint32_t w[8] = {pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]),
+                           pack_bf16(v[8], v[9]), pack_bf16(v[10], v[11]), pack_bf16(v[12], v[13]), pack_bf16(v[14], v[15])};
+    __nv_bfloat16* p = E.c16 + (size_t)row * E.ldc16 + col;
+    if (E.c16_v8) {
+      st_global_v8(p, w);
+    } else {
+      uint4* q = (uint4*)p;
+      q[0] = make_uint4(w[0], w[1], w[2], w[3]);
+      q[1] = make_uint4(w[4], w[5], w[6], w[7]);
+    }
   }
   if (E.ct16) {
     __nv_bfloat16* ct = E.ct16 + (size_t)g * E.gn * E.ldct + (row - g * E.gm);
@@ -383,6 +407,7 @@ struct XentArgs {
   uint32_t ldgt;
   float* loss_sum;
   uint32_t* err;
+  uint32_t g32;  // g and ldg keep every 16-column piece of a row 32-byte aligned: one 256-bit store per piece
 };
 
 size_t xent_smem(uint32_t num_k, uint32_t n) {
@@ -547,9 +572,14 @@ __global__ void __launch_bounds__(kXentThreads, 1)
               if ((int32_t)(col + 2 * i + 1) == lab) p1 -= 1.0f;
               w[i] = valid ? pack_bf16(p0 * X.scale, p1 * X.scale) : 0u;
             }
-            uint4* gp = (uint4*)(X.g + (size_t)row * X.ldg + col);
-            gp[0] = make_uint4(w[0], w[1], w[2], w[3]);
-            gp[1] = make_uint4(w[4], w[5], w[6], w[7]);
+            __nv_bfloat16* gr = X.g + (size_t)row * X.ldg + col;
+            if (X.g32) {
+              st_global_v8(gr, w);
+            } else {
+              uint4* gp = (uint4*)gr;
+              gp[0] = make_uint4(w[0], w[1], w[2], w[3]);
+              gp[1] = make_uint4(w[4], w[5], w[6], w[7]);
+            }
             __nv_bfloat16* gt = X.gt + ((size_t)grp * n + col) * X.ldgt + rowl;
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
@@ -1252,6 +1282,8 @@ extern "C" rt_status rt_gemm_bf16(const rt_gemm_desc* d, rt_stream stream) {
   E.c32 = d->c_f32; E.ldc32 = d->ldc_f32; E.c16 = (__nv_bfloat16*)d->c_bf16; E.ldc16 = d->ldc_bf16;
   E.ct16 = (__nv_bfloat16*)d->ct_bf16; E.ldct = d->ldct;
   E.gm = d->m; E.gn = d->n;
+  E.c32_v8 = (d->c_f32 && d->ldc_f32 % 8 == 0 && ((uintptr_t)d->c_f32 & 31u) == 0) ? 1u : 0u;
+  E.c16_v8 = (d->c_bf16 && d->ldc_bf16 % 16 == 0 && ((uintptr_t)d->c_bf16 & 31u) == 0) ? 1u : 0u;
   const size_t smem = gemm_smem(bn);
   static std::once_flag once;
   std::call_once(once, [] { cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem(256)); });
@@ -1301,6 +1333,7 @@ extern "C" rt_status rt_gemm_xent_bf16(const rt_gemm_xent_desc* d, rt_stream str
   X.bias = d->bias; X.labels = d->labels; X.n = d->n; X.gm = d->m; X.scale = d->scale;
   X.g = (__nv_bfloat16*)d->g; X.ldg = d->ldg; X.gt = (__nv_bfloat16*)d->gt; X.ldgt = d->ldgt; X.loss_sum = d->loss_sum;
   X.err = d->error_word;
+  X.g32 = (d->ldg % 16 == 0 && ((uintptr_t)d->g & 31u) == 0) ? 1u : 0u;
   const uint32_t num_k = d->k / kBK;
   static std::once_flag once;
   std::call_once(once, [] {
