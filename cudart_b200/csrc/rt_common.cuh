@@ -29,6 +29,12 @@ __device__ __forceinline__ float4 f4max(float4 a, float4 b) {
 // while the reading kernel runs.
 __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
 __device__ __forceinline__ uint4 ldg4(const uint4* p) { return __ldg(p); }
+// Two consecutive float4 in one 32-byte read-only load (256-bit, sm_100); p must be 32-byte aligned.
+__device__ __forceinline__ void ldg8(const float4* p, float4& a, float4& b) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 

@@ -272,8 +272,12 @@ __device__ __forceinline__ void cswap_tr(float (&t)[4], uint32_t (&r)[4], int a,
 }
 __device__ __forceinline__ void wide_test(const float4* __restrict__ wn, const float4& o, float ix, float iy, float iz, float tbest,
                                           uint32_t skip, float (&t)[4], uint32_t (&r)[4]) {
-  const float4 w0 = ldg4(wn), w1 = ldg4(wn + 1), w2 = ldg4(wn + 2), w3 = ldg4(wn + 3), w4 = ldg4(wn + 4), w5 = ldg4(wn + 5);
-  const uint4 wr = ldg4((const uint4*)(wn + 6));
+  float4 w0, w1, w2, w3, w4, w5, wrf, spare;  // the 128-byte record in four 32-byte loads
+  ldg8(wn, w0, w1);
+  ldg8(wn + 2, w2, w3);
+  ldg8(wn + 4, w4, w5);
+  ldg8(wn + 6, wrf, spare);
+  const uint4 wr = make_uint4(__float_as_uint(wrf.x), __float_as_uint(wrf.y), __float_as_uint(wrf.z), __float_as_uint(wrf.w));
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const uint32_t rk = u4c(wr, k);

@@ -243,7 +243,9 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
           }
         } else {
         const float4* tn = C.tnodes + 4 * (size_t)ref;
-        const float4 a0 = ldg4(tn), a1 = ldg4(tn + 1), b0 = ldg4(tn + 2), b1 = ldg4(tn + 3);
+        float4 a0, a1, b0, b1;
+        ldg8(tn, a0, a1);
+        ldg8(tn + 2, b0, b1);
         if (kCount) visits += 2;
         float ta, tb;
         bool ha = slab2(a0, a1, o, ix, iy, iz, bt, ta);
@@ -280,8 +282,8 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
       if (kCount) ++visits;
       const uint32_t first = L.x, cnt = L.y, gbase = L.z;
       for (uint32_t g = 0; g * 8 < cnt; ++g) {
-        const float4 gmn = ldg4(C.groups + 2 * ((size_t)gbase + g));
-        const float4 gmx = ldg4(C.groups + 2 * ((size_t)gbase + g) + 1);
+        float4 gmn, gmx;
+        ldg8(C.groups + 2 * ((size_t)gbase + g), gmn, gmx);
         if (kCount) ++visits;
         float tg;
         if (!slab2(gmn, gmx, o, ix, iy, iz, bt, tg)) continue;
@@ -400,7 +402,9 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
           }
         } else {
         const float4* tn = C.tnodes + 4 * (size_t)ref;
-        const float4 a0 = ldg4(tn), a1 = ldg4(tn + 1), b0 = ldg4(tn + 2), b1 = ldg4(tn + 3);
+        float4 a0, a1, b0, b1;
+        ldg8(tn, a0, a1);
+        ldg8(tn + 2, b0, b1);
         if (kCount) visits += 2;
         float ta, tb;
         bool ha = slab2(a0, a1, o, ix, iy, iz, bt, ta);
@@ -441,8 +445,8 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
       const uint32_t gbase = L.z;
       const uint32_t ng = (cnt + 7) >> 3;
       for (uint32_t g = 0; g < ng; ++g) {
-        const float4 gmn = ldg4(C.groups + 2 * ((size_t)gbase + g));
-        const float4 gmx = ldg4(C.groups + 2 * ((size_t)gbase + g) + 1);
+        float4 gmn, gmx;
+        ldg8(C.groups + 2 * ((size_t)gbase + g), gmn, gmx);
         if (kCount) ++visits;
         float tg;
         if (slab2(gmn, gmx, o, ix, iy, iz, bt, tg)) {
@@ -536,8 +540,8 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
       // groups beyond the first 32 (leaves of more than 256 triangles): this lane alone
       for (uint32_t g = 32; g * 8 < cnt; ++g) {
         const uint32_t gbase = __ldg(C.leaves + (~ref)).z;
-        const float4 gmn = ldg4(C.groups + 2 * ((size_t)gbase + g));
-        const float4 gmx = ldg4(C.groups + 2 * ((size_t)gbase + g) + 1);
+        float4 gmn, gmx;
+        ldg8(C.groups + 2 * ((size_t)gbase + g), gmn, gmx);
         float tg;
         if (!slab2(gmn, gmx, o, ix, iy, iz, bt, tg)) continue;
         const uint32_t kend = min(cnt, g * 8 + 8);
