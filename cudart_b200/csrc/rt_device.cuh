@@ -249,14 +249,34 @@ __device__ __forceinline__ bool box_test(float bx0, float by0, float bz0, float 
   return tn <= tf && tf >= 0.0f && tn <= tbest * kCullSlack;
 }
 
-__device__ __forceinline__ bool slab2(const float4& mn, const float4& mx, const float4& o, float ix, float iy, float iz, float tbest,
+// Three-input min / max (one instruction each on sm_100).
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
+// Slab test of a padded box. `oi` is the ray origin scaled by the inverse
+// direction (o.x * ix, o.y * iy, o.z * iz): each plane distance is one fused
+// multiply-add, box * inv - origin * inv, whose error (the rounding of o * inv
+// and of the result) is of the same order as that of (box - origin) * inv and
+// is absorbed the same way by the 2^-13 padding and the cull slack.
+__device__ __forceinline__ bool slab2(const float4& mn, const float4& mx, const float4& oi, float ix, float iy, float iz, float tbest,
                                       float& tn) {
-  const float t0x = (mn.x - o.x) * ix, t1x = (mx.x - o.x) * ix;
-  const float t0y = (mn.y - o.y) * iy, t1y = (mx.y - o.y) * iy;
-  const float t0z = (mn.z - o.z) * iz, t1z = (mx.z - o.z) * iz;
-  tn = fmax_sel(fmax_sel(fmin_sel(t0x, t1x), fmin_sel(t0y, t1y)), fmin_sel(t0z, t1z));
-  const float tf = fmin_sel(fmin_sel(fmax_sel(t0x, t1x), fmax_sel(t0y, t1y)), fmax_sel(t0z, t1z));
+  const float t0x = __fmaf_rn(mn.x, ix, -oi.x), t1x = __fmaf_rn(mx.x, ix, -oi.x);
+  const float t0y = __fmaf_rn(mn.y, iy, -oi.y), t1y = __fmaf_rn(mx.y, iy, -oi.y);
+  const float t0z = __fmaf_rn(mn.z, iz, -oi.z), t1z = __fmaf_rn(mx.z, iz, -oi.z);
+  tn = max3f(fminf(t0x, t1x), fminf(t0y, t1y), fminf(t0z, t1z));
+  const float tf = min3f(fmaxf(t0x, t1x), fmaxf(t0y, t1y), fmaxf(t0z, t1z));
   return tn <= tf && tf >= 0.0f && tn <= tbest * kCullSlack;
+}
+__device__ __forceinline__ float4 scaled_origin(const float4& o, float ix, float iy, float iz) {
+  return make_float4(o.x * ix, o.y * iy, o.z * iz, 0.0f);
 }
 
 // One 4-wide record against a ray: entry distance of every child the ray
@@ -270,7 +290,7 @@ __device__ __forceinline__ void cswap_tr(float (&t)[4], uint32_t (&r)[4], int a,
     const uint32_t rr = r[a]; r[a] = r[b]; r[b] = rr;
   }
 }
-__device__ __forceinline__ void wide_test(const float4* __restrict__ wn, const float4& o, float ix, float iy, float iz, float tbest,
+__device__ __forceinline__ void wide_test(const float4* __restrict__ wn, const float4& oi, float ix, float iy, float iz, float tbest,
                                           uint32_t skip, float (&t)[4], uint32_t (&r)[4]) {
   float4 w0, w1, w2, w3, w4, w5, wrf, spare;  // the 128-byte record in four 32-byte loads
   ldg8(wn, w0, w1);
@@ -283,7 +303,7 @@ __device__ __forceinline__ void wide_test(const float4* __restrict__ wn, const f
     const uint32_t rk = u4c(wr, k);
     float tn;
     const bool h = rk != kNoChild && rk != skip &&
-                   slab2(make_float4(f4c(w0, k), f4c(w1, k), f4c(w2, k), 0.0f), make_float4(f4c(w3, k), f4c(w4, k), f4c(w5, k), 0.0f), o,
+                   slab2(make_float4(f4c(w0, k), f4c(w1, k), f4c(w2, k), 0.0f), make_float4(f4c(w3, k), f4c(w4, k), f4c(w5, k), 0.0f), oi,
                          ix, iy, iz, tbest, tn);
     t[k] = h ? tn : INFINITY;
     r[k] = rk;

@@ -161,7 +161,7 @@ __device__ __forceinline__ bool seed_ref_ok(uint32_t q, const AccelArgs& C) {
 // subtree can be hit, so phase 0 is skipped and the subtree is still cut out.
 // Returns false when nothing is left to walk.
 template <bool kCount>
-__device__ __forceinline__ bool seed_start(uint32_t r, const SeedArgs& S, const AccelArgs& C, const float4& o, float ix, float iy,
+__device__ __forceinline__ bool seed_start(uint32_t r, const SeedArgs& S, const AccelArgs& C, const float4& oi, float ix, float iy,
                                            float iz, float bt, uint32_t root, uint32_t& ref, uint32_t& skip, uint32_t& phase,
                                            uint32_t& visits) {
   const int32_t p = __ldg(S.proposal + r);
@@ -172,7 +172,7 @@ __device__ __forceinline__ bool seed_start(uint32_t r, const SeedArgs& S, const 
   if (S.slot_box) {
     if (kCount) ++visits;
     float tb;
-    if (!slab2(ldg4(S.slot_box + 2 * p), ldg4(S.slot_box + 2 * p + 1), o, ix, iy, iz, bt, tb)) return root != skip;
+    if (!slab2(ldg4(S.slot_box + 2 * p), ldg4(S.slot_box + 2 * p + 1), oi, ix, iy, iz, bt, tb)) return root != skip;
   }
   ref = q;
   phase = 0;
@@ -190,6 +190,7 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
   uint32_t phase = 1, best_phase = 1;
   if (tmax0 > 0.0f) {
     const float ix = 1.0f / fix_dir(d.x), iy = 1.0f / fix_dir(d.y), iz = 1.0f / fix_dir(d.z);
+    const float4 oi = scaled_origin(o, ix, iy, iz);
     const float zu = o.w * 0.0f, zv = d.w * 0.0f;
     uint32_t st_ref[kStack];
     float st_t[kStack];
@@ -197,7 +198,7 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
     const uint32_t root = __ldg(C.hdr);
     uint32_t ref = root, skip = kNoSkip;
     bool alive = true;
-    if (kSeed) alive = seed_start<kCount>(r, S, C, o, ix, iy, iz, bt, root, ref, skip, phase, visits);
+    if (kSeed) alive = seed_start<kCount>(r, S, C, oi, ix, iy, iz, bt, root, ref, skip, phase, visits);
     // next reference to walk: the nearest stacked subtree still within reach,
     // else (phase 0) the root of phase 1; false when the walk is over
     auto next = [&]() -> bool {
@@ -219,7 +220,7 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
           // 4-wide record: up to four children tested at once, nearest first
           float wt[4];
           uint32_t wr[4];
-          wide_test(C.wide + 8 * (size_t)ref, o, ix, iy, iz, bt, (kSeed && phase) ? skip : kNoSkip, wt, wr);
+          wide_test(C.wide + 8 * (size_t)ref, oi, ix, iy, iz, bt, (kSeed && phase) ? skip : kNoSkip, wt, wr);
           if (kCount) visits += 4;
           if (wt[0] == INFINITY) {
             if (!next()) {
@@ -248,8 +249,8 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
         ldg8(tn + 2, b0, b1);
         if (kCount) visits += 2;
         float ta, tb;
-        bool ha = slab2(a0, a1, o, ix, iy, iz, bt, ta);
-        bool hb = slab2(b0, b1, o, ix, iy, iz, bt, tb);
+        bool ha = slab2(a0, a1, oi, ix, iy, iz, bt, ta);
+        bool hb = slab2(b0, b1, oi, ix, iy, iz, bt, tb);
         const uint32_t ra = __float_as_uint(a0.w), rb = __float_as_uint(b0.w);
         if (kSeed && phase) {
           if (ra == skip) ha = false;
@@ -286,7 +287,7 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
         ldg8(C.groups + 2 * ((size_t)gbase + g), gmn, gmx);
         if (kCount) ++visits;
         float tg;
-        if (!slab2(gmn, gmx, o, ix, iy, iz, bt, tg)) continue;
+        if (!slab2(gmn, gmx, oi, ix, iy, iz, bt, tg)) continue;
         const uint32_t kend = min(cnt, g * 8 + 8);
         for (uint32_t k = g * 8; k < kend; ++k) {
           const uint32_t pos = first + k;
@@ -347,6 +348,7 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
   float bt = tmax0, bu = 0.0f, bv = 0.0f;
   uint32_t visits = 0, tests = 0;
   const float ix = 1.0f / fix_dir(d.x), iy = 1.0f / fix_dir(d.y), iz = 1.0f / fix_dir(d.z);
+  const float4 oi = scaled_origin(o, ix, iy, iz);
   const float zu = o.w * 0.0f, zv = d.w * 0.0f;
   uint32_t st_ref[kStack];
   float st_t[kStack];
@@ -355,7 +357,7 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
   uint32_t ref = root, skip = kNoSkip;
   uint32_t phase = 1, best_phase = 1;
   bool go = true;
-  if (kSeed && valid && tmax0 > 0.0f) go = seed_start<kCount>(r, S, C, o, ix, iy, iz, bt, root, ref, skip, phase, visits);
+  if (kSeed && valid && tmax0 > 0.0f) go = seed_start<kCount>(r, S, C, oi, ix, iy, iz, bt, root, ref, skip, phase, visits);
   auto next = [&]() -> bool {
     while (sp > 0) {
       --sp;
@@ -378,7 +380,7 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
           // 4-wide record: up to four children tested at once, nearest first
           float wt[4];
           uint32_t wr[4];
-          wide_test(C.wide + 8 * (size_t)ref, o, ix, iy, iz, bt, (kSeed && phase) ? skip : kNoSkip, wt, wr);
+          wide_test(C.wide + 8 * (size_t)ref, oi, ix, iy, iz, bt, (kSeed && phase) ? skip : kNoSkip, wt, wr);
           if (kCount) visits += 4;
           if (wt[0] == INFINITY) {
             if (!next()) {
@@ -407,8 +409,8 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
         ldg8(tn + 2, b0, b1);
         if (kCount) visits += 2;
         float ta, tb;
-        bool ha = slab2(a0, a1, o, ix, iy, iz, bt, ta);
-        bool hb = slab2(b0, b1, o, ix, iy, iz, bt, tb);
+        bool ha = slab2(a0, a1, oi, ix, iy, iz, bt, ta);
+        bool hb = slab2(b0, b1, oi, ix, iy, iz, bt, tb);
         const uint32_t ra = __float_as_uint(a0.w), rb = __float_as_uint(b0.w);
         if (kSeed && phase) {
           if (ra == skip) ha = false;
@@ -449,7 +451,7 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
         ldg8(C.groups + 2 * ((size_t)gbase + g), gmn, gmx);
         if (kCount) ++visits;
         float tg;
-        if (slab2(gmn, gmx, o, ix, iy, iz, bt, tg)) {
+        if (slab2(gmn, gmx, oi, ix, iy, iz, bt, tg)) {
           if (g < 32) mask |= 1u << g;
         }
       }
@@ -543,7 +545,7 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
         float4 gmn, gmx;
         ldg8(C.groups + 2 * ((size_t)gbase + g), gmn, gmx);
         float tg;
-        if (!slab2(gmn, gmx, o, ix, iy, iz, bt, tg)) continue;
+        if (!slab2(gmn, gmx, oi, ix, iy, iz, bt, tg)) continue;
         const uint32_t kend = min(cnt, g * 8 + 8);
         for (uint32_t kk = g * 8; kk < kend; ++kk) {
           const uint32_t pos = first + kk;
