@@ -907,6 +907,35 @@ size_t fuse_smem() {
          64;
 }
 
+// Two IEEE single additions in one packed instruction (add.rn.f32x2, sm_100):
+// each lane rounds exactly as a scalar add.
+__device__ __forceinline__ void add2(float a0, float a1, float b0, float b1, float& d0, float& d1) {
+  asm("{\n\t.reg .b64 pa, pb, pd;\n\t"
+      "mov.b64 pa, {%2, %3};\n\t"
+      "mov.b64 pb, {%4, %5};\n\t"
+      "add.rn.f32x2 pd, pa, pb;\n\t"
+      "mov.b64 {%0, %1}, pd;\n\t}"
+      : "=f"(d0), "=f"(d1)
+      : "f"(a0), "f"(a1), "f"(b0), "f"(b1));
+}
+
+// Top-1 sweep of 16 logits (TMEM columns col .. col + 15 of this row) plus
+// their biases into the four interleaved chains (chain j: columns = j mod 4).
+__device__ __forceinline__ void sweep16_top1(const uint32_t (&r)[16], const float* sb, uint32_t col, float (&bk)[4], int32_t (&ik)[4]) {
+  const float4* bp = (const float4*)(sb + col);
+#pragma unroll
+  for (int i4 = 0; i4 < 4; ++i4) {
+    const float4 b = bp[i4];
+    float x[4];
+    add2(__uint_as_float(r[4 * i4]), __uint_as_float(r[4 * i4 + 1]), b.x, b.y, x[0], x[1]);
+    add2(__uint_as_float(r[4 * i4 + 2]), __uint_as_float(r[4 * i4 + 3]), b.z, b.w, x[2], x[3]);
+    const int32_t base = (int32_t)(col + 4 * i4);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (x[j] > bk[j]) { bk[j] = x[j]; ik[j] = base; }
+  }
+}
+
 // kTop2: also track each row's runner-up (for a margin); without it the logit
 // sweep keeps only the maximum and its index (the same index either way).
 template <bool kTop2>
@@ -1145,7 +1174,24 @@ __global__ void __launch_bounds__(kFuseThreads, 1)
         const uint32_t buf = n4 & 1u;
         ok = ok && __all_sync(0xffffffffu, wait(acc_full + buf, (n4 >> 1) & 1u));
         tc_fence_after();
-        if (ok) {
+        if (ok && !kTop2) {
+          // four 16-column loads, each started before the previous one is swept
+          const uint32_t c0 = cq * (kArgBN / 4);
+          const uint32_t tl = tmem + ((qw * 32u) << 16) + buf * kArgBN + c0;
+          const uint32_t col0 = t * kArgBN + c0;
+          uint32_t ra[16], rb[16];
+          tmem_ld16_issue(tl, ra);
+          tmem_ld_wait(ra);
+#pragma unroll
+          for (uint32_t c = 0; c < kArgBN / 4; c += 32) {
+            tmem_ld16_issue(tl + c + 16, rb);
+            sweep16_top1(ra, sb, col0 + c, bk, ik);
+            tmem_ld_wait(rb);
+            if (c + 32 < kArgBN / 4) tmem_ld16_issue(tl + c + 32, ra);
+            sweep16_top1(rb, sb, col0 + c + 16, bk, ik);
+            if (c + 32 < kArgBN / 4) tmem_ld_wait(ra);
+          }
+        } else if (ok) {
           const uint32_t c0 = cq * (kArgBN / 4);
           const uint32_t tl = tmem + ((qw * 32u) << 16) + buf * kArgBN + c0;
 #pragma unroll
