@@ -18,9 +18,11 @@
 //                    leaf counts, pre-order ranks and node ids
 //   k_leaves         one warp per final leaf: expands median subtrees, writes
 //                    node records, reorders faces, pre-gathers triangles
-//                    {v0, e1, e2}, reduces the leaf box and propagates boxes to
-//                    the root with per-node arrival counters (the second
-//                    arrival merges; nobody waits)
+//                    {v0, e1, e2}, reduces the leaf box and records the
+//                    parents of median nodes
+//   k_propagate      one thread per node: each leaf climbs to the root with
+//                    per-node arrival counters (the second arrival merges the
+//                    two child boxes; nobody waits)
 //
 // Node numbering follows the reference's recursion: the k-th internal node in
 // pre-order gets children 2k+1 and 2k+2. A node's pre-order rank among
@@ -338,7 +340,7 @@ struct LeafArgs {
   const uint32_t* ml_lambda;
   const uint4* ml_rec;
   const uint32_t* ml_rank;
-  const uint32_t* parent_id;
+  uint32_t* parent_id;
   uint32_t* arrive;
   uint32_t* nodes;
   uint32_t max_nodes;
@@ -352,25 +354,35 @@ struct LeafArgs {
   uint32_t pos_base;      // first position of this mesh (node records store positions relative to it)
   uint32_t vert_base;     // first vertex of this mesh (faces index vertices relative to it)
   uint32_t* local_indices; // optional: indices[i] - pos_base written here (batched build)
+  uint32_t parent_cap;     // entries of parent_id (median nodes' parents are written here)
 };
 
 constexpr int kMaxMedianDepth = 40;
 // One final leaf (leaf-order index g of its mesh), processed by one warp.
-__device__ __forceinline__ void leaf_body(const LeafArgs& A, const uint32_t g) {
+// `hint` (lane 0's) is the Morton leaf of the warp's previous leaf of the same
+// mesh, or ~0u: a warp walking consecutive leaves then finds each one's Morton
+// leaf in a step or two instead of a binary search.
+__device__ __forceinline__ void leaf_body(const LeafArgs& A, const uint32_t g, uint32_t& hint) {
   const uint32_t lane = lane_id();
   const uint32_t mleaf_count = A.hdr[1];
   {
     uint32_t leaf_id = 0, first = 0, cnt = 0;
-    // median path (ids and ranks from the median root down to the leaf's parent)
-    uint32_t path_id[kMaxMedianDepth], path_rank[kMaxMedianDepth];
-    int plen = 0;
+    int plen = 0;  // median levels walked
     if (lane == 0) {
       // Morton leaf owning global leaf slot g: last k with ml_lambda[k] <= g
-      uint32_t lo = 0, hi = mleaf_count - 1;
-      while (lo < hi) {
-        uint32_t mid = (lo + hi + 1) >> 1;
-        if (A.ml_lambda[mid] <= g) lo = mid; else hi = mid - 1;
+      // (ml_lambda is non-decreasing)
+      uint32_t lo = 0;
+      if (hint < mleaf_count && A.ml_lambda[hint] <= g) {
+        lo = hint;
+        while (lo + 1 < mleaf_count && A.ml_lambda[lo + 1] <= g) ++lo;
+      } else {
+        uint32_t hi = mleaf_count - 1;
+        while (lo < hi) {
+          uint32_t mid = (lo + hi + 1) >> 1;
+          if (A.ml_lambda[mid] <= g) lo = mid; else hi = mid - 1;
+        }
       }
+      hint = lo;
       const uint4 rec = A.ml_rec[lo];
       leaf_id = rec.x; first = rec.y; cnt = rec.z;  // first: absolute position
       if (rec.w & 0x80000000u) {
@@ -381,9 +393,15 @@ __device__ __forceinline__ void leaf_body(const LeafArgs& A, const uint32_t g) {
         while (size >= A.max_leaf && plen < kMaxMedianDepth) {
           const uint32_t left = size >> 1, right = size - left;
           const uint32_t ll = median_leaves(left, A.max_leaf);
-          if (q == 0 && nid < A.max_nodes)
+          // the subtree's first leaf writes the internal record and its children's parent ids
+          if (q == 0 && nid < A.max_nodes) {
             *(uint2*)(A.nodes + 8 * (size_t)nid) = make_uint2((depth % 3u) << 1, 2 * rank + 1);
-          path_id[plen] = nid; path_rank[plen] = rank; ++plen;
+            if (2 * rank + 2 < A.parent_cap) {
+              A.parent_id[2 * rank + 1] = nid;
+              A.parent_id[2 * rank + 2] = nid;
+            }
+          }
+          ++plen;
           if (q < ll) { nid = 2 * rank + 1; rank = rank + 1; size = left; }
           else { q -= ll; nid = 2 * rank + 2; rank = rank + ll; a += left; size = right; }
           ++depth;
@@ -455,38 +473,51 @@ __device__ __forceinline__ void leaf_body(const LeafArgs& A, const uint32_t g) {
       uint32_t* nd = A.nodes + 8 * (size_t)leaf_id;
       *(uint2*)nd = make_uint2(1u | (cnt << 1), lfirst);
       write_box(nd, mn, mx);
-      // propagate up: the second child to arrive merges the two boxes
-      uint32_t cur = leaf_id;
-      for (;;) {
-        uint32_t p, c0;
-        if (plen > 0) { --plen; p = path_id[plen]; c0 = 2 * path_rank[plen] + 1; }
-        else {
-          p = A.parent_id[cur];
-          if (p == kNone) break;
-          c0 = A.nodes[8 * (size_t)p + 1];
-        }
-        __threadfence();
-        if (atomicAdd(A.arrive + p, 1u) == 0u) break;
-        __threadfence();
-        const float* l = (const float*)(A.nodes + 8 * (size_t)c0);
-        const float* r = (const float*)(A.nodes + 8 * (size_t)(c0 + 1));
-        float lb[6], rb[6];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) { lb[q] = __ldcg(l + 2 + q); rb[q] = __ldcg(r + 2 + q); }
-        float3 bmn, bmx;
-        // kernels/CUDA_buildMeshTreeLBVH.cu:269-300: merged only when both children have a positive z extent
-        if (lb[5] - lb[2] > 0.0f && rb[5] - rb[2] > 0.0f) {
-          bmn = make_float3(fmin_sel(lb[0], rb[0]), fmin_sel(lb[1], rb[1]), fmin_sel(lb[2], rb[2]));
-          bmx = make_float3(fmax_sel(lb[3], rb[3]), fmax_sel(lb[4], rb[4]), fmax_sel(lb[5], rb[5]));
-        } else {
-          bmn = make_float3(kHuge, kHuge, kHuge);
-          bmx = make_float3(-kHuge, -kHuge, -kHuge);
-        }
-        write_box(A.nodes + 8 * (size_t)p, bmn, bmx);
-        cur = p;
-      }
     }
   }
+}
+
+// Node boxes bottom-up, one thread per leaf: the leaf (its box written by the
+// leaf kernel) climbs through parent_id; at each internal node the first of
+// its two children to arrive stops, the second merges both children's boxes
+// and climbs on. cap bounds every node id (the node array's capacity).
+__device__ __forceinline__ void climb(uint32_t* __restrict__ nodes, const uint32_t* __restrict__ parent_id, uint32_t* __restrict__ arrive,
+                                      uint32_t cap, uint32_t leaf) {
+  uint32_t cur = leaf;
+  for (;;) {
+    const uint32_t p = parent_id[cur];
+    if (p == kNone || p >= cap) break;
+    __threadfence();
+    if (atomicAdd(arrive + p, 1u) == 0u) break;
+    __threadfence();
+    const uint32_t c0 = __ldcg(nodes + 8 * (size_t)p + 1);
+    if (c0 + 1 >= cap) break;
+    const float* l = (const float*)(nodes + 8 * (size_t)c0);
+    const float* r = (const float*)(nodes + 8 * (size_t)(c0 + 1));
+    float lb[6], rb[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) { lb[q] = __ldcg(l + 2 + q); rb[q] = __ldcg(r + 2 + q); }
+    float3 bmn, bmx;
+    // kernels/CUDA_buildMeshTreeLBVH.cu:269-300: merged only when both children have a positive z extent
+    if (lb[5] - lb[2] > 0.0f && rb[5] - rb[2] > 0.0f) {
+      bmn = make_float3(fmin_sel(lb[0], rb[0]), fmin_sel(lb[1], rb[1]), fmin_sel(lb[2], rb[2]));
+      bmx = make_float3(fmax_sel(lb[3], rb[3]), fmax_sel(lb[4], rb[4]), fmax_sel(lb[5], rb[5]));
+    } else {
+      bmn = make_float3(kHuge, kHuge, kHuge);
+      bmx = make_float3(-kHuge, -kHuge, -kHuge);
+    }
+    write_box(nodes + 8 * (size_t)p, bmn, bmx);
+    cur = p;
+  }
+}
+
+// Bottom-up boxes of a single mesh: one thread per node, the leaves climb.
+__global__ __launch_bounds__(256) void k_propagate(uint32_t* __restrict__ nodes, const uint32_t* __restrict__ parent_id,
+                                                   uint32_t* __restrict__ arrive, const uint32_t* __restrict__ hdr, uint32_t cap) {
+  if (hdr[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) return;
+  const uint32_t node_count = min(hdr[2], cap);
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < node_count; p += gridDim.x * blockDim.x)
+    if (nodes[8 * (size_t)p] & 1u) climb(nodes, parent_id, arrive, cap, p);
 }
 
 __global__ __launch_bounds__(256) void k_leaves(LeafArgs A) {
@@ -494,7 +525,11 @@ __global__ __launch_bounds__(256) void k_leaves(LeafArgs A) {
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t leaf_count = A.hdr[0];
   if (A.hdr[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) return;
-  for (uint32_t g = warp_global; g < leaf_count; g += nwarps) leaf_body(A, g);
+  // a contiguous run of leaves per warp (the grid is one resident wave)
+  const uint32_t per = (leaf_count + nwarps - 1) / nwarps;
+  const uint32_t g0 = min(leaf_count, warp_global * per), g1 = min(leaf_count, g0 + per);
+  uint32_t hint = ~0u;
+  for (uint32_t g = g0; g < g1; ++g) leaf_body(A, g, hint);
 }
 
 // Two-child traversal records, indexed by pre-order rank (internal node p
@@ -600,6 +635,19 @@ int sm_count() {
     if (sms <= 0) sms = 148;
   }
   return sms;
+}
+
+// Blocks of `kernel` (with `threads` per block and no dynamic shared memory)
+// that one SM holds at once: a grid of sm_count() times this is one resident
+// wave. Queried once per kernel (the first call).
+template <typename K>
+int resident_blocks_of(K kernel, int threads) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, 0) != cudaSuccess || nb <= 0) {
+    cudaGetLastError();
+    nb = 1;
+  }
+  return nb;
 }
 
 }  // namespace
@@ -725,8 +773,11 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
     A.pos_base = 0;
     A.vert_base = 0;
     A.local_indices = nullptr;
-    k_leaves<<<sms * 8, 256, 0, st>>>(A);
-    note_launch();
+    A.parent_cap = count;
+    static const int leaf_blocks = resident_blocks_of(k_leaves, 256);
+    k_leaves<<<sms * leaf_blocks, 256, 0, st>>>(A);
+    k_propagate<<<sms * 8, 256, 0, st>>>(d->nodes, L.parent_id, L.arrive, L.hdr, count);
+    note_launch(2);
     RT_CHECK_LAUNCH();
     if (accel) {
       k_accel_nodes<<<sms * 4, 256, 0, st>>>(d->nodes, L.hdr, L.leaf_lambda, AL.tnodes, AL.hdr);
@@ -950,18 +1001,51 @@ __global__ __launch_bounds__(256) void k_batch_leaves(BatchArgs B) {
   const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t total = B.leaf_base[B.M];
-  for (uint32_t g = warp_global; g < total; g += nwarps) {
-    const uint32_t m = find_seg(B.leaf_base, B.M, g);
+  // a contiguous run of leaves per warp (the grid is one resident wave): the
+  // mesh and the Morton-leaf search carry over from one leaf to the next
+  const uint32_t per = (total + nwarps - 1) / nwarps;
+  const uint32_t g0 = min(total, warp_global * per), g1 = min(total, g0 + per);
+  if (g0 >= g1) return;
+  uint32_t m = find_seg(B.leaf_base, B.M, g0), hint = ~0u;
+  LeafArgs A;
+  auto mesh_args = [&]() {
     const uint32_t F = B.foff[m], n = B.foff[m + 1] - F;
     const uint32_t bb = bfs_base(F, m), nb = node_base(F, m);
-    LeafArgs A;
     A.verts = B.verts; A.faces_in = B.faces_in; A.faces_out = B.faces_out; A.tris = B.tris; A.indices = B.idx;
     A.ml_lambda = B.ml_lambda + bb; A.ml_rec = B.ml_rec + bb; A.ml_rank = B.ml_rank + bb;
     A.parent_id = B.parent_id + nb; A.arrive = B.arrive + nb; A.nodes = B.nodes + 8 * (size_t)nb; A.max_nodes = 2 * n - 1;
     A.max_leaf = B.q.max_leaf; A.hdr = B.hdr + 16 * m; A.err = B.err;
     A.acc_leaves = B.acc_leaves + F; A.acc_groups = B.groups + 2 * (size_t)group_base(F, m); A.leaf_lambda = B.leaf_lambda + nb;
-    A.pos_base = F; A.vert_base = B.voff[m]; A.local_indices = B.indices_out;
-    leaf_body(A, g - B.leaf_base[m]);
+    A.pos_base = F; A.vert_base = B.voff[m]; A.local_indices = B.indices_out; A.parent_cap = 2 * n - 1;
+  };
+  mesh_args();
+  for (uint32_t g = g0; g < g1; ++g) {
+    if (B.leaf_base[m + 1] <= g) {  // the next non-empty mesh
+      while (B.leaf_base[m + 1] <= g) ++m;
+      mesh_args();
+      hint = ~0u;
+    }
+    leaf_body(A, g - B.leaf_base[m], hint);
+  }
+}
+
+// Bottom-up boxes of every mesh: one thread per node slot, the leaves climb.
+__global__ __launch_bounds__(256) void k_batch_propagate(BatchArgs B) {
+  const uint32_t slots = 2 * B.N - B.M;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < slots; p += gridDim.x * blockDim.x) {
+    // mesh whose node range holds slot p: largest m with 2 F_m - m <= p
+    uint32_t lo = 0, hi = B.M - 1;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (node_base(__ldg(B.foff + mid), mid) <= p) lo = mid; else hi = mid - 1;
+    }
+    const uint32_t m = lo, F = B.foff[m], n = B.foff[m + 1] - F, nb = node_base(F, m);
+    const uint32_t* h = B.hdr + 16 * m;
+    if (h[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) continue;
+    const uint32_t lp = p - nb, cap = 2 * n - 1;
+    if (lp >= h[2] || lp >= cap) continue;
+    uint32_t* nodes = B.nodes + 8 * (size_t)nb;
+    if (nodes[8 * (size_t)lp] & 1u) climb(nodes, B.parent_id + nb, B.arrive + nb, cap, lp);
   }
 }
 
@@ -1116,11 +1200,13 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   note_launch(3);
   RT_CHECK_LAUNCH();
   if (cudaMemsetAsync(B.arrive, 0, (2 * (size_t)N) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
-  k_batch_leaves<<<sms * 8, 256, 0, st>>>(B);
+  static const int leaf_blocks = resident_blocks_of(k_batch_leaves, 256);
+  k_batch_leaves<<<sms * leaf_blocks, 256, 0, st>>>(B);
+  k_batch_propagate<<<sms * 8, 256, 0, st>>>(B);
   k_batch_accel_nodes<<<sms * 4, 256, 0, st>>>(B);
   k_batch_wide_nodes<<<sms * 4, 256, 0, st>>>(B);
   k_batch_info<<<(M + 255) / 256, 256, 0, st>>>(B);
-  note_launch(4);
+  note_launch(5);
   RT_CHECK_LAUNCH();
   return RT_OK;
 }

@@ -9,6 +9,7 @@ steady-state launch. Cases (kernel of interest in brackets):
 
   bench_step     three steps of the main workload (build, primary, bounce)     [launch list]
   build_16m      LBVH build of a 2^24-face soup, twice                            [k_radix_scatter, k_leaves, k_boxes_morton]
+  batch_build    batched build of 1024 meshes (9.9M faces), twice                 [launch list]
   trace_primary  2^20-face soup, 1920x1080 primary rays, tuned tile schedule   [k_trace_accel]
   trace_bounce   the same scene's diffuse bounces, cooperative schedule          [k_trace_coop]
   mlp_propose    proposal network inference on 2^18 rays (4096 slots)            [k_mlp_propose_tc]
@@ -87,6 +88,18 @@ def build_16m():
     torch.cuda.synchronize()
 
 
+def batch_build():
+    from . import core, scenes
+    meshes = scenes.batch_meshes(1024, seed=3)
+    verts, faces, fo, vo = scenes.concat_batch(meshes)
+    del meshes
+    v = torch.from_numpy(verts).cuda()
+    f = torch.from_numpy(faces.view(np.int32)).cuda()
+    t = core.batch_build(v, f, fo, vo)
+    core.batch_build(v, f, fo, vo, out=t)
+    torch.cuda.synchronize()
+
+
 def mlp_propose():
     from . import proposal, scenes
     box = (-1.5, -0.6, -1.5, 1.5, 1.4, 1.5)
@@ -146,7 +159,7 @@ def mlp_grouped():
     torch.cuda.synchronize()
 
 
-CASES = {"bench_step": bench_step, "build_16m": build_16m, "trace_primary": trace_primary, "trace_bounce": trace_bounce, "mlp_propose": mlp_propose, "mlp_train": mlp_train,
+CASES = {"bench_step": bench_step, "build_16m": build_16m, "batch_build": batch_build, "trace_primary": trace_primary, "trace_bounce": trace_bounce, "mlp_propose": mlp_propose, "mlp_train": mlp_train,
          "sah_build": sah_build, "raster": raster, "mlp_grouped": mlp_grouped}
 
 if __name__ == "__main__":
