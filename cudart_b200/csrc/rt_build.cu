@@ -877,20 +877,38 @@ struct BatchArgs {
   rt_build_info* info_out;
 };
 
-__global__ __launch_bounds__(256) void k_batch_hitbox(BatchArgs B) {
+// Per-mesh hitbox: one 512-thread block per mesh, four loads in flight per
+// thread (the largest meshes bound the launch).
+__global__ __launch_bounds__(512) void k_batch_hitbox(BatchArgs B) {
   const uint32_t m = blockIdx.x;
   const uint32_t v0 = B.voff[m], v1 = B.voff[m + 1];
-  float4 mn = make_float4(kHuge, kHuge, kHuge, kHuge), mx = make_float4(-kHuge, -kHuge, -kHuge, -kHuge);
-  for (uint32_t i = v0 + threadIdx.x; i < v1; i += blockDim.x) {
-    const float4 p = ldg4(B.verts + i);
-    mn = f4min(mn, p);
-    mx = f4max(mx, p);
+  float4 mn[4], mx[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    mn[k] = make_float4(kHuge, kHuge, kHuge, kHuge);
+    mx[k] = make_float4(-kHuge, -kHuge, -kHuge, -kHuge);
   }
-  __shared__ float4 s_mn[256], s_mx[256];
-  s_mn[threadIdx.x] = mn;
-  s_mx[threadIdx.x] = mx;
+  uint32_t i = v0 + threadIdx.x;
+  for (; i + 3 * 512 < v1; i += 4 * 512) {
+    float4 p[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) p[k] = ldg4(B.verts + i + k * 512);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      mn[k] = f4min(mn[k], p[k]);
+      mx[k] = f4max(mx[k], p[k]);
+    }
+  }
+  for (; i < v1; i += 512) {
+    const float4 p = ldg4(B.verts + i);
+    mn[0] = f4min(mn[0], p);
+    mx[0] = f4max(mx[0], p);
+  }
+  __shared__ float4 s_mn[512], s_mx[512];
+  s_mn[threadIdx.x] = f4min(f4min(mn[0], mn[1]), f4min(mn[2], mn[3]));
+  s_mx[threadIdx.x] = f4max(f4max(mx[0], mx[1]), f4max(mx[2], mx[3]));
   __syncthreads();
-  for (int o = 128; o > 0; o >>= 1) {
+  for (int o = 256; o > 0; o >>= 1) {
     if (threadIdx.x < o) {
       s_mn[threadIdx.x] = f4min(s_mn[threadIdx.x], s_mn[threadIdx.x + o]);
       s_mx[threadIdx.x] = f4max(s_mx[threadIdx.x], s_mx[threadIdx.x + o]);
@@ -1173,7 +1191,7 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   cudaStream_t st = (cudaStream_t)stream_;
   const int sms = sm_count();
   const uint32_t fblocks = (uint32_t)hmin<uint64_t>((N + 255) / 256, (uint64_t)sms * 16);
-  k_batch_hitbox<<<M, 256, 0, st>>>(B);
+  k_batch_hitbox<<<M, 512, 0, st>>>(B);
   k_batch_boxes_morton<<<fblocks, 256, 0, st>>>(B);
   note_launch(2);
   RT_CHECK_LAUNCH();
