@@ -1200,7 +1200,13 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   k_batch_meshkey<<<fblocks, 256, 0, st>>>(B);
   note_launch();
   RT_CHECK_LAUNCH();
-  s = radix_sort_pairs(B.mkey, B.idx, N, 0, 16, 0, sort_scratch, sort_bytes, st, nullptr);
+  // key widths in whole 8-bit digits: mesh ids < M, level keys < 64 (M - 1) + 33
+  auto digit_bits = [](uint64_t maxval) -> uint32_t {
+    uint32_t b = 1;
+    while (b < 64 && (1ull << b) <= maxval) ++b;
+    return b > 24 ? 32u : (b + 7) / 8 * 8;
+  };
+  s = radix_sort_pairs(B.mkey, B.idx, N, 0, digit_bits(M - 1), 0, sort_scratch, sort_bytes, st, nullptr);
   if (s != RT_OK) return s;
   if (cudaMemsetAsync(B.hist, 0, ((size_t)M * 64 + 1) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   k_batch_levels<<<fblocks, 256, 0, st>>>(B);
@@ -1208,7 +1214,7 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   note_launch(2);
   RT_CHECK_LAUNCH();
   if (N > 1) {
-    s = radix_sort_pairs(B.lev, B.C, N - 1, 0, 24, 0, sort_scratch, sort_bytes, st, nullptr);
+    s = radix_sort_pairs(B.lev, B.C, N - 1, 0, digit_bits(64ull * (M - 1) + 32), 0, sort_scratch, sort_bytes, st, nullptr);
     if (s != RT_OK) return s;
   }
   k_batch_level_starts<<<1, 1024, 0, st>>>(B);
