@@ -56,15 +56,33 @@ __global__ void k_set_hitbox(float4* hit, float4 mn, float4 mx) {
 }
 
 __global__ __launch_bounds__(256) void k_hitbox_partial(const float4* __restrict__ v, uint32_t count, float4* __restrict__ partial) {
-  float4 mn = make_float4(kHuge, kHuge, kHuge, kHuge), mx = make_float4(-kHuge, -kHuge, -kHuge, -kHuge);
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    float4 p = ldg4(v + i);
-    mn = f4min(mn, p);
-    mx = f4max(mx, p);
+  // four loads in flight per thread, one accumulator each
+  float4 mn[4], mx[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    mn[k] = make_float4(kHuge, kHuge, kHuge, kHuge);
+    mx[k] = make_float4(-kHuge, -kHuge, -kHuge, -kHuge);
+  }
+  const uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (; (uint64_t)i + 3ull * stride < count; i += 4 * stride) {
+    float4 p[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) p[k] = ldg4(v + i + k * stride);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      mn[k] = f4min(mn[k], p[k]);
+      mx[k] = f4max(mx[k], p[k]);
+    }
+  }
+  for (; i < count; i += stride) {
+    const float4 p = ldg4(v + i);
+    mn[0] = f4min(mn[0], p);
+    mx[0] = f4max(mx[0], p);
   }
   __shared__ float4 s_mn[256], s_mx[256];
-  s_mn[threadIdx.x] = mn;
-  s_mx[threadIdx.x] = mx;
+  s_mn[threadIdx.x] = f4min(f4min(mn[0], mn[1]), f4min(mn[2], mn[3]));
+  s_mx[threadIdx.x] = f4max(f4max(mx[0], mx[1]), f4max(mx[2], mx[3]));
   __syncthreads();
   for (int o = 128; o > 0; o >>= 1) {
     if (threadIdx.x < o) {
@@ -115,21 +133,31 @@ __global__ __launch_bounds__(256) void k_boxes_morton(const float4* __restrict__
   const float sx = (layout == 30 ? 1023.0f : 2047.0f) / lx;
   const float sy = (layout == 30 ? 1023.0f : 2047.0f) / ly;
   const float sz = 1023.0f / lz;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    uint4 f = ldg4(faces + k);
-    float4 v0 = ldg4(verts + f.x), v1 = ldg4(verts + f.y), v2 = ldg4(verts + f.z);
-    float4 mn = f4min(f4min(v0, v1), v2);
-    float4 mx = f4max(f4max(v0, v1), v2);
+  auto face = [&](uint32_t k, const float4& v0, const float4& v1, const float4& v2) {
+    const float4 mn = f4min(f4min(v0, v1), v2);
+    const float4 mx = f4max(f4max(v0, v1), v2);
     boxes[2 * (size_t)k] = mn;
     boxes[2 * (size_t)k + 1] = mx;
     if (idx) idx[k] = k;
     if (codes) {
-      float cx = 0.5f * (mn.x + mx.x), cy = 0.5f * (mn.y + mx.y), cz = 0.5f * (mn.z + mx.z);
-      uint32_t qx = f2u_sat((cx - hmin.x) * sx);
-      uint32_t qy = f2u_sat((cy - hmin.y) * sy);
-      uint32_t qz = f2u_sat((cz - hmin.z) * sz);
+      const float cx = 0.5f * (mn.x + mx.x), cy = 0.5f * (mn.y + mx.y), cz = 0.5f * (mn.z + mx.z);
+      const uint32_t qx = f2u_sat((cx - hmin.x) * sx);
+      const uint32_t qy = f2u_sat((cy - hmin.y) * sy);
+      const uint32_t qz = f2u_sat((cz - hmin.z) * sz);
       codes[k] = spread_code(qx, qy, qz, layout);
     }
+  };
+  // two faces per iteration: their face and vertex loads are in flight together
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += 2 * stride) {
+    const uint32_t k2 = k + stride;
+    const bool two = k2 < n;
+    const uint4 f = ldg4(faces + k);
+    const uint4 f2 = two ? ldg4(faces + k2) : f;
+    const float4 v0 = ldg4(verts + f.x), v1 = ldg4(verts + f.y), v2 = ldg4(verts + f.z);
+    const float4 w0 = ldg4(verts + f2.x), w1 = ldg4(verts + f2.y), w2 = ldg4(verts + f2.z);
+    face(k, v0, v1, v2);
+    if (two) face(k2, w0, w1, w2);
   }
 }
 
@@ -584,7 +612,7 @@ struct BuildLayout {
   uint4* faces_tmp;
 };
 
-constexpr uint32_t kHitParts = 296;
+constexpr uint32_t kHitParts = 1184;  // 8 blocks per SM on 148 SMs
 
 __host__ __device__ uint32_t morton_cap_dev(uint32_t n, uint32_t D) {
   uint64_t a = (D >= 31) ? (1ull << 32) : ((1ull << (D + 1)) - 1);
