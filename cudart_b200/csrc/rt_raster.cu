@@ -62,14 +62,21 @@ __global__ __launch_bounds__(256) void k_raster_setup(const float4* __restrict__
     if (fc.x >= vcount || fc.y >= vcount || fc.z >= vcount) {
       atomicOr(err, (uint32_t)RT_DEVERR_NODE_CAPACITY);
     } else {
-      const float4 a = project(M, __ldg(verts + fc.x)), b = project(M, __ldg(verts + fc.y)), cc = project(M, __ldg(verts + fc.z));
+      float4 a = project(M, __ldg(verts + fc.x));
+      const float4 b = project(M, __ldg(verts + fc.y)), cc = project(M, __ldg(verts + fc.z));
+      // the face's determinant (intersectTriPoint, :52-71, the same arithmetic as the
+      // zone pass would do per pixel): a face the test always rejects gets no zone
+      // pairs; otherwise its reciprocal rides in a.w
+      const float det = (b.x - a.x) * (cc.y - a.y) - (cc.x - a.x) * (b.y - a.y);
+      const bool degenerate = det > -kRasterEps && det < kRasterEps;
+      a.w = degenerate ? 0.0f : 1.0f / det;
       tri[3 * (size_t)f] = a;
       tri[3 * (size_t)f + 1] = b;
       tri[3 * (size_t)f + 2] = cc;
       const float mnx = fminf(fminf(fminf(kHuge, a.x), b.x), cc.x), mny = fminf(fminf(fminf(kHuge, a.y), b.y), cc.y);
       const float mxx = fmaxf(fmaxf(fmaxf(-kHuge, a.x), b.x), cc.x), mxy = fmaxf(fmaxf(fmaxf(-kHuge, a.y), b.y), cc.y);
       // intersectRectRect with [-1, 1]^2 (:47-50, :150)
-      if (mnx < 1.0f && mxx > -1.0f && mny < 1.0f && mxy > -1.0f) {
+      if (!degenerate && mnx < 1.0f && mxx > -1.0f && mny < 1.0f && mxy > -1.0f) {
         const int x0 = max(__float2int_rz(Z.zsx * (mnx + 1.0f)), 0) / 2 * 2;
         const int y0 = max(__float2int_rz(Z.zsy * (1.0f - mxy)), 0) / 2 * 2;
         const int x1 = min(__float2int_rz(Z.zsx * (mxx + 1.0f)), Z.zcx - 1);
@@ -134,10 +141,9 @@ __global__ __launch_bounds__(256) void k_raster_zones(const float4* __restrict__
     for (uint32_t p = s; p < e; ++p) {
       const uint32_t f = __ldg(vals + p);
       const float4 a = __ldg(tri + 3 * (size_t)f), b = __ldg(tri + 3 * (size_t)f + 1), c = __ldg(tri + 3 * (size_t)f + 2);
-      // intersectTriPoint (:52-71)
-      const float det = (b.x - a.x) * (c.y - a.y) - (c.x - a.x) * (b.y - a.y);
-      if (det > -kRasterEps && det < kRasterEps) continue;
-      const float inv_det = 1.0f / det;
+      // intersectTriPoint (:52-71); the face setup pass computed 1 / det (a.w) and
+      // emitted no pairs for faces with |det| below the threshold
+      const float inv_det = a.w;
       const float u = ((c.x - px) * (a.y - py) - (a.x - px) * (c.y - py)) * inv_det;
       if (u < 0.0f || u > 1.0f) continue;
       const float v = ((a.x - px) * (b.y - py) - (b.x - px) * (a.y - py)) * inv_det;
