@@ -4,14 +4,16 @@
 // The reference runs 2 x 2 blocks of 8 x 4 threads over the whole screen,
 // each block walking every face through a 192-face shared-memory cache. Here
 // the work is binned instead: one thread per face transforms its vertices,
-// drops faces off screen and computes the reference's zone rectangle; every
-// (zone, face) pair is emitted in face order and stably sorted by zone; then
-// one warp per 8 x 4 zone (lane = pixel, the reference's thread layout) walks
-// its zone's faces in index order, keeping depth / id / (u, v) in registers.
-// The per-pixel result is the reference's: the same tests on the same faces in
-// the same order. Faces are processed in chunks whose pair count fits the
-// scratch (a face can cover many zones); the surfaces carry the state across
-// chunks, which keeps the face order.
+// drops faces off screen (and faces the barycentric test always rejects) and
+// computes the reference's zone rectangle; every face is appended to the list
+// of each zone of its rectangle (a counting sort: count, scan, fill); then one
+// warp per 8 x 4 zone (lane = pixel, the reference's thread layout) walks its
+// zone's faces, keeping depth / id / (u, v) in registers and taking the
+// minimum (depth, face index). The per-pixel result is the reference's: the
+// same tests on the same faces, and the face the reference's index-order walk
+// with a strict depth test keeps. Faces are processed in chunks, in index
+// order, whose pair count fits the scratch (a face can cover many zones); the
+// surfaces carry the state across chunks.
 #include <cstring>
 #include <vector>
 
@@ -94,29 +96,32 @@ __global__ __launch_bounds__(256) void k_raster_setup(const float4* __restrict__
 }
 
 // (zone, face) pairs of faces [f0, f1) at their offsets, in face order.
-__global__ __launch_bounds__(256) void k_raster_emit(const int4* __restrict__ rect, const uint32_t* __restrict__ cnt,
-                                                     const uint32_t* __restrict__ off, uint32_t f0, uint32_t f1, int zcx,
-                                                     uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+// The (zone, face) pairs of faces [f0, f1) binned by zone without a sort:
+// k_raster_count counts each zone's faces, an exclusive scan turns the counts
+// into list starts, and k_raster_fill appends every face to its zones' lists.
+// The order inside a list is whatever the atomics give; the zone pass takes
+// the minimum (depth, face index), which is what visiting the faces in index
+// order with a strict depth test keeps.
+__global__ __launch_bounds__(256) void k_raster_count(const int4* __restrict__ rect, const uint32_t* __restrict__ cnt, uint32_t f0,
+                                                      uint32_t f1, int zcx, uint32_t* __restrict__ zcount) {
   for (uint32_t f = f0 + blockIdx.x * blockDim.x + threadIdx.x; f < f1; f += gridDim.x * blockDim.x) {
-    const uint32_t c = cnt[f];
-    if (!c) continue;
+    if (!cnt[f]) continue;
     const int4 r = rect[f];
-    uint32_t o = off[f - f0];
     for (int j = r.y; j <= r.w; ++j)
-      for (int i = r.x; i <= r.z; ++i) {
-        keys[o] = (uint32_t)(j * zcx + i);
-        vals[o] = f;
-        ++o;
-      }
+      for (int i = r.x; i <= r.z; ++i) atomicAdd(zcount + (uint32_t)(j * zcx + i), 1u);
   }
 }
-
-__global__ __launch_bounds__(256) void k_zone_ranges(const uint32_t* __restrict__ keys, uint32_t P, uint32_t* __restrict__ zs,
-                                                     uint32_t* __restrict__ ze) {
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
-    const uint32_t z = keys[p];
-    if (p == 0 || keys[p - 1] != z) zs[z] = p;
-    if (p + 1 == P || keys[p + 1] != z) ze[z] = p + 1;
+__global__ __launch_bounds__(256) void k_raster_fill(const int4* __restrict__ rect, const uint32_t* __restrict__ cnt, uint32_t f0,
+                                                     uint32_t f1, int zcx, const uint32_t* __restrict__ zoff, uint32_t* __restrict__ zfill,
+                                                     uint32_t* __restrict__ vals) {
+  for (uint32_t f = f0 + blockIdx.x * blockDim.x + threadIdx.x; f < f1; f += gridDim.x * blockDim.x) {
+    if (!cnt[f]) continue;
+    const int4 r = rect[f];
+    for (int j = r.y; j <= r.w; ++j)
+      for (int i = r.x; i <= r.z; ++i) {
+        const uint32_t z = (uint32_t)(j * zcx + i);
+        vals[zoff[z] + atomicAdd(zfill + z, 1u)] = f;
+      }
   }
 }
 
@@ -149,7 +154,9 @@ __global__ __launch_bounds__(256) void k_raster_zones(const float4* __restrict__
       const float v = ((a.x - px) * (b.y - py) - (b.x - px) * (a.y - py)) * inv_det;
       if (v < 0.0f || u + v > 1.0f) continue;
       const float t = (1.0f - u - v) * a.z + u * b.z + v * c.z;
-      if (inside && t > 0 && t < best) {
+      // the earliest face wins a depth tie: faces arrive in any order, and the
+      // depth of an earlier chunk (bf < 0) is only beaten by a strictly nearer face
+      if (inside && t > 0 && (t < best || (t == best && bf >= 0 && (int32_t)f < bf))) {
         best = t;
         bf = (int32_t)f;
         bu = u;
@@ -183,9 +190,7 @@ Zones zones_of(uint32_t width, uint32_t height) {
 struct RasterLayout {
   float4* tri;
   int4* rect;
-  uint32_t *cnt, *block_sum, *off, *sums, *keys, *vals, *zs, *ze, *err;
-  void* sort_scratch;
-  size_t sort_bytes;
+  uint32_t *cnt, *block_sum, *vals, *zoff, *zfill, *zsums, *err;
   uint32_t cap;
 };
 
@@ -199,15 +204,11 @@ size_t carve_raster(Carve& c, RasterLayout& L, uint32_t n, uint32_t width, uint3
   L.rect = c.take<int4>(n);
   L.cnt = c.take<uint32_t>(n);
   L.block_sum = c.take<uint32_t>(n / kFacesPerBlock + 1);
-  L.off = c.take<uint32_t>(n + 1);
-  L.sums = c.take<uint32_t>(n / 1024 + 2);
-  L.keys = c.take<uint32_t>(L.cap);
   L.vals = c.take<uint32_t>(L.cap);
-  L.zs = c.take<uint32_t>(nz);
-  L.ze = c.take<uint32_t>(nz);
+  L.zoff = c.take<uint32_t>(nz + 1);
+  L.zfill = c.take<uint32_t>(nz);
+  L.zsums = c.take<uint32_t>(nz / 1024 + 2);
   L.err = c.take<uint32_t>(1);
-  L.sort_bytes = radix_scratch_bytes(L.cap);
-  L.sort_scratch = c.take<char>(L.sort_bytes);
   return c.off + 256;
 }
 
@@ -263,23 +264,19 @@ extern "C" rt_status rt_rasterize(const rt_raster_desc* d, rt_stream stream) {
     const uint32_t f0 = b * kFacesPerBlock, f1 = e * kFacesPerBlock < n ? e * kFacesPerBlock : n;
     b = e;
     if (P == 0) continue;
-    const uint32_t m = f1 - f0;
-    if (cudaMemcpyAsync(L.off, L.cnt + f0, (size_t)m * 4, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return RT_ERR_CUDA;
-    excl_scan(L.off, m, L.sums, nullptr, st);
-    k_raster_emit<<<(uint32_t)hmin<uint64_t>((m + 255) / 256, (uint64_t)sms * 8), 256, 0, st>>>(L.rect, L.cnt, L.off, f0, f1, Z.zcx, L.keys,
-                                                                                              L.vals);
+    const uint32_t fblocks = (uint32_t)hmin<uint64_t>((f1 - f0 + 255) / 256, (uint64_t)sms * 8);
+    if (cudaMemsetAsync(L.zoff, 0, ((size_t)nz + 1) * 4, st) != cudaSuccess || cudaMemsetAsync(L.zfill, 0, (size_t)nz * 4, st) != cudaSuccess)
+      return RT_ERR_CUDA;
+    k_raster_count<<<fblocks, 256, 0, st>>>(L.rect, L.cnt, f0, f1, Z.zcx, L.zoff);
     note_launch();
     RT_CHECK_LAUNCH();
-    uint32_t bits = 1;
-    while (bits < 32 && (1ull << bits) < nz) ++bits;
-    const rt_status s = radix_sort_pairs(L.keys, L.vals, (uint32_t)P, 0, bits, 0, L.sort_scratch, L.sort_bytes, st, nullptr);
-    if (s != RT_OK) return s;
-    if (cudaMemsetAsync(L.zs, 0, (size_t)nz * 4, st) != cudaSuccess || cudaMemsetAsync(L.ze, 0, (size_t)nz * 4, st) != cudaSuccess)
-      return RT_ERR_CUDA;
-    k_zone_ranges<<<(uint32_t)hmin<uint64_t>((P + 255) / 256, (uint64_t)sms * 16), 256, 0, st>>>(L.keys, (uint32_t)P, L.zs, L.ze);
+    excl_scan(L.zoff, nz + 1, L.zsums, nullptr, st);
+    k_raster_fill<<<fblocks, 256, 0, st>>>(L.rect, L.cnt, f0, f1, Z.zcx, L.zoff, L.zfill, L.vals);
+    note_launch();
+    RT_CHECK_LAUNCH();
     k_raster_zones<<<(uint32_t)hmin<uint64_t>(((uint64_t)nz * 32 + 255) / 256, (uint64_t)sms * 16), 256, 0, st>>>(
-        L.tri, L.vals, L.zs, L.ze, nz, Z.zcx, (int)d->width, (int)d->height, d->id_mode, d->face_id, (float2*)d->uv, d->depth);
-    note_launch(2);
+        L.tri, L.vals, L.zoff, L.zoff + 1, nz, Z.zcx, (int)d->width, (int)d->height, d->id_mode, d->face_id, (float2*)d->uv, d->depth);
+    note_launch();
     RT_CHECK_LAUNCH();
   }
   return RT_OK;

@@ -10,7 +10,7 @@
  * of its zone rectangle (start rounded down to an even zone) at each pixel's
  * corner (x * 2 / width - 1, 1 - y * 2 / height) with a 2-D barycentric test
  * (|det| < 1e-6 rejected); a pixel takes the face of smallest depth t > 0,
- * the earliest face on equal depth (faces are tested in index order).
+ * the earliest face on equal depth (the reference tests faces in index order).
  */
 #ifndef RT_RASTER_H
 #define RT_RASTER_H

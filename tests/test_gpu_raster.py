@@ -2,7 +2,8 @@
 the reference's rasteriser kernel (tests/test_oracle_raster.py): face id,
 (u, v) and depth bit for bit, for face-index ids and for the reference's
 block-start ids; pre-filled depth surfaces; a scene whose pairs need several
-chunks; and a 1920 x 1080 frame of the 2^20-face soup."""
+chunks; faces drawn twice (exact depth ties); and a 1920 x 1080 frame of the
+2^20-face soup."""
 import numpy as np
 import pytest
 import torch
@@ -86,6 +87,22 @@ def test_raster_many_chunks(oracle):
     m, vv, ff = _setup(oracle, mesh, (0.01, 0.02, -1.0), (0.0, 0.0, 0.0), w, h)
     hit = _compare(oracle, mesh, m, vv, ff, w, h, pair_capacity=1)
     assert hit.mean() > 0.9
+
+
+@pytest.mark.parametrize("pair_capacity", [0, 1])
+def test_raster_exact_depth_ties(oracle, pair_capacity):
+    """Every face drawn twice (the face list followed by itself, in reverse
+    order in the copy): each covered pixel sees two faces at exactly the same
+    depth, and the earlier index must win however the zone lists order them;
+    at the smallest pair budget the two copies fall in different chunks."""
+    from cudart_b200 import scenes
+    src = scenes.soup(20000, 9)
+    faces = np.concatenate([src.faces, src.faces[::-1]]).copy()
+    mesh = scenes.Mesh(src.vertices, faces)
+    w, h = 160, 96
+    m, v, f = _setup(oracle, mesh, (0.62, 0.71, -0.45), (0.5, 0.5, 0.5), w, h)
+    hit = _compare(oracle, mesh, m, v, f, w, h, pair_capacity=pair_capacity)
+    assert hit.mean() > 0.05
 
 
 def test_raster_full_frame_soup(oracle):
