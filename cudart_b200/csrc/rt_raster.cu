@@ -115,13 +115,25 @@ __global__ __launch_bounds__(256) void k_raster_fill(const int4* __restrict__ re
                                                      uint32_t f1, int zcx, const uint32_t* __restrict__ zoff, uint32_t* __restrict__ zfill,
                                                      uint32_t* __restrict__ vals) {
   for (uint32_t f = f0 + blockIdx.x * blockDim.x + threadIdx.x; f < f1; f += gridDim.x * blockDim.x) {
-    if (!cnt[f]) continue;
+    const uint32_t c = cnt[f];
+    if (!c) continue;
     const int4 r = rect[f];
-    for (int j = r.y; j <= r.w; ++j)
-      for (int i = r.x; i <= r.z; ++i) {
-        const uint32_t z = (uint32_t)(j * zcx + i);
-        vals[zoff[z] + atomicAdd(zfill + z, 1u)] = f;
+    int i = r.x, j = r.y;
+    // four zones at a time: their atomics are in flight together before the stores
+    for (uint32_t q = 0; q < c; q += 4) {
+      uint32_t z[4], pos[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        z[k] = q + k < c ? (uint32_t)(j * zcx + i) : ~0u;
+        if (++i > r.z) { i = r.x; ++j; }
       }
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (z[k] != ~0u) pos[k] = zoff[z[k]] + atomicAdd(zfill + z[k], 1u);
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (z[k] != ~0u) vals[pos[k]] = f;
+    }
   }
 }
 
