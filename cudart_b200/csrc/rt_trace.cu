@@ -753,24 +753,25 @@ __global__ __launch_bounds__(128) void k_batch_trace_persistent(TraceArgs A, Bat
   }
 }
 
-// Sort key of a ray: direction octant (3 bits) above a 29-bit Morton code of
-// its origin in the given box; inactive rays (tmax <= 0) sort last.
+// Sort key of a ray: direction octant (3 bits) above a 21-bit Morton code of
+// its origin in the given box (128 cells per axis); inactive rays (tmax <= 0)
+// sort last.
 __global__ __launch_bounds__(256) void k_ray_keys(const float4* __restrict__ orig, const float4* __restrict__ dir,
                                                  const float* __restrict__ tmax, uint32_t count, float3 lo, float3 scale,
                                                  uint32_t* __restrict__ keys, uint32_t* __restrict__ idx) {
   for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < count; r += gridDim.x * blockDim.x) {
     idx[r] = r;
-    if (tmax && !(__ldg(tmax + r) > 0.0f)) { keys[r] = 0xFFFFFFFFu; continue; }
+    if (tmax && !(__ldg(tmax + r) > 0.0f)) { keys[r] = 0xFFFFFFu; continue; }
     const float4 o = ldg4(orig + r), d = ldg4(dir + r);
     const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
     uint32_t q[3];
     const float c[3] = {(o.x - lo.x) * scale.x, (o.y - lo.y) * scale.y, (o.z - lo.z) * scale.z};
 #pragma unroll
-    for (int a = 0; a < 3; ++a) q[a] = min(__float2uint_rz(fmaxf(c[a], 0.0f)), 511u);
+    for (int a = 0; a < 3; ++a) q[a] = min(__float2uint_rz(fmaxf(c[a], 0.0f)), 511u) >> 2;  // 7 bits per axis
     uint32_t m = 0;
 #pragma unroll
-    for (int b = 0; b < 9; ++b) m |= ((q[0] >> b) & 1u) << (3 * b + 2) | ((q[1] >> b) & 1u) << (3 * b + 1) | ((q[2] >> b) & 1u) << (3 * b);
-    keys[r] = (oct << 27) | m;  // 3 + 27 bits
+    for (int b = 0; b < 7; ++b) m |= ((q[0] >> b) & 1u) << (3 * b + 2) | ((q[1] >> b) & 1u) << (3 * b + 1) | ((q[2] >> b) & 1u) << (3 * b);
+    keys[r] = (oct << 21) | m;  // 3 + 21 bits: three radix passes (a finer code sorts slower than it gains)
   }
 }
 
@@ -1012,7 +1013,7 @@ extern "C" rt_status rt_ray_order(const float* orig, const float* dir, const flo
   k_ray_keys<<<blocks, 256, 0, st>>>((const float4*)orig, (const float4*)dir, tmax, count, lo, sc, keys, order);
   note_launch();
   RT_CHECK_LAUNCH();
-  return radix_sort_pairs(keys, order, count, 0, 32, 0, sort_scratch, radix_scratch_bytes(count), st, nullptr);
+  return radix_sort_pairs(keys, order, count, 0, 24, 0, sort_scratch, radix_scratch_bytes(count), st, nullptr);
 }
 
 extern "C" rt_status rt_primary_rays(const rt_camera* cam, uint32_t w, uint32_t h, float* orig, float* dir, rt_stream stream) {
