@@ -1087,7 +1087,7 @@ __global__ __launch_bounds__(256) void k_batch_propagate(BatchArgs B) {
     }
     const uint32_t m = lo, F = B.foff[m], n = B.foff[m + 1] - F, nb = node_base(F, m);
     const uint32_t* h = B.hdr + 16 * m;
-    if (h[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) continue;
+    if (n == 0 || (h[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY))) continue;
     const uint32_t lp = p - nb, cap = 2 * n - 1;
     if (lp >= h[2] || lp >= cap) continue;
     uint32_t* nodes = B.nodes + 8 * (size_t)nb;

@@ -115,7 +115,8 @@ rt_status rt_lbvh_build(const rt_build_desc* desc, rt_stream stream);
 /* Batched build of M meshes in one set of launches (no per-mesh host work).
  * Faces and vertices of all meshes are concatenated; face_offsets[m] and
  * vertex_offsets[m] (DEVICE arrays of M + 1 entries) delimit mesh m, and its
- * faces index its own vertices from 0. Every per-mesh output equals what
+ * faces index its own vertices from 0; every mesh has at least one face.
+ * Every per-mesh output equals what
  * rt_lbvh_build gives for that mesh alone (same bits), stored at fixed
  * offsets derived from F_m = face_offsets[m]:
  *   faces_out, boxes, codes, tris, indices  at position F_m (indices hold mesh-local face ids),
