@@ -823,6 +823,56 @@ __global__ __launch_bounds__(256) void k_adam(float* __restrict__ p, const float
 
 // The same update over 32 x 32 tiles (block 32 x 8), with the BF16 transpose
 // staged through shared memory so that both copies are written coalesced.
+// The same update with four consecutive columns per thread (16-byte loads
+// and stores; rows, cols, the BF16 leading dimensions and the group rows are
+// multiples of 4 and the FP32 arrays 16-byte aligned): 256 threads per 32 x 32
+// tile, the transposed BF16 copy through shared memory, 4 rows per 8-byte store.
+__global__ __launch_bounds__(256) void k_adam_t4(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                                                 float* __restrict__ v, uint32_t rows, uint32_t cols, float lr, float b1, float b2,
+                                                 float eps, float c1, float c2, __nv_bfloat16* __restrict__ out16, uint32_t ld16,
+                                                 __nv_bfloat16* __restrict__ out16t, uint32_t ld16t, uint32_t group_rows) {
+  __shared__ __nv_bfloat16 tile[32][40];
+  const uint32_t c0 = blockIdx.x * 32, r0 = blockIdx.y * 32, t = threadIdx.x;
+  {
+    const uint32_t lr_ = t >> 3, lc = (t & 7u) * 4u, r = r0 + lr_, c = c0 + lc;
+    if (r < rows && c < cols) {
+      const size_t i = (size_t)r * cols + c;
+      const float4 gi = *(const float4*)(g + i);
+      float4 mi = *(const float4*)(m + i), vi = *(const float4*)(v + i), pi = *(const float4*)(p + i);
+      const float gv[4] = {gi.x, gi.y, gi.z, gi.w};
+      float mv[4] = {mi.x, mi.y, mi.z, mi.w}, vv[4] = {vi.x, vi.y, vi.z, vi.w}, pv[4] = {pi.x, pi.y, pi.z, pi.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        // adam_update's arithmetic, element by element
+        mv[k] = b1 * mv[k] + (1.0f - b1) * gv[k];
+        vv[k] = b2 * vv[k] + (1.0f - b2) * gv[k] * gv[k];
+        pv[k] = pv[k] - lr * (mv[k] * c1) / (sqrtf(vv[k] * c2) + eps);
+      }
+      *(float4*)(m + i) = make_float4(mv[0], mv[1], mv[2], mv[3]);
+      *(float4*)(v + i) = make_float4(vv[0], vv[1], vv[2], vv[3]);
+      *(float4*)(p + i) = make_float4(pv[0], pv[1], pv[2], pv[3]);
+      __nv_bfloat16 h[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        h[k] = __float2bfloat16_rn(pv[k]);
+        tile[lr_][lc + k] = h[k];
+      }
+      if (out16) *(uint2*)(out16 + (size_t)r * ld16 + c) = *(const uint2*)h;
+    }
+  }
+  __syncthreads();
+  {
+    const uint32_t lc = t >> 3, lr_ = (t & 7u) * 4u, c = c0 + lc, r = r0 + lr_;
+    if (r < rows && c < cols) {
+      __nv_bfloat16 h[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) h[k] = tile[lr_ + k][lc];
+      const uint32_t q = r / group_rows;
+      *(uint2*)(out16t + ((size_t)q * cols + c) * ld16t + (r - q * group_rows)) = *(const uint2*)h;
+    }
+  }
+}
+
 __global__ __launch_bounds__(256) void k_adam_t(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
                                                 float* __restrict__ v, uint32_t rows, uint32_t cols, float lr, float b1, float b2,
                                                 float eps, float c1, float c2, __nv_bfloat16* __restrict__ out16, uint32_t ld16,
@@ -1527,7 +1577,14 @@ extern "C" rt_status rt_adam_step(const rt_adam_desc* d, rt_stream stream) {
   const float c1 = 1.0f / (1.0f - powf(d->beta1, (float)d->step));
   const float c2 = 1.0f / (1.0f - powf(d->beta2, (float)d->step));
   const uint32_t gr = G > 1 ? d->rows / G : (d->rows ? d->rows : 1u);
-  if (d->out_bf16_t) {
+  const bool by4 = d->rows % 4 == 0 && d->cols % 4 == 0 && gr % 4 == 0 && d->ld_bf16_t % 4 == 0 && (!d->out_bf16 || d->ld_bf16 % 4 == 0) &&
+                   aligned16(d->param) && aligned16(d->grad) && aligned16(d->m) && aligned16(d->v) &&
+                   ((uintptr_t)d->out_bf16 & 7u) == 0 && ((uintptr_t)d->out_bf16_t & 7u) == 0;
+  if (d->out_bf16_t && by4) {
+    k_adam_t4<<<dim3((d->cols + 31) / 32, (d->rows + 31) / 32), 256, 0, (cudaStream_t)stream>>>(
+        d->param, d->grad, d->m, d->v, d->rows, d->cols, d->lr, d->beta1, d->beta2, d->eps, c1, c2, (__nv_bfloat16*)d->out_bf16,
+        d->ld_bf16, (__nv_bfloat16*)d->out_bf16_t, d->ld_bf16_t, gr);
+  } else if (d->out_bf16_t) {
     k_adam_t<<<dim3((d->cols + 31) / 32, (d->rows + 31) / 32), dim3(32, 8), 0, (cudaStream_t)stream>>>(
         d->param, d->grad, d->m, d->v, d->rows, d->cols, d->lr, d->beta1, d->beta2, d->eps, c1, c2, (__nv_bfloat16*)d->out_bf16,
         d->ld_bf16, (__nv_bfloat16*)d->out_bf16_t, d->ld_bf16_t, gr);
