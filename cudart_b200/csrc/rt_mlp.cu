@@ -124,23 +124,25 @@ __device__ __forceinline__ void epilogue16(const GemmEpi& E, uint32_t g, uint32_
 
 // ----------------------------------------------------------------------------
 // Generic GEMM: grid (n / bn, m / 128, groups), 128 threads. Warp 0 lane 0 loads
-// (TMA), warp 1 lane 0 issues the MMAs, then all four warps drain TMEM.
+// (TMA) through a ring of `stages` stages (no more than the K chunks, so that a
+// short-K GEMM leaves room for more CTAs per SM), warp 1 lane 0 issues the
+// MMAs, then all four warps drain TMEM.
 // ----------------------------------------------------------------------------
 __global__ void __launch_bounds__(128, 1)
     k_gemm_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmEpi E, uint32_t bn,
-              uint32_t tmem_cols, uint32_t num_k, uint32_t* err) {
+              uint32_t tmem_cols, uint32_t num_k, uint32_t stages, uint32_t* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t tile_b = bn * 128u;
   uint8_t* sA = smem;
-  uint8_t* sB = smem + kStages * kTileA;
-  uint64_t* full = (uint64_t*)(sB + kStages * tile_b);
-  uint64_t* empty = full + kStages;
-  uint64_t* done = empty + kStages;
+  uint8_t* sB = smem + stages * kTileA;
+  uint64_t* full = (uint64_t*)(sB + stages * tile_b);
+  uint64_t* empty = full + stages;
+  uint64_t* done = empty + stages;
   uint32_t* tmem_slot = (uint32_t*)(done + 1);
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   if (threadIdx.x == 0) {
-    for (uint32_t s = 0; s < kStages; ++s) {
+    for (uint32_t s = 0; s < stages; ++s) {
       mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
     }
@@ -165,19 +167,19 @@ __global__ void __launch_bounds__(128, 1)
     const int32_t b0 = (int32_t)(g * E.gn) + n0;
     uint32_t kc = 0;
     for (; kc < num_k; ++kc) {
-      const uint32_t s = kc % kStages;
-      if (kc >= kStages && !mbar_wait(empty + s, ((kc / kStages) - 1u) & 1u, err)) break;
+      const uint32_t s = kc % stages;
+      if (kc >= stages && !mbar_wait(empty + s, ((kc / stages) - 1u) & 1u, err)) break;
       mbar_arrive_expect_tx(full + s, kTileA + tile_b);
       tma_load_2d(sA + s * kTileA, &ta, (int32_t)(kc * kBK), m0, full + s);
       tma_load_2d(sB + s * tile_b, &tb, (int32_t)(kc * kBK), b0, full + s);
     }
     // the latest load of each stage has landed before the CTA may exit
-    for (uint32_t j = kc > kStages ? kc - kStages : 0u; j < kc; ++j) mbar_wait(full + j % kStages, (j / kStages) & 1u, err);
+    for (uint32_t j = kc > stages ? kc - stages : 0u; j < kc; ++j) mbar_wait(full + j % stages, (j / stages) & 1u, err);
   } else if (warp == 1 && lane == 0) {
     const uint32_t idesc = idesc_bf16_f32(kBM, bn);
     for (uint32_t kc = 0; kc < num_k; ++kc) {
-      const uint32_t s = kc % kStages;
-      if (!mbar_wait(full + s, (kc / kStages) & 1u, err)) break;
+      const uint32_t s = kc % stages;
+      if (!mbar_wait(full + s, (kc / stages) & 1u, err)) break;
       tc_fence_after();
       const uint32_t a = smem_u32(sA + s * kTileA), b = smem_u32(sB + s * tile_b);
 #pragma unroll
@@ -1345,7 +1347,7 @@ uint32_t pow2_cols(uint32_t n) {
   return c;
 }
 
-size_t gemm_smem(uint32_t bn) { return 1024 + kStages * (kTileA + (size_t)bn * 128u) + 256; }
+size_t gemm_smem(uint32_t bn, uint32_t stages = kStages) { return 1024 + stages * (kTileA + (size_t)bn * 128u) + 256; }
 size_t argmax_smem(uint32_t num_k, uint32_t n) {
   return 1024 + num_k * (size_t)kTileA + kStages * (size_t)kArgTileB + (size_t)n * 4 + kBM * sizeof(Top2) + 256;
 }
@@ -1380,11 +1382,12 @@ extern "C" rt_status rt_gemm_bf16(const rt_gemm_desc* d, rt_stream stream) {
   E.gm = d->m; E.gn = d->n;
   E.c32_v8 = (d->c_f32 && d->ldc_f32 % 8 == 0 && ((uintptr_t)d->c_f32 & 31u) == 0) ? 1u : 0u;
   E.c16_v8 = (d->c_bf16 && d->ldc_bf16 % 16 == 0 && ((uintptr_t)d->c_bf16 & 31u) == 0) ? 1u : 0u;
-  const size_t smem = gemm_smem(bn);
+  const uint32_t num_k = d->k / kBK, stages = num_k < kStages ? num_k : kStages;
+  const size_t smem = gemm_smem(bn, stages);
   static std::once_flag once;
   std::call_once(once, [] { cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem(256)); });
   dim3 grid(d->n / bn, d->m / kBM, G);
-  k_gemm_tc<<<grid, 128, smem, (cudaStream_t)stream>>>(ta, tb, E, bn, pow2_cols(bn), d->k / kBK, d->error_word);
+  k_gemm_tc<<<grid, 128, smem, (cudaStream_t)stream>>>(ta, tb, E, bn, pow2_cols(bn), num_k, stages, d->error_word);
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
