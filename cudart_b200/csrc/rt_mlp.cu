@@ -721,6 +721,48 @@ __global__ __launch_bounds__(256) void k_transpose_bf16(const __nv_bfloat16* __r
 // out[g cols + c] = sum of in[g rows + r][c] over r < rows, FP32, in a fixed
 // order: block (32, 8) per 32 columns of one group (blockIdx.y); thread y sums
 // rows y, y + 8, ... and the eight partial sums are added in order y = 0..7.
+// The same sums with two columns per thread (4-byte loads, whole 128-byte
+// rows per warp) and four rows in flight; each column's summation order is
+// unchanged (row y, y + 8, ... per thread, then the eight partials in order),
+// so the results are the same bits. Needs even cols and ld.
+__global__ __launch_bounds__(256) void k_colsum2_bf16(const __nv_bfloat16* __restrict__ in, uint32_t rows, uint32_t cols, uint32_t ld,
+                                                      float* __restrict__ out) {
+  __shared__ float2 part[8][33];
+  const uint32_t c = (blockIdx.x * 32 + threadIdx.x) * 2, g = blockIdx.y;
+  const __nv_bfloat162* p = (const __nv_bfloat162*)(in + (size_t)g * rows * ld + c);
+  const uint32_t ld2 = ld / 2;
+  float s0 = 0.0f, s1 = 0.0f;
+  if (c < cols) {
+    uint32_t r = threadIdx.y;
+    for (; r + 24 < rows; r += 32) {
+      __nv_bfloat162 h[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) h[k] = p[(size_t)(r + 8 * k) * ld2];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        s0 += __low2float(h[k]);
+        s1 += __high2float(h[k]);
+      }
+    }
+    for (; r < rows; r += 8) {
+      const __nv_bfloat162 h = p[(size_t)r * ld2];
+      s0 += __low2float(h);
+      s1 += __high2float(h);
+    }
+  }
+  part[threadIdx.y][threadIdx.x] = make_float2(s0, s1);
+  __syncthreads();
+  if (threadIdx.y == 0 && c < cols) {
+    float2 t = part[0][threadIdx.x];
+#pragma unroll
+    for (int y = 1; y < 8; ++y) {
+      t.x += part[y][threadIdx.x].x;
+      t.y += part[y][threadIdx.x].y;
+    }
+    *(float2*)(out + (size_t)g * cols + c) = t;
+  }
+}
+
 __global__ __launch_bounds__(256) void k_colsum_bf16(const __nv_bfloat16* __restrict__ in, uint32_t rows, uint32_t cols, uint32_t ld,
                                                      float* __restrict__ out) {
   __shared__ float part[8][33];
@@ -1534,7 +1576,10 @@ extern "C" rt_status rt_colsum_bf16_grouped(const void* in, uint32_t groups, uin
   if (!in || !out || ld < cols || groups == 0 || groups > 65535u) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   if (cols == 0) return RT_OK;
-  k_colsum_bf16<<<dim3((cols + 31) / 32, groups), dim3(32, 8), 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)in, rows, cols, ld, out);
+  if (cols % 2 == 0 && ld % 2 == 0 && ((uintptr_t)in & 3u) == 0 && ((uintptr_t)out & 7u) == 0)
+    k_colsum2_bf16<<<dim3((cols + 63) / 64, groups), dim3(32, 8), 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)in, rows, cols, ld, out);
+  else
+    k_colsum_bf16<<<dim3((cols + 31) / 32, groups), dim3(32, 8), 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)in, rows, cols, ld, out);
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
