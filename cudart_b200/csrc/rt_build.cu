@@ -97,25 +97,27 @@ __global__ __launch_bounds__(256) void k_hitbox_partial(const float4* __restrict
   }
 }
 
-__global__ void k_hitbox_final(const float4* __restrict__ partial, uint32_t parts, float4* __restrict__ hit) {
-  // one warp: strided accumulation, then a shuffle reduction
+__global__ __launch_bounds__(256) void k_hitbox_final(const float4* __restrict__ partial, uint32_t parts, float4* __restrict__ hit) {
+  // one block: strided accumulation, then a shared-memory tree
   float4 mn = make_float4(kHuge, kHuge, kHuge, kHuge), mx = make_float4(-kHuge, -kHuge, -kHuge, -kHuge);
-  for (uint32_t i = threadIdx.x; i < parts; i += 32) {
+  for (uint32_t i = threadIdx.x; i < parts; i += blockDim.x) {
     mn = f4min(mn, partial[2 * i]);
     mx = f4max(mx, partial[2 * i + 1]);
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    float4 omn = make_float4(__shfl_xor_sync(0xffffffffu, mn.x, o), __shfl_xor_sync(0xffffffffu, mn.y, o),
-                             __shfl_xor_sync(0xffffffffu, mn.z, o), __shfl_xor_sync(0xffffffffu, mn.w, o));
-    float4 omx = make_float4(__shfl_xor_sync(0xffffffffu, mx.x, o), __shfl_xor_sync(0xffffffffu, mx.y, o),
-                             __shfl_xor_sync(0xffffffffu, mx.z, o), __shfl_xor_sync(0xffffffffu, mx.w, o));
-    mn = f4min(mn, omn);
-    mx = f4max(mx, omx);
+  __shared__ float4 s_mn[256], s_mx[256];
+  s_mn[threadIdx.x] = mn;
+  s_mx[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      s_mn[threadIdx.x] = f4min(s_mn[threadIdx.x], s_mn[threadIdx.x + o]);
+      s_mx[threadIdx.x] = f4max(s_mx[threadIdx.x], s_mx[threadIdx.x + o]);
+    }
+    __syncthreads();
   }
   if (threadIdx.x == 0) {
-    hit[0] = mn;
-    hit[1] = mx;
+    hit[0] = s_mn[0];
+    hit[1] = s_mx[0];
   }
 }
 
@@ -737,7 +739,7 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
     note_launch();
   } else {
     k_hitbox_partial<<<kHitParts, 256, 0, st>>>((const float4*)d->vertices, d->vertex_count, L.partial);
-    k_hitbox_final<<<1, 32, 0, st>>>(L.partial, kHitParts, L.hit);
+    k_hitbox_final<<<1, 256, 0, st>>>(L.partial, kHitParts, L.hit);
     note_launch(2);
   }
   RT_CHECK_LAUNCH();
