@@ -1,19 +1,30 @@
-"""Benchmark: LBVH build + closest-hit traversal on the incoherent 1M-triangle scene.
+"""Benchmark: LBVH build + closest-hit traversal, headline on the instanced-frame workload.
 
-Workload (one "step"): a 2^20-triangle soup in the unit cube (vertex noise
-sigma 0.01), LBVH build (tree depth 12, complete), 1920 x 1080 primary rays,
-closest-hit trace, one cosine-weighted diffuse bounce per hit, closest-hit trace
-of the bounces. Build and trace are timed separately with CUDA events on the
-launching stream; `value` is closest-hit Mrays/s over both trace passes
-(primary + active bounce rays), `build` carries LBVH Mtri/s.
+Headline workload (one "step" = one frame of the plain path): 64 deformed
+instances of the 4,022,242-triangle terrain + soup scene at 1/16 size
+(251,518 triangles each, 16,097,152 per frame). Every frame each instance's
+vertices move by fresh N(0, 0.002^2) noise (input generation, outside the
+timed events), then the timed frame runs: one batched LBVH build of all 64
+instances, 64 pinhole cameras' primary rays (a 3840 x 2160 frame at 4 samples
+per pixel, 480 x 270 tiles rendered at 960 x 540 each), the batched
+closest-hit trace, one cosine-weighted diffuse bounce per hit and the batched
+trace of the bounces. `value` = closest-hit rays (primaries + active bounces)
+per frame / frame time, in Mrays/s; `build` = the frame's LBVH build in Mtri/s;
+`nn_over_plain` = the learned proposal path (grouped per-instance networks +
+seeded traversal) against the plain traversal on the same rays, hits compared
+bit for bit.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+Output: one JSON line per secondary workload ({"leg": ...}: the 128^2 terrain,
+the 2^20-face soup, the 16M-face build, the 1024-mesh batch, the 4M-triangle
+learned scene, SAH / Hybrid trees, the rasteriser), then the headline line last.
 With N > 1 (torchrun, one rank per GPU) every rank runs its own replica of the
-workload (weak scaling); the time is the max over ranks.
+workload (weak scaling); times are the max over ranks.
 `--impl reference` times the reference algorithm's CPU implementation (the
-oracle restatement; the reference's own GPU code cannot be built with CUDA 12)
-on the host cores, on rank 0 only.
+oracle restatement, checked bit-exact against the reference's own code; the
+reference's GPU code cannot be built with CUDA 12) on the host cores, on rank 0
+only, on a bounded sample of the same frame workload.
 """
 from __future__ import annotations
 
@@ -31,33 +42,32 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "closest-hit Mrays/s (plain vs NN-proposal, bit-exact) and LBVH build Mtri/s"
-WORKLOAD = "soup 2^20 triangles, 1920x1080 primary rays + 1 diffuse bounce per hit"
+WORKLOAD_SHORT = "c4 instanced frames: 64 x 251,518-tri instances rebuilt per frame, 3840x2160 at 4 spp + 1 bounce"
+WORKLOAD = ("instanced frames: 64 deformed instances of the terrain + soup scene at 1/16 size (16,097,152 triangles rebuilt per "
+            "frame), 3840x2160 at 4 spp over 64 cameras (33,177,600 primary rays) + 1 diffuse bounce per hit")
 SEED_MESH = 1
 SEED_BOUNCE = 1234
 L2_FLUSH_BYTES = 512 << 20  # > 126 MB L2
+C4_SCALE, C4_W, C4_H = 1 / 16, 960, 540
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--faces", type=int, default=1 << 20)
-    ap.add_argument("--build16m", type=int, default=1, help="also time the LBVH build alone on a 2^24-face soup")
-    ap.add_argument("--batch", type=int, default=1, help="also time the batched workload (1024 meshes, CUDA graph)")
-    ap.add_argument("--learned", type=int, default=1, help="also train and time the learned subtree proposal (4M-triangle scene)")
-    ap.add_argument("--sah", type=int, default=1, help="also time the SAH and Hybrid builds and tracing through their trees")
-    ap.add_argument("--raster", type=int, default=1, help="also time the rasteriser on the same frame")
-    ap.add_argument("--learned-scale", type=float, default=1.0, help="triangle-count scale of the learned-proposal scene")
-    ap.add_argument("--instanced", type=int, default=1,
-                    help="also time the instanced workload: 64 deformed copies of the learned scene rebuilt every frame, "
-                         "per-instance networks fine-tuned on the previous frame")
-    ap.add_argument("--instanced-frames", type=int, default=16)
-    ap.add_argument("--instanced-count", type=int, default=64)
+    ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--nn-frames", type=int, default=3, help="frames of the learned path (fine-tuning + proposals) timed beside plain")
+    ap.add_argument("--legs", default="c0,c1,build16m,c2,c3,sah,raster",
+                    help="secondary workloads printed before the headline line (comma list, or 'none')")
     return ap.parse_args()
+
+
+def emit(obj):
+    print(json.dumps(obj, separators=(",", ":")), flush=True)
 
 
 def capture_graphs(stages):
@@ -95,14 +105,45 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic(kernel: str):
-    """DRAM bytes (read + write) of one primary-ray trace launch of this workload,
-    from the committed ncu summary for that kernel (profiles/trace_traffic.json)."""
+def load_traffic(key: str):
+    """DRAM bytes (read + write) per launch of one kernel on one workload, from the committed ncu capture
+    summary profiles/trace_traffic.json (a figure of an earlier capture, not of this run)."""
     p = os.path.join(ROOT, "profiles", "trace_traffic.json")
     if os.path.exists(p):
         with open(p) as f:
-            return json.load(f).get(kernel)
+            return json.load(f).get(key)
     return None
+
+
+def max_over_ranks(values, world, dev):
+    if world == 1:
+        return values
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def trace_roofline(kernel, launch, model_bytes, ms, ray_slots, peak, peak_kind, traffic_key):
+    """Roofline of one trace launch. The bound that applies is HBM; `frac` is the DRAM fraction: ncu's DRAM
+    bytes per launch (a committed capture of this kernel on this workload) over the live launch time. The
+    per-ray model bytes (32 B ray + 16 B hit per slot, 32 B per box record read, 48 B per triangle tested)
+    include every node and triangle read that L1 / L2 serve; they are reported as `model_frac`, not as HBM."""
+    t = load_traffic(traffic_key)
+    traffic = None if t is None else int(t["dram_bytes_per_launch"])
+    model_gbs = model_bytes / (ms * 1e-3) / 1e9
+    out = {"bound": "hbm", "kernel": kernel, "launch": launch, "ray_slots": ray_slots, "launch_ms": round(ms, 3), "unit": "GB/s",
+           "peak": peak, "peak_kind": peak_kind, "traffic": traffic,
+           "model_bytes": int(model_bytes), "model_gbs": round(model_gbs, 1), "model_frac": round(model_gbs / peak, 4),
+           "model_note": "per-ray bytes incl. L1/L2-served node and triangle reads (not DRAM)"}
+    if traffic is not None:
+        a = traffic / (ms * 1e-3) / 1e9
+        out.update(achieved=round(a, 1), frac=round(a / peak, 4), traffic_source=t.get("source", ""), l1_frac=t.get("l1tex_frac"),
+                   limiter=t.get("limiter"))
+    else:
+        out.update(achieved=None, frac=None, traffic_source="no capture of this kernel on this workload")
+    return out
 
 
 class ClockSampler:
@@ -173,435 +214,552 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------
-# our arm
+# headline: instanced frames (plain path timed per frame; learned path beside it)
 # ----------------------------------------------------------------------------
-def run_ours(args, rank, world, local_rank):
+def batch_kernel(sched):
+    if sched.get("coop"):
+        return "k_batch_trace_coop"
+    return "k_batch_trace_persistent" if sched.get("persistent") else "k_batch_trace"
+
+
+def run_headline(args, rank, world, local_rank):
     import torch
 
-    from cudart_b200 import _abi, core, scenes
+    from cudart_b200 import _abi, core
+    from cudart_b200.instances import InstancedFrames
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     if not core.device_check():
         raise RuntimeError("no CUDA device: the CUDA path has no CPU fallback")
-    mesh, cam = scenes.soup_1m_scene(n=args.faces, seed=SEED_MESH)
-    N = mesh.face_count
-    W, H = cam.width, cam.height
-    R = W * H
-    v = torch.from_numpy(mesh.vertices).to(dev)
-    f = torch.from_numpy(mesh.faces.view(np.int32)).to(dev)
-    camera = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
+    w = InstancedFrames(args.instances, C4_SCALE, C4_W, C4_H, device=dev)
+    w.displace(0)
+    w.build()
+    w.make_slots()
+    sched, tim = w.tune()  # untimed; results never depend on the schedule
+    plain = w.trace_plain()
+    torch.cuda.synchronize()
+    R = w.ray_count
+    F = w.face_count
     stream = torch.cuda.current_stream()
-
-    tree = core.build_lbvh(v, f)
-    rays = core.primary_rays(camera, W, H)
-    hits1 = core.trace(tree, rays[0], rays[1])
-    bounce = core.bounce_rays(tree.tris, rays[0], rays[1], hits1["id"], hits1["t"], SEED_BOUNCE)
-    hits2 = core.trace(tree, bounce[0], bounce[1], tmax=bounce[2])
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    # autotune the traversal schedule on this workload's rays (untimed); results never depend on it
-    from cudart_b200 import tune
-    sched1, tim1 = tune.tune_trace(tree, rays[0], rays[1], image_width=W, key=f"soup{N}-primary", use_cache=False)
-    sched2, tim2 = tune.tune_trace(tree, bounce[0], bounce[1], tmax=bounce[2], image_width=W, key=f"soup{N}-bounce", use_cache=False)
 
-    # each stage of a step is captured once as a CUDA graph and replayed (one launch per stage), with the
-    # timing events recorded between the replays
-    stages = [lambda: core.build_lbvh(v, f, out=tree),
-              lambda: core.primary_rays(camera, W, H, out=rays),
-              lambda: core.trace(tree, rays[0], rays[1], out=hits1, schedule=sched1),
-              lambda: core.bounce_rays(tree.tris, rays[0], rays[1], hits1["id"], hits1["t"], SEED_BOUNCE, out=bounce),
-              lambda: core.trace(tree, bounce[0], bounce[1], tmax=bounce[2], out=hits2, schedule=sched2)]
+    def trace1():
+        core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, out=plain["h1"], schedule=sched)
+
+    def trace2():
+        b = plain["b"]
+        core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], out=plain["h2"], schedule=sched)
+
+    stages = [lambda: w.build(), w.primary_rays, trace1, lambda: w.bounce(plain["h1"], out=plain["b"]), trace2]
     graphs, kernels_per_step = capture_graphs(stages)
+    active = torch.zeros(1, dtype=torch.int64, device=dev)
 
-    def step(ev):
+    def step(frame, timed_list=None):
+        w.displace(frame)  # the frame's input (outside the events)
+        flush.zero_()  # L2 flush between frames (outside the events)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
         ev[0].record(stream)
         for i, g in enumerate(graphs):
             g.replay()
             ev[i + 1].record(stream)
+        if timed_list is not None:
+            timed_list.append(ev)
+            active.add_((plain["b"][2] > 0).sum())  # rays of the frame (counted after its last event)
 
-    def new_events():
-        return [torch.cuda.Event(enable_timing=True) for _ in range(6)]
-
-    for _ in range(args.warmup):
-        flush.zero_()
-        step(new_events())
+    for k in range(args.warmup):
+        step(1 + k)
     torch.cuda.synchronize()
-    info = tree.info_host()
-    n_primary_hits = int((hits1["id"] >= 0).sum().item())
-    n_active_bounce = int((bounce[2] > 0).sum().item())
-    rays_per_step = R + n_active_bounce
-
-    # counted pass (untimed): per-ray node visits and triangle tests of both trace launches
-    cnt1 = core.trace(tree, rays[0], rays[1], counters=True)
-    cnt2 = core.trace(tree, bounce[0], bounce[1], tmax=bounce[2], counters=True)
-    torch.cuda.synchronize()
-    vis1, tst1 = int(cnt1["visits"].sum().item()), int(cnt1["tests"].sum().item())
-    vis = vis1 + int(cnt2["visits"].sum().item())
-    tst = tst1 + int(cnt2["tests"].sum().item())
-    same = torch.equal(cnt1["id"], hits1["id"]) and torch.equal(cnt2["id"], hits2["id"])
-    # algorithmic bytes: 32 B ray in + 16 B hit out per ray slot, 32 B per box record read, 48 B per triangle tested
-    primary_bytes = 48 * R + 32 * vis1 + 48 * tst1
-    bounce_bytes = 48 * R + 32 * (vis - vis1) + 48 * (tst - tst1)
-
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
-    launches0 = _abi.lib().rt_launch_count()
     evs = []
     sampler = ClockSampler(local_rank).start()
     with sampler as clk:
-        t_wall = time.perf_counter()
-        for _ in range(args.steps):
-            flush.zero_()  # L2 flush between timed steps (outside the event brackets)
-            ev = new_events()
-            step(ev)
-            evs.append(ev)
+        for k in range(args.steps):
+            step(1 + args.warmup + k, evs)
         torch.cuda.synchronize()
-        t_wall = time.perf_counter() - t_wall
-    # the kernels run inside graph replays, so the library's launch counter does not see them: count the
-    # kernels each step's graphs hold
-    launches = kernels_per_step * args.steps + (_abi.lib().rt_launch_count() - launches0)
-    build_ms = sum(e[0].elapsed_time(e[1]) for e in evs)
-    trace1_ms = sum(e[2].elapsed_time(e[3]) for e in evs)
-    trace2_ms = sum(e[4].elapsed_time(e[5]) for e in evs)
-    step_ms = sum(e[0].elapsed_time(e[5]) for e in evs)
-    trace_ms = trace1_ms + trace2_ms
-    times = torch.tensor([build_ms, trace_ms, step_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-        dist.barrier()
-    build_ms, trace_ms, step_ms = times.tolist()
-    K = args.steps
-    value = world * rays_per_step * K / (trace_ms * 1e-3) / 1e6
-    build_mtri = world * N * K / (build_ms * 1e-3) / 1e6
-    peak, peak_kind = load_peaks()
-    # roofline of the dominant kernel: the bounce launch (54% of a step's GPU time in the launch list of
-    # `python -m cudart_b200.profile_cases bench_step`), and of the primary launch beside it
-    def trace_kernel(sch):
-        if getattr(tree, "accel", None) is None:
-            return "k_trace"
-        if sch.get("coop"):
-            return "k_trace_coop_persistent" if sch.get("persistent") else "k_trace_coop"
-        return "k_trace_accel_persistent" if sch.get("persistent") else "k_trace_accel"
-
-    def roofline(bytes_, ms, kernel, what):
-        achieved = bytes_ / (ms * 1e-3) / 1e9  # GB/s of one GPU's launch
-        traffic = load_traffic(kernel)
-        return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "peak_kind": peak_kind, "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
-                "kernel": f"{kernel} ({what}, {R} ray slots)", "algorithmic_bytes_per_launch": bytes_, "launch_ms": round(ms, 4)}
-
-    roof_bounce = roofline(bounce_bytes, trace2_ms / K, trace_kernel(sched2), "bounce-ray launch")
-    roof_primary = roofline(primary_bytes, trace1_ms / K, trace_kernel(sched1), "primary-ray launch")
-
-    result = {
-        "metric": METRIC,
-        "value": round(value, 3),
-        "unit": "Mrays/s",
-        "n_gpus": world,
-        "steps": K,
-        "warmup": args.warmup,
-        "ms_per_step": round(step_ms / K, 4),
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "f32",
-        "data": "synthetic (seeded numpy PCG64 soup; PCG32 bounce directions)",
-        "config": {"workload": WORKLOAD, "faces": N, "primary_rays": R, "bounce_rays_active": n_active_bounce,
-                   "rays_per_step": rays_per_step, "tree_depth": 12, "parallelism": f"replicas x{world}",
-                   "l2": "flushed between steps (512 MB write)"},
-        "build": {"value": round(build_mtri, 3), "unit": "Mtri/s", "ms": round(build_ms / K, 4), "node_count": info["node_count"],
-                  "leaf_count": info["leaf_count"], "real_depth": info["real_depth"]},
-        "trace": {"ms": round(trace_ms / K, 4), "primary_ms": round(trace1_ms / K, 4), "bounce_ms": round(trace2_ms / K, 4),
-                  "primary_hits": n_primary_hits, "mean_visits": round(vis / (2 * R), 3), "mean_tests": round(tst / (2 * R), 3),
-                  "counted_run_identical": bool(same), "schedule_primary": sched1, "schedule_bounce": sched2,
-                  "tuning_ms_primary": {json.dumps(k, sort_keys=True): round(v, 4) for k, v in tim1},
-                  "tuning_ms_bounce": {json.dumps(k, sort_keys=True): round(v, 4) for k, v in tim2}},
-        "roofline": roof_bounce,
-        "roofline_primary": roof_primary,
-        "gpu_launches": int(launches),
-        "graphs": f"each step = 5 CUDA graph replays (build, primary rays, trace, bounce rays, trace) holding {kernels_per_step} kernels",
-        "wall_s_timed": round(t_wall, 3),
-    }
-    if args.build16m or args.batch:
-        del flush
-    if args.build16m:
-        result["build_16m"] = build_only(24, args, dev, world)
-    if args.batch:
-        result["batch_c2"] = batched(args, dev, world)
-    if args.sah:
-        result["sah"] = sah_leg(args, dev, world, mesh, camera, W, H, tree)
-    if args.raster:
-        result["raster"] = raster_leg(dev, world, cam, tree, v, W, H)
-    if args.learned:
-        result["nn_proposal_c3"] = learned(args, dev, world)
-    if args.instanced:
-        result["instanced_c4"] = instanced(args, dev, world)
-    clocks = clk.summary()
     sampler.stop()
+    K = args.steps
+    frame_ms = sum(e[0].elapsed_time(e[5]) for e in evs)
+    build_ms = sum(e[0].elapsed_time(e[1]) for e in evs)
+    rays_ms = sum(e[1].elapsed_time(e[2]) for e in evs)
+    t1_ms = sum(e[2].elapsed_time(e[3]) for e in evs)
+    t2_ms = sum(e[4].elapsed_time(e[5]) for e in evs)
+    frame_ms, build_ms, rays_ms, t1_ms, t2_ms = max_over_ranks([frame_ms, build_ms, rays_ms, t1_ms, t2_ms], world, dev)
+    rays_total = K * R + int(active.item())
+    value = world * rays_total / (frame_ms * 1e-3) / 1e6
+    info = w.tree.info.cpu().numpy()
+    nodes_total = int(info[:, 0].astype(np.int64).sum())
+    dev_errors = int((info[:, 7] != 0).sum())
+    hits1 = int((plain["h1"]["id"] >= 0).sum().item())
+    active_last = int((plain["b"][2] > 0).sum().item())
+
+    # counted launches (untimed) of the last frame's rays: box records read and triangles tested per ray
+    b = plain["b"]
+    c1 = core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, counters=True, schedule=sched)
+    c2 = core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], counters=True, schedule=sched)
+    torch.cuda.synchronize()
+    same = torch.equal(c1["id"], plain["h1"]["id"]) and torch.equal(c2["id"], plain["h2"]["id"])
+    m1 = 48 * R + 32 * int(c1["visits"].sum().item()) + 48 * int(c1["tests"].sum().item())
+    m2 = 48 * R + 32 * int(c2["visits"].sum().item()) + 48 * int(c2["tests"].sum().item())
+    del c1, c2
+    peak, peak_kind = load_peaks()
+    kname = batch_kernel(sched)
+    if t1_ms >= t2_ms:
+        roof = trace_roofline(kname, "primary", m1, t1_ms / K, R, peak, peak_kind, f"c4:{kname}:primary")
+    else:
+        roof = trace_roofline(kname, "bounce", m2, t2_ms / K, R, peak, peak_kind, f"c4:{kname}:bounce")
+    # build: algorithmic bytes per face = 16 face + 48 vertices + 32 box + 8 code/index + 64 sort + 4 split scan
+    # + 32 leaf gather + 36 reorder + 48 triangle stream, + 64 per node (write + child read)
+    build_bytes = F * (16 + 48 + 32 + 8 + 64 + 4 + 32 + 36 + 48) + 64 * nodes_total
+    bgbs = build_bytes / (build_ms / K * 1e-3) / 1e9
+    result = {
+        "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": round(frame_ms / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic, seeded",
+        "config": {"workload": WORKLOAD_SHORT, "faces": F, "primary_rays": R, "rays_per_step": round(rays_total / K),
+                   "l2": "flushed between frames; inputs > L2"},
+        "build": {"value": round(world * F * K / (build_ms * 1e-3) / 1e6, 1), "unit": "Mtri/s", "ms": round(build_ms / K, 3),
+                  "roofline": {"bound": "hbm", "achieved": round(bgbs, 1), "peak": peak, "unit": "GB/s", "frac": round(bgbs / peak, 4)}},
+        "trace": {"mrays_s": round(world * rays_total / ((t1_ms + t2_ms) * 1e-3) / 1e6, 1), "primary_ms": round(t1_ms / K, 3),
+                  "bounce_ms": round(t2_ms / K, 3)},
+        "roofline": {k: roof[k] for k in ("bound", "kernel", "launch", "launch_ms", "achieved", "peak", "unit", "frac", "traffic",
+                                          "model_frac", "l1_frac", "limiter")},
+        "gpu_launches": int(kernels_per_step * K),
+    }
+    clocks = clk.summary()
     result["clocks"] = {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
                         "samples": clocks["samples"]}
+    legs = {"c4_tuning": {"ms": {json.dumps(k, sort_keys=True): round(v, 3) for k, v in tim}},
+            "c4_detail": {"workload": WORKLOAD, "schedule": sched, "counted_identical": bool(same), "device_errors": dev_errors,
+                          "nodes": nodes_total, "build_bytes": int(build_bytes), "rays_ms": round(rays_ms / K, 3),
+                          "primary_hits_last": hits1, "active_bounces_last": active_last, "kernels_per_frame": kernels_per_step,
+                          "graphs": "5 CUDA graph replays per frame: build, primary rays, trace, bounce rays, trace",
+                          "roofline": roof}}
+    del graphs
+    # learned proposal on the same frames (fine-tuning, grouped proposals + seeded traversal), hits bit for bit
+    if args.nn_frames > 0:
+        legs["c4_learned"] = learned_frames(w, args, dev, world, plain, first_frame=1 + args.warmup + K)
+        nn = legs["c4_learned"]
+        result["nn_over_plain"] = nn["nn_over_plain"]
+        result["nn"] = {k: nn[k] for k in ("bit_exact", "proposal_accuracy", "oracle_seeded_over_plain")}
     if not args.no_e2e:
-        result["e2e"] = run_e2e(args, mesh, camera, W, H, dev, world, sched1, sched2)
+        e2e = run_e2e(w, args, dev, world, sched)
+        legs["c4_e2e"] = e2e
+        result["e2e"] = {k: e2e[k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step", "ms_per_step")}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(mesh, cam, budget_s=12.0)
-    return result
+        cb = cpu_baseline_c4(w.count, frame=0, steps=1, one_thread=True)
+        legs["c4_cpu_baseline"] = cb
+        result["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "value_1_thread")}
+        result["cpu_baseline"]["sample"] = f"1/{w.count} frame (1 instance built + all its rays), oracle port"
+    del flush
+    return result, legs
 
 
-def build_only(log2n, args, dev, world):
-    """LBVH build alone on a 2^log2n-face soup (the 16M-face build target), replayed from a CUDA graph, CUDA
-    events, L2 flushed between builds."""
+def learned_frames(w, args, dev, world, plain, first_frame):
+    """`nn_frames` frames of the learned path beside the plain one: each frame rebuilds, fine-tunes every
+    instance's network (200 grouped Adam steps of 1024 rays) on the previous frame's plain hits, then traces
+    the frame plain and through the grouped proposals + seeded traversal; all hits compared bit for bit. The
+    `oracle` figure seeds every ray with the slot its plain hit lies in: what a perfect proposal gives."""
     import torch
 
-    from cudart_b200 import core, scenes
+    from cudart_b200 import proposal
 
-    mesh = scenes.soup(1 << log2n, seed=7)
-    v = torch.from_numpy(mesh.vertices).to(dev)
-    f = torch.from_numpy(mesh.faces.view(np.int32)).to(dev)
-    del mesh
-    tree = core.build_lbvh(v, f)
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream()
-    (graph,), _ = capture_graphs([lambda: core.build_lbvh(v, f, out=tree)])
-    for _ in range(2):
-        graph.replay()
+    w.remember(plain)
+    learned = w.trace_learned()
     torch.cuda.synchronize()
-    ms = 0.0
-    reps = max(3, min(args.steps, 10))
-    for _ in range(reps):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        graph.replay()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms += e0.elapsed_time(e1)
-    info = tree.info_host()
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = t.item() / reps
-    n = 1 << log2n
-    return {"faces": n, "value": round(world * n / (ms * 1e-3) / 1e6, 2), "unit": "Mtri/s", "ms": round(ms, 4),
-            "node_count": info["node_count"], "reps": reps}
-
-
-def batched(args, dev, world, count=1024):
-    """1024 independent meshes (face counts log-uniform in [64, 65536], terrain or
-    soup by coin flip), each with side x side rays (side log-uniform in
-    [64, 512]) from its bounding sphere aimed uniformly inward. One batched
-    build (all meshes) and one batched trace (all rays), captured together in a
-    CUDA graph and replayed; CUDA events around each replay."""
-    import math
-
-    import torch
-
-    from cudart_b200 import core, scenes
-
-    meshes = scenes.batch_meshes(count, seed=3)
-    verts, faces, fo, vo = scenes.concat_batch(meshes)
-    rng = np.random.default_rng(11)
-    sides = np.exp(rng.uniform(math.log(64), math.log(512), count)).astype(np.int64)
-    counts = sides * sides
-    ro = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
-    centers, radii = [], []
-    for m in meshes:
-        v = m.vertices[:, :3].astype(np.float64)
-        c = 0.5 * (v.min(0) + v.max(0))
-        centers.append(c)
-        radii.append(max(float(np.linalg.norm(v - c, axis=1).max()), 1e-6) * 1.01)
-    R = int(ro[-1])
-    del meshes
-    V = torch.from_numpy(verts).to(dev)
-    Fc = torch.from_numpy(faces.view(np.int32)).to(dev)
-    mesh_of_ray = torch.repeat_interleave(torch.arange(count, device=dev), torch.from_numpy(counts).to(dev))
-    cen = torch.tensor(np.array(centers), dtype=torch.float64, device=dev)[mesh_of_ray]
-    rad = torch.tensor(radii, dtype=torch.float64, device=dev)[mesh_of_ray].unsqueeze(1)
-    g = torch.Generator(device=dev).manual_seed(5)
-    p = torch.randn((R, 3), generator=g, device=dev, dtype=torch.float64)
-    p = p / p.norm(dim=1, keepdim=True)
-    q = torch.randn((R, 3), generator=g, device=dev, dtype=torch.float64)
-    q = q / q.norm(dim=1, keepdim=True) * torch.rand((R, 1), generator=g, device=dev, dtype=torch.float64).pow(1.0 / 3.0)
-    orig = torch.zeros((R, 4), dtype=torch.float32, device=dev)
-    dirs = torch.zeros((R, 4), dtype=torch.float32, device=dev)
-    orig[:, :3] = (cen + rad * p).float()
-    dirs[:, :3] = ((cen + rad * q) - (cen + rad * p)).float()
-    del p, q, cen, rad, mesh_of_ray
-    roff = torch.tensor(ro.astype(np.int32), device=dev)
-    tree = core.batch_build(V, Fc, fo, vo)
-    from cudart_b200 import tune
-    sched, tim = tune.tune_batch_trace(tree, orig, dirs, roff, key=f"batch{count}", use_cache=False)  # untimed
-    hits = core.batch_trace(tree, orig, dirs, roff, schedule=sched)
+    ev = []
+    mism = torch.zeros(1, dtype=torch.int64, device=dev)
+    inprop = torch.zeros(2, dtype=torch.int64, device=dev)
+    for f in range(args.nn_frames):
+        w.displace(first_frame + f)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(7)]
+        w.build()
+        w.make_slots()
+        e[0].record()
+        w.fine_tune()
+        e[1].record()
+        w.trace_plain(out=plain)
+        e[2].record()
+        R = w.rays_per_instance
+        learned["p1"] = w.nets.propose(w.orig, w.dir, w.box, R, out=learned["p1"])
+        e[3].record()
+        proposal.batch_trace_seeded(w.tree, w.orig, w.dir, w.ray_offsets, learned["p1"], w.slots, in_proposal=True,
+                                    out=learned["h1"], schedule=w.schedule)
+        e[4].record()
+        b = plain["b"]  # the seeded hits equal the plain ones, so the bounces are the same rays
+        learned["p2"] = w.nets.propose(b[0], b[1], w.box, R, out=learned["p2"], tmax=b[2])
+        e[5].record()
+        proposal.batch_trace_seeded(w.tree, b[0], b[1], w.ray_offsets, learned["p2"], w.slots, tmax=b[2], in_proposal=True,
+                                    out=learned["h2"], schedule=w.schedule)
+        e[6].record()
+        for k in ("h1", "h2"):
+            mism += (plain[k]["id"] != learned[k]["id"]).sum() + (plain[k]["t"].view(torch.int32) != learned[k]["t"].view(torch.int32)).sum()
+            mism += (plain[k]["uv"].view(torch.int32) != learned[k]["uv"].view(torch.int32)).sum()
+            hit = plain[k]["id"] >= 0
+            inprop[0] += (learned[k]["in_proposal"].bool() & hit).sum()
+            inprop[1] += hit.sum()
+        w.remember(plain)
+        ev.append(e)
     torch.cuda.synchronize()
-    graph = torch.cuda.CUDAGraph()
-    cap = torch.cuda.Stream()
-    cap.wait_stream(torch.cuda.current_stream())
-    with torch.cuda.stream(cap):
-        core.batch_build(V, Fc, fo, vo, out=tree)
-        core.batch_trace(tree, orig, dirs, roff, out=hits, schedule=sched)
-        torch.cuda.synchronize()
-        with torch.cuda.graph(graph, stream=cap):
-            core.batch_build(V, Fc, fo, vo, out=tree)
-            core.batch_trace(tree, orig, dirs, roff, out=hits, schedule=sched)
-    torch.cuda.current_stream().wait_stream(cap)
+    n = args.nn_frames
+    tune_ms = sum(e[0].elapsed_time(e[1]) for e in ev) / n
+    plain_ms = sum(e[1].elapsed_time(e[2]) for e in ev) / n
+    mlp_ms = sum(e[2].elapsed_time(e[3]) + e[4].elapsed_time(e[5]) for e in ev) / n
+    seeded_ms = sum(e[3].elapsed_time(e[4]) + e[5].elapsed_time(e[6]) for e in ev) / n
+    # a perfect proposal (the slot of each ray's plain hit), seeded traversal only
+    l1, l2 = w.labels(plain)
     torch.cuda.synchronize()
-    reps = 3
-    for _ in range(2):
-        graph.replay()
+    o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    o0.record()
+    proposal.batch_trace_seeded(w.tree, w.orig, w.dir, w.ray_offsets, l1, w.slots, out=learned["h1"], schedule=w.schedule)
+    b = plain["b"]
+    proposal.batch_trace_seeded(w.tree, b[0], b[1], w.ray_offsets, l2, w.slots, tmax=b[2], out=learned["h2"], schedule=w.schedule)
+    o1.record()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(reps):
-        graph.replay()
-    e1.record()
-    torch.cuda.synchronize()
-    graph_ms = e0.elapsed_time(e1) / reps
-    # build and trace separately (plain launches) for the split
-    b0, b1, t1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-    b0.record()
-    core.batch_build(V, Fc, fo, vo, out=tree)
-    b1.record()
-    core.batch_trace(tree, orig, dirs, roff, out=hits, schedule=sched)
-    t1.record()
-    torch.cuda.synchronize()
-    build_ms, trace_ms = b0.elapsed_time(b1), b1.elapsed_time(t1)
-    info = tree.info.cpu().numpy()
-    hit_frac = float((hits["id"] >= 0).float().mean().item())
-    N = int(fo[-1])
-    res = {"meshes": count, "faces": N, "rays": R, "schedule": sched,
-           "tuning_ms": {json.dumps(k, sort_keys=True): round(v, 3) for k, v in tim}, "graph_ms_per_step": round(graph_ms, 4),
-           "graph_mrays_s": round(world * R / (graph_ms * 1e-3) / 1e6, 2), "build_ms": round(build_ms, 4),
-           "build_mtri_s": round(world * N / (build_ms * 1e-3) / 1e6, 2), "trace_ms": round(trace_ms, 4),
-           "trace_mrays_s": round(world * R / (trace_ms * 1e-3) / 1e6, 2), "hit_fraction": round(hit_frac, 4),
-           "device_errors": int((info[:, 7] != 0).sum()), "graph": "build + trace captured in one CUDA graph"}
-    del graph
-    return res
+    oracle_ms = o0.elapsed_time(o1)
+    plain_ms, mlp_ms, seeded_ms, tune_ms, oracle_ms = max_over_ranks([plain_ms, mlp_ms, seeded_ms, tune_ms, oracle_ms], world, dev)
+    return {"frames": n, "bit_exact": int(mism.item()) == 0,
+            "proposal_accuracy": round(int(inprop[0].item()) / max(1, int(inprop[1].item())), 4),
+            "finetune_ms": round(tune_ms, 2), "plain_ms": round(plain_ms, 3), "mlp_ms": round(mlp_ms, 3), "seeded_ms": round(seeded_ms, 3),
+            "nn_over_plain": round(plain_ms / (mlp_ms + seeded_ms), 4), "seeded_only_over_plain": round(plain_ms / seeded_ms, 4),
+            "oracle_seeded_over_plain": round(plain_ms / oracle_ms, 4),
+            "note": "nn = grouped MLP proposals + seeded traversal of primaries and bounces; fine-tuning reported apart"}
 
 
-def raster_leg(dev, world, cam, tree, verts, W, H):
-    """The rasteriser on the same 2^20-face soup (faces in the build's position
-    order) and a W x H frame, beside the primary-ray trace of the same view.
-    The camera is moved off the z axis: the reference's view matrix is NaN for
-    a camera looking exactly along z. CUDA events, L2 flushed, surfaces cleared
-    (as CUDABuffer::clearOutputSurfaces) before each run."""
+def run_e2e(w, args, dev, world, sched):
+    """The headline metric through the public API with host buffers, as a frame pipeline: every frame copies
+    the 64 instances' displaced vertices from pinned host memory, builds, makes the primary rays, traces them
+    and their bounces, and copies every hit (id, t, u, v of primaries and bounces) back to pinned host memory.
+    The copies run on two copy streams (one per direction) with the device vertices and hits double-buffered,
+    so that frame k+1's upload and frame k-1's download overlap frame k's kernels (one CUDA graph per buffer
+    set); the timed region holds every frame's copies and kernels. The faces (the instances' fixed topology)
+    stay resident."""
     import torch
 
     from cudart_b200 import core
 
-    center = (cam.center[0] + 0.05, cam.center[1] + 0.1, cam.center[2])
-    camera = core.make_camera(center, cam.target, fov=cam.fov, ratio=cam.ratio)
-    m = core.raster_matrix(camera, cam.target)
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    P = W * H
-    out = dict(id=torch.zeros(P, dtype=torch.int32, device=dev), uv=torch.zeros((P, 2), dtype=torch.float32, device=dev),
-               depth=torch.full((P,), 3.402823466e38, dtype=torch.float32, device=dev), err=torch.zeros(1, dtype=torch.int32, device=dev))
-    faces = tree.faces
-    ms = []
-    for rep in range(6):
-        out["id"].zero_()
-        out["uv"].zero_()
-        out["depth"].fill_(3.402823466e38)
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        core.rasterize(verts, faces, m, W, H, out=out)
-        e1.record()
-        torch.cuda.synchronize()
-        if rep:
-            ms.append(e0.elapsed_time(e1))
-    o, d = core.primary_rays(camera, W, H)
-    core.trace(tree, o, d)
+    vh = w.verts.cpu().pin_memory()
+    R = w.ray_count
+    comp = torch.cuda.current_stream()
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+    v = [torch.empty_like(w.verts) for _ in range(2)]
+    for s in range(2):
+        v[s].copy_(vh)
+    outs = [w.trace_plain() for _ in range(2)]
+    out_id = torch.empty((2, 2, R), dtype=torch.int32).pin_memory()
+    out_t = torch.empty((2, 2, R), dtype=torch.float32).pin_memory()
+    out_uv = torch.empty((2, 2, R, 2), dtype=torch.float32).pin_memory()
+    ev = {k: [torch.cuda.Event(), torch.cuda.Event()] for k in ("uploaded", "traced", "downloaded")}
+
+    def compute(s):
+        w.build(v[s])
+        w.primary_rays()
+        o = outs[s]
+        core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, out=o["h1"], schedule=sched)
+        w.bounce(o["h1"], out=o["b"])
+        core.batch_trace(w.tree, o["b"][0], o["b"][1], w.ray_offsets, tmax=o["b"][2], out=o["h2"], schedule=sched)
+
+    graphs, _ = capture_graphs([lambda: compute(0), lambda: compute(1)])
+
+    def step(k):
+        s = k % 2
+        if k >= 2:
+            up.wait_event(ev["traced"][s])  # frame k-2's kernels are done with this vertex buffer
+        with torch.cuda.stream(up):
+            v[s].copy_(vh, non_blocking=True)
+        ev["uploaded"][s].record(up)
+        comp.wait_event(ev["uploaded"][s])
+        if k >= 2:
+            comp.wait_event(ev["downloaded"][s])  # frame k-2's hits have reached the host
+        graphs[s].replay()
+        ev["traced"][s].record(comp)
+        down.wait_event(ev["traced"][s])
+        with torch.cuda.stream(down):
+            for i, h in enumerate((outs[s]["h1"], outs[s]["h2"])):
+                out_id[s, i].copy_(h["id"], non_blocking=True)
+                out_t[s, i].copy_(h["t"], non_blocking=True)
+                out_uv[s, i].copy_(h["uv"], non_blocking=True)
+        ev["downloaded"][s].record(down)
+
+    for k in range(args.warmup):
+        step(k)
     torch.cuda.synchronize()
-    tms = []
-    for rep in range(4):
+    active = sum(int((outs[s]["b"][2] > 0).sum().item()) for s in range(2)) / 2.0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(comp)
+    up.wait_event(e0)
+    down.wait_event(e0)
+    for k in range(args.steps):
+        step(k)
+    comp.wait_event(ev["downloaded"][(args.steps - 1) % 2])
+    e1.record(comp)
+    torch.cuda.synchronize()
+    ms, = max_over_ranks([e0.elapsed_time(e1)], world, dev)
+    ok = torch.equal(out_id[(args.steps - 1) % 2, 0], outs[(args.steps - 1) % 2]["h1"]["id"].cpu())
+    h2d = vh.numel() * 4
+    d2h = (out_id[0].numel() + out_t[0].numel() + out_uv[0].numel()) * 4
+    del graphs
+    return {"value": round(world * (R + active) * args.steps / (ms * 1e-3) / 1e6, 2), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": round(ms / args.steps, 3), "download_checked": bool(ok),
+            "pipeline": "vertices up / hits down on two copy streams, double-buffered around one CUDA graph per frame"}
+
+
+# ----------------------------------------------------------------------------
+# CPU baseline / reference arm: the oracle (the reference algorithm restated in
+# C++, checked against the reference's own code) on the host cores
+# ----------------------------------------------------------------------------
+_C4_HOST = {}
+
+
+def c4_host_scene(count):
+    """Host copy of the instanced scene: base mesh and the instances' cameras (the same generators as the GPU arm)."""
+    if count not in _C4_HOST:
+        from cudart_b200 import scenes
+        _C4_HOST[count] = (scenes.learned_scene(C4_SCALE), scenes.instance_cameras(count, C4_W, C4_H))
+    return _C4_HOST[count]
+
+
+def c4_instance_sample(count, frame, threads, ray_stride=1):
+    """One instance of one frame on the host cores: its displaced vertices (numpy N(0, 0.002^2), seeded by the
+    frame and instance), its LBVH build, its camera's primary rays (every `ray_stride`-th) traced, their
+    diffuse bounces traced. Returns (seconds, rays traced, faces built, seconds of the build)."""
+    from oracle import api as O
+
+    base, cams = c4_host_scene(count)
+    i = frame % count
+    rng = np.random.default_rng(7_000_003 + 64 * frame + i)
+    verts = base.vertices.copy()
+    verts[:, :3] += rng.normal(0.0, 0.002, size=(len(verts), 3)).astype(np.float32)
+    o, d, _, _ = O.primary_rays(cams[i])
+    if ray_stride > 1:
+        o, d = np.ascontiguousarray(o[::ray_stride]), np.ascontiguousarray(d[::ray_stride])
+    O.set_threads(threads)
+    t0 = time.perf_counter()
+    ref = O.lbvh_build(verts, base.faces)
+    t_build = time.perf_counter() - t0
+    e = O.trace(ref["nodes"], ref["tris"], ref["indices"], o, d, threads=threads)
+    bo, bd, bt = O.bounce_rays(ref["tris"], o, d, e["id"], e["t"], 1000 + frame)
+    O.trace(ref["nodes"], ref["tris"], ref["indices"], bo, bd, bt, threads=threads)
+    total = time.perf_counter() - t0
+    O.set_threads(0)
+    return total, len(o) + int((bt > 0).sum()), base.face_count, t_build
+
+
+def cpu_baseline_c4(count, frame=0, steps=1, one_thread=True):
+    """The frame workload's rate on the host cores: instance (frame mod count) of a frame, built and traced
+    whole (1/count of the frame) with all threads; the 1-thread figure on every 16th of its primary rays."""
+    from oracle import api as O
+
+    cores = O.max_threads()
+    c4_instance_sample(count, frame, cores, ray_stride=64)  # load the library, page the scene in
+    vals, builds = [], []
+    for k in range(steps):
+        sec, rays, faces, tb = c4_instance_sample(count, frame + k, cores)
+        vals.append(rays / sec / 1e6)
+        builds.append(faces / tb / 1e6)
+    out = {"value": round(statistics.median(vals), 4), "unit": "Mrays/s", "cores": cores, "kind": "port",
+           "sample": f"1/{count} of a frame per step: one instance's build ({faces} faces) + its {C4_W * C4_H} primary rays "
+                     f"and their bounces ({rays} rays), oracle port, all {cores} threads",
+           "build_mtri_s": round(statistics.median(builds), 3)}
+    if one_thread:
+        sec, rays, faces, tb = c4_instance_sample(count, frame, 1, ray_stride=16)
+        out["value_1_thread"] = round(rays / sec / 1e6, 4)
+        out["build_mtri_s_1_thread"] = round(faces / tb / 1e6, 3)
+    return out
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from oracle import api as O
+
+    cores = O.max_threads()
+    c4_instance_sample(args.instances, 0, cores, ray_stride=64)  # load the library, page the scene in
+    vals, builds, secs = [], [], []
+    for k in range(args.warmup + args.steps):
+        sec, rays, faces, tb = c4_instance_sample(args.instances, k, cores)
+        if k >= args.warmup:
+            vals.append(rays / sec / 1e6)
+            builds.append(faces / tb / 1e6)
+            secs.append(sec)
+    value = round(statistics.median(vals), 4)
+    sample = (f"1/{args.instances} of a frame per step: instance (step mod {args.instances})'s build ({faces} faces) + its "
+              f"{C4_W * C4_H} primary rays and their bounces, all {cores} threads")
+    return {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(statistics.median(secs) * 1e3, 2), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded PCG64 scene, numpy N(0,0.002^2) displacement per frame and instance)",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "instances": args.instances, "tree_depth": 12, "parallelism": f"host cores ({cores} threads)"},
+        "build": {"value": round(statistics.median(builds), 3), "unit": "Mtri/s"},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's GPU kernels use texture references and string-named symbol copies that CUDA 12 removed; "
+                "its algorithm runs here as the oracle port (checked bit-exact against the reference's own code)",
+    }
+
+
+# ----------------------------------------------------------------------------
+# secondary workloads (one JSON line each, before the headline)
+# ----------------------------------------------------------------------------
+def timed_ms(fn, flush, reps=5, agg=statistics.median):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        core.trace(tree, o, d)
+        fn()
         e1.record()
         torch.cuda.synchronize()
-        tms.append(e0.elapsed_time(e1))
-    r = statistics.median(ms)
-    covered = float((out["depth"] < 3.4e38).float().mean().item())
-    del flush
-    return {"width": W, "height": H, "faces": int(faces.shape[0]), "raster_ms": round(r, 4),
-            "raster_mpix_s": round(world * W * H / (r * 1e-3) / 1e6, 2), "covered_fraction": round(covered, 4),
-            "trace_primary_ms_same_view": round(statistics.median(tms), 4), "device_errors": int(out["err"].item())}
+        ms.append(e0.elapsed_time(e1))
+    return agg(ms)
 
 
-def sah_leg(args, dev, world, mesh, camera, W, H, lbvh_tree):
-    """SAH and Hybrid (LBVH depth 12, then SAH) builds of the 2^20-face soup
-    (CUDA events, L2 flushed), and the primary + bounce trace through each tree
-    with its own tuned schedule, beside the LBVH tree's."""
+def leg_single_scene(args, dev, world, mesh, cam, key, with_roofline=False):
+    """One scene: LBVH build and the primary + bounce traces, each stage replayed from a CUDA graph, CUDA
+    events between the replays, L2 flushed between steps, tuned schedules."""
     import torch
 
     from cudart_b200 import core, tune
 
     v = torch.from_numpy(mesh.vertices).to(dev)
     f = torch.from_numpy(mesh.faces.view(np.int32)).to(dev)
+    N, W, H = mesh.face_count, cam.width, cam.height
+    R = W * H
+    camera = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
+    tree = core.build_lbvh(v, f)
+    rays = core.primary_rays(camera, W, H)
+    h1 = core.trace(tree, rays[0], rays[1])
+    bounce = core.bounce_rays(tree.tris, rays[0], rays[1], h1["id"], h1["t"], SEED_BOUNCE)
+    h2 = core.trace(tree, bounce[0], bounce[1], tmax=bounce[2])
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    o, d = core.primary_rays(camera, W, H)
-    base_hits = core.trace(lbvh_tree, o, d)
-    b = core.bounce_rays(lbvh_tree.tris, o, d, base_hits["id"], base_hits["t"], SEED_BOUNCE)
-    R = o.shape[0]
-
-    def timed(fn, reps=5):
-        fn()
+    s1, _ = tune.tune_trace(tree, rays[0], rays[1], image_width=W, key=f"{key}-primary", use_cache=False)
+    s2, _ = tune.tune_trace(tree, bounce[0], bounce[1], tmax=bounce[2], image_width=W, key=f"{key}-bounce", use_cache=False)
+    stages = [lambda: core.build_lbvh(v, f, out=tree), lambda: core.primary_rays(camera, W, H, out=rays),
+              lambda: core.trace(tree, rays[0], rays[1], out=h1, schedule=s1),
+              lambda: core.bounce_rays(tree.tris, rays[0], rays[1], h1["id"], h1["t"], SEED_BOUNCE, out=bounce),
+              lambda: core.trace(tree, bounce[0], bounce[1], tmax=bounce[2], out=h2, schedule=s2)]
+    graphs, kernels = capture_graphs(stages)
+    steps = max(3, min(args.steps, 10))
+    evs = []
+    for k in range(args.warmup + steps):
+        flush.zero_()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+        ev[0].record()
+        for i, g in enumerate(graphs):
+            g.replay()
+            ev[i + 1].record()
+        if k >= args.warmup:
+            evs.append(ev)
+    torch.cuda.synchronize()
+    build_ms = sum(e[0].elapsed_time(e[1]) for e in evs) / steps
+    t1 = sum(e[2].elapsed_time(e[3]) for e in evs) / steps
+    t2 = sum(e[4].elapsed_time(e[5]) for e in evs) / steps
+    build_ms, t1, t2 = max_over_ranks([build_ms, t1, t2], world, dev)
+    active = int((bounce[2] > 0).sum().item())
+    info = tree.info_host()
+    out = {"faces": N, "primary_rays": R, "active_bounces": active, "build_ms": round(build_ms, 4),
+           "build_mtri_s": round(world * N / (build_ms * 1e-3) / 1e6, 1), "primary_ms": round(t1, 4), "bounce_ms": round(t2, 4),
+           "mrays_s": round(world * (R + active) / ((t1 + t2) * 1e-3) / 1e6, 1), "nodes": info["node_count"],
+           "schedule_primary": s1, "schedule_bounce": s2, "kernels_per_step": kernels}
+    if with_roofline:
+        c1 = core.trace(tree, rays[0], rays[1], counters=True, schedule=s1)
+        c2 = core.trace(tree, bounce[0], bounce[1], tmax=bounce[2], counters=True, schedule=s2)
         torch.cuda.synchronize()
-        ms = []
-        for _ in range(reps):
-            flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            fn()
-            e1.record()
-            torch.cuda.synchronize()
-            ms.append(e0.elapsed_time(e1))
-        return statistics.median(ms)
+        m1 = 48 * R + 32 * int(c1["visits"].sum().item()) + 48 * int(c1["tests"].sum().item())
+        m2 = 48 * R + 32 * int(c2["visits"].sum().item()) + 48 * int(c2["tests"].sum().item())
+        peak, kind = load_peaks()
 
-    out = {"faces": int(f.shape[0])}
-    trees = {"lbvh": lbvh_tree}
-    sah = core.build_sah(v, f)
-    hyb = core.build_sah(v, f, lbvh_depth=12)
-    out["sah_build_ms"] = round(timed(lambda: core.build_sah(v, f, out=sah)), 4)
-    out["hybrid12_build_ms"] = round(timed(lambda: core.build_sah(v, f, lbvh_depth=12, out=hyb)), 4)
-    out["lbvh_build_ms"] = round(timed(lambda: core.build_lbvh(v, f, out=lbvh_tree)), 4)
-    out["sah_levels"] = sah.info_host()["real_depth"]
-    trees["sah"], trees["hybrid12"] = sah, hyb
-    for name, tr in trees.items():
-        s1, _ = tune.tune_trace(tr, o, d, image_width=W, key=f"sah-{name}-p", use_cache=False)
-        s2, _ = tune.tune_trace(tr, b[0], b[1], tmax=b[2], key=f"sah-{name}-b", use_cache=False)
-        tp = timed(lambda: core.trace(tr, o, d, schedule=s1))
-        tb = timed(lambda: core.trace(tr, b[0], b[1], tmax=b[2], schedule=s2))
-        cnt = core.trace(tr, o, d, counters=True)
-        out[name] = {"nodes": tr.node_count, "primary_ms": round(tp, 4), "bounce_ms": round(tb, 4),
-                     "mrays_s": round(world * 2 * R / ((tp + tb) * 1e-3) / 1e6, 2),
-                     "primary_visits_per_ray": round(cnt["visits"].float().mean().item(), 2),
-                     "primary_tests_per_ray": round(cnt["tests"].float().mean().item(), 2)}
-    del flush
+        def kname(sch):
+            if sch.get("coop"):
+                return "k_trace_coop_persistent" if sch.get("persistent") else "k_trace_coop"
+            return "k_trace_accel_persistent" if sch.get("persistent") else "k_trace_accel"
+        out["roofline_primary"] = trace_roofline(kname(s1), "primary", m1, t1, R, peak, kind, kname(s1))
+        out["roofline_bounce"] = trace_roofline(kname(s2), "bounce", m2, t2, R, peak, kind, kname(s2))
+        bb = N * (16 + 48 + 32 + 8 + 64 + 4 + 32 + 36 + 48) + 64 * info["node_count"]
+        a = bb / (build_ms * 1e-3) / 1e9
+        out["build_roofline"] = {"bound": "hbm", "achieved": round(a, 1), "peak": peak, "unit": "GB/s", "frac": round(a / peak, 4)}
+    del graphs, flush
     return out
 
 
-def learned(args, dev, world, train_rays=16 << 20, eval_rays=8 << 20, batch=8192, lr=2e-3):
-    """Learned subtree proposal: 4,022,242-triangle terrain + soup scene, tree
-    cut at depth 12 (4096 slots). Training set: 16M rays (origins uniform in the
-    scene box grown 1.5x, directions uniform on the sphere) labelled by the plain
-    traversal; rays that miss are left out. One epoch of Adam (batch 8192,
-    cosine learning rate) on the GPU through the project's GEMM / softmax / Adam
-    kernels. Evaluation: 8M fresh rays traced plain and with the proposal (MLP
-    inference + seeded traversal); hits compared bit for bit. The "oracle" line
-    seeds every ray with its true slot: the most any proposal can save."""
+def leg_build_16m(args, dev, world):
+    """LBVH build alone on a 2^24-face soup, replayed from a CUDA graph, CUDA events, L2 flushed."""
+    import torch
+
+    from cudart_b200 import core, scenes
+
+    mesh = scenes.soup(1 << 24, seed=7)
+    v = torch.from_numpy(mesh.vertices).to(dev)
+    f = torch.from_numpy(mesh.faces.view(np.int32)).to(dev)
+    del mesh
+    tree = core.build_lbvh(v, f)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    (graph,), kernels = capture_graphs([lambda: core.build_lbvh(v, f, out=tree)])
+    ms = timed_ms(graph.replay, flush, reps=max(3, min(args.steps, 10)))
+    ms, = max_over_ranks([ms], world, dev)
+    info = tree.info_host()
+    n = 1 << 24
+    peak, _ = load_peaks()
+    bb = n * (16 + 48 + 32 + 8 + 64 + 4 + 32 + 36 + 48) + 64 * info["node_count"]
+    a = bb / (ms * 1e-3) / 1e9
+    del graph, flush
+    return {"faces": n, "mtri_s": round(world * n / (ms * 1e-3) / 1e6, 1), "ms": round(ms, 4), "nodes": info["node_count"],
+            "kernels": kernels, "roofline": {"bound": "hbm", "achieved": round(a, 1), "peak": peak, "unit": "GB/s", "frac": round(a / peak, 4)}}
+
+
+def leg_batch(args, dev, world, count=1024):
+    """1024 independent meshes (face counts log-uniform in [64, 65536], terrain or soup by coin flip), each
+    with side x side rays (side log-uniform in [64, 512]) from its bounding sphere aimed uniformly inward.
+    One batched build and one batched trace, captured together in a CUDA graph and replayed."""
+    import torch
+
+    from cudart_b200 import core, scenes, tune
+
+    meshes = scenes.batch_meshes(count, seed=3)
+    verts, faces, fo, vo = scenes.concat_batch(meshes)
+    orig, dirs, ro = scenes.batch_sphere_rays_torch(meshes, device=dev)
+    R = int(ro[-1])
+    del meshes
+    V = torch.from_numpy(verts).to(dev)
+    Fc = torch.from_numpy(faces.view(np.int32)).to(dev)
+    roff = torch.tensor(ro.astype(np.int32), device=dev)
+    tree = core.batch_build(V, Fc, fo, vo)
+    sched, _ = tune.tune_batch_trace(tree, orig, dirs, roff, key=f"batch{count}", use_cache=False)  # untimed
+    hits = core.batch_trace(tree, orig, dirs, roff, schedule=sched)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    (gb, gt), kernels = capture_graphs([lambda: core.batch_build(V, Fc, fo, vo, out=tree),
+                                        lambda: core.batch_trace(tree, orig, dirs, roff, out=hits, schedule=sched)])
+    bms = timed_ms(gb.replay, flush, reps=3)
+    tms = timed_ms(gt.replay, flush, reps=3)
+    bms, tms = max_over_ranks([bms, tms], world, dev)
+    info = tree.info.cpu().numpy()
+    N = int(fo[-1])
+    del gb, gt, flush
+    return {"meshes": count, "faces": N, "rays": R, "schedule": sched, "build_ms": round(bms, 4),
+            "build_mtri_s": round(world * N / (bms * 1e-3) / 1e6, 1), "trace_ms": round(tms, 4),
+            "trace_mrays_s": round(world * R / (tms * 1e-3) / 1e6, 1), "graph_mrays_s": round(world * R / ((bms + tms) * 1e-3) / 1e6, 1),
+            "kernels": kernels, "hit_fraction": round(float((hits["id"] >= 0).float().mean().item()), 4),
+            "device_errors": int((info[:, 7] != 0).sum())}
+
+
+def leg_learned(args, dev, world, train_rays=16 << 20, eval_rays=8 << 20, batch=8192, lr=2e-3):
+    """Learned subtree proposal on the 4,022,242-triangle terrain + soup scene, tree cut at depth 12 (4096
+    slots): one epoch of Adam on 16M rays labelled by the plain traversal, then 8M fresh rays traced plain
+    and with the proposal (MLP inference + seeded traversal); hits compared bit for bit."""
     import math
 
     import torch
 
     from cudart_b200 import core, proposal, scenes, tune
 
-    scale = args.learned_scale
-    mesh = scenes.learned_scene(scale)
+    mesh = scenes.learned_scene(1.0)
     box = scenes.scene_box(mesh, 1.5)
     V = torch.from_numpy(mesh.vertices).to(dev)
     Fc = torch.from_numpy(mesh.faces.view(np.int32)).to(dev)
@@ -609,8 +767,8 @@ def learned(args, dev, world, train_rays=16 << 20, eval_rays=8 << 20, batch=8192
     del mesh
     tree = core.build_lbvh(V, Fc)
     slots = proposal.subtree_slots(tree, proposal.DEPTH)
-    to, td = scenes.box_rays_torch(int(train_rays * scale) if scale < 1 else train_rays, box, seed=1, device=dev)
-    eo, ed = scenes.box_rays_torch(int(eval_rays * scale) if scale < 1 else eval_rays, box, seed=2, device=dev)
+    to, td = scenes.box_rays_torch(train_rays, box, seed=1, device=dev)
+    eo, ed = scenes.box_rays_torch(eval_rays, box, seed=2, device=dev)
     sched, _ = tune.tune_trace(tree, eo, ed, key=f"learned{N}", use_cache=False)
     lab_hits = core.trace(tree, to, td, schedule=sched)
     labels = proposal.hit_labels(lab_hits["id"], slots["pos_label"])
@@ -627,308 +785,139 @@ def learned(args, dev, world, train_rays=16 << 20, eval_rays=8 << 20, batch=8192
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record()
-    first_loss = None
     for st in range(steps):
         sl = slice(st * batch, (st + 1) * batch)
-        cur = lr * 0.5 * (1.0 + math.cos(math.pi * st / steps))
-        loss = net.train_step(to[sl], td[sl], tl[sl], box, lr=cur)
-        if st == 0:
-            first_loss = loss
+        loss = net.train_step(to[sl], td[sl], tl[sl], box, lr=lr * 0.5 * (1.0 + math.cos(math.pi * st / steps)))
     ev1.record()
     torch.cuda.synchronize()
     train_ms = ev0.elapsed_time(ev1)
-    last_loss = loss.item()
     flop_fwd = 2.0 * (144 * 128 + 2 * 128 * 128 + 128 * 4096)
     del to, td, tl
-
     R = eo.shape[0]
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    plain = core.trace(tree, eo, ed, counters=True, schedule=sched)
+    plain = core.trace(tree, eo, ed, schedule=sched)
     prop = net.propose(eo, ed, box)
-    seeded = proposal.trace_seeded(tree, eo, ed, prop, slots, counters=True, in_proposal=True, schedule=sched)
+    seeded = proposal.trace_seeded(tree, eo, ed, prop, slots, in_proposal=True, schedule=sched)
     oracle_prop = proposal.hit_labels(plain["id"], slots["pos_label"])
-    best = proposal.trace_seeded(tree, eo, ed, oracle_prop, slots, counters=True, schedule=sched)
     torch.cuda.synchronize()
     exact = (torch.equal(plain["id"], seeded["id"]) and torch.equal(plain["t"].view(torch.int32), seeded["t"].view(torch.int32))
              and torch.equal(plain["uv"].view(torch.int32), seeded["uv"].view(torch.int32)))
     hit = plain["id"] >= 0
     acc = float(seeded["in_proposal"][hit].float().mean().item())
-    vp, tp = plain["visits"].sum().item(), plain["tests"].sum().item()
-
-    def timed(fn, reps=3):
-        out = []
-        for _ in range(reps):
-            flush.zero_()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
-            fn()
-            b.record()
-            torch.cuda.synchronize()
-            out.append(a.elapsed_time(b))
-        return min(out)
-
-    hits_p = core.trace(tree, eo, ed, schedule=sched)
-    hits_s = proposal.trace_seeded(tree, eo, ed, prop, slots, schedule=sched)
-    ms_plain = timed(lambda: core.trace(tree, eo, ed, schedule=sched, out=hits_p))
-    ms_mlp = timed(lambda: net.propose(eo, ed, box, out=prop))
-    ms_seeded = timed(lambda: proposal.trace_seeded(tree, eo, ed, prop, slots, schedule=sched, out=hits_s))
-    ms_oracle = timed(lambda: proposal.trace_seeded(tree, eo, ed, oracle_prop, slots, schedule=sched, out=hits_s))
-    ms_nn = ms_mlp + ms_seeded
+    hs = proposal.trace_seeded(tree, eo, ed, prop, slots, schedule=sched)
+    ms_plain = timed_ms(lambda: core.trace(tree, eo, ed, schedule=sched, out=plain), flush, reps=3, agg=min)
+    ms_mlp = timed_ms(lambda: net.propose(eo, ed, box, out=prop), flush, reps=3, agg=min)
+    ms_seeded = timed_ms(lambda: proposal.trace_seeded(tree, eo, ed, prop, slots, schedule=sched, out=hs), flush, reps=3, agg=min)
+    ms_oracle = timed_ms(lambda: proposal.trace_seeded(tree, eo, ed, oracle_prop, slots, schedule=sched, out=hs), flush, reps=3, agg=min)
+    ms_plain, ms_mlp, ms_seeded, ms_oracle = max_over_ranks([ms_plain, ms_mlp, ms_seeded, ms_oracle], world, dev)
     del flush
-    return {"faces": N, "train_rays": train_rays, "train_hits": n_train, "train_steps": steps, "batch": batch,
-            "train_ms": round(train_ms, 2), "train_ms_per_step": round(train_ms / max(steps, 1), 4),
-            "train_tflops": round(3 * flop_fwd * n_train / (train_ms * 1e-3) / 1e12, 1),
-            "loss_first": round(float(first_loss.item()), 4), "loss_last": round(last_loss, 4),
-            "eval_rays": R, "hit_fraction": round(float(hit.float().mean().item()), 4), "schedule": sched,
-            "bit_exact": bool(exact), "proposal_accuracy": round(acc, 4),
-            "plain_ms": round(ms_plain, 4), "plain_mrays_s": round(world * R / (ms_plain * 1e-3) / 1e6, 2),
-            "mlp_ms": round(ms_mlp, 4), "mlp_tflops": round(flop_fwd * R / (ms_mlp * 1e-3) / 1e12, 1),
-            "seeded_ms": round(ms_seeded, 4), "nn_mrays_s": round(world * R / (ms_nn * 1e-3) / 1e6, 2),
-            "nn_over_plain": round(ms_plain / ms_nn, 4), "seeded_only_over_plain": round(ms_plain / ms_seeded, 4),
-            "visits_ratio": round(seeded["visits"].sum().item() / vp, 4), "tests_ratio": round(seeded["tests"].sum().item() / tp, 4),
-            "oracle_proposal": {"ms": round(ms_oracle, 4), "over_plain": round(ms_plain / ms_oracle, 4),
-                                "visits_ratio": round(best["visits"].sum().item() / vp, 4),
-                                "tests_ratio": round(best["tests"].sum().item() / tp, 4)},
-            "mean_visits_plain": round(vp / R, 3), "mean_tests_plain": round(tp / R, 3)}
+    return {"faces": N, "train_steps": steps, "batch": batch, "train_ms": round(train_ms, 1),
+            "train_tflops": round(3 * flop_fwd * n_train / (train_ms * 1e-3) / 1e12, 1), "loss_last": round(float(loss.item()), 4),
+            "eval_rays": R, "bit_exact": bool(exact), "proposal_accuracy": round(acc, 4), "plain_ms": round(ms_plain, 3),
+            "plain_mrays_s": round(world * R / (ms_plain * 1e-3) / 1e6, 1), "mlp_ms": round(ms_mlp, 3),
+            "mlp_tflops": round(flop_fwd * R / (ms_mlp * 1e-3) / 1e12, 1), "seeded_ms": round(ms_seeded, 3),
+            "nn_over_plain": round(ms_plain / (ms_mlp + ms_seeded), 4), "oracle_seeded_over_plain": round(ms_plain / ms_oracle, 4)}
 
 
-def instanced(args, dev, world, scale=1 / 16, width=960, height=540, steps=200, batch=1024, lr=1e-3):
-    """Instanced frames: `count` (64) copies of the learned scene at 1/16 size
-    (251,518 triangles each, 16.1M per frame), every vertex moved by fresh
-    N(0, 0.002^2) noise each frame and all copies rebuilt by one batched LBVH
-    build. Each copy renders a 480 x 270 tile of a 3840 x 2160 frame at 4
-    samples per pixel (its own camera at 960 x 540: a regular 2 x 2 sub-pixel
-    grid), plus one diffuse bounce per hit. Each copy has its own proposal
-    network, fine-tuned every frame for `steps` grouped Adam steps of `batch`
-    rays on the previous frame's plain-traversal labels. Per frame, timed on
-    the device: the build, the fine-tuning, the plain traversal (primaries +
-    bounces) and the learned one (grouped MLP proposals + seeded traversal),
-    side by side; hits compared bit for bit every frame."""
+def leg_sah(args, dev, world):
+    """SAH and Hybrid (LBVH depth 12, then SAH) builds of the 2^20-face soup, and the primary + bounce trace
+    through each tree with its own tuned schedule, beside the LBVH tree's."""
     import torch
 
-    from cudart_b200.instances import InstancedFrames
+    from cudart_b200 import core, scenes, tune
 
-    count, frames = args.instanced_count, args.instanced_frames
-    w = InstancedFrames(count, scale, width, height, device=dev, batch=batch, steps=steps, lr=lr)
-    # frame 0 (untimed): labels for frame 1, workspaces, first launches
-    w.displace(0)
-    w.build()
-    w.make_slots()
-    sched, _ = w.tune()
-    plain = w.trace_plain()
-    learned = w.trace_learned()
-    w.remember(plain)
-    w.fine_tune(steps=2)
-    torch.cuda.synchronize()
-    R = w.ray_count
-    ev = []
-    mism = torch.zeros(1, dtype=torch.int64, device=dev)
-    active = torch.zeros(1, dtype=torch.int64, device=dev)
-    inprop = torch.zeros(2, dtype=torch.int64, device=dev)
-    loss0 = loss1 = None
-    for f in range(1, frames + 1):
-        w.displace(f)  # the frame's input (untimed)
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
-        e[0].record()
-        w.build()
-        w.make_slots()
-        e[1].record()
-        loss = w.fine_tune()
-        e[2].record()
-        w.trace_plain(out=plain)
-        e[3].record()
-        w.trace_learned(out=learned, in_proposal=True)
-        e[4].record()
-        for k in ("h1", "h2"):
-            mism += (plain[k]["id"] != learned[k]["id"]).sum() + (plain[k]["t"].view(torch.int32) != learned[k]["t"].view(torch.int32)).sum()
-            mism += (plain[k]["uv"].view(torch.int32) != learned[k]["uv"].view(torch.int32)).sum()
-            hit = plain[k]["id"] >= 0
-            inprop[0] += (learned[k]["in_proposal"].bool() & hit).sum()
-            inprop[1] += hit.sum()
-        active += (plain["b"][2] > 0).sum()
-        if f == 1:
-            loss0 = loss.clone() / count
-        loss1 = loss.clone() / count
-        w.remember(plain)
-        e[5].record()
-        ev.append(e)
-    torch.cuda.synchronize()
-    build_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
-    tune_ms = sum(e[1].elapsed_time(e[2]) for e in ev)
-    plain_ms = sum(e[2].elapsed_time(e[3]) for e in ev)
-    nn_ms = sum(e[3].elapsed_time(e[4]) for e in ev)
-    rays = frames * R + int(active.item())  # primaries + active bounces
-    F = w.face_count
-    return {"instances": count, "faces_per_frame": F, "frames": frames, "tile": [width // 2, height // 2], "spp": 4, "schedule": sched,
-            "primary_rays_per_frame": R, "rays_timed": rays, "finetune_steps_per_frame": steps, "batch_per_instance": batch,
-            "build_ms_per_frame": round(build_ms / frames, 3), "build_mtri_s": round(world * F * frames / (build_ms * 1e-3) / 1e6, 1),
-            "finetune_ms_per_frame": round(tune_ms / frames, 3),
-            "plain_ms_per_frame": round(plain_ms / frames, 3), "plain_mrays_s": round(world * rays / (plain_ms * 1e-3) / 1e6, 2),
-            "nn_ms_per_frame": round(nn_ms / frames, 3), "nn_mrays_s": round(world * rays / (nn_ms * 1e-3) / 1e6, 2),
-            "nn_over_plain": round(plain_ms / nn_ms, 4), "bit_exact": int(mism.item()) == 0,
-            "proposal_accuracy": round(int(inprop[0].item()) / max(1, int(inprop[1].item())), 4),
-            "loss_first_frame": round(float(loss0.item()), 4), "loss_last_frame": round(float(loss1.item()), 4),
-            "frame_ms": round(sum(e[0].elapsed_time(e[4]) for e in ev) / frames, 3)}
+    mesh, cam = scenes.soup_1m_scene(seed=SEED_MESH)
+    v = torch.from_numpy(mesh.vertices).to(dev)
+    f = torch.from_numpy(mesh.faces.view(np.int32)).to(dev)
+    camera = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
+    W, H = cam.width, cam.height
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    trees = {"lbvh": core.build_lbvh(v, f), "sah": core.build_sah(v, f), "hybrid12": core.build_sah(v, f, lbvh_depth=12)}
+    o, d = core.primary_rays(camera, W, H)
+    base = core.trace(trees["lbvh"], o, d)
+    b = core.bounce_rays(trees["lbvh"].tris, o, d, base["id"], base["t"], SEED_BOUNCE)
+    R = o.shape[0]
+    out = {"faces": int(f.shape[0]),
+           "sah_build_ms": round(timed_ms(lambda: core.build_sah(v, f, out=trees["sah"]), flush), 4),
+           "hybrid12_build_ms": round(timed_ms(lambda: core.build_sah(v, f, lbvh_depth=12, out=trees["hybrid12"]), flush), 4),
+           "lbvh_build_ms": round(timed_ms(lambda: core.build_lbvh(v, f, out=trees["lbvh"]), flush), 4)}
+    for name, tr in trees.items():
+        s1, _ = tune.tune_trace(tr, o, d, image_width=W, key=f"sah-{name}-p", use_cache=False)
+        s2, _ = tune.tune_trace(tr, b[0], b[1], tmax=b[2], key=f"sah-{name}-b", use_cache=False)
+        tp = timed_ms(lambda: core.trace(tr, o, d, schedule=s1), flush)
+        tb = timed_ms(lambda: core.trace(tr, b[0], b[1], tmax=b[2], schedule=s2), flush)
+        out[name] = {"nodes": tr.node_count, "primary_ms": round(tp, 4), "bounce_ms": round(tb, 4),
+                     "mrays_s": round(world * 2 * R / ((tp + tb) * 1e-3) / 1e6, 1)}
+    del flush
+    return out
 
 
-def run_e2e(args, mesh, camera, W, H, dev, world, sched1=None, sched2=None):
-    """Same metric through the public API with host buffers, as a frame
-    pipeline: every step copies its mesh from pinned host memory, builds,
-    traces the primary rays and the bounces, and copies all hits back to pinned
-    host memory. The copies run on two copy streams (one per direction) with
-    the device mesh and hits double-buffered, so that step k+1's upload and
-    step k-1's download overlap step k's kernels, which are replayed from a
-    CUDA graph per buffer set; the timed region holds every step's copies and
-    kernels."""
+def leg_raster(args, dev, world):
+    """The rasteriser on the 2^20-face soup (faces in the build's position order) at 1920 x 1080, beside the
+    primary-ray trace of the same view; camera moved off the z axis (the reference's view matrix is NaN for
+    a camera looking exactly along z)."""
     import torch
 
-    from cudart_b200 import core
+    from cudart_b200 import core, scenes
 
-    vh = torch.from_numpy(mesh.vertices).pin_memory()
-    fh = torch.from_numpy(mesh.faces.view(np.int32)).pin_memory()
-    R = W * H
-    comp = torch.cuda.current_stream()
-    up, down = torch.cuda.Stream(), torch.cuda.Stream()
-    v = [torch.empty_like(vh, device=dev) for _ in range(2)]
-    f = [torch.empty_like(fh, device=dev) for _ in range(2)]
-    out_id = torch.empty((2, 2, R), dtype=torch.int32).pin_memory()
-    out_t = torch.empty((2, 2, R), dtype=torch.float32).pin_memory()
-    out_uv = torch.empty((2, 2, R, 2), dtype=torch.float32).pin_memory()
-    for s in range(2):
-        v[s].copy_(vh)
-        f[s].copy_(fh)
-    tree = core.build_lbvh(v[0], f[0])
-    rays = core.primary_rays(camera, W, H)
-    h1 = [core.trace(tree, rays[0], rays[1]) for _ in range(2)]
-    b = core.bounce_rays(tree.tris, rays[0], rays[1], h1[0]["id"], h1[0]["t"], SEED_BOUNCE)
-    h2 = [core.trace(tree, b[0], b[1], tmax=b[2]) for _ in range(2)]
-    ev = {k: [torch.cuda.Event(), torch.cuda.Event()] for k in ("uploaded", "traced", "downloaded")}
+    mesh, cam = scenes.soup_1m_scene(seed=SEED_MESH)
+    v = torch.from_numpy(mesh.vertices).to(dev)
+    f = torch.from_numpy(mesh.faces.view(np.int32)).to(dev)
+    tree = core.build_lbvh(v, f)
+    W, H = cam.width, cam.height
+    center = (cam.center[0] + 0.05, cam.center[1] + 0.1, cam.center[2])
+    camera = core.make_camera(center, cam.target, fov=cam.fov, ratio=cam.ratio)
+    m = core.raster_matrix(camera, cam.target)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    P = W * H
+    out = dict(id=torch.zeros(P, dtype=torch.int32, device=dev), uv=torch.zeros((P, 2), dtype=torch.float32, device=dev),
+               depth=torch.full((P,), 3.402823466e38, dtype=torch.float32, device=dev), err=torch.zeros(1, dtype=torch.int32, device=dev))
 
-    def compute(s):  # build, primary rays, trace, bounces, trace of buffer set s
-        core.build_lbvh(v[s], f[s], out=tree)
-        core.primary_rays(camera, W, H, out=rays)
-        core.trace(tree, rays[0], rays[1], out=h1[s], schedule=sched1)
-        core.bounce_rays(tree.tris, rays[0], rays[1], h1[s]["id"], h1[s]["t"], SEED_BOUNCE, out=b)
-        core.trace(tree, b[0], b[1], tmax=b[2], out=h2[s], schedule=sched2)
+    def draw():
+        out["depth"].fill_(3.402823466e38)  # CUDABuffer::clearOutputSurfaces
+        core.rasterize(v, tree.faces, m, W, H, out=out)
 
-    graphs, _ = capture_graphs([lambda: compute(0), lambda: compute(1)])  # one replay per step
-    torch.cuda.synchronize()
-
-    def step(k):
-        s = k % 2
-        if k >= 2:
-            up.wait_event(ev["traced"][s])  # step k-2's kernels are done with this mesh buffer
-        with torch.cuda.stream(up):
-            v[s].copy_(vh, non_blocking=True)
-            f[s].copy_(fh, non_blocking=True)
-        ev["uploaded"][s].record(up)
-        comp.wait_event(ev["uploaded"][s])
-        if k >= 2:
-            comp.wait_event(ev["downloaded"][s])  # step k-2's hits have reached the host
-        graphs[s].replay()
-        ev["traced"][s].record(comp)
-        down.wait_event(ev["traced"][s])
-        with torch.cuda.stream(down):
-            for i, h in enumerate((h1[s], h2[s])):
-                out_id[s, i].copy_(h["id"], non_blocking=True)
-                out_t[s, i].copy_(h["t"], non_blocking=True)
-                out_uv[s, i].copy_(h["uv"], non_blocking=True)
-        ev["downloaded"][s].record(down)
-
-    for k in range(args.warmup):
-        step(k)
-    torch.cuda.synchronize()
-    active = int((b[2] > 0).sum().item())
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(comp)
-    up.wait_event(e0)
-    down.wait_event(e0)
-    for k in range(args.steps):
-        step(k)
-    comp.wait_event(ev["downloaded"][(args.steps - 1) % 2])
-    e1.record(comp)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = t.item()
-    rays_per_step = R + active
-    h2d = vh.numel() * 4 + fh.numel() * 4
-    d2h = (out_id[0].numel() + out_t[0].numel() + out_uv[0].numel()) * 4
-    return {"value": round(world * rays_per_step * args.steps / (ms * 1e-3) / 1e6, 3), "unit": "Mrays/s",
-            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": round(ms / args.steps, 4),
-            "pipeline": "upload and download on two copy streams, double-buffered, overlapping the neighbouring steps' kernels; "
-                        "each step's kernels replayed from a CUDA graph"}
+    r = timed_ms(draw, flush)
+    o, d = core.primary_rays(camera, W, H)
+    t = timed_ms(lambda: core.trace(tree, o, d), flush)
+    del flush
+    return {"width": W, "height": H, "faces": int(f.shape[0]), "raster_ms": round(r, 4), "raster_mpix_s": round(world * P / (r * 1e-3) / 1e6, 1),
+            "covered_fraction": round(float((out["depth"] < 3.4e38).float().mean().item()), 4), "trace_primary_ms_same_view": round(t, 4),
+            "device_errors": int(out["err"].item())}
 
 
-# ----------------------------------------------------------------------------
-# CPU baseline / reference arm: the oracle (the reference algorithm restated in
-# C++, checked against the reference's own code) on the host cores
-# ----------------------------------------------------------------------------
-def cpu_baseline(mesh, cam, budget_s=12.0, threads=0):
-    from oracle import api as O
+def run_legs(args, rank, world, local_rank):
+    import torch
 
-    t0 = time.perf_counter()
-    ref = O.lbvh_build(mesh.vertices, mesh.faces)
-    t_build = time.perf_counter() - t0
-    o, d, _, _ = O.primary_rays(cam)
-    R = len(o)
-    # bounded sample of rays: grow until ~budget seconds of trace work
-    n = 20000
-    t_trace = 0.0
-    traced = 0
-    while True:
-        sl = slice(0, min(n, R))
-        oo, dd = np.ascontiguousarray(o[sl]), np.ascontiguousarray(d[sl])
-        t0 = time.perf_counter()
-        e = O.trace(ref["nodes"], ref["tris"], ref["indices"], oo, dd, threads=threads)
-        t1 = time.perf_counter() - t0
-        bo, bd, bt = O.bounce_rays(ref["tris"], oo, dd, e["id"], e["t"], SEED_BOUNCE)
-        t0 = time.perf_counter()
-        O.trace(ref["nodes"], ref["tris"], ref["indices"], bo, bd, bt, threads=threads)
-        t2 = time.perf_counter() - t0
-        t_trace, traced = t1 + t2, len(oo) + int((bt > 0).sum())
-        if t_trace > budget_s / 4 or n >= R:
-            break
-        n = min(R, int(n * max(2.0, (budget_s / 4) / max(t_trace, 1e-3))))
-    cores = threads if threads > 0 else O.max_threads()
-    return {"value": round(traced / t_trace / 1e6, 4), "unit": "Mrays/s", "cores": cores, "kind": "port",
-            "sample": f"build of all {mesh.face_count} faces ({mesh.face_count / t_build / 1e6:.3f} Mtri/s, 1 thread topology); "
-                      f"trace of the first {len(oo)} primary rays + their bounces ({traced} rays)",
-            "build_mtri_s": round(mesh.face_count / t_build / 1e6, 4)}
-
-
-def run_reference(args, rank, world):
-    if rank != 0:
-        return None
     from cudart_b200 import scenes
-    from oracle import api as O
 
-    mesh, cam = scenes.soup_1m_scene(n=args.faces, seed=SEED_MESH)
-    O.lbvh_build(mesh.vertices[:3 * 4096], mesh.faces[:4096])  # load / warm the library
-    vals, builds = [], []
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(mesh, cam, budget_s=8.0)
-        if i >= args.warmup:
-            vals.append(cb["value"])
-            builds.append(cb["build_mtri_s"])
-    value = statistics.median(vals)
-    return {
-        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded numpy PCG64 soup; PCG32 bounce directions)",
-        "config": {"workload": WORKLOAD, "faces": mesh.face_count, "primary_rays": cam.width * cam.height, "tree_depth": 12,
-                   "parallelism": "host cores (OpenMP)"},
-        "impl": "reference",
-        "build": {"value": statistics.median(builds), "unit": "Mtri/s"},
-        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": O.max_threads(), "kind": "port",
-                         "sample": cb["sample"]},
-        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference's GPU kernels use texture references and string-named symbol copies that CUDA 12 removed; "
-                "its algorithm runs here as the oracle port (checked bit-exact against the reference's own code)",
-    }
+    dev = torch.device("cuda", local_rank)
+    names = [] if args.legs in ("", "none") else args.legs.split(",")
+    for name in names:
+        if name == "c0":
+            mesh, cam = scenes.terrain_small_scene()
+            d = leg_single_scene(args, dev, world, mesh, cam, "terrain128")
+            d["workload"] = "terrain 128^2 vertices (32,258 triangles), 512x512 primary rays + 1 bounce per hit"
+        elif name == "c1":
+            mesh, cam = scenes.soup_1m_scene(seed=SEED_MESH)
+            d = leg_single_scene(args, dev, world, mesh, cam, "soup1m", with_roofline=True)
+            d["workload"] = "soup 2^20 triangles, 1920x1080 primary rays + 1 diffuse bounce per hit"
+        elif name == "build16m":
+            d = leg_build_16m(args, dev, world)
+        elif name == "c2":
+            d = leg_batch(args, dev, world)
+        elif name == "c3":
+            d = leg_learned(args, dev, world)
+        elif name == "sah":
+            d = leg_sah(args, dev, world)
+        elif name == "raster":
+            d = leg_raster(args, dev, world)
+        else:
+            raise SystemExit(f"unknown leg {name}")
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        if rank == 0:
+            emit({"leg": name, **d})
 
 
 def main():
@@ -939,7 +928,7 @@ def main():
     if args.impl == "reference":
         res = run_reference(args, rank, world)
         if res is not None:
-            print(json.dumps(res), flush=True)
+            emit(res)
         return
     if world > 1:
         import datetime
@@ -948,13 +937,18 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    res = run_ours(args, rank, world, local_rank)
+    import torch
+    torch.cuda.set_device(local_rank)
+    run_legs(args, rank, world, local_rank)
+    res, legs = run_headline(args, rank, world, local_rank)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
-        print(json.dumps(res), flush=True)
+        for k, d in legs.items():
+            emit({"leg": k, **d})
+        emit(res)
 
 
 if __name__ == "__main__":

@@ -29,7 +29,7 @@ TRACE_WIDE = 0x4
 EXPORTS = (
     "rt_lbvh_scratch_bytes", "rt_lbvh_accel_bytes", "rt_lbvh_build", "rt_batch_sizes", "rt_batch_build", "rt_batch_trace", "rt_mesh_boxes", "rt_reorder_faces", "rt_sort_scratch_bytes",
     "rt_radix_sort_pairs", "rt_radix_sort_pairs_static", "rt_radix_sort_keys", "rt_camera_look_at", "rt_camera_basis", "rt_primary_rays",
-    "rt_trace_closest", "rt_ray_order_scratch_bytes", "rt_ray_order", "rt_interpolate", "rt_bounce_rays", "rt_mesh_file_save", "rt_mesh_file_info", "rt_mesh_file_load", "rt_tree_file_save", "rt_tree_file_info",
+    "rt_trace_closest", "rt_ray_order_scratch_bytes", "rt_ray_order", "rt_interpolate", "rt_bounce_rays", "rt_batch_bounce_rays", "rt_mesh_file_save", "rt_mesh_file_info", "rt_mesh_file_load", "rt_tree_file_save", "rt_tree_file_info",
     "rt_tree_file_load", "rt_status_string", "rt_version", "rt_abi_version", "rt_device_check", "rt_launch_count",
 )
 # every symbol include/rt_sah.h declares
@@ -41,7 +41,7 @@ PROPOSE_EXPORTS = (
     "rt_propose_abi_version", "rt_gemm_bf16", "rt_gemm_argmax_bf16", "rt_ray_features", "rt_softmax_xent", "rt_transpose_bf16",
     "rt_colsum_bf16", "rt_adam_step", "rt_subtree_slots", "rt_hit_labels", "rt_trace_closest_seeded", "rt_transpose_bf16_grouped",
     "rt_colsum_bf16_grouped", "rt_gather_batch", "rt_batch_subtree_slots", "rt_batch_hit_labels", "rt_batch_trace_seeded",
-    "rt_group_select", "rt_mlp_propose", "rt_gemm_xent_bf16",
+    "rt_group_select", "rt_mlp_propose", "rt_gemm_xent_bf16", "rt_tc_wait_selftest",
 )
 
 _P = C.c_void_p
@@ -209,6 +209,7 @@ def lib():
         L.rt_ray_order_scratch_bytes.argtypes = [_U32, C.POINTER(C.c_size_t)]
         L.rt_ray_order.argtypes = [_P, _P, _P, _U32, C.POINTER(C.c_float), _P, _P, C.c_size_t, _P]
         L.rt_bounce_rays.argtypes = [_P, _P, _P, _P, _P, _U32, C.c_uint64, _P, _P, _P, _P]
+        L.rt_batch_bounce_rays.argtypes = [_P, _P, _P, _U32, _P, _P, _P, _P, _U32, C.c_uint64, _P, _P, _P, _P]
         for fn, st in (("mesh", MeshFile), ("tree", TreeFile)):
             getattr(L, f"rt_{fn}_file_save").argtypes = [C.c_char_p, C.c_int, C.POINTER(st)]
             getattr(L, f"rt_{fn}_file_info").argtypes = [C.c_char_p, C.POINTER(st)]
@@ -239,6 +240,7 @@ def lib():
         L.rt_group_select.argtypes = [_P, _U32, _U32, _P, _P, _P]
         L.rt_mlp_propose.argtypes = [C.POINTER(MlpProposeDesc), _P]
         L.rt_gemm_xent_bf16.argtypes = [C.POINTER(GemmXentDesc), _P]
+        L.rt_tc_wait_selftest.argtypes = [_U32, _P, _P, _P]
         L.rt_batch_subtree_slots.argtypes = [C.POINTER(BatchSlotDesc), _P]
         L.rt_batch_hit_labels.argtypes = [_P, _U32, _U32, _P, _P, _P, _P, _P]
         L.rt_batch_trace_seeded.argtypes = [C.POINTER(BatchTraceDesc), C.POINTER(SeedDesc), _P]

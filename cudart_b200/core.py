@@ -390,6 +390,20 @@ def bounce_rays(tris, orig, dir, hit_pos, hit_t, seed: int, out=None, ray_count:
     return out
 
 
+def batch_bounce_rays(tree, ray_offsets, orig, dir, hit_pos, hit_t, seed: int, out=None, stream=None):
+    """bounce_rays for the rays of a batched build: hit_pos are positions inside each ray's own mesh
+    (batch_trace's ids); the same rays as bounce_rays given the global positions."""
+    R = orig.shape[0]
+    dev = orig.device
+    if out is None:
+        out = (torch.empty((R, 4), dtype=torch.float32, device=dev), torch.empty((R, 4), dtype=torch.float32, device=dev),
+               torch.empty(R, dtype=torch.float32, device=dev))
+    _abi.check("rt_batch_bounce_rays", _abi.lib().rt_batch_bounce_rays(
+        _p(tree.tris), _p(tree.face_offsets), _p(ray_offsets), tree.mesh_count, _p(orig), _p(dir), _p(hit_pos), _p(hit_t), R,
+        C.c_uint64(seed), _p(out[0]), _p(out[1]), _p(out[2]), _stream(stream)))
+    return out
+
+
 def sort_pairs(keys: torch.Tensor, values: torch.Tensor, bit_depth: int = 32, init_values: bool = False, stream=None):
     """In place, stable (CUDA_radixSortGeneral)."""
     _need_cuda(keys, "keys", _I32)

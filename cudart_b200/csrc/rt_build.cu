@@ -656,15 +656,17 @@ size_t carve_build(Carve& c, BuildLayout& L, uint32_t n, uint32_t D, bool need_c
   return c.off + 256;
 }
 
+// SM count of the current device (cached per device).
 int sm_count() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
+  static std::atomic<int> cache[PerDeviceOnce::kMaxDevices];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= PerDeviceOnce::kMaxDevices) return 148;
+  int s = cache[dev].load(std::memory_order_relaxed);
+  if (s <= 0) {
+    if (cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || s <= 0) s = 148;
+    cache[dev].store(s, std::memory_order_relaxed);
   }
-  return sms;
+  return s;
 }
 
 // Blocks of `kernel` (with `threads` per block and no dynamic shared memory)
@@ -717,17 +719,26 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
   if (!d || d->face_count == 0 || !d->vertices || !d->faces_in || !d->boxes || !d->indices || !d->nodes || d->max_nodes == 0)
     return RT_ERR_INVALID_ARGUMENT;
   if (d->face_count > 0x7FFFFFFFu) return RT_ERR_INVALID_ARGUMENT;
-  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   const rt_build_params q = normalized(&d->params);
   if (q.morton_bits != 32 && q.morton_bits != 30) return RT_ERR_INVALID_ARGUMENT;
   const uint32_t n = d->face_count;
-  cudaStream_t st = (cudaStream_t)stream_;
+  // every size check comes before the first launch, so that a refused call leaves the caller's buffers untouched
+  if (d->max_nodes < 2 * n - 1) return RT_ERR_CAPACITY;
   const bool complete = q.tree_complete != 0;
   const bool in_place = complete && d->faces_out && (d->faces_out == d->faces_in);
   Carve c(d->scratch, d->scratch_bytes);
   BuildLayout L;
   carve_build(c, L, n, q.tree_depth, d->codes == nullptr, in_place);
   if (!d->scratch || !c.ok()) return RT_ERR_SCRATCH_TOO_SMALL;
+  AccelLayout AL{};
+  const bool accel = complete && d->accel && d->tris;
+  if (accel) {
+    Carve ca(d->accel, d->accel_bytes);
+    carve_accel(ca, AL, n);
+    if (!ca.ok()) return RT_ERR_SCRATCH_TOO_SMALL;
+  }
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  cudaStream_t st = (cudaStream_t)stream_;
   uint32_t* codes = d->codes ? d->codes : L.codes;
   const int sms = sm_count();
 
@@ -790,13 +801,6 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
     A.tris = complete ? (float4*)d->tris : nullptr;
     A.indices = d->indices; A.ml_lambda = L.ml_lambda; A.ml_rec = L.ml_rec; A.ml_rank = L.ml_rank; A.parent_id = L.parent_id;
     A.arrive = L.arrive; A.nodes = d->nodes; A.max_nodes = d->max_nodes; A.max_leaf = q.max_leaf; A.hdr = L.hdr; A.err = L.err;
-    AccelLayout AL{};
-    const bool accel = complete && d->accel && d->tris;
-    if (accel) {
-      Carve ca(d->accel, d->accel_bytes);
-      carve_accel(ca, AL, n);
-      if (!ca.ok()) return RT_ERR_SCRATCH_TOO_SMALL;
-    }
     A.acc_leaves = accel ? AL.leaves : nullptr;
     A.acc_groups = accel ? AL.groups : nullptr;
     A.leaf_lambda = L.leaf_lambda;
@@ -1199,7 +1203,6 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
     return RT_ERR_INVALID_ARGUMENT;
   if (d->faces_out == d->faces_in) return RT_ERR_INVALID_ARGUMENT;
   if (d->mesh_count > 65536u || d->face_count > 0x3FFFFFFFu) return RT_ERR_INVALID_ARGUMENT;
-  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   rt_build_params q = normalized(&d->params);
   if (!q.tree_complete || (q.morton_bits != 32 && q.morton_bits != 30)) return RT_ERR_INVALID_ARGUMENT;
   const uint32_t M = d->mesh_count, N = d->face_count;
@@ -1215,6 +1218,7 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
     carve_batch_accel(a, B, M, N);
     if (!a.ok()) return RT_ERR_SCRATCH_TOO_SMALL;
   }
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   B.M = M; B.N = N; B.foff = d->face_offsets; B.voff = d->vertex_offsets; B.verts = (const float4*)d->vertices;
   B.faces_in = (const uint4*)d->faces_in; B.faces_out = (uint4*)d->faces_out; B.boxes = (float4*)d->boxes;
   B.indices_out = d->indices; B.codes = d->codes; B.nodes = d->nodes; B.tris = (float4*)d->tris; B.q = q; B.info_out = d->info;

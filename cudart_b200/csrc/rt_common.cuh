@@ -8,6 +8,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <mutex>
+
 #include "../../include/rt_core.h"
 
 namespace rt {
@@ -65,6 +68,30 @@ inline rt_status cuda_status(cudaError_t e) { return e == cudaSuccess ? RT_OK : 
     cudaError_t _e = cudaGetLastError();                    \
     if (_e != cudaSuccess) return RT_ERR_CUDA;              \
   } while (0)
+
+// A host-side set-up step (cudaFuncSetAttribute, a device query) that holds per device: `run` calls `fn` the
+// first time it is reached with a given device current, remembers whether it succeeded, and answers from
+// that record afterwards. Threads that race on the first call meet at the mutex; later calls only load an atomic.
+struct PerDeviceOnce {
+  static constexpr int kMaxDevices = 64;
+  std::atomic<int> state[kMaxDevices];  // 0 not yet, 1 done, -1 failed (static storage: zero-initialized)
+  std::mutex mu;
+  template <typename F>
+  bool run(F&& fn) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
+    int s = state[dev].load(std::memory_order_acquire);
+    if (s == 0) {
+      std::lock_guard<std::mutex> lock(mu);
+      s = state[dev].load(std::memory_order_relaxed);
+      if (s == 0) {
+        s = fn() ? 1 : -1;
+        state[dev].store(s, std::memory_order_release);
+      }
+    }
+    return s == 1;
+  }
+};
 
 // Number of kernels this library has launched (process-wide); exported as
 // rt_launch_count() so that a caller can count the kernels inside a timed region.

@@ -32,6 +32,12 @@ using namespace tc;
 constexpr uint32_t kBM = 128, kBK = 64, kStages = 4;
 constexpr uint32_t kTileA = kBM * kBK * 2;  // 16 KB per A stage
 
+// Four bf16 values as one 8-byte word, the first at the lowest address (an 8-byte store writes them in order).
+__device__ __forceinline__ uint2 pack_bf16x4(__nv_bfloat16 a, __nv_bfloat16 b, __nv_bfloat16 c, __nv_bfloat16 d) {
+  return make_uint2((uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16),
+                    (uint32_t)__bfloat16_as_ushort(c) | ((uint32_t)__bfloat16_as_ushort(d) << 16));
+}
+
 int num_sms() {
   int dev = 0, n = 148;
   cudaGetDevice(&dev);
@@ -901,7 +907,7 @@ __global__ __launch_bounds__(256) void k_adam_t4(float* __restrict__ p, const fl
         h[k] = __float2bfloat16_rn(pv[k]);
         tile[lr_][lc + k] = h[k];
       }
-      if (out16) *(uint2*)(out16 + (size_t)r * ld16 + c) = *(const uint2*)h;
+      if (out16) *(uint2*)(out16 + (size_t)r * ld16 + c) = pack_bf16x4(h[0], h[1], h[2], h[3]);
     }
   }
   __syncthreads();
@@ -912,7 +918,7 @@ __global__ __launch_bounds__(256) void k_adam_t4(float* __restrict__ p, const fl
 #pragma unroll
       for (int k = 0; k < 4; ++k) h[k] = tile[lr_ + k][lc];
       const uint32_t q = r / group_rows;
-      *(uint2*)(out16t + ((size_t)q * cols + c) * ld16t + (r - q * group_rows)) = *(const uint2*)h;
+      *(uint2*)(out16t + ((size_t)q * cols + c) * ld16t + (r - q * group_rows)) = pack_bf16x4(h[0], h[1], h[2], h[3]);
     }
   }
 }
@@ -1394,10 +1400,48 @@ size_t argmax_smem(uint32_t num_k, uint32_t n) {
   return 1024 + num_k * (size_t)kTileA + kStages * (size_t)kArgTileB + (size_t)n * 4 + kBM * sizeof(Top2) + 256;
 }
 
+// Self-test of the bounded-wait path that every tensor-core kernel above takes when a copy or an MMA never
+// completes: one warp allocates 32 TMEM columns, waits on a barrier that nothing arrives at for limit_ns,
+// records the outcome, releases the TMEM and returns. Nothing is in flight while it waits.
+__global__ void __launch_bounds__(32, 1) k_wait_selftest(unsigned long long limit_ns, uint32_t* err, uint32_t* result) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t slot;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  tmem_alloc(&slot, 32);
+  tmem_relinquish();
+  tc_fence_before();
+  __syncwarp();
+  tc_fence_after();
+  const uint32_t tmem = slot;
+  const unsigned long long t0 = global_ns();
+  const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar, 0, err, limit_ns));
+  const unsigned long long t1 = global_ns();
+  if (threadIdx.x == 0) {
+    result[0] = ok ? 1u : 0u;
+    result[1] = (uint32_t)((t1 - t0) / 1000ull);
+  }
+  tc_fence_before();
+  __syncwarp();
+  tmem_dealloc(tmem, 32);
+}
+
 }  // namespace
 }  // namespace rt
 
 using namespace rt;
+
+extern "C" rt_status rt_tc_wait_selftest(uint32_t limit_us, uint32_t* error_word, uint32_t* result, rt_stream stream) {
+  if (!error_word || !result || limit_us == 0 || limit_us > 2000000u) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  k_wait_selftest<<<1, 32, 0, (cudaStream_t)stream>>>(1000ull * limit_us, error_word, result);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
 
 extern "C" uint32_t rt_propose_abi_version(void) { return RT_PROPOSE_ABI_VERSION; }
 
@@ -1426,8 +1470,9 @@ extern "C" rt_status rt_gemm_bf16(const rt_gemm_desc* d, rt_stream stream) {
   E.c16_v8 = (d->c_bf16 && d->ldc_bf16 % 16 == 0 && ((uintptr_t)d->c_bf16 & 31u) == 0) ? 1u : 0u;
   const uint32_t num_k = d->k / kBK, stages = num_k < kStages ? num_k : kStages;
   const size_t smem = gemm_smem(bn, stages);
-  static std::once_flag once;
-  std::call_once(once, [] { cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem(256)); });
+  static PerDeviceOnce once;
+  if (!once.run([] { return cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem(256)) == cudaSuccess; }))
+    return RT_ERR_CUDA;
   dim3 grid(d->n / bn, d->m / kBM, G);
   k_gemm_tc<<<grid, 128, smem, (cudaStream_t)stream>>>(ta, tb, E, bn, pow2_cols(bn), num_k, stages, d->error_word);
   note_launch();
@@ -1447,10 +1492,12 @@ extern "C" rt_status rt_gemm_argmax_bf16(const rt_gemm_argmax_desc* d, rt_stream
   CUtensorMap ta, tb;
   if (!make_map(&ta, d->a, d->k, G * d->m, d->lda, kBM) || !make_map(&tb, d->b, d->k, G * d->n, d->ldb, kArgBN)) return RT_ERR_UNSUPPORTED;
   const uint32_t num_k = d->k / kBK;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    cudaFuncSetAttribute(k_gemm_argmax_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)argmax_smem(4, kArgMaxN));
-  });
+  static PerDeviceOnce once;
+  if (!once.run([] {
+        return cudaFuncSetAttribute(k_gemm_argmax_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)argmax_smem(4, kArgMaxN)) ==
+               cudaSuccess;
+      }))
+    return RT_ERR_CUDA;
   k_gemm_argmax_tc<<<dim3(d->m / kBM, G), kArgThreads, argmax_smem(num_k, d->n), (cudaStream_t)stream>>>(
       ta, tb, d->bias, d->n, d->m, num_k, d->min_margin, d->out_index, d->out_value, d->out_margin, d->error_word);
   note_launch();
@@ -1476,10 +1523,12 @@ extern "C" rt_status rt_gemm_xent_bf16(const rt_gemm_xent_desc* d, rt_stream str
   X.err = d->error_word;
   X.g32 = (d->ldg % 16 == 0 && ((uintptr_t)d->g & 31u) == 0) ? 1u : 0u;
   const uint32_t num_k = d->k / kBK;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    cudaFuncSetAttribute(k_gemm_xent_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xent_smem(4, kArgMaxN));
-  });
+  static PerDeviceOnce once;
+  if (!once.run([] {
+        return cudaFuncSetAttribute(k_gemm_xent_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xent_smem(4, kArgMaxN)) ==
+               cudaSuccess;
+      }))
+    return RT_ERR_CUDA;
   k_gemm_xent_tc<<<dim3(d->m / kBM, G), kXentThreads, xent_smem(num_k, d->n), (cudaStream_t)stream>>>(ta, tb, X, num_k);
   note_launch();
   RT_CHECK_LAUNCH();
@@ -1510,11 +1559,14 @@ extern "C" rt_status rt_mlp_propose(const rt_mlp_propose_desc* d, rt_stream stre
   P.group_rows = G > 1 ? d->group_rows : P.tiles * kBM;
   P.min_margin = d->min_margin; P.out_idx = d->out_index; P.out_val = d->out_value; P.out_margin = d->out_margin; P.err = d->error_word;
   P.tmax = d->tmax;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    cudaFuncSetAttribute(k_mlp_propose_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fuse_smem());
-    cudaFuncSetAttribute(k_mlp_propose_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fuse_smem());
-  });
+  static PerDeviceOnce once;
+  if (!once.run([] {
+        return cudaFuncSetAttribute(k_mlp_propose_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fuse_smem()) ==
+                   cudaSuccess &&
+               cudaFuncSetAttribute(k_mlp_propose_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fuse_smem()) ==
+                   cudaSuccess;
+      }))
+    return RT_ERR_CUDA;
   const uint32_t grid = (uint32_t)hmin<uint32_t>(P.tiles, (uint32_t)num_sms());
   if (d->out_margin || d->min_margin > 0.0f)
     k_mlp_propose_tc<true><<<grid, kFuseThreads, fuse_smem(), (cudaStream_t)stream>>>(t1, t2, t3, t4, P);

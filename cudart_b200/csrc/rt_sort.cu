@@ -242,14 +242,14 @@ __global__ void k_iota(uint32_t* v, uint32_t n) {
 
 constexpr size_t kSmallSmem = 4 * kTile * sizeof(uint32_t);
 
+// The single-block sort's 64 KB of dynamic shared memory, allowed once per device.
 bool small_smem_ready() {
-  static int done = -1;
-  if (done < 0) {
+  static PerDeviceOnce once;
+  return once.run([] {
     cudaError_t a = cudaFuncSetAttribute(k_radix_small<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmem);
     cudaError_t b = cudaFuncSetAttribute(k_radix_small<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmem);
-    done = (a == cudaSuccess && b == cudaSuccess) ? 1 : 0;
-  }
-  return done == 1;
+    return a == cudaSuccess && b == cudaSuccess;
+  });
 }
 
 }  // namespace
@@ -330,6 +330,7 @@ static uint32_t bits_of(uint32_t bit_depth) {
 extern "C" rt_status rt_radix_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t n, uint32_t bit_depth, int init_values,
                                          void* scratch, size_t scratch_bytes, rt_stream stream) {
   if (n && (!keys || !values)) return RT_ERR_INVALID_ARGUMENT;
+  if (n > (uint32_t)kTile && (!scratch || scratch_bytes < radix_scratch_bytes(n))) return RT_ERR_SCRATCH_TOO_SMALL;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   if (n == 1 && init_values) {
     k_iota<<<1, 32, 0, (cudaStream_t)stream>>>(values, 1);
@@ -342,6 +343,7 @@ extern "C" rt_status rt_radix_sort_pairs(uint32_t* keys, uint32_t* values, uint3
 
 extern "C" rt_status rt_radix_sort_keys(uint32_t* keys, uint32_t n, uint32_t bit_depth, void* scratch, size_t scratch_bytes, rt_stream stream) {
   if (n && !keys) return RT_ERR_INVALID_ARGUMENT;
+  if (n > (uint32_t)kTile && (!scratch || scratch_bytes < radix_scratch_bytes(n))) return RT_ERR_SCRATCH_TOO_SMALL;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   return radix_sort_pairs(keys, nullptr, n, 0, bits_of(bit_depth), 0, scratch, scratch_bytes, (cudaStream_t)stream, nullptr);
 }

@@ -52,14 +52,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Wait for the phase of `parity` to complete, for at most kWaitNs.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t* err) {
+// Wait for the phase of `parity` to complete, for at most limit_ns (default kWaitNs).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t* err, unsigned long long limit_ns = kWaitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   for (;;) {
     for (int i = 0; i < 256; ++i)
       if (mbar_try_wait(bar, parity)) return true;
-    if (global_ns() - t0 > kWaitNs) {
+    if (global_ns() - t0 > limit_ns) {
       if (err) atomicOr(err, (uint32_t)RT_DEVERR_WAIT_TIMEOUT);
       return false;
     }

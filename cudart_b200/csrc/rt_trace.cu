@@ -771,7 +771,9 @@ __global__ __launch_bounds__(256) void k_ray_keys(const float4* __restrict__ ori
     uint32_t m = 0;
 #pragma unroll
     for (int b = 0; b < 7; ++b) m |= ((q[0] >> b) & 1u) << (3 * b + 2) | ((q[1] >> b) & 1u) << (3 * b + 1) | ((q[2] >> b) & 1u) << (3 * b);
-    keys[r] = (oct << 21) | m;  // 3 + 21 bits: three radix passes (a finer code sorts slower than it gains)
+    // 3 + 21 bits: three radix passes (a finer code sorts slower than it gains). 0xFFFFFF is kept for the
+    // inactive rays, so an octant-7 ray in the top cell on all three axes shares the key of its neighbour cell.
+    keys[r] = min((oct << 21) | m, 0xFFFFFEu);
   }
 }
 
@@ -806,12 +808,25 @@ struct Pcg {
   }
 };
 
+// kBatch: hit_pos is a position inside the ray's own mesh of a batched build (the rays of mesh m are
+// ray_off[m] .. ray_off[m + 1]); the mesh's first face position face_off[m] is added before the triangle
+// is read. The PCG stream is the ray index either way.
+template <bool kBatch>
 __global__ __launch_bounds__(256) void k_bounce(const float4* __restrict__ tris, const float4* __restrict__ orig,
                                                const float4* __restrict__ dir, const int32_t* __restrict__ hit_pos,
                                                const float* __restrict__ hit_t, uint32_t count, uint64_t seed,
-                                               float4* __restrict__ orig_out, float4* __restrict__ dir_out, float* __restrict__ tmax_out) {
+                                               float4* __restrict__ orig_out, float4* __restrict__ dir_out, float* __restrict__ tmax_out,
+                                               const uint32_t* __restrict__ ray_off, const uint32_t* __restrict__ face_off, uint32_t M) {
   for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < count; r += gridDim.x * blockDim.x) {
-    const int32_t pos = hit_pos[r];
+    int32_t pos = hit_pos[r];
+    if (kBatch && pos >= 0) {
+      uint32_t lo = 0, hi = M;  // largest m with ray_off[m] <= r
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(ray_off + mid) <= r) lo = mid; else hi = mid;
+      }
+      pos += (int32_t)__ldg(face_off + lo);
+    }
     if (pos < 0) {
       orig_out[r] = make_float4(0.f, 0.f, 0.f, 0.f);
       dir_out[r] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -848,13 +863,15 @@ __global__ __launch_bounds__(256) void k_bounce(const float4* __restrict__ tris,
   }
 }
 
+// SM count of the current device (cached per device).
 int sms() {
-  static int s = 0;
-  if (!s) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, dev);
-    if (s <= 0) s = 148;
+  static std::atomic<int> cache[PerDeviceOnce::kMaxDevices];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= PerDeviceOnce::kMaxDevices) return 148;
+  int s = cache[dev].load(std::memory_order_relaxed);
+  if (s <= 0) {
+    if (cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || s <= 0) s = 148;
+    cache[dev].store(s, std::memory_order_relaxed);
   }
   return s;
 }
@@ -1038,8 +1055,25 @@ extern "C" rt_status rt_bounce_rays(const float* tris, const float* orig, const 
   if (!tris || !orig || !dir || !hit_pos || !hit_t || !orig_out || !dir_out || !tmax_out) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   const uint32_t blocks = (uint32_t)hmin<size_t>((count + 255) / 256, (size_t)sms() * 16);
-  k_bounce<<<blocks, 256, 0, (cudaStream_t)stream>>>((const float4*)tris, (const float4*)orig, (const float4*)dir, hit_pos, hit_t, count,
-                                                     seed, (float4*)orig_out, (float4*)dir_out, tmax_out);
+  k_bounce<false><<<blocks, 256, 0, (cudaStream_t)stream>>>((const float4*)tris, (const float4*)orig, (const float4*)dir, hit_pos, hit_t,
+                                                            count, seed, (float4*)orig_out, (float4*)dir_out, tmax_out, nullptr, nullptr, 0);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_batch_bounce_rays(const float* tris, const uint32_t* face_offsets, const uint32_t* ray_offsets, uint32_t mesh_count,
+                                          const float* orig, const float* dir, const int32_t* hit_pos, const float* hit_t, uint32_t count,
+                                          uint64_t seed, float* orig_out, float* dir_out, float* tmax_out, rt_stream stream) {
+  if (count == 0) return RT_OK;
+  if (!tris || !face_offsets || !ray_offsets || mesh_count == 0 || !orig || !dir || !hit_pos || !hit_t || !orig_out || !dir_out ||
+      !tmax_out)
+    return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  const uint32_t blocks = (uint32_t)hmin<size_t>((count + 255) / 256, (size_t)sms() * 16);
+  k_bounce<true><<<blocks, 256, 0, (cudaStream_t)stream>>>((const float4*)tris, (const float4*)orig, (const float4*)dir, hit_pos, hit_t,
+                                                           count, seed, (float4*)orig_out, (float4*)dir_out, tmax_out, ray_offsets,
+                                                           face_offsets, mesh_count);
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;

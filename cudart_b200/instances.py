@@ -50,9 +50,8 @@ class InstancedFrames:
         self.rays_per_instance = R
         self.orig = torch.empty((count * R, 4), dtype=torch.float32, device=self.dev)
         self.dir = torch.empty((count * R, 4), dtype=torch.float32, device=self.dev)
-        for i, c in enumerate(self.cams):
-            cam = core.make_camera(c.center, c.target, fov=c.fov, ratio=c.ratio)
-            core.primary_rays(cam, width, height, out=(self.orig[i * R:(i + 1) * R], self.dir[i * R:(i + 1) * R]))
+        self.rt_cams = [core.make_camera(c.center, c.target, fov=c.fov, ratio=c.ratio) for c in self.cams]
+        self.primary_rays()
         self.ray_offsets = torch.tensor([i * R for i in range(count + 1)], dtype=torch.int32, device=self.dev)
         self.ray_face_base = torch.repeat_interleave(torch.tensor(self.face_offsets[:-1], dtype=torch.int32, device=self.dev),
                                                      torch.full((count,), R, dtype=torch.int64, device=self.dev))
@@ -81,8 +80,16 @@ class InstancedFrames:
         self.frame_index = frame
         self.verts = scenes.displace_instances(self.base_v, self.count, frame, self.seed, self.sigma, out=self.verts)
 
-    def build(self):
-        self.tree = core.batch_build(self.verts, self.faces, self.face_offsets, self.vertex_offsets, out=self.tree)
+    def primary_rays(self):
+        """Every instance's pinhole rays (rt_primary_rays per camera) into its rows of orig / dir."""
+        R = self.rays_per_instance
+        for i, cam in enumerate(self.rt_cams):
+            core.primary_rays(cam, self.width, self.height, out=(self.orig[i * R:(i + 1) * R], self.dir[i * R:(i + 1) * R]))
+
+    def build(self, verts=None):
+        """One batched LBVH build of all instances, from `verts` (default: the displaced frame)."""
+        v = self.verts if verts is None else verts
+        self.tree = core.batch_build(v, self.faces, self.face_offsets, self.vertex_offsets, out=self.tree)
         return self.tree
 
     def make_slots(self):
@@ -90,8 +97,9 @@ class InstancedFrames:
         return self.slots
 
     def bounce(self, hits, out=None):
-        gpos = torch.where(hits["id"] >= 0, hits["id"] + self.ray_face_base, hits["id"])
-        return core.bounce_rays(self.tree.tris, self.orig, self.dir, gpos, hits["t"], 1000 + self.frame_index, out=out)
+        """One diffuse bounce per primary hit (rt_batch_bounce_rays: hit ids are instance-local positions)."""
+        return core.batch_bounce_rays(self.tree, self.ray_offsets, self.orig, self.dir, hits["id"], hits["t"], 1000 + self.frame_index,
+                                      out=out)
 
     def tune(self):
         """Pick the batched traversal schedule on this frame's primary rays (untimed)."""

@@ -18,6 +18,9 @@ steady-state launch. Cases (kernel of interest in brackets):
   raster         rasteriser, 2^20-face soup, 1920x1080                           [k_raster_zones, k_raster_emit]
   mlp_grouped    64 grouped networks: 3 training steps of 1024 rays each,        [k_gemm_tc, k_softmax_xent, ...]
                  then proposals for 64 x 518,400 rays
+  c4_frame [M]   M (default 64) deformed instances of the 1/16-size learned       [launch list, k_batch_trace_coop]
+                 scene, three frames of the plain path: batched build, primary
+                 rays, batched trace, bounce rays, batched trace
 """
 from __future__ import annotations
 
@@ -159,12 +162,26 @@ def mlp_grouped():
     torch.cuda.synchronize()
 
 
+def c4_frame(count: int = 64):
+    """Three frames of the instanced workload's plain path with the schedule the tuner picks on it."""
+    from .instances import InstancedFrames
+    w = InstancedFrames(count, 1 / 16, 960, 540)
+    w.schedule = dict(while_while=True, wide=True, persistent=True, blocks_per_sm=8, coop=True)
+    plain = None
+    for f in range(3):
+        w.displace(f)
+        w.build()
+        w.primary_rays()
+        plain = w.trace_plain(out=plain)
+    torch.cuda.synchronize()
+
+
 CASES = {"bench_step": bench_step, "build_16m": build_16m, "batch_build": batch_build, "trace_primary": trace_primary, "trace_bounce": trace_bounce, "mlp_propose": mlp_propose, "mlp_train": mlp_train,
-         "sah_build": sah_build, "raster": raster, "mlp_grouped": mlp_grouped}
+         "sah_build": sah_build, "raster": raster, "mlp_grouped": mlp_grouped, "c4_frame": c4_frame}
 
 if __name__ == "__main__":
-    if len(sys.argv) != 2 or sys.argv[1] not in CASES:
-        raise SystemExit("usage: python -m cudart_b200.profile_cases {" + ",".join(CASES) + "}")
+    if len(sys.argv) not in (2, 3) or sys.argv[1] not in CASES:
+        raise SystemExit("usage: python -m cudart_b200.profile_cases {" + ",".join(CASES) + "} [size]")
     torch.cuda.set_device(0)
-    CASES[sys.argv[1]]()
+    CASES[sys.argv[1]](*(int(a) for a in sys.argv[2:]))
     print("ok", sys.argv[1])

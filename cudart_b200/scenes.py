@@ -233,3 +233,39 @@ def sphere_rays(mesh: Mesh, side: int, seed: int):
     orig[:, :3] = o
     dirs[:, :3] = d
     return orig, dirs
+
+
+def batch_sphere_rays_torch(meshes, seed_sides: int = 11, seed_rays: int = 5, min_side: int = 64, max_side: int = 512,
+                            device="cuda"):
+    """Ray sets of a batch of meshes: mesh m gets side x side rays (side log-uniform in [min_side, max_side],
+    numpy PCG64 seeded by seed_sides) with origins uniform on its bounding sphere (centre of its vertex box,
+    radius 1.01 x the farthest vertex), each aimed at a uniform point inside that sphere; drawn in float64 on
+    the device from a generator seeded by seed_rays. Returns (orig, dir, ray_offsets) with ray_offsets an
+    int64 numpy array of mesh_count + 1 entries."""
+    import torch
+
+    count = len(meshes)
+    rng = np.random.default_rng(seed_sides)
+    sides = np.exp(rng.uniform(math.log(min_side), math.log(max_side), count)).astype(np.int64)
+    counts = sides * sides
+    ro = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    centers, radii = [], []
+    for m in meshes:
+        v = m.vertices[:, :3].astype(np.float64)
+        c = 0.5 * (v.min(0) + v.max(0))
+        centers.append(c)
+        radii.append(max(float(np.linalg.norm(v - c, axis=1).max()), 1e-6) * 1.01)
+    R = int(ro[-1])
+    mesh_of_ray = torch.repeat_interleave(torch.arange(count, device=device), torch.from_numpy(counts).to(device))
+    cen = torch.tensor(np.array(centers), dtype=torch.float64, device=device)[mesh_of_ray]
+    rad = torch.tensor(radii, dtype=torch.float64, device=device)[mesh_of_ray].unsqueeze(1)
+    g = torch.Generator(device=device).manual_seed(seed_rays)
+    p = torch.randn((R, 3), generator=g, device=device, dtype=torch.float64)
+    p = p / p.norm(dim=1, keepdim=True)
+    q = torch.randn((R, 3), generator=g, device=device, dtype=torch.float64)
+    q = q / q.norm(dim=1, keepdim=True) * torch.rand((R, 1), generator=g, device=device, dtype=torch.float64).pow(1.0 / 3.0)
+    orig = torch.zeros((R, 4), dtype=torch.float32, device=device)
+    dirs = torch.zeros((R, 4), dtype=torch.float32, device=device)
+    orig[:, :3] = (cen + rad * p).float()
+    dirs[:, :3] = ((cen + rad * q) - (cen + rad * p)).float()
+    return orig, dirs, ro

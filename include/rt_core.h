@@ -85,7 +85,7 @@ typedef struct rt_build_desc {
   uint32_t* indices;        /* uint[N]: position -> original face id (CUDAMeshTree::indices) */
   uint32_t* codes;          /* uint[N]: sorted Morton codes; NULL = kept in scratch */
   uint32_t* nodes;          /* bvnode[max_nodes] (CUDAMeshTree::nodes) */
-  uint32_t max_nodes;       /* >= rt_lbvh_scratch_bytes' max_nodes guarantees no overflow */
+  uint32_t max_nodes;       /* >= 2N - 1 (rt_lbvh_scratch_bytes' max_nodes); smaller: RT_ERR_CAPACITY before any launch */
   float* tris;              /* float4[3N] {v0, v1 - v0, v2 - v0} per position (w = 0); NULL = not produced */
   rt_build_info* info;      /* device pointer, may be NULL */
   void* scratch;
@@ -303,6 +303,14 @@ rt_status rt_interpolate(const rt_interp_desc* desc, rt_stream stream);
  * incoherent scene; no reference counterpart. */
 rt_status rt_bounce_rays(const float* tris, const float* orig, const float* dir, const int32_t* hit_pos, const float* hit_t,
                          uint32_t ray_count, uint64_t seed, float* orig_out, float* dir_out, float* tmax_out, rt_stream stream);
+/* rt_bounce_rays for the rays of a batched build: hit_pos holds positions inside
+ * each ray's own mesh (rt_batch_trace, id_mode 0), the rays of mesh m being
+ * ray_offsets[m] .. ray_offsets[m+1] (DEVICE, mesh_count + 1 entries), and
+ * face_offsets (DEVICE, as given to rt_batch_build) place each mesh in tris.
+ * Same rays as rt_bounce_rays given the global positions. No reference counterpart. */
+rt_status rt_batch_bounce_rays(const float* tris, const uint32_t* face_offsets, const uint32_t* ray_offsets, uint32_t mesh_count,
+                               const float* orig, const float* dir, const int32_t* hit_pos, const float* hit_t, uint32_t ray_count,
+                               uint64_t seed, float* orig_out, float* dir_out, float* tmax_out, rt_stream stream);
 
 /* Mesh and tree chunk files (HOST calls; arrays may be device or host memory).
  * Same bytes as CUDAMesh::quickSave / CUDAMeshTree::quickSave with

@@ -141,6 +141,14 @@ typedef struct rt_gemm_xent_desc {
 } rt_gemm_xent_desc;
 rt_status rt_gemm_xent_bf16(const rt_gemm_xent_desc* d, rt_stream stream);
 
+/* Self-test of the bounded waits of the tensor-core kernels: one warp
+ * allocates 32 TMEM columns, waits on a shared-memory barrier that nothing
+ * arrives at for limit_us microseconds (1 .. 2,000,000), then releases the TMEM
+ * and returns. Results (DEVICE): RT_DEVERR_WAIT_TIMEOUT is OR-ed into
+ * *error_word; result[0] = 1 if the wait completed (it cannot), else 0;
+ * result[1] = microseconds the kernel waited. The context stays usable. */
+rt_status rt_tc_wait_selftest(uint32_t limit_us, uint32_t* error_word, uint32_t* result, rt_stream stream);
+
 /* Ray features: u = ((o - c) * 2 / (hi - lo), d / |d|), c = (lo + hi) / 2;
  * f[24 i + 2 j] = sin(pi 2^j u_i), f[24 i + 2 j + 1] = cos(pi 2^j u_i), j < 12;
  * columns 144 .. 191 are zero. out: BF16 [count][ld_out] (ld_out >= 192, a

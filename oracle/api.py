@@ -300,6 +300,11 @@ def max_threads() -> int:
     return int(lib().or_max_threads())
 
 
+def set_threads(n: int) -> None:
+    """Thread count of the oracle's parallel loops (n <= 0: all processors)."""
+    lib().or_set_threads(C.c_int(n))
+
+
 # ----------------------------------------------------------------------------
 # reference checker wrappers (functions compiled from the reference sources)
 # ----------------------------------------------------------------------------

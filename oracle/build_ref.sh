@@ -16,13 +16,13 @@
 # ref_mesh_quick_load, ref_tree_quick_save, ref_sah_build, ref_raster_matrix,
 # ref_rasterize. TEST INFRASTRUCTURE ONLY.
 #
-# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+# Usage: oracle/build_ref.sh [reference_root]   (default: $CUDART_REFERENCE)
 set -euo pipefail
-REF="${1:-/root/reference}"
+REF="${1:-${CUDART_REFERENCE:-}}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 SHIM="$HERE/ref_shim"
 OUT="$HERE/_ref"
-if [ ! -d "$REF/kernels" ]; then
+if [ -z "$REF" ] || [ ! -d "$REF/kernels" ]; then
   echo "build_ref.sh: reference not found at $REF; skipping" >&2
   exit 0
 fi

@@ -1054,3 +1054,13 @@ OR_API int or_max_threads() {
   return 1;
 #endif
 }
+
+// Thread count of every parallel oracle loop that takes no explicit count (the
+// CPU baseline times the build with one thread and with all of them).
+OR_API void or_set_threads(int n) {
+#ifdef _OPENMP
+  omp_set_num_threads(n > 0 ? n : omp_get_num_procs());
+#else
+  (void)n;
+#endif
+}

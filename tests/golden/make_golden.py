@@ -19,8 +19,8 @@ reference's own functions, compiled from its sources by oracle/build_ref.sh
                   Internal nodes keep only bits 0-2 of their first word (the
                   reference leaves the rest unset).
 
-Run:  python tests/golden/make_golden.py [sah]   (needs /root/reference and a built oracle/_ref;
-      "sah" writes sah.npz only)
+Run:  CUDART_REFERENCE=<reference tree> make -C oracle   (builds oracle/_ref from the reference's sources)
+      python tests/golden/make_golden.py [sah]           ("sah" writes sah.npz only)
 """
 import hashlib
 import os

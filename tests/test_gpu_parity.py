@@ -394,3 +394,32 @@ def test_batch_build_and_trace_match_single_mesh(T, oracle):
         T.cuda.synchronize()
         assert int(_host(h["err"])[0]) == 0, sch
         assert T.equal(h["id"], hits["id"]) and T.equal(h["t"], hits["t"]) and T.equal(h["uv"], hits["uv"]), sch
+
+
+def test_ray_order_puts_inactive_rays_last(T):
+    """rt_ray_order returns a permutation of the rays with the active ones grouped by direction octant
+    (ascending) and the inactive ones (tmax <= 0) strictly last, also beside an octant-7 ray whose origin is
+    the box's max corner, the largest key an active ray can have."""
+    from cudart_b200 import core
+    rng = np.random.default_rng(12)
+    R = 5000
+    o = np.zeros((R, 4), np.float32)
+    d = np.zeros((R, 4), np.float32)
+    o[:, :3] = rng.uniform(0.0, 1.0, (R, 3))
+    d[:, :3] = rng.normal(size=(R, 3))
+    tmax = np.full(R, 3.0e38, np.float32)
+    tmax[::3] = -1.0
+    tmax[7::11] = 0.0
+    for r in (5, 17, 4999):  # active, octant 7, origin at the max corner
+        o[r, :3] = 1.0
+        d[r, :3] = -1.0
+        tmax[r] = 3.0e38
+    tmax[6] = tmax[18] = -1.0
+    order = _host(core.ray_order(_dev(T, o), _dev(T, d), _dev(T, tmax), [0.0, 0.0, 0.0, 1.0, 1.0, 1.0])).astype(np.int64)
+    assert np.array_equal(np.sort(order), np.arange(R))
+    active = tmax[order] > 0
+    n_act = int((tmax > 0).sum())
+    assert active[:n_act].all() and not active[n_act:].any()
+    dd = d[order[:n_act]]
+    oct_ = (dd[:, 0] < 0).astype(int) | 2 * (dd[:, 1] < 0) | 4 * (dd[:, 2] < 0)
+    assert np.all(np.diff(oct_) >= 0)

@@ -79,3 +79,28 @@ def test_static_sort_rejects_oversize():
     status = lib.rt_radix_sort_pairs_static(C.c_void_p(k.data_ptr()), C.c_void_p(k.data_ptr()), max_n + 1, 32, 0, None)
     assert status == 5  # RT_ERR_CAPACITY
     assert lib.rt_status_string(status) == b"capacity exceeded"
+
+
+def test_static_sort_sizes_that_skip_the_scratch():
+    """Sizes whose sort never touches the shared array: one key (only the values may be set) and up to one
+    4096-key tile (a single-block sort in shared memory), plus 4097 keys, the first size that uses the array;
+    each compared exactly with rt_radix_sort_pairs."""
+    import torch
+    from cudart_b200 import _abi
+    lib = _abi.lib()
+    lib.rt_radix_sort_pairs_static.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_int, C.c_void_p]
+    lib.rt_radix_sort_pairs_static.restype = C.c_int
+    rng = np.random.default_rng(7)
+    for n, bits, init in ((1, 32, True), (1, 32, False), (4096, 32, True), (4096, 8, False), (4097, 21, True), (4097, 32, False)):
+        keys = rng.integers(0, 1 << bits, n, dtype=np.int64).astype(np.uint32).view(np.int32)
+        vals = rng.integers(1, 1 << 31, n, dtype=np.int64).astype(np.int32)  # nonzero: an unset value would show
+        k_ref = torch.from_numpy(keys.copy()).cuda()
+        v_ref = torch.from_numpy(vals.copy()).cuda()
+        k_new, v_new = k_ref.clone(), v_ref.clone()
+        _sort_with_scratch(lib, torch, k_ref, v_ref, bits, init)
+        assert _sort_static(lib, torch, k_new, v_new, bits, init) == 0
+        torch.cuda.synchronize()
+        assert torch.equal(k_new, k_ref), (n, bits, init)
+        assert torch.equal(v_new, v_ref), (n, bits, init)
+        if init:
+            assert torch.equal(torch.sort(v_new.long()).values, torch.arange(n, device="cuda")), (n, bits)
