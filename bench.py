@@ -236,7 +236,7 @@ def run_headline(args, rank, world, local_rank):
     w.displace(0)
     w.build()
     w.make_slots()
-    sched, tim = w.tune()  # untimed; results never depend on the schedule
+    (s1, s2), (tim1, tim2) = w.tune()  # untimed; results never depend on the schedules
     plain = w.trace_plain()
     torch.cuda.synchronize()
     R = w.ray_count
@@ -245,11 +245,11 @@ def run_headline(args, rank, world, local_rank):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
     def trace1():
-        core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, out=plain["h1"], schedule=sched)
+        core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, out=plain["h1"], schedule=s1)
 
     def trace2():
         b = plain["b"]
-        core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], out=plain["h2"], schedule=sched)
+        core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], out=plain["h2"], schedule=s2)
 
     stages = [lambda: w.build(), w.primary_rays, trace1, lambda: w.bounce(plain["h1"], out=plain["b"]), trace2]
     graphs, kernels_per_step = capture_graphs(stages)
@@ -298,18 +298,19 @@ def run_headline(args, rank, world, local_rank):
 
     # counted launches (untimed) of the last frame's rays: box records read and triangles tested per ray
     b = plain["b"]
-    c1 = core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, counters=True, schedule=sched)
-    c2 = core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], counters=True, schedule=sched)
+    c1 = core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, counters=True, schedule=s1)
+    c2 = core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], counters=True, schedule=s2)
     torch.cuda.synchronize()
     same = torch.equal(c1["id"], plain["h1"]["id"]) and torch.equal(c2["id"], plain["h2"]["id"])
     m1 = 48 * R + 32 * int(c1["visits"].sum().item()) + 48 * int(c1["tests"].sum().item())
     m2 = 48 * R + 32 * int(c2["visits"].sum().item()) + 48 * int(c2["tests"].sum().item())
     del c1, c2
     peak, peak_kind = load_peaks()
-    kname = batch_kernel(sched)
     if t1_ms >= t2_ms:
+        kname = batch_kernel(s1)
         roof = trace_roofline(kname, "primary", m1, t1_ms / K, R, peak, peak_kind, f"c4:{kname}:primary")
     else:
+        kname = batch_kernel(s2)
         roof = trace_roofline(kname, "bounce", m2, t2_ms / K, R, peak, peak_kind, f"c4:{kname}:bounce")
     # build: algorithmic bytes per face = 16 face + 48 vertices + 32 box + 8 code/index + 64 sort + 4 split scan
     # + 32 leaf gather + 36 reorder + 48 triangle stream, + 64 per node (write + child read)
@@ -332,8 +333,9 @@ def run_headline(args, rank, world, local_rank):
     clocks = clk.summary()
     result["clocks"] = {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
                         "samples": clocks["samples"]}
-    legs = {"c4_tuning": {"ms": {json.dumps(k, sort_keys=True): round(v, 3) for k, v in tim}},
-            "c4_detail": {"workload": WORKLOAD, "schedule": sched, "counted_identical": bool(same), "device_errors": dev_errors,
+    legs = {"c4_tuning": {"primary_ms": {json.dumps(k, sort_keys=True): round(v, 3) for k, v in tim1},
+                          "bounce_ms": {json.dumps(k, sort_keys=True): round(v, 3) for k, v in tim2}},
+            "c4_detail": {"workload": WORKLOAD, "schedule_primary": s1, "schedule_bounce": s2, "counted_identical": bool(same), "device_errors": dev_errors,
                           "nodes": nodes_total, "build_bytes": int(build_bytes), "rays_ms": round(rays_ms / K, 3),
                           "primary_hits_last": hits1, "active_bounces_last": active_last, "kernels_per_frame": kernels_per_step,
                           "graphs": "5 CUDA graph replays per frame: build, primary rays, trace, bounce rays, trace",
@@ -346,7 +348,7 @@ def run_headline(args, rank, world, local_rank):
         result["nn_over_plain"] = nn["nn_over_plain"]
         result["nn"] = {k: nn[k] for k in ("bit_exact", "proposal_accuracy", "oracle_seeded_over_plain")}
     if not args.no_e2e:
-        e2e = run_e2e(w, args, dev, world, sched)
+        e2e = run_e2e(w, args, dev, world, s1, s2)
         legs["c4_e2e"] = e2e
         result["e2e"] = {k: e2e[k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step", "ms_per_step")}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -387,13 +389,13 @@ def learned_frames(w, args, dev, world, plain, first_frame):
         learned["p1"] = w.nets.propose(w.orig, w.dir, w.box, R, out=learned["p1"])
         e[3].record()
         proposal.batch_trace_seeded(w.tree, w.orig, w.dir, w.ray_offsets, learned["p1"], w.slots, in_proposal=True,
-                                    out=learned["h1"], schedule=w.schedule)
+                                    out=learned["h1"], schedule=w.schedule_primary)
         e[4].record()
         b = plain["b"]  # the seeded hits equal the plain ones, so the bounces are the same rays
         learned["p2"] = w.nets.propose(b[0], b[1], w.box, R, out=learned["p2"], tmax=b[2])
         e[5].record()
         proposal.batch_trace_seeded(w.tree, b[0], b[1], w.ray_offsets, learned["p2"], w.slots, tmax=b[2], in_proposal=True,
-                                    out=learned["h2"], schedule=w.schedule)
+                                    out=learned["h2"], schedule=w.schedule_bounce)
         e[6].record()
         for k in ("h1", "h2"):
             mism += (plain[k]["id"] != learned[k]["id"]).sum() + (plain[k]["t"].view(torch.int32) != learned[k]["t"].view(torch.int32)).sum()
@@ -414,9 +416,9 @@ def learned_frames(w, args, dev, world, plain, first_frame):
     torch.cuda.synchronize()
     o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     o0.record()
-    proposal.batch_trace_seeded(w.tree, w.orig, w.dir, w.ray_offsets, l1, w.slots, out=learned["h1"], schedule=w.schedule)
+    proposal.batch_trace_seeded(w.tree, w.orig, w.dir, w.ray_offsets, l1, w.slots, out=learned["h1"], schedule=w.schedule_primary)
     b = plain["b"]
-    proposal.batch_trace_seeded(w.tree, b[0], b[1], w.ray_offsets, l2, w.slots, tmax=b[2], out=learned["h2"], schedule=w.schedule)
+    proposal.batch_trace_seeded(w.tree, b[0], b[1], w.ray_offsets, l2, w.slots, tmax=b[2], out=learned["h2"], schedule=w.schedule_bounce)
     o1.record()
     torch.cuda.synchronize()
     oracle_ms = o0.elapsed_time(o1)
@@ -429,7 +431,7 @@ def learned_frames(w, args, dev, world, plain, first_frame):
             "note": "nn = grouped MLP proposals + seeded traversal of primaries and bounces; fine-tuning reported apart"}
 
 
-def run_e2e(w, args, dev, world, sched):
+def run_e2e(w, args, dev, world, s1, s2):
     """The headline metric through the public API with host buffers, as a frame pipeline: every frame copies
     the 64 instances' displaced vertices from pinned host memory, builds, makes the primary rays, traces them
     and their bounces, and copies every hit (id, t, u, v of primaries and bounces) back to pinned host memory.
@@ -458,9 +460,9 @@ def run_e2e(w, args, dev, world, sched):
         w.build(v[s])
         w.primary_rays()
         o = outs[s]
-        core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, out=o["h1"], schedule=sched)
+        core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, out=o["h1"], schedule=s1)
         w.bounce(o["h1"], out=o["b"])
-        core.batch_trace(w.tree, o["b"][0], o["b"][1], w.ray_offsets, tmax=o["b"][2], out=o["h2"], schedule=sched)
+        core.batch_trace(w.tree, o["b"][0], o["b"][1], w.ray_offsets, tmax=o["b"][2], out=o["h2"], schedule=s2)
 
     graphs, _ = capture_graphs([lambda: compute(0), lambda: compute(1)])
 

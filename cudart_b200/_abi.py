@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librt_core.so")
 
 RT_OK = 0
-ABI_VERSION = 6  # RT_ABI_VERSION of include/rt_core.h that the structs below mirror
+ABI_VERSION = 7  # RT_ABI_VERSION of include/rt_core.h that the structs below mirror
 STATUS_NAMES = {0: "RT_OK", 1: "RT_ERR_INVALID_ARGUMENT", 2: "RT_ERR_NO_DEVICE", 3: "RT_ERR_CUDA",
                 4: "RT_ERR_SCRATCH_TOO_SMALL", 5: "RT_ERR_CAPACITY", 6: "RT_ERR_UNSUPPORTED"}
 DEVERR_NODE_CAPACITY = 0x1
@@ -29,7 +29,8 @@ TRACE_WIDE = 0x4
 EXPORTS = (
     "rt_lbvh_scratch_bytes", "rt_lbvh_accel_bytes", "rt_lbvh_build", "rt_batch_sizes", "rt_batch_build", "rt_batch_trace", "rt_mesh_boxes", "rt_reorder_faces", "rt_sort_scratch_bytes",
     "rt_radix_sort_pairs", "rt_radix_sort_pairs_static", "rt_radix_sort_keys", "rt_camera_look_at", "rt_camera_basis", "rt_primary_rays",
-    "rt_trace_closest", "rt_ray_order_scratch_bytes", "rt_ray_order", "rt_interpolate", "rt_bounce_rays", "rt_batch_bounce_rays", "rt_mesh_file_save", "rt_mesh_file_info", "rt_mesh_file_load", "rt_tree_file_save", "rt_tree_file_info",
+    "rt_trace_closest", "rt_ray_order_scratch_bytes", "rt_ray_order", "rt_batch_ray_order_scratch_bytes", "rt_batch_ray_order",
+    "rt_image_tile_order", "rt_interpolate", "rt_bounce_rays", "rt_batch_bounce_rays", "rt_mesh_file_save", "rt_mesh_file_info", "rt_mesh_file_load", "rt_tree_file_save", "rt_tree_file_info",
     "rt_tree_file_load", "rt_status_string", "rt_version", "rt_abi_version", "rt_device_check", "rt_launch_count",
 )
 # every symbol include/rt_sah.h declares
@@ -105,7 +106,7 @@ class BatchTraceDesc(C.Structure):
     _fields_ = [("mesh_count", _U32), ("face_offsets", _P), ("ray_offsets", _P), ("accel", _P), ("tris", _P), ("indices", _P),
                 ("face_count", _U32), ("orig", _P), ("dir", _P), ("tmax", _P), ("ray_count", _U32), ("id_mode", _U32),
                 ("hit_id", _P), ("hit_t", _P), ("hit_uv", _P), ("ray_visits", _P), ("ray_tests", _P), ("error_word", _P),
-                ("schedule", _U32), ("work_counter", _P), ("persistent_blocks_per_sm", _U32)]
+                ("schedule", _U32), ("work_counter", _P), ("persistent_blocks_per_sm", _U32), ("ray_order", _P)]
 
 
 class SahDesc(C.Structure):
@@ -208,6 +209,9 @@ def lib():
         L.rt_interpolate.argtypes = [C.POINTER(InterpDesc), _P]
         L.rt_ray_order_scratch_bytes.argtypes = [_U32, C.POINTER(C.c_size_t)]
         L.rt_ray_order.argtypes = [_P, _P, _P, _U32, C.POINTER(C.c_float), _P, _P, C.c_size_t, _P]
+        L.rt_batch_ray_order_scratch_bytes.argtypes = [_U32, C.POINTER(C.c_size_t)]
+        L.rt_batch_ray_order.argtypes = [_P, _P, _P, _U32, _P, _U32, C.POINTER(C.c_float), _U32, _P, _P, C.c_size_t, _P]
+        L.rt_image_tile_order.argtypes = [_U32, _U32, _U32, _P, _P]
         L.rt_bounce_rays.argtypes = [_P, _P, _P, _P, _P, _U32, C.c_uint64, _P, _P, _P, _P]
         L.rt_batch_bounce_rays.argtypes = [_P, _P, _P, _U32, _P, _P, _P, _P, _U32, C.c_uint64, _P, _P, _P, _P]
         for fn, st in (("mesh", MeshFile), ("tree", TreeFile)):

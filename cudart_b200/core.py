@@ -589,12 +589,61 @@ def batch_build(vertices: torch.Tensor, faces: torch.Tensor, face_offsets: list,
     return out
 
 
+_TILE_ORDERS = {}
+
+
+def image_tile_order(images: int, width: int, height: int, device="cuda", stream=None) -> torch.Tensor:
+    """rt_image_tile_order: the slot -> ray permutation that gives each warp an 8 x 4 pixel tile of one of
+    `images` consecutive row-major width x height images (made once per shape and device, then reused)."""
+    dev = torch.device(device)
+    key = (dev.index or 0, images, width, height)
+    o = _TILE_ORDERS.get(key)
+    if o is None:
+        o = torch.empty(images * width * height, dtype=torch.int32, device=dev)
+        _abi.check("rt_image_tile_order", _abi.lib().rt_image_tile_order(images, width, height, _p(o), _stream(stream)))
+        _TILE_ORDERS[key] = o
+    return o
+
+
+def batch_tree_box(tree: "BatchTree"):
+    """Box around every mesh of a batched build (host floats), from the meshes' root nodes; read once and
+    cached on the tree. A tree rebuilt in place keeps the first box: it only steers the ray order."""
+    box = getattr(tree, "_box", None)
+    if box is None:
+        M = tree.mesh_count
+        F = torch.tensor(tree.face_offsets_host[:M], dtype=torch.int64, device=tree.nodes.device)
+        roots = tree.nodes[2 * F - torch.arange(M, device=F.device)].view(torch.float32)[:, 2:8].cpu()
+        ok = roots.abs().max(dim=1).values < 1e30
+        r = roots[ok] if bool(ok.any()) else tree.boxes.view(-1, 8)[:, [0, 1, 2, 4, 5, 6]].cpu()
+        box = r[:, :3].min(0).values.tolist() + r[:, 3:].max(0).values.tolist()
+        tree._box = box
+    return box
+
+
+def batch_ray_order(orig, dir, tmax, ray_offsets, mesh_count: int, box, morton_bits: int, ray_count: int | None = None, out=None,
+                    stream=None) -> torch.Tensor:
+    """rt_batch_ray_order: rays sorted by mesh, direction octant and the top `morton_bits` bits of their origin's
+    Morton code in `box`; inactive rays (tmax <= 0) last."""
+    R = orig.shape[0] if ray_count is None else ray_count
+    nb = C.c_size_t(0)
+    _abi.lib().rt_batch_ray_order_scratch_bytes(R, C.byref(nb))
+    scratch = _ORDER_SCRATCH.get(nb.value, orig.device)
+    order = torch.empty(R, dtype=torch.int32, device=orig.device) if out is None else out
+    b = (C.c_float * 6)(*box)
+    _abi.check("rt_batch_ray_order", _abi.lib().rt_batch_ray_order(_p(orig), _p(dir), _p(tmax), R, _p(ray_offsets), mesh_count, b,
+                                                                   morton_bits, _p(order), _p(scratch), scratch.numel(), _stream(stream)))
+    return order
+
+
 def batch_trace(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax=None, id_mode: int = 0, counters: bool = False,
                 while_while: bool = True, out: dict | None = None, schedule: dict | None = None, stream=None) -> dict:
     """Closest hits for the rays of all meshes (rays of mesh m: ray_offsets[m] .. ray_offsets[m+1]).
     schedule (results never depend on it): while_while, wide (4-wide records),
     persistent + blocks_per_sm (warps fetching 32 rays at a time), coop
-    (warp-cooperative leaf tests; always persistent)."""
+    (warp-cooperative leaf tests; always persistent), tiles = (images, width,
+    height) (every mesh's rays are one image: warps take 8 x 4 pixel tiles) or
+    sorted_bits (rays sorted by mesh, octant and that many bits of their
+    origin's Morton code, inactive rays last; the sort is part of the call)."""
     d, out = batch_trace_desc(tree, orig, dir, ray_offsets, tmax, id_mode, counters, while_while, out, schedule)
     _abi.check("rt_batch_trace", _abi.lib().rt_batch_trace(C.byref(d), _stream(stream)))
     return out
@@ -623,6 +672,16 @@ def batch_trace_desc(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax
     d.schedule = ((_abi.TRACE_WHILE_WHILE if sch.get("while_while", False) else 0)
                   | (_abi.TRACE_WIDE if sch.get("wide", False) else 0)
                   | (_abi.TRACE_COOP if sch.get("coop", False) else 0))
+    if sch.get("tiles"):  # every mesh's rays are a row-major image of the same size: 8 x 4 pixel tiles per warp
+        images, width, height = sch["tiles"]
+        order = image_tile_order(images, width, height, dev)
+        out["_order"] = order
+        d.ray_order = order.data_ptr()
+    elif sch.get("sorted_bits") is not None:  # sorted by mesh, octant and origin Morton code (part of the call)
+        order = batch_ray_order(orig, dir, tmax, ray_offsets, tree.mesh_count, batch_tree_box(tree), int(sch["sorted_bits"]),
+                                ray_count=R)
+        out["_order"] = order  # keep it alive until the trace has run
+        d.ray_order = order.data_ptr()
     if sch.get("persistent", False) or sch.get("coop", False):
         if "_counter" not in out:
             out["_counter"] = torch.zeros(1, dtype=torch.int32, device=dev)

@@ -762,8 +762,9 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
     note_launch();
     RT_CHECK_LAUNCH();
   }
-  // 3. sort (code, index)
-  rt_status s = radix_sort_pairs(codes, d->indices, n, 0, 32, 0, L.sort_scratch, L.sort_bytes, st, nullptr);
+  // 3. sort (code, index); the build's error word starts here, so that the sorts' bounded waits report into it
+  if (cudaMemsetAsync(L.err, 0, 16, st) != cudaSuccess) return RT_ERR_CUDA;
+  rt_status s = radix_sort_pairs(codes, d->indices, n, 0, 32, 0, L.sort_scratch, L.sort_bytes, st, nullptr, L.err);
   if (s != RT_OK) return s;
   // 4. per-level split lists
   if (cudaMemsetAsync(L.lev_count, 0, 256 * 4, st) != cudaSuccess) return RT_ERR_CUDA;
@@ -772,11 +773,10 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
     k_levels<<<blocks, 256, 0, st>>>(codes, n, L.lev, L.C);
     note_launch();
     RT_CHECK_LAUNCH();
-    s = radix_sort_pairs(L.lev, L.C, n - 1, 0, 8, 0, L.sort_scratch, L.sort_bytes, st, L.lev_count);
+    s = radix_sort_pairs(L.lev, L.C, n - 1, 0, 8, 0, L.sort_scratch, L.sort_bytes, st, L.lev_count, L.err);
     if (s != RT_OK) return s;
   }
   // 5. Morton top tree
-  if (cudaMemsetAsync(L.err, 0, 16, st) != cudaSuccess) return RT_ERR_CUDA;
   {
     TopoArgs A;
     A.C = L.C; A.lev_count = L.lev_count; A.n = n; A.D = q.tree_depth; A.min_leaf = q.min_leaf; A.max_leaf = q.max_leaf;
@@ -1229,7 +1229,8 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   k_batch_boxes_morton<<<fblocks, 256, 0, st>>>(B);
   note_launch(2);
   RT_CHECK_LAUNCH();
-  rt_status s = radix_sort_pairs(B.codes, B.idx, N, 0, 32, 0, sort_scratch, sort_bytes, st, nullptr);
+  if (cudaMemsetAsync(B.err, 0, 16, st) != cudaSuccess) return RT_ERR_CUDA;
+  rt_status s = radix_sort_pairs(B.codes, B.idx, N, 0, 32, 0, sort_scratch, sort_bytes, st, nullptr, B.err);
   if (s != RT_OK) return s;
   k_batch_meshkey<<<fblocks, 256, 0, st>>>(B);
   note_launch();
@@ -1240,7 +1241,7 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
     while (b < 64 && (1ull << b) <= maxval) ++b;
     return b > 24 ? 32u : (b + 7) / 8 * 8;
   };
-  s = radix_sort_pairs(B.mkey, B.idx, N, 0, digit_bits(M - 1), 0, sort_scratch, sort_bytes, st, nullptr);
+  s = radix_sort_pairs(B.mkey, B.idx, N, 0, digit_bits(M - 1), 0, sort_scratch, sort_bytes, st, nullptr, B.err);
   if (s != RT_OK) return s;
   if (cudaMemsetAsync(B.hist, 0, ((size_t)M * 64 + 1) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   k_batch_levels<<<fblocks, 256, 0, st>>>(B);
@@ -1248,11 +1249,10 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   note_launch(2);
   RT_CHECK_LAUNCH();
   if (N > 1) {
-    s = radix_sort_pairs(B.lev, B.C, N - 1, 0, digit_bits(64ull * (M - 1) + 32), 0, sort_scratch, sort_bytes, st, nullptr);
+    s = radix_sort_pairs(B.lev, B.C, N - 1, 0, digit_bits(64ull * (M - 1) + 32), 0, sort_scratch, sort_bytes, st, nullptr, B.err);
     if (s != RT_OK) return s;
   }
   k_batch_level_starts<<<1, 1024, 0, st>>>(B);
-  if (cudaMemsetAsync(B.err, 0, 16, st) != cudaSuccess) return RT_ERR_CUDA;
   k_batch_topo<<<M, kTopoThreads, 0, st>>>(B);
   k_batch_leaf_base<<<1, 1024, 0, st>>>(B);
   note_launch(3);

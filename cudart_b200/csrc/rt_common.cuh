@@ -102,8 +102,20 @@ void note_launch(uint32_t kernels = 1);
 void excl_scan(uint32_t* v, uint32_t n, uint32_t* sums, uint32_t* total, cudaStream_t st);
 
 // Radix sort internals shared by the build (rt_sort.cu).
+// Scratch bytes of an n-key sort (n > 4096 keys; n <= 4096 needs none): the other key and value buffers, and
+// per digit pass (at most 4) one status word per (4096-key tile, digit), a tile counter and 256 digit counts;
+// each region starts on a 256-byte boundary, plus 256 bytes of slack. radix_scratch_bytes() returns this.
+constexpr size_t radix_scratch_bytes_of(uint32_t n) {
+  const size_t tiles = ((size_t)n + 4095) / 4096;
+  const size_t a = ((size_t)n * 4 + 255) / 256 * 256;
+  return 2 * a + 4 * (4 * tiles * 256 + 4 * 64 + 4 * 256) + 256;
+}
 size_t radix_scratch_bytes(uint32_t n);
+// Stable sort of (key, value) pairs by bits [begin_bit, end_bit) of the key; digit_totals_out (device, 256 words,
+// optional) receives the digit counts of the last pass; err (device, optional) receives RT_DEVERR_WAIT_TIMEOUT
+// if a bounded wait between tiles ran out.
 rt_status radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t begin_bit, uint32_t end_bit, int init_vals,
-                           void* scratch, size_t scratch_bytes, cudaStream_t stream, uint32_t* digit_totals_out);
+                           void* scratch, size_t scratch_bytes, cudaStream_t stream, uint32_t* digit_totals_out,
+                           uint32_t* err = nullptr);
 
 }  // namespace rt

@@ -16,9 +16,10 @@
 // caches it per device. That first call should come before any stream capture.
 //
 // Sharing: all calls (all streams, all threads) use the same array, which keeps
-// whatever the previous call left in it. The sort writes every scratch word it
-// later reads (tile histograms, their scans, the digit totals, the ping-pong
-// key/value buffers), so nothing has to start at zero. Two calls that overlap
+// whatever the previous call left in it. Each sort first zeroes the part that
+// must start at zero (the tiles' status words, the tile counters and the digit
+// counts) and writes every other word before reading it (the ping-pong key and
+// value buffers), so a call never sees the previous call's contents. Two calls that overlap
 // on the GPU (different streams, or host threads without ordering) race on the
 // array and corrupt each other's results; callers must serialize them.
 #include <mutex>
@@ -27,11 +28,9 @@
 
 namespace {
 
-constexpr uint32_t kTile = 4096;  // keys per tile of the radix passes (rt_sort.cu)
 constexpr uint32_t kMaxN = RT_STATIC_SORT_MAX_N;
 constexpr size_t kScratchBytes = RT_STATIC_SORT_SCRATCH_BYTES;
-static_assert(kScratchBytes >= 2ull * kMaxN * 4 + (size_t)((kMaxN + kTile - 1) / kTile) * 256 * 4 + 256 * 4 + 6 * 256,
-              "static scratch too small for RT_STATIC_SORT_MAX_N keys");
+static_assert(kScratchBytes >= rt::radix_scratch_bytes_of(kMaxN), "static scratch too small for RT_STATIC_SORT_MAX_N keys");
 
 static __device__ __align__(256) unsigned char g_sort_scratch[kScratchBytes];
 

@@ -657,6 +657,8 @@ struct BatchTraceArgs {
   const uint32_t* foff;
   const uint32_t* roff;
   BatchAccel acc;
+  const uint32_t* order;  // optional slot -> ray permutation (rt_batch_ray_order, rt_image_tile_order)
+  __device__ __forceinline__ uint32_t ray_of(uint32_t s) const { return order ? __ldg(order + s) : s; }
 };
 
 // Seeded: the slot tables of mesh m start at m slot_count entries.
@@ -685,8 +687,8 @@ __device__ __forceinline__ void batch_trace_ray(uint32_t r, const TraceArgs& A, 
 
 template <bool kCount, bool kWW, bool kSeed, bool kWide>
 __global__ __launch_bounds__(128) void k_batch_trace(TraceArgs A, BatchTraceArgs B, SeedArgs S) {
-  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < A.ray_count) batch_trace_ray<kCount, kWW, kSeed, kWide>(r, A, B, S);
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < A.ray_count) batch_trace_ray<kCount, kWW, kSeed, kWide>(B.ray_of(s), A, B, S);
 }
 
 // The per-ray arguments of batched ray r: its mesh's part of the blob, triangle
@@ -725,8 +727,9 @@ __global__ __launch_bounds__(128, kSeed ? 6 : (kCount ? 0 : 7)) void k_batch_tra
     if (lane == 0) base = atomicAdd(counter, 32u);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= A.ray_count) break;
-    const uint32_t r = base + lane;
-    const bool valid = r < A.ray_count;
+    const uint32_t slot = base + lane;
+    const bool valid = slot < A.ray_count;
+    const uint32_t r = valid ? B.ray_of(slot) : slot;
     TraceArgs Am = A;
     AccelArgs C = {};
     SeedArgs Sm = S;
@@ -748,8 +751,8 @@ __global__ __launch_bounds__(128) void k_batch_trace_persistent(TraceArgs A, Bat
     if (lane == 0) base = atomicAdd(counter, 32u);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= A.ray_count) break;
-    const uint32_t r = base + lane;
-    if (r < A.ray_count) batch_trace_ray<kCount, kWW, kSeed, kWide>(r, A, B, S);
+    const uint32_t slot = base + lane;
+    if (slot < A.ray_count) batch_trace_ray<kCount, kWW, kSeed, kWide>(B.ray_of(slot), A, B, S);
   }
 }
 
@@ -774,6 +777,45 @@ __global__ __launch_bounds__(256) void k_ray_keys(const float4* __restrict__ ori
     // 3 + 21 bits: three radix passes (a finer code sorts slower than it gains). 0xFFFFFF is kept for the
     // inactive rays, so an octant-7 ray in the top cell on all three axes shares the key of its neighbour cell.
     keys[r] = min((oct << 21) | m, 0xFFFFFEu);
+  }
+}
+
+// Sort key of a batched ray: its mesh id (found in ray_offsets) above its direction octant above the top
+// `mbits` bits (a multiple of 3) of the 21-bit Morton code of its origin in `box`; inactive rays get the key of
+// a mesh id one past the last, so that they sort after every active ray.
+__global__ __launch_bounds__(256) void k_batch_ray_keys(const float4* __restrict__ orig, const float4* __restrict__ dir,
+                                                       const float* __restrict__ tmax, uint32_t count, const uint32_t* __restrict__ roff,
+                                                       uint32_t M, uint32_t mbits, float3 lo, float3 scale, uint32_t* __restrict__ keys,
+                                                       uint32_t* __restrict__ idx) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < count; r += gridDim.x * blockDim.x) {
+    idx[r] = r;
+    if (tmax && !(__ldg(tmax + r) > 0.0f)) { keys[r] = M << (3 + mbits); continue; }
+    const uint32_t m = find_seg(roff, M, r);
+    const float4 o = ldg4(orig + r), d = ldg4(dir + r);
+    const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+    uint32_t mc = 0;
+    if (mbits) {
+      uint32_t q[3];
+      const float c[3] = {(o.x - lo.x) * scale.x, (o.y - lo.y) * scale.y, (o.z - lo.z) * scale.z};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) q[a] = min(__float2uint_rz(fmaxf(c[a], 0.0f)), 511u) >> 2;  // 7 bits per axis
+#pragma unroll
+      for (int b = 0; b < 7; ++b)
+        mc |= ((q[0] >> b) & 1u) << (3 * b + 2) | ((q[1] >> b) & 1u) << (3 * b + 1) | ((q[2] >> b) & 1u) << (3 * b);
+      mc >>= 21 - mbits;
+    }
+    keys[r] = (m << (3 + mbits)) | (oct << mbits) | mc;
+  }
+}
+
+// Slot -> ray of `images` row-major width x height images stored one after the other: a warp's 32 slots are
+// an 8 x 4 pixel tile of one image, tiles in row-major order (width % 8 == 0, height % 4 == 0).
+__global__ __launch_bounds__(256) void k_image_tile_order(uint32_t total, uint32_t width, uint32_t height, uint32_t* __restrict__ order) {
+  const uint32_t per = width * height, tiles_x = width / 8;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x) {
+    const uint32_t img = s / per, k = s - img * per, tile = k >> 5, w = k & 31u;
+    const uint32_t x = (tile % tiles_x) * 8 + (w & 7u), y = (tile / tiles_x) * 4 + (w >> 3);
+    order[s] = img * per + y * width + x;
   }
 }
 
@@ -1033,6 +1075,50 @@ extern "C" rt_status rt_ray_order(const float* orig, const float* dir, const flo
   return radix_sort_pairs(keys, order, count, 0, 24, 0, sort_scratch, radix_scratch_bytes(count), st, nullptr);
 }
 
+extern "C" rt_status rt_batch_ray_order_scratch_bytes(uint32_t count, size_t* bytes) { return rt_ray_order_scratch_bytes(count, bytes); }
+
+extern "C" rt_status rt_batch_ray_order(const float* orig, const float* dir, const float* tmax, uint32_t count, const uint32_t* ray_offsets,
+                                        uint32_t mesh_count, const float box[6], uint32_t morton_bits, uint32_t* order, void* scratch,
+                                        size_t scratch_bytes, rt_stream stream) {
+  if (!orig || !dir || !order || !box || !ray_offsets || mesh_count == 0 || mesh_count > (1u << 20)) return RT_ERR_INVALID_ARGUMENT;
+  if (morton_bits > 21 || morton_bits % 3) return RT_ERR_INVALID_ARGUMENT;
+  uint32_t mesh_bits = 1;
+  while ((1u << mesh_bits) <= mesh_count) ++mesh_bits;  // ids 0 .. mesh_count (the inactive rays' id)
+  if (mesh_bits + 3 + morton_bits > 32) morton_bits = (29 - mesh_bits) / 3 * 3;  // as many Morton bits as fit in 32
+  const uint32_t key_bits = mesh_bits + 3 + morton_bits;
+  size_t need = 0;
+  rt_ray_order_scratch_bytes(count, &need);
+  if (count && (!scratch || scratch_bytes < need)) return RT_ERR_SCRATCH_TOO_SMALL;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  if (count == 0) return RT_OK;
+  Carve c(scratch, scratch_bytes);
+  uint32_t* keys = c.take<uint32_t>(count);
+  void* sort_scratch = c.take<char>(radix_scratch_bytes(count));
+  const float3 lo = make_float3(box[0], box[1], box[2]);
+  const float3 sc = make_float3(511.0f / fmaxf(box[3] - box[0], 1e-30f), 511.0f / fmaxf(box[4] - box[1], 1e-30f),
+                                511.0f / fmaxf(box[5] - box[2], 1e-30f));
+  const uint32_t blocks = (uint32_t)hmin<size_t>((count + 255) / 256, (size_t)sms() * 16);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_batch_ray_keys<<<blocks, 256, 0, st>>>((const float4*)orig, (const float4*)dir, tmax, count, ray_offsets, mesh_count, morton_bits, lo, sc,
+                                           keys, order);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return radix_sort_pairs(keys, order, count, 0, (key_bits + 7) / 8 * 8, 0, sort_scratch, radix_scratch_bytes(count), st, nullptr);
+}
+
+extern "C" rt_status rt_image_tile_order(uint32_t images, uint32_t width, uint32_t height, uint32_t* order, rt_stream stream) {
+  if (!order || width == 0 || height == 0 || width % 8 || height % 4) return RT_ERR_INVALID_ARGUMENT;
+  const uint64_t total = (uint64_t)images * width * height;
+  if (total > 0xFFFFFFFFull) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  if (total == 0) return RT_OK;
+  const uint32_t blocks = (uint32_t)hmin<uint64_t>((total + 255) / 256, (uint64_t)sms() * 16);
+  k_image_tile_order<<<blocks, 256, 0, (cudaStream_t)stream>>>((uint32_t)total, width, height, order);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
 extern "C" rt_status rt_primary_rays(const rt_camera* cam, uint32_t w, uint32_t h, float* orig, float* dir, rt_stream stream) {
   if (!cam || !orig || !dir || w == 0 || h == 0) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
@@ -1122,7 +1208,7 @@ rt_status batch_launch(const rt_batch_trace_desc* d, const SeedArgs& S, cudaStre
   A.tmax = d->tmax; A.ray_count = d->ray_count; A.id_mode = d->id_mode; A.hit_id = d->hit_id; A.hit_t = d->hit_t;
   A.hit_uv = (float2*)d->hit_uv; A.visits = d->ray_visits; A.tests = d->ray_tests; A.err = d->error_word;
   BatchTraceArgs B;
-  B.M = d->mesh_count; B.foff = d->face_offsets; B.roff = d->ray_offsets;
+  B.M = d->mesh_count; B.foff = d->face_offsets; B.roff = d->ray_offsets; B.order = d->ray_order;
   Carve c((void*)d->accel, ~(size_t)0);
   carve_batch_accel_layout(c, B.acc, d->mesh_count, d->face_count);
   const bool count = d->ray_visits || d->ray_tests;

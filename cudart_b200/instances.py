@@ -64,8 +64,18 @@ class InstancedFrames:
         self.tree = None
         self.slots = None
         self.frame_index = -1
-        self.schedule = None  # batched traversal schedule (tune() picks one); results never depend on it
+        # batched traversal schedules of the primary and bounce launches (tune() picks them); results never depend on them
+        self.schedule_primary = self.schedule_bounce = None
         self.prev = None  # (bounce orig, bounce dir, primary labels, bounce labels) of the previous frame
+
+    @property
+    def schedule(self):
+        return self.schedule_primary
+
+    @schedule.setter
+    def schedule(self, sch):
+        """One schedule for both launches."""
+        self.schedule_primary = self.schedule_bounce = sch
 
     @property
     def face_count(self) -> int:
@@ -102,17 +112,23 @@ class InstancedFrames:
                                       out=out)
 
     def tune(self):
-        """Pick the batched traversal schedule on this frame's primary rays (untimed)."""
+        """Pick the batched traversal schedules on this frame's rays (untimed): the primary launch's on the
+        primary rays (8 x 4 pixel tiles of each instance's image are a candidate), the bounce launch's on their
+        bounces (ray orders by instance, octant and origin are candidates). Returns both and their timings."""
         from . import tune
-        self.schedule, timings = tune.tune_batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, use_cache=False)
-        return self.schedule, timings
+        self.schedule_primary, t1 = tune.tune_batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, use_cache=False,
+                                                          images=(self.count, self.width, self.height))
+        h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, schedule=self.schedule_primary)
+        b = self.bounce(h1)
+        self.schedule_bounce, t2 = tune.tune_batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], use_cache=False)
+        return (self.schedule_primary, self.schedule_bounce), (t1, t2)
 
     def trace_plain(self, out=None):
         """Primary hits, bounce rays and bounce hits through rt_batch_trace."""
         out = out or {}
-        h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, out=out.get("h1"), schedule=self.schedule)
+        h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, out=out.get("h1"), schedule=self.schedule_primary)
         b = self.bounce(h1, out=out.get("b"))
-        h2 = core.batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], out=out.get("h2"), schedule=self.schedule)
+        h2 = core.batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], out=out.get("h2"), schedule=self.schedule_bounce)
         return dict(h1=h1, b=b, h2=h2)
 
     def trace_learned(self, out=None, in_proposal: bool = False):
@@ -121,11 +137,11 @@ class InstancedFrames:
         R = self.rays_per_instance
         p1 = self.nets.propose(self.orig, self.dir, self.box, R, out=out.get("p1"))
         h1 = proposal.batch_trace_seeded(self.tree, self.orig, self.dir, self.ray_offsets, p1, self.slots, in_proposal=in_proposal,
-                                         out=out.get("h1"), schedule=self.schedule)
+                                         out=out.get("h1"), schedule=self.schedule_primary)
         b = self.bounce(h1, out=out.get("b"))
         p2 = self.nets.propose(b[0], b[1], self.box, R, out=out.get("p2"), tmax=b[2])  # bounces of misses are inactive
         h2 = proposal.batch_trace_seeded(self.tree, b[0], b[1], self.ray_offsets, p2, self.slots, tmax=b[2], in_proposal=in_proposal,
-                                         out=out.get("h2"), schedule=self.schedule)
+                                         out=out.get("h2"), schedule=self.schedule_bounce)
         return dict(p1=p1, h1=h1, b=b, p2=p2, h2=h2)
 
     def labels(self, plain):

@@ -18,6 +18,7 @@ steady-state launch. Cases (kernel of interest in brackets):
   raster         rasteriser, 2^20-face soup, 1920x1080                           [k_raster_zones, k_raster_emit]
   mlp_grouped    64 grouped networks: 3 training steps of 1024 rays each,        [k_gemm_tc, k_softmax_xent, ...]
                  then proposals for 64 x 518,400 rays
+  sort_16m       2^24 random (key, value) pairs, 32-bit keys, sorted twice         [k_onesweep, k_sort_hist]
   c4_frame [M]   M (default 64) deformed instances of the 1/16-size learned       [launch list, k_batch_trace_coop]
                  scene, three frames of the plain path: batched build, primary
                  rays, batched trace, bounce rays, batched trace
@@ -162,6 +163,17 @@ def mlp_grouped():
     torch.cuda.synchronize()
 
 
+def sort_16m():
+    from . import core
+    g = torch.Generator(device="cuda").manual_seed(5)
+    k0 = torch.randint(-(1 << 31), (1 << 31) - 1, (1 << 24,), dtype=torch.int32, device="cuda", generator=g)
+    for _ in range(2):
+        k = k0.clone()
+        v = torch.empty_like(k)
+        core.sort_pairs(k, v, 32, init_values=True)
+    torch.cuda.synchronize()
+
+
 def c4_frame(count: int = 64):
     """Three frames of the instanced workload's plain path with the schedule the tuner picks on it."""
     from .instances import InstancedFrames
@@ -177,7 +189,7 @@ def c4_frame(count: int = 64):
 
 
 CASES = {"bench_step": bench_step, "build_16m": build_16m, "batch_build": batch_build, "trace_primary": trace_primary, "trace_bounce": trace_bounce, "mlp_propose": mlp_propose, "mlp_train": mlp_train,
-         "sah_build": sah_build, "raster": raster, "mlp_grouped": mlp_grouped, "c4_frame": c4_frame}
+         "sah_build": sah_build, "raster": raster, "mlp_grouped": mlp_grouped, "c4_frame": c4_frame, "sort_16m": sort_16m}
 
 if __name__ == "__main__":
     if len(sys.argv) not in (2, 3) or sys.argv[1] not in CASES:

@@ -87,8 +87,9 @@ def tune_trace(tree, orig, dir, tmax=None, image_width: int = 0, key: str = "def
     return best, timings
 
 
-def batch_candidates():
-    """Schedules of the batched traversal (rt_batch_trace)."""
+def batch_candidates(images=None):
+    """Schedules of the batched traversal (rt_batch_trace). images = (count, width, height) when every mesh's
+    rays form one row-major image of that size (8 x 4 pixel tiles per warp become a candidate)."""
     out = []
     for ww, wide in itertools.product((False, True), (False, True)):
         out.append({"while_while": ww, "wide": wide, "persistent": False, "blocks_per_sm": 0})
@@ -97,11 +98,19 @@ def batch_candidates():
     # warp-cooperative leaf tests (persistent, while-while)
     for wide, bps in itertools.product((False, True), (8, 16)):
         out.append({"while_while": True, "wide": wide, "persistent": True, "blocks_per_sm": bps, "coop": True})
+    # ray orders on the 4-wide records: rays sorted by mesh, octant and 0..21 Morton bits of the origin
+    for bits, coop in itertools.product((0, 6, 12, 21), (False, True)):
+        out.append({"while_while": True, "wide": True, "persistent": True, "blocks_per_sm": 16 if coop else 8, "coop": coop,
+                    "sorted_bits": bits})
+    if images is not None and images[1] % 8 == 0 and images[2] % 4 == 0:
+        for coop, bps in ((False, 8), (False, 16), (True, 16)):
+            out.append({"while_while": True, "wide": True, "persistent": True, "blocks_per_sm": bps, "coop": coop,
+                        "tiles": list(images)})
     return out
 
 
-def tune_batch_trace(tree, orig, dir, ray_offsets, tmax=None, key: str = "batch", reps: int = 2, use_cache: bool = True):
-    """tune_trace for core.batch_trace: (best_schedule, [(schedule, ms), ...])."""
+def tune_batch_trace(tree, orig, dir, ray_offsets, tmax=None, key: str = "batch", reps: int = 2, use_cache: bool = True, images=None):
+    """tune_trace for core.batch_trace: (best_schedule, [(schedule, ms), ...]); `images` as for batch_candidates."""
     gpu = torch.cuda.get_device_name(orig.device)
     cache = _load() if use_cache else {}
     ck = f"{gpu}|{key}"
@@ -110,7 +119,7 @@ def tune_batch_trace(tree, orig, dir, ray_offsets, tmax=None, key: str = "batch"
     out = core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax)
     stream = torch.cuda.current_stream()
     timings = []
-    for sch in batch_candidates():
+    for sch in batch_candidates(images):
         core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax, out=out, schedule=sch)  # warm
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)

@@ -35,7 +35,7 @@ typedef struct CUstream_st* rt_stream; /* a cudaStream_t; NULL = legacy default 
 /* Layout version of the structs below. A caller compiled against this header
  * must check rt_abi_version() == RT_ABI_VERSION before passing any struct:
  * a library built from a different header reads different field offsets. */
-#define RT_ABI_VERSION 6u
+#define RT_ABI_VERSION 7u
 
 typedef enum rt_status {
   RT_OK = 0,
@@ -175,8 +175,27 @@ typedef struct rt_batch_trace_desc {
   uint32_t schedule;              /* RT_TRACE_WHILE_WHILE, RT_TRACE_WIDE, RT_TRACE_COOP (with work_counter) */
   uint32_t* work_counter;         /* optional device word: persistent warps fetch rays through it (the call zeroes it) */
   uint32_t persistent_blocks_per_sm; /* with work_counter: CTAs of 128 threads per SM (0 = 8) */
+  const uint32_t* ray_order;      /* optional DEVICE permutation of the rays: threads take rays in this order
+                                     (rt_batch_ray_order, rt_image_tile_order); results stay in each ray's own slot */
 } rt_batch_trace_desc;
 rt_status rt_batch_trace(const rt_batch_trace_desc* desc, rt_stream stream);
+
+/* A tracing order for the rays of a batched trace: ray indices sorted by mesh
+ * (ray_offsets, DEVICE, mesh_count + 1 entries), then by direction octant, then
+ * by the top morton_bits bits (0, 3, .., 21; fewer when the mesh id, octant and
+ * Morton bits would not fit in 32 bits) of the 21-bit Morton code of the
+ * origin inside box (min xyz, max xyz, HOST); rays with tmax <= 0 go last; the
+ * sort is stable, so rays with equal keys keep their order. Scratch as for
+ * rt_ray_order. No reference counterpart. */
+rt_status rt_batch_ray_order_scratch_bytes(uint32_t count, size_t* scratch_bytes);
+rt_status rt_batch_ray_order(const float* orig, const float* dir, const float* tmax, uint32_t count, const uint32_t* ray_offsets,
+                             uint32_t mesh_count, const float box[6], uint32_t morton_bits, uint32_t* order, void* scratch,
+                             size_t scratch_bytes, rt_stream stream);
+
+/* A tracing order for `images` row-major width x height images stored one after
+ * the other (width % 8 == 0, height % 4 == 0): each run of 32 slots is an 8 x 4
+ * pixel tile of one image. No reference counterpart. */
+rt_status rt_image_tile_order(uint32_t images, uint32_t width, uint32_t height, uint32_t* order, rt_stream stream);
 
 /* Per-face boxes and indices[k] = k.
  * Replaces CUDA_calcMeshBoxes (kernels/CUDA_calcMeshBoxes.cu:65-104). */
@@ -210,7 +229,7 @@ rt_status rt_radix_sort_keys(uint32_t* keys, uint32_t n, uint32_t bit_depth, voi
  * array's device address (make it before any stream capture). All calls share
  * the array: calls that overlap on the GPU race and must be serialized. */
 #define RT_STATIC_SORT_MAX_N (1u << 20)
-#define RT_STATIC_SORT_SCRATCH_BYTES ((8u << 20) + (272u << 10))
+#define RT_STATIC_SORT_SCRATCH_BYTES ((9u << 20) + (16u << 10))
 rt_status rt_radix_sort_pairs_static(uint32_t* keys, uint32_t* values, uint32_t n, uint32_t bit_depth, int init_values,
                                      rt_stream stream);
 

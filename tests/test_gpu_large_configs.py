@@ -157,3 +157,48 @@ def test_batch_bounce_rays_match_global_positions():
     assert (h1["id"] >= 0).any() and (h1["id"] < 0).any()
     for x, y in zip(b, b2):
         assert torch.equal(x.view(torch.int32), y.view(torch.int32))
+
+
+def test_batch_ray_orders_and_schedules_identical():
+    """rt_batch_ray_order is a permutation with the rays grouped by mesh, then octant, inactive rays last;
+    rt_image_tile_order maps each 32 slots to an 8 x 4 tile of one instance's image; and every batched
+    schedule, the ordered ones included, returns the same bits for primaries and bounces."""
+    from cudart_b200 import core, tune
+    from cudart_b200.instances import InstancedFrames
+    w = InstancedFrames(4, 1 / 256, 64, 48)
+    w.displace(2)
+    w.build()
+    h1 = core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets)
+    b = w.bounce(h1)
+    h2 = core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2])
+    torch.cuda.synchronize()
+    R, W, H = w.ray_count, w.width, w.height
+    tiles = core.image_tile_order(w.count, W, H).cpu().numpy().astype(np.int64)
+    assert np.array_equal(np.sort(tiles), np.arange(R))
+    s = np.arange(R)
+    img, k = s // (W * H), s % (W * H)
+    x = (k // 32 % (W // 8)) * 8 + (k % 32) % 8
+    y = (k // 32 // (W // 8)) * 4 + (k % 32) // 8
+    assert np.array_equal(tiles, img * W * H + y * W + x)
+    tm = b[2].cpu().numpy()
+    dirs = b[1].cpu().numpy()
+    mesh = np.repeat(np.arange(w.count), w.rays_per_instance)
+    for bits in (0, 6, 21):
+        order = core.batch_ray_order(b[0], b[1], b[2], w.ray_offsets, w.count, core.batch_tree_box(w.tree), bits).cpu().numpy()
+        order = order.astype(np.int64)
+        assert np.array_equal(np.sort(order), np.arange(R))
+        act = tm[order] > 0
+        n_act = int((tm > 0).sum())
+        assert act[:n_act].all() and not act[n_act:].any()
+        key = mesh[order[:n_act]] * 8 + ((dirs[order[:n_act], 0] < 0) | 2 * (dirs[order[:n_act], 1] < 0) | 4 * (dirs[order[:n_act], 2] < 0))
+        assert np.all(np.diff(key) >= 0), bits
+        if bits == 0:  # stable: equal keys keep their index order
+            same = np.diff(key) == 0
+            assert np.all(np.diff(order[:n_act])[same] > 0)
+    for sch in tune.batch_candidates(images=(w.count, W, H)):
+        a = core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, schedule=sch)
+        c = core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], schedule=sch)
+        torch.cuda.synchronize()
+        for x_, y_ in ((a, h1), (c, h2)):
+            assert int(x_["err"].item()) == 0, sch
+            assert torch.equal(x_["id"], y_["id"]) and torch.equal(x_["t"], y_["t"]) and torch.equal(x_["uv"], y_["uv"]), sch
