@@ -249,7 +249,7 @@ def run_headline(args, rank, world, local_rank):
 
     def trace2():
         b = plain["b"]
-        core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], out=plain["h2"], schedule=s2)
+        core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], out=plain["h2"], schedule=s2, order=w.bounce_order(b))
 
     stages = [lambda: w.build(), w.primary_rays, trace1, lambda: w.bounce(plain["h1"], out=plain["b"]), trace2]
     graphs, kernels_per_step = capture_graphs(stages)
@@ -299,7 +299,7 @@ def run_headline(args, rank, world, local_rank):
     # counted launches (untimed) of the last frame's rays: box records read and triangles tested per ray
     b = plain["b"]
     c1 = core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, counters=True, schedule=s1)
-    c2 = core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], counters=True, schedule=s2)
+    c2 = core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], counters=True, schedule=s2, order=w.bounce_order(b))
     torch.cuda.synchronize()
     same = torch.equal(c1["id"], plain["h1"]["id"]) and torch.equal(c2["id"], plain["h2"]["id"])
     m1 = 48 * R + 32 * int(c1["visits"].sum().item()) + 48 * int(c1["tests"].sum().item())
@@ -395,7 +395,7 @@ def learned_frames(w, args, dev, world, plain, first_frame):
         learned["p2"] = w.nets.propose(b[0], b[1], w.box, R, out=learned["p2"], tmax=b[2])
         e[5].record()
         proposal.batch_trace_seeded(w.tree, b[0], b[1], w.ray_offsets, learned["p2"], w.slots, tmax=b[2], in_proposal=True,
-                                    out=learned["h2"], schedule=w.schedule_bounce)
+                                    out=learned["h2"], schedule=w.schedule_bounce, order=w.bounce_order(b))
         e[6].record()
         for k in ("h1", "h2"):
             mism += (plain[k]["id"] != learned[k]["id"]).sum() + (plain[k]["t"].view(torch.int32) != learned[k]["t"].view(torch.int32)).sum()
@@ -418,7 +418,8 @@ def learned_frames(w, args, dev, world, plain, first_frame):
     o0.record()
     proposal.batch_trace_seeded(w.tree, w.orig, w.dir, w.ray_offsets, l1, w.slots, out=learned["h1"], schedule=w.schedule_primary)
     b = plain["b"]
-    proposal.batch_trace_seeded(w.tree, b[0], b[1], w.ray_offsets, l2, w.slots, tmax=b[2], out=learned["h2"], schedule=w.schedule_bounce)
+    proposal.batch_trace_seeded(w.tree, b[0], b[1], w.ray_offsets, l2, w.slots, tmax=b[2], out=learned["h2"], schedule=w.schedule_bounce,
+                                order=w.bounce_order(b))
     o1.record()
     torch.cuda.synchronize()
     oracle_ms = o0.elapsed_time(o1)
@@ -462,7 +463,8 @@ def run_e2e(w, args, dev, world, s1, s2):
         o = outs[s]
         core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, out=o["h1"], schedule=s1)
         w.bounce(o["h1"], out=o["b"])
-        core.batch_trace(w.tree, o["b"][0], o["b"][1], w.ray_offsets, tmax=o["b"][2], out=o["h2"], schedule=s2)
+        core.batch_trace(w.tree, o["b"][0], o["b"][1], w.ray_offsets, tmax=o["b"][2], out=o["h2"], schedule=s2,
+                         order=w.bounce_order(o["b"]))
 
     graphs, _ = capture_graphs([lambda: compute(0), lambda: compute(1)])
 

@@ -213,7 +213,7 @@ def lib():
         L.rt_batch_ray_order.argtypes = [_P, _P, _P, _U32, _P, _U32, C.POINTER(C.c_float), _U32, _P, _P, C.c_size_t, _P]
         L.rt_image_tile_order.argtypes = [_U32, _U32, _U32, _P, _P]
         L.rt_bounce_rays.argtypes = [_P, _P, _P, _P, _P, _U32, C.c_uint64, _P, _P, _P, _P]
-        L.rt_batch_bounce_rays.argtypes = [_P, _P, _P, _U32, _P, _P, _P, _P, _U32, C.c_uint64, _P, _P, _P, _P]
+        L.rt_batch_bounce_rays.argtypes = [_P, _P, _P, _U32, _P, _P, _P, _P, _U32, C.c_uint64, _P, _P, _P, _P, _P, _P]
         for fn, st in (("mesh", MeshFile), ("tree", TreeFile)):
             getattr(L, f"rt_{fn}_file_save").argtypes = [C.c_char_p, C.c_int, C.POINTER(st)]
             getattr(L, f"rt_{fn}_file_info").argtypes = [C.c_char_p, C.POINTER(st)]

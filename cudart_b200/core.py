@@ -390,17 +390,22 @@ def bounce_rays(tris, orig, dir, hit_pos, hit_t, seed: int, out=None, ray_count:
     return out
 
 
-def batch_bounce_rays(tree, ray_offsets, orig, dir, hit_pos, hit_t, seed: int, out=None, stream=None):
+def batch_bounce_rays(tree, ray_offsets, orig, dir, hit_pos, hit_t, seed: int, out=None, order: bool = False, stream=None):
     """bounce_rays for the rays of a batched build: hit_pos are positions inside each ray's own mesh
-    (batch_trace's ids); the same rays as bounce_rays given the global positions."""
+    (batch_trace's ids); the same rays as bounce_rays given the global positions. With order=True the result
+    has a fourth tensor: a tracing order with the active rays first (for batch_trace's `order`)."""
     R = orig.shape[0]
     dev = orig.device
     if out is None:
         out = (torch.empty((R, 4), dtype=torch.float32, device=dev), torch.empty((R, 4), dtype=torch.float32, device=dev),
                torch.empty(R, dtype=torch.float32, device=dev))
+        if order:
+            out = out + (torch.empty(R + 2, dtype=torch.int32, device=dev),)  # R order entries, then two counters
+    ord_ = out[3] if len(out) > 3 else None
     _abi.check("rt_batch_bounce_rays", _abi.lib().rt_batch_bounce_rays(
         _p(tree.tris), _p(tree.face_offsets), _p(ray_offsets), tree.mesh_count, _p(orig), _p(dir), _p(hit_pos), _p(hit_t), R,
-        C.c_uint64(seed), _p(out[0]), _p(out[1]), _p(out[2]), _stream(stream)))
+        C.c_uint64(seed), _p(out[0]), _p(out[1]), _p(out[2]), None if ord_ is None else C.c_void_p(ord_.data_ptr()),
+        None if ord_ is None else C.c_void_p(ord_[R:].data_ptr()), _stream(stream)))
     return out
 
 
@@ -636,21 +641,22 @@ def batch_ray_order(orig, dir, tmax, ray_offsets, mesh_count: int, box, morton_b
 
 
 def batch_trace(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax=None, id_mode: int = 0, counters: bool = False,
-                while_while: bool = True, out: dict | None = None, schedule: dict | None = None, stream=None) -> dict:
+                while_while: bool = True, out: dict | None = None, schedule: dict | None = None, order=None, stream=None) -> dict:
     """Closest hits for the rays of all meshes (rays of mesh m: ray_offsets[m] .. ray_offsets[m+1]).
     schedule (results never depend on it): while_while, wide (4-wide records),
     persistent + blocks_per_sm (warps fetching 32 rays at a time), coop
     (warp-cooperative leaf tests; always persistent), tiles = (images, width,
     height) (every mesh's rays are one image: warps take 8 x 4 pixel tiles) or
     sorted_bits (rays sorted by mesh, octant and that many bits of their
-    origin's Morton code, inactive rays last; the sort is part of the call)."""
-    d, out = batch_trace_desc(tree, orig, dir, ray_offsets, tmax, id_mode, counters, while_while, out, schedule)
+    origin's Morton code, inactive rays last; the sort is part of the call). `order`: a tracing order given by
+    the caller (for instance batch_bounce_rays' order), used in place of the schedule's."""
+    d, out = batch_trace_desc(tree, orig, dir, ray_offsets, tmax, id_mode, counters, while_while, out, schedule, order)
     _abi.check("rt_batch_trace", _abi.lib().rt_batch_trace(C.byref(d), _stream(stream)))
     return out
 
 
 def batch_trace_desc(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax=None, id_mode: int = 0, counters: bool = False,
-                     while_while: bool = True, out: dict | None = None, schedule: dict | None = None):
+                     while_while: bool = True, out: dict | None = None, schedule: dict | None = None, order=None):
     """The rt_batch_trace_desc of batch_trace and its output tensors."""
     R = orig.shape[0]
     dev = orig.device
@@ -672,7 +678,9 @@ def batch_trace_desc(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax
     d.schedule = ((_abi.TRACE_WHILE_WHILE if sch.get("while_while", False) else 0)
                   | (_abi.TRACE_WIDE if sch.get("wide", False) else 0)
                   | (_abi.TRACE_COOP if sch.get("coop", False) else 0))
-    if sch.get("tiles"):  # every mesh's rays are a row-major image of the same size: 8 x 4 pixel tiles per warp
+    if order is not None:
+        d.ray_order = order.data_ptr()
+    elif sch.get("tiles"):  # every mesh's rays are a row-major image of the same size: 8 x 4 pixel tiles per warp
         images, width, height = sch["tiles"]
         order = image_tile_order(images, width, height, dev)
         out["_order"] = order

@@ -182,13 +182,13 @@ __device__ __forceinline__ bool seed_start(uint32_t r, const SeedArgs& S, const 
 template <bool kCount, bool kWW, bool kSeed = false, bool kWide = false>
 __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArgs& A, const AccelArgs& C,
                                                 const SeedArgs& S = SeedArgs{}) {
-  const float4 o = ldg4(A.orig + r), d = ldg4(A.dir + r);
   const float tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
   int32_t best = -1;
   float bt = tmax0, bu = 0.0f, bv = 0.0f;
   uint32_t visits = 0, tests = 0;
   uint32_t phase = 1, best_phase = 1;
-  if (tmax0 > 0.0f) {
+  if (tmax0 > 0.0f) {  // an inactive ray (tmax <= 0) reads nothing more
+    const float4 o = ldg4(A.orig + r), d = ldg4(A.dir + r);
     const float ix = 1.0f / fix_dir(d.x), iy = 1.0f / fix_dir(d.y), iz = 1.0f / fix_dir(d.z);
     const float4 oi = scaled_origin(o, ix, iy, iz);
     const float zu = o.w * 0.0f, zv = d.w * 0.0f;
@@ -340,9 +340,11 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
   float4 o = make_float4(0.f, 0.f, 0.f, 0.f), d = make_float4(0.f, 0.f, 1.f, 0.f);
   float tmax0 = -1.0f;
   if (valid) {
-    o = ldg4(A.orig + r);
-    d = ldg4(A.dir + r);
     tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
+    if (tmax0 > 0.0f) {  // an inactive ray (tmax <= 0) reads nothing more
+      o = ldg4(A.orig + r);
+      d = ldg4(A.dir + r);
+    }
   }
   int32_t best = -1;
   float bt = tmax0, bu = 0.0f, bv = 0.0f;
@@ -905,6 +907,43 @@ __global__ __launch_bounds__(256) void k_bounce(const float4* __restrict__ tris,
   }
 }
 
+// A tracing order with the active rays (tmax > 0) first: each warp takes a run of 1024 consecutive rays, counts
+// its active ones, reserves one contiguous stretch for them (and one, from the end backwards, for the inactive
+// ones) and writes them in ray order, so that neighbouring rays stay together in the order. ctr: 2 zeroed words.
+constexpr uint32_t kOrderRun = 1024;
+__global__ __launch_bounds__(256) void k_active_first_order(const float* __restrict__ tmax, uint32_t count, uint32_t* __restrict__ order,
+                                                            uint32_t* __restrict__ ctr) {
+  const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t run = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); (size_t)run * kOrderRun < count; run += warps) {
+    const uint32_t r0 = run * kOrderRun, r1 = min(count, r0 + kOrderRun);
+    uint32_t na = 0, ni = 0;
+    for (uint32_t b = r0; b < r1; b += 32) {
+      const bool in = b + lane < r1;
+      const bool act = in && __ldg(tmax + b + lane) > 0.0f;
+      na += __popc(__ballot_sync(0xffffffffu, act));
+      ni += __popc(__ballot_sync(0xffffffffu, in && !act));
+    }
+    uint32_t ab = 0, ib = 0;
+    if (lane == 0) {
+      if (na) ab = atomicAdd(ctr, na);
+      if (ni) ib = atomicAdd(ctr + 1, ni);
+    }
+    ab = __shfl_sync(0xffffffffu, ab, 0);
+    ib = __shfl_sync(0xffffffffu, ib, 0);
+    for (uint32_t b = r0; b < r1; b += 32) {
+      const uint32_t r = b + lane;
+      const bool in = r < r1;
+      const bool act = in && __ldg(tmax + r) > 0.0f;
+      const uint32_t am = __ballot_sync(0xffffffffu, act), im = __ballot_sync(0xffffffffu, in && !act);
+      if (act) order[ab + __popc(am & lt)] = r;
+      else if (in) order[count - 1u - (ib + __popc(im & lt))] = r;
+      ab += __popc(am);
+      ib += __popc(im);
+    }
+  }
+}
+
 // SM count of the current device (cached per device).
 int sms() {
   static std::atomic<int> cache[PerDeviceOnce::kMaxDevices];
@@ -1150,18 +1189,27 @@ extern "C" rt_status rt_bounce_rays(const float* tris, const float* orig, const 
 
 extern "C" rt_status rt_batch_bounce_rays(const float* tris, const uint32_t* face_offsets, const uint32_t* ray_offsets, uint32_t mesh_count,
                                           const float* orig, const float* dir, const int32_t* hit_pos, const float* hit_t, uint32_t count,
-                                          uint64_t seed, float* orig_out, float* dir_out, float* tmax_out, rt_stream stream) {
+                                          uint64_t seed, float* orig_out, float* dir_out, float* tmax_out, uint32_t* order_out,
+                                          uint32_t* order_counters, rt_stream stream) {
   if (count == 0) return RT_OK;
   if (!tris || !face_offsets || !ray_offsets || mesh_count == 0 || !orig || !dir || !hit_pos || !hit_t || !orig_out || !dir_out ||
-      !tmax_out)
+      !tmax_out || (order_out && !order_counters))
     return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  if (order_out && cudaMemsetAsync(order_counters, 0, 8, (cudaStream_t)stream) != cudaSuccess) return RT_ERR_CUDA;
   const uint32_t blocks = (uint32_t)hmin<size_t>((count + 255) / 256, (size_t)sms() * 16);
   k_bounce<true><<<blocks, 256, 0, (cudaStream_t)stream>>>((const float4*)tris, (const float4*)orig, (const float4*)dir, hit_pos, hit_t,
                                                            count, seed, (float4*)orig_out, (float4*)dir_out, tmax_out, ray_offsets,
                                                            face_offsets, mesh_count);
   note_launch();
   RT_CHECK_LAUNCH();
+  if (order_out) {
+    const uint32_t runs = (count + kOrderRun - 1) / kOrderRun;
+    const uint32_t oblocks = (uint32_t)hmin<size_t>((runs + 7) / 8, (size_t)sms() * 16);
+    k_active_first_order<<<oblocks, 256, 0, (cudaStream_t)stream>>>(tmax_out, count, order_out, order_counters);
+    note_launch();
+    RT_CHECK_LAUNCH();
+  }
   return RT_OK;
 }
 

@@ -107,9 +107,15 @@ class InstancedFrames:
         return self.slots
 
     def bounce(self, hits, out=None):
-        """One diffuse bounce per primary hit (rt_batch_bounce_rays: hit ids are instance-local positions)."""
+        """One diffuse bounce per primary hit (rt_batch_bounce_rays: hit ids are instance-local positions):
+        (orig, dir, tmax, order), the order listing the active bounces first."""
         return core.batch_bounce_rays(self.tree, self.ray_offsets, self.orig, self.dir, hits["id"], hits["t"], 1000 + self.frame_index,
-                                      out=out)
+                                      out=out, order=True)
+
+    def bounce_order(self, b):
+        """The tracing order of the bounce launch: the generator's active-first order when the bounce schedule asks
+        for it, else None (the schedule's own)."""
+        return b[3] if (self.schedule_bounce or {}).get("given_order") else None
 
     def tune(self):
         """Pick the batched traversal schedules on this frame's rays (untimed): the primary launch's on the
@@ -120,7 +126,8 @@ class InstancedFrames:
                                                           images=(self.count, self.width, self.height))
         h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, schedule=self.schedule_primary)
         b = self.bounce(h1)
-        self.schedule_bounce, t2 = tune.tune_batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], use_cache=False)
+        self.schedule_bounce, t2 = tune.tune_batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], use_cache=False,
+                                                         order=b[3])
         return (self.schedule_primary, self.schedule_bounce), (t1, t2)
 
     def trace_plain(self, out=None):
@@ -128,7 +135,8 @@ class InstancedFrames:
         out = out or {}
         h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, out=out.get("h1"), schedule=self.schedule_primary)
         b = self.bounce(h1, out=out.get("b"))
-        h2 = core.batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], out=out.get("h2"), schedule=self.schedule_bounce)
+        h2 = core.batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], out=out.get("h2"), schedule=self.schedule_bounce,
+                              order=self.bounce_order(b))
         return dict(h1=h1, b=b, h2=h2)
 
     def trace_learned(self, out=None, in_proposal: bool = False):
@@ -141,7 +149,7 @@ class InstancedFrames:
         b = self.bounce(h1, out=out.get("b"))
         p2 = self.nets.propose(b[0], b[1], self.box, R, out=out.get("p2"), tmax=b[2])  # bounces of misses are inactive
         h2 = proposal.batch_trace_seeded(self.tree, b[0], b[1], self.ray_offsets, p2, self.slots, tmax=b[2], in_proposal=in_proposal,
-                                         out=out.get("h2"), schedule=self.schedule_bounce)
+                                         out=out.get("h2"), schedule=self.schedule_bounce, order=self.bounce_order(b))
         return dict(p1=p1, h1=h1, b=b, p2=p2, h2=h2)
 
     def labels(self, plain):

@@ -563,10 +563,10 @@ def batch_hit_labels(tree, hit_pos, ray_offsets, pos_label, out=None, stream=Non
 
 def batch_trace_seeded(tree, orig, dir, ray_offsets, proposal, slots: dict, tmax=None, id_mode: int = 0, counters: bool = False,
                        in_proposal: bool = False, while_while: bool = True, box_test: bool = True, out: dict | None = None,
-                       schedule: dict | None = None, stream=None) -> dict:
+                       schedule: dict | None = None, order=None, stream=None) -> dict:
     """core.batch_trace with each ray's proposed subtree (of its own mesh) walked first; same outputs, bit for bit."""
     from .core import batch_trace_desc
-    d, out = batch_trace_desc(tree, orig, dir, ray_offsets, tmax, id_mode, counters, while_while, out, schedule)
+    d, out = batch_trace_desc(tree, orig, dir, ray_offsets, tmax, id_mode, counters, while_while, out, schedule, order)
     s = _abi.SeedDesc()
     s.proposal, s.slot_ref, s.slot_count = proposal.data_ptr(), slots["slot_ref"].data_ptr(), slots["slot_ref"].shape[1]
     if box_test:

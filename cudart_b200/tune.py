@@ -109,8 +109,11 @@ def batch_candidates(images=None):
     return out
 
 
-def tune_batch_trace(tree, orig, dir, ray_offsets, tmax=None, key: str = "batch", reps: int = 2, use_cache: bool = True, images=None):
-    """tune_trace for core.batch_trace: (best_schedule, [(schedule, ms), ...]); `images` as for batch_candidates."""
+def tune_batch_trace(tree, orig, dir, ray_offsets, tmax=None, key: str = "batch", reps: int = 2, use_cache: bool = True, images=None,
+                     order=None):
+    """tune_trace for core.batch_trace: (best_schedule, [(schedule, ms), ...]); `images` as for batch_candidates.
+    `order`: a tracing order the caller already has (such as the bounce generator's active-first order); the
+    schedules marked given_order use it."""
     gpu = torch.cuda.get_device_name(orig.device)
     cache = _load() if use_cache else {}
     ck = f"{gpu}|{key}"
@@ -119,12 +122,17 @@ def tune_batch_trace(tree, orig, dir, ray_offsets, tmax=None, key: str = "batch"
     out = core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax)
     stream = torch.cuda.current_stream()
     timings = []
-    for sch in batch_candidates(images):
-        core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax, out=out, schedule=sch)  # warm
+    cands = batch_candidates(images)
+    if order is not None:
+        cands += [{"while_while": True, "wide": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "given_order": True}
+                  for coop, bps in ((True, 16), (True, 8), (False, 8))]
+    for sch in cands:
+        given = order if sch.get("given_order") else None
+        core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax, out=out, schedule=sch, order=given)  # warm
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(reps):
-            core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax, out=out, schedule=sch)
+            core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax, out=out, schedule=sch, order=given)
         e1.record(stream)
         torch.cuda.synchronize()
         timings.append((sch, e0.elapsed_time(e1) / reps))

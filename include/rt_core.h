@@ -326,10 +326,15 @@ rt_status rt_bounce_rays(const float* tris, const float* orig, const float* dir,
  * each ray's own mesh (rt_batch_trace, id_mode 0), the rays of mesh m being
  * ray_offsets[m] .. ray_offsets[m+1] (DEVICE, mesh_count + 1 entries), and
  * face_offsets (DEVICE, as given to rt_batch_build) place each mesh in tris.
- * Same rays as rt_bounce_rays given the global positions. No reference counterpart. */
+ * Same rays as rt_bounce_rays given the global positions. Optional order_out
+ * (DEVICE, ray_count entries, with order_counters: 2 DEVICE words the call
+ * zeroes): a tracing order for rt_batch_trace_desc.ray_order, the active rays
+ * first, in runs of neighbouring rays (ray order inside each run of 1024
+ * rays). No reference counterpart. */
 rt_status rt_batch_bounce_rays(const float* tris, const uint32_t* face_offsets, const uint32_t* ray_offsets, uint32_t mesh_count,
                                const float* orig, const float* dir, const int32_t* hit_pos, const float* hit_t, uint32_t ray_count,
-                               uint64_t seed, float* orig_out, float* dir_out, float* tmax_out, rt_stream stream);
+                               uint64_t seed, float* orig_out, float* dir_out, float* tmax_out, uint32_t* order_out,
+                               uint32_t* order_counters, rt_stream stream);
 
 /* Mesh and tree chunk files (HOST calls; arrays may be device or host memory).
  * Same bytes as CUDAMesh::quickSave / CUDAMeshTree::quickSave with

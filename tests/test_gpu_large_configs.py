@@ -132,7 +132,7 @@ def test_c4_instances_of_one_frame(oracle):
         e = oracle.trace(ref["nodes"], ref["tris"], ref["indices"], o, d)
         _same_hits(plain["h1"]["id"][sl], plain["h1"]["t"][sl], plain["h1"]["uv"][sl], e)
         b = plain["b"]
-        bo, bd, btm = (np.ascontiguousarray(_h(x[sl])) for x in b)
+        bo, bd, btm = (np.ascontiguousarray(_h(x[sl])) for x in b[:3])
         if i == 0:  # ray indices of instance 0 start at 0, as the oracle's generator counts them
             eo, ed, et = oracle.bounce_rays(ref["tris"], o, d, e["id"], e["t"], 1000 + w.frame_index)
             assert np.array_equal(_u32(bo), _u32(eo)) and np.array_equal(_u32(bd), _u32(ed)) and np.array_equal(_u32(btm), _u32(et))
@@ -202,3 +202,28 @@ def test_batch_ray_orders_and_schedules_identical():
         for x_, y_ in ((a, h1), (c, h2)):
             assert int(x_["err"].item()) == 0, sch
             assert torch.equal(x_["id"], y_["id"]) and torch.equal(x_["t"], y_["t"]) and torch.equal(x_["uv"], y_["uv"]), sch
+
+
+def test_bounce_order_is_active_first_and_traces_the_same():
+    """rt_batch_bounce_rays' order lists every ray once, the active bounces first; the bounce launch traced in
+    that order returns the same bits as in ray order."""
+    from cudart_b200 import core
+    from cudart_b200.instances import InstancedFrames
+    w = InstancedFrames(4, 1 / 256, 64, 48)
+    w.displace(5)
+    w.build()
+    h1 = core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets)
+    b = w.bounce(h1)
+    base = core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2])
+    R = w.ray_count
+    order = b[3][:R].cpu().numpy().astype(np.int64)
+    tm = b[2].cpu().numpy()
+    assert np.array_equal(np.sort(order), np.arange(R))
+    n_act = int((tm > 0).sum())
+    assert 0 < n_act < R
+    assert (tm[order[:n_act]] > 0).all() and not (tm[order[n_act:]] > 0).any()
+    for coop in (False, True):
+        sch = dict(while_while=True, wide=True, persistent=True, blocks_per_sm=8, coop=coop)
+        h = core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], schedule=sch, order=b[3])
+        torch.cuda.synchronize()
+        assert torch.equal(h["id"], base["id"]) and torch.equal(h["t"], base["t"]) and torch.equal(h["uv"], base["uv"])
