@@ -126,9 +126,17 @@ __global__ __launch_bounds__(256) void k_hitbox_final(const float4* __restrict__
 // ----------------------------------------------------------------------------
 // kernels/CUDA_calcMeshBoxes.cu:30-58 (boxes, iota) fused with
 // kernels/CUDA_buildMeshTreeLBVH.cu:115-173 (Morton code of the box centre).
+// code_counts (optional, 4 x 256 zeroed words): the digit counts of the codes for the four 8-bit passes of their
+// sort, so that the sort need not read the codes once more to count them.
 __global__ __launch_bounds__(256) void k_boxes_morton(const float4* __restrict__ verts, const uint4* __restrict__ faces, uint32_t n,
                                                      const float4* __restrict__ hit, int layout, float4* __restrict__ boxes,
-                                                     uint32_t* __restrict__ codes, uint32_t* __restrict__ idx) {
+                                                     uint32_t* __restrict__ codes, uint32_t* __restrict__ idx,
+                                                     uint32_t* __restrict__ code_counts) {
+  __shared__ uint32_t s_cc[4 * 256];
+  if (code_counts) {
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) s_cc[i] = 0;
+    __syncthreads();
+  }
   const float4 hmin = codes ? hit[0] : make_float4(0.f, 0.f, 0.f, 0.f);
   const float4 hmax = codes ? hit[1] : make_float4(1.f, 1.f, 1.f, 1.f);
   const float lx = hmax.x - hmin.x, ly = hmax.y - hmin.y, lz = hmax.z - hmin.z;
@@ -146,7 +154,12 @@ __global__ __launch_bounds__(256) void k_boxes_morton(const float4* __restrict__
       const uint32_t qx = f2u_sat((cx - hmin.x) * sx);
       const uint32_t qy = f2u_sat((cy - hmin.y) * sy);
       const uint32_t qz = f2u_sat((cz - hmin.z) * sz);
-      codes[k] = spread_code(qx, qy, qz, layout);
+      const uint32_t code = spread_code(qx, qy, qz, layout);
+      codes[k] = code;
+      if (code_counts) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) atomicAdd(&s_cc[p * 256 + ((code >> (8 * p)) & 255u)], 1u);
+      }
     }
   };
   // two faces per iteration: their face and vertex loads are in flight together
@@ -161,19 +174,32 @@ __global__ __launch_bounds__(256) void k_boxes_morton(const float4* __restrict__
     face(k, v0, v1, v2);
     if (two) face(k2, w0, w1, w2);
   }
+  if (code_counts) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x)
+      if (s_cc[i]) atomicAdd(code_counts + i, s_cc[i]);
+  }
 }
 
 // ----------------------------------------------------------------------------
 // split levels: key = clz(code[i] ^ code[i+1]) (32 when equal), value = i + 1
 // (kernels/CUDA_buildMeshTreeLBVH.cu:175-233)
 // ----------------------------------------------------------------------------
+// lev_counts (256 zeroed words): how many pairs have each level, the digit counts of the level sort's one pass.
 __global__ __launch_bounds__(256) void k_levels(const uint32_t* __restrict__ codes, uint32_t n, uint32_t* __restrict__ lev,
-                                               uint32_t* __restrict__ pos) {
+                                               uint32_t* __restrict__ pos, uint32_t* __restrict__ lev_counts) {
+  __shared__ uint32_t s_lc[33];
+  if (threadIdx.x < 33) s_lc[threadIdx.x] = 0;
+  __syncthreads();
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i + 1 < n; i += gridDim.x * blockDim.x) {
     uint32_t d = __ldg(codes + i) ^ __ldg(codes + i + 1);
-    lev[i] = d ? (uint32_t)__clz(d) : 32u;
+    const uint32_t l = d ? (uint32_t)__clz(d) : 32u;
+    lev[i] = l;
     pos[i] = i + 1;
+    atomicAdd(&s_lc[l], 1u);
   }
+  __syncthreads();
+  if (threadIdx.x < 33 && s_lc[threadIdx.x]) atomicAdd(lev_counts + threadIdx.x, s_lc[threadIdx.x]);
 }
 
 // ----------------------------------------------------------------------------
@@ -195,7 +221,8 @@ struct TopoArgs {
   uint32_t max_nodes;
   uint32_t* hdr;       // [16] header: 0 leaf_count, 1 morton_leaves, 2 node_count, 3 real_depth, 4 split_count,
                        //             5 overrun, 6 nondet, 7 past_end, 8 error
-  const uint32_t* level_start;  // optional [33] absolute starts of the level lists in C (batched build); else from lev_count
+  const uint32_t* level_hist;   // optional [33] pair counts of this mesh's levels (batched build); else lev_count
+  uint32_t level_base;          // with level_hist: where this mesh's level lists start in C
   uint32_t pos_base;            // first position of this mesh (0 for a single mesh)
 };
 
@@ -207,8 +234,9 @@ __device__ __forceinline__ void topo_morton(const TopoArgs& A) {
   __shared__ uint32_t s_overrun, s_nondet, s_past, s_err, s_depth;
   const uint32_t tid = threadIdx.x;
   if (tid == 0) {
-    if (A.level_start) {
-      for (int l = 0; l < 33; ++l) s_start[l] = A.level_start[l];
+    if (A.level_hist) {
+      uint32_t acc = A.level_base;
+      for (int l = 0; l < 33; ++l) { s_start[l] = acc; acc += (l < 32) ? A.level_hist[l] : 0u; }
     } else {
       uint32_t acc = 0;
       for (int l = 0; l < 33; ++l) { s_start[l] = acc; acc += (l < 32) ? A.lev_count[l] : 0u; }
@@ -567,7 +595,7 @@ __global__ __launch_bounds__(256) void k_leaves(LeafArgs A) {
 // references (rank for an internal child, ~leaf index for a leaf child).
 __global__ __launch_bounds__(256) void k_accel_nodes(const uint32_t* __restrict__ nodes, const uint32_t* __restrict__ hdr,
                                                     const uint32_t* __restrict__ leaf_lambda, float4* __restrict__ tnodes,
-                                                    uint32_t* __restrict__ acc_hdr) {
+                                                    float4* __restrict__ wide, uint32_t* __restrict__ acc_hdr) {
   const uint32_t node_count = hdr[2];
   if (hdr[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -577,7 +605,7 @@ __global__ __launch_bounds__(256) void k_accel_nodes(const uint32_t* __restrict_
     acc_hdr[2] = node_count;
   }
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < node_count; p += gridDim.x * blockDim.x)
-    accel_node(nodes, leaf_lambda, tnodes, p);
+    accel_wide_node(nodes, leaf_lambda, tnodes, wide, p);
 }
 
 __global__ void k_write_info(const uint32_t* __restrict__ hdr, const uint32_t* __restrict__ err, rt_build_info* info) {
@@ -612,6 +640,7 @@ struct BuildLayout {
   uint32_t* err;
   uint32_t* leaf_lambda;
   uint4* faces_tmp;
+  uint32_t* counts;  // [5 x 256]: the code sort's digit counts (4 passes), then the level sort's (1 pass)
 };
 
 constexpr uint32_t kHitParts = 1184;  // 8 blocks per SM on 148 SMs
@@ -653,6 +682,7 @@ size_t carve_build(Carve& c, BuildLayout& L, uint32_t n, uint32_t D, bool need_c
   L.err = c.take<uint32_t>(4);
   L.leaf_lambda = c.take<uint32_t>(L.max_nodes);
   L.faces_tmp = need_faces_tmp ? c.take<uint4>(n) : nullptr;
+  L.counts = c.take<uint32_t>(5 * 256);
   return c.off + 256;
 }
 
@@ -754,26 +784,27 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
     note_launch(2);
   }
   RT_CHECK_LAUNCH();
-  // 2. boxes, indices, codes
+  // 2. boxes, indices, codes (and the digit counts of both sorts, counted by the kernels that make the keys)
+  if (cudaMemsetAsync(L.counts, 0, 5 * 256 * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   {
     uint32_t blocks = (uint32_t)hmin<uint64_t>((n + 255) / 256, (uint64_t)sms * 16);
     k_boxes_morton<<<blocks, 256, 0, st>>>((const float4*)d->vertices, (const uint4*)d->faces_in, n, L.hit, (int)q.morton_bits,
-                                           (float4*)d->boxes, codes, d->indices);
+                                           (float4*)d->boxes, codes, d->indices, L.counts);
     note_launch();
     RT_CHECK_LAUNCH();
   }
   // 3. sort (code, index); the build's error word starts here, so that the sorts' bounded waits report into it
   if (cudaMemsetAsync(L.err, 0, 16, st) != cudaSuccess) return RT_ERR_CUDA;
-  rt_status s = radix_sort_pairs(codes, d->indices, n, 0, 32, 0, L.sort_scratch, L.sort_bytes, st, nullptr, L.err);
+  rt_status s = radix_sort_pairs(codes, d->indices, n, 0, 32, 0, L.sort_scratch, L.sort_bytes, st, nullptr, L.err, L.counts);
   if (s != RT_OK) return s;
   // 4. per-level split lists
   if (cudaMemsetAsync(L.lev_count, 0, 256 * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   if (n > 1) {
     uint32_t blocks = (uint32_t)hmin<uint64_t>((n + 255) / 256, (uint64_t)sms * 16);
-    k_levels<<<blocks, 256, 0, st>>>(codes, n, L.lev, L.C);
+    k_levels<<<blocks, 256, 0, st>>>(codes, n, L.lev, L.C, L.counts + 4 * 256);
     note_launch();
     RT_CHECK_LAUNCH();
-    s = radix_sort_pairs(L.lev, L.C, n - 1, 0, 8, 0, L.sort_scratch, L.sort_bytes, st, L.lev_count, L.err);
+    s = radix_sort_pairs(L.lev, L.C, n - 1, 0, 8, 0, L.sort_scratch, L.sort_bytes, st, L.lev_count, L.err, L.counts + 4 * 256);
     if (s != RT_OK) return s;
   }
   // 5. Morton top tree
@@ -785,7 +816,7 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
     A.rank = L.rank; A.lambda = L.lambda; A.ord = L.ord; A.id = L.id;
     A.ml_lambda = L.ml_lambda; A.ml_rec = L.ml_rec; A.ml_rank = L.ml_rank; A.parent_id = L.parent_id;
     A.nodes = d->nodes; A.max_nodes = d->max_nodes; A.hdr = L.hdr;
-    A.level_start = nullptr; A.pos_base = 0;
+    A.level_hist = nullptr; A.level_base = 0; A.pos_base = 0;
     k_topo_morton<<<1, kTopoThreads, 0, st>>>(A);
     note_launch();
     RT_CHECK_LAUNCH();
@@ -814,9 +845,7 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
     note_launch(2);
     RT_CHECK_LAUNCH();
     if (accel) {
-      k_accel_nodes<<<sms * 4, 256, 0, st>>>(d->nodes, L.hdr, L.leaf_lambda, AL.tnodes, AL.hdr);
-      k_wide_nodes<<<sms * 4, 256, 0, st>>>(AL.tnodes, AL.hdr, AL.wide);
-      note_launch();
+      k_accel_nodes<<<sms * 4, 256, 0, st>>>(d->nodes, L.hdr, L.leaf_lambda, AL.tnodes, AL.wide, AL.hdr);
       note_launch();
       RT_CHECK_LAUNCH();
     }
@@ -837,7 +866,7 @@ extern "C" rt_status rt_mesh_boxes(const float* vertices, const uint32_t* faces,
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   uint32_t blocks = (uint32_t)hmin<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 16);
   k_boxes_morton<<<blocks, 256, 0, (cudaStream_t)st>>>((const float4*)vertices, (const uint4*)faces, n, nullptr, 32, (float4*)boxes,
-                                                      nullptr, indices);
+                                                      nullptr, indices, nullptr);
     note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;
@@ -891,7 +920,6 @@ struct BatchArgs {
   uint32_t* lev;          // [N] (mesh, level) keys
   uint32_t* C;            // [N] split positions
   uint32_t* hist;         // [M * 64 + 1]
-  uint32_t* level_start;  // [M * 64 + 1]
   uint32_t *ra, *rb, *parent, *info, *child, *leaves, *mleaves, *rank, *lambda, *ord, *id;  // [2N + 3M]
   uint32_t* ml_lambda;
   uint4* ml_rec;
@@ -902,6 +930,9 @@ struct BatchArgs {
   uint32_t* hdr;          // [16 M]
   uint32_t* leaf_base;    // [M + 1]
   uint32_t* err;          // [4]
+  uint32_t* counts;       // [9 x 256 + 64]: digit counts of the code sort (4 passes), the mesh sort (2), the level
+                          // sort (3), then the count of finished topology CTAs
+
   // traversal blob
   uint32_t* acc_hdr;      // [64 M]
   float4* tnodes;         // [4 N]
@@ -916,6 +947,11 @@ struct BatchArgs {
 __global__ __launch_bounds__(512) void k_batch_hitbox(BatchArgs B) {
   const uint32_t m = blockIdx.x;
   const uint32_t v0 = B.voff[m], v1 = B.voff[m + 1];
+  if (threadIdx.x == 0) {  // the mesh sort's digit counts: mesh m holds foff[m + 1] - foff[m] keys of value m
+    const uint32_t faces = B.foff[m + 1] - B.foff[m];
+    atomicAdd(B.counts + 4 * 256 + (m & 255u), faces);
+    atomicAdd(B.counts + 5 * 256 + ((m >> 8) & 255u), faces);
+  }
   float4 mn[4], mx[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -953,6 +989,9 @@ __global__ __launch_bounds__(512) void k_batch_hitbox(BatchArgs B) {
 }
 
 __global__ __launch_bounds__(256) void k_batch_boxes_morton(BatchArgs B) {
+  __shared__ uint32_t s_cc[4 * 256];  // the code sort's digit counts of this block's faces
+  for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) s_cc[i] = 0;
+  __syncthreads();
   const int layout = (int)B.q.morton_bits;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < B.N; k += gridDim.x * blockDim.x) {
     const uint32_t m = find_seg(B.foff, B.M, k);
@@ -972,50 +1011,42 @@ __global__ __launch_bounds__(256) void k_batch_boxes_morton(BatchArgs B) {
     const uint32_t code = spread_code(f2u_sat((cx - hmin.x) * sx), f2u_sat((cy - hmin.y) * sy), f2u_sat((cz - hmin.z) * sz), layout);
     B.codes[k] = code;
     B.codes_raw[k] = code;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) atomicAdd(&s_cc[p * 256 + ((code >> (8 * p)) & 255u)], 1u);
   }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x)
+    if (s_cc[i]) atomicAdd(B.counts + i, s_cc[i]);
 }
 
-__global__ __launch_bounds__(256) void k_batch_meshkey(BatchArgs B) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < B.N; i += gridDim.x * blockDim.x)
-    B.mkey[i] = find_seg(B.foff, B.M, B.idx[i]);
-}
-
-// After the (mesh, code) order is complete: codes per position, and the split
-// level key (mesh * 64 + level; 32 = no split, also across meshes) per pair.
+// After the (mesh, code) order is complete: the code of each position, and per pair (i, i + 1) the split level
+// key (mesh * 64 + level; 32 = no split, also across meshes), its (mesh, level) count and the level sort's digit
+// counts (up to three 8-bit passes).
 __global__ __launch_bounds__(256) void k_batch_levels(BatchArgs B) {
+  __shared__ uint32_t s_lc[3 * 256];
+  for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) s_lc[i] = 0;
+  __syncthreads();
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < B.N; i += gridDim.x * blockDim.x) {
-    B.codes[i] = B.codes_raw[B.idx[i]];
-  }
-}
-__global__ __launch_bounds__(256) void k_batch_levels2(BatchArgs B) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i + 1 < B.N; i += gridDim.x * blockDim.x) {
-    const uint32_t m = B.mkey[i];
-    uint32_t lev = 32;
-    if (B.mkey[i + 1] == m) {
-      const uint32_t d = B.codes[i] ^ B.codes[i + 1];
-      if (d) lev = (uint32_t)__clz(d);
+    const uint32_t c0 = B.codes_raw[B.idx[i]];
+    B.codes[i] = c0;
+    if (i + 1 < B.N) {
+      const uint32_t m = B.mkey[i];
+      uint32_t lev = 32;
+      if (B.mkey[i + 1] == m) {
+        const uint32_t d = c0 ^ B.codes_raw[B.idx[i + 1]];
+        if (d) lev = (uint32_t)__clz(d);
+      }
+      const uint32_t key = m * 64 + lev;
+      B.lev[i] = key;
+      B.C[i] = i + 1;
+      atomicAdd(B.hist + key, 1u);
+#pragma unroll
+      for (int p = 0; p < 3; ++p) atomicAdd(&s_lc[p * 256 + ((key >> (8 * p)) & 255u)], 1u);
     }
-    const uint32_t key = m * 64 + lev;
-    B.lev[i] = key;
-    B.C[i] = i + 1;
-    atomicAdd(B.hist + key, 1u);
   }
-}
-
-// Exclusive scan of the (mesh, level) histogram: absolute start of each list in C.
-__global__ __launch_bounds__(1024) void k_batch_level_starts(BatchArgs B) {
-  __shared__ uint32_t s_warp[32];
-  const uint32_t total_keys = B.M * 64;
-  uint32_t running = 0;
-  for (uint32_t c = 0; c < total_keys; c += 1024) {
-    const uint32_t i = c + threadIdx.x;
-    const uint32_t v = i < total_keys ? B.hist[i] : 0u;
-    uint32_t tot;
-    const uint32_t ex = block_excl_scan_nt<1024>(v, s_warp, tot);
-    if (i < total_keys) B.level_start[i] = running + ex;
-    running += tot;
-  }
-  if (threadIdx.x == 0) B.level_start[total_keys] = running;
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x)
+    if (s_lc[i]) atomicAdd(B.counts + 6 * 256 + i, s_lc[i]);
 }
 
 __global__ __launch_bounds__(kTopoThreads) void k_batch_topo(BatchArgs B) {
@@ -1029,20 +1060,29 @@ __global__ __launch_bounds__(kTopoThreads) void k_batch_topo(BatchArgs B) {
   A.leaves = B.leaves + bb; A.mleaves = B.mleaves + bb; A.rank = B.rank + bb; A.lambda = B.lambda + bb; A.ord = B.ord + bb;
   A.id = B.id + bb; A.ml_lambda = B.ml_lambda + bb; A.ml_rec = B.ml_rec + bb; A.ml_rank = B.ml_rank + bb;
   A.parent_id = B.parent_id + nb; A.nodes = B.nodes + 8 * (size_t)nb; A.max_nodes = 2 * n - 1; A.hdr = B.hdr + 16 * m;
-  A.level_start = B.level_start + 64 * m; A.pos_base = F;
+  // the pairs of the meshes before m are their F positions (every position but the last of all has one pair),
+  // so this mesh's level lists start at F in the level order
+  A.level_hist = B.hist + 64 * m; A.level_base = F; A.pos_base = F;
   topo_morton(A);
-}
-
-// Leaf-order bases per mesh (exclusive scan of the leaf counts) and the total.
-__global__ __launch_bounds__(1024) void k_batch_leaf_base(BatchArgs B) {
-  __shared__ uint32_t s_warp[32];
+  // the CTA that finishes last (every other mesh's header is written) makes the leaf-order bases per mesh (an
+  // exclusive scan of the leaf counts) and their total; nothing waits for it inside this kernel
+  __shared__ uint32_t s_last;
+  __shared__ uint32_t s_warp2[kTopoWarps];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(B.counts + 9 * 256, 1u) == B.M - 1 ? 1u : 0u;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
   uint32_t running = 0;
-  for (uint32_t c = 0; c < B.M; c += 1024) {
+  for (uint32_t c = 0; c < B.M; c += kTopoThreads) {
     const uint32_t i = c + threadIdx.x;
-    const uint32_t bad = i < B.M ? (B.hdr[16 * i + 8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) : 0u;
-    const uint32_t v = (i < B.M && !bad) ? B.hdr[16 * i] : 0u;
+    const uint32_t bad = i < B.M ? (__ldcg(B.hdr + 16 * i + 8) & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) : 0u;
+    const uint32_t v = (i < B.M && !bad) ? __ldcg(B.hdr + 16 * i) : 0u;
     uint32_t tot;
-    const uint32_t ex = block_excl_scan_nt<1024>(v, s_warp, tot);
+    const uint32_t ex = block_excl_scan_nt<kTopoThreads>(v, s_warp2, tot);
     if (i < B.M) B.leaf_base[i] = running + ex;
     running += tot;
   }
@@ -1101,7 +1141,8 @@ __global__ __launch_bounds__(256) void k_batch_propagate(BatchArgs B) {
   }
 }
 
-__global__ __launch_bounds__(256) void k_batch_accel_nodes(BatchArgs B) {
+// Traversal records of every mesh (two-child and 4-wide, per internal node) and each mesh's build info.
+__global__ __launch_bounds__(256) void k_batch_records(BatchArgs B) {
   const uint32_t slots = 2 * B.N - B.M;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < slots; p += gridDim.x * blockDim.x) {
     // mesh whose node range holds slot p: largest m with 2 F_m - m <= p
@@ -1121,24 +1162,8 @@ __global__ __launch_bounds__(256) void k_batch_accel_nodes(BatchArgs B) {
       ah[1] = h[0];
       ah[2] = h[2];
     }
-    accel_node(B.nodes + 8 * (size_t)nb, B.leaf_lambda + nb, B.tnodes + 4 * (size_t)F, lp);
+    accel_wide_node(B.nodes + 8 * (size_t)nb, B.leaf_lambda + nb, B.tnodes + 4 * (size_t)F, B.wide + 8 * (size_t)F, lp);
   }
-}
-
-// 4-wide records of every mesh (after all two-child records exist).
-__global__ __launch_bounds__(256) void k_batch_wide_nodes(BatchArgs B) {
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < B.N; p += gridDim.x * blockDim.x) {
-    const uint32_t m = find_seg(B.foff, B.M, p);
-    const uint32_t F = __ldg(B.foff + m);
-    const uint32_t* h = B.hdr + 16 * m;
-    if (h[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) continue;
-    const uint32_t leaves = B.acc_hdr[64 * (size_t)m + 1];
-    const uint32_t lp = p - F;
-    if (lp + 1 < leaves) wide_node(B.tnodes + 4 * (size_t)F, B.wide + 8 * (size_t)F, lp);
-  }
-}
-
-__global__ void k_batch_info(BatchArgs B) {
   for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < B.M; m += gridDim.x * blockDim.x) {
     const uint32_t* h = B.hdr + 16 * m;
     rt_build_info* o = B.info_out + m;
@@ -1155,7 +1180,6 @@ size_t carve_batch(Carve& c, BatchArgs& B, uint32_t M, uint32_t N) {
   B.lev = c.take<uint32_t>(N);
   B.C = c.take<uint32_t>(N);
   B.hist = c.take<uint32_t>((size_t)M * 64 + 1);
-  B.level_start = c.take<uint32_t>((size_t)M * 64 + 1);
   const size_t bfs = 2 * (size_t)N + 3 * (size_t)M + 4;
   uint32_t** arrs[] = {&B.ra, &B.rb, &B.parent, &B.info, &B.child, &B.leaves, &B.mleaves, &B.rank, &B.lambda, &B.ord, &B.id};
   for (auto a : arrs) *a = c.take<uint32_t>(bfs);
@@ -1169,6 +1193,7 @@ size_t carve_batch(Carve& c, BatchArgs& B, uint32_t M, uint32_t N) {
   B.hdr = c.take<uint32_t>(16 * (size_t)M);
   B.leaf_base = c.take<uint32_t>((size_t)M + 1);
   B.err = c.take<uint32_t>(4);
+  B.counts = c.take<uint32_t>(9 * 256 + 64);
   const size_t sort_bytes = radix_scratch_bytes(N);
   c.take<char>(sort_bytes);
   return c.off + 256;
@@ -1225,46 +1250,43 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   cudaStream_t st = (cudaStream_t)stream_;
   const int sms = sm_count();
   const uint32_t fblocks = (uint32_t)hmin<uint64_t>((N + 255) / 256, (uint64_t)sms * 16);
+  // the error word and every sort's digit counts (counted by the kernels that make the keys) start at zero
+  if (cudaMemsetAsync(B.err, 0, 16, st) != cudaSuccess) return RT_ERR_CUDA;
+  if (cudaMemsetAsync(B.counts, 0, (9 * 256 + 64) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
+  if (cudaMemsetAsync(B.hist, 0, ((size_t)M * 64 + 1) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   k_batch_hitbox<<<M, 512, 0, st>>>(B);
   k_batch_boxes_morton<<<fblocks, 256, 0, st>>>(B);
   note_launch(2);
   RT_CHECK_LAUNCH();
-  if (cudaMemsetAsync(B.err, 0, 16, st) != cudaSuccess) return RT_ERR_CUDA;
-  rt_status s = radix_sort_pairs(B.codes, B.idx, N, 0, 32, 0, sort_scratch, sort_bytes, st, nullptr, B.err);
+  // Morton order of all faces; its last pass also writes each position's mesh (the key of the next sort)
+  rt_status s = radix_sort_pairs(B.codes, B.idx, N, 0, 32, 0, sort_scratch, sort_bytes, st, nullptr, B.err, B.counts, B.foff, M,
+                                 B.mkey);
   if (s != RT_OK) return s;
-  k_batch_meshkey<<<fblocks, 256, 0, st>>>(B);
-  note_launch();
-  RT_CHECK_LAUNCH();
   // key widths in whole 8-bit digits: mesh ids < M, level keys < 64 (M - 1) + 33
   auto digit_bits = [](uint64_t maxval) -> uint32_t {
     uint32_t b = 1;
     while (b < 64 && (1ull << b) <= maxval) ++b;
     return b > 24 ? 32u : (b + 7) / 8 * 8;
   };
-  s = radix_sort_pairs(B.mkey, B.idx, N, 0, digit_bits(M - 1), 0, sort_scratch, sort_bytes, st, nullptr, B.err);
+  s = radix_sort_pairs(B.mkey, B.idx, N, 0, digit_bits(M - 1), 0, sort_scratch, sort_bytes, st, nullptr, B.err, B.counts + 4 * 256);
   if (s != RT_OK) return s;
-  if (cudaMemsetAsync(B.hist, 0, ((size_t)M * 64 + 1) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   k_batch_levels<<<fblocks, 256, 0, st>>>(B);
-  k_batch_levels2<<<fblocks, 256, 0, st>>>(B);
-  note_launch(2);
+  note_launch();
   RT_CHECK_LAUNCH();
   if (N > 1) {
-    s = radix_sort_pairs(B.lev, B.C, N - 1, 0, digit_bits(64ull * (M - 1) + 32), 0, sort_scratch, sort_bytes, st, nullptr, B.err);
+    s = radix_sort_pairs(B.lev, B.C, N - 1, 0, digit_bits(64ull * (M - 1) + 32), 0, sort_scratch, sort_bytes, st, nullptr, B.err,
+                         B.counts + 6 * 256);
     if (s != RT_OK) return s;
   }
-  k_batch_level_starts<<<1, 1024, 0, st>>>(B);
   k_batch_topo<<<M, kTopoThreads, 0, st>>>(B);
-  k_batch_leaf_base<<<1, 1024, 0, st>>>(B);
-  note_launch(3);
+  note_launch();
   RT_CHECK_LAUNCH();
   if (cudaMemsetAsync(B.arrive, 0, (2 * (size_t)N) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   static const int leaf_blocks = resident_blocks_of(k_batch_leaves, 256);
   k_batch_leaves<<<sms * leaf_blocks, 256, 0, st>>>(B);
   k_batch_propagate<<<sms * 8, 256, 0, st>>>(B);
-  k_batch_accel_nodes<<<sms * 4, 256, 0, st>>>(B);
-  k_batch_wide_nodes<<<sms * 4, 256, 0, st>>>(B);
-  k_batch_info<<<(M + 255) / 256, 256, 0, st>>>(B);
-  note_launch(5);
+  k_batch_records<<<sms * 4, 256, 0, st>>>(B);
+  note_launch(3);
   RT_CHECK_LAUNCH();
   return RT_OK;
 }

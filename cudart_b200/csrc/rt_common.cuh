@@ -113,9 +113,14 @@ constexpr size_t radix_scratch_bytes_of(uint32_t n) {
 size_t radix_scratch_bytes(uint32_t n);
 // Stable sort of (key, value) pairs by bits [begin_bit, end_bit) of the key; digit_totals_out (device, 256 words,
 // optional) receives the digit counts of the last pass; err (device, optional) receives RT_DEVERR_WAIT_TIMEOUT
-// if a bounded wait between tiles ran out.
+// if a bounded wait between tiles ran out. digit_counts_in (device, optional): the digit counts of every pass
+// (pass p's 256 counts at p * 256, digit p = bits [begin_bit + 8p, begin_bit + 8p + 8)), counted by the keys'
+// producer; the sort then reads the keys once less. seg_off / seg_count / seg_out (optional, with values):
+// the last pass also writes seg_out[position] = the segment of the value placed there (the largest m < seg_count
+// with seg_off[m] <= value).
 rt_status radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t begin_bit, uint32_t end_bit, int init_vals,
                            void* scratch, size_t scratch_bytes, cudaStream_t stream, uint32_t* digit_totals_out,
-                           uint32_t* err = nullptr);
+                           uint32_t* err = nullptr, const uint32_t* digit_counts_in = nullptr, const uint32_t* seg_off = nullptr,
+                           uint32_t seg_count = 0, uint32_t* seg_out = nullptr);
 
 }  // namespace rt

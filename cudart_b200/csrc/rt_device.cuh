@@ -199,6 +199,64 @@ __device__ __forceinline__ void wide_node(const float4* __restrict__ tnodes, flo
   w[6] = make_float4(__uint_as_float(ref[0]), __uint_as_float(ref[1]), __uint_as_float(ref[2]), __uint_as_float(ref[3]));
   w[7] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
+// The two-child record and the 4-wide record of internal node p, both from the nodes (the same values as
+// accel_node followed by wide_node, in one pass: a grandchild's padded box and reference are computed from its
+// node as accel_node computes them for the child's record).
+__device__ __forceinline__ void accel_wide_node(const uint32_t* __restrict__ nodes, const uint32_t* __restrict__ leaf_lambda,
+                                                float4* __restrict__ tnodes, float4* __restrict__ wide, const uint32_t p) {
+  const uint2 w = *(const uint2*)(nodes + 8 * (size_t)p);
+  if (w.x & 1u) return;
+  const uint32_t rank = (w.y - 1u) >> 1;
+  // padded box and reference of node c, as a parent's record holds them
+  auto child = [&](uint32_t c, float3& mn, float3& mx, uint32_t& ref, uint32_t& first_child) {
+    const uint32_t* cn = nodes + 8 * (size_t)c;
+    const uint32_t cw0 = cn[0], cw1 = cn[1];
+    mn = make_float3(__uint_as_float(cn[2]), __uint_as_float(cn[3]), __uint_as_float(cn[4]));
+    mx = make_float3(__uint_as_float(cn[5]), __uint_as_float(cn[6]), __uint_as_float(cn[7]));
+    pad_box(mn, mx);
+    const bool leaf = (cw0 & 1u) != 0;
+    ref = leaf ? ~leaf_lambda[c] : ((cw1 - 1u) >> 1);
+    first_child = leaf ? kNone : cw1;
+  };
+  float4 out[4];
+  float mnx[4] = {0.f, 0.f, 0.f, 0.f}, mny[4] = {0.f, 0.f, 0.f, 0.f}, mnz[4] = {0.f, 0.f, 0.f, 0.f};
+  float mxx[4] = {0.f, 0.f, 0.f, 0.f}, mxy[4] = {0.f, 0.f, 0.f, 0.f}, mxz[4] = {0.f, 0.f, 0.f, 0.f};
+  uint32_t wref[4] = {kNoChild, kNoChild, kNoChild, kNoChild};
+  int k = 0;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    float3 mn, mx;
+    uint32_t ref, fc;
+    child(w.y + side, mn, mx, ref, fc);
+    out[2 * side] = make_float4(mn.x, mn.y, mn.z, __uint_as_float(ref));
+    out[2 * side + 1] = make_float4(mx.x, mx.y, mx.z, 0.0f);
+    if (fc == kNone) {
+      mnx[k] = mn.x; mny[k] = mn.y; mnz[k] = mn.z; mxx[k] = mx.x; mxy[k] = mx.y; mxz[k] = mx.z; wref[k] = ref;
+      ++k;
+    } else {
+#pragma unroll
+      for (int s2 = 0; s2 < 2; ++s2) {
+        float3 gmn, gmx;
+        uint32_t gref, gfc;
+        child(fc + s2, gmn, gmx, gref, gfc);
+        mnx[k] = gmn.x; mny[k] = gmn.y; mnz[k] = gmn.z; mxx[k] = gmx.x; mxy[k] = gmx.y; mxz[k] = gmx.z; wref[k] = gref;
+        ++k;
+      }
+    }
+  }
+  float4* dst = tnodes + 4 * (size_t)rank;
+  dst[0] = out[0]; dst[1] = out[1]; dst[2] = out[2]; dst[3] = out[3];
+  float4* wd = wide + 8 * (size_t)rank;
+  wd[0] = make_float4(mnx[0], mnx[1], mnx[2], mnx[3]);
+  wd[1] = make_float4(mny[0], mny[1], mny[2], mny[3]);
+  wd[2] = make_float4(mnz[0], mnz[1], mnz[2], mnz[3]);
+  wd[3] = make_float4(mxx[0], mxx[1], mxx[2], mxx[3]);
+  wd[4] = make_float4(mxy[0], mxy[1], mxy[2], mxy[3]);
+  wd[5] = make_float4(mxz[0], mxz[1], mxz[2], mxz[3]);
+  wd[6] = make_float4(__uint_as_float(wref[0]), __uint_as_float(wref[1]), __uint_as_float(wref[2]), __uint_as_float(wref[3]));
+  wd[7] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
 // All records of a blob whose header holds the leaf count (hdr[1]).
 static __global__ __launch_bounds__(256) void k_wide_nodes(const float4* __restrict__ tnodes, const uint32_t* __restrict__ acc_hdr,
                                                     float4* __restrict__ wide) {

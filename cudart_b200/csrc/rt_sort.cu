@@ -120,6 +120,22 @@ __global__ __launch_bounds__(256) void k_sort_hist(const uint32_t* __restrict__ 
   }
 }
 
+// Optional epilogue of a pass: out[position] = the segment of the value written there (largest m with
+// off[m] <= value, m < count), for a caller that needs each sorted value's segment next.
+struct SegOut {
+  const uint32_t* off;
+  uint32_t count;
+  uint32_t* out;
+};
+__device__ __forceinline__ uint32_t find_seg(const uint32_t* __restrict__ off, uint32_t M, uint32_t x) {
+  uint32_t lo = 0, hi = M - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (__ldg(off + mid) <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
 // One digit pass. status[tile * 256 + d] holds a flag (bits 30-31) and a count (bits 0-29); all zero at the start.
 // vals_in == nullptr with kVals: the values are the keys' input positions (first pass of an index sort).
 template <bool kVals>
@@ -127,7 +143,8 @@ __global__ __launch_bounds__(kOsThreads, 2) void k_onesweep(const uint32_t* __re
                                                             uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n,
                                                             uint32_t shift, const uint32_t* __restrict__ digit_counts,
                                                             uint32_t* __restrict__ status, uint32_t* __restrict__ tile_counter,
-                                                            uint32_t* __restrict__ digit_totals_out, uint32_t* __restrict__ err) {
+                                                            uint32_t* __restrict__ digit_totals_out, uint32_t* __restrict__ err,
+                                                            SegOut seg) {
   __shared__ uint32_t s_keys[kOsTile];
   __shared__ uint32_t s_vals[kVals ? kOsTile : 1];
   __shared__ uint16_t s_cnt[kOsWarps][kRadix];  // per warp and digit: count, then the warp's offset in the tile's run (<= 4096)
@@ -222,7 +239,10 @@ __global__ __launch_bounds__(kOsThreads, 2) void k_onesweep(const uint32_t* __re
     const uint32_t d = (k >> shift) & 255u;
     const size_t out = (size_t)s_glob[d] + (i - s_tile_start[d]);
     keys_out[out] = k;
-    if (kVals) vals_out[out] = s_vals[i];
+    if (kVals) {
+      vals_out[out] = s_vals[i];
+      if (seg.out) seg.out[out] = find_seg(seg.off, seg.count, s_vals[i]);
+    }
   }
 }
 
@@ -231,7 +251,7 @@ __global__ __launch_bounds__(kOsThreads, 2) void k_onesweep(const uint32_t* __re
 template <bool kVals>
 __global__ __launch_bounds__(kThreads) void k_radix_small(uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t n,
                                                          uint32_t begin_bit, uint32_t passes, int init_vals,
-                                                         uint32_t* __restrict__ digit_totals_out) {
+                                                         uint32_t* __restrict__ digit_totals_out, SegOut seg) {
   extern __shared__ uint32_t dyn[];
   uint32_t* kbuf[2] = {dyn, dyn + kTile};
   uint32_t* vbuf[2] = {dyn + 2 * kTile, dyn + 3 * kTile};
@@ -290,7 +310,10 @@ __global__ __launch_bounds__(kThreads) void k_radix_small(uint32_t* __restrict__
   }
   for (uint32_t i = threadIdx.x; i < n; i += kThreads) {
     keys[i] = kbuf[cur][i];
-    if (kVals) vals[i] = vbuf[cur][i];
+    if (kVals) {
+      vals[i] = vbuf[cur][i];
+      if (seg.out) seg.out[i] = find_seg(seg.off, seg.count, vbuf[cur][i]);
+    }
   }
 }
 
@@ -336,7 +359,8 @@ size_t radix_scratch_bytes(uint32_t n) {
 }
 
 rt_status radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t begin_bit, uint32_t end_bit, int init_vals,
-                           void* scratch, size_t scratch_bytes, cudaStream_t stream, uint32_t* digit_totals_out, uint32_t* err) {
+                           void* scratch, size_t scratch_bytes, cudaStream_t stream, uint32_t* digit_totals_out, uint32_t* err,
+                           const uint32_t* digit_counts_in, const uint32_t* seg_off, uint32_t seg_count, uint32_t* seg_out) {
   if (n == 0) return RT_OK;
   if (end_bit <= begin_bit || end_bit > 32) return RT_ERR_INVALID_ARGUMENT;
   if (n > kCountMask) return RT_ERR_INVALID_ARGUMENT;
@@ -344,9 +368,10 @@ rt_status radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t 
   if (n <= (uint32_t)kTile) {
     if (!small_smem_ready()) return RT_ERR_CUDA;
     if (vals)
-      k_radix_small<true><<<1, kThreads, kSmallSmem, stream>>>(keys, vals, n, begin_bit, passes, init_vals, digit_totals_out);
+      k_radix_small<true><<<1, kThreads, kSmallSmem, stream>>>(keys, vals, n, begin_bit, passes, init_vals, digit_totals_out,
+                                                               SegOut{seg_off, seg_count, (seg_off && seg_count) ? seg_out : nullptr});
     else
-      k_radix_small<false><<<1, kThreads, kSmallSmem, stream>>>(keys, nullptr, n, begin_bit, passes, 0, digit_totals_out);
+      k_radix_small<false><<<1, kThreads, kSmallSmem, stream>>>(keys, nullptr, n, begin_bit, passes, 0, digit_totals_out, SegOut{});
     note_launch();
     RT_CHECK_LAUNCH();
     return RT_OK;
@@ -360,21 +385,27 @@ rt_status radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t 
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
     sms = 148;
-  const uint32_t hist_blocks = (uint32_t)hmin<size_t>((n / 4 + 255) / 256, (size_t)sms * 4);
-  k_sort_hist<<<hist_blocks ? hist_blocks : 1, 256, 0, stream>>>(keys, n, begin_bit, passes, L.counts);
-  note_launch();
-  RT_CHECK_LAUNCH();
+  const uint32_t* counts = digit_counts_in;
+  if (!counts) {  // one read of the keys for every pass's digit counts, unless the keys' producer counted them
+    const uint32_t hist_blocks = (uint32_t)hmin<size_t>((n / 4 + 255) / 256, (size_t)sms * 4);
+    k_sort_hist<<<hist_blocks ? hist_blocks : 1, 256, 0, stream>>>(keys, n, begin_bit, passes, L.counts);
+    note_launch();
+    RT_CHECK_LAUNCH();
+    counts = L.counts;
+  }
   uint32_t *ks = keys, *vs = vals, *kd = L.kalt, *vd = L.valt;
   for (uint32_t p = 0; p < passes; ++p) {
     const uint32_t shift = begin_bit + 8 * p;
     uint32_t* st = L.status + (size_t)p * tiles * kRadix;
     uint32_t* ctr = L.counters + (size_t)p * 64;
-    const uint32_t* dc = L.counts + (size_t)p * kRadix;
+    const uint32_t* dc = counts + (size_t)p * kRadix;
     uint32_t* dto = p + 1 == passes ? digit_totals_out : nullptr;
+    const SegOut seg{seg_off, seg_count, (p + 1 == passes && seg_off && seg_count) ? seg_out : nullptr};
     if (vals)
-      k_onesweep<true><<<tiles, kOsThreads, 0, stream>>>(ks, (p == 0 && init_vals) ? nullptr : vs, kd, vd, n, shift, dc, st, ctr, dto, err);
+      k_onesweep<true><<<tiles, kOsThreads, 0, stream>>>(ks, (p == 0 && init_vals) ? nullptr : vs, kd, vd, n, shift, dc, st, ctr, dto, err,
+                                                          seg);
     else
-      k_onesweep<false><<<tiles, kOsThreads, 0, stream>>>(ks, nullptr, kd, nullptr, n, shift, dc, st, ctr, dto, err);
+      k_onesweep<false><<<tiles, kOsThreads, 0, stream>>>(ks, nullptr, kd, nullptr, n, shift, dc, st, ctr, dto, err, SegOut{});
     note_launch();
     RT_CHECK_LAUNCH();
     uint32_t* t;
