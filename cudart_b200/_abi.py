@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librt_core.so")
 
 RT_OK = 0
-ABI_VERSION = 7  # RT_ABI_VERSION of include/rt_core.h that the structs below mirror
+ABI_VERSION = 8  # RT_ABI_VERSION of include/rt_core.h that the structs below mirror
 STATUS_NAMES = {0: "RT_OK", 1: "RT_ERR_INVALID_ARGUMENT", 2: "RT_ERR_NO_DEVICE", 3: "RT_ERR_CUDA",
                 4: "RT_ERR_SCRATCH_TOO_SMALL", 5: "RT_ERR_CAPACITY", 6: "RT_ERR_UNSUPPORTED"}
 DEVERR_NODE_CAPACITY = 0x1
@@ -76,7 +76,7 @@ class TraceDesc(C.Structure):
                 ("tmax", _P), ("ray_count", _U32), ("id_mode", _U32), ("hit_id", _P), ("hit_t", _P), ("hit_uv", _P),
                 ("ray_visits", _P), ("ray_tests", _P), ("error_word", _P), ("accel", _P), ("face_count_hint", _U32),
                 ("image_width", _U32), ("work_counter", _P), ("persistent_blocks_per_sm", _U32), ("schedule", _U32),
-                ("ray_order", _P)]
+                ("ray_order", _P), ("treelet_depth", _U32)]
 
 
 class InterpDesc(C.Structure):

@@ -313,6 +313,7 @@ def trace_desc(tree: Tree, orig, dir, tmax=None, id_mode: int = 0, counters: boo
         if sch.get("persistent", False):
             d.work_counter = _work_counter(dev, stream).data_ptr()
             d.persistent_blocks_per_sm = int(sch.get("blocks_per_sm", 8))
+            d.treelet_depth = int(sch.get("treelet", 0))  # top levels staged in shared memory (4-wide walks)
         d.schedule = ((_abi.TRACE_WHILE_WHILE if sch.get("while_while", False) else 0) | (_abi.TRACE_COOP if sch.get("coop", False) else 0)
                       | (_abi.TRACE_WIDE if sch.get("wide", False) else 0))
         if sch.get("sorted", False):

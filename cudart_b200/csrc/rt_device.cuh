@@ -348,13 +348,11 @@ __device__ __forceinline__ void cswap_tr(float (&t)[4], uint32_t (&r)[4], int a,
     const uint32_t rr = r[a]; r[a] = r[b]; r[b] = rr;
   }
 }
-__device__ __forceinline__ void wide_test(const float4* __restrict__ wn, const float4& oi, float ix, float iy, float iz, float tbest,
-                                          uint32_t skip, float (&t)[4], uint32_t (&r)[4]) {
-  float4 w0, w1, w2, w3, w4, w5, wrf, spare;  // the 128-byte record in four 32-byte loads
-  ldg8(wn, w0, w1);
-  ldg8(wn + 2, w2, w3);
-  ldg8(wn + 4, w4, w5);
-  ldg8(wn + 6, wrf, spare);
+// The test of a 4-wide record held in registers (w[0..5]: min x / y / z, max x / y / z of the 4 children;
+// w[6]: their references): entry distances (INFINITY for a miss) and references, nearest first.
+__device__ __forceinline__ void wide_test_regs(const float4 (&w)[8], const float4& oi, float ix, float iy, float iz, float tbest,
+                                               uint32_t skip, float (&t)[4], uint32_t (&r)[4]) {
+  const float4 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3], w4 = w[4], w5 = w[5], wrf = w[6];
   const uint4 wr = make_uint4(__float_as_uint(wrf.x), __float_as_uint(wrf.y), __float_as_uint(wrf.z), __float_as_uint(wrf.w));
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -371,6 +369,15 @@ __device__ __forceinline__ void wide_test(const float4* __restrict__ wn, const f
   cswap_tr(t, r, 0, 2);
   cswap_tr(t, r, 1, 3);
   cswap_tr(t, r, 1, 2);
+}
+__device__ __forceinline__ void wide_test(const float4* __restrict__ wn, const float4& oi, float ix, float iy, float iz, float tbest,
+                                          uint32_t skip, float (&t)[4], uint32_t (&r)[4]) {
+  float4 w[8];  // the 128-byte record in four 32-byte loads
+  ldg8(wn, w[0], w[1]);
+  ldg8(wn + 2, w[2], w[3]);
+  ldg8(wn + 4, w[4], w[5]);
+  ldg8(wn + 6, w[6], w[7]);
+  wide_test_regs(w, oi, ix, iy, iz, tbest, skip, t, r);
 }
 
 // ---------------------------------------------------------------------------

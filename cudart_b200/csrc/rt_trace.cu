@@ -129,7 +129,81 @@ struct AccelArgs {
   const float4* groups;
   const uint32_t* hdr;
   const float4* wide;  // 4-wide records
+  uint32_t stage = 0;        // shared-memory address of the staged top treelet (0: none; see stage_treelet)
+  uint32_t stage_depth = 0;  // levels of 4-wide records a persistent kernel stages (0: none)
 };
+
+// Top treelet in shared memory: the 4-wide records of the first `depth` levels below the root (breadth first, at
+// most 1 + 4 + 16 + 64 = 85 records, 10.9 KB), copied once per CTA of a persistent kernel. Inside the copy, the
+// reference to a child record that is staged as well becomes kStagedBit | slot, so a walk that starts at the
+// staged root reads those levels from shared memory and leaves them by an ordinary (global) reference.
+// Record indices are below 2^30 and the walk only looks for the bit on internal references.
+constexpr uint32_t kStagedBit = 0x40000000u;
+constexpr uint32_t kMaxStageDepth = 4;
+constexpr uint32_t kMaxStaged = 85;
+__host__ __device__ constexpr uint32_t staged_slots(uint32_t depth) {
+  return depth == 0 ? 0u : (depth == 1 ? 1u : (depth == 2 ? 5u : (depth == 3 ? 21u : 85u)));
+}
+
+__device__ uint32_t stage_treelet(const AccelArgs& C, float4* s_tree, uint32_t* s_rec, uint32_t depth) {
+  __shared__ uint32_t s_count;
+  if (threadIdx.x == 0) {
+    uint32_t n = 0;
+    if (__ldg(C.hdr) == 0u) {  // the root is record 0 (a leaf root has nothing to stage)
+      s_rec[n++] = 0;
+      uint32_t lo = 0;
+      for (uint32_t l = 1; l < depth; ++l) {
+        const uint32_t hi = n;
+        for (uint32_t q = lo; q < hi; ++q) {
+          const uint4 refs = __ldg((const uint4*)(C.wide + 8 * (size_t)s_rec[q] + 6));
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const uint32_t rk = u4c(refs, k);
+            if (rk != kNoChild && !(rk & 0x80000000u) && n < kMaxStaged) s_rec[n++] = rk;
+          }
+        }
+        lo = hi;
+      }
+    }
+    s_count = n;
+  }
+  __syncthreads();
+  const uint32_t n = s_count;
+  for (uint32_t i = threadIdx.x; i < n * 8; i += blockDim.x) {
+    const uint32_t q = i >> 3, j = i & 7u;
+    float4 v = __ldg(C.wide + 8 * (size_t)s_rec[q] + j);
+    if (j == 6) {  // child references: staged children become slot references
+      uint32_t rv[4] = {__float_as_uint(v.x), __float_as_uint(v.y), __float_as_uint(v.z), __float_as_uint(v.w)};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (rv[k] == kNoChild || (rv[k] & 0x80000000u)) continue;
+        for (uint32_t t = 1; t < n; ++t)
+          if (s_rec[t] == rv[k]) { rv[k] = kStagedBit | t; break; }
+      }
+      v = make_float4(__uint_as_float(rv[0]), __uint_as_float(rv[1]), __uint_as_float(rv[2]), __uint_as_float(rv[3]));
+    }
+    s_tree[i] = v;
+  }
+  __syncthreads();
+  return n ? (uint32_t)__cvta_generic_to_shared(s_tree) : 0u;
+}
+
+// The 128-byte record at shared-memory address a, as wide_test reads a global one.
+__device__ __forceinline__ void wide_test_staged(uint32_t a, const float4& oi, float ix, float iy, float iz, float tbest, uint32_t skip,
+                                                 float (&t)[4], uint32_t (&r)[4]) {
+  float4 w[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(w[j].x), "=f"(w[j].y), "=f"(w[j].z), "=f"(w[j].w) : "r"(a + 16u * j));
+  wide_test_regs(w, oi, ix, iy, iz, tbest, skip, t, r);
+}
+
+// A 4-wide record's test from global memory (staged == false) or from the staged treelet.
+__device__ __forceinline__ void wide_record_test(const AccelArgs& C, uint32_t ref, const float4& oi, float ix, float iy, float iz,
+                                                 float tbest, uint32_t skip, float (&t)[4], uint32_t (&r)[4]) {
+  if (ref & kStagedBit) wide_test_staged(C.stage + 128u * (ref & ~kStagedBit), oi, ix, iy, iz, tbest, skip, t, r);
+  else wide_test(C.wide + 8 * (size_t)ref, oi, ix, iy, iz, tbest, skip, t, r);
+}
 
 // One ray through the blob. kWW: "while-while" schedule (descend internal
 // nodes until the ray holds a leaf, then test the leaf), which keeps the lanes
@@ -195,7 +269,7 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
     uint32_t st_ref[kStack];
     float st_t[kStack];
     int sp = 0;
-    const uint32_t root = __ldg(C.hdr);
+    const uint32_t root = C.stage ? kStagedBit : __ldg(C.hdr);
     uint32_t ref = root, skip = kNoSkip;
     bool alive = true;
     if (kSeed) alive = seed_start<kCount>(r, S, C, oi, ix, iy, iz, bt, root, ref, skip, phase, visits);
@@ -220,7 +294,7 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
           // 4-wide record: up to four children tested at once, nearest first
           float wt[4];
           uint32_t wr[4];
-          wide_test(C.wide + 8 * (size_t)ref, oi, ix, iy, iz, bt, (kSeed && phase) ? skip : kNoSkip, wt, wr);
+          wide_record_test(C, ref, oi, ix, iy, iz, bt, (kSeed && phase) ? skip : kNoSkip, wt, wr);
           if (kCount) visits += 4;
           if (wt[0] == INFINITY) {
             if (!next()) {
@@ -355,7 +429,7 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
   uint32_t st_ref[kStack];
   float st_t[kStack];
   int sp = 0;
-  const uint32_t root = __ldg(C.hdr);
+  const uint32_t root = C.stage ? kStagedBit : __ldg(C.hdr);
   uint32_t ref = root, skip = kNoSkip;
   uint32_t phase = 1, best_phase = 1;
   bool go = true;
@@ -382,7 +456,7 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
           // 4-wide record: up to four children tested at once, nearest first
           float wt[4];
           uint32_t wr[4];
-          wide_test(C.wide + 8 * (size_t)ref, oi, ix, iy, iz, bt, (kSeed && phase) ? skip : kNoSkip, wt, wr);
+          wide_record_test(C, ref, oi, ix, iy, iz, bt, (kSeed && phase) ? skip : kNoSkip, wt, wr);
           if (kCount) visits += 4;
           if (wt[0] == INFINITY) {
             if (!next()) {
@@ -622,6 +696,9 @@ __global__ __launch_bounds__(128, kSeed ? 6 : (kCount ? 0 : 7)) void k_trace_coo
                                                                           SeedArgs S) {
   __shared__ unsigned long long s_key[kCoopWarps][32];
   __shared__ float2 s_uv[kCoopWarps][32];
+  __shared__ uint32_t s_rec[kMaxStaged];
+  extern __shared__ float4 s_tree[];
+  if (kWide && C.stage_depth) C.stage = stage_treelet(C, s_tree, s_rec, C.stage_depth);
   const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
   for (;;) {
     uint32_t base = 0;
@@ -639,6 +716,9 @@ __global__ __launch_bounds__(128, kSeed ? 6 : (kCount ? 0 : 7)) void k_trace_coo
 // until the slots run out (the counter is zeroed before the launch).
 template <bool kCount, bool kWW, bool kSeed, bool kWide>
 __global__ __launch_bounds__(128) void k_trace_accel_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter, SeedArgs S) {
+  __shared__ uint32_t s_rec[kMaxStaged];
+  extern __shared__ float4 s_tree[];
+  if (kWide && C.stage_depth) C.stage = stage_treelet(C, s_tree, s_rec, C.stage_depth);
   const uint32_t lane = lane_id();
   for (;;) {
     uint32_t base = 0;
@@ -987,6 +1067,9 @@ rt_status launch_accel_w(const rt_trace_desc* d, const TraceArgs& A, const SeedA
     carve_accel(c, AL, (uint32_t)n);
     C.hdr = AL.hdr; C.tnodes = AL.tnodes; C.leaves = AL.leaves; C.groups = AL.groups; C.wide = AL.wide;
   }
+  // the top treelet is staged by the persistent kernels of the 4-wide walk only (one copy per CTA)
+  C.stage_depth = (kWide && d->work_counter) ? (d->treelet_depth < kMaxStageDepth ? d->treelet_depth : kMaxStageDepth) : 0u;
+  const size_t stage_smem = (size_t)staged_slots(C.stage_depth) * 128;
   SlotMap M;
   M.order = d->ray_order;
   const uint32_t R = d->ray_count;
@@ -1006,14 +1089,15 @@ rt_status launch_accel_w(const rt_trace_desc* d, const TraceArgs& A, const SeedA
   if (d->work_counter && cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
   if (d->schedule & RT_TRACE_COOP) {
     if (d->work_counter) {
-      if (count) k_trace_coop_persistent<true, kSeed, kWide><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter, S);
-      else k_trace_coop_persistent<false, kSeed, kWide><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter, S);
+      if (count) k_trace_coop_persistent<true, kSeed, kWide><<<pblocks, 128, stage_smem, st>>>(A, C, M, d->work_counter, S);
+      else k_trace_coop_persistent<false, kSeed, kWide><<<pblocks, 128, stage_smem, st>>>(A, C, M, d->work_counter, S);
     } else {
       if (count) k_trace_coop<true, kSeed, kWide><<<sblocks, 128, 0, st>>>(A, C, M, S);
       else k_trace_coop<false, kSeed, kWide><<<sblocks, 128, 0, st>>>(A, C, M, S);
     }
   } else if (d->work_counter) {
-#define RT_LAUNCH_P(CNT, WW) k_trace_accel_persistent<CNT, WW, kSeed, kWide><<<pblocks, 128, 0, st>>>(A, C, M, d->work_counter, S)
+#define RT_LAUNCH_P(CNT, WW) \
+  k_trace_accel_persistent<CNT, WW, kSeed, kWide><<<pblocks, 128, stage_smem, st>>>(A, C, M, d->work_counter, S)
     if (count) { if (ww) RT_LAUNCH_P(true, true); else RT_LAUNCH_P(true, false); }
     else { if (ww) RT_LAUNCH_P(false, true); else RT_LAUNCH_P(false, false); }
 #undef RT_LAUNCH_P

@@ -1,6 +1,8 @@
 """Autotuner for the traversal schedule.
 
-The blob traversal has knobs that change its speed and never its results:
+The blob traversal has knobs that change its speed and never its results
+(including how many top levels of 4-wide records a persistent CTA stages in
+shared memory):
 the ray-to-thread mapping (linear, 8x4 pixel tiles of a row-major image, or
 an order sorted by direction octant and origin Morton code, whose cost is
 part of the timed trace),
@@ -41,6 +43,9 @@ def candidates(image_width: int):
         out.append({"image_width": w, "persistent": p, "blocks_per_sm": bps, "while_while": True, "sorted": srt, "coop": True})
     # every schedule again with the 4-wide records
     out += [dict(c, wide=True) for c in out]
+    # persistent while-while 4-wide walks with the top 2 or 3 levels of records staged in shared memory per CTA
+    out += [dict(c, treelet=depth) for c in out if c.get("wide") and c.get("persistent") and c.get("while_while")
+            and c.get("blocks_per_sm") == 8 for depth in (2, 3)]
     return out
 
 

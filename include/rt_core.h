@@ -35,7 +35,7 @@ typedef struct CUstream_st* rt_stream; /* a cudaStream_t; NULL = legacy default 
 /* Layout version of the structs below. A caller compiled against this header
  * must check rt_abi_version() == RT_ABI_VERSION before passing any struct:
  * a library built from a different header reads different field offsets. */
-#define RT_ABI_VERSION 7u
+#define RT_ABI_VERSION 8u
 
 typedef enum rt_status {
   RT_OK = 0,
@@ -275,6 +275,8 @@ typedef struct rt_trace_desc {
   uint32_t persistent_blocks_per_sm; /* with work_counter: CTAs of 128 threads per SM (0 = 8) */
   uint32_t schedule;        /* RT_TRACE_* bits */
   const uint32_t* ray_order; /* optional permutation from rt_ray_order: threads take rays in this order */
+  uint32_t treelet_depth;   /* persistent 4-wide walks: levels of 4-wide records below the root (0..4, at most 85
+                               records, 10.9 KB) that each CTA copies to shared memory and reads from there (0: none) */
 } rt_trace_desc;
 
 #define RT_TRACE_WHILE_WHILE 0x1u /* descend until a leaf is held, then test it (else: interleaved) */
