@@ -131,6 +131,11 @@ struct AccelArgs {
   const float4* wide;  // 4-wide records
   uint32_t stage = 0;        // shared-memory address of the staged top treelet (0: none; see stage_treelet)
   uint32_t stage_depth = 0;  // levels of 4-wide records a persistent kernel stages (0: none)
+  // Batched walks: the ray's mesh's first face position F and first group G. Its records, leaves, groups and
+  // triangles are addressed from the batch's base pointers plus these offsets (two 32-bit registers per lane
+  // instead of a 64-bit pointer per array); a single mesh has F = G = 0.
+  uint32_t F = 0;
+  uint32_t G = 0;
 };
 
 // Top treelet in shared memory: the 4-wide records of the first `depth` levels below the root (breadth first, at
@@ -202,7 +207,7 @@ __device__ __forceinline__ void wide_test_staged(uint32_t a, const float4& oi, f
 __device__ __forceinline__ void wide_record_test(const AccelArgs& C, uint32_t ref, const float4& oi, float ix, float iy, float iz,
                                                  float tbest, uint32_t skip, float (&t)[4], uint32_t (&r)[4]) {
   if (ref & kStagedBit) wide_test_staged(C.stage + 128u * (ref & ~kStagedBit), oi, ix, iy, iz, tbest, skip, t, r);
-  else wide_test(C.wide + 8 * (size_t)ref, oi, ix, iy, iz, tbest, skip, t, r);
+  else wide_test(C.wide + 8 * ((size_t)C.F + ref), oi, ix, iy, iz, tbest, skip, t, r);
 }
 
 // One ray through the blob. kWW: "while-while" schedule (descend internal
@@ -317,7 +322,7 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
             ref = wr[0];
           }
         } else {
-        const float4* tn = C.tnodes + 4 * (size_t)ref;
+        const float4* tn = C.tnodes + 4 * ((size_t)C.F + ref);
         float4 a0, a1, b0, b1;
         ldg8(tn, a0, a1);
         ldg8(tn + 2, b0, b1);
@@ -353,21 +358,21 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
       }
       if (!alive) break;
       // leaf: group boxes, then the triangles of the groups that pass
-      const uint4 L = __ldg(C.leaves + (~ref));
+      const uint4 L = __ldg(C.leaves + (C.F + ~ref));
       if (kCount) ++visits;
       const uint32_t first = L.x, cnt = L.y, gbase = L.z;
       for (uint32_t g = 0; g * 8 < cnt; ++g) {
         float4 gmn, gmx;
-        ldg8(C.groups + 2 * ((size_t)gbase + g), gmn, gmx);
+        ldg8(C.groups + 2 * ((size_t)C.G + gbase + g), gmn, gmx);
         if (kCount) ++visits;
         float tg;
         if (!slab2(gmn, gmx, oi, ix, iy, iz, bt, tg)) continue;
         const uint32_t kend = min(cnt, g * 8 + 8);
         for (uint32_t k = g * 8; k < kend; ++k) {
           const uint32_t pos = first + k;
-          const float4 v0 = ldg4(A.tris + 3 * (size_t)pos);
-          const float4 e1 = ldg4(A.tris + 3 * (size_t)pos + 1);
-          const float4 e2 = ldg4(A.tris + 3 * (size_t)pos + 2);
+          const float4 v0 = ldg4(A.tris + 3 * ((size_t)C.F + pos));
+          const float4 e1 = ldg4(A.tris + 3 * ((size_t)C.F + pos) + 1);
+          const float4 e2 = ldg4(A.tris + 3 * ((size_t)C.F + pos) + 2);
           if (kCount) ++tests;
           float t, u, v;
           if (!mt_test(o, d, zu, zv, v0, e1, e2, t, u, v)) continue;
@@ -382,7 +387,7 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
     }
   }
   if (best >= 0) {
-    A.hit_id[r] = A.id_mode == 1 ? (int32_t)__ldg(A.indices + best) : best;
+    A.hit_id[r] = A.id_mode == 1 ? (int32_t)__ldg(A.indices + C.F + best) : best;
     A.hit_t[r] = bt;
     A.hit_uv[r] = make_float2(bu, bv);
   } else {
@@ -479,7 +484,7 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
             ref = wr[0];
           }
         } else {
-        const float4* tn = C.tnodes + 4 * (size_t)ref;
+        const float4* tn = C.tnodes + 4 * ((size_t)C.F + ref);
         float4 a0, a1, b0, b1;
         ldg8(tn, a0, a1);
         ldg8(tn + 2, b0, b1);
@@ -517,14 +522,14 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
     // 2. own leaf: group boxes -> mask of groups to test
     uint32_t mask = 0, first = 0, cnt = 0;
     if (has_leaf) {
-      const uint4 L = __ldg(C.leaves + (~ref));
+      const uint4 L = __ldg(C.leaves + (C.F + ~ref));
       if (kCount) ++visits;
       first = L.x; cnt = L.y;
       const uint32_t gbase = L.z;
       const uint32_t ng = (cnt + 7) >> 3;
       for (uint32_t g = 0; g < ng; ++g) {
         float4 gmn, gmx;
-        ldg8(C.groups + 2 * ((size_t)gbase + g), gmn, gmx);
+        ldg8(C.groups + 2 * ((size_t)C.G + gbase + g), gmn, gmx);
         if (kCount) ++visits;
         float tg;
         if (slab2(gmn, gmx, oi, ix, iy, iz, bt, tg)) {
@@ -579,7 +584,7 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
       const uint32_t ofirst = __shfl_sync(0xffffffffu, first, owner);
       const uint32_t ocnt = __shfl_sync(0xffffffffu, cnt, owner);
       // the owner's triangle stream (lanes of a batched launch may trace different meshes)
-      const float4* otris = (const float4*)__shfl_sync(0xffffffffu, (unsigned long long)A.tris, owner);
+      const float4* otris = A.tris + 3 * (size_t)__shfl_sync(0xffffffffu, C.F, owner);
       if (item < total) {
         const uint32_t g = __fns(omask, 0, (int)(item - oexcl) + 1);
         const uint32_t kend = min(ocnt, g * 8 + 8);
@@ -617,17 +622,17 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
       }
       // groups beyond the first 32 (leaves of more than 256 triangles): this lane alone
       for (uint32_t g = 32; g * 8 < cnt; ++g) {
-        const uint32_t gbase = __ldg(C.leaves + (~ref)).z;
+        const uint32_t gbase = __ldg(C.leaves + (C.F + ~ref)).z;
         float4 gmn, gmx;
-        ldg8(C.groups + 2 * ((size_t)gbase + g), gmn, gmx);
+        ldg8(C.groups + 2 * ((size_t)C.G + gbase + g), gmn, gmx);
         float tg;
         if (!slab2(gmn, gmx, oi, ix, iy, iz, bt, tg)) continue;
         const uint32_t kend = min(cnt, g * 8 + 8);
         for (uint32_t kk = g * 8; kk < kend; ++kk) {
           const uint32_t pos = first + kk;
-          const float4 v0 = ldg4(A.tris + 3 * (size_t)pos);
-          const float4 e1 = ldg4(A.tris + 3 * (size_t)pos + 1);
-          const float4 e2 = ldg4(A.tris + 3 * (size_t)pos + 2);
+          const float4 v0 = ldg4(A.tris + 3 * ((size_t)C.F + pos));
+          const float4 e1 = ldg4(A.tris + 3 * ((size_t)C.F + pos) + 1);
+          const float4 e2 = ldg4(A.tris + 3 * ((size_t)C.F + pos) + 2);
           if (kCount) ++tests;
           float t, u, v;
           if (!mt_test(o, d, zu, zv, v0, e1, e2, t, u, v)) continue;
@@ -644,7 +649,7 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
   if (!valid) return;
   if (kSeed && S.in_prop) S.in_prop[r] = (best >= 0 && best_phase == 0) ? 1 : 0;
   if (best >= 0) {
-    A.hit_id[r] = A.id_mode == 1 ? (int32_t)__ldg(A.indices + best) : best;
+    A.hit_id[r] = A.id_mode == 1 ? (int32_t)__ldg(A.indices + C.F + best) : best;
     A.hit_t[r] = bt;
     A.hit_uv[r] = make_float2(bu, bv);
   } else {
@@ -677,6 +682,7 @@ template <bool kCount, bool kWW, bool kSeed, bool kWide>
 __global__ __launch_bounds__(128) void k_trace_accel(TraceArgs A, AccelArgs C, SlotMap M, SeedArgs S) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t r;
+  C.F = C.G = 0;  // one mesh: no offsets (known to the compiler)
   if (s < M.slots && M.ray_of(s, r)) trace_ray_accel<kCount, kWW, kSeed, kWide>(r, A, C, S);
 }
 
@@ -688,6 +694,7 @@ __global__ __launch_bounds__(128, kSeed ? 6 : 0) void k_trace_coop(TraceArgs A, 
   uint32_t r = 0;
   const bool valid = s < M.slots && M.ray_of(s, r);
   const uint32_t w = threadIdx.x >> 5;
+  C.F = C.G = 0;
   trace_warp_coop<kCount, kSeed, kWide>(r, valid, A, C, s_key[w], s_uv[w], S);
 }
 
@@ -698,6 +705,7 @@ __global__ __launch_bounds__(128, kSeed ? 6 : (kCount ? 0 : 7)) void k_trace_coo
   __shared__ float2 s_uv[kCoopWarps][32];
   __shared__ uint32_t s_rec[kMaxStaged];
   extern __shared__ float4 s_tree[];
+  C.F = C.G = 0;
   if (kWide && C.stage_depth) C.stage = stage_treelet(C, s_tree, s_rec, C.stage_depth);
   const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
   for (;;) {
@@ -718,6 +726,7 @@ template <bool kCount, bool kWW, bool kSeed, bool kWide>
 __global__ __launch_bounds__(128) void k_trace_accel_persistent(TraceArgs A, AccelArgs C, SlotMap M, uint32_t* counter, SeedArgs S) {
   __shared__ uint32_t s_rec[kMaxStaged];
   extern __shared__ float4 s_tree[];
+  C.F = C.G = 0;
   if (kWide && C.stage_depth) C.stage = stage_treelet(C, s_tree, s_rec, C.stage_depth);
   const uint32_t lane = lane_id();
   for (;;) {
@@ -750,20 +759,19 @@ __device__ __forceinline__ void batch_trace_ray(uint32_t r, const TraceArgs& A, 
   const uint32_t F = __ldg(B.foff + m);
   AccelArgs C;
   C.hdr = B.acc.hdr + 64 * (size_t)m;
-  C.tnodes = B.acc.tnodes + 4 * (size_t)F;
-  C.leaves = B.acc.leaves + F;
-  C.groups = B.acc.groups + 2 * (size_t)group_base(F, m);
-  C.wide = B.acc.wide + 8 * (size_t)F;
-  TraceArgs Am = A;
-  Am.tris = A.tris + 3 * (size_t)F;
-  Am.indices = A.indices + F;
+  C.tnodes = B.acc.tnodes;
+  C.leaves = B.acc.leaves;
+  C.groups = B.acc.groups;
+  C.wide = B.acc.wide;
+  C.F = F;
+  C.G = group_base(F, m);
   if constexpr (kSeed) {
     SeedArgs Sm = S;
     Sm.slot_ref = S.slot_ref + (size_t)m * S.slot_count;
     if (S.slot_box) Sm.slot_box = S.slot_box + 2 * (size_t)m * S.slot_count;
-    trace_ray_accel<kCount, kWW, true, kWide>(r, Am, C, Sm);
+    trace_ray_accel<kCount, kWW, true, kWide>(r, A, C, Sm);
   } else {
-    trace_ray_accel<kCount, kWW, false, kWide>(r, Am, C);
+    trace_ray_accel<kCount, kWW, false, kWide>(r, A, C);
   }
 }
 
@@ -781,13 +789,9 @@ __device__ __forceinline__ void batch_ray_args(uint32_t r, const TraceArgs& A, c
   const uint32_t m = find_seg(B.roff, B.M, r);
   const uint32_t F = __ldg(B.foff + m);
   C.hdr = B.acc.hdr + 64 * (size_t)m;
-  C.tnodes = B.acc.tnodes + 4 * (size_t)F;
-  C.leaves = B.acc.leaves + F;
-  C.groups = B.acc.groups + 2 * (size_t)group_base(F, m);
-  C.wide = B.acc.wide + 8 * (size_t)F;
+  C.F = F;
+  C.G = group_base(F, m);
   Am = A;
-  Am.tris = A.tris + 3 * (size_t)F;
-  Am.indices = A.indices + F;
   Sm = S;
   if (kSeed) {
     Sm.slot_ref = S.slot_ref + (size_t)m * S.slot_count;
@@ -813,13 +817,10 @@ __global__ __launch_bounds__(128, kSeed ? 6 : (kCount ? 0 : 7)) void k_batch_tra
     const bool valid = slot < A.ray_count;
     const uint32_t r = valid ? B.ray_of(slot) : slot;
     TraceArgs Am = A;
-    AccelArgs C = {};
+    AccelArgs C = {};  // the batch's base pointers (uniform); each lane adds its mesh's offsets
+    C.hdr = B.acc.hdr; C.tnodes = B.acc.tnodes; C.leaves = B.acc.leaves; C.groups = B.acc.groups; C.wide = B.acc.wide;
     SeedArgs Sm = S;
-    if (valid) {
-      batch_ray_args<kSeed>(r, A, B, S, Am, C, Sm);
-    } else {  // idle lanes read mesh 0's header only
-      C.hdr = B.acc.hdr; C.tnodes = B.acc.tnodes; C.leaves = B.acc.leaves; C.groups = B.acc.groups; C.wide = B.acc.wide;
-    }
+    if (valid) batch_ray_args<kSeed>(r, A, B, S, Am, C, Sm);  // idle lanes keep mesh 0's header and zero offsets
     trace_warp_coop<kCount, kSeed, kWide>(r, valid, Am, C, s_key[w], s_uv[w], Sm);
   }
 }
