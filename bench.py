@@ -217,9 +217,10 @@ class ClockSampler:
 # headline: instanced frames (plain path timed per frame; learned path beside it)
 # ----------------------------------------------------------------------------
 def batch_kernel(sched):
+    base = "k_batch_trace_clusters" if sched.get("clusters") else "k_batch_trace"
     if sched.get("coop"):
-        return "k_batch_trace_coop"
-    return "k_batch_trace_persistent" if sched.get("persistent") else "k_batch_trace"
+        return base + "_coop"
+    return base + "_persistent" if sched.get("persistent") else base
 
 
 def run_headline(args, rank, world, local_rank):
@@ -315,6 +316,8 @@ def run_headline(args, rank, world, local_rank):
     # build: algorithmic bytes per face = 16 face + 48 vertices + 32 box + 8 code/index + 64 sort + 4 split scan
     # + 32 leaf gather + 36 reorder + 48 triangle stream, + 64 per node (write + child read)
     build_bytes = F * (16 + 48 + 32 + 8 + 64 + 4 + 32 + 36 + 48) + 64 * nodes_total
+    if w.clusters:  # cluster trees: codes + triangles read, position and node boxes, child pairs, arrival words
+        build_bytes += F * (4 + 48 + 32 + 32 + 8 + 4)
     bgbs = build_bytes / (build_ms / K * 1e-3) / 1e9
     result = {
         "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
@@ -326,8 +329,8 @@ def run_headline(args, rank, world, local_rank):
                   "roofline": {"bound": "hbm", "achieved": round(bgbs, 1), "peak": peak, "unit": "GB/s", "frac": round(bgbs / peak, 4)}},
         "trace": {"mrays_s": round(world * rays_total / ((t1_ms + t2_ms) * 1e-3) / 1e6, 1), "primary_ms": round(t1_ms / K, 3),
                   "bounce_ms": round(t2_ms / K, 3)},
-        "roofline": {k: roof[k] for k in ("bound", "kernel", "launch", "launch_ms", "achieved", "peak", "unit", "frac", "traffic",
-                                          "model_frac", "l1_frac", "limiter")},
+        "roofline": {k: roof.get(k) for k in ("bound", "kernel", "launch", "launch_ms", "achieved", "peak", "unit", "frac", "traffic",
+                                              "model_frac", "l1_frac", "limiter")},
         "gpu_launches": int(kernels_per_step * K),
     }
     clocks = clk.summary()
@@ -371,6 +374,7 @@ def learned_frames(w, args, dev, world, plain, first_frame):
 
     w.remember(plain)
     learned = w.trace_learned()
+    sp, sb = w.seeded_schedules()
     torch.cuda.synchronize()
     ev = []
     mism = torch.zeros(1, dtype=torch.int64, device=dev)
@@ -389,13 +393,13 @@ def learned_frames(w, args, dev, world, plain, first_frame):
         learned["p1"] = w.nets.propose(w.orig, w.dir, w.box, R, out=learned["p1"])
         e[3].record()
         proposal.batch_trace_seeded(w.tree, w.orig, w.dir, w.ray_offsets, learned["p1"], w.slots, in_proposal=True,
-                                    out=learned["h1"], schedule=w.schedule_primary)
+                                    out=learned["h1"], schedule=sp)
         e[4].record()
         b = plain["b"]  # the seeded hits equal the plain ones, so the bounces are the same rays
         learned["p2"] = w.nets.propose(b[0], b[1], w.box, R, out=learned["p2"], tmax=b[2])
         e[5].record()
         proposal.batch_trace_seeded(w.tree, b[0], b[1], w.ray_offsets, learned["p2"], w.slots, tmax=b[2], in_proposal=True,
-                                    out=learned["h2"], schedule=w.schedule_bounce, order=w.bounce_order(b))
+                                    out=learned["h2"], schedule=sb, order=w.seeded_order(b))
         e[6].record()
         for k in ("h1", "h2"):
             mism += (plain[k]["id"] != learned[k]["id"]).sum() + (plain[k]["t"].view(torch.int32) != learned[k]["t"].view(torch.int32)).sum()
@@ -416,10 +420,10 @@ def learned_frames(w, args, dev, world, plain, first_frame):
     torch.cuda.synchronize()
     o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     o0.record()
-    proposal.batch_trace_seeded(w.tree, w.orig, w.dir, w.ray_offsets, l1, w.slots, out=learned["h1"], schedule=w.schedule_primary)
+    proposal.batch_trace_seeded(w.tree, w.orig, w.dir, w.ray_offsets, l1, w.slots, out=learned["h1"], schedule=sp)
     b = plain["b"]
-    proposal.batch_trace_seeded(w.tree, b[0], b[1], w.ray_offsets, l2, w.slots, tmax=b[2], out=learned["h2"], schedule=w.schedule_bounce,
-                                order=w.bounce_order(b))
+    proposal.batch_trace_seeded(w.tree, b[0], b[1], w.ray_offsets, l2, w.slots, tmax=b[2], out=learned["h2"], schedule=sb,
+                                order=w.seeded_order(b))
     o1.record()
     torch.cuda.synchronize()
     oracle_ms = o0.elapsed_time(o1)

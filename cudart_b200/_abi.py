@@ -13,17 +13,20 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librt_core.so")
 
 RT_OK = 0
-ABI_VERSION = 8  # RT_ABI_VERSION of include/rt_core.h that the structs below mirror
+ABI_VERSION = 9  # RT_ABI_VERSION of include/rt_core.h that the structs below mirror
 STATUS_NAMES = {0: "RT_OK", 1: "RT_ERR_INVALID_ARGUMENT", 2: "RT_ERR_NO_DEVICE", 3: "RT_ERR_CUDA",
                 4: "RT_ERR_SCRATCH_TOO_SMALL", 5: "RT_ERR_CAPACITY", 6: "RT_ERR_UNSUPPORTED"}
 DEVERR_NODE_CAPACITY = 0x1
 DEVERR_STACK_OVERFLOW = 0x2
 DEVERR_MORTON_CAPACITY = 0x4
 DEVERR_WAIT_TIMEOUT = 0x8
+DEVERR_ACCEL_MISSING = 0x10
 PROPOSE_ABI_VERSION = 2  # RT_PROPOSE_ABI_VERSION of include/rt_propose.h
 TRACE_WHILE_WHILE = 0x1
 TRACE_COOP = 0x2
 TRACE_WIDE = 0x4
+TRACE_CLUSTERS = 0x8
+ACCEL_CLUSTERS = 0x2
 
 # every symbol include/rt_core.h declares
 EXPORTS = (
@@ -56,7 +59,8 @@ class RtError(RuntimeError):
 
 
 class BuildParams(C.Structure):
-    _fields_ = [("tree_depth", _U32), ("tree_complete", _U32), ("min_leaf", _U32), ("max_leaf", _U32), ("morton_bits", _U32)]
+    _fields_ = [("tree_depth", _U32), ("tree_complete", _U32), ("min_leaf", _U32), ("max_leaf", _U32), ("morton_bits", _U32),
+                ("accel_trees", _U32), ("cluster_leaf", _U32)]
 
 
 class BuildInfo(C.Structure):

@@ -96,6 +96,7 @@ class Tree:
     tris: torch.Tensor  # float32 (N, 12) {v0, e1, e2}
     info: torch.Tensor  # int32 (8,) rt_build_info, on the device
     accel: torch.Tensor | None = None  # uint8 traversal blob (two-child records, leaf table, group boxes)
+    clusters: bool = False  # the blob also holds the cluster tree (schedules with "clusters": True walk it)
 
     def info_host(self) -> dict:
         vals = self.info.cpu().tolist()
@@ -110,8 +111,8 @@ class Tree:
         return self.nodes[: self.node_count].cpu()
 
 
-def lbvh_scratch_bytes(face_count: int, tree_depth=12, tree_complete=True, morton_bits=32, min_leaf=0, max_leaf=0):
-    params = _abi.BuildParams(tree_depth, int(tree_complete), min_leaf, max_leaf, morton_bits)
+def lbvh_scratch_bytes(face_count: int, tree_depth=12, tree_complete=True, morton_bits=32, min_leaf=0, max_leaf=0, clusters=False):
+    params = _abi.BuildParams(tree_depth, int(tree_complete), min_leaf, max_leaf, morton_bits, _abi.ACCEL_CLUSTERS if clusters else 0)
     nb = C.c_size_t(0)
     mx = C.c_uint32(0)
     _abi.check("rt_lbvh_scratch_bytes", _abi.lib().rt_lbvh_scratch_bytes(face_count, C.byref(params), C.byref(nb), C.byref(mx)))
@@ -126,15 +127,17 @@ def accel_bytes(face_count: int) -> int:
 
 def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_depth: int = 12, tree_complete: bool = True,
                morton_bits: int = 32, out: Tree | None = None, accel: bool = True, min_leaf: int = 0, max_leaf: int = 0,
-               stream=None) -> Tree:
+               stream=None, clusters: bool = False, cluster_leaf: int = 0) -> Tree:
     """LBVH build of a mesh given as float4 vertices (V, 4) and uint4 faces (N, 4).
     hitbox: host sequence of 8 floats (min xyzw, max xyzw) or None for the
-    vertices' min/max."""
+    vertices' min/max. clusters: also write the cluster tree into the blob
+    (RT_ACCEL_CLUSTERS, leaves of at most cluster_leaf positions, 0 = 4), for
+    schedules with "clusters": True."""
     _need_cuda(vertices, "vertices", _F32, 4)
     _need_cuda(faces, "faces", _I32, 4)
     n = faces.shape[0]
     dev = vertices.device
-    nbytes, max_nodes = lbvh_scratch_bytes(n, tree_depth, tree_complete, morton_bits, min_leaf, max_leaf)
+    nbytes, max_nodes = lbvh_scratch_bytes(n, tree_depth, tree_complete, morton_bits, min_leaf, max_leaf, clusters=clusters)
     if out is None:
         out = Tree(
             nodes=torch.empty((max_nodes, 8), dtype=torch.int32, device=dev),
@@ -157,7 +160,8 @@ def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_de
     d.faces_in = faces.data_ptr()
     d.faces_out = out.faces.data_ptr()
     d.hitbox = C.cast(hb, C.c_void_p).value if hb is not None else None
-    d.params = _abi.BuildParams(tree_depth, int(tree_complete), min_leaf, max_leaf, morton_bits)
+    d.params = _abi.BuildParams(tree_depth, int(tree_complete), min_leaf, max_leaf, morton_bits,
+                                _abi.ACCEL_CLUSTERS if clusters else 0, cluster_leaf)
     d.boxes = out.boxes.data_ptr()
     d.indices = out.indices.data_ptr()
     d.codes = out.codes.data_ptr()
@@ -171,6 +175,7 @@ def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_de
         d.accel = out.accel.data_ptr()
         d.accel_bytes = out.accel.numel()
     _abi.check("rt_lbvh_build", _abi.lib().rt_lbvh_build(C.byref(d), _stream(stream)))
+    out.clusters = bool(clusters and out.accel is not None)
     if hitbox is not None:  # the scene box for ray ordering, known on the host: no device read later
         out._box = [float(hitbox[i]) for i in (0, 1, 2, 4, 5, 6)]
     return out
@@ -315,7 +320,7 @@ def trace_desc(tree: Tree, orig, dir, tmax=None, id_mode: int = 0, counters: boo
             d.persistent_blocks_per_sm = int(sch.get("blocks_per_sm", 8))
             d.treelet_depth = int(sch.get("treelet", 0))  # top levels staged in shared memory (4-wide walks)
         d.schedule = ((_abi.TRACE_WHILE_WHILE if sch.get("while_while", False) else 0) | (_abi.TRACE_COOP if sch.get("coop", False) else 0)
-                      | (_abi.TRACE_WIDE if sch.get("wide", False) else 0))
+                      | (_abi.TRACE_WIDE if sch.get("wide", False) else 0) | (_abi.TRACE_CLUSTERS if sch.get("clusters", False) else 0))
         if sch.get("sorted", False):
             order = ray_order(orig, dir, tmax, tree_box(tree), ray_count=R, stream=stream)
             out["_order"] = order  # keep it alive until the trace has run
@@ -545,6 +550,7 @@ class BatchTree:
     tris: torch.Tensor
     accel: torch.Tensor
     info: torch.Tensor            # int32 (M, 8)
+    clusters: bool = False        # the blob also holds every mesh's cluster tree
 
     @property
     def mesh_count(self) -> int:
@@ -558,14 +564,15 @@ class BatchTree:
 
 
 def batch_build(vertices: torch.Tensor, faces: torch.Tensor, face_offsets: list, vertex_offsets: list, tree_depth: int = 12,
-                out: BatchTree | None = None, stream=None) -> BatchTree:
-    """Builds every mesh of a concatenated batch (faces index their own mesh's vertices from 0)."""
+                out: BatchTree | None = None, stream=None, clusters: bool = False, cluster_leaf: int = 0) -> BatchTree:
+    """Builds every mesh of a concatenated batch (faces index their own mesh's vertices from 0); clusters: also
+    every mesh's cluster tree (RT_ACCEL_CLUSTERS), for schedules with "clusters": True."""
     _need_cuda(vertices, "vertices", _F32, 4)
     _need_cuda(faces, "faces", _I32, 4)
     M = len(face_offsets) - 1
     N = faces.shape[0]
     dev = vertices.device
-    params = _abi.BuildParams(tree_depth, 1, 0, 0, 32)
+    params = _abi.BuildParams(tree_depth, 1, 0, 0, 32, _abi.ACCEL_CLUSTERS if clusters else 0, cluster_leaf)
     sb, ab = C.c_size_t(0), C.c_size_t(0)
     _abi.check("rt_batch_sizes", _abi.lib().rt_batch_sizes(M, N, C.byref(params), C.byref(sb), C.byref(ab)))
     if out is None:
@@ -592,6 +599,7 @@ def batch_build(vertices: torch.Tensor, faces: torch.Tensor, face_offsets: list,
     d.tris, d.accel, d.accel_bytes = out.tris.data_ptr(), out.accel.data_ptr(), out.accel.numel()
     d.info, d.scratch, d.scratch_bytes = out.info.data_ptr(), scratch.data_ptr(), scratch.numel()
     _abi.check("rt_batch_build", _abi.lib().rt_batch_build(C.byref(d), _stream(stream)))
+    out.clusters = bool(clusters)
     return out
 
 
@@ -678,7 +686,8 @@ def batch_trace_desc(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax
     sch = dict(while_while=while_while) if schedule is None else schedule
     d.schedule = ((_abi.TRACE_WHILE_WHILE if sch.get("while_while", False) else 0)
                   | (_abi.TRACE_WIDE if sch.get("wide", False) else 0)
-                  | (_abi.TRACE_COOP if sch.get("coop", False) else 0))
+                  | (_abi.TRACE_COOP if sch.get("coop", False) else 0)
+                  | (_abi.TRACE_CLUSTERS if sch.get("clusters", False) else 0))
     if order is not None:
         d.ray_order = order.data_ptr()
     elif sch.get("tiles"):  # every mesh's rays are a row-major image of the same size: 8 x 4 pixel tiles per warp

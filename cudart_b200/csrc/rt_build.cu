@@ -597,6 +597,7 @@ __global__ __launch_bounds__(256) void k_accel_nodes(const uint32_t* __restrict_
                                                     const uint32_t* __restrict__ leaf_lambda, float4* __restrict__ tnodes,
                                                     float4* __restrict__ wide, uint32_t* __restrict__ acc_hdr) {
   const uint32_t node_count = hdr[2];
+  if (blockIdx.x == 0 && threadIdx.x == 0) acc_hdr[kHdrClusterValid] = 0;  // set again by the cluster build, if any
   if (hdr[8] & (RT_DEVERR_NODE_CAPACITY | RT_DEVERR_MORTON_CAPACITY)) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     const bool root_leaf = (nodes[0] & 1u) != 0;
@@ -641,6 +642,7 @@ struct BuildLayout {
   uint32_t* leaf_lambda;
   uint4* faces_tmp;
   uint32_t* counts;  // [5 x 256]: the code sort's digit counts (4 passes), then the level sort's (1 pass)
+  ClusterTemps ct;   // cluster tree build (RT_ACCEL_CLUSTERS only)
 };
 
 constexpr uint32_t kHitParts = 1184;  // 8 blocks per SM on 148 SMs
@@ -659,7 +661,7 @@ uint32_t morton_cap(uint32_t n, uint32_t D) {
   return (uint32_t)(c + 2);
 }
 
-size_t carve_build(Carve& c, BuildLayout& L, uint32_t n, uint32_t D, bool need_codes, bool need_faces_tmp) {
+size_t carve_build(Carve& c, BuildLayout& L, uint32_t n, uint32_t D, bool need_codes, bool need_faces_tmp, bool clusters) {
   L.n = n;
   L.cap_m = morton_cap(n, D);
   L.max_nodes = 2 * n - 1;
@@ -683,6 +685,8 @@ size_t carve_build(Carve& c, BuildLayout& L, uint32_t n, uint32_t D, bool need_c
   L.leaf_lambda = c.take<uint32_t>(L.max_nodes);
   L.faces_tmp = need_faces_tmp ? c.take<uint4>(n) : nullptr;
   L.counts = c.take<uint32_t>(5 * 256);
+  L.ct = ClusterTemps{};
+  if (clusters) carve_cluster_temps(c, L.ct, n, 1);
   return c.off + 256;
 }
 
@@ -724,6 +728,7 @@ static rt_build_params normalized(const rt_build_params* p) {
   if (q.min_leaf == 0) q.min_leaf = kMinLeafDefault;
   if (q.max_leaf == 0) q.max_leaf = kMaxLeafDefault;
   if (q.morton_bits == 0) q.morton_bits = 32;
+  if (q.cluster_leaf == 0) q.cluster_leaf = kClusterLeafDefault;
   return q;
 }
 
@@ -732,7 +737,7 @@ extern "C" rt_status rt_lbvh_scratch_bytes(uint32_t face_count, const rt_build_p
   rt_build_params q = normalized(params);
   Carve c(nullptr, 0);
   BuildLayout L;
-  *scratch_bytes = carve_build(c, L, face_count, q.tree_depth, true, true);
+  *scratch_bytes = carve_build(c, L, face_count, q.tree_depth, true, true, (q.accel_trees & RT_ACCEL_CLUSTERS) != 0);
   if (max_nodes) *max_nodes = 2 * face_count - 1;
   return RT_OK;
 }
@@ -758,7 +763,9 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
   const bool in_place = complete && d->faces_out && (d->faces_out == d->faces_in);
   Carve c(d->scratch, d->scratch_bytes);
   BuildLayout L;
-  carve_build(c, L, n, q.tree_depth, d->codes == nullptr, in_place);
+  const bool clusters = (q.accel_trees & RT_ACCEL_CLUSTERS) != 0;
+  if (clusters && (n > kClusterFirstMask || q.cluster_leaf > kClusterLeafMax)) return RT_ERR_UNSUPPORTED;
+  carve_build(c, L, n, q.tree_depth, d->codes == nullptr, in_place, clusters);
   if (!d->scratch || !c.ok()) return RT_ERR_SCRATCH_TOO_SMALL;
   AccelLayout AL{};
   const bool accel = complete && d->accel && d->tris;
@@ -848,6 +855,10 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
       k_accel_nodes<<<sms * 4, 256, 0, st>>>(d->nodes, L.hdr, L.leaf_lambda, AL.tnodes, AL.wide, AL.hdr);
       note_launch();
       RT_CHECK_LAUNCH();
+      if (clusters) {
+        s = build_cluster_tree((const float4*)d->tris, codes, n, q.cluster_leaf, L.ct, AL.hdr, AL.crec, st);
+        if (s != RT_OK) return s;
+      }
     }
   }
   if (in_place && cudaMemcpyAsync(d->faces_out, L.faces_tmp, (size_t)n * 16, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
@@ -939,6 +950,8 @@ struct BatchArgs {
   uint4* acc_leaves;      // [N]
   float4* groups;         // [2 (N + N/8 + M + 1)]
   float4* wide;           // [8 N]
+  float4* crec;           // cluster records (from F_m per mesh)
+  ClusterTemps ct;        // cluster tree build temporaries (RT_ACCEL_CLUSTERS only)
   rt_build_info* info_out;
 };
 
@@ -1166,13 +1179,14 @@ __global__ __launch_bounds__(256) void k_batch_records(BatchArgs B) {
   }
   for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < B.M; m += gridDim.x * blockDim.x) {
     const uint32_t* h = B.hdr + 16 * m;
+    B.acc_hdr[64 * (size_t)m + kHdrClusterValid] = 0;  // set again by the cluster build, if any
     rt_build_info* o = B.info_out + m;
     o->leaf_count = h[0]; o->node_count = h[2]; o->real_depth = h[3]; o->split_count = h[4];
     o->overrun_visits = h[5]; o->nondet_reads = h[6]; o->past_end_reads = h[7]; o->error = h[8] | *B.err;
   }
 }
 
-size_t carve_batch(Carve& c, BatchArgs& B, uint32_t M, uint32_t N) {
+size_t carve_batch(Carve& c, BatchArgs& B, uint32_t M, uint32_t N, bool clusters) {
   B.hits = c.take<float4>(2 * (size_t)M);
   B.idx = c.take<uint32_t>(N);
   B.codes_raw = c.take<uint32_t>(N);
@@ -1194,6 +1208,8 @@ size_t carve_batch(Carve& c, BatchArgs& B, uint32_t M, uint32_t N) {
   B.leaf_base = c.take<uint32_t>((size_t)M + 1);
   B.err = c.take<uint32_t>(4);
   B.counts = c.take<uint32_t>(9 * 256 + 64);
+  B.ct = ClusterTemps{};
+  if (clusters) carve_cluster_temps(c, B.ct, N, M);
   const size_t sort_bytes = radix_scratch_bytes(N);
   c.take<char>(sort_bytes);
   return c.off + 256;
@@ -1202,7 +1218,7 @@ size_t carve_batch(Carve& c, BatchArgs& B, uint32_t M, uint32_t N) {
 size_t carve_batch_accel(Carve& c, BatchArgs& B, uint32_t M, uint32_t N) {
   BatchAccel L;
   const size_t bytes = carve_batch_accel_layout(c, L, M, N);
-  B.acc_hdr = L.hdr; B.tnodes = L.tnodes; B.acc_leaves = L.leaves; B.groups = L.groups; B.wide = L.wide;
+  B.acc_hdr = L.hdr; B.tnodes = L.tnodes; B.acc_leaves = L.leaves; B.groups = L.groups; B.wide = L.wide; B.crec = L.crec;
   return bytes;
 }
 
@@ -1211,10 +1227,10 @@ size_t carve_batch_accel(Carve& c, BatchArgs& B, uint32_t M, uint32_t N) {
 
 extern "C" rt_status rt_batch_sizes(uint32_t M, uint32_t N, const rt_build_params* params, size_t* scratch_bytes, size_t* accel_bytes) {
   if (M == 0 || N < M || !scratch_bytes) return RT_ERR_INVALID_ARGUMENT;
-  (void)params;
+  const rt_build_params q = normalized(params);
   Carve c(nullptr, 0);
   BatchArgs B;
-  *scratch_bytes = carve_batch(c, B, M, N);
+  *scratch_bytes = carve_batch(c, B, M, N, (q.accel_trees & RT_ACCEL_CLUSTERS) != 0);
   if (accel_bytes) {
     Carve a(nullptr, 0);
     *accel_bytes = carve_batch_accel(a, B, M, N);
@@ -1231,9 +1247,11 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   rt_build_params q = normalized(&d->params);
   if (!q.tree_complete || (q.morton_bits != 32 && q.morton_bits != 30)) return RT_ERR_INVALID_ARGUMENT;
   const uint32_t M = d->mesh_count, N = d->face_count;
+  const bool clusters = (q.accel_trees & RT_ACCEL_CLUSTERS) != 0;
+  if (clusters && (N > kClusterFirstMask || q.cluster_leaf > kClusterLeafMax)) return RT_ERR_UNSUPPORTED;
   Carve c(d->scratch, d->scratch_bytes);
   BatchArgs B;
-  carve_batch(c, B, M, N);
+  carve_batch(c, B, M, N, clusters);
   if (!d->scratch || !c.ok()) return RT_ERR_SCRATCH_TOO_SMALL;
   // the sort scratch is the last region
   const size_t sort_bytes = radix_scratch_bytes(N);
@@ -1288,5 +1306,6 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   k_batch_records<<<sms * 4, 256, 0, st>>>(B);
   note_launch(3);
   RT_CHECK_LAUNCH();
+  if (clusters) return batch_build_cluster_tree(B.tris, B.codes, B.foff, M, N, q.cluster_leaf, B.ct, B.acc_hdr, B.crec, st);
   return RT_OK;
 }

@@ -140,15 +140,68 @@ __device__ __forceinline__ void accel_node(const uint32_t* __restrict__ nodes, c
   dst[0] = out[0]; dst[1] = out[1]; dst[2] = out[2]; dst[3] = out[3];
 }
 
+// ---------------------------------------------------------------------------
+// Cluster tree: a second traversal tree in the blob, independent of the node
+// tree, whose leaves hold at most `leaf_max` (1..8, default 4) triangles. It is
+// the binary radix tree of the mesh's sorted keys (Morton code, position)
+// built bottom-up (rt_clusters.cu), cut at subtrees of at most leaf_max
+// positions (a "cluster": a contiguous run of positions) and stored as 4-wide
+// records. Internal node p of the radix tree (0 <= p < n - 1) is the split
+// between positions p and p + 1; its record, at record index p, holds the
+// boxes of up to four children: each child of p that is a cluster, or else
+// that child's two children. The root's record is at the index in the header;
+// a mesh whose root is itself a cluster (n <= leaf_max) gets a one-slot record
+// at index n - 1. Records of mesh m sit at F_m + index (F_m = its first face).
+// A record (128 B) is eight float4: min x, min y, min z, max x, max y, max z of
+// the four slots (component k = slot k), the four slot references and a spare.
+// A reference is a record index, or kClusterLeaf | (count - 1) << 28 | first
+// for the positions first .. first + count - 1; an unused slot has kNoChild
+// and NaN bounds, which every slab comparison rejects.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kClusterLeaf = 0x80000000u;
+constexpr uint32_t kClusterFirstMask = 0x0FFFFFFFu;  // meshes of fewer than 2^28 positions
+constexpr uint32_t kClusterLeafMax = 8;
+constexpr uint32_t kClusterLeafDefault = 4;
+// Header words (per mesh, inside the blob header of 64 words) describing the cluster tree. Every build clears
+// the valid word (in the kernel that writes the node records' header words); the cluster build sets it last.
+constexpr int kHdrClusterValid = 16;  // 1 once the build wrote the cluster tree for this mesh, else 0
+constexpr int kHdrClusterN = 17;      // positions n
+constexpr int kHdrClusterRoot = 18;   // record index of the root
+__host__ __device__ __forceinline__ uint32_t cluster_leaf_ref(uint32_t first, uint32_t count) {
+  return kClusterLeaf | ((count - 1u) << 28) | first;
+}
+// Build temporaries (per position of all meshes): the arrival word of each internal node, its two child
+// references (kClusterLeaf | position for a position), the padded boxes of internal nodes and of positions.
+// The build works in chunks of kClusterChunk positions (one CTA each, never across meshes; mesh m's chunks start
+// at chunk cluster_chunk_base(F_m, m)); each chunk leaves at most two nodes for the global pass (`frontier`).
+constexpr uint32_t kClusterChunk = 512;
+__host__ __device__ __forceinline__ uint32_t cluster_chunk_base(uint32_t F, uint32_t m) { return F / kClusterChunk + m; }
+__host__ __device__ __forceinline__ uint32_t cluster_chunks(uint32_t N, uint32_t M) { return N / kClusterChunk + M + 1; }
+struct ClusterTemps {
+  uint32_t* other;
+  uint32_t* child;
+  float4* ibox;
+  float4* lbox;
+  uint4* frontier;  // [2 chunks]: (reference, first, last, 1) of a node whose parent lies outside its chunk, else zero
+};
+inline void carve_cluster_temps(Carve& c, ClusterTemps& T, size_t N, size_t M) {
+  T.other = c.take<uint32_t>(N);
+  T.child = c.take<uint32_t>(2 * N);
+  T.ibox = c.take<float4>(2 * N);
+  T.lbox = c.take<float4>(2 * N);
+  T.frontier = c.take<uint4>(2 * (N / kClusterChunk + M + 1));
+}
+
 // Traversal blob: header (256 B), internal-node records (64 B, <= N - 1),
-// leaf table (16 B, <= N), group boxes (32 B, <= N/8 + N).
-// Single-mesh blobs also hold 4-wide records (128 B, <= N - 1), see wide_node.
+// leaf table (16 B, <= N), group boxes (32 B, <= N/8 + N), 4-wide records
+// (128 B, <= N - 1, see wide_node) and the cluster tree (128 B records, <= N).
 struct AccelLayout {
   uint32_t* hdr;
   float4* tnodes;
   uint4* leaves;
   float4* groups;
   float4* wide;
+  float4* crec;
 };
 inline size_t carve_accel(Carve& c, AccelLayout& A, uint32_t n) {
   A.hdr = c.take<uint32_t>(64);
@@ -156,6 +209,7 @@ inline size_t carve_accel(Carve& c, AccelLayout& A, uint32_t n) {
   A.leaves = c.take<uint4>(n);
   A.groups = c.take<float4>(2 * ((size_t)n / 8 + n + 1));
   A.wide = c.take<float4>(8 * (size_t)n);
+  A.crec = c.take<float4>(8 * (size_t)n);
   return c.off + 256;
 }
 
@@ -380,6 +434,32 @@ __device__ __forceinline__ void wide_test(const float4* __restrict__ wn, const f
   wide_test_regs(w, oi, ix, iy, iz, tbest, skip, t, r);
 }
 
+// The four slots of a cluster record against a ray: entry distance of each slot the ray enters within reach
+// (+inf otherwise), nearest first, with the slot references alongside.
+__device__ __forceinline__ void cluster_test(const float4* __restrict__ rec, const float4& oi, float ix, float iy, float iz,
+                                             float tbest, float (&t)[4], uint32_t (&r)[4]) {
+  float4 w0, w1, w2, w3, w4, w5;
+  ldg8(rec, w0, w1);
+  ldg8(rec + 2, w2, w3);
+  ldg8(rec + 4, w4, w5);
+  const uint4 wr = ldg4((const uint4*)(rec + 6));
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const float t0x = __fmaf_rn(f4c(w0, s), ix, -oi.x), t1x = __fmaf_rn(f4c(w3, s), ix, -oi.x);
+    const float t0y = __fmaf_rn(f4c(w1, s), iy, -oi.y), t1y = __fmaf_rn(f4c(w4, s), iy, -oi.y);
+    const float t0z = __fmaf_rn(f4c(w2, s), iz, -oi.z), t1z = __fmaf_rn(f4c(w5, s), iz, -oi.z);
+    const float tn = max3f(fminf(t0x, t1x), fminf(t0y, t1y), fminf(t0z, t1z));
+    const float tf = min3f(fmaxf(t0x, t1x), fmaxf(t0y, t1y), fmaxf(t0z, t1z));
+    t[s] = (tn <= tf && tf >= 0.0f && tn <= tbest * kCullSlack) ? tn : INFINITY;
+    r[s] = u4c(wr, s);
+  }
+  cswap_tr(t, r, 0, 1);
+  cswap_tr(t, r, 2, 3);
+  cswap_tr(t, r, 0, 2);
+  cswap_tr(t, r, 1, 3);
+  cswap_tr(t, r, 1, 2);
+}
+
 // ---------------------------------------------------------------------------
 // batched meshes
 // ---------------------------------------------------------------------------
@@ -410,6 +490,7 @@ struct BatchAccel {
   uint4* leaves;
   float4* groups;
   float4* wide;
+  float4* crec;  // cluster records, 8 float4 each; mesh m's from record F_m
 };
 inline size_t carve_batch_accel_layout(Carve& c, BatchAccel& L, uint32_t M, uint32_t N) {
   L.hdr = c.take<uint32_t>(64 * (size_t)M);
@@ -417,7 +498,16 @@ inline size_t carve_batch_accel_layout(Carve& c, BatchAccel& L, uint32_t M, uint
   L.leaves = c.take<uint4>(N);
   L.groups = c.take<float4>(2 * ((size_t)N + N / 8 + M + 1));
   L.wide = c.take<float4>(8 * (size_t)N);
+  L.crec = c.take<float4>(8 * (size_t)N);
   return c.off + 256;
 }
+
+// Cluster tree builds (rt_clusters.cu), from the sorted Morton codes and the pre-gathered triangles of the
+// position order: a single mesh (header hdr, records crec) and all meshes of a batched build (headers 64 words
+// apart, records of mesh m from F_m). Two launches each (the chunk pass and the global pass).
+rt_status build_cluster_tree(const float4* tris, const uint32_t* codes, uint32_t n, uint32_t leaf_max, const ClusterTemps& T,
+                             uint32_t* hdr, float4* crec, cudaStream_t st);
+rt_status batch_build_cluster_tree(const float4* tris, const uint32_t* codes, const uint32_t* foff, uint32_t M, uint32_t N,
+                                   uint32_t leaf_max, const ClusterTemps& T, uint32_t* hdr, float4* crec, cudaStream_t st);
 
 }  // namespace rt

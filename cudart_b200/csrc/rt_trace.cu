@@ -412,6 +412,85 @@ __device__ __forceinline__ void trace_ray_accel(const uint32_t r, const TraceArg
 // are written by the lane whose key is the minimum right after its merge.
 constexpr int kCoopWarps = 4;  // 128-thread CTAs
 
+// The triangle tests of one warp-cooperative step. Each lane holds `mask`:
+// bit g set = group g of its leaf is to be tested, i.e. positions
+// first + kGroup g .. min(cnt, kGroup (g + 1)) - 1 + first of its mesh (whose
+// positions start at F in the triangle stream). The (ray, group) items of the
+// whole warp are spread over the 32 lanes: a lane tests one group against the
+// ray of the item's owner (fetched by shuffles) and merges its best hit into
+// the owner's slot with a 64-bit shared-memory atomicMin on (t bits, position),
+// the same (t, position) rule as the other schedules. The (u, v) of the
+// current best are written by the lane whose key is the minimum right after
+// its merge. key0 is this lane's best so far (t bits, position); on return
+// s_key[lane] / s_uv[lane] hold the merged best of this lane's ray.
+template <uint32_t kGroup>
+__device__ __forceinline__ void coop_items(const uint32_t lane, const uint32_t mask, const uint32_t first, const uint32_t cnt,
+                                           const uint32_t F, const float4& o, const float4& d, const float zu, const float zv,
+                                           const float4* __restrict__ tris, const unsigned long long key0, const float bu,
+                                           const float bv, unsigned long long* s_key, float2* s_uv) {
+  const uint32_t my_items = __popc(mask);
+  uint32_t incl = my_items;
+#pragma unroll
+  for (int k = 1; k < 32; k <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, k);
+    if (lane >= (uint32_t)k) incl += y;
+  }
+  const uint32_t excl = incl - my_items;
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+  s_key[lane] = key0;
+  s_uv[lane] = make_float2(bu, bv);
+  __syncwarp();
+  for (uint32_t base = 0; base < total; base += 32) {
+    const uint32_t item = base + lane;
+    unsigned long long cand = ~0ull;
+    float cu = 0.f, cv = 0.f;
+    // owner: last lane whose exclusive offset is <= item
+    uint32_t lo = 0, hi = 31;
+#pragma unroll
+    for (int it = 0; it < 5; ++it) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      const uint32_t off_mid = __shfl_sync(0xffffffffu, excl, mid);
+      if (off_mid <= item) lo = mid; else hi = mid - 1;
+    }
+    const uint32_t owner = lo;
+    const float4 oo = make_float4(__shfl_sync(0xffffffffu, o.x, owner), __shfl_sync(0xffffffffu, o.y, owner),
+                                  __shfl_sync(0xffffffffu, o.z, owner), 0.0f);
+    const float4 od = make_float4(__shfl_sync(0xffffffffu, d.x, owner), __shfl_sync(0xffffffffu, d.y, owner),
+                                  __shfl_sync(0xffffffffu, d.z, owner), 0.0f);
+    const float ozu = __shfl_sync(0xffffffffu, zu, owner), ozv = __shfl_sync(0xffffffffu, zv, owner);
+    const uint32_t omask = __shfl_sync(0xffffffffu, mask, owner);
+    const uint32_t oexcl = __shfl_sync(0xffffffffu, excl, owner);
+    const uint32_t ofirst = __shfl_sync(0xffffffffu, first, owner);
+    const uint32_t ocnt = __shfl_sync(0xffffffffu, cnt, owner);
+    // the owner's triangle stream (lanes of a batched launch may trace different meshes)
+    const float4* otris = tris + 3 * (size_t)__shfl_sync(0xffffffffu, F, owner);
+    if (item < total) {
+      const uint32_t g = __fns(omask, 0, (int)(item - oexcl) + 1);
+      const uint32_t kend = min(ocnt, g * kGroup + kGroup);
+      const unsigned long long cur = s_key[owner];
+      unsigned long long mine = ~0ull;
+      float mu = 0.f, mv = 0.f;
+      for (uint32_t k = g * kGroup; k < kend; ++k) {
+        const uint32_t pos = ofirst + k;
+        const float4 v0 = ldg4(otris + 3 * (size_t)pos);
+        const float4 e1 = ldg4(otris + 3 * (size_t)pos + 1);
+        const float4 e2 = ldg4(otris + 3 * (size_t)pos + 2);
+        float t, u, v;
+        if (!mt_test(oo, od, ozu, ozv, v0, e1, e2, t, u, v)) continue;
+        const unsigned long long key = ((unsigned long long)__float_as_uint(t) << 32) | pos;
+        if (key < mine) { mine = key; mu = u; mv = v; }
+      }
+      if (mine < cur) atomicMin(s_key + owner, mine);
+      cand = mine;
+      cu = mu; cv = mv;
+    }
+    __syncwarp();
+    // (u, v) of the owner's minimum, written by the one lane holding that key
+    if (item < total && cand != ~0ull && s_key[owner] == cand) s_uv[owner] = make_float2(cu, cv);
+    __syncwarp();
+  }
+}
+
 template <bool kCount, bool kSeed = false, bool kWide = false>
 __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool valid, const TraceArgs& A, const AccelArgs& C,
                                                 unsigned long long* s_key, float2* s_uv, const SeedArgs& S = SeedArgs{}) {
@@ -546,70 +625,10 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
       // past 32 to this lane: they are tested below by the owner alone
     }
     // 3. spread the warp's (ray, group) items over the lanes
-    const uint32_t my_items = __popc(mask);
-    uint32_t incl = my_items;
-#pragma unroll
-    for (int k = 1; k < 32; k <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, k);
-      if (lane >= (uint32_t)k) incl += y;
-    }
-    const uint32_t excl = incl - my_items;
-    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
     // (t bits, position) of the best hit so far; with no hit yet, (tmax bits, 0),
     // which no accepted hit equals (t < tmax is required)
     const unsigned long long key0 = ((unsigned long long)__float_as_uint(bt) << 32) | (uint32_t)(best >= 0 ? best : 0);
-    s_key[lane] = key0;
-    s_uv[lane] = make_float2(bu, bv);
-    __syncwarp();
-    for (uint32_t base = 0; base < total; base += 32) {
-      const uint32_t item = base + lane;
-      unsigned long long cand = ~0ull;
-      float cu = 0.f, cv = 0.f;
-      // owner: last lane whose exclusive offset is <= item
-      uint32_t lo = 0, hi = 31;
-#pragma unroll
-      for (int it = 0; it < 5; ++it) {
-        const uint32_t mid = (lo + hi + 1) >> 1;
-        const uint32_t off_mid = __shfl_sync(0xffffffffu, excl, mid);
-        if (off_mid <= item) lo = mid; else hi = mid - 1;
-      }
-      const uint32_t owner = lo;
-      const float4 oo = make_float4(__shfl_sync(0xffffffffu, o.x, owner), __shfl_sync(0xffffffffu, o.y, owner),
-                                    __shfl_sync(0xffffffffu, o.z, owner), 0.0f);
-      const float4 od = make_float4(__shfl_sync(0xffffffffu, d.x, owner), __shfl_sync(0xffffffffu, d.y, owner),
-                                    __shfl_sync(0xffffffffu, d.z, owner), 0.0f);
-      const float ozu = __shfl_sync(0xffffffffu, zu, owner), ozv = __shfl_sync(0xffffffffu, zv, owner);
-      const uint32_t omask = __shfl_sync(0xffffffffu, mask, owner);
-      const uint32_t oexcl = __shfl_sync(0xffffffffu, excl, owner);
-      const uint32_t ofirst = __shfl_sync(0xffffffffu, first, owner);
-      const uint32_t ocnt = __shfl_sync(0xffffffffu, cnt, owner);
-      // the owner's triangle stream (lanes of a batched launch may trace different meshes)
-      const float4* otris = A.tris + 3 * (size_t)__shfl_sync(0xffffffffu, C.F, owner);
-      if (item < total) {
-        const uint32_t g = __fns(omask, 0, (int)(item - oexcl) + 1);
-        const uint32_t kend = min(ocnt, g * 8 + 8);
-        const unsigned long long cur = s_key[owner];
-        unsigned long long mine = ~0ull;
-        float mu = 0.f, mv = 0.f;
-        for (uint32_t k = g * 8; k < kend; ++k) {
-          const uint32_t pos = ofirst + k;
-          const float4 v0 = ldg4(otris + 3 * (size_t)pos);
-          const float4 e1 = ldg4(otris + 3 * (size_t)pos + 1);
-          const float4 e2 = ldg4(otris + 3 * (size_t)pos + 2);
-          float t, u, v;
-          if (!mt_test(oo, od, ozu, ozv, v0, e1, e2, t, u, v)) continue;
-          const unsigned long long key = ((unsigned long long)__float_as_uint(t) << 32) | pos;
-          if (key < mine) { mine = key; mu = u; mv = v; }
-        }
-        if (mine < cur) atomicMin(s_key + owner, mine);
-        cand = mine;
-        cu = mu; cv = mv;
-      }
-      __syncwarp();
-      // (u, v) of the owner's minimum, written by the one lane holding that key
-      if (item < total && cand != ~0ull && s_key[owner] == cand) s_uv[owner] = make_float2(cu, cv);
-      __syncwarp();
-    }
+    coop_items<8>(lane, mask, first, cnt, C.F, o, d, zu, zv, A.tris, key0, bu, bv, s_key, s_uv);
     // 4. read back the merged best and move on
     if (has_leaf) {
       const unsigned long long k = s_key[lane];
@@ -657,6 +676,218 @@ __device__ __forceinline__ void trace_warp_coop(const uint32_t r, const bool val
     A.hit_t[r] = tmax0;
     A.hit_uv[r] = make_float2(0.0f, 0.0f);
   }
+  if (kCount) {
+    if (A.visits) A.visits[r] = visits;
+    if (A.tests) A.tests[r] = tests;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cluster tree walks (RT_TRACE_CLUSTERS; layout in rt_device.cuh)
+// ---------------------------------------------------------------------------
+struct ClusterArgs {
+  const float4* crec;   // cluster records (a batched launch: the batch's, from its base)
+  const uint32_t* hdr;  // header words of the ray's mesh
+  uint32_t F = 0;       // the mesh's first position (and first record)
+  uint32_t n = 0;       // the mesh's face count, as the caller gives it
+};
+
+__device__ __forceinline__ void write_hit(const uint32_t r, const TraceArgs& A, const uint32_t F, const int32_t best, const float bt,
+                                          const float bu, const float bv, const float tmax0) {
+  if (best >= 0) {
+    A.hit_id[r] = A.id_mode == 1 ? (int32_t)__ldg(A.indices + F + best) : best;
+    A.hit_t[r] = bt;
+    A.hit_uv[r] = make_float2(bu, bv);
+  } else {
+    A.hit_id[r] = -1;
+    A.hit_t[r] = tmax0;
+    A.hit_uv[r] = make_float2(0.0f, 0.0f);
+  }
+}
+
+// The header of the ray's mesh describes a cluster tree built for the mesh's face count; root = its record.
+__device__ __forceinline__ bool cluster_tree_ok(const ClusterArgs& C, uint32_t& root) {
+  root = __ldg(C.hdr + kHdrClusterRoot);
+  return __ldg(C.hdr + kHdrClusterValid) == 1u && __ldg(C.hdr + kHdrClusterN) == C.n && C.n > 0 && root < C.n;
+}
+// A reference inside the mesh: a record index below n, or a cluster whose positions are below n. Anything else
+// (a blob written for other sizes) ends the walk with RT_DEVERR_ACCEL_MISSING instead of reading past the mesh.
+__device__ __forceinline__ bool cluster_ref_ok(uint32_t ref, uint32_t n) {
+  return (ref & kClusterLeaf) ? (ref & kClusterFirstMask) + ((ref >> 28) & 7u) < n : ref < n;
+}
+
+// Pops the nearest stacked reference that can still hold a closer hit.
+__device__ __forceinline__ bool pop_within(const uint32_t (&st_ref)[kStack], const float (&st_t)[kStack], int& sp, float bt,
+                                           uint32_t& ref) {
+  while (sp > 0) {
+    --sp;
+    if (st_t[sp] <= bt * kCullSlack) {
+      ref = st_ref[sp];
+      return true;
+    }
+  }
+  return false;
+}
+
+// One ray, one lane: nearest-first descent through the 4-wide records; a
+// cluster is tested when the walk reaches it (entered nearest first, skipped
+// once it can no longer hold a closer hit).
+template <bool kCount>
+__device__ __forceinline__ void trace_ray_clusters(const uint32_t r, const TraceArgs& A, const ClusterArgs& C) {
+  const float tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
+  int32_t best = -1;
+  float bt = tmax0, bu = 0.0f, bv = 0.0f;
+  uint32_t visits = 0, tests = 0;
+  uint32_t ref = 0;
+  if (tmax0 > 0.0f && !cluster_tree_ok(C, ref)) {
+    if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+  } else if (tmax0 > 0.0f) {
+    const float4 o = ldg4(A.orig + r), d = ldg4(A.dir + r);
+    const float ix = 1.0f / fix_dir(d.x), iy = 1.0f / fix_dir(d.y), iz = 1.0f / fix_dir(d.z);
+    const float4 oi = scaled_origin(o, ix, iy, iz);
+    const float zu = o.w * 0.0f, zv = d.w * 0.0f;
+    const float4* tris = A.tris + 3 * (size_t)C.F;
+    const float4* recs = C.crec + 8 * (size_t)C.F;
+    uint32_t st_ref[kStack];
+    float st_t[kStack];
+    int sp = 0;
+    for (;;) {
+      if (!cluster_ref_ok(ref, C.n)) {
+        if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+        break;
+      }
+      if (!(ref & kClusterLeaf)) {
+        float t[4];
+        uint32_t k[4];
+        cluster_test(recs + 8 * (size_t)ref, oi, ix, iy, iz, bt, t, k);
+        if (kCount) visits += 4;
+        if (t[0] != INFINITY) {
+#pragma unroll
+          for (int j = 3; j >= 1; --j) {
+            if (t[j] != INFINITY) {
+              if (sp < kStack) {
+                st_ref[sp] = k[j];
+                st_t[sp] = t[j];
+                ++sp;
+              } else if (A.err) {
+                atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
+              }
+            }
+          }
+          ref = k[0];
+          continue;
+        }
+      } else {
+        const uint32_t p0 = ref & kClusterFirstMask, p1 = p0 + ((ref >> 28) & 7u) + 1u;
+        for (uint32_t pos = p0; pos < p1; ++pos) {
+          const float4 v0 = ldg4(tris + 3 * (size_t)pos);
+          const float4 e1 = ldg4(tris + 3 * (size_t)pos + 1);
+          const float4 e2 = ldg4(tris + 3 * (size_t)pos + 2);
+          if (kCount) ++tests;
+          float th, u, v;
+          if (!mt_test(o, d, zu, zv, v0, e1, e2, th, u, v)) continue;
+          if (th < bt || (best >= 0 && th == bt && (int32_t)pos < best)) {
+            best = (int32_t)pos; bt = th; bu = u; bv = v;
+          }
+        }
+      }
+      if (!pop_within(st_ref, st_t, sp, bt, ref)) break;
+    }
+  }
+  write_hit(r, A, C.F, best, bt, bu, bv, tmax0);
+  if (kCount) {
+    if (A.visits) A.visits[r] = visits;
+    if (A.tests) A.tests[r] = tests;
+  }
+}
+
+// Warp-cooperative cluster walk: each lane descends its own ray until it holds
+// a cluster; then the clusters of all lanes (one item of up to 8 triangles per
+// lane) are tested by the whole warp (coop_items), and every lane moves on.
+template <bool kCount>
+__device__ __forceinline__ void trace_warp_coop_clusters(const uint32_t r, const bool valid, const TraceArgs& A, const ClusterArgs& C,
+                                                         unsigned long long* s_key, float2* s_uv) {
+  const uint32_t lane = lane_id();
+  float4 o = make_float4(0.f, 0.f, 0.f, 0.f), d = make_float4(0.f, 0.f, 1.f, 0.f);
+  float tmax0 = -1.0f;
+  uint32_t ref = 0;
+  bool ok = false;
+  if (valid) {
+    tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
+    if (tmax0 > 0.0f) {  // an inactive ray (tmax <= 0) reads nothing more
+      ok = cluster_tree_ok(C, ref);
+      if (!ok && A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+      o = ldg4(A.orig + r);
+      d = ldg4(A.dir + r);
+    }
+  }
+  int32_t best = -1;
+  float bt = tmax0, bu = 0.0f, bv = 0.0f;
+  uint32_t visits = 0, tests = 0;
+  const float ix = 1.0f / fix_dir(d.x), iy = 1.0f / fix_dir(d.y), iz = 1.0f / fix_dir(d.z);
+  const float4 oi = scaled_origin(o, ix, iy, iz);
+  const float zu = o.w * 0.0f, zv = d.w * 0.0f;
+  const float4* recs = C.crec + 8 * (size_t)C.F;
+  uint32_t st_ref[kStack];
+  float st_t[kStack];
+  int sp = 0;
+  bool alive = ok;
+  while (__any_sync(0xffffffffu, alive)) {
+    // 1. descend until this ray holds a cluster
+    uint32_t mask = 0, first = 0, cnt = 0;
+    while (alive) {
+      if (!cluster_ref_ok(ref, C.n)) {
+        if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+        alive = false;
+        break;
+      }
+      if (ref & kClusterLeaf) {
+        mask = 1u;
+        first = ref & kClusterFirstMask;
+        cnt = ((ref >> 28) & 7u) + 1u;
+        break;
+      }
+      float t[4];
+      uint32_t k[4];
+      cluster_test(recs + 8 * (size_t)ref, oi, ix, iy, iz, bt, t, k);
+      if (kCount) visits += 4;
+      if (t[0] != INFINITY) {
+#pragma unroll
+        for (int j = 3; j >= 1; --j) {
+          if (t[j] != INFINITY) {
+            if (sp < kStack) {
+              st_ref[sp] = k[j];
+              st_t[sp] = t[j];
+              ++sp;
+            } else if (A.err) {
+              atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
+            }
+          }
+        }
+        ref = k[0];
+        continue;
+      }
+      if (!pop_within(st_ref, st_t, sp, bt, ref)) alive = false;
+    }
+    if (kCount) tests += cnt;
+    // 2. the warp's clusters, spread over the lanes
+    const unsigned long long key0 = ((unsigned long long)__float_as_uint(bt) << 32) | (uint32_t)(best >= 0 ? best : 0);
+    coop_items<kClusterLeafMax>(lane, mask, first, cnt, C.F, o, d, zu, zv, A.tris, key0, bu, bv, s_key, s_uv);
+    // 3. read back the merged best and move on
+    if (mask) {
+      const unsigned long long key = s_key[lane];
+      if (key < key0) {
+        bt = __uint_as_float((uint32_t)(key >> 32));
+        best = (int32_t)(key & 0xFFFFFFFFu);
+        const float2 uv = s_uv[lane];
+        bu = uv.x; bv = uv.y;
+      }
+      if (!pop_within(st_ref, st_t, sp, bt, ref)) alive = false;
+    }
+    __syncwarp();
+  }
+  if (!valid) return;
+  write_hit(r, A, C.F, best, bt, bu, bv, tmax0);
   if (kCount) {
     if (A.visits) A.visits[r] = visits;
     if (A.tests) A.tests[r] = tests;
@@ -836,6 +1067,102 @@ __global__ __launch_bounds__(128) void k_batch_trace_persistent(TraceArgs A, Bat
     if (base >= A.ray_count) break;
     const uint32_t slot = base + lane;
     if (slot < A.ray_count) batch_trace_ray<kCount, kWW, kSeed, kWide>(B.ray_of(slot), A, B, S);
+  }
+}
+
+// Cluster tree kernels: single mesh (slots through a SlotMap) and batched (each ray's mesh by binary search).
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_trace_clusters(TraceArgs A, ClusterArgs C, SlotMap M) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t r;
+  C.F = 0;
+  if (s < M.slots && M.ray_of(s, r)) trace_ray_clusters<kCount>(r, A, C);
+}
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_trace_clusters_persistent(TraceArgs A, ClusterArgs C, SlotMap M, uint32_t* counter) {
+  const uint32_t lane = lane_id();
+  C.F = 0;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= M.slots) break;
+    uint32_t r;
+    const uint32_t s = base + lane;
+    if (s < M.slots && M.ray_of(s, r)) trace_ray_clusters<kCount>(r, A, C);
+  }
+}
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_trace_clusters_coop(TraceArgs A, ClusterArgs C, SlotMap M, uint32_t* counter) {
+  __shared__ unsigned long long s_key[kCoopWarps][32];
+  __shared__ float2 s_uv[kCoopWarps][32];
+  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  C.F = 0;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= M.slots) break;
+    uint32_t r = 0;
+    const uint32_t s = base + lane;
+    const bool valid = s < M.slots && M.ray_of(s, r);
+    trace_warp_coop_clusters<kCount>(r, valid, A, C, s_key[w], s_uv[w]);
+  }
+}
+
+__device__ __forceinline__ void batch_cluster_args(uint32_t r, const BatchTraceArgs& B, ClusterArgs& C) {
+  const uint32_t m = find_seg(B.roff, B.M, r);
+  const uint32_t F = __ldg(B.foff + m);
+  C.hdr = B.acc.hdr + 64 * (size_t)m;
+  C.F = F;
+  C.n = __ldg(B.foff + m + 1) - F;
+}
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_batch_trace_clusters(TraceArgs A, BatchTraceArgs B) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= A.ray_count) return;
+  const uint32_t r = B.ray_of(s);
+  ClusterArgs C;
+  C.crec = B.acc.crec;
+  batch_cluster_args(r, B, C);
+  trace_ray_clusters<kCount>(r, A, C);
+}
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_batch_trace_clusters_persistent(TraceArgs A, BatchTraceArgs B, uint32_t* counter) {
+  const uint32_t lane = lane_id();
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= A.ray_count) break;
+    const uint32_t slot = base + lane;
+    if (slot < A.ray_count) {
+      const uint32_t r = B.ray_of(slot);
+      ClusterArgs C;
+      C.crec = B.acc.crec;
+      batch_cluster_args(r, B, C);
+      trace_ray_clusters<kCount>(r, A, C);
+    }
+  }
+}
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_batch_trace_clusters_coop(TraceArgs A, BatchTraceArgs B, uint32_t* counter) {
+  __shared__ unsigned long long s_key[kCoopWarps][32];
+  __shared__ float2 s_uv[kCoopWarps][32];
+  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= A.ray_count) break;
+    const uint32_t slot = base + lane;
+    const bool valid = slot < A.ray_count;
+    const uint32_t r = valid ? B.ray_of(slot) : slot;
+    ClusterArgs C;  // idle lanes: mesh 0's header, no walk
+    C.crec = B.acc.crec;
+    C.hdr = B.acc.hdr;
+    if (valid) batch_cluster_args(r, B, C);
+    trace_warp_coop_clusters<kCount>(r, valid, A, C, s_key[w], s_uv[w]);
   }
 }
 
@@ -1055,6 +1382,59 @@ extern "C" rt_status rt_device_check(void) {
 
 namespace {
 
+// Thread slots of a single-mesh launch: a given ray order, 8x4 pixel tiles of an image, or the rays in order.
+SlotMap slot_map(const rt_trace_desc* d) {
+  SlotMap M;
+  M.order = d->ray_order;
+  const uint32_t R = d->ray_count;
+  if (d->ray_order) {
+    M.width = 0; M.height = 0; M.tiles_x = 0; M.slots = R;
+  } else if (d->image_width && R % d->image_width == 0) {
+    M.width = d->image_width;
+    M.height = R / d->image_width;
+    M.tiles_x = (M.width + 7) / 8;
+    M.slots = M.tiles_x * ((M.height + 3) / 4) * 32;
+  } else {
+    M.width = 0; M.height = 0; M.tiles_x = 0; M.slots = R;
+  }
+  return M;
+}
+
+// Cluster tree launch (RT_TRACE_CLUSTERS): per-lane walks (a grid, or persistent warps with a work counter) or
+// the warp-cooperative walk (RT_TRACE_COOP, persistent warps; without a work counter the per-lane grid).
+rt_status launch_clusters(const rt_trace_desc* d, const TraceArgs& A, cudaStream_t st) {
+  const bool count = d->ray_visits || d->ray_tests;
+  ClusterArgs C;
+  {
+    Carve c((void*)d->accel, ~(size_t)0);
+    AccelLayout AL;
+    carve_accel(c, AL, d->face_count_hint);
+    C.crec = AL.crec;
+    C.hdr = AL.hdr;
+  }
+  C.n = d->face_count_hint;
+  const SlotMap M = slot_map(d);
+  if (d->work_counter) {
+    if (cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
+    const uint32_t blocks = (uint32_t)hmin<uint64_t>((uint64_t)sms() * (d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u),
+                                                     ((uint64_t)M.slots + 127) / 128);
+    if (d->schedule & RT_TRACE_COOP) {
+      if (count) k_trace_clusters_coop<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
+      else k_trace_clusters_coop<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
+    } else {
+      if (count) k_trace_clusters_persistent<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
+      else k_trace_clusters_persistent<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
+    }
+  } else {
+    const uint32_t blocks = (M.slots + 127) / 128;
+    if (count) k_trace_clusters<true><<<blocks, 128, 0, st>>>(A, C, M);
+    else k_trace_clusters<false><<<blocks, 128, 0, st>>>(A, C, M);
+  }
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
 // Blob traversal launch for every schedule of rt_trace_desc.
 template <bool kSeed, bool kWide>
 rt_status launch_accel_w(const rt_trace_desc* d, const TraceArgs& A, const SeedArgs& S, cudaStream_t st) {
@@ -1071,19 +1451,7 @@ rt_status launch_accel_w(const rt_trace_desc* d, const TraceArgs& A, const SeedA
   // the top treelet is staged by the persistent kernels of the 4-wide walk only (one copy per CTA)
   C.stage_depth = (kWide && d->work_counter) ? (d->treelet_depth < kMaxStageDepth ? d->treelet_depth : kMaxStageDepth) : 0u;
   const size_t stage_smem = (size_t)staged_slots(C.stage_depth) * 128;
-  SlotMap M;
-  M.order = d->ray_order;
-  const uint32_t R = d->ray_count;
-  if (d->ray_order) {
-    M.width = 0; M.height = 0; M.tiles_x = 0; M.slots = R;
-  } else if (d->image_width && R % d->image_width == 0) {
-    M.width = d->image_width;
-    M.height = R / d->image_width;
-    M.tiles_x = (M.width + 7) / 8;
-    M.slots = M.tiles_x * ((M.height + 3) / 4) * 32;
-  } else {
-    M.width = 0; M.height = 0; M.tiles_x = 0; M.slots = R;
-  }
+  const SlotMap M = slot_map(d);
   const bool ww = (d->schedule & RT_TRACE_WHILE_WHILE) != 0;
   const uint32_t pblocks = (uint32_t)sms() * (d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u);
   const uint32_t sblocks = (M.slots + 127) / 128;
@@ -1115,6 +1483,7 @@ rt_status launch_accel_w(const rt_trace_desc* d, const TraceArgs& A, const SeedA
 
 template <bool kSeed>
 rt_status launch_accel(const rt_trace_desc* d, const TraceArgs& A, const SeedArgs& S, cudaStream_t st) {
+  if (d->schedule & RT_TRACE_CLUSTERS) return kSeed ? RT_ERR_UNSUPPORTED : launch_clusters(d, A, st);
   if (d->schedule & RT_TRACE_WIDE) return launch_accel_w<kSeed, true>(d, A, S, st);
   return launch_accel_w<kSeed, false>(d, A, S, st);
 }
@@ -1334,6 +1703,28 @@ rt_status batch_launch_w(const rt_batch_trace_desc* d, const TraceArgs& A, const
   return RT_OK;
 }
 
+rt_status batch_launch_clusters(const rt_batch_trace_desc* d, const TraceArgs& A, const BatchTraceArgs& B, cudaStream_t st, bool count) {
+  if (d->work_counter) {
+    if (cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
+    const uint32_t per_sm = d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u;
+    const uint32_t blocks = (uint32_t)hmin<uint64_t>((uint64_t)sms() * per_sm, ((uint64_t)d->ray_count + 127) / 128);
+    if (d->schedule & RT_TRACE_COOP) {
+      if (count) k_batch_trace_clusters_coop<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
+      else k_batch_trace_clusters_coop<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
+    } else {
+      if (count) k_batch_trace_clusters_persistent<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
+      else k_batch_trace_clusters_persistent<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
+    }
+  } else {
+    const uint32_t blocks = (d->ray_count + 127) / 128;
+    if (count) k_batch_trace_clusters<true><<<blocks, 128, 0, st>>>(A, B);
+    else k_batch_trace_clusters<false><<<blocks, 128, 0, st>>>(A, B);
+  }
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
 template <bool kSeed>
 rt_status batch_launch(const rt_batch_trace_desc* d, const SeedArgs& S, cudaStream_t st) {
   TraceArgs A = {};
@@ -1346,6 +1737,7 @@ rt_status batch_launch(const rt_batch_trace_desc* d, const SeedArgs& S, cudaStre
   carve_batch_accel_layout(c, B.acc, d->mesh_count, d->face_count);
   const bool count = d->ray_visits || d->ray_tests;
   const bool ww = (d->schedule & RT_TRACE_WHILE_WHILE) != 0;
+  if (d->schedule & RT_TRACE_CLUSTERS) return kSeed ? RT_ERR_UNSUPPORTED : batch_launch_clusters(d, A, B, st, count);
   if (d->schedule & RT_TRACE_WIDE) return batch_launch_w<kSeed, true>(d, A, B, S, st, count, ww);
   return batch_launch_w<kSeed, false>(d, A, B, S, st, count, ww);
 }

@@ -31,7 +31,8 @@ HOP = 7919  # a prime: consecutive samples of a batch lie far apart in the list 
 
 class InstancedFrames:
     def __init__(self, count: int, scale: float, width: int, height: int, device="cuda", seed: int = 7, depth: int = proposal.DEPTH,
-                 batch: int = 1024, steps: int = 200, lr: float = 1e-3, sigma: float = 0.002, net_seed: int = 0):
+                 batch: int = 1024, steps: int = 200, lr: float = 1e-3, sigma: float = 0.002, net_seed: int = 0,
+                 clusters: bool = True):
         if (width * height) % 128:
             raise ValueError("width * height must be a multiple of 128 (one grouped GEMM tile of rays)")
         self.count, self.width, self.height = count, width, height
@@ -67,6 +68,7 @@ class InstancedFrames:
         # batched traversal schedules of the primary and bounce launches (tune() picks them); results never depend on them
         self.schedule_primary = self.schedule_bounce = None
         self.prev = None  # (bounce orig, bounce dir, primary labels, bounce labels) of the previous frame
+        self.clusters = clusters  # every build also makes the cluster trees (the tuner then tries their walks)
 
     @property
     def schedule(self):
@@ -99,7 +101,7 @@ class InstancedFrames:
     def build(self, verts=None):
         """One batched LBVH build of all instances, from `verts` (default: the displaced frame)."""
         v = self.verts if verts is None else verts
-        self.tree = core.batch_build(v, self.faces, self.face_offsets, self.vertex_offsets, out=self.tree)
+        self.tree = core.batch_build(v, self.faces, self.face_offsets, self.vertex_offsets, out=self.tree, clusters=self.clusters)
         return self.tree
 
     def make_slots(self):
@@ -128,7 +130,21 @@ class InstancedFrames:
         b = self.bounce(h1)
         self.schedule_bounce, t2 = tune.tune_batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], use_cache=False,
                                                          order=b[3])
+        # the seeded walks go through the node records: the fastest schedule of those for each launch
+        self.seeded_primary = min((x for x in t1 if not x[0].get("clusters")), key=lambda x: x[1])[0]
+        self.seeded_bounce = min((x for x in t2 if not x[0].get("clusters")), key=lambda x: x[1])[0]
         return (self.schedule_primary, self.schedule_bounce), (t1, t2)
+
+    def seeded_schedules(self):
+        """Schedules of the seeded (learned) launches: tune()'s fastest node-record schedules, else the plain ones
+        (which then must not walk the cluster tree: seeded walks start inside the node tree)."""
+        sp = getattr(self, "seeded_primary", None) or self.schedule_primary
+        sb = getattr(self, "seeded_bounce", None) or self.schedule_bounce
+        return sp, sb
+
+    def seeded_order(self, b):
+        """The bounce tracing order of the seeded launch (see bounce_order)."""
+        return b[3] if (self.seeded_schedules()[1] or {}).get("given_order") else None
 
     def trace_plain(self, out=None):
         """Primary hits, bounce rays and bounce hits through rt_batch_trace."""
@@ -144,12 +160,13 @@ class InstancedFrames:
         out = out or {}
         R = self.rays_per_instance
         p1 = self.nets.propose(self.orig, self.dir, self.box, R, out=out.get("p1"))
+        sp, sb = self.seeded_schedules()
         h1 = proposal.batch_trace_seeded(self.tree, self.orig, self.dir, self.ray_offsets, p1, self.slots, in_proposal=in_proposal,
-                                         out=out.get("h1"), schedule=self.schedule_primary)
+                                         out=out.get("h1"), schedule=sp)
         b = self.bounce(h1, out=out.get("b"))
         p2 = self.nets.propose(b[0], b[1], self.box, R, out=out.get("p2"), tmax=b[2])  # bounces of misses are inactive
         h2 = proposal.batch_trace_seeded(self.tree, b[0], b[1], self.ray_offsets, p2, self.slots, tmax=b[2], in_proposal=in_proposal,
-                                         out=out.get("h2"), schedule=self.schedule_bounce, order=self.bounce_order(b))
+                                         out=out.get("h2"), schedule=sb, order=self.seeded_order(b))
         return dict(p1=p1, h1=h1, b=b, p2=p2, h2=h2)
 
     def labels(self, plain):

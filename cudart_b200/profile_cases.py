@@ -175,10 +175,13 @@ def sort_16m():
 
 
 def c4_frame(count: int = 64):
-    """Three frames of the instanced workload's plain path with the schedule the tuner picks on it."""
+    """Three frames of the instanced workload's plain path (cluster trees) with the schedules the tuner picks on
+    it: per-lane cluster walks, 8 x 4 pixel tiles for the primaries, the bounces ordered by mesh, octant and
+    12 Morton bits."""
     from .instances import InstancedFrames
     w = InstancedFrames(count, 1 / 16, 960, 540)
-    w.schedule = dict(while_while=True, wide=True, persistent=True, blocks_per_sm=8, coop=True)
+    w.schedule_primary = dict(clusters=True, persistent=True, blocks_per_sm=8, tiles=[count, 960, 540])
+    w.schedule_bounce = dict(clusters=True, persistent=True, blocks_per_sm=16, sorted_bits=12)
     plain = None
     for f in range(3):
         w.displace(f)

@@ -49,6 +49,19 @@ def candidates(image_width: int):
     return out
 
 
+def cluster_candidates(image_width: int):
+    """Single-mesh schedules that walk the cluster tree (a build with clusters=True)."""
+    widths = [0, image_width] if image_width else [0]
+    out = []
+    for w in widths:
+        out.append({"clusters": True, "image_width": w, "persistent": False, "blocks_per_sm": 0})
+        for coop, bps in ((False, 8), (False, 16), (True, 8), (True, 16)):
+            out.append({"clusters": True, "image_width": w, "persistent": True, "blocks_per_sm": bps, "coop": coop})
+    for coop in (False, True):
+        out.append({"clusters": True, "image_width": 0, "persistent": True, "blocks_per_sm": 16, "coop": coop, "sorted": True})
+    return out
+
+
 def _load():
     try:
         with open(CACHE) as f:
@@ -76,7 +89,8 @@ def tune_trace(tree, orig, dir, tmax=None, image_width: int = 0, key: str = "def
     out = core.trace(tree, orig, dir, tmax=tmax)
     stream = torch.cuda.current_stream()
     timings = []
-    for sch in candidates(image_width):
+    cands = candidates(image_width) + (cluster_candidates(image_width) if getattr(tree, "clusters", False) else [])
+    for sch in cands:
         core.trace(tree, orig, dir, tmax=tmax, out=out, schedule=sch)  # warm
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -90,6 +104,19 @@ def tune_trace(tree, orig, dir, tmax=None, image_width: int = 0, key: str = "def
         cache[ck] = {"best": best, "timings": timings}
         _store(cache)
     return best, timings
+
+
+def cluster_batch_candidates(images=None):
+    """Batched schedules that walk the cluster tree (a build with clusters=True): per-lane walks (one thread per
+    ray, persistent warps), the warp-cooperative walk, each with the ray orders of batch_candidates."""
+    out = [{"clusters": True, "persistent": False, "blocks_per_sm": 0}]
+    for coop, bps in ((False, 8), (False, 16), (True, 8), (True, 16)):
+        out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop})
+        for bits in (0, 12):
+            out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "sorted_bits": bits})
+        if images is not None and images[1] % 8 == 0 and images[2] % 4 == 0:
+            out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "tiles": list(images)})
+    return out
 
 
 def batch_candidates(images=None):
@@ -131,6 +158,11 @@ def tune_batch_trace(tree, orig, dir, ray_offsets, tmax=None, key: str = "batch"
     if order is not None:
         cands += [{"while_while": True, "wide": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "given_order": True}
                   for coop, bps in ((True, 16), (True, 8), (False, 8))]
+    if getattr(tree, "clusters", False):
+        cands += cluster_batch_candidates(images)
+        if order is not None:
+            cands += [{"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "given_order": True}
+                      for coop, bps in ((True, 16), (False, 8))]
     for sch in cands:
         given = order if sch.get("given_order") else None
         core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax, out=out, schedule=sch, order=given)  # warm

@@ -35,7 +35,7 @@ typedef struct CUstream_st* rt_stream; /* a cudaStream_t; NULL = legacy default 
 /* Layout version of the structs below. A caller compiled against this header
  * must check rt_abi_version() == RT_ABI_VERSION before passing any struct:
  * a library built from a different header reads different field offsets. */
-#define RT_ABI_VERSION 8u
+#define RT_ABI_VERSION 9u
 
 typedef enum rt_status {
   RT_OK = 0,
@@ -52,6 +52,7 @@ typedef enum rt_status {
 #define RT_DEVERR_STACK_OVERFLOW 0x2u /* traversal stack exhausted (result of that ray may be wrong) */
 #define RT_DEVERR_MORTON_CAPACITY 0x4u
 #define RT_DEVERR_WAIT_TIMEOUT 0x8u    /* a bounded wait inside a kernel ran out (2 s); that kernel's output is invalid */
+#define RT_DEVERR_ACCEL_MISSING 0x10u  /* the blob lacks the tree the schedule walks (or was built for other sizes) */
 
 typedef struct rt_build_params {
   uint32_t tree_depth;    /* Morton levels; reference default 12 (CUDAMeshTree.h:118); 1..32 */
@@ -59,7 +60,18 @@ typedef struct rt_build_params {
   uint32_t min_leaf;      /* 16, kernels/CUDA_buildMeshTreeLBVH.cu:39 (0 = default) */
   uint32_t max_leaf;      /* 224, kernels/CUDA_buildMeshTreeLBVH.cu:40 (0 = default) */
   uint32_t morton_bits;   /* 32: reference 11/11/10 interleave; 30: 10/10/10 left-aligned (0 = 32) */
+  uint32_t accel_trees;   /* traversal trees written into the blob besides the node records: RT_ACCEL_* bits (0 = none) */
+  uint32_t cluster_leaf;  /* RT_ACCEL_CLUSTERS: most positions per cluster tree leaf, 1..8 (0 = 4) */
 } rt_build_params;
+
+/* rt_build_params.accel_trees. The blob always holds records of the build's
+ * node tree (whose leaves hold ~N / 2^tree_depth triangles). RT_ACCEL_CLUSTERS
+ * adds the cluster tree: the binary radix tree of the sorted (Morton code,
+ * position) keys, cut at subtrees of at most cluster_leaf positions and stored
+ * as 4-wide records (two more launches; scratch grows by ~76 bytes per face;
+ * meshes below 2^28 faces), walked by the RT_TRACE_CLUSTERS schedules. No
+ * reference counterpart. */
+#define RT_ACCEL_CLUSTERS 0x2u
 
 /* Written by rt_lbvh_build on the device. */
 typedef struct rt_build_info {
@@ -282,6 +294,8 @@ typedef struct rt_trace_desc {
 #define RT_TRACE_WHILE_WHILE 0x1u /* descend until a leaf is held, then test it (else: interleaved) */
 #define RT_TRACE_COOP 0x2u        /* the warp's lanes share the triangle tests of all its rays' leaves */
 #define RT_TRACE_WIDE 0x4u /* descend through the blob's 4-wide records */
+#define RT_TRACE_CLUSTERS 0x8u /* walk the blob's cluster tree (built with RT_ACCEL_CLUSTERS; else every ray reports a miss
+                                  and RT_DEVERR_ACCEL_MISSING is raised); WHILE_WHILE and WIDE are ignored */
 
 /* A tracing order for incoherent rays: ray indices sorted by direction octant,
  * then by the Morton code of the origin inside box (min xyz, max xyz, HOST);
