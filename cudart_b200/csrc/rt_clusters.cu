@@ -20,20 +20,26 @@
 // hands over its far end of the range), the second completes the parent
 // (box, 4-wide record) and climbs on, so no thread ever waits.
 //
-// Two passes keep almost all of that in shared memory:
+// Three launches keep almost all of that in shared memory:
 //   k_cluster_chunk     one CTA per chunk of 512 positions of one mesh: the
 //                       climb through the parents whose boundary lies inside
-//                       the chunk, with shared-memory arrival words, child
-//                       references and boxes (every node completed here has
-//                       both children inside the chunk). A node whose parent
-//                       boundary lies outside the chunk (at most one per side)
-//                       is left in the chunk's frontier; at the end the CTA
-//                       writes its arrival words to global memory.
+//                       the chunk, in rounds over a compacted list of the
+//                       nodes moving up, with shared-memory arrival words,
+//                       child references and boxes (every node completed here
+//                       has both children inside the chunk), then the records
+//                       of those nodes. A node whose parent boundary lies
+//                       outside the chunk (at most one per side) is left in the
+//                       chunk's frontier; the CTA writes all its arrival words
+//                       and, for the next passes, the few nodes they read.
 //   k_cluster_frontier  one thread per frontier node: the rest of the climb
-//                       through global memory (device fence before each
-//                       exchange and after a second arrival, reads through L2).
-// Boxes and child references always go to global memory too, for the records
-// and completions of the second pass.
+//                       through global memory; an arriving child stores its
+//                       reference and box in its side of the parent's slots,
+//                       then exchanges the parent's word (acquire-release), so
+//                       the second arrival reads the sibling's box at once.
+//   k_cluster_records   the records of the nodes the frontier pass completed
+//                       (each frontier thread lists the nodes it completed).
+#include <cuda/atomic>
+
 #include "rt_common.cuh"
 #include "rt_device.cuh"
 
@@ -81,8 +87,8 @@ __device__ __forceinline__ void tri_box(const float4* tr, float3& mn, float3& mx
   pad_box(mn, mx);
 }
 
-// Where a pass reads the boxes and child references of completed nodes: shared memory for the chunk pass (the
-// chunk's positions and inner boundaries), global memory (through L2) for the frontier pass.
+// Where a pass reads the child references and child boxes of completed nodes: shared memory for the chunk pass
+// (the chunk's positions and inner boundaries), global memory (through L2) for the record pass.
 struct SmemNodes {
   const float (*lbox)[kClusterChunk];
   const float (*ibox)[kClusterChunk];
@@ -95,44 +101,44 @@ struct SmemNodes {
     mx = make_float3(b[3][k], b[4][k], b[5][k]);
   }
   __device__ __forceinline__ uint32_t kid(uint32_t p, uint32_t side) const { return child[2 * (p - s) + side]; }
+  __device__ __forceinline__ void kid_box(uint32_t p, uint32_t side, float3& mn, float3& mx) const { box(kid(p, side), mn, mx); }
 };
 struct GlobalNodes {
   const ClusterTemps* T;
   uint32_t F;
-  __device__ __forceinline__ void box(uint32_t ref, float3& mn, float3& mx) const {
-    const float4* p = (ref & kClusterLeaf) ? T->lbox + 2 * ((size_t)F + (ref & ~kClusterLeaf)) : T->ibox + 2 * ((size_t)F + ref);
-    const float4 a = __ldcg(p), b = __ldcg(p + 1);
+  __device__ __forceinline__ uint32_t kid(uint32_t p, uint32_t side) const { return __ldcg(T->child + 2 * ((size_t)F + p) + side); }
+  __device__ __forceinline__ void kid_box(uint32_t p, uint32_t side, float3& mn, float3& mx) const {
+    const float4* q = T->cbox + 4 * ((size_t)F + p) + 2 * side;
+    const float4 a = __ldcg(q), b = __ldcg(q + 1);
     mn = make_float3(a.x, a.y, a.z);
     mx = make_float3(b.x, b.y, b.z);
   }
-  __device__ __forceinline__ uint32_t kid(uint32_t p, uint32_t side) const { return __ldcg(T->child + 2 * ((size_t)F + p) + side); }
 };
 
-// The 4-wide record of a completed internal node p (positions l .. r, children c0 = l .. p and c1 = p + 1 .. r):
-// child c0 fills slots 0 and 1, c1 slots 2 and 3 -- a child that is a cluster (at most leaf_max positions) its
-// first slot (the second keeps NaN bounds), any other child one slot for each of its two children.
+// The 4-wide record of a completed internal node p (positions l .. r, children l .. p and p + 1 .. r): child 0
+// fills slots 0 and 1, child 1 slots 2 and 3 -- a child that is a cluster (at most leaf_max positions) its first
+// slot (the second keeps NaN bounds), any other child one slot for each of its two children.
 template <class Nodes>
-__device__ __forceinline__ void write_record(const ClusterBuild& B, const Nodes& Nd, float4* rec, uint32_t p, uint32_t l, uint32_t r,
-                                             uint32_t c0, uint32_t c1) {
+__device__ __forceinline__ void write_record(const ClusterBuild& B, const Nodes& Nd, float4* rec, uint32_t p, uint32_t l, uint32_t r) {
   const float qnan = __int_as_float(0x7fffffff);
   float3 mn[4], mx[4];
   uint32_t ref[4];
-  auto child = [&](const int k, uint32_t c, uint32_t lo, uint32_t hi) {
-    auto put = [&](const int q, uint32_t sref, uint32_t slo, uint32_t shi) {
-      Nd.box(sref, mn[q], mx[q]);
-      ref[q] = (shi - slo + 1 <= B.leaf_max) ? cluster_leaf_ref(slo, shi - slo + 1) : sref;
-    };
+  auto child = [&](const int k, uint32_t lo, uint32_t hi) {
+    const uint32_t c = Nd.kid(p, (uint32_t)(k >> 1));
     if (hi - lo + 1 <= B.leaf_max) {
-      put(k, c, lo, hi);
+      Nd.kid_box(p, (uint32_t)(k >> 1), mn[k], mx[k]);
+      ref[k] = cluster_leaf_ref(lo, hi - lo + 1);
       mn[k + 1] = mx[k + 1] = make_float3(qnan, qnan, qnan);
       ref[k + 1] = kNoChild;
     } else {  // an internal node (more than leaf_max >= 1 positions); its split is its own index
-      put(k, Nd.kid(c, 0), lo, c);
-      put(k + 1, Nd.kid(c, 1), c + 1, hi);
+      Nd.kid_box(c, 0, mn[k], mx[k]);
+      Nd.kid_box(c, 1, mn[k + 1], mx[k + 1]);
+      ref[k] = (c - lo + 1 <= B.leaf_max) ? cluster_leaf_ref(lo, c - lo + 1) : Nd.kid(c, 0);
+      ref[k + 1] = (hi - c <= B.leaf_max) ? cluster_leaf_ref(c + 1, hi - c) : Nd.kid(c, 1);
     }
   };
-  child(0, c0, l, p);
-  child(2, c1, p + 1, r);
+  child(0, l, p);
+  child(2, p + 1, r);
   rec[0] = make_float4(mn[0].x, mn[1].x, mn[2].x, mn[3].x);
   rec[1] = make_float4(mn[0].y, mn[1].y, mn[2].y, mn[3].y);
   rec[2] = make_float4(mn[0].z, mn[1].z, mn[2].z, mn[3].z);
@@ -174,15 +180,15 @@ __device__ __forceinline__ void finish_root(const ClusterBuild& B, uint32_t m, u
 // (range and box, in shared memory) and lists it for the next round, so the threads of a warp work on listed
 // nodes side by side. After the last round the CTA writes, with coalesced stores, every position's box, every
 // inner boundary's child references, box and arrival word, and the records of the nodes completed here.
-__global__ __launch_bounds__(kClusterChunk, 2) void k_cluster_chunk(ClusterBuild B) {
+__global__ __launch_bounds__(kClusterChunk, 4) void k_cluster_chunk(ClusterBuild B) {
   __shared__ uint32_t s_other[kClusterChunk];
   __shared__ uint32_t s_child[2 * kClusterChunk];
   __shared__ uint32_t s_range[2][kClusterChunk];  // first and last position of a node completed here (else last = 0)
   __shared__ float s_ibox[6][kClusterChunk];
   __shared__ float s_lbox[6][kClusterChunk];
   __shared__ uint32_t s_code[kClusterChunk + 2];  // codes of positions s - 1 .. s + 512
-  __shared__ uint32_t s_list[2][kClusterChunk];   // per round: the listed nodes' references
-  __shared__ uint32_t s_count[2];
+  __shared__ uint32_t s_list[3][kClusterChunk];   // round r reads list r % 3 and fills list (r + 1) % 3
+  __shared__ uint32_t s_count[3];
   const uint32_t t = threadIdx.x;
   uint32_t m, F, n, j;
   if (B.foff && B.M <= kClusterChunk) {
@@ -210,8 +216,6 @@ __global__ __launch_bounds__(kClusterChunk, 2) void k_cluster_chunk(ClusterBuild
     float3 mn, mx;
     tri_box(B.tris + 3 * ((size_t)F + i), mn, mx);
     s_lbox[0][t] = mn.x; s_lbox[1][t] = mn.y; s_lbox[2][t] = mn.z; s_lbox[3][t] = mx.x; s_lbox[4][t] = mx.y; s_lbox[5][t] = mx.z;
-    B.T.lbox[2 * ((size_t)F + i)] = make_float4(mn.x, mn.y, mn.z, 0.f);
-    B.T.lbox[2 * ((size_t)F + i) + 1] = make_float4(mx.x, mx.y, mx.z, 0.f);
     s_list[0][t] = kClusterLeaf | i;
   }
   if (t == 0) {
@@ -221,7 +225,8 @@ __global__ __launch_bounds__(kClusterChunk, 2) void k_cluster_chunk(ClusterBuild
   __syncthreads();
   const SmemNodes Nd{s_lbox, s_ibox, s_child, s};
   for (uint32_t round = 0;; ++round) {
-    const uint32_t cb = round & 1u, nb = cb ^ 1u;
+    // one barrier per round: the list after next (read two rounds ago) is emptied during this round
+    const uint32_t cb = round % 3u, nb = (round + 1u) % 3u;
     const uint32_t count = s_count[cb];
     if (count == 0) break;
     if (t < count) {
@@ -259,65 +264,123 @@ __global__ __launch_bounds__(kClusterChunk, 2) void k_cluster_chunk(ClusterBuild
             s_ibox[3][k] = fmaxf(amx.x, bmx.x); s_ibox[4][k] = fmaxf(amx.y, bmx.y); s_ibox[5][k] = fmaxf(amx.z, bmx.z);
             s_range[0][k] = l;
             s_range[1][k] = r;
-            s_list[nb][atomicAdd(s_count + nb, 1u)] = p;
+            // append to the next list, one shared-memory atomic per warp
+            const uint32_t am = __activemask();
+            const uint32_t lane = t & 31u, leader = __ffs(am) - 1u;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(s_count + nb, (uint32_t)__popc(am));
+            base = __shfl_sync(am, base, leader);
+            s_list[nb][base + __popc(am & ((1u << lane) - 1u))] = p;
           }
         }
       }
     }
-    __syncthreads();
-    if (t == 0) s_count[cb] = 0;  // the list after next starts empty
+    if (t == 0) s_count[(round + 2u) % 3u] = 0;
     __syncthreads();
   }
-  // write-out (coalesced): boundary i's child references, box and arrival word (e's is zero: its children are
-  // never both inside one chunk), and the record of node i when it was completed here and holds > leaf_max positions
+  // Write-out. Every boundary's arrival word (coalesced; e's is zero: its children are never both inside one chunk),
+  // the record of each node completed here with more than leaf_max positions, and
+  // for the global pass and its records the nodes they read: the frontier nodes and the first child to arrive at
+  // each parent still pending, each with its box and, when internal, its child references and their boxes.
+  auto put_box = [&](float4* dst, uint32_t ref) {
+    float3 mn, mx;
+    Nd.box(ref, mn, mx);
+    dst[0] = make_float4(mn.x, mn.y, mn.z, 0.f);
+    dst[1] = make_float4(mx.x, mx.y, mx.z, 0.f);
+  };
+  auto export_kids = [&](uint32_t ref) {
+    if (ref & kClusterLeaf) return;
+    const uint32_t k0 = Nd.kid(ref, 0), k1 = Nd.kid(ref, 1);
+    *(uint2*)(B.T.child + 2 * ((size_t)F + ref)) = make_uint2(k0, k1);
+    put_box(B.T.cbox + 4 * ((size_t)F + ref), k0);
+    put_box(B.T.cbox + 4 * ((size_t)F + ref) + 2, k1);
+  };
   if (i < e) {
-    *(uint2*)(B.T.child + 2 * ((size_t)F + i)) = make_uint2(s_child[2 * t], s_child[2 * t + 1]);
-    B.T.ibox[2 * ((size_t)F + i)] = make_float4(s_ibox[0][t], s_ibox[1][t], s_ibox[2][t], 0.f);
-    B.T.ibox[2 * ((size_t)F + i) + 1] = make_float4(s_ibox[3][t], s_ibox[4][t], s_ibox[5][t], 0.f);
-    B.T.other[(size_t)F + i] = s_other[t];
+    const uint32_t word = s_other[t];
+    B.T.other[(size_t)F + i] = word;
     const uint32_t l = s_range[0][t], r = s_range[1][t];
-    if (r != 0 && r - l + 1 > B.leaf_max) write_record(B, Nd, B.crec + 8 * ((size_t)F + i), i, l, r, s_child[2 * t], s_child[2 * t + 1]);
+    if (r != 0) {
+      if (r - l + 1 > B.leaf_max) write_record(B, Nd, B.crec + 8 * ((size_t)F + i), i, l, r);
+    } else if (word != 0) {  // one child arrived: a left child stored its first position (<= i), a right one its last
+      const uint32_t side = (word - 1u <= i) ? 0u : 1u;
+      const uint32_t c = s_child[2 * t + side];
+      B.T.child[2 * ((size_t)F + i) + side] = c;
+      put_box(B.T.cbox + 4 * ((size_t)F + i) + 2 * side, c);
+      export_kids(c);
+    }
   } else if (i == e && i + 1 < n) {
     B.T.other[(size_t)F + i] = 0u;
   }
+  if (t < 2) {
+    const uint4 fr = B.T.frontier[2 * (size_t)blockIdx.x + t];
+    if (fr.w) {
+      put_box(B.T.fbox + 4 * (size_t)blockIdx.x + 2 * t, fr.x);
+      export_kids(fr.x);
+    }
+  }
 }
 
+// The rest of the climb, from the frontier nodes, through global memory. Each arriving child stores its
+// reference and box in its side of the parent's slots, then exchanges the parent's arrival word with
+// acquire-release order at device scope; the second arrival reads the sibling's box, completes the parent and
+// marks it (its range) for k_cluster_records.
 __global__ __launch_bounds__(128) void k_cluster_frontier(ClusterBuild B) {
   const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= 2 * cluster_chunks(B.N, B.M)) return;
   const uint4 fr = B.T.frontier[f];
-  if (fr.w == 0) return;
+  if (fr.w == 0) {
+    B.T.chain[(size_t)f * (kClusterChain + 1) + kClusterChain] = 0;
+    return;
+  }
   uint32_t m, F, n, j;
   mesh_of_chunk(B, f >> 1, m, F, n, j);
-  const GlobalNodes Nd{&B.T, F};
   const uint32_t* codes = B.codes + F;
   uint32_t cur = fr.x, l = fr.y, r = fr.z;
-  float3 mn, mx;
-  Nd.box(cur, mn, mx);
+  const float4 b0 = B.T.fbox[2 * (size_t)f], b1 = B.T.fbox[2 * (size_t)f + 1];
+  float3 mn = make_float3(b0.x, b0.y, b0.z), mx = make_float3(b1.x, b1.y, b1.z);
+  uint32_t* chain = B.T.chain + (size_t)f * (kClusterChain + 1);
+  uint32_t done = 0;  // nodes completed by this climb (listed in chain for k_cluster_records)
   for (;;) {
     if (l == 0 && r == n - 1) {
       finish_root(B, m, F, n, cur, mn, mx);
-      return;
+      break;
     }
     const bool left_child = (l == 0) || (r != n - 1 && key_xor(__ldg(codes + r), __ldg(codes + r + 1), r) <
                                                          key_xor(__ldg(codes + l - 1), __ldg(codes + l), l - 1));
     const uint32_t p = left_child ? r : l - 1;
     const uint32_t side = left_child ? 0u : 1u;
+    float4* slot = B.T.cbox + 4 * ((size_t)F + p);
     B.T.child[2 * ((size_t)F + p) + side] = cur;
-    __threadfence();
-    const uint32_t old = atomicExch(B.T.other + F + p, (left_child ? l : r) + 1u);
-    if (old == 0) return;  // the sibling completes the parent
-    __threadfence();
+    slot[2 * side] = make_float4(mn.x, mn.y, mn.z, 0.f);
+    slot[2 * side + 1] = make_float4(mx.x, mx.y, mx.z, 0.f);
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> word(B.T.other[(size_t)F + p]);
+    const uint32_t old = word.exchange((left_child ? l : r) + 1u, cuda::memory_order_acq_rel);
+    if (old == 0) break;  // the sibling completes the parent
     if (left_child) r = old - 1u; else l = old - 1u;
-    const uint32_t c0 = Nd.kid(p, 0), c1 = Nd.kid(p, 1);
-    float3 smn, smx;
-    Nd.box(left_child ? c1 : c0, smn, smx);
-    mn = make_float3(fminf(mn.x, smn.x), fminf(mn.y, smn.y), fminf(mn.z, smn.z));
-    mx = make_float3(fmaxf(mx.x, smx.x), fmaxf(mx.y, smx.y), fmaxf(mx.z, smx.z));
-    __stcg(B.T.ibox + 2 * ((size_t)F + p), make_float4(mn.x, mn.y, mn.z, 0.f));
-    __stcg(B.T.ibox + 2 * ((size_t)F + p) + 1, make_float4(mx.x, mx.y, mx.z, 0.f));
-    if (r - l + 1 > B.leaf_max) write_record(B, Nd, B.crec + 8 * ((size_t)F + p), p, l, r, c0, c1);
+    const float4 s0 = __ldcg(slot + 2 * (1 - side)), s1 = __ldcg(slot + 2 * (1 - side) + 1);
+    mn = make_float3(fminf(mn.x, s0.x), fminf(mn.y, s0.y), fminf(mn.z, s0.z));
+    mx = make_float3(fmaxf(mx.x, s1.x), fmaxf(mx.y, s1.y), fmaxf(mx.z, s1.z));
+    B.T.prange[(size_t)F + p] = make_uint2(l, r + 1u);
+    if (done < kClusterChain) chain[done++] = p;
     cur = p;
+  }
+  chain[kClusterChain] = done;
+}
+
+// Records of the nodes the frontier pass completed: one warp per frontier node, a lane per node of its climb.
+__global__ __launch_bounds__(256) void k_cluster_records(ClusterBuild B) {
+  const uint32_t f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
+  if (f >= 2 * cluster_chunks(B.N, B.M)) return;
+  const uint32_t* chain = B.T.chain + (size_t)f * (kClusterChain + 1);
+  const uint32_t done = chain[kClusterChain];
+  if (done == 0) return;
+  uint32_t m, F, n, j;
+  mesh_of_chunk(B, f >> 1, m, F, n, j);
+  for (uint32_t k = lane; k < done; k += 32) {
+    const uint32_t p = chain[k];
+    const uint2 pr = B.T.prange[(size_t)F + p];
+    const uint32_t l = pr.x, r = pr.y - 1u;
+    if (r - l + 1 > B.leaf_max) write_record(B, GlobalNodes{&B.T, F}, B.crec + 8 * ((size_t)F + p), p, l, r);
   }
 }
 
@@ -337,7 +400,8 @@ rt_status batch_build_cluster_tree(const float4* tris, const uint32_t* codes, co
   const uint32_t chunks = cluster_chunks(N, M);
   k_cluster_chunk<<<chunks, kClusterChunk, 0, st>>>(B);
   k_cluster_frontier<<<(2 * chunks + 127) / 128, 128, 0, st>>>(B);
-  note_launch(2);
+  k_cluster_records<<<(2 * chunks * 32 + 255) / 256, 256, 0, st>>>(B);
+  note_launch(3);
   RT_CHECK_LAUNCH();
   return RT_OK;
 }

@@ -170,26 +170,34 @@ constexpr int kHdrClusterRoot = 18;   // record index of the root
 __host__ __device__ __forceinline__ uint32_t cluster_leaf_ref(uint32_t first, uint32_t count) {
   return kClusterLeaf | ((count - 1u) << 28) | first;
 }
-// Build temporaries (per position of all meshes): the arrival word of each internal node, its two child
-// references (kClusterLeaf | position for a position), the padded boxes of internal nodes and of positions.
 // The build works in chunks of kClusterChunk positions (one CTA each, never across meshes; mesh m's chunks start
 // at chunk cluster_chunk_base(F_m, m)); each chunk leaves at most two nodes for the global pass (`frontier`).
 constexpr uint32_t kClusterChunk = 512;
 __host__ __device__ __forceinline__ uint32_t cluster_chunk_base(uint32_t F, uint32_t m) { return F / kClusterChunk + m; }
 __host__ __device__ __forceinline__ uint32_t cluster_chunks(uint32_t N, uint32_t M) { return N / kClusterChunk + M + 1; }
+// Build temporaries (per position of all meshes, indexed by F_m + boundary): the arrival word of each internal
+// node, its two child references (kClusterLeaf | position for a position) and the padded boxes of those two
+// children, the range of each node the global pass completes (first, last + 1); per chunk the (at most two)
+// frontier nodes, their boxes and the nodes their climbs completed.
 struct ClusterTemps {
   uint32_t* other;
   uint32_t* child;
-  float4* ibox;
-  float4* lbox;
+  float4* cbox;     // [4 N]: box of child k of boundary b at 4 b + 2 k (min, max)
+  uint2* prange;
   uint4* frontier;  // [2 chunks]: (reference, first, last, 1) of a node whose parent lies outside its chunk, else zero
+  float4* fbox;     // [4 chunks]: the frontier nodes' boxes (min, max)
+  uint32_t* chain;  // [2 chunks x kClusterChain]: the nodes each frontier node's climb completed, then their count
 };
+constexpr uint32_t kClusterChain = 64;  // a climb completes at most one node per bit of the 64-bit keys
 inline void carve_cluster_temps(Carve& c, ClusterTemps& T, size_t N, size_t M) {
+  const size_t chunks = N / kClusterChunk + M + 1;
   T.other = c.take<uint32_t>(N);
   T.child = c.take<uint32_t>(2 * N);
-  T.ibox = c.take<float4>(2 * N);
-  T.lbox = c.take<float4>(2 * N);
-  T.frontier = c.take<uint4>(2 * (N / kClusterChunk + M + 1));
+  T.cbox = c.take<float4>(4 * N);
+  T.prange = c.take<uint2>(N);
+  T.frontier = c.take<uint4>(2 * chunks);
+  T.fbox = c.take<float4>(4 * chunks);
+  T.chain = c.take<uint32_t>(2 * chunks * (kClusterChain + 1));
 }
 
 // Traversal blob: header (256 B), internal-node records (64 B, <= N - 1),

@@ -113,9 +113,11 @@ rt_status rt_lbvh_scratch_bytes(uint32_t face_count, const rt_build_params* para
 
 /* Bytes of the optional traversal blob of an N-face build: two-child records
  * of the internal nodes (both children's padded boxes, indexed by pre-order
- * rank), the leaf table, and one padded box per 8 consecutive triangles of a
- * leaf. Derived from the same tree; the nodes stay the reference's. No
- * reference counterpart (the reference traverses bvnodes directly). */
+ * rank), the leaf table, one padded box per 8 consecutive triangles of a
+ * leaf, 4-wide records, and room for the cluster tree (RT_ACCEL_CLUSTERS,
+ * 128 bytes per face). Derived from the same build; the nodes stay the
+ * reference's. No reference counterpart (the reference traverses bvnodes
+ * directly). */
 rt_status rt_lbvh_accel_bytes(uint32_t face_count, size_t* bytes);
 
 /* LBVH build: boxes, Morton codes, key+index sort, split lists, topology,
