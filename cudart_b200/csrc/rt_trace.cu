@@ -731,8 +731,10 @@ __device__ __forceinline__ bool pop_within(const uint32_t (&st_ref)[kStack], con
 
 // One ray, one lane: nearest-first descent through the 4-wide records; a
 // cluster is tested when the walk reaches it (entered nearest first, skipped
-// once it can no longer hold a closer hit).
-template <bool kCount>
+// once it can no longer hold a closer hit). kWW (while-while): each step first
+// descends until the lane holds a cluster, then tests it, so the lanes of a
+// warp test triangles together instead of interleaving box and triangle steps.
+template <bool kCount, bool kWW>
 __device__ __forceinline__ void trace_ray_clusters(const uint32_t r, const TraceArgs& A, const ClusterArgs& C) {
   const float tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
   int32_t best = -1;
@@ -751,47 +753,70 @@ __device__ __forceinline__ void trace_ray_clusters(const uint32_t r, const Trace
     uint32_t st_ref[kStack];
     float st_t[kStack];
     int sp = 0;
-    for (;;) {
+    // one record step: false when the walk is over (nothing hit and nothing stacked within reach)
+    auto record_step = [&]() -> bool {
+      float t[4];
+      uint32_t k[4];
+      cluster_test(recs + 8 * (size_t)ref, oi, ix, iy, iz, bt, t, k);
+      if (kCount) visits += 4;
+      if (t[0] != INFINITY) {
+#pragma unroll
+        for (int j = 3; j >= 1; --j) {
+          if (t[j] != INFINITY) {
+            if (sp < kStack) {
+              st_ref[sp] = k[j];
+              st_t[sp] = t[j];
+              ++sp;
+            } else if (A.err) {
+              atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
+            }
+          }
+        }
+        ref = k[0];
+        return true;
+      }
+      return pop_within(st_ref, st_t, sp, bt, ref);
+    };
+    auto cluster_step = [&]() {
+      const uint32_t p0 = ref & kClusterFirstMask, p1 = p0 + ((ref >> 28) & 7u) + 1u;
+      for (uint32_t pos = p0; pos < p1; ++pos) {
+        const float4 v0 = ldg4(tris + 3 * (size_t)pos);
+        const float4 e1 = ldg4(tris + 3 * (size_t)pos + 1);
+        const float4 e2 = ldg4(tris + 3 * (size_t)pos + 2);
+        if (kCount) ++tests;
+        float th, u, v;
+        if (!mt_test(o, d, zu, zv, v0, e1, e2, th, u, v)) continue;
+        if (th < bt || (best >= 0 && th == bt && (int32_t)pos < best)) {
+          best = (int32_t)pos; bt = th; bu = u; bv = v;
+        }
+      }
+    };
+    bool alive = true;
+    while (alive) {
       if (!cluster_ref_ok(ref, C.n)) {
         if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
         break;
       }
-      if (!(ref & kClusterLeaf)) {
-        float t[4];
-        uint32_t k[4];
-        cluster_test(recs + 8 * (size_t)ref, oi, ix, iy, iz, bt, t, k);
-        if (kCount) visits += 4;
-        if (t[0] != INFINITY) {
-#pragma unroll
-          for (int j = 3; j >= 1; --j) {
-            if (t[j] != INFINITY) {
-              if (sp < kStack) {
-                st_ref[sp] = k[j];
-                st_t[sp] = t[j];
-                ++sp;
-              } else if (A.err) {
-                atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
-              }
-            }
+      if constexpr (kWW) {
+        while (!(ref & kClusterLeaf)) {
+          if (!record_step()) { alive = false; break; }
+          if (!cluster_ref_ok(ref, C.n)) {
+            if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+            alive = false;
+            break;
           }
-          ref = k[0];
-          continue;
         }
+        if (!alive) break;
+        cluster_step();
+        alive = pop_within(st_ref, st_t, sp, bt, ref);
       } else {
-        const uint32_t p0 = ref & kClusterFirstMask, p1 = p0 + ((ref >> 28) & 7u) + 1u;
-        for (uint32_t pos = p0; pos < p1; ++pos) {
-          const float4 v0 = ldg4(tris + 3 * (size_t)pos);
-          const float4 e1 = ldg4(tris + 3 * (size_t)pos + 1);
-          const float4 e2 = ldg4(tris + 3 * (size_t)pos + 2);
-          if (kCount) ++tests;
-          float th, u, v;
-          if (!mt_test(o, d, zu, zv, v0, e1, e2, th, u, v)) continue;
-          if (th < bt || (best >= 0 && th == bt && (int32_t)pos < best)) {
-            best = (int32_t)pos; bt = th; bu = u; bv = v;
-          }
+        if (!(ref & kClusterLeaf)) {
+          alive = record_step();
+        } else {
+          cluster_step();
+          alive = pop_within(st_ref, st_t, sp, bt, ref);
         }
       }
-      if (!pop_within(st_ref, st_t, sp, bt, ref)) break;
     }
   }
   write_hit(r, A, C.F, best, bt, bu, bv, tmax0);
@@ -1071,14 +1096,14 @@ __global__ __launch_bounds__(128) void k_batch_trace_persistent(TraceArgs A, Bat
 }
 
 // Cluster tree kernels: single mesh (slots through a SlotMap) and batched (each ray's mesh by binary search).
-template <bool kCount>
+template <bool kCount, bool kWW>
 __global__ __launch_bounds__(128) void k_trace_clusters(TraceArgs A, ClusterArgs C, SlotMap M) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t r;
   C.F = 0;
-  if (s < M.slots && M.ray_of(s, r)) trace_ray_clusters<kCount>(r, A, C);
+  if (s < M.slots && M.ray_of(s, r)) trace_ray_clusters<kCount, kWW>(r, A, C);
 }
-template <bool kCount>
+template <bool kCount, bool kWW>
 __global__ __launch_bounds__(128) void k_trace_clusters_persistent(TraceArgs A, ClusterArgs C, SlotMap M, uint32_t* counter) {
   const uint32_t lane = lane_id();
   C.F = 0;
@@ -1089,7 +1114,7 @@ __global__ __launch_bounds__(128) void k_trace_clusters_persistent(TraceArgs A, 
     if (base >= M.slots) break;
     uint32_t r;
     const uint32_t s = base + lane;
-    if (s < M.slots && M.ray_of(s, r)) trace_ray_clusters<kCount>(r, A, C);
+    if (s < M.slots && M.ray_of(s, r)) trace_ray_clusters<kCount, kWW>(r, A, C);
   }
 }
 template <bool kCount>
@@ -1117,7 +1142,7 @@ __device__ __forceinline__ void batch_cluster_args(uint32_t r, const BatchTraceA
   C.F = F;
   C.n = __ldg(B.foff + m + 1) - F;
 }
-template <bool kCount>
+template <bool kCount, bool kWW>
 __global__ __launch_bounds__(128) void k_batch_trace_clusters(TraceArgs A, BatchTraceArgs B) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= A.ray_count) return;
@@ -1125,9 +1150,9 @@ __global__ __launch_bounds__(128) void k_batch_trace_clusters(TraceArgs A, Batch
   ClusterArgs C;
   C.crec = B.acc.crec;
   batch_cluster_args(r, B, C);
-  trace_ray_clusters<kCount>(r, A, C);
+  trace_ray_clusters<kCount, kWW>(r, A, C);
 }
-template <bool kCount>
+template <bool kCount, bool kWW>
 __global__ __launch_bounds__(128) void k_batch_trace_clusters_persistent(TraceArgs A, BatchTraceArgs B, uint32_t* counter) {
   const uint32_t lane = lane_id();
   for (;;) {
@@ -1141,7 +1166,7 @@ __global__ __launch_bounds__(128) void k_batch_trace_clusters_persistent(TraceAr
       ClusterArgs C;
       C.crec = B.acc.crec;
       batch_cluster_args(r, B, C);
-      trace_ray_clusters<kCount>(r, A, C);
+      trace_ray_clusters<kCount, kWW>(r, A, C);
     }
   }
 }
@@ -1404,6 +1429,7 @@ SlotMap slot_map(const rt_trace_desc* d) {
 // the warp-cooperative walk (RT_TRACE_COOP, persistent warps; without a work counter the per-lane grid).
 rt_status launch_clusters(const rt_trace_desc* d, const TraceArgs& A, cudaStream_t st) {
   const bool count = d->ray_visits || d->ray_tests;
+  const bool ww = (d->schedule & RT_TRACE_WHILE_WHILE) != 0;
   ClusterArgs C;
   {
     Carve c((void*)d->accel, ~(size_t)0);
@@ -1422,13 +1448,17 @@ rt_status launch_clusters(const rt_trace_desc* d, const TraceArgs& A, cudaStream
       if (count) k_trace_clusters_coop<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
       else k_trace_clusters_coop<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
     } else {
-      if (count) k_trace_clusters_persistent<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
-      else k_trace_clusters_persistent<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
+#define RT_LAUNCH_CP(CNT, WW) k_trace_clusters_persistent<CNT, WW><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter)
+      if (count) { if (ww) RT_LAUNCH_CP(true, true); else RT_LAUNCH_CP(true, false); }
+      else { if (ww) RT_LAUNCH_CP(false, true); else RT_LAUNCH_CP(false, false); }
+#undef RT_LAUNCH_CP
     }
   } else {
     const uint32_t blocks = (M.slots + 127) / 128;
-    if (count) k_trace_clusters<true><<<blocks, 128, 0, st>>>(A, C, M);
-    else k_trace_clusters<false><<<blocks, 128, 0, st>>>(A, C, M);
+#define RT_LAUNCH_CS(CNT, WW) k_trace_clusters<CNT, WW><<<blocks, 128, 0, st>>>(A, C, M)
+    if (count) { if (ww) RT_LAUNCH_CS(true, true); else RT_LAUNCH_CS(true, false); }
+    else { if (ww) RT_LAUNCH_CS(false, true); else RT_LAUNCH_CS(false, false); }
+#undef RT_LAUNCH_CS
   }
   note_launch();
   RT_CHECK_LAUNCH();
@@ -1704,6 +1734,7 @@ rt_status batch_launch_w(const rt_batch_trace_desc* d, const TraceArgs& A, const
 }
 
 rt_status batch_launch_clusters(const rt_batch_trace_desc* d, const TraceArgs& A, const BatchTraceArgs& B, cudaStream_t st, bool count) {
+  const bool ww = (d->schedule & RT_TRACE_WHILE_WHILE) != 0;
   if (d->work_counter) {
     if (cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
     const uint32_t per_sm = d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u;
@@ -1712,13 +1743,17 @@ rt_status batch_launch_clusters(const rt_batch_trace_desc* d, const TraceArgs& A
       if (count) k_batch_trace_clusters_coop<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
       else k_batch_trace_clusters_coop<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
     } else {
-      if (count) k_batch_trace_clusters_persistent<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
-      else k_batch_trace_clusters_persistent<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
+#define RT_LAUNCH_BCP(CNT, WW) k_batch_trace_clusters_persistent<CNT, WW><<<blocks, 128, 0, st>>>(A, B, d->work_counter)
+      if (count) { if (ww) RT_LAUNCH_BCP(true, true); else RT_LAUNCH_BCP(true, false); }
+      else { if (ww) RT_LAUNCH_BCP(false, true); else RT_LAUNCH_BCP(false, false); }
+#undef RT_LAUNCH_BCP
     }
   } else {
     const uint32_t blocks = (d->ray_count + 127) / 128;
-    if (count) k_batch_trace_clusters<true><<<blocks, 128, 0, st>>>(A, B);
-    else k_batch_trace_clusters<false><<<blocks, 128, 0, st>>>(A, B);
+#define RT_LAUNCH_BCS(CNT, WW) k_batch_trace_clusters<CNT, WW><<<blocks, 128, 0, st>>>(A, B)
+    if (count) { if (ww) RT_LAUNCH_BCS(true, true); else RT_LAUNCH_BCS(true, false); }
+    else { if (ww) RT_LAUNCH_BCS(false, true); else RT_LAUNCH_BCS(false, false); }
+#undef RT_LAUNCH_BCS
   }
   note_launch();
   RT_CHECK_LAUNCH();

@@ -53,12 +53,15 @@ def cluster_candidates(image_width: int):
     """Single-mesh schedules that walk the cluster tree (a build with clusters=True)."""
     widths = [0, image_width] if image_width else [0]
     out = []
-    for w in widths:
-        out.append({"clusters": True, "image_width": w, "persistent": False, "blocks_per_sm": 0})
-        for coop, bps in ((False, 8), (False, 16), (True, 8), (True, 16)):
-            out.append({"clusters": True, "image_width": w, "persistent": True, "blocks_per_sm": bps, "coop": coop})
-    for coop in (False, True):
-        out.append({"clusters": True, "image_width": 0, "persistent": True, "blocks_per_sm": 16, "coop": coop, "sorted": True})
+    for w, ww in itertools.product(widths, (False, True)):
+        out.append({"clusters": True, "image_width": w, "persistent": False, "blocks_per_sm": 0, "while_while": ww})
+        for bps in (8, 16):
+            out.append({"clusters": True, "image_width": w, "persistent": True, "blocks_per_sm": bps, "while_while": ww})
+    for w, bps in itertools.product(widths, (8, 16)):
+        out.append({"clusters": True, "image_width": w, "persistent": True, "blocks_per_sm": bps, "coop": True})
+    for coop, ww in ((False, False), (False, True), (True, False)):
+        out.append({"clusters": True, "image_width": 0, "persistent": True, "blocks_per_sm": 16, "coop": coop, "while_while": ww,
+                    "sorted": True})
     return out
 
 
@@ -109,13 +112,13 @@ def tune_trace(tree, orig, dir, tmax=None, image_width: int = 0, key: str = "def
 def cluster_batch_candidates(images=None):
     """Batched schedules that walk the cluster tree (a build with clusters=True): per-lane walks (one thread per
     ray, persistent warps), the warp-cooperative walk, each with the ray orders of batch_candidates."""
-    out = [{"clusters": True, "persistent": False, "blocks_per_sm": 0}]
-    for coop, bps in ((False, 8), (False, 16), (True, 8), (True, 16)):
-        out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop})
+    out = [{"clusters": True, "persistent": False, "blocks_per_sm": 0, "while_while": ww} for ww in (False, True)]
+    for coop, ww, bps in ((False, False, 8), (False, False, 16), (False, True, 8), (False, True, 16), (True, False, 8), (True, False, 16)):
+        out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "while_while": ww})
         for bits in (0, 12):
-            out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "sorted_bits": bits})
+            out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "while_while": ww, "sorted_bits": bits})
         if images is not None and images[1] % 8 == 0 and images[2] % 4 == 0:
-            out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "tiles": list(images)})
+            out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "while_while": ww, "tiles": list(images)})
     return out
 
 
@@ -161,8 +164,8 @@ def tune_batch_trace(tree, orig, dir, ray_offsets, tmax=None, key: str = "batch"
     if getattr(tree, "clusters", False):
         cands += cluster_batch_candidates(images)
         if order is not None:
-            cands += [{"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "given_order": True}
-                      for coop, bps in ((True, 16), (False, 8))]
+            cands += [{"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "while_while": ww, "given_order": True}
+                      for coop, ww, bps in ((True, False, 16), (False, False, 8), (False, True, 8))]
     for sch in cands:
         given = order if sch.get("given_order") else None
         core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax, out=out, schedule=sch, order=given)  # warm

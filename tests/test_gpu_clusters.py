@@ -16,7 +16,9 @@ pytestmark = pytest.mark.gpu
 
 CLUSTER_SCHEDULES = [
     dict(clusters=True),                                                    # per-lane, one thread per ray
+    dict(clusters=True, while_while=True),                                  # per-lane, descend-then-test
     dict(clusters=True, persistent=True, blocks_per_sm=8),                   # per-lane, persistent warps
+    dict(clusters=True, persistent=True, blocks_per_sm=8, while_while=True, sorted=True),
     dict(clusters=True, persistent=True, blocks_per_sm=16, coop=True),       # warp-cooperative cluster tests
     dict(clusters=True, persistent=True, blocks_per_sm=16, coop=True, sorted=True),
 ]
@@ -168,7 +170,7 @@ def test_blob_without_cluster_tree_reports_it(T, oracle):
     mesh = scenes.soup(5000, seed=34)
     tree, ref = _build(T, oracle, mesh, clusters=False)
     o, d = (_dev(T, a) for a in scenes.sphere_rays(mesh, 32, seed=4))
-    for sch in CLUSTER_SCHEDULES[:3]:
+    for sch in CLUSTER_SCHEDULES:
         out = core.trace(tree, o, d, schedule=sch)
         T.cuda.synchronize()
         assert int(_host(out["err"])[0]) & _abi.DEVERR_ACCEL_MISSING, sch
@@ -210,7 +212,8 @@ def test_batched_cluster_walks_match_single_mesh(T, oracle):
         e = oracle.trace(ref["nodes"], ref["tris"], ref["indices"], rays[m][0], rays[m][1], None, mode=0)
         exp_id.append(e["id"]); exp_t.append(e["t"]); exp_uv.append(e["uv"])
     e = dict(id=np.concatenate(exp_id), t=np.concatenate(exp_t), uv=np.concatenate(exp_uv))
-    schedules = [dict(clusters=True), dict(clusters=True, persistent=True, blocks_per_sm=8),
+    schedules = [dict(clusters=True), dict(clusters=True, while_while=True), dict(clusters=True, persistent=True, blocks_per_sm=8),
+                 dict(clusters=True, persistent=True, blocks_per_sm=8, while_while=True, sorted_bits=12),
                  dict(clusters=True, persistent=True, blocks_per_sm=16, coop=True),
                  dict(clusters=True, persistent=True, blocks_per_sm=16, coop=True, sorted_bits=12),
                  dict(clusters=True, persistent=True, blocks_per_sm=8, sorted_bits=0)]
@@ -221,7 +224,8 @@ def test_batched_cluster_walks_match_single_mesh(T, oracle):
     # a batched build without cluster trees: refused per ray, no stale reads
     from cudart_b200 import _abi
     b2 = core.batch_build(_dev(T, verts), _dev(T, faces.view(np.int32)), fo, vo)
-    h = core.batch_trace(b2, O, D, roff, schedule=schedules[2])
-    T.cuda.synchronize()
-    assert int(_host(h["err"])[0]) & _abi.DEVERR_ACCEL_MISSING
-    assert (_host(h["id"]) == -1).all()
+    for sch in schedules:
+        h = core.batch_trace(b2, O, D, roff, schedule=sch)
+        T.cuda.synchronize()
+        assert int(_host(h["err"])[0]) & _abi.DEVERR_ACCEL_MISSING, sch
+        assert (_host(h["id"]) == -1).all(), sch
