@@ -26,6 +26,7 @@ TRACE_WHILE_WHILE = 0x1
 TRACE_COOP = 0x2
 TRACE_WIDE = 0x4
 TRACE_CLUSTERS = 0x8
+TRACE_PACKET = 0x10
 ACCEL_CLUSTERS = 0x2
 
 # every symbol include/rt_core.h declares

@@ -320,7 +320,8 @@ def trace_desc(tree: Tree, orig, dir, tmax=None, id_mode: int = 0, counters: boo
             d.persistent_blocks_per_sm = int(sch.get("blocks_per_sm", 8))
             d.treelet_depth = int(sch.get("treelet", 0))  # top levels staged in shared memory (4-wide walks)
         d.schedule = ((_abi.TRACE_WHILE_WHILE if sch.get("while_while", False) else 0) | (_abi.TRACE_COOP if sch.get("coop", False) else 0)
-                      | (_abi.TRACE_WIDE if sch.get("wide", False) else 0) | (_abi.TRACE_CLUSTERS if sch.get("clusters", False) else 0))
+                      | (_abi.TRACE_WIDE if sch.get("wide", False) else 0) | (_abi.TRACE_CLUSTERS if sch.get("clusters", False) else 0)
+                      | (_abi.TRACE_PACKET if sch.get("packet", False) else 0))
         if sch.get("sorted", False):
             order = ray_order(orig, dir, tmax, tree_box(tree), ray_count=R, stream=stream)
             out["_order"] = order  # keep it alive until the trace has run
@@ -687,7 +688,8 @@ def batch_trace_desc(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax
     d.schedule = ((_abi.TRACE_WHILE_WHILE if sch.get("while_while", False) else 0)
                   | (_abi.TRACE_WIDE if sch.get("wide", False) else 0)
                   | (_abi.TRACE_COOP if sch.get("coop", False) else 0)
-                  | (_abi.TRACE_CLUSTERS if sch.get("clusters", False) else 0))
+                  | (_abi.TRACE_CLUSTERS if sch.get("clusters", False) else 0)
+                  | (_abi.TRACE_PACKET if sch.get("packet", False) else 0))
     if order is not None:
         d.ray_order = order.data_ptr()
     elif sch.get("tiles"):  # every mesh's rays are a row-major image of the same size: 8 x 4 pixel tiles per warp

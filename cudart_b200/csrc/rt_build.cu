@@ -646,6 +646,7 @@ struct BuildLayout {
 };
 
 constexpr uint32_t kHitParts = 1184;  // 8 blocks per SM on 148 SMs
+constexpr uint32_t kHitSplit = 8;     // CTAs per mesh of the batched hit box
 
 __host__ __device__ uint32_t morton_cap_dev(uint32_t n, uint32_t D) {
   uint64_t a = (D >= 31) ? (1ull << 32) : ((1ull << (D + 1)) - 1);
@@ -925,6 +926,7 @@ struct BatchArgs {
   rt_build_params q;
   // scratch
   float4* hits;           // [2M]
+  float4* hitpart;        // [2 M kHitSplit]: the hit box shares of k_batch_hitbox
   uint32_t* idx;          // [N] global face index in sorted order
   uint32_t* codes_raw;    // [N] codes before sorting
   uint32_t* mkey;         // [N] mesh id per position
@@ -958,9 +960,11 @@ struct BatchArgs {
 // Per-mesh hitbox: one 512-thread block per mesh, four loads in flight per
 // thread (the largest meshes bound the launch).
 __global__ __launch_bounds__(512) void k_batch_hitbox(BatchArgs B) {
-  const uint32_t m = blockIdx.x;
-  const uint32_t v0 = B.voff[m], v1 = B.voff[m + 1];
-  if (threadIdx.x == 0) {  // the mesh sort's digit counts: mesh m holds foff[m + 1] - foff[m] keys of value m
+  // kHitSplit CTAs per mesh, each over its share of the mesh's vertices; k_batch_hitfinal combines the shares
+  const uint32_t m = blockIdx.x / kHitSplit, part = blockIdx.x % kHitSplit;
+  const uint32_t w0 = B.voff[m], w1 = B.voff[m + 1], share = (w1 - w0 + kHitSplit - 1) / kHitSplit;
+  const uint32_t v0 = min(w1, w0 + part * share), v1 = min(w1, v0 + share);
+  if (part == 0 && threadIdx.x == 0) {  // the mesh sort's digit counts: mesh m holds foff[m + 1] - foff[m] keys of value m
     const uint32_t faces = B.foff[m + 1] - B.foff[m];
     atomicAdd(B.counts + 4 * 256 + (m & 255u), faces);
     atomicAdd(B.counts + 5 * 256 + ((m >> 8) & 255u), faces);
@@ -998,7 +1002,22 @@ __global__ __launch_bounds__(512) void k_batch_hitbox(BatchArgs B) {
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) { B.hits[2 * m] = s_mn[0]; B.hits[2 * m + 1] = s_mx[0]; }
+  if (threadIdx.x == 0) {
+    B.hitpart[2 * (size_t)blockIdx.x] = s_mn[0];
+    B.hitpart[2 * (size_t)blockIdx.x + 1] = s_mx[0];
+  }
+}
+// Each mesh's hit box from its kHitSplit shares (an empty share holds +-huge and changes nothing).
+__global__ __launch_bounds__(128) void k_batch_hitfinal(BatchArgs B) {
+  const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= B.M) return;
+  float4 mn = B.hitpart[2 * (size_t)m * kHitSplit], mx = B.hitpart[2 * (size_t)m * kHitSplit + 1];
+  for (uint32_t p = 1; p < kHitSplit; ++p) {
+    mn = f4min(mn, B.hitpart[2 * ((size_t)m * kHitSplit + p)]);
+    mx = f4max(mx, B.hitpart[2 * ((size_t)m * kHitSplit + p) + 1]);
+  }
+  B.hits[2 * m] = mn;
+  B.hits[2 * m + 1] = mx;
 }
 
 __global__ __launch_bounds__(256) void k_batch_boxes_morton(BatchArgs B) {
@@ -1039,22 +1058,33 @@ __global__ __launch_bounds__(256) void k_batch_levels(BatchArgs B) {
   __shared__ uint32_t s_lc[3 * 256];
   for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) s_lc[i] = 0;
   __syncthreads();
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < B.N; i += gridDim.x * blockDim.x) {
-    const uint32_t c0 = B.codes_raw[B.idx[i]];
-    B.codes[i] = c0;
-    if (i + 1 < B.N) {
-      const uint32_t m = B.mkey[i];
-      uint32_t lev = 32;
-      if (B.mkey[i + 1] == m) {
-        const uint32_t d = c0 ^ B.codes_raw[B.idx[i + 1]];
-        if (d) lev = (uint32_t)__clz(d);
+  // whole warps step together, so that equal keys of a warp are counted with one atomic (the keys of a mesh
+  // crowd onto a few levels: one atomic per position would queue on those few counters)
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < B.N; base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + lane;
+    uint32_t key = ~0u;
+    if (i < B.N) {
+      const uint32_t c0 = B.codes_raw[B.idx[i]];
+      B.codes[i] = c0;
+      if (i + 1 < B.N) {
+        const uint32_t m = B.mkey[i];
+        uint32_t lev = 32;
+        if (B.mkey[i + 1] == m) {
+          const uint32_t d = c0 ^ B.codes_raw[B.idx[i + 1]];
+          if (d) lev = (uint32_t)__clz(d);
+        }
+        key = m * 64 + lev;
+        B.lev[i] = key;
+        B.C[i] = i + 1;
       }
-      const uint32_t key = m * 64 + lev;
-      B.lev[i] = key;
-      B.C[i] = i + 1;
-      atomicAdd(B.hist + key, 1u);
+    }
+    const uint32_t peers = __match_any_sync(0xffffffffu, key);
+    if (key != ~0u && lane == (uint32_t)(__ffs(peers) - 1)) {
+      const uint32_t cnt = (uint32_t)__popc(peers);
+      atomicAdd(B.hist + key, cnt);
 #pragma unroll
-      for (int p = 0; p < 3; ++p) atomicAdd(&s_lc[p * 256 + ((key >> (8 * p)) & 255u)], 1u);
+      for (int p = 0; p < 3; ++p) atomicAdd(&s_lc[p * 256 + ((key >> (8 * p)) & 255u)], cnt);
     }
   }
   __syncthreads();
@@ -1188,6 +1218,7 @@ __global__ __launch_bounds__(256) void k_batch_records(BatchArgs B) {
 
 size_t carve_batch(Carve& c, BatchArgs& B, uint32_t M, uint32_t N, bool clusters) {
   B.hits = c.take<float4>(2 * (size_t)M);
+  B.hitpart = c.take<float4>(2 * (size_t)M * kHitSplit);
   B.idx = c.take<uint32_t>(N);
   B.codes_raw = c.take<uint32_t>(N);
   B.mkey = c.take<uint32_t>(N);
@@ -1272,9 +1303,10 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   if (cudaMemsetAsync(B.err, 0, 16, st) != cudaSuccess) return RT_ERR_CUDA;
   if (cudaMemsetAsync(B.counts, 0, (9 * 256 + 64) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   if (cudaMemsetAsync(B.hist, 0, ((size_t)M * 64 + 1) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
-  k_batch_hitbox<<<M, 512, 0, st>>>(B);
+  k_batch_hitbox<<<M * kHitSplit, 512, 0, st>>>(B);
+  k_batch_hitfinal<<<(M + 127) / 128, 128, 0, st>>>(B);
   k_batch_boxes_morton<<<fblocks, 256, 0, st>>>(B);
-  note_launch(2);
+  note_launch(3);
   RT_CHECK_LAUNCH();
   // Morton order of all faces; its last pass also writes each position's mesh (the key of the next sort)
   rt_status s = radix_sort_pairs(B.codes, B.idx, N, 0, 32, 0, sort_scratch, sort_bytes, st, nullptr, B.err, B.counts, B.foff, M,

@@ -442,10 +442,10 @@ __device__ __forceinline__ void wide_test(const float4* __restrict__ wn, const f
   wide_test_regs(w, oi, ix, iy, iz, tbest, skip, t, r);
 }
 
-// The four slots of a cluster record against a ray: entry distance of each slot the ray enters within reach
-// (+inf otherwise), nearest first, with the slot references alongside.
-__device__ __forceinline__ void cluster_test(const float4* __restrict__ rec, const float4& oi, float ix, float iy, float iz,
-                                             float tbest, float (&t)[4], uint32_t (&r)[4]) {
+// The four slots of a cluster record against a ray, in slot order: entry distance of each slot the ray enters
+// within reach (+inf otherwise) and the slot references.
+__device__ __forceinline__ void cluster_slots(const float4* __restrict__ rec, const float4& oi, float ix, float iy, float iz,
+                                              float tbest, float (&t)[4], uint32_t (&r)[4]) {
   float4 w0, w1, w2, w3, w4, w5;
   ldg8(rec, w0, w1);
   ldg8(rec + 2, w2, w3);
@@ -461,6 +461,11 @@ __device__ __forceinline__ void cluster_test(const float4* __restrict__ rec, con
     t[s] = (tn <= tf && tf >= 0.0f && tn <= tbest * kCullSlack) ? tn : INFINITY;
     r[s] = u4c(wr, s);
   }
+}
+// The same, nearest first (5-comparator network).
+__device__ __forceinline__ void cluster_test(const float4* __restrict__ rec, const float4& oi, float ix, float iy, float iz,
+                                             float tbest, float (&t)[4], uint32_t (&r)[4]) {
+  cluster_slots(rec, oi, ix, iy, iz, tbest, t, r);
   cswap_tr(t, r, 0, 1);
   cswap_tr(t, r, 2, 3);
   cswap_tr(t, r, 0, 2);

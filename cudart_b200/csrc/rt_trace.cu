@@ -919,6 +919,131 @@ __device__ __forceinline__ void trace_warp_coop_clusters(const uint32_t r, const
   }
 }
 
+// A float as an unsigned key of the same order (for warp minimum reductions).
+__device__ __forceinline__ uint32_t order_key(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+// Compare-exchange of packet slots on a warp-uniform key, the lane's own entry distance and the reference riding along.
+__device__ __forceinline__ void cswap_packet(uint32_t (&key)[4], float (&t)[4], uint32_t (&r)[4], int a, int b) {
+  if (key[b] < key[a]) {
+    const uint32_t kk = key[a]; key[a] = key[b]; key[b] = kk;
+    const float tt = t[a]; t[a] = t[b]; t[b] = tt;
+    const uint32_t rr = r[a]; r[a] = r[b]; r[b] = rr;
+  }
+}
+
+// Packet walk of the cluster tree: the 32 lanes of a warp trace rays of one
+// mesh along one node sequence. Every lane tests the same record (one load,
+// shared by the warp) against its own ray; a slot is entered when some lane's
+// ray enters it within that lane's reach, slots in order of the warp's
+// smallest entry distance, and a stacked slot is skipped once no lane can
+// still find a closer hit in it (each lane keeps its own entry distances).
+// At a cluster every lane tests the cluster's triangles. Lanes whose ray is
+// idle (no ray, or tmax <= 0) ride along without tests. For coherent rays
+// (pixel tiles) the warp stays converged where per-lane walks diverge.
+template <bool kCount>
+__device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, const bool valid, const TraceArgs& A, const ClusterArgs& C) {
+  float4 o = make_float4(0.f, 0.f, 0.f, 0.f), d = make_float4(0.f, 0.f, 1.f, 0.f);
+  float tmax0 = -1.0f;
+  if (valid) {
+    tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
+    if (tmax0 > 0.0f) {
+      o = ldg4(A.orig + r);
+      d = ldg4(A.dir + r);
+    }
+  }
+  const bool live = valid && tmax0 > 0.0f;
+  int32_t best = -1;
+  float bt = tmax0, bu = 0.0f, bv = 0.0f;
+  uint32_t visits = 0, tests = 0;
+  uint32_t ref = 0;
+  const bool ok = cluster_tree_ok(C, ref);  // the same header for every lane
+  if (!ok) {
+    if (live && A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+  } else if (__any_sync(0xffffffffu, live)) {
+    const float ix = 1.0f / fix_dir(d.x), iy = 1.0f / fix_dir(d.y), iz = 1.0f / fix_dir(d.z);
+    const float4 oi = scaled_origin(o, ix, iy, iz);
+    const float zu = o.w * 0.0f, zv = d.w * 0.0f;
+    const float4* tris = A.tris + 3 * (size_t)C.F;
+    const float4* recs = C.crec + 8 * (size_t)C.F;
+    uint32_t st_ref[kStack];
+    float st_t[kStack];
+    int sp = 0;
+    const uint32_t kMiss = order_key(INFINITY);
+    for (;;) {
+      if (!cluster_ref_ok(ref, C.n)) {
+        if (live && A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+        break;
+      }
+      bool next = false;
+      if (!(ref & kClusterLeaf)) {
+        float t[4];
+        uint32_t k[4], key[4];
+        cluster_slots(recs + 8 * (size_t)ref, oi, ix, iy, iz, bt, t, k);
+        if (kCount && live) visits += 4;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (!live) t[q] = INFINITY;
+          key[q] = __reduce_min_sync(0xffffffffu, order_key(t[q]));
+        }
+        cswap_packet(key, t, k, 0, 1);
+        cswap_packet(key, t, k, 2, 3);
+        cswap_packet(key, t, k, 0, 2);
+        cswap_packet(key, t, k, 1, 3);
+        cswap_packet(key, t, k, 1, 2);
+        if (key[0] != kMiss) {
+#pragma unroll
+          for (int q = 3; q >= 1; --q) {
+            if (key[q] != kMiss) {
+              if (sp < kStack) {
+                st_ref[sp] = k[q];
+                st_t[sp] = t[q];
+                ++sp;
+              } else if (live && A.err) {
+                atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
+              }
+            }
+          }
+          ref = k[0];
+          next = true;
+        }
+      } else if (live) {
+        const uint32_t p0 = ref & kClusterFirstMask, p1 = p0 + ((ref >> 28) & 7u) + 1u;
+        for (uint32_t pos = p0; pos < p1; ++pos) {
+          const float4 v0 = ldg4(tris + 3 * (size_t)pos);
+          const float4 e1 = ldg4(tris + 3 * (size_t)pos + 1);
+          const float4 e2 = ldg4(tris + 3 * (size_t)pos + 2);
+          if (kCount) ++tests;
+          float th, u, v;
+          if (!mt_test(o, d, zu, zv, v0, e1, e2, th, u, v)) continue;
+          if (th < bt || (best >= 0 && th == bt && (int32_t)pos < best)) {
+            best = (int32_t)pos; bt = th; bu = u; bv = v;
+          }
+        }
+      }
+      if (next) continue;
+      // the nearest stacked slot some lane can still use
+      bool more = false;
+      while (sp > 0) {
+        --sp;
+        if (__any_sync(0xffffffffu, live && st_t[sp] <= bt * kCullSlack)) {
+          ref = st_ref[sp];
+          more = true;
+          break;
+        }
+      }
+      if (!more) break;
+    }
+  }
+  if (!valid) return;
+  write_hit(r, A, C.F, best, bt, bu, bv, tmax0);
+  if (kCount) {
+    if (A.visits) A.visits[r] = visits;
+    if (A.tests) A.tests[r] = tests;
+  }
+}
+
 // Slot -> ray. With an image width, slots walk 8x4 pixel tiles of the
 // row-major image (a warp traces one tile); otherwise slots are ray indices.
 struct SlotMap {
@@ -1135,6 +1260,22 @@ __global__ __launch_bounds__(128) void k_trace_clusters_coop(TraceArgs A, Cluste
   }
 }
 
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_trace_clusters_packet(TraceArgs A, ClusterArgs C, SlotMap M, uint32_t* counter) {
+  const uint32_t lane = lane_id();
+  C.F = 0;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= M.slots) break;
+    uint32_t r = 0;
+    const uint32_t s = base + lane;
+    const bool valid = s < M.slots && M.ray_of(s, r);
+    trace_warp_packet_clusters<kCount>(r, valid, A, C);
+  }
+}
+
 __device__ __forceinline__ void batch_cluster_args(uint32_t r, const BatchTraceArgs& B, ClusterArgs& C) {
   const uint32_t m = find_seg(B.roff, B.M, r);
   const uint32_t F = __ldg(B.foff + m);
@@ -1170,6 +1311,38 @@ __global__ __launch_bounds__(128) void k_batch_trace_clusters_persistent(TraceAr
     }
   }
 }
+// Packet walks over batched rays: a warp whose valid rays all belong to one mesh walks it as a packet; a warp
+// spanning meshes falls back to per-lane walks.
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_batch_trace_clusters_packet(TraceArgs A, BatchTraceArgs B, uint32_t* counter) {
+  const uint32_t lane = lane_id();
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= A.ray_count) break;
+    const uint32_t slot = base + lane;
+    const bool valid = slot < A.ray_count;
+    const uint32_t r = valid ? B.ray_of(slot) : 0u;
+    ClusterArgs C;
+    C.crec = B.acc.crec;
+    C.hdr = B.acc.hdr;
+    if (valid) batch_cluster_args(r, B, C);
+    // lane 0 always holds a valid slot (base < ray_count); its mesh is the packet's
+    const uint32_t F0 = __shfl_sync(0xffffffffu, C.F, 0);
+    if (__all_sync(0xffffffffu, !valid || C.F == F0)) {
+      ClusterArgs P;
+      P.crec = B.acc.crec;
+      P.hdr = (const uint32_t*)__shfl_sync(0xffffffffu, (unsigned long long)C.hdr, 0);
+      P.F = F0;
+      P.n = __shfl_sync(0xffffffffu, C.n, 0);
+      trace_warp_packet_clusters<kCount>(r, valid, A, P);
+    } else if (valid) {
+      trace_ray_clusters<kCount, false>(r, A, C);
+    }
+  }
+}
+
 template <bool kCount>
 __global__ __launch_bounds__(128) void k_batch_trace_clusters_coop(TraceArgs A, BatchTraceArgs B, uint32_t* counter) {
   __shared__ unsigned long long s_key[kCoopWarps][32];
@@ -1444,7 +1617,10 @@ rt_status launch_clusters(const rt_trace_desc* d, const TraceArgs& A, cudaStream
     if (cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
     const uint32_t blocks = (uint32_t)hmin<uint64_t>((uint64_t)sms() * (d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u),
                                                      ((uint64_t)M.slots + 127) / 128);
-    if (d->schedule & RT_TRACE_COOP) {
+    if (d->schedule & RT_TRACE_PACKET) {
+      if (count) k_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
+      else k_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
+    } else if (d->schedule & RT_TRACE_COOP) {
       if (count) k_trace_clusters_coop<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
       else k_trace_clusters_coop<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
     } else {
@@ -1739,7 +1915,10 @@ rt_status batch_launch_clusters(const rt_batch_trace_desc* d, const TraceArgs& A
     if (cudaMemsetAsync(d->work_counter, 0, 4, st) != cudaSuccess) return RT_ERR_CUDA;
     const uint32_t per_sm = d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u;
     const uint32_t blocks = (uint32_t)hmin<uint64_t>((uint64_t)sms() * per_sm, ((uint64_t)d->ray_count + 127) / 128);
-    if (d->schedule & RT_TRACE_COOP) {
+    if (d->schedule & RT_TRACE_PACKET) {
+      if (count) k_batch_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
+      else k_batch_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
+    } else if (d->schedule & RT_TRACE_COOP) {
       if (count) k_batch_trace_clusters_coop<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
       else k_batch_trace_clusters_coop<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
     } else {

@@ -297,7 +297,9 @@ typedef struct rt_trace_desc {
 #define RT_TRACE_COOP 0x2u        /* the warp's lanes share the triangle tests of all its rays' leaves */
 #define RT_TRACE_WIDE 0x4u /* descend through the blob's 4-wide records */
 #define RT_TRACE_CLUSTERS 0x8u /* walk the blob's cluster tree (built with RT_ACCEL_CLUSTERS; else every ray reports a miss
-                                  and RT_DEVERR_ACCEL_MISSING is raised); WHILE_WHILE and WIDE are ignored */
+                                  and RT_DEVERR_ACCEL_MISSING is raised); WIDE is ignored */
+#define RT_TRACE_PACKET 0x10u  /* with RT_TRACE_CLUSTERS and a work_counter: each warp walks the cluster tree as one packet
+                                  (one node sequence for its 32 rays; for coherent rays such as 8 x 4 pixel tiles) */
 
 /* A tracing order for incoherent rays: ray indices sorted by direction octant,
  * then by the Morton code of the origin inside box (min xyz, max xyz, HOST);

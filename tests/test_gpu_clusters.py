@@ -21,6 +21,8 @@ CLUSTER_SCHEDULES = [
     dict(clusters=True, persistent=True, blocks_per_sm=8, while_while=True, sorted=True),
     dict(clusters=True, persistent=True, blocks_per_sm=16, coop=True),       # warp-cooperative cluster tests
     dict(clusters=True, persistent=True, blocks_per_sm=16, coop=True, sorted=True),
+    dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True),     # warp packets
+    dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, sorted=True),
 ]
 
 
@@ -138,7 +140,8 @@ def test_cluster_walks_camera_tmax_degenerate_and_ids(T, oracle):
     bo, bd, bt = core.bounce_rays(tree.tris, o, d, base["id"], base["t"], 77)
     eb = _expect(oracle, ref, bo, bd, bt)
     for sch in CLUSTER_SCHEDULES + [dict(clusters=True, image_width=cam.width), dict(clusters=True, persistent=True, image_width=cam.width,
-                                                                                     coop=True)]:
+                                                                                     coop=True),
+                                    dict(clusters=True, persistent=True, image_width=cam.width, packet=True)]:
         _same(T, core.trace(tree, o, dd, tmax=tm, schedule=sch), e)
         _same(T, core.trace(tree, o, d, id_mode=1, schedule=sch), e1)
         _same(T, core.trace(tree, bo, bd, tmax=bt, schedule=sch), eb)
@@ -216,7 +219,9 @@ def test_batched_cluster_walks_match_single_mesh(T, oracle):
                  dict(clusters=True, persistent=True, blocks_per_sm=8, while_while=True, sorted_bits=12),
                  dict(clusters=True, persistent=True, blocks_per_sm=16, coop=True),
                  dict(clusters=True, persistent=True, blocks_per_sm=16, coop=True, sorted_bits=12),
-                 dict(clusters=True, persistent=True, blocks_per_sm=8, sorted_bits=0)]
+                 dict(clusters=True, persistent=True, blocks_per_sm=8, sorted_bits=0),
+                 dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True),  # warps spanning meshes: per-lane walks
+                 dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, sorted_bits=21)]
     for sch in schedules:
         h = core.batch_trace(bt, O, D, roff, schedule=sch)
         T.cuda.synchronize()

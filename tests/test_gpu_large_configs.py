@@ -3,7 +3,8 @@ workloads (the 4,022,242-triangle learned scene, the 1024-mesh batch, the
 64-instance frame) set beside the CPU oracle, which is pinned to the
 reference's own code. Builds are compared whole; hits on every 16th ray (c3),
 on up to 4096 rays of each of 32 meshes spread over the size range (c2) and on
-all rays of two instances (c4), bit for bit (tolerance: exact)."""
+all rays of two instances (c4, through the cluster trees and the node records), bit for bit (tolerance:
+exact)."""
 import numpy as np
 import pytest
 import torch
@@ -15,6 +16,9 @@ pytestmark = pytest.mark.gpu
 # the schedules the autotuner picks on these workloads (results never depend on the schedule)
 C3_SCHEDULE = dict(image_width=0, persistent=True, blocks_per_sm=8, while_while=True, sorted=True, coop=True, wide=True)
 BATCH_SCHEDULE = dict(while_while=True, wide=True, persistent=True, blocks_per_sm=8, coop=True)
+# the instanced frame's picks on the cluster trees (primary: 8 x 4 pixel tiles; bounce: rays ordered by mesh, octant, Morton)
+C4_PRIMARY = dict(clusters=True, persistent=True, blocks_per_sm=8, tiles=[64, 960, 540])
+C4_BOUNCE = dict(clusters=True, persistent=True, blocks_per_sm=16, sorted_bits=12)
 
 
 def _u32(a):
@@ -109,10 +113,15 @@ def test_c4_instances_of_one_frame(oracle):
     assert w.face_count == 16097152 and w.ray_count == 33177600
     w.displace(1)
     w.build()
-    w.schedule = BATCH_SCHEDULE
+    w.schedule_primary, w.schedule_bounce = C4_PRIMARY, C4_BOUNCE
     plain = w.trace_plain()
+    w.schedule = BATCH_SCHEDULE  # the node-record walk: the same bits for every ray
+    rec = w.trace_plain()
     torch.cuda.synchronize()
     assert int(plain["h1"]["err"].item()) == 0 and int(plain["h2"]["err"].item()) == 0
+    for k in ("h1", "h2"):
+        assert int(rec[k]["err"].item()) == 0
+        assert torch.equal(rec[k]["id"], plain[k]["id"]) and torch.equal(rec[k]["t"], plain[k]["t"]) and torch.equal(rec[k]["uv"], plain[k]["uv"])
     info = _h(w.tree.info)
     assert np.all(info[:, 7] == 0)
     N, V, R = w.face_offsets[1], w.vertex_offsets[1], w.rays_per_instance
@@ -195,7 +204,7 @@ def test_batch_ray_orders_and_schedules_identical():
         if bits == 0:  # stable: equal keys keep their index order
             same = np.diff(key) == 0
             assert np.all(np.diff(order[:n_act])[same] > 0)
-    for sch in tune.batch_candidates(images=(w.count, W, H)):
+    for sch in tune.batch_candidates(images=(w.count, W, H)) + tune.cluster_batch_candidates(images=(w.count, W, H)):
         a = core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, schedule=sch)
         c = core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], schedule=sch)
         torch.cuda.synchronize()
@@ -222,8 +231,8 @@ def test_bounce_order_is_active_first_and_traces_the_same():
     n_act = int((tm > 0).sum())
     assert 0 < n_act < R
     assert (tm[order[:n_act]] > 0).all() and not (tm[order[n_act:]] > 0).any()
-    for coop in (False, True):
-        sch = dict(while_while=True, wide=True, persistent=True, blocks_per_sm=8, coop=coop)
+    for sch in [dict(while_while=True, wide=True, persistent=True, blocks_per_sm=8, coop=coop) for coop in (False, True)] + \
+            [dict(clusters=True, persistent=True, blocks_per_sm=8, coop=coop) for coop in (False, True)]:
         h = core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], schedule=sch, order=b[3])
         torch.cuda.synchronize()
         assert torch.equal(h["id"], base["id"]) and torch.equal(h["t"], base["t"]) and torch.equal(h["uv"], base["uv"])
