@@ -939,11 +939,15 @@ __device__ __forceinline__ void cswap_packet(uint32_t (&key)[4], float (&t)[4], 
 // ray enters it within that lane's reach, slots in order of the warp's
 // smallest entry distance, and a stacked slot is skipped once no lane can
 // still find a closer hit in it (each lane keeps its own entry distances).
-// At a cluster every lane tests the cluster's triangles. Lanes whose ray is
-// idle (no ray, or tmax <= 0) ride along without tests. For coherent rays
-// (pixel tiles) the warp stays converged where per-lane walks diverge.
+// At a cluster the lanes whose ray enters it test its triangles. Lanes whose
+// ray is idle (no ray, or tmax <= 0) ride along without tests. For coherent
+// rays (pixel tiles) the warp stays converged where per-lane walks diverge.
+// min_lanes > 0: once fewer lanes than that want the node the packet is at,
+// the warp leaves the packet walk and every lane walks on alone from its own
+// copy of the stack (which already holds its own entry distances).
 template <bool kCount>
-__device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, const bool valid, const TraceArgs& A, const ClusterArgs& C) {
+__device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, const bool valid, const TraceArgs& A, const ClusterArgs& C,
+                                                           const uint32_t min_lanes) {
   float4 o = make_float4(0.f, 0.f, 0.f, 0.f), d = make_float4(0.f, 0.f, 1.f, 0.f);
   float tmax0 = -1.0f;
   if (valid) {
@@ -971,9 +975,40 @@ __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, con
     float st_t[kStack];
     int sp = 0;
     const uint32_t kMiss = order_key(INFINITY);
+    float cur_t = live ? 0.0f : INFINITY;  // this lane's entry distance of the node at hand
+    auto push = [&](uint32_t sref, float st) {
+      if (sp < kStack) {
+        st_ref[sp] = sref;
+        st_t[sp] = st;
+        ++sp;
+      } else if (A.err) {
+        atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
+      }
+    };
+    auto test_cluster = [&]() {
+      const uint32_t p0 = ref & kClusterFirstMask, p1 = p0 + ((ref >> 28) & 7u) + 1u;
+      for (uint32_t pos = p0; pos < p1; ++pos) {
+        const float4 v0 = ldg4(tris + 3 * (size_t)pos);
+        const float4 e1 = ldg4(tris + 3 * (size_t)pos + 1);
+        const float4 e2 = ldg4(tris + 3 * (size_t)pos + 2);
+        if (kCount) ++tests;
+        float th, u, v;
+        if (!mt_test(o, d, zu, zv, v0, e1, e2, th, u, v)) continue;
+        if (th < bt || (best >= 0 && th == bt && (int32_t)pos < best)) {
+          best = (int32_t)pos; bt = th; bu = u; bv = v;
+        }
+      }
+    };
+    bool alone = false;  // this warp left the packet walk
     for (;;) {
       if (!cluster_ref_ok(ref, C.n)) {
         if (live && A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+        break;
+      }
+      const bool want = live && cur_t <= bt * kCullSlack;
+      if (min_lanes && (uint32_t)__popc(__ballot_sync(0xffffffffu, want)) < min_lanes) {
+        if (want) push(ref, cur_t);
+        alone = true;
         break;
       }
       bool next = false;
@@ -981,10 +1016,10 @@ __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, con
         float t[4];
         uint32_t k[4], key[4];
         cluster_slots(recs + 8 * (size_t)ref, oi, ix, iy, iz, bt, t, k);
-        if (kCount && live) visits += 4;
+        if (kCount && want) visits += 4;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          if (!live) t[q] = INFINITY;
+          if (!want) t[q] = INFINITY;
           key[q] = __reduce_min_sync(0xffffffffu, order_key(t[q]));
         }
         cswap_packet(key, t, k, 0, 1);
@@ -994,33 +1029,14 @@ __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, con
         cswap_packet(key, t, k, 1, 2);
         if (key[0] != kMiss) {
 #pragma unroll
-          for (int q = 3; q >= 1; --q) {
-            if (key[q] != kMiss) {
-              if (sp < kStack) {
-                st_ref[sp] = k[q];
-                st_t[sp] = t[q];
-                ++sp;
-              } else if (live && A.err) {
-                atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
-              }
-            }
-          }
+          for (int q = 3; q >= 1; --q)
+            if (key[q] != kMiss) push(k[q], t[q]);
           ref = k[0];
+          cur_t = t[0];
           next = true;
         }
-      } else if (live) {
-        const uint32_t p0 = ref & kClusterFirstMask, p1 = p0 + ((ref >> 28) & 7u) + 1u;
-        for (uint32_t pos = p0; pos < p1; ++pos) {
-          const float4 v0 = ldg4(tris + 3 * (size_t)pos);
-          const float4 e1 = ldg4(tris + 3 * (size_t)pos + 1);
-          const float4 e2 = ldg4(tris + 3 * (size_t)pos + 2);
-          if (kCount) ++tests;
-          float th, u, v;
-          if (!mt_test(o, d, zu, zv, v0, e1, e2, th, u, v)) continue;
-          if (th < bt || (best >= 0 && th == bt && (int32_t)pos < best)) {
-            best = (int32_t)pos; bt = th; bu = u; bv = v;
-          }
-        }
+      } else if (want) {
+        test_cluster();
       }
       if (next) continue;
       // the nearest stacked slot some lane can still use
@@ -1029,11 +1045,37 @@ __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, con
         --sp;
         if (__any_sync(0xffffffffu, live && st_t[sp] <= bt * kCullSlack)) {
           ref = st_ref[sp];
+          cur_t = st_t[sp];
           more = true;
           break;
         }
       }
       if (!more) break;
+    }
+    if (alone && live) {  // every lane on its own, from its stack
+      bool walking = pop_within(st_ref, st_t, sp, bt, ref);
+      while (walking) {
+        if (!cluster_ref_ok(ref, C.n)) {
+          if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+          break;
+        }
+        if (!(ref & kClusterLeaf)) {
+          float t[4];
+          uint32_t k[4];
+          cluster_test(recs + 8 * (size_t)ref, oi, ix, iy, iz, bt, t, k);
+          if (kCount) visits += 4;
+          if (t[0] != INFINITY) {
+#pragma unroll
+            for (int q = 3; q >= 1; --q)
+              if (t[q] != INFINITY) push(k[q], t[q]);
+            ref = k[0];
+            continue;
+          }
+        } else {
+          test_cluster();
+        }
+        walking = pop_within(st_ref, st_t, sp, bt, ref);
+      }
     }
   }
   if (!valid) return;
@@ -1261,7 +1303,8 @@ __global__ __launch_bounds__(128) void k_trace_clusters_coop(TraceArgs A, Cluste
 }
 
 template <bool kCount>
-__global__ __launch_bounds__(128) void k_trace_clusters_packet(TraceArgs A, ClusterArgs C, SlotMap M, uint32_t* counter) {
+__global__ __launch_bounds__(128) void k_trace_clusters_packet(TraceArgs A, ClusterArgs C, SlotMap M, uint32_t* counter,
+                                                                uint32_t min_lanes) {
   const uint32_t lane = lane_id();
   C.F = 0;
   for (;;) {
@@ -1272,7 +1315,7 @@ __global__ __launch_bounds__(128) void k_trace_clusters_packet(TraceArgs A, Clus
     uint32_t r = 0;
     const uint32_t s = base + lane;
     const bool valid = s < M.slots && M.ray_of(s, r);
-    trace_warp_packet_clusters<kCount>(r, valid, A, C);
+    trace_warp_packet_clusters<kCount>(r, valid, A, C, min_lanes);
   }
 }
 
@@ -1314,7 +1357,8 @@ __global__ __launch_bounds__(128) void k_batch_trace_clusters_persistent(TraceAr
 // Packet walks over batched rays: a warp whose valid rays all belong to one mesh walks it as a packet; a warp
 // spanning meshes falls back to per-lane walks.
 template <bool kCount>
-__global__ __launch_bounds__(128) void k_batch_trace_clusters_packet(TraceArgs A, BatchTraceArgs B, uint32_t* counter) {
+__global__ __launch_bounds__(128) void k_batch_trace_clusters_packet(TraceArgs A, BatchTraceArgs B, uint32_t* counter,
+                                                                      uint32_t min_lanes) {
   const uint32_t lane = lane_id();
   for (;;) {
     uint32_t base = 0;
@@ -1336,7 +1380,7 @@ __global__ __launch_bounds__(128) void k_batch_trace_clusters_packet(TraceArgs A
       P.hdr = (const uint32_t*)__shfl_sync(0xffffffffu, (unsigned long long)C.hdr, 0);
       P.F = F0;
       P.n = __shfl_sync(0xffffffffu, C.n, 0);
-      trace_warp_packet_clusters<kCount>(r, valid, A, P);
+      trace_warp_packet_clusters<kCount>(r, valid, A, P, min_lanes);
     } else if (valid) {
       trace_ray_clusters<kCount, false>(r, A, C);
     }
@@ -1618,8 +1662,8 @@ rt_status launch_clusters(const rt_trace_desc* d, const TraceArgs& A, cudaStream
     const uint32_t blocks = (uint32_t)hmin<uint64_t>((uint64_t)sms() * (d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u),
                                                      ((uint64_t)M.slots + 127) / 128);
     if (d->schedule & RT_TRACE_PACKET) {
-      if (count) k_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
-      else k_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
+      if (count) k_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->packet_min_lanes);
+      else k_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->packet_min_lanes);
     } else if (d->schedule & RT_TRACE_COOP) {
       if (count) k_trace_clusters_coop<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
       else k_trace_clusters_coop<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
@@ -1916,8 +1960,8 @@ rt_status batch_launch_clusters(const rt_batch_trace_desc* d, const TraceArgs& A
     const uint32_t per_sm = d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u;
     const uint32_t blocks = (uint32_t)hmin<uint64_t>((uint64_t)sms() * per_sm, ((uint64_t)d->ray_count + 127) / 128);
     if (d->schedule & RT_TRACE_PACKET) {
-      if (count) k_batch_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
-      else k_batch_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
+      if (count) k_batch_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->packet_min_lanes);
+      else k_batch_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->packet_min_lanes);
     } else if (d->schedule & RT_TRACE_COOP) {
       if (count) k_batch_trace_clusters_coop<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
       else k_batch_trace_clusters_coop<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter);

@@ -62,11 +62,14 @@ def cluster_candidates(image_width: int):
     for coop, ww in ((False, False), (False, True), (True, False)):
         out.append({"clusters": True, "image_width": 0, "persistent": True, "blocks_per_sm": 16, "coop": coop, "while_while": ww,
                     "sorted": True})
-    # warp packets: pixel tiles of the image, or rays sorted by octant and origin
-    for bps in (8, 16):
-        out.append({"clusters": True, "image_width": 0, "persistent": True, "blocks_per_sm": bps, "packet": True, "sorted": True})
+    # warp packets: pixel tiles of the image, or rays sorted by octant and origin (leaving the packet below
+    # packet_min_lanes lanes)
+    for bps, ml in itertools.product((8, 16), (0, 8, 16)):
+        out.append({"clusters": True, "image_width": 0, "persistent": True, "blocks_per_sm": bps, "packet": True, "packet_min_lanes": ml,
+                    "sorted": True})
         if image_width:
-            out.append({"clusters": True, "image_width": image_width, "persistent": True, "blocks_per_sm": bps, "packet": True})
+            out.append({"clusters": True, "image_width": image_width, "persistent": True, "blocks_per_sm": bps, "packet": True,
+                        "packet_min_lanes": ml})
     return out
 
 
@@ -124,11 +127,16 @@ def cluster_batch_candidates(images=None):
             out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "while_while": ww, "sorted_bits": bits})
         if images is not None and images[1] % 8 == 0 and images[2] % 4 == 0:
             out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "while_while": ww, "tiles": list(images)})
-    # warp packets (one node sequence per warp): pixel tiles, and rays ordered by mesh, octant and origin
+    # warp packets (one node sequence per warp): pixel tiles, and rays ordered by mesh, octant and origin; a warp
+    # leaves the packet for per-lane walks once fewer than packet_min_lanes lanes want its node (0: never)
     for bps in (8, 16):
-        out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "packet": True, "sorted_bits": 21})
+        for ml in (0, 8, 16, 24):
+            out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "packet": True, "packet_min_lanes": ml,
+                        "sorted_bits": 21})
         if images is not None and images[1] % 8 == 0 and images[2] % 4 == 0:
-            out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "packet": True, "tiles": list(images)})
+            for ml in (0, 4, 8):
+                out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "packet": True, "packet_min_lanes": ml,
+                            "tiles": list(images)})
     return out
 
 

@@ -191,6 +191,7 @@ typedef struct rt_batch_trace_desc {
   uint32_t persistent_blocks_per_sm; /* with work_counter: CTAs of 128 threads per SM (0 = 8) */
   const uint32_t* ray_order;      /* optional DEVICE permutation of the rays: threads take rays in this order
                                      (rt_batch_ray_order, rt_image_tile_order); results stay in each ray's own slot */
+  uint32_t packet_min_lanes;      /* as in rt_trace_desc */
 } rt_batch_trace_desc;
 rt_status rt_batch_trace(const rt_batch_trace_desc* desc, rt_stream stream);
 
@@ -291,6 +292,8 @@ typedef struct rt_trace_desc {
   const uint32_t* ray_order; /* optional permutation from rt_ray_order: threads take rays in this order */
   uint32_t treelet_depth;   /* persistent 4-wide walks: levels of 4-wide records below the root (0..4, at most 85
                                records, 10.9 KB) that each CTA copies to shared memory and reads from there (0: none) */
+  uint32_t packet_min_lanes; /* RT_TRACE_PACKET: a warp leaves the packet walk for per-lane walks (from the same stacks)
+                                once fewer than this many lanes still want the node it is at (0: never) */
 } rt_trace_desc;
 
 #define RT_TRACE_WHILE_WHILE 0x1u /* descend until a leaf is held, then test it (else: interleaved) */
