@@ -218,6 +218,11 @@ class ClockSampler:
 # ----------------------------------------------------------------------------
 def batch_kernel(sched):
     base = "k_batch_trace_clusters" if sched.get("clusters") else "k_batch_trace"
+    if sched.get("clusters") and sched.get("persistent"):
+        if sched.get("packet"):
+            return base + "_packet"
+        if sched.get("refill"):
+            return base + "_refill"
     if sched.get("coop"):
         return base + "_coop"
     return base + "_persistent" if sched.get("persistent") else base

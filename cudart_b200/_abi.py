@@ -27,6 +27,7 @@ TRACE_COOP = 0x2
 TRACE_WIDE = 0x4
 TRACE_CLUSTERS = 0x8
 TRACE_PACKET = 0x10
+TRACE_REFILL = 0x20
 ACCEL_CLUSTERS = 0x2
 
 # every symbol include/rt_core.h declares
@@ -81,7 +82,7 @@ class TraceDesc(C.Structure):
                 ("tmax", _P), ("ray_count", _U32), ("id_mode", _U32), ("hit_id", _P), ("hit_t", _P), ("hit_uv", _P),
                 ("ray_visits", _P), ("ray_tests", _P), ("error_word", _P), ("accel", _P), ("face_count_hint", _U32),
                 ("image_width", _U32), ("work_counter", _P), ("persistent_blocks_per_sm", _U32), ("schedule", _U32),
-                ("ray_order", _P), ("treelet_depth", _U32), ("packet_min_lanes", _U32)]
+                ("ray_order", _P), ("treelet_depth", _U32), ("lane_threshold", _U32)]
 
 
 class InterpDesc(C.Structure):
@@ -112,7 +113,7 @@ class BatchTraceDesc(C.Structure):
                 ("face_count", _U32), ("orig", _P), ("dir", _P), ("tmax", _P), ("ray_count", _U32), ("id_mode", _U32),
                 ("hit_id", _P), ("hit_t", _P), ("hit_uv", _P), ("ray_visits", _P), ("ray_tests", _P), ("error_word", _P),
                 ("schedule", _U32), ("work_counter", _P), ("persistent_blocks_per_sm", _U32), ("ray_order", _P),
-                ("packet_min_lanes", _U32)]
+                ("lane_threshold", _U32)]
 
 
 class SahDesc(C.Structure):

@@ -319,10 +319,10 @@ def trace_desc(tree: Tree, orig, dir, tmax=None, id_mode: int = 0, counters: boo
             d.work_counter = _work_counter(dev, stream).data_ptr()
             d.persistent_blocks_per_sm = int(sch.get("blocks_per_sm", 8))
             d.treelet_depth = int(sch.get("treelet", 0))  # top levels staged in shared memory (4-wide walks)
-            d.packet_min_lanes = int(sch.get("packet_min_lanes", 0))  # packet walks: fall back to per-lane walks
+            d.lane_threshold = int(sch.get("lane_threshold", 0))  # packet walks: fall back to per-lane walks
         d.schedule = ((_abi.TRACE_WHILE_WHILE if sch.get("while_while", False) else 0) | (_abi.TRACE_COOP if sch.get("coop", False) else 0)
                       | (_abi.TRACE_WIDE if sch.get("wide", False) else 0) | (_abi.TRACE_CLUSTERS if sch.get("clusters", False) else 0)
-                      | (_abi.TRACE_PACKET if sch.get("packet", False) else 0))
+                      | (_abi.TRACE_PACKET if sch.get("packet", False) else 0) | (_abi.TRACE_REFILL if sch.get("refill", False) else 0))
         if sch.get("sorted", False):
             order = ray_order(orig, dir, tmax, tree_box(tree), ray_count=R, stream=stream)
             out["_order"] = order  # keep it alive until the trace has run
@@ -690,7 +690,8 @@ def batch_trace_desc(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax
                   | (_abi.TRACE_WIDE if sch.get("wide", False) else 0)
                   | (_abi.TRACE_COOP if sch.get("coop", False) else 0)
                   | (_abi.TRACE_CLUSTERS if sch.get("clusters", False) else 0)
-                  | (_abi.TRACE_PACKET if sch.get("packet", False) else 0))
+                  | (_abi.TRACE_PACKET if sch.get("packet", False) else 0)
+                  | (_abi.TRACE_REFILL if sch.get("refill", False) else 0))
     if order is not None:
         d.ray_order = order.data_ptr()
     elif sch.get("tiles"):  # every mesh's rays are a row-major image of the same size: 8 x 4 pixel tiles per warp
@@ -708,5 +709,5 @@ def batch_trace_desc(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax
             out["_counter"] = torch.zeros(1, dtype=torch.int32, device=dev)
         d.work_counter = out["_counter"].data_ptr()
         d.persistent_blocks_per_sm = int(sch.get("blocks_per_sm", 8))
-    d.packet_min_lanes = int(sch.get("packet_min_lanes", 0))
+    d.lane_threshold = int(sch.get("lane_threshold", 0))
     return d, out

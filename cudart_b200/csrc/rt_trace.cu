@@ -710,10 +710,12 @@ __device__ __forceinline__ bool cluster_tree_ok(const ClusterArgs& C, uint32_t& 
   root = __ldg(C.hdr + kHdrClusterRoot);
   return __ldg(C.hdr + kHdrClusterValid) == 1u && __ldg(C.hdr + kHdrClusterN) == C.n && C.n > 0 && root < C.n;
 }
-// A reference inside the mesh: a record index below n, or a cluster whose positions are below n. Anything else
-// (a blob written for other sizes) ends the walk with RT_DEVERR_ACCEL_MISSING instead of reading past the mesh.
-__device__ __forceinline__ bool cluster_ref_ok(uint32_t ref, uint32_t n) {
-  return (ref & kClusterLeaf) ? (ref & kClusterFirstMask) + ((ref >> 28) & 7u) < n : ref < n;
+// A reference inside the mesh (a record index below n, or a cluster whose positions are below n), reached
+// within the walk's step bound: a walk of a well-formed tree enters every record and every cluster at most once,
+// 2n steps in all. Anything else (a blob written for other sizes, or damaged) ends the walk with
+// RT_DEVERR_ACCEL_MISSING instead of reading past the mesh or looping.
+__device__ __forceinline__ bool cluster_ref_ok(uint32_t ref, uint32_t n, uint32_t& steps) {
+  return ++steps <= 2 * n + 2 && ((ref & kClusterLeaf) ? (ref & kClusterFirstMask) + ((ref >> 28) & 7u) < n : ref < n);
 }
 
 // Pops the nearest stacked reference that can still hold a closer hit.
@@ -753,6 +755,7 @@ __device__ __forceinline__ void trace_ray_clusters(const uint32_t r, const Trace
     uint32_t st_ref[kStack];
     float st_t[kStack];
     int sp = 0;
+    uint32_t steps = 0;
     // one record step: false when the walk is over (nothing hit and nothing stacked within reach)
     auto record_step = [&]() -> bool {
       float t[4];
@@ -793,14 +796,14 @@ __device__ __forceinline__ void trace_ray_clusters(const uint32_t r, const Trace
     };
     bool alive = true;
     while (alive) {
-      if (!cluster_ref_ok(ref, C.n)) {
+      if (!cluster_ref_ok(ref, C.n, steps)) {
         if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
         break;
       }
       if constexpr (kWW) {
         while (!(ref & kClusterLeaf)) {
           if (!record_step()) { alive = false; break; }
-          if (!cluster_ref_ok(ref, C.n)) {
+          if (!cluster_ref_ok(ref, C.n, steps)) {
             if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
             alive = false;
             break;
@@ -856,12 +859,13 @@ __device__ __forceinline__ void trace_warp_coop_clusters(const uint32_t r, const
   uint32_t st_ref[kStack];
   float st_t[kStack];
   int sp = 0;
+  uint32_t steps = 0;
   bool alive = ok;
   while (__any_sync(0xffffffffu, alive)) {
     // 1. descend until this ray holds a cluster
     uint32_t mask = 0, first = 0, cnt = 0;
     while (alive) {
-      if (!cluster_ref_ok(ref, C.n)) {
+      if (!cluster_ref_ok(ref, C.n, steps)) {
         if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
         alive = false;
         break;
@@ -974,6 +978,7 @@ __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, con
     uint32_t st_ref[kStack];
     float st_t[kStack];
     int sp = 0;
+    uint32_t steps = 0;
     const uint32_t kMiss = order_key(INFINITY);
     float cur_t = live ? 0.0f : INFINITY;  // this lane's entry distance of the node at hand
     auto push = [&](uint32_t sref, float st) {
@@ -1001,7 +1006,7 @@ __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, con
     };
     bool alone = false;  // this warp left the packet walk
     for (;;) {
-      if (!cluster_ref_ok(ref, C.n)) {
+      if (!cluster_ref_ok(ref, C.n, steps)) {
         if (live && A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
         break;
       }
@@ -1055,7 +1060,7 @@ __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, con
     if (alone && live) {  // every lane on its own, from its stack
       bool walking = pop_within(st_ref, st_t, sp, bt, ref);
       while (walking) {
-        if (!cluster_ref_ok(ref, C.n)) {
+        if (!cluster_ref_ok(ref, C.n, steps)) {
           if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
           break;
         }
@@ -1083,6 +1088,116 @@ __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, con
   if (kCount) {
     if (A.visits) A.visits[r] = visits;
     if (A.tests) A.tests[r] = tests;
+  }
+}
+
+// Per-lane cluster walks in warps that refill idle lanes: a lane whose ray is
+// done (or was inactive) waits until `threshold` lanes of its warp are idle,
+// then the warp takes that many new rays with one atomic and every lane steps
+// its own walk again, so a warp no longer waits for its slowest ray. `start`
+// maps a slot to a ray and its mesh: false for a slot without a ray.
+template <bool kCount, class Start>
+__device__ __forceinline__ void refill_walks(const TraceArgs& A, uint32_t* counter, const uint32_t slots, const uint32_t threshold,
+                                             const Start& start) {
+  const uint32_t lane = lane_id();
+  const uint32_t need = threshold ? min(threshold, 32u) : 16u;
+  bool busy = false, exhausted = false;
+  uint32_t r = 0, ref = 0, visits = 0, tests = 0;
+  int32_t best = -1;
+  float4 o = make_float4(0.f, 0.f, 0.f, 0.f), d = o, oi = o;
+  float ix = 0.f, iy = 0.f, iz = 0.f, zu = 0.f, zv = 0.f, tmax0 = 0.f, bt = 0.f, bu = 0.f, bv = 0.f;
+  ClusterArgs C;
+  uint32_t st_ref[kStack];
+  float st_t[kStack];
+  int sp = 0;
+  uint32_t steps = 0;
+  auto finish = [&]() {
+    write_hit(r, A, C.F, best, bt, bu, bv, tmax0);
+    if (kCount) {
+      if (A.visits) A.visits[r] = visits;
+      if (A.tests) A.tests[r] = tests;
+    }
+    busy = false;
+  };
+  for (;;) {
+    const uint32_t idle = __ballot_sync(0xffffffffu, !busy);
+    if (!exhausted && (uint32_t)__popc(idle) >= need) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(counter, (uint32_t)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base + (uint32_t)__popc(idle) >= slots) exhausted = true;
+      const uint32_t slot = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
+      if (!busy && slot < slots && start(slot, r, C)) {
+        tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
+        best = -1;
+        bt = tmax0; bu = bv = 0.0f;
+        visits = tests = 0;
+        if (tmax0 > 0.0f) {
+          if (cluster_tree_ok(C, ref)) {
+            o = ldg4(A.orig + r);
+            d = ldg4(A.dir + r);
+            ix = 1.0f / fix_dir(d.x); iy = 1.0f / fix_dir(d.y); iz = 1.0f / fix_dir(d.z);
+            oi = scaled_origin(o, ix, iy, iz);
+            zu = o.w * 0.0f; zv = d.w * 0.0f;
+            sp = 0;
+            steps = 0;
+            busy = true;
+          } else if (A.err) {
+            atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+          }
+        }
+        if (!busy) finish();  // an inactive ray (or no cluster tree): a miss at once
+      }
+    }
+    if (!__any_sync(0xffffffffu, busy)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (!busy) continue;
+    // one step of this lane's walk
+    if (!cluster_ref_ok(ref, C.n, steps)) {
+      if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+      finish();
+      continue;
+    }
+    const float4* recs = C.crec + 8 * (size_t)C.F;
+    if (!(ref & kClusterLeaf)) {
+      float t[4];
+      uint32_t k[4];
+      cluster_test(recs + 8 * (size_t)ref, oi, ix, iy, iz, bt, t, k);
+      if (kCount) visits += 4;
+      if (t[0] != INFINITY) {
+#pragma unroll
+        for (int q = 3; q >= 1; --q) {
+          if (t[q] != INFINITY) {
+            if (sp < kStack) {
+              st_ref[sp] = k[q];
+              st_t[sp] = t[q];
+              ++sp;
+            } else if (A.err) {
+              atomicOr(A.err, (uint32_t)RT_DEVERR_STACK_OVERFLOW);
+            }
+          }
+        }
+        ref = k[0];
+        continue;
+      }
+    } else {
+      const float4* tris = A.tris + 3 * (size_t)C.F;
+      const uint32_t p0 = ref & kClusterFirstMask, p1 = p0 + ((ref >> 28) & 7u) + 1u;
+      for (uint32_t pos = p0; pos < p1; ++pos) {
+        const float4 v0 = ldg4(tris + 3 * (size_t)pos);
+        const float4 e1 = ldg4(tris + 3 * (size_t)pos + 1);
+        const float4 e2 = ldg4(tris + 3 * (size_t)pos + 2);
+        if (kCount) ++tests;
+        float th, u, v;
+        if (!mt_test(o, d, zu, zv, v0, e1, e2, th, u, v)) continue;
+        if (th < bt || (best >= 0 && th == bt && (int32_t)pos < best)) {
+          best = (int32_t)pos; bt = th; bu = u; bv = v;
+        }
+      }
+    }
+    if (!pop_within(st_ref, st_t, sp, bt, ref)) finish();
   }
 }
 
@@ -1319,6 +1434,16 @@ __global__ __launch_bounds__(128) void k_trace_clusters_packet(TraceArgs A, Clus
   }
 }
 
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_trace_clusters_refill(TraceArgs A, ClusterArgs C, SlotMap M, uint32_t* counter,
+                                                                uint32_t threshold) {
+  C.F = 0;
+  refill_walks<kCount>(A, counter, M.slots, threshold, [&](uint32_t slot, uint32_t& r, ClusterArgs& Cl) {
+    Cl = C;
+    return M.ray_of(slot, r);
+  });
+}
+
 __device__ __forceinline__ void batch_cluster_args(uint32_t r, const BatchTraceArgs& B, ClusterArgs& C) {
   const uint32_t m = find_seg(B.roff, B.M, r);
   const uint32_t F = __ldg(B.foff + m);
@@ -1354,6 +1479,17 @@ __global__ __launch_bounds__(128) void k_batch_trace_clusters_persistent(TraceAr
     }
   }
 }
+template <bool kCount>
+__global__ __launch_bounds__(128) void k_batch_trace_clusters_refill(TraceArgs A, BatchTraceArgs B, uint32_t* counter,
+                                                                      uint32_t threshold) {
+  refill_walks<kCount>(A, counter, A.ray_count, threshold, [&](uint32_t slot, uint32_t& r, ClusterArgs& C) {
+    r = B.ray_of(slot);
+    C.crec = B.acc.crec;
+    batch_cluster_args(r, B, C);
+    return true;
+  });
+}
+
 // Packet walks over batched rays: a warp whose valid rays all belong to one mesh walks it as a packet; a warp
 // spanning meshes falls back to per-lane walks.
 template <bool kCount>
@@ -1662,8 +1798,11 @@ rt_status launch_clusters(const rt_trace_desc* d, const TraceArgs& A, cudaStream
     const uint32_t blocks = (uint32_t)hmin<uint64_t>((uint64_t)sms() * (d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u),
                                                      ((uint64_t)M.slots + 127) / 128);
     if (d->schedule & RT_TRACE_PACKET) {
-      if (count) k_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->packet_min_lanes);
-      else k_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->packet_min_lanes);
+      if (count) k_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->lane_threshold);
+      else k_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->lane_threshold);
+    } else if (d->schedule & RT_TRACE_REFILL) {
+      if (count) k_trace_clusters_refill<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->lane_threshold);
+      else k_trace_clusters_refill<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->lane_threshold);
     } else if (d->schedule & RT_TRACE_COOP) {
       if (count) k_trace_clusters_coop<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
       else k_trace_clusters_coop<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
@@ -1960,8 +2099,11 @@ rt_status batch_launch_clusters(const rt_batch_trace_desc* d, const TraceArgs& A
     const uint32_t per_sm = d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u;
     const uint32_t blocks = (uint32_t)hmin<uint64_t>((uint64_t)sms() * per_sm, ((uint64_t)d->ray_count + 127) / 128);
     if (d->schedule & RT_TRACE_PACKET) {
-      if (count) k_batch_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->packet_min_lanes);
-      else k_batch_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->packet_min_lanes);
+      if (count) k_batch_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold);
+      else k_batch_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold);
+    } else if (d->schedule & RT_TRACE_REFILL) {
+      if (count) k_batch_trace_clusters_refill<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold);
+      else k_batch_trace_clusters_refill<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold);
     } else if (d->schedule & RT_TRACE_COOP) {
       if (count) k_batch_trace_clusters_coop<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
       else k_batch_trace_clusters_coop<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter);

@@ -19,7 +19,7 @@ steady-state launch. Cases (kernel of interest in brackets):
   mlp_grouped    64 grouped networks: 3 training steps of 1024 rays each,        [k_gemm_tc, k_softmax_xent, ...]
                  then proposals for 64 x 518,400 rays
   sort_16m       2^24 random (key, value) pairs, 32-bit keys, sorted twice         [k_onesweep, k_sort_hist]
-  c4_frame [M]   M (default 64) deformed instances of the 1/16-size learned       [launch list, k_batch_trace_coop]
+  c4_frame [M]   M (default 64) deformed instances of the 1/16-size learned       [launch list, k_batch_trace_clusters*]
                  scene, three frames of the plain path: batched build, primary
                  rays, batched trace, bounce rays, batched trace
 """
@@ -176,12 +176,12 @@ def sort_16m():
 
 def c4_frame(count: int = 64):
     """Three frames of the instanced workload's plain path (cluster trees) with the schedules the tuner picks on
-    it: per-lane cluster walks, 8 x 4 pixel tiles for the primaries, the bounces ordered by mesh, octant and
-    12 Morton bits."""
+    it: the primaries as warp packets over 8 x 4 pixel tiles, the bounces as per-lane walks in warps that take
+    new rays once 8 lanes are idle."""
     from .instances import InstancedFrames
     w = InstancedFrames(count, 1 / 16, 960, 540)
-    w.schedule_primary = dict(clusters=True, persistent=True, blocks_per_sm=8, tiles=[count, 960, 540])
-    w.schedule_bounce = dict(clusters=True, persistent=True, blocks_per_sm=16, sorted_bits=12)
+    w.schedule_primary = dict(clusters=True, persistent=True, blocks_per_sm=16, packet=True, tiles=[count, 960, 540])
+    w.schedule_bounce = dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=8)
     plain = None
     for f in range(3):
         w.displace(f)

@@ -62,14 +62,18 @@ def cluster_candidates(image_width: int):
     for coop, ww in ((False, False), (False, True), (True, False)):
         out.append({"clusters": True, "image_width": 0, "persistent": True, "blocks_per_sm": 16, "coop": coop, "while_while": ww,
                     "sorted": True})
+    # per-lane walks in warps that refill their idle lanes
+    for ml, srt in itertools.product((4, 8, 16), (False, True)):
+        out.append({"clusters": True, "image_width": 0, "persistent": True, "blocks_per_sm": 8, "refill": True, "lane_threshold": ml,
+                    "sorted": srt})
     # warp packets: pixel tiles of the image, or rays sorted by octant and origin (leaving the packet below
-    # packet_min_lanes lanes)
+    # lane_threshold lanes)
     for bps, ml in itertools.product((8, 16), (0, 8, 16)):
-        out.append({"clusters": True, "image_width": 0, "persistent": True, "blocks_per_sm": bps, "packet": True, "packet_min_lanes": ml,
+        out.append({"clusters": True, "image_width": 0, "persistent": True, "blocks_per_sm": bps, "packet": True, "lane_threshold": ml,
                     "sorted": True})
         if image_width:
             out.append({"clusters": True, "image_width": image_width, "persistent": True, "blocks_per_sm": bps, "packet": True,
-                        "packet_min_lanes": ml})
+                        "lane_threshold": ml})
     return out
 
 
@@ -127,15 +131,19 @@ def cluster_batch_candidates(images=None):
             out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "while_while": ww, "sorted_bits": bits})
         if images is not None and images[1] % 8 == 0 and images[2] % 4 == 0:
             out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "while_while": ww, "tiles": list(images)})
+    # per-lane walks in warps that refill their idle lanes once lane_threshold of them are idle
+    for ml, bits in itertools.product((2, 4, 8, 16), (None, 12)):
+        c = {"clusters": True, "persistent": True, "blocks_per_sm": 8, "refill": True, "lane_threshold": ml}
+        out.append(c if bits is None else dict(c, sorted_bits=bits))
     # warp packets (one node sequence per warp): pixel tiles, and rays ordered by mesh, octant and origin; a warp
-    # leaves the packet for per-lane walks once fewer than packet_min_lanes lanes want its node (0: never)
+    # leaves the packet for per-lane walks once fewer than lane_threshold lanes want its node (0: never)
     for bps in (8, 16):
         for ml in (0, 8, 16, 24):
-            out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "packet": True, "packet_min_lanes": ml,
+            out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "packet": True, "lane_threshold": ml,
                         "sorted_bits": 21})
         if images is not None and images[1] % 8 == 0 and images[2] % 4 == 0:
             for ml in (0, 4, 8):
-                out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "packet": True, "packet_min_lanes": ml,
+                out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "packet": True, "lane_threshold": ml,
                             "tiles": list(images)})
     return out
 
@@ -184,6 +192,8 @@ def tune_batch_trace(tree, orig, dir, ray_offsets, tmax=None, key: str = "batch"
         if order is not None:
             cands += [{"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "while_while": ww, "given_order": True}
                       for coop, ww, bps in ((True, False, 16), (False, False, 8), (False, True, 8))]
+            cands += [{"clusters": True, "persistent": True, "blocks_per_sm": 8, "refill": True, "lane_threshold": ml, "given_order": True}
+                      for ml in (4, 8)]
     for sch in cands:
         given = order if sch.get("given_order") else None
         core.batch_trace(tree, orig, dir, ray_offsets, tmax=tmax, out=out, schedule=sch, order=given)  # warm

@@ -191,7 +191,7 @@ typedef struct rt_batch_trace_desc {
   uint32_t persistent_blocks_per_sm; /* with work_counter: CTAs of 128 threads per SM (0 = 8) */
   const uint32_t* ray_order;      /* optional DEVICE permutation of the rays: threads take rays in this order
                                      (rt_batch_ray_order, rt_image_tile_order); results stay in each ray's own slot */
-  uint32_t packet_min_lanes;      /* as in rt_trace_desc */
+  uint32_t lane_threshold;        /* as in rt_trace_desc */
 } rt_batch_trace_desc;
 rt_status rt_batch_trace(const rt_batch_trace_desc* desc, rt_stream stream);
 
@@ -292,8 +292,9 @@ typedef struct rt_trace_desc {
   const uint32_t* ray_order; /* optional permutation from rt_ray_order: threads take rays in this order */
   uint32_t treelet_depth;   /* persistent 4-wide walks: levels of 4-wide records below the root (0..4, at most 85
                                records, 10.9 KB) that each CTA copies to shared memory and reads from there (0: none) */
-  uint32_t packet_min_lanes; /* RT_TRACE_PACKET: a warp leaves the packet walk for per-lane walks (from the same stacks)
-                                once fewer than this many lanes still want the node it is at (0: never) */
+  uint32_t lane_threshold;  /* RT_TRACE_PACKET: a warp leaves the packet walk for per-lane walks (from the same stacks)
+                               once fewer than this many lanes still want the node it is at (0: never);
+                               RT_TRACE_REFILL: a warp fetches new rays for its idle lanes once this many are idle */
 } rt_trace_desc;
 
 #define RT_TRACE_WHILE_WHILE 0x1u /* descend until a leaf is held, then test it (else: interleaved) */
@@ -303,6 +304,8 @@ typedef struct rt_trace_desc {
                                   and RT_DEVERR_ACCEL_MISSING is raised); WIDE is ignored */
 #define RT_TRACE_PACKET 0x10u  /* with RT_TRACE_CLUSTERS and a work_counter: each warp walks the cluster tree as one packet
                                   (one node sequence for its 32 rays; for coherent rays such as 8 x 4 pixel tiles) */
+#define RT_TRACE_REFILL 0x20u  /* with RT_TRACE_CLUSTERS and a work_counter: per-lane walks in which a warp takes new rays
+                                  for its idle lanes (lane_threshold of them, 0 = 16) instead of waiting for its slowest ray */
 
 /* A tracing order for incoherent rays: ray indices sorted by direction octant,
  * then by the Morton code of the origin inside box (min xyz, max xyz, HOST);

@@ -23,8 +23,10 @@ CLUSTER_SCHEDULES = [
     dict(clusters=True, persistent=True, blocks_per_sm=16, coop=True, sorted=True),
     dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True),     # warp packets
     dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, sorted=True),
-    dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, packet_min_lanes=16, sorted=True),  # packet, then per lane
-    dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, packet_min_lanes=32),
+    dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, lane_threshold=16, sorted=True),  # packet, then per lane
+    dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, lane_threshold=32),
+    dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=16),  # warps refill idle lanes
+    dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=1, sorted=True),
 ]
 
 
@@ -224,7 +226,9 @@ def test_batched_cluster_walks_match_single_mesh(T, oracle):
                  dict(clusters=True, persistent=True, blocks_per_sm=8, sorted_bits=0),
                  dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True),  # warps spanning meshes: per-lane walks
                  dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, sorted_bits=21),
-                 dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, packet_min_lanes=16, sorted_bits=21)]
+                 dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, lane_threshold=16, sorted_bits=21),
+                 dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=8),
+                 dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=32, sorted_bits=12)]
     for sch in schedules:
         h = core.batch_trace(bt, O, D, roff, schedule=sch)
         T.cuda.synchronize()
