@@ -33,7 +33,7 @@ ACCEL_CLUSTERS = 0x2
 # every symbol include/rt_core.h declares
 EXPORTS = (
     "rt_lbvh_scratch_bytes", "rt_lbvh_accel_bytes", "rt_lbvh_build", "rt_batch_sizes", "rt_batch_build", "rt_batch_trace", "rt_mesh_boxes", "rt_reorder_faces", "rt_sort_scratch_bytes",
-    "rt_radix_sort_pairs", "rt_radix_sort_pairs_static", "rt_radix_sort_keys", "rt_camera_look_at", "rt_camera_basis", "rt_primary_rays",
+    "rt_radix_sort_pairs", "rt_radix_sort_pairs_static", "rt_radix_sort_keys", "rt_camera_look_at", "rt_camera_basis", "rt_primary_rays", "rt_batch_primary_rays",
     "rt_trace_closest", "rt_ray_order_scratch_bytes", "rt_ray_order", "rt_batch_ray_order_scratch_bytes", "rt_batch_ray_order",
     "rt_image_tile_order", "rt_interpolate", "rt_bounce_rays", "rt_batch_bounce_rays", "rt_mesh_file_save", "rt_mesh_file_info", "rt_mesh_file_load", "rt_tree_file_save", "rt_tree_file_info",
     "rt_tree_file_load", "rt_status_string", "rt_version", "rt_abi_version", "rt_device_check", "rt_launch_count",
@@ -212,6 +212,7 @@ def lib():
         L.rt_camera_look_at.argtypes = [C.POINTER(Camera), C.POINTER(C.c_float)]
         L.rt_camera_basis.argtypes = [C.POINTER(Camera), _U32, _U32, C.POINTER(C.c_float)]
         L.rt_primary_rays.argtypes = [C.POINTER(Camera), _U32, _U32, _P, _P, _P]
+        L.rt_batch_primary_rays.argtypes = [_P, _U32, _U32, _U32, _P, _P, _P]
         L.rt_trace_closest.argtypes = [C.POINTER(TraceDesc), _P]
         L.rt_interpolate.argtypes = [C.POINTER(InterpDesc), _P]
         L.rt_ray_order_scratch_bytes.argtypes = [_U32, C.POINTER(C.c_size_t)]

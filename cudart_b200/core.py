@@ -387,6 +387,22 @@ def primary_rays(cam: _abi.Camera, width: int, height: int, out=None, device="cu
     return out
 
 
+def camera_bases(cams, width: int, height: int, device="cuda") -> torch.Tensor:
+    """The rt_camera_basis of every camera, as the DEVICE float[16 * count] that batch_primary_rays reads."""
+    return torch.tensor([camera_basis(c, width, height) for c in cams], dtype=torch.float32, device=device)
+
+
+def batch_primary_rays(bases: torch.Tensor, width: int, height: int, out=None, stream=None):
+    """rt_batch_primary_rays: every camera's rays in one launch (camera c's at rows c * width * height)."""
+    count = bases.shape[0]
+    R = count * width * height
+    if out is None:
+        out = (torch.empty((R, 4), dtype=torch.float32, device=bases.device), torch.empty((R, 4), dtype=torch.float32, device=bases.device))
+    _abi.check("rt_batch_primary_rays", _abi.lib().rt_batch_primary_rays(_p(bases), count, width, height, _p(out[0]), _p(out[1]),
+                                                                         _stream(stream)))
+    return out
+
+
 def bounce_rays(tris, orig, dir, hit_pos, hit_t, seed: int, out=None, ray_count: int | None = None, stream=None):
     R = orig.shape[0] if ray_count is None else ray_count
     dev = orig.device

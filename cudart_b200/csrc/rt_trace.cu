@@ -1608,6 +1608,21 @@ __global__ __launch_bounds__(256) void k_image_tile_order(uint32_t total, uint32
 }
 
 // kernels/CUDA_calcPrimaryRays.cu:20-32
+// The rays of `count` cameras, camera c's rows at c w h: the arithmetic of k_primary with camera c's basis
+// (origin, direction, x step, y step) read from `bases` (four float4 per camera).
+__global__ __launch_bounds__(256) void k_batch_primary(const float4* __restrict__ bases, uint32_t count, uint32_t w, uint32_t h,
+                                                       float4* __restrict__ orig, float4* __restrict__ dir) {
+  const uint32_t per = w * h;
+  const size_t total = (size_t)count * per;
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t c = (uint32_t)(g / per), n = (uint32_t)(g % per);
+    const float4 ro = __ldg(bases + 4 * c), rd = __ldg(bases + 4 * c + 1), rx = __ldg(bases + 4 * c + 2), ry = __ldg(bases + 4 * c + 3);
+    const float x = (float)(n % w), y = (float)(n / w);
+    orig[g] = ro;
+    dir[g] = make_float4((rd.x - x * rx.x) - y * ry.x, (rd.y - x * rx.y) - y * ry.y, (rd.z - x * rx.z) - y * ry.z,
+                         (rd.w - x * rx.w) - y * ry.w);
+  }
+}
 __global__ __launch_bounds__(256) void k_primary(float4 ro, float4 rd, float4 rx, float4 ry, uint32_t w, uint32_t h,
                                                  float4* __restrict__ orig, float4* __restrict__ dir) {
   const size_t total = (size_t)w * h;
@@ -2012,6 +2027,20 @@ extern "C" rt_status rt_primary_rays(const rt_camera* cam, uint32_t w, uint32_t 
   k_primary<<<blocks, 256, 0, (cudaStream_t)stream>>>(make_float4(b[0], b[1], b[2], b[3]), make_float4(b[4], b[5], b[6], b[7]),
                                                       make_float4(b[8], b[9], b[10], b[11]), make_float4(b[12], b[13], b[14], b[15]), w, h,
                                                       (float4*)orig, (float4*)dir);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
+extern "C" rt_status rt_batch_primary_rays(const float* bases, uint32_t count, uint32_t w, uint32_t h, float* orig, float* dir,
+                                           rt_stream stream) {
+  if (count == 0) return RT_OK;
+  if (!bases || !orig || !dir || w == 0 || h == 0) return RT_ERR_INVALID_ARGUMENT;
+  if ((uint64_t)count * w * h > 0xFFFFFFFFull) return RT_ERR_INVALID_ARGUMENT;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  const size_t total = (size_t)count * w * h;
+  const uint32_t blocks = (uint32_t)hmin<size_t>((total + 255) / 256, (size_t)sms() * 16);
+  k_batch_primary<<<blocks, 256, 0, (cudaStream_t)stream>>>((const float4*)bases, count, w, h, (float4*)orig, (float4*)dir);
   note_launch();
   RT_CHECK_LAUNCH();
   return RT_OK;

@@ -52,6 +52,7 @@ class InstancedFrames:
         self.orig = torch.empty((count * R, 4), dtype=torch.float32, device=self.dev)
         self.dir = torch.empty((count * R, 4), dtype=torch.float32, device=self.dev)
         self.rt_cams = [core.make_camera(c.center, c.target, fov=c.fov, ratio=c.ratio) for c in self.cams]
+        self.cam_bases = core.camera_bases(self.rt_cams, width, height, device=self.dev)  # the cameras stay put
         self.primary_rays()
         self.ray_offsets = torch.tensor([i * R for i in range(count + 1)], dtype=torch.int32, device=self.dev)
         self.ray_face_base = torch.repeat_interleave(torch.tensor(self.face_offsets[:-1], dtype=torch.int32, device=self.dev),
@@ -92,17 +93,30 @@ class InstancedFrames:
         self.frame_index = frame
         self.verts = scenes.displace_instances(self.base_v, self.count, frame, self.seed, self.sigma, out=self.verts)
 
-    def primary_rays(self):
-        """Every instance's pinhole rays (rt_primary_rays per camera) into its rows of orig / dir."""
-        R = self.rays_per_instance
-        for i, cam in enumerate(self.rt_cams):
-            core.primary_rays(cam, self.width, self.height, out=(self.orig[i * R:(i + 1) * R], self.dir[i * R:(i + 1) * R]))
+    def primary_rays(self, stream=None):
+        """Every instance's pinhole rays (one rt_batch_primary_rays launch for all cameras) into orig / dir."""
+        core.batch_primary_rays(self.cam_bases, self.width, self.height, out=(self.orig, self.dir), stream=stream)
 
     def build(self, verts=None):
         """One batched LBVH build of all instances, from `verts` (default: the displaced frame)."""
         v = self.verts if verts is None else verts
         self.tree = core.batch_build(v, self.faces, self.face_offsets, self.vertex_offsets, out=self.tree, clusters=self.clusters)
         return self.tree
+
+    def build_and_rays(self, verts=None, aux=None):
+        """The frame's build and its primary rays side by side: the rays do not depend on the build, so they are
+        made on stream `aux` (forked from and joined back into the current stream; inside a graph capture this
+        becomes two parallel branches)."""
+        if aux is None:
+            self.primary_rays()
+            return self.build(verts)
+        cur = torch.cuda.current_stream()
+        aux.wait_stream(cur)
+        with torch.cuda.stream(aux):
+            self.primary_rays()
+        tree = self.build(verts)
+        cur.wait_stream(aux)
+        return tree
 
     def make_slots(self):
         self.slots = proposal.batch_subtree_slots(self.tree, self.depth)

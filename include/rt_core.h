@@ -264,6 +264,12 @@ rt_status rt_camera_basis(const rt_camera* camera, uint32_t width, uint32_t heig
 /* One pinhole ray per pixel, row-major, float4 origin and direction.
  * Replaces CUDA_calcPrimaryRays (kernels/CUDA_calcPrimaryRays.cu:20-69). */
 rt_status rt_primary_rays(const rt_camera* camera, uint32_t width, uint32_t height, float* orig, float* dir, rt_stream stream);
+/* The rays of `count` cameras in one launch: camera c's width x height rays at
+ * rows c * width * height. `bases` is a DEVICE float[16 * count], camera c's
+ * rt_camera_basis at 16 c (made once while the cameras stay put); the rays are
+ * bit-identical to rt_primary_rays per camera. No reference counterpart. */
+rt_status rt_batch_primary_rays(const float* bases, uint32_t count, uint32_t width, uint32_t height, float* orig, float* dir,
+                                rt_stream stream);
 
 typedef struct rt_trace_desc {
   const uint32_t* nodes;    /* bvnode[] from rt_lbvh_build */

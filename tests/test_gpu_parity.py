@@ -166,6 +166,21 @@ def test_primary_rays_match_oracle(T, oracle, scene):
     assert np.array_equal(_u32(_host(d)), _u32(ed))
 
 
+def test_batch_primary_rays_equal_per_camera(T):
+    """rt_batch_primary_rays (all cameras in one launch) gives each camera's rays bit for bit as
+    rt_primary_rays (which the oracle pins), for an image size that is no multiple of anything."""
+    from cudart_b200 import core
+    cams = [core.make_camera((0.1 * i, 0.5, -1.0 - i), (0.5, 0.4, 0.5), fov=0.9 + 0.1 * i, ratio=1.3) for i in range(5)]
+    w, h = 37, 23
+    o, d = core.batch_primary_rays(core.camera_bases(cams, w, h), w, h)
+    T.cuda.synchronize()
+    for i, c in enumerate(cams):
+        po, pd = core.primary_rays(c, w, h)
+        T.cuda.synchronize()
+        sl = slice(i * w * h, (i + 1) * w * h)
+        assert T.equal(o[sl].view(T.int32), po.view(T.int32)) and T.equal(d[sl].view(T.int32), pd.view(T.int32)), i
+
+
 def _check_trace(T, oracle, tree, ref, o, d, tmax=None, id_mode=0, use_tris=True, vertices=None, sel=None):
     from cudart_b200 import core
     out = core.trace(tree, o, d, tmax=tmax, id_mode=id_mode, counters=True, use_tris=use_tris, vertices=vertices, use_accel=False)
