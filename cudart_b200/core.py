@@ -131,7 +131,7 @@ def build_lbvh(vertices: torch.Tensor, faces: torch.Tensor, hitbox=None, tree_de
     """LBVH build of a mesh given as float4 vertices (V, 4) and uint4 faces (N, 4).
     hitbox: host sequence of 8 floats (min xyzw, max xyzw) or None for the
     vertices' min/max. clusters: also write the cluster tree into the blob
-    (RT_ACCEL_CLUSTERS, leaves of at most cluster_leaf positions, 0 = 4), for
+    (RT_ACCEL_CLUSTERS, leaves of at most cluster_leaf positions, 0 = 3), for
     schedules with "clusters": True."""
     _need_cuda(vertices, "vertices", _F32, 4)
     _need_cuda(faces, "faces", _I32, 4)

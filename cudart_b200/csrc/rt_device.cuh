@@ -142,7 +142,7 @@ __device__ __forceinline__ void accel_node(const uint32_t* __restrict__ nodes, c
 
 // ---------------------------------------------------------------------------
 // Cluster tree: a second traversal tree in the blob, independent of the node
-// tree, whose leaves hold at most `leaf_max` (1..8, default 4) triangles. It is
+// tree, whose leaves hold at most `leaf_max` (1..8, default 3) triangles. It is
 // the binary radix tree of the mesh's sorted keys (Morton code, position)
 // built bottom-up (rt_clusters.cu), cut at subtrees of at most leaf_max
 // positions (a "cluster": a contiguous run of positions) and stored as 4-wide
@@ -161,7 +161,7 @@ __device__ __forceinline__ void accel_node(const uint32_t* __restrict__ nodes, c
 constexpr uint32_t kClusterLeaf = 0x80000000u;
 constexpr uint32_t kClusterFirstMask = 0x0FFFFFFFu;  // meshes of fewer than 2^28 positions
 constexpr uint32_t kClusterLeafMax = 8;
-constexpr uint32_t kClusterLeafDefault = 4;
+constexpr uint32_t kClusterLeafDefault = 3;
 // Header words (per mesh, inside the blob header of 64 words) describing the cluster tree. Every build clears
 // the valid word (in the kernel that writes the node records' header words); the cluster build sets it last.
 constexpr int kHdrClusterValid = 16;  // 1 once the build wrote the cluster tree for this mesh, else 0

@@ -61,7 +61,7 @@ typedef struct rt_build_params {
   uint32_t max_leaf;      /* 224, kernels/CUDA_buildMeshTreeLBVH.cu:40 (0 = default) */
   uint32_t morton_bits;   /* 32: reference 11/11/10 interleave; 30: 10/10/10 left-aligned (0 = 32) */
   uint32_t accel_trees;   /* traversal trees written into the blob besides the node records: RT_ACCEL_* bits (0 = none) */
-  uint32_t cluster_leaf;  /* RT_ACCEL_CLUSTERS: most positions per cluster tree leaf, 1..8 (0 = 4) */
+  uint32_t cluster_leaf;  /* RT_ACCEL_CLUSTERS: most positions per cluster tree leaf, 1..8 (0 = 3) */
 } rt_build_params;
 
 /* rt_build_params.accel_trees. The blob always holds records of the build's
