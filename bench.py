@@ -649,7 +649,7 @@ def leg_single_scene(args, dev, world, mesh, cam, key, with_roofline=False):
     N, W, H = mesh.face_count, cam.width, cam.height
     R = W * H
     camera = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
-    tree = core.build_lbvh(v, f)
+    tree = core.build_lbvh(v, f, clusters=True)  # with the cluster tree: the tuner tries both trees' walks
     rays = core.primary_rays(camera, W, H)
     h1 = core.trace(tree, rays[0], rays[1])
     bounce = core.bounce_rays(tree.tris, rays[0], rays[1], h1["id"], h1["t"], SEED_BOUNCE)
@@ -657,7 +657,7 @@ def leg_single_scene(args, dev, world, mesh, cam, key, with_roofline=False):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     s1, _ = tune.tune_trace(tree, rays[0], rays[1], image_width=W, key=f"{key}-primary", use_cache=False)
     s2, _ = tune.tune_trace(tree, bounce[0], bounce[1], tmax=bounce[2], image_width=W, key=f"{key}-bounce", use_cache=False)
-    stages = [lambda: core.build_lbvh(v, f, out=tree), lambda: core.primary_rays(camera, W, H, out=rays),
+    stages = [lambda: core.build_lbvh(v, f, out=tree, clusters=True), lambda: core.primary_rays(camera, W, H, out=rays),
               lambda: core.trace(tree, rays[0], rays[1], out=h1, schedule=s1),
               lambda: core.bounce_rays(tree.tris, rays[0], rays[1], h1["id"], h1["t"], SEED_BOUNCE, out=bounce),
               lambda: core.trace(tree, bounce[0], bounce[1], tmax=bounce[2], out=h2, schedule=s2)]
@@ -693,12 +693,19 @@ def leg_single_scene(args, dev, world, mesh, cam, key, with_roofline=False):
         peak, kind = load_peaks()
 
         def kname(sch):
+            if sch.get("clusters"):
+                if sch.get("persistent"):
+                    for k in ("packet", "refill", "coop"):
+                        if sch.get(k):
+                            return "k_trace_clusters_" + k
+                    return "k_trace_clusters_persistent"
+                return "k_trace_clusters"
             if sch.get("coop"):
                 return "k_trace_coop_persistent" if sch.get("persistent") else "k_trace_coop"
             return "k_trace_accel_persistent" if sch.get("persistent") else "k_trace_accel"
         out["roofline_primary"] = trace_roofline(kname(s1), "primary", m1, t1, R, peak, kind, kname(s1))
         out["roofline_bounce"] = trace_roofline(kname(s2), "bounce", m2, t2, R, peak, kind, kname(s2))
-        bb = N * (16 + 48 + 32 + 8 + 64 + 4 + 32 + 36 + 48) + 64 * info["node_count"]
+        bb = N * (16 + 48 + 32 + 8 + 64 + 4 + 32 + 36 + 48) + 64 * info["node_count"] + N * (4 + 48 + 32 + 32 + 8 + 4)
         a = bb / (build_ms * 1e-3) / 1e9
         out["build_roofline"] = {"bound": "hbm", "achieved": round(a, 1), "peak": peak, "unit": "GB/s", "frac": round(a / peak, 4)}
     del graphs, flush
@@ -746,11 +753,11 @@ def leg_batch(args, dev, world, count=1024):
     V = torch.from_numpy(verts).to(dev)
     Fc = torch.from_numpy(faces.view(np.int32)).to(dev)
     roff = torch.tensor(ro.astype(np.int32), device=dev)
-    tree = core.batch_build(V, Fc, fo, vo)
+    tree = core.batch_build(V, Fc, fo, vo, clusters=True)
     sched, _ = tune.tune_batch_trace(tree, orig, dirs, roff, key=f"batch{count}", use_cache=False)  # untimed
     hits = core.batch_trace(tree, orig, dirs, roff, schedule=sched)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    (gb, gt), kernels = capture_graphs([lambda: core.batch_build(V, Fc, fo, vo, out=tree),
+    (gb, gt), kernels = capture_graphs([lambda: core.batch_build(V, Fc, fo, vo, out=tree, clusters=True),
                                         lambda: core.batch_trace(tree, orig, dirs, roff, out=hits, schedule=sched)])
     bms = timed_ms(gb.replay, flush, reps=3)
     tms = timed_ms(gt.replay, flush, reps=3)
