@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-legs", action="store_true", help="only the oracle port on the host cores for c0-c3 (no GPU work)")
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--nn-frames", type=int, default=3, help="frames of the learned path (fine-tuning + proposals) timed beside plain")
     ap.add_argument("--legs", default="c0,c1,build16m,c2,c3,sah,raster",
@@ -587,6 +588,62 @@ def cpu_baseline_c4(count, frame=0, steps=1, one_thread=True):
     return out
 
 
+def cpu_legs():
+    """--cpu-legs: the oracle port (the reference algorithm) on the host cores for the secondary configs, each
+    with all threads and with one: LBVH build Mtri/s and closest-hit Mrays/s on a bounded sample of the leg's
+    rays (primaries and their bounces where the GPU leg traces bounces). c0 terrain (512 x 512 rays), c1 2^20-face
+    soup (1920 x 1080 rays), c2 every 32nd mesh of the 1024-mesh batch (32 x 32 sphere rays each), c3 the
+    4,022,242-face scene (rays uniform in its box, as the GPU leg's evaluation rays). One JSON line per leg."""
+    import torch
+
+    from cudart_b200 import scenes
+    from oracle import api as O
+
+    cores = O.max_threads()
+
+    def run(mesh, o, d, bounce, threads, stride):
+        o, d = np.ascontiguousarray(o[::stride]), np.ascontiguousarray(d[::stride])
+        O.set_threads(threads)
+        t0 = time.perf_counter()
+        ref = O.lbvh_build(mesh.vertices, mesh.faces)
+        t1 = time.perf_counter()
+        e = O.trace(ref["nodes"], ref["tris"], ref["indices"], o, d, threads=threads)
+        rays = len(o)
+        if bounce:
+            bo, bd, bt = O.bounce_rays(ref["tris"], o, d, e["id"], e["t"], SEED_BOUNCE)
+            O.trace(ref["nodes"], ref["tris"], ref["indices"], bo, bd, bt, threads=threads)
+            rays += int((bt > 0).sum())
+        t2 = time.perf_counter()
+        O.set_threads(0)
+        return mesh.face_count / (t1 - t0) / 1e6, rays / (t2 - t1) / 1e6
+
+    def leg(name, meshes_rays, bounce, stride_all, stride_one, note):
+        res = {"leg": f"cpu_{name}", "kind": "port", "cores": cores}
+        for label, threads, stride in (("all", cores, stride_all), ("1_thread", 1, stride_one)):
+            builds, rates = [], []
+            for mesh, o, d in meshes_rays:
+                b, r = run(mesh, o, d, bounce, threads, stride)
+                builds.append(b)
+                rates.append(r)
+            res[f"build_mtri_s_{label}"] = round(statistics.median(builds), 3)
+            res[f"mrays_s_{label}"] = round(statistics.median(rates), 4)
+        res["sample"] = note
+        emit(res)
+
+    m, cam = scenes.terrain_small_scene()
+    o, d, _, _ = O.primary_rays(cam)
+    leg("c0", [(m, o, d)], True, 1, 4, "terrain 32,258 faces; all 262,144 primaries + bounces (1 thread: every 4th)")
+    m, cam = scenes.soup_1m_scene()
+    o, d, _, _ = O.primary_rays(cam)
+    leg("c1", [(m, o, d)], True, 8, 64, "soup 2^20 faces; every 8th of 2,073,600 primaries + bounces (1 thread: every 64th)")
+    ms = scenes.batch_meshes(1024, seed=3)[::32]
+    leg("c2", [(x, *scenes.sphere_rays(x, 32, seed=i)) for i, x in enumerate(ms)], False, 1, 1,
+        "32 of the 1024 meshes (every 32nd), each built and traced with 32 x 32 sphere rays; medians over the meshes")
+    m = scenes.learned_scene(1.0)
+    eo, ed = scenes.box_rays_torch(1 << 18, scenes.scene_box(m, 1.5), seed=2, device="cpu")
+    leg("c3", [(m, eo.numpy(), ed.numpy())], False, 1, 16, "4,022,242 faces; 262,144 rays uniform in the scene box (1 thread: every 16th)")
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -952,6 +1009,10 @@ def main():
         res = run_reference(args, rank, world)
         if res is not None:
             emit(res)
+        return
+    if args.cpu_legs:
+        if rank == 0:
+            cpu_legs()
         return
     if world > 1:
         import datetime

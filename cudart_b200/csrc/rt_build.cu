@@ -718,6 +718,29 @@ int resident_blocks_of(K kernel, int threads) {
 }
 
 }  // namespace
+
+SideStream* side_stream() {
+  // one per host thread and device (a stream takes part in one capture at a time, and a thread's calls are
+  // ordered, so the fork and join events of two calls never interleave); kept until the process exits
+  constexpr int kMaxDevices = 64;
+  thread_local SideStream per_device[kMaxDevices];
+  thread_local int state[kMaxDevices] = {};  // 0 not yet, 1 ready, -1 refused
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (state[dev] == 0) {
+    SideStream& x = per_device[dev];
+    const bool ok = cudaStreamCreateWithFlags(&x.s, cudaStreamNonBlocking) == cudaSuccess &&
+                    cudaEventCreateWithFlags(&x.fork, cudaEventDisableTiming) == cudaSuccess &&
+                    cudaEventCreateWithFlags(&x.join, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+    state[dev] = ok ? 1 : -1;
+  }
+  return state[dev] == 1 ? &per_device[dev] : nullptr;
+}
+
 }  // namespace rt
 
 using namespace rt;
@@ -964,7 +987,9 @@ __global__ __launch_bounds__(512) void k_batch_hitbox(BatchArgs B) {
   const uint32_t m = blockIdx.x / kHitSplit, part = blockIdx.x % kHitSplit;
   const uint32_t w0 = B.voff[m], w1 = B.voff[m + 1], share = (w1 - w0 + kHitSplit - 1) / kHitSplit;
   const uint32_t v0 = min(w1, w0 + part * share), v1 = min(w1, v0 + share);
-  if (part == 0 && threadIdx.x == 0) {  // the mesh sort's digit counts: mesh m holds foff[m + 1] - foff[m] keys of value m
+  if (part == 0 && threadIdx.x == 0) {
+    B.acc_hdr[64 * (size_t)m + kHdrClusterValid] = 0;  // set again by the cluster build, if any
+    // the mesh sort's digit counts: mesh m holds foff[m + 1] - foff[m] keys of value m
     const uint32_t faces = B.foff[m + 1] - B.foff[m];
     atomicAdd(B.counts + 4 * 256 + (m & 255u), faces);
     atomicAdd(B.counts + 5 * 256 + ((m >> 8) & 255u), faces);
@@ -1209,7 +1234,6 @@ __global__ __launch_bounds__(256) void k_batch_records(BatchArgs B) {
   }
   for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < B.M; m += gridDim.x * blockDim.x) {
     const uint32_t* h = B.hdr + 16 * m;
-    B.acc_hdr[64 * (size_t)m + kHdrClusterValid] = 0;  // set again by the cluster build, if any
     rt_build_info* o = B.info_out + m;
     o->leaf_count = h[0]; o->node_count = h[2]; o->real_depth = h[3]; o->split_count = h[4];
     o->overrun_visits = h[5]; o->nondet_reads = h[6]; o->past_end_reads = h[7]; o->error = h[8] | *B.err;
@@ -1334,10 +1358,26 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   if (cudaMemsetAsync(B.arrive, 0, (2 * (size_t)N) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   static const int leaf_blocks = resident_blocks_of(k_batch_leaves, 256);
   k_batch_leaves<<<sms * leaf_blocks, 256, 0, st>>>(B);
-  k_batch_propagate<<<sms * 8, 256, 0, st>>>(B);
-  k_batch_records<<<sms * 4, 256, 0, st>>>(B);
-  note_launch(3);
+  note_launch();
   RT_CHECK_LAUNCH();
-  if (clusters) return batch_build_cluster_tree(B.tris, B.codes, B.foff, M, N, q.cluster_leaf, B.ct, B.acc_hdr, B.crec, st);
+  // the node boxes and records (from the nodes) and the cluster trees (from the codes and triangles) are
+  // independent: with cluster trees, the node half runs on a side stream beside them
+  SideStream* side = clusters ? side_stream() : nullptr;
+  cudaStream_t ns = st;
+  if (side) {
+    if (cudaEventRecord(side->fork, st) != cudaSuccess || cudaStreamWaitEvent(side->s, side->fork, 0) != cudaSuccess)
+      return RT_ERR_CUDA;
+    ns = side->s;
+  }
+  k_batch_propagate<<<sms * 8, 256, 0, ns>>>(B);
+  k_batch_records<<<sms * 4, 256, 0, ns>>>(B);
+  note_launch(2);
+  RT_CHECK_LAUNCH();
+  if (clusters) {
+    s = batch_build_cluster_tree(B.tris, B.codes, B.foff, M, N, q.cluster_leaf, B.ct, B.acc_hdr, B.crec, st);
+    if (side && (cudaEventRecord(side->join, side->s) != cudaSuccess || cudaStreamWaitEvent(st, side->join, 0) != cudaSuccess))
+      return RT_ERR_CUDA;
+    if (s != RT_OK) return s;
+  }
   return RT_OK;
 }

@@ -93,6 +93,15 @@ struct PerDeviceOnce {
   }
 };
 
+// A side stream and two events for this host thread and the current device: a call forks an independent part of
+// its work onto the side stream and joins it back (event record, stream wait: stream capture turns that into two
+// parallel branches). Created on first use; nullptr when CUDA refuses (the caller then runs both parts in order).
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+SideStream* side_stream();
+
 // Number of kernels this library has launched (process-wide); exported as
 // rt_launch_count() so that a caller can count the kernels inside a timed region.
 void note_launch(uint32_t kernels = 1);
