@@ -417,7 +417,8 @@ def bounce_rays(tris, orig, dir, hit_pos, hit_t, seed: int, out=None, ray_count:
 def batch_bounce_rays(tree, ray_offsets, orig, dir, hit_pos, hit_t, seed: int, out=None, order: bool = False, stream=None):
     """bounce_rays for the rays of a batched build: hit_pos are positions inside each ray's own mesh
     (batch_trace's ids); the same rays as bounce_rays given the global positions. With order=True the result
-    has a fourth tensor: a tracing order with the active rays first (for batch_trace's `order`)."""
+    has a fourth tensor: a tracing order with the active rays first (for batch_trace's `order`); a given `out`
+    with four tensors keeps its fourth unwritten when order=False."""
     R = orig.shape[0]
     dev = orig.device
     if out is None:
@@ -425,7 +426,7 @@ def batch_bounce_rays(tree, ray_offsets, orig, dir, hit_pos, hit_t, seed: int, o
                torch.empty(R, dtype=torch.float32, device=dev))
         if order:
             out = out + (torch.empty(R + 2, dtype=torch.int32, device=dev),)  # R order entries, then two counters
-    ord_ = out[3] if len(out) > 3 else None
+    ord_ = out[3] if (order and len(out) > 3) else None
     _abi.check("rt_batch_bounce_rays", _abi.lib().rt_batch_bounce_rays(
         _p(tree.tris), _p(tree.face_offsets), _p(ray_offsets), tree.mesh_count, _p(orig), _p(dir), _p(hit_pos), _p(hit_t), R,
         C.c_uint64(seed), _p(out[0]), _p(out[1]), _p(out[2]), None if ord_ is None else C.c_void_p(ord_.data_ptr()),

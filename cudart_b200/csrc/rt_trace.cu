@@ -1096,7 +1096,7 @@ __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, con
 // then the warp takes that many new rays with one atomic and every lane steps
 // its own walk again, so a warp no longer waits for its slowest ray. `start`
 // maps a slot to a ray and its mesh: false for a slot without a ray.
-template <bool kCount, class Start>
+template <bool kCount, bool kWW, class Start>
 __device__ __forceinline__ void refill_walks(const TraceArgs& A, uint32_t* counter, const uint32_t slots, const uint32_t threshold,
                                              const Start& start) {
   const uint32_t lane = lane_id();
@@ -1161,7 +1161,9 @@ __device__ __forceinline__ void refill_walks(const TraceArgs& A, uint32_t* count
       continue;
     }
     const float4* recs = C.crec + 8 * (size_t)C.F;
-    if (!(ref & kClusterLeaf)) {
+    const bool was_cluster = (ref & kClusterLeaf) != 0;
+    bool done_walk = false;  // the descent found nothing more to walk
+    while (!(ref & kClusterLeaf)) {  // one record (if-if), or records until a cluster is held (while-while)
       float t[4];
       uint32_t k[4];
       cluster_test(recs + 8 * (size_t)ref, oi, ix, iy, iz, bt, t, k);
@@ -1180,9 +1182,23 @@ __device__ __forceinline__ void refill_walks(const TraceArgs& A, uint32_t* count
           }
         }
         ref = k[0];
-        continue;
+      } else if (!pop_within(st_ref, st_t, sp, bt, ref)) {
+        done_walk = true;
+        break;
       }
-    } else {
+      if (!kWW) break;
+      if (!cluster_ref_ok(ref, C.n, steps)) {
+        if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+        done_walk = true;
+        break;
+      }
+    }
+    if (done_walk) {
+      finish();
+      continue;
+    }
+    if (!kWW && !was_cluster) continue;  // if-if: a step is one record or one cluster
+    {
       const float4* tris = A.tris + 3 * (size_t)C.F;
       const uint32_t p0 = ref & kClusterFirstMask, p1 = p0 + ((ref >> 28) & 7u) + 1u;
       for (uint32_t pos = p0; pos < p1; ++pos) {
@@ -1434,11 +1450,11 @@ __global__ __launch_bounds__(128) void k_trace_clusters_packet(TraceArgs A, Clus
   }
 }
 
-template <bool kCount>
+template <bool kCount, bool kWW>
 __global__ __launch_bounds__(128) void k_trace_clusters_refill(TraceArgs A, ClusterArgs C, SlotMap M, uint32_t* counter,
                                                                 uint32_t threshold) {
   C.F = 0;
-  refill_walks<kCount>(A, counter, M.slots, threshold, [&](uint32_t slot, uint32_t& r, ClusterArgs& Cl) {
+  refill_walks<kCount, kWW>(A, counter, M.slots, threshold, [&](uint32_t slot, uint32_t& r, ClusterArgs& Cl) {
     Cl = C;
     return M.ray_of(slot, r);
   });
@@ -1479,10 +1495,10 @@ __global__ __launch_bounds__(128) void k_batch_trace_clusters_persistent(TraceAr
     }
   }
 }
-template <bool kCount>
+template <bool kCount, bool kWW>
 __global__ __launch_bounds__(128) void k_batch_trace_clusters_refill(TraceArgs A, BatchTraceArgs B, uint32_t* counter,
                                                                       uint32_t threshold) {
-  refill_walks<kCount>(A, counter, A.ray_count, threshold, [&](uint32_t slot, uint32_t& r, ClusterArgs& C) {
+  refill_walks<kCount, kWW>(A, counter, A.ray_count, threshold, [&](uint32_t slot, uint32_t& r, ClusterArgs& C) {
     r = B.ray_of(slot);
     C.crec = B.acc.crec;
     batch_cluster_args(r, B, C);
@@ -1816,8 +1832,10 @@ rt_status launch_clusters(const rt_trace_desc* d, const TraceArgs& A, cudaStream
       if (count) k_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->lane_threshold);
       else k_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->lane_threshold);
     } else if (d->schedule & RT_TRACE_REFILL) {
-      if (count) k_trace_clusters_refill<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->lane_threshold);
-      else k_trace_clusters_refill<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->lane_threshold);
+#define RT_LAUNCH_CR(CNT, WW) k_trace_clusters_refill<CNT, WW><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter, d->lane_threshold)
+      if (count) { if (ww) RT_LAUNCH_CR(true, true); else RT_LAUNCH_CR(true, false); }
+      else { if (ww) RT_LAUNCH_CR(false, true); else RT_LAUNCH_CR(false, false); }
+#undef RT_LAUNCH_CR
     } else if (d->schedule & RT_TRACE_COOP) {
       if (count) k_trace_clusters_coop<true><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
       else k_trace_clusters_coop<false><<<blocks, 128, 0, st>>>(A, C, M, d->work_counter);
@@ -2131,8 +2149,10 @@ rt_status batch_launch_clusters(const rt_batch_trace_desc* d, const TraceArgs& A
       if (count) k_batch_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold);
       else k_batch_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold);
     } else if (d->schedule & RT_TRACE_REFILL) {
-      if (count) k_batch_trace_clusters_refill<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold);
-      else k_batch_trace_clusters_refill<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold);
+#define RT_LAUNCH_BCR(CNT, WW) k_batch_trace_clusters_refill<CNT, WW><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold)
+      if (count) { if (ww) RT_LAUNCH_BCR(true, true); else RT_LAUNCH_BCR(true, false); }
+      else { if (ww) RT_LAUNCH_BCR(false, true); else RT_LAUNCH_BCR(false, false); }
+#undef RT_LAUNCH_BCR
     } else if (d->schedule & RT_TRACE_COOP) {
       if (count) k_batch_trace_clusters_coop<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter);
       else k_batch_trace_clusters_coop<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter);

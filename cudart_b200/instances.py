@@ -122,11 +122,15 @@ class InstancedFrames:
         self.slots = proposal.batch_subtree_slots(self.tree, self.depth)
         return self.slots
 
-    def bounce(self, hits, out=None):
+    def bounce(self, hits, out=None, order=None):
         """One diffuse bounce per primary hit (rt_batch_bounce_rays: hit ids are instance-local positions):
-        (orig, dir, tmax, order), the order listing the active bounces first."""
+        (orig, dir, tmax, order), the order listing the active bounces first. The order is made when `order` is
+        true, by default only when a traced schedule reads it (or before tune() has picked the schedules)."""
+        if order is None:
+            order = self.schedule_bounce is None or bool(self.schedule_bounce.get("given_order")) or \
+                bool((self.seeded_schedules()[1] or {}).get("given_order"))
         return core.batch_bounce_rays(self.tree, self.ray_offsets, self.orig, self.dir, hits["id"], hits["t"], 1000 + self.frame_index,
-                                      out=out, order=True)
+                                      out=out, order=order)
 
     def bounce_order(self, b):
         """The tracing order of the bounce launch: the generator's active-first order when the bounce schedule asks
@@ -141,7 +145,7 @@ class InstancedFrames:
         self.schedule_primary, t1 = tune.tune_batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, use_cache=False,
                                                           images=(self.count, self.width, self.height))
         h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, schedule=self.schedule_primary)
-        b = self.bounce(h1)
+        b = self.bounce(h1, order=True)
         self.schedule_bounce, t2 = tune.tune_batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], use_cache=False,
                                                          order=b[3])
         # the seeded walks go through the node records: the fastest schedule of those for each launch

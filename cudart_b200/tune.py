@@ -63,9 +63,9 @@ def cluster_candidates(image_width: int):
         out.append({"clusters": True, "image_width": 0, "persistent": True, "blocks_per_sm": 16, "coop": coop, "while_while": ww,
                     "sorted": True})
     # per-lane walks in warps that refill their idle lanes
-    for ml, srt in itertools.product((4, 8, 16), (False, True)):
+    for ml, srt, ww in itertools.product((4, 8, 16), (False, True), (False, True)):
         out.append({"clusters": True, "image_width": 0, "persistent": True, "blocks_per_sm": 8, "refill": True, "lane_threshold": ml,
-                    "sorted": srt})
+                    "sorted": srt, "while_while": ww})
     # warp packets: pixel tiles of the image, or rays sorted by octant and origin (leaving the packet below
     # lane_threshold lanes)
     for bps, ml in itertools.product((8, 16), (0, 8, 16)):
@@ -132,8 +132,8 @@ def cluster_batch_candidates(images=None):
         if images is not None and images[1] % 8 == 0 and images[2] % 4 == 0:
             out.append({"clusters": True, "persistent": True, "blocks_per_sm": bps, "coop": coop, "while_while": ww, "tiles": list(images)})
     # per-lane walks in warps that refill their idle lanes once lane_threshold of them are idle
-    for ml, bits in itertools.product((2, 4, 8, 16), (None, 12)):
-        c = {"clusters": True, "persistent": True, "blocks_per_sm": 8, "refill": True, "lane_threshold": ml}
+    for ml, bits, ww in itertools.product((2, 4, 8, 16), (None, 12), (False, True)):
+        c = {"clusters": True, "persistent": True, "blocks_per_sm": 8, "refill": True, "lane_threshold": ml, "while_while": ww}
         out.append(c if bits is None else dict(c, sorted_bits=bits))
     # warp packets (one node sequence per warp): pixel tiles, and rays ordered by mesh, octant and origin; a warp
     # leaves the packet for per-lane walks once fewer than lane_threshold lanes want its node (0: never)

@@ -27,6 +27,7 @@ CLUSTER_SCHEDULES = [
     dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, lane_threshold=32),
     dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=16),  # warps refill idle lanes
     dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=1, sorted=True),
+    dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=8, while_while=True),
 ]
 
 
@@ -228,7 +229,8 @@ def test_batched_cluster_walks_match_single_mesh(T, oracle):
                  dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, sorted_bits=21),
                  dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, lane_threshold=16, sorted_bits=21),
                  dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=8),
-                 dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=32, sorted_bits=12)]
+                 dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=32, sorted_bits=12),
+                 dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=4, while_while=True)]
     for sch in schedules:
         h = core.batch_trace(bt, O, D, roff, schedule=sch)
         T.cuda.synchronize()
