@@ -139,7 +139,7 @@ __device__ __forceinline__ uint32_t find_seg(const uint32_t* __restrict__ off, u
 // One digit pass. status[tile * 256 + d] holds a flag (bits 30-31) and a count (bits 0-29); all zero at the start.
 // vals_in == nullptr with kVals: the values are the keys' input positions (first pass of an index sort).
 template <bool kVals>
-__global__ __launch_bounds__(kOsThreads, 2) void k_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+__global__ __launch_bounds__(kOsThreads, 3) void k_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                                                             uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n,
                                                             uint32_t shift, const uint32_t* __restrict__ digit_counts,
                                                             uint32_t* __restrict__ status, uint32_t* __restrict__ tile_counter,
@@ -200,21 +200,27 @@ __global__ __launch_bounds__(kOsThreads, 2) void k_onesweep(const uint32_t* __re
   const uint32_t dbase = block_excl_scan<kOsThreads>(dc, s_warp, total);
   if (tid < kRadix) {
     s_tile_start[tid] = start;
-    // keys of this digit in the tiles before this one
+    // keys of this digit in the tiles before this one: the look-back reads four earlier tiles' words at a time
+    // (independent loads, one round trip) and walks them nearest first; a word not yet published is read again
     uint32_t excl = 0, spins = 0;
     for (int64_t j = (int64_t)tile - 1; j >= 0;) {
-      const uint32_t s = ld_relaxed(status + (size_t)j * kRadix + tid);
-      const uint32_t flag = s & ~kCountMask;
-      if (flag == 0u) {
-        if (++spins > kSpinLimit) {
-          if (err) atomicOr(err, (uint32_t)RT_DEVERR_WAIT_TIMEOUT);
-          break;
-        }
-        continue;
+      uint32_t w4[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) w4[q] = (j - q >= 0) ? ld_relaxed(status + (size_t)(j - q) * kRadix + tid) : kFlagPrefix;
+      bool done = false;
+      int q = 0;
+      for (; q < 4; ++q) {
+        const uint32_t flag = w4[q] & ~kCountMask;
+        if (flag == 0u) break;  // tile j - q has published nothing yet
+        excl += w4[q] & kCountMask;
+        if (flag == kFlagPrefix) { done = true; break; }
       }
-      excl += s & kCountMask;
-      if (flag == kFlagPrefix) break;
-      --j;
+      if (done) break;
+      j -= q;
+      if (q == 0 && ++spins > kSpinLimit) {
+        if (err) atomicOr(err, (uint32_t)RT_DEVERR_WAIT_TIMEOUT);
+        break;
+      }
     }
     if (tile > 0) st_relaxed(status + (size_t)tile * kRadix + tid, kFlagPrefix | (excl + tile_count));
     s_glob[tid] = dbase + excl;
