@@ -19,6 +19,8 @@ steady-state launch. Cases (kernel of interest in brackets):
   mlp_grouped    64 grouped networks: 3 training steps of 1024 rays each,        [k_gemm_tc, k_softmax_xent, ...]
                  then proposals for 64 x 518,400 rays
   sort_16m       2^24 random (key, value) pairs, 32-bit keys, sorted twice         [k_onesweep, k_sort_hist]
+  trace_clusters 2^20-face soup with its cluster tree: packet primaries, per-lane [k_trace_clusters*]
+                 bounces, twice each
   c4_frame [M]   M (default 64) deformed instances of the 1/16-size learned       [launch list, k_batch_trace_clusters*]
                  scene, three frames of the plain path: batched build, primary
                  rays, batched trace, bounce rays, batched trace
@@ -60,6 +62,24 @@ def trace_bounce():
     for _ in range(2):
         core.trace(tree, b[0], b[1], tmax=b[2], schedule=dict(persistent=True, blocks_per_sm=16, while_while=True, sorted=True,
                                                               coop=True, wide=True))  # the tuner's pick for these rays
+    torch.cuda.synchronize()
+
+
+def trace_clusters():
+    """The 2^20-face soup with its cluster tree: primary rays as warp packets over 8 x 4 pixel tiles, then their
+    bounces as per-lane walks over 8 x 4 tiles (the c1 leg's picks), twice each."""
+    from . import core
+    mesh, cam, v, f, _ = _soup_scene()
+    tree = core.build_lbvh(v, f, clusters=True)
+    c = core.make_camera(cam.center, cam.target, fov=cam.fov, ratio=cam.ratio)
+    o, d = core.primary_rays(c, cam.width, cam.height)
+    s1 = dict(clusters=True, image_width=cam.width, persistent=True, blocks_per_sm=16, packet=True)
+    s2 = dict(clusters=True, image_width=cam.width)
+    h = core.trace(tree, o, d, schedule=s1)
+    b = core.bounce_rays(tree.tris, o, d, h["id"], h["t"], 1234)
+    for _ in range(2):
+        core.trace(tree, o, d, schedule=s1)
+        core.trace(tree, b[0], b[1], tmax=b[2], schedule=s2)
     torch.cuda.synchronize()
 
 
@@ -191,7 +211,7 @@ def c4_frame(count: int = 64):
     torch.cuda.synchronize()
 
 
-CASES = {"bench_step": bench_step, "build_16m": build_16m, "batch_build": batch_build, "trace_primary": trace_primary, "trace_bounce": trace_bounce, "mlp_propose": mlp_propose, "mlp_train": mlp_train,
+CASES = {"bench_step": bench_step, "trace_clusters": trace_clusters, "build_16m": build_16m, "batch_build": batch_build, "trace_primary": trace_primary, "trace_bounce": trace_bounce, "mlp_propose": mlp_propose, "mlp_train": mlp_train,
          "sah_build": sah_build, "raster": raster, "mlp_grouped": mlp_grouped, "c4_frame": c4_frame, "sort_16m": sort_16m}
 
 if __name__ == "__main__":
