@@ -82,6 +82,41 @@ def test_batch_build_and_sort_refusals_before_launch():
     assert lib.rt_radix_sort_pairs(C.c_void_p(FAKE), C.c_void_p(FAKE), n, 32, 0, C.c_void_p(FAKE), nb.value, None) == 2
 
 
+@pytest.mark.skipif(cuda_available(), reason="host-side refusals, checked where no buffer can be touched")
+def test_cluster_tree_and_batched_rays_refusals_before_launch():
+    """A cluster tree with leaves of more than 8 positions is refused (RT_ERR_UNSUPPORTED) before any launch, single
+    and batched; the scratch of a build with the cluster tree is larger than without; rt_batch_primary_rays refuses
+    a null pointer or an empty image before the device check, and more than 2^32 rays in all."""
+    from cudart_b200 import _abi, core
+    lib = _abi.lib()
+    n = 100000
+    plain, max_nodes = core.lbvh_scratch_bytes(n)
+    with_clusters, _ = core.lbvh_scratch_bytes(n, clusters=True)
+    assert with_clusters > plain + 60 * n  # arrival words, child pairs, child boxes and ranges per face
+    acc = core.accel_bytes(n)
+    d = _build_desc(n, max_nodes, with_clusters, acc)
+    d.params = _abi.BuildParams(12, 1, 0, 0, 32, _abi.ACCEL_CLUSTERS, 9)
+    assert lib.rt_lbvh_build(C.byref(d), None) == 6  # RT_ERR_UNSUPPORTED
+    d.params = _abi.BuildParams(12, 1, 0, 0, 32, _abi.ACCEL_CLUSTERS, 3)
+    assert lib.rt_lbvh_build(C.byref(d), None) == 2  # everything else in order: only the missing device stops it
+    M, N = 4, 40000
+    params = _abi.BuildParams(12, 1, 0, 0, 32, _abi.ACCEL_CLUSTERS, 9)
+    sb, ab = C.c_size_t(0), C.c_size_t(0)
+    assert lib.rt_batch_sizes(M, N, C.byref(params), C.byref(sb), C.byref(ab)) == 0
+    b = _abi.BatchBuildDesc()
+    b.mesh_count, b.face_count, b.vertex_count = M, N, 3 * N
+    b.face_offsets = b.vertex_offsets = b.vertices = b.faces_in = b.boxes = b.indices = b.codes = b.nodes = b.tris = FAKE
+    b.faces_out = FAKE + 4096
+    b.accel, b.info, b.scratch = FAKE, FAKE, FAKE
+    b.params = params
+    b.accel_bytes, b.scratch_bytes = ab.value, sb.value
+    assert lib.rt_batch_build(C.byref(b), None) == 6
+    assert lib.rt_batch_primary_rays(None, 4, 8, 8, C.c_void_p(FAKE), C.c_void_p(FAKE), None) == 1
+    assert lib.rt_batch_primary_rays(C.c_void_p(FAKE), 4, 0, 8, C.c_void_p(FAKE), C.c_void_p(FAKE), None) == 1
+    assert lib.rt_batch_primary_rays(C.c_void_p(FAKE), 1 << 12, 1 << 10, 1 << 10, C.c_void_p(FAKE), C.c_void_p(FAKE), None) == 1
+    assert lib.rt_batch_primary_rays(C.c_void_p(FAKE), 0, 8, 8, None, None, None) == 0  # nothing to make
+
+
 @pytest.mark.gpu
 def test_bounded_wait_runs_out_and_returns():
     import torch
