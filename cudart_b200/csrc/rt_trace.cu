@@ -1092,16 +1092,23 @@ __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, con
 }
 
 // Per-lane cluster walks in warps that refill idle lanes: a lane whose ray is
-// done (or was inactive) waits until `threshold` lanes of its warp are idle,
-// then the warp takes that many new rays with one atomic and every lane steps
-// its own walk again, so a warp no longer waits for its slowest ray. `start`
-// maps a slot to a ray and its mesh: false for a slot without a ray.
-template <bool kCount, bool kWW, class Start>
+// done waits until `threshold` lanes of its warp are idle, then those lanes
+// take the next rays of the warp's queue and every lane steps its own walk
+// again, so a warp no longer waits for its slowest ray. The queue (64 entries
+// of shared memory per warp) holds active rays only: the warp takes 32 slots
+// at a time with one atomic, reads their tmax together, writes the inactive
+// ones (tmax <= 0) as misses at once and appends the others in slot order.
+// `slot_ray` maps a slot to a ray (false for a slot without one); `mesh_args`
+// sets the cluster-tree arguments of an active ray's mesh.
+constexpr uint32_t kRefillQueue = 64;
+template <bool kCount, bool kWW, class SlotRay, class MeshArgs>
 __device__ __forceinline__ void refill_walks(const TraceArgs& A, uint32_t* counter, const uint32_t slots, const uint32_t threshold,
-                                             const Start& start) {
+                                             uint32_t* q_ray, float* q_tmax, const SlotRay& slot_ray, const MeshArgs& mesh_args) {
   const uint32_t lane = lane_id();
+  const uint32_t below = (1u << lane) - 1u;
   const uint32_t need = threshold ? min(threshold, 32u) : 16u;
   bool busy = false, exhausted = false;
+  uint32_t q_head = 0, q_count = 0;  // warp-uniform
   uint32_t r = 0, ref = 0, visits = 0, tests = 0;
   int32_t best = -1;
   float4 o = make_float4(0.f, 0.f, 0.f, 0.f), d = o, oi = o;
@@ -1121,36 +1128,69 @@ __device__ __forceinline__ void refill_walks(const TraceArgs& A, uint32_t* count
   };
   for (;;) {
     const uint32_t idle = __ballot_sync(0xffffffffu, !busy);
-    if (!exhausted && (uint32_t)__popc(idle) >= need) {
-      uint32_t base = 0;
-      if (lane == 0) base = atomicAdd(counter, (uint32_t)__popc(idle));
-      base = __shfl_sync(0xffffffffu, base, 0);
-      if (base + (uint32_t)__popc(idle) >= slots) exhausted = true;
-      const uint32_t slot = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
-      if (!busy && slot < slots && start(slot, r, C)) {
-        tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
+    const uint32_t n_idle = (uint32_t)__popc(idle);
+    if (n_idle >= need && (q_count || !exhausted)) {
+      // top the queue up to n_idle rays (it never holds more than 31 + 32)
+      while (q_count < n_idle && !exhausted) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(counter, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= slots || slots - base <= 32u) exhausted = true;
+        const uint32_t slot = base + lane;
+        uint32_t sr = 0;
+        float st = 0.0f;
+        bool act = false;
+        if (slot < slots && slot_ray(slot, sr)) {
+          st = A.tmax ? __ldg(A.tmax + sr) : kHuge;
+          if (st > 0.0f) {
+            act = true;
+          } else {
+            write_hit(sr, A, 0, -1, 0.0f, 0.0f, 0.0f, st);  // an inactive ray: a miss at once
+            if (kCount) {
+              if (A.visits) A.visits[sr] = 0;
+              if (A.tests) A.tests[sr] = 0;
+            }
+          }
+        }
+        const uint32_t am = __ballot_sync(0xffffffffu, act);
+        if (act) {
+          const uint32_t e = (q_head + q_count + (uint32_t)__popc(am & below)) & (kRefillQueue - 1u);
+          q_ray[e] = sr;
+          q_tmax[e] = st;
+        }
+        q_count += (uint32_t)__popc(am);
+      }
+      __syncwarp();
+      const uint32_t take = min(q_count, n_idle);
+      const uint32_t k = (uint32_t)__popc(idle & below);
+      if (!busy && k < take) {
+        const uint32_t e = (q_head + k) & (kRefillQueue - 1u);
+        r = q_ray[e];
+        tmax0 = q_tmax[e];
+        mesh_args(r, C);
         best = -1;
         bt = tmax0; bu = bv = 0.0f;
         visits = tests = 0;
-        if (tmax0 > 0.0f) {
-          if (cluster_tree_ok(C, ref)) {
-            o = ldg4(A.orig + r);
-            d = ldg4(A.dir + r);
-            ix = 1.0f / fix_dir(d.x); iy = 1.0f / fix_dir(d.y); iz = 1.0f / fix_dir(d.z);
-            oi = scaled_origin(o, ix, iy, iz);
-            zu = o.w * 0.0f; zv = d.w * 0.0f;
-            sp = 0;
-            steps = 0;
-            busy = true;
-          } else if (A.err) {
-            atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
-          }
+        if (cluster_tree_ok(C, ref)) {
+          o = ldg4(A.orig + r);
+          d = ldg4(A.dir + r);
+          ix = 1.0f / fix_dir(d.x); iy = 1.0f / fix_dir(d.y); iz = 1.0f / fix_dir(d.z);
+          oi = scaled_origin(o, ix, iy, iz);
+          zu = o.w * 0.0f; zv = d.w * 0.0f;
+          sp = 0;
+          steps = 0;
+          busy = true;
+        } else {
+          if (A.err) atomicOr(A.err, (uint32_t)RT_DEVERR_ACCEL_MISSING);
+          finish();  // no cluster tree: a miss
         }
-        if (!busy) finish();  // an inactive ray (or no cluster tree): a miss at once
       }
+      __syncwarp();
+      q_head = (q_head + take) & (kRefillQueue - 1u);
+      q_count -= take;
     }
     if (!__any_sync(0xffffffffu, busy)) {
-      if (exhausted) break;
+      if (exhausted && !q_count) break;
       continue;
     }
     if (!busy) continue;
@@ -1453,11 +1493,13 @@ __global__ __launch_bounds__(128) void k_trace_clusters_packet(TraceArgs A, Clus
 template <bool kCount, bool kWW>
 __global__ __launch_bounds__(128) void k_trace_clusters_refill(TraceArgs A, ClusterArgs C, SlotMap M, uint32_t* counter,
                                                                 uint32_t threshold) {
+  __shared__ uint32_t q_ray[4][kRefillQueue];
+  __shared__ float q_tmax[4][kRefillQueue];
   C.F = 0;
-  refill_walks<kCount, kWW>(A, counter, M.slots, threshold, [&](uint32_t slot, uint32_t& r, ClusterArgs& Cl) {
-    Cl = C;
-    return M.ray_of(slot, r);
-  });
+  const uint32_t w = threadIdx.x >> 5;
+  refill_walks<kCount, kWW>(
+      A, counter, M.slots, threshold, q_ray[w], q_tmax[w], [&](uint32_t slot, uint32_t& r) { return M.ray_of(slot, r); },
+      [&](uint32_t, ClusterArgs& Cl) { Cl = C; });
 }
 
 __device__ __forceinline__ void batch_cluster_args(uint32_t r, const BatchTraceArgs& B, ClusterArgs& C) {
@@ -1498,12 +1540,19 @@ __global__ __launch_bounds__(128) void k_batch_trace_clusters_persistent(TraceAr
 template <bool kCount, bool kWW>
 __global__ __launch_bounds__(128) void k_batch_trace_clusters_refill(TraceArgs A, BatchTraceArgs B, uint32_t* counter,
                                                                       uint32_t threshold) {
-  refill_walks<kCount, kWW>(A, counter, A.ray_count, threshold, [&](uint32_t slot, uint32_t& r, ClusterArgs& C) {
-    r = B.ray_of(slot);
-    C.crec = B.acc.crec;
-    batch_cluster_args(r, B, C);
-    return true;
-  });
+  __shared__ uint32_t q_ray[4][kRefillQueue];
+  __shared__ float q_tmax[4][kRefillQueue];
+  const uint32_t w = threadIdx.x >> 5;
+  refill_walks<kCount, kWW>(
+      A, counter, A.ray_count, threshold, q_ray[w], q_tmax[w],
+      [&](uint32_t slot, uint32_t& r) {
+        r = B.ray_of(slot);
+        return true;
+      },
+      [&](uint32_t r, ClusterArgs& C) {
+        C.crec = B.acc.crec;
+        batch_cluster_args(r, B, C);
+      });
 }
 
 // Packet walks over batched rays: a warp whose valid rays all belong to one mesh walks it as a packet; a warp

@@ -311,7 +311,9 @@ typedef struct rt_trace_desc {
 #define RT_TRACE_PACKET 0x10u  /* with RT_TRACE_CLUSTERS and a work_counter: each warp walks the cluster tree as one packet
                                   (one node sequence for its 32 rays; for coherent rays such as 8 x 4 pixel tiles) */
 #define RT_TRACE_REFILL 0x20u  /* with RT_TRACE_CLUSTERS and a work_counter: per-lane walks in which a warp takes new rays
-                                  for its idle lanes (lane_threshold of them, 0 = 16) instead of waiting for its slowest ray */
+                                  for its idle lanes (lane_threshold of them, 0 = 16) instead of waiting for its slowest ray;
+                                  it claims 32 slots per atomic, writes the inactive ones (tmax <= 0) as misses at once and
+                                  queues the active ones for its lanes */
 
 /* A tracing order for incoherent rays: ray indices sorted by direction octant,
  * then by the Morton code of the origin inside box (min xyz, max xyz, HOST);
