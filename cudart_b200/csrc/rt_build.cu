@@ -55,7 +55,11 @@ __global__ void k_set_hitbox(float4* hit, float4 mn, float4 mx) {
   hit[1] = mx;
 }
 
-__global__ __launch_bounds__(256) void k_hitbox_partial(const float4* __restrict__ v, uint32_t count, float4* __restrict__ partial) {
+// Hit box over all vertices: each block reduces its grid-stride share to a partial box; the block that finishes
+// last (a counter the host zeroes) combines the partials, strided over its threads and then as a shared-memory
+// tree, and writes hit[0..1]. Nothing waits for it inside the launch.
+__global__ __launch_bounds__(256) void k_hitbox(const float4* __restrict__ v, uint32_t count, float4* __restrict__ partial,
+                                               uint32_t* __restrict__ done, float4* __restrict__ hit) {
   // four loads in flight per thread, one accumulator each
   float4 mn[4], mx[4];
 #pragma unroll
@@ -81,6 +85,7 @@ __global__ __launch_bounds__(256) void k_hitbox_partial(const float4* __restrict
     mx[0] = f4max(mx[0], p);
   }
   __shared__ float4 s_mn[256], s_mx[256];
+  __shared__ uint32_t s_last;
   s_mn[threadIdx.x] = f4min(f4min(mn[0], mn[1]), f4min(mn[2], mn[3]));
   s_mx[threadIdx.x] = f4max(f4max(mx[0], mx[1]), f4max(mx[2], mx[3]));
   __syncthreads();
@@ -94,19 +99,19 @@ __global__ __launch_bounds__(256) void k_hitbox_partial(const float4* __restrict
   if (threadIdx.x == 0) {
     partial[2 * blockIdx.x] = s_mn[0];
     partial[2 * blockIdx.x + 1] = s_mx[0];
+    __threadfence();
+    s_last = atomicAdd(done, 1u) == gridDim.x - 1 ? 1u : 0u;
   }
-}
-
-__global__ __launch_bounds__(256) void k_hitbox_final(const float4* __restrict__ partial, uint32_t parts, float4* __restrict__ hit) {
-  // one block: strided accumulation, then a shared-memory tree
-  float4 mn = make_float4(kHuge, kHuge, kHuge, kHuge), mx = make_float4(-kHuge, -kHuge, -kHuge, -kHuge);
-  for (uint32_t i = threadIdx.x; i < parts; i += blockDim.x) {
-    mn = f4min(mn, partial[2 * i]);
-    mx = f4max(mx, partial[2 * i + 1]);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  float4 a = make_float4(kHuge, kHuge, kHuge, kHuge), b = make_float4(-kHuge, -kHuge, -kHuge, -kHuge);
+  for (uint32_t j = threadIdx.x; j < gridDim.x; j += blockDim.x) {
+    a = f4min(a, __ldcg(partial + 2 * j));
+    b = f4max(b, __ldcg(partial + 2 * j + 1));
   }
-  __shared__ float4 s_mn[256], s_mx[256];
-  s_mn[threadIdx.x] = mn;
-  s_mx[threadIdx.x] = mx;
+  s_mn[threadIdx.x] = a;
+  s_mx[threadIdx.x] = b;
   __syncthreads();
   for (int o = 128; o > 0; o >>= 1) {
     if (threadIdx.x < o) {
@@ -685,7 +690,7 @@ size_t carve_build(Carve& c, BuildLayout& L, uint32_t n, uint32_t D, bool need_c
   L.err = c.take<uint32_t>(4);
   L.leaf_lambda = c.take<uint32_t>(L.max_nodes);
   L.faces_tmp = need_faces_tmp ? c.take<uint4>(n) : nullptr;
-  L.counts = c.take<uint32_t>(5 * 256);
+  L.counts = c.take<uint32_t>(5 * 256 + 1);  // digit counts of the code and level sorts, then the hit box's block counter
   L.ct = ClusterTemps{};
   if (clusters) carve_cluster_temps(c, L.ct, n, 1);
   return c.off + 256;
@@ -803,20 +808,19 @@ extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
   uint32_t* codes = d->codes ? d->codes : L.codes;
   const int sms = sm_count();
 
-  // 1. hit box
+  // 1. hit box (the sorts' digit counts and the hit box's block counter start at zero)
+  if (cudaMemsetAsync(L.counts, 0, (5 * 256 + 1) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   if (d->hitbox) {
     float4 mn = make_float4(d->hitbox[0], d->hitbox[1], d->hitbox[2], d->hitbox[3]);
     float4 mx = make_float4(d->hitbox[4], d->hitbox[5], d->hitbox[6], d->hitbox[7]);
     k_set_hitbox<<<1, 1, 0, st>>>(L.hit, mn, mx);
     note_launch();
   } else {
-    k_hitbox_partial<<<kHitParts, 256, 0, st>>>((const float4*)d->vertices, d->vertex_count, L.partial);
-    k_hitbox_final<<<1, 256, 0, st>>>(L.partial, kHitParts, L.hit);
-    note_launch(2);
+    k_hitbox<<<kHitParts, 256, 0, st>>>((const float4*)d->vertices, d->vertex_count, L.partial, L.counts + 5 * 256, L.hit);
+    note_launch();
   }
   RT_CHECK_LAUNCH();
   // 2. boxes, indices, codes (and the digit counts of both sorts, counted by the kernels that make the keys)
-  if (cudaMemsetAsync(L.counts, 0, 5 * 256 * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   {
     uint32_t blocks = (uint32_t)hmin<uint64_t>((n + 255) / 256, (uint64_t)sms * 16);
     k_boxes_morton<<<blocks, 256, 0, st>>>((const float4*)d->vertices, (const uint4*)d->faces_in, n, L.hit, (int)q.morton_bits,
@@ -950,6 +954,7 @@ struct BatchArgs {
   // scratch
   float4* hits;           // [2M]
   float4* hitpart;        // [2 M kHitSplit]: the hit box shares of k_batch_hitbox
+  uint32_t* hitdone;      // [M]: finished shares per mesh
   uint32_t* idx;          // [N] global face index in sorted order
   uint32_t* codes_raw;    // [N] codes before sorting
   uint32_t* mkey;         // [N] mesh id per position
@@ -983,7 +988,7 @@ struct BatchArgs {
 // Per-mesh hitbox: one 512-thread block per mesh, four loads in flight per
 // thread (the largest meshes bound the launch).
 __global__ __launch_bounds__(512) void k_batch_hitbox(BatchArgs B) {
-  // kHitSplit CTAs per mesh, each over its share of the mesh's vertices; k_batch_hitfinal combines the shares
+  // kHitSplit CTAs per mesh, each over its share of the mesh's vertices; the last of them combines the shares
   const uint32_t m = blockIdx.x / kHitSplit, part = blockIdx.x % kHitSplit;
   const uint32_t w0 = B.voff[m], w1 = B.voff[m + 1], share = (w1 - w0 + kHitSplit - 1) / kHitSplit;
   const uint32_t v0 = min(w1, w0 + part * share), v1 = min(w1, v0 + share);
@@ -1030,19 +1035,20 @@ __global__ __launch_bounds__(512) void k_batch_hitbox(BatchArgs B) {
   if (threadIdx.x == 0) {
     B.hitpart[2 * (size_t)blockIdx.x] = s_mn[0];
     B.hitpart[2 * (size_t)blockIdx.x + 1] = s_mx[0];
+    __threadfence();
+    // the mesh's last share to finish combines its kHitSplit shares in share order (an empty share holds +-huge
+    // and changes nothing); nothing waits for it inside the launch
+    if (atomicAdd(B.hitdone + m, 1u) == kHitSplit - 1) {
+      __threadfence();
+      float4 a = __ldcg(B.hitpart + 2 * (size_t)m * kHitSplit), b = __ldcg(B.hitpart + 2 * (size_t)m * kHitSplit + 1);
+      for (uint32_t p = 1; p < kHitSplit; ++p) {
+        a = f4min(a, __ldcg(B.hitpart + 2 * ((size_t)m * kHitSplit + p)));
+        b = f4max(b, __ldcg(B.hitpart + 2 * ((size_t)m * kHitSplit + p) + 1));
+      }
+      B.hits[2 * m] = a;
+      B.hits[2 * m + 1] = b;
+    }
   }
-}
-// Each mesh's hit box from its kHitSplit shares (an empty share holds +-huge and changes nothing).
-__global__ __launch_bounds__(128) void k_batch_hitfinal(BatchArgs B) {
-  const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= B.M) return;
-  float4 mn = B.hitpart[2 * (size_t)m * kHitSplit], mx = B.hitpart[2 * (size_t)m * kHitSplit + 1];
-  for (uint32_t p = 1; p < kHitSplit; ++p) {
-    mn = f4min(mn, B.hitpart[2 * ((size_t)m * kHitSplit + p)]);
-    mx = f4max(mx, B.hitpart[2 * ((size_t)m * kHitSplit + p) + 1]);
-  }
-  B.hits[2 * m] = mn;
-  B.hits[2 * m + 1] = mx;
 }
 
 __global__ __launch_bounds__(256) void k_batch_boxes_morton(BatchArgs B) {
@@ -1243,6 +1249,7 @@ __global__ __launch_bounds__(256) void k_batch_records(BatchArgs B) {
 size_t carve_batch(Carve& c, BatchArgs& B, uint32_t M, uint32_t N, bool clusters) {
   B.hits = c.take<float4>(2 * (size_t)M);
   B.hitpart = c.take<float4>(2 * (size_t)M * kHitSplit);
+  B.hitdone = c.take<uint32_t>(M);
   B.idx = c.take<uint32_t>(N);
   B.codes_raw = c.take<uint32_t>(N);
   B.mkey = c.take<uint32_t>(N);
@@ -1327,10 +1334,10 @@ extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stre
   if (cudaMemsetAsync(B.err, 0, 16, st) != cudaSuccess) return RT_ERR_CUDA;
   if (cudaMemsetAsync(B.counts, 0, (9 * 256 + 64) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   if (cudaMemsetAsync(B.hist, 0, ((size_t)M * 64 + 1) * 4, st) != cudaSuccess) return RT_ERR_CUDA;
+  if (cudaMemsetAsync(B.hitdone, 0, (size_t)M * 4, st) != cudaSuccess) return RT_ERR_CUDA;
   k_batch_hitbox<<<M * kHitSplit, 512, 0, st>>>(B);
-  k_batch_hitfinal<<<(M + 127) / 128, 128, 0, st>>>(B);
   k_batch_boxes_morton<<<fblocks, 256, 0, st>>>(B);
-  note_launch(3);
+  note_launch(2);
   RT_CHECK_LAUNCH();
   // Morton order of all faces; its last pass also writes each position's mesh (the key of the next sort)
   rt_status s = radix_sort_pairs(B.codes, B.idx, N, 0, 32, 0, sort_scratch, sort_bytes, st, nullptr, B.err, B.counts, B.foff, M,
