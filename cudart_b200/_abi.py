@@ -29,6 +29,7 @@ TRACE_CLUSTERS = 0x8
 TRACE_PACKET = 0x10
 TRACE_REFILL = 0x20
 ACCEL_CLUSTERS = 0x2
+MAX_RAYS = 0x7FFFFFFF  # RT_MAX_RAYS: the most rays one trace call takes
 
 # every symbol include/rt_core.h declares
 EXPORTS = (

@@ -1963,6 +1963,7 @@ rt_status trace_args(const rt_trace_desc* d, TraceArgs& A) {
   if (!d || !d->nodes || !d->orig || !d->dir || !d->hit_id || !d->hit_t || !d->hit_uv) return RT_ERR_INVALID_ARGUMENT;
   if (!d->tris && (!d->vertices || !d->faces)) return RT_ERR_INVALID_ARGUMENT;
   if (d->id_mode == 1 && !d->indices) return RT_ERR_INVALID_ARGUMENT;
+  if (d->ray_count > RT_MAX_RAYS) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   A.nodes = (const uint4*)d->nodes; A.tris = (const float4*)d->tris; A.verts = (const float4*)d->vertices;
   A.faces = (const uint4*)d->faces; A.indices = d->indices; A.orig = (const float4*)d->orig; A.dir = (const float4*)d->dir;
@@ -2245,6 +2246,7 @@ rt_status batch_check(const rt_batch_trace_desc* d) {
       !d->hit_id || !d->hit_t || !d->hit_uv || d->face_count < d->mesh_count)
     return RT_ERR_INVALID_ARGUMENT;
   if (d->id_mode == 1 && !d->indices) return RT_ERR_INVALID_ARGUMENT;
+  if (d->ray_count > RT_MAX_RAYS) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   return RT_OK;
 }

@@ -178,7 +178,7 @@ typedef struct rt_batch_trace_desc {
   const float* orig;
   const float* dir;
   const float* tmax;              /* optional */
-  uint32_t ray_count;
+  uint32_t ray_count;             /* at most RT_MAX_RAYS */
   uint32_t id_mode;
   int32_t* hit_id;
   float* hit_t;
@@ -280,7 +280,7 @@ typedef struct rt_trace_desc {
   const float* orig;        /* float4[ray_count] */
   const float* dir;         /* float4[ray_count] */
   const float* tmax;        /* float[ray_count] initial depth; NULL = CUDART_NORM_HUGE_F. A ray with tmax <= 0 misses. */
-  uint32_t ray_count;
+  uint32_t ray_count;       /* at most RT_MAX_RAYS */
   uint32_t id_mode;         /* 0: position in the reordered faces (the reference's faces_id); 1: original face id */
   int32_t* hit_id;          /* out: -1 on a miss */
   float* hit_t;             /* out: t of the hit, or tmax on a miss (may alias tmax, as CUDABuffer depths do) */
@@ -302,6 +302,10 @@ typedef struct rt_trace_desc {
                                once fewer than this many lanes still want the node it is at (0: never);
                                RT_TRACE_REFILL: a warp fetches new rays for its idle lanes once this many are idle */
 } rt_trace_desc;
+
+/* The most rays one trace call takes (2^31 - 1, 64 GB of origins and directions): the persistent schedules' slot
+   counters then never wrap. A larger ray_count is refused with RT_ERR_INVALID_ARGUMENT before any launch. */
+#define RT_MAX_RAYS 0x7FFFFFFFu
 
 #define RT_TRACE_WHILE_WHILE 0x1u /* descend until a leaf is held, then test it (else: interleaved) */
 #define RT_TRACE_COOP 0x2u        /* the warp's lanes share the triangle tests of all its rays' leaves */

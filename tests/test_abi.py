@@ -69,6 +69,26 @@ def test_invalid_arguments_rejected():
     assert lib.rt_reorder_faces(C.c_void_p(4096), C.c_void_p(64), 100, C.c_void_p(4096 + 16), None) == 1  # overlap
 
 
+def test_ray_count_above_limit_refused():
+    """More than RT_MAX_RAYS rays is refused before the device check (single and batched traces); the limit itself
+    passes the argument checks, so only the missing device stops it."""
+    from cudart_b200 import _abi
+    lib = _abi.lib()
+    desc = _abi.TraceDesc()
+    desc.nodes = desc.orig = desc.dir = desc.hit_id = desc.hit_t = desc.hit_uv = desc.tris = 16  # never dereferenced
+    desc.ray_count = _abi.MAX_RAYS + 1
+    assert lib.rt_trace_closest(C.byref(desc), None) == 1
+    desc.ray_count = _abi.MAX_RAYS
+    assert lib.rt_trace_closest(C.byref(desc), None) == 2
+    b = _abi.BatchTraceDesc()
+    b.mesh_count, b.face_count = 2, 8
+    b.face_offsets = b.ray_offsets = b.accel = b.tris = b.orig = b.dir = b.hit_id = b.hit_t = b.hit_uv = 16
+    b.ray_count = 0xFFFFFFFF
+    assert lib.rt_batch_trace(C.byref(b), None) == 1
+    b.ray_count = _abi.MAX_RAYS
+    assert lib.rt_batch_trace(C.byref(b), None) == 2
+
+
 def test_scratch_queries():
     from cudart_b200 import core
     nb, mx = core.lbvh_scratch_bytes(1 << 20)
