@@ -1239,18 +1239,27 @@ __device__ __forceinline__ void refill_walks(const TraceArgs& A, uint32_t* count
     }
     if (!kWW && !was_cluster) continue;  // if-if: a step is one record or one cluster
     {
-      const float4* tris = A.tris + 3 * (size_t)C.F;
-      const uint32_t p0 = ref & kClusterFirstMask, p1 = p0 + ((ref >> 28) & 7u) + 1u;
-      for (uint32_t pos = p0; pos < p1; ++pos) {
-        const float4 v0 = ldg4(tris + 3 * (size_t)pos);
-        const float4 e1 = ldg4(tris + 3 * (size_t)pos + 1);
-        const float4 e2 = ldg4(tris + 3 * (size_t)pos + 2);
+      // the cluster's triangles in position order; the next triangle's loads are issued before the test of the one
+      // at hand, so a cluster of two or three waits for memory once
+      const float4* tp = A.tris + 3 * ((size_t)C.F + (ref & kClusterFirstMask));
+      const uint32_t p0 = ref & kClusterFirstMask, cnt = ((ref >> 28) & 7u) + 1u;
+      auto test_tri = [&](const float4& v0, const float4& e1, const float4& e2, uint32_t pos) {
         if (kCount) ++tests;
         float th, u, v;
-        if (!mt_test(o, d, zu, zv, v0, e1, e2, th, u, v)) continue;
-        if (th < bt || (best >= 0 && th == bt && (int32_t)pos < best)) {
+        if (mt_test(o, d, zu, zv, v0, e1, e2, th, u, v) && (th < bt || (best >= 0 && th == bt && (int32_t)pos < best))) {
           best = (int32_t)pos; bt = th; bu = u; bv = v;
         }
+      };
+      float4 a0 = ldg4(tp), a1 = ldg4(tp + 1), a2 = ldg4(tp + 2);
+      float4 b0 = a0, b1 = a1, b2 = a2;
+      if (cnt > 1) { b0 = ldg4(tp + 3); b1 = ldg4(tp + 4); b2 = ldg4(tp + 5); }
+      test_tri(a0, a1, a2, p0);
+      for (uint32_t i = 1; i < cnt; i += 2) {
+        if (i + 1 < cnt) { a0 = ldg4(tp + 3 * i + 3); a1 = ldg4(tp + 3 * i + 4); a2 = ldg4(tp + 3 * i + 5); }
+        test_tri(b0, b1, b2, p0 + i);
+        if (i + 1 >= cnt) break;
+        if (i + 2 < cnt) { b0 = ldg4(tp + 3 * i + 6); b1 = ldg4(tp + 3 * i + 7); b2 = ldg4(tp + 3 * i + 8); }
+        test_tri(a0, a1, a2, p0 + i + 1);
       }
     }
     if (!pop_within(st_ref, st_t, sp, bt, ref)) finish();
@@ -1490,8 +1499,10 @@ __global__ __launch_bounds__(128) void k_trace_clusters_packet(TraceArgs A, Clus
   }
 }
 
+// Refill walks are latency-bound: eight CTAs (32 warps) per SM, 64 registers, outrun seven CTAs at the 72 registers
+// the compiler would take for the pipelined triangle loads.
 template <bool kCount, bool kWW>
-__global__ __launch_bounds__(128) void k_trace_clusters_refill(TraceArgs A, ClusterArgs C, SlotMap M, uint32_t* counter,
+__global__ __launch_bounds__(128, 8) void k_trace_clusters_refill(TraceArgs A, ClusterArgs C, SlotMap M, uint32_t* counter,
                                                                 uint32_t threshold) {
   __shared__ uint32_t q_ray[4][kRefillQueue];
   __shared__ float q_tmax[4][kRefillQueue];
@@ -1538,7 +1549,7 @@ __global__ __launch_bounds__(128) void k_batch_trace_clusters_persistent(TraceAr
   }
 }
 template <bool kCount, bool kWW>
-__global__ __launch_bounds__(128) void k_batch_trace_clusters_refill(TraceArgs A, BatchTraceArgs B, uint32_t* counter,
+__global__ __launch_bounds__(128, 8) void k_batch_trace_clusters_refill(TraceArgs A, BatchTraceArgs B, uint32_t* counter,
                                                                       uint32_t threshold) {
   __shared__ uint32_t q_ray[4][kRefillQueue];
   __shared__ float q_tmax[4][kRefillQueue];
