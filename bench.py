@@ -251,22 +251,29 @@ def run_headline(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
+    # the primary call also writes the bounce rays (the packet walk, as each ray finishes) unless the bounce
+    # schedule reads the generator's order; then the bounces are a stage of their own
+    fused = not w.bounce_needs_order()
+
     def trace1():
-        core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, out=plain["h1"], schedule=s1)
+        if fused:
+            w.primary(plain["h1"], plain["b"])
+        else:
+            core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, out=plain["h1"], schedule=s1)
 
     def trace2():
         b = plain["b"]
         core.batch_trace(w.tree, b[0], b[1], w.ray_offsets, tmax=b[2], out=plain["h2"], schedule=s2, order=w.bounce_order(b))
 
     aux = torch.cuda.Stream()  # the primary rays run beside the build (they do not depend on it)
-    stages = [lambda: w.build_and_rays(aux=aux), trace1, lambda: w.bounce(plain["h1"], out=plain["b"]), trace2]
+    stages = [lambda: w.build_and_rays(aux=aux), trace1] + ([] if fused else [lambda: w.bounce(plain["h1"], out=plain["b"])]) + [trace2]
     graphs, kernels_per_step = capture_graphs(stages)
     active = torch.zeros(1, dtype=torch.int64, device=dev)
 
     def step(frame, timed_list=None):
         w.displace(frame)  # the frame's input (outside the events)
         flush.zero_()  # L2 flush between frames (outside the events)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(graphs) + 1)]
         ev[0].record(stream)
         for i, g in enumerate(graphs):
             g.replay()
@@ -290,11 +297,11 @@ def run_headline(args, rank, world, local_rank):
         torch.cuda.synchronize()
     sampler.stop()
     K = args.steps
-    frame_ms = sum(e[0].elapsed_time(e[4]) for e in evs)
+    frame_ms = sum(e[0].elapsed_time(e[-1]) for e in evs)
     build_ms = sum(e[0].elapsed_time(e[1]) for e in evs)  # the build, with the primary rays made beside it
-    t1_ms = sum(e[1].elapsed_time(e[2]) for e in evs)
-    bounce_gen_ms = sum(e[2].elapsed_time(e[3]) for e in evs)
-    t2_ms = sum(e[3].elapsed_time(e[4]) for e in evs)
+    t1_ms = sum(e[1].elapsed_time(e[2]) for e in evs)  # the primary trace (with the bounce rays when fused)
+    bounce_gen_ms = 0.0 if fused else sum(e[2].elapsed_time(e[3]) for e in evs)
+    t2_ms = sum(e[-2].elapsed_time(e[-1]) for e in evs)
     frame_ms, build_ms, t1_ms, bounce_gen_ms, t2_ms = max_over_ranks([frame_ms, build_ms, t1_ms, bounce_gen_ms, t2_ms], world, dev)
     rays_total = K * R + int(active.item())
     value = world * rays_total / (frame_ms * 1e-3) / 1e6
@@ -346,10 +353,12 @@ def run_headline(args, rank, world, local_rank):
     legs = {"c4_tuning": {"primary_ms": {json.dumps(k, sort_keys=True): round(v, 3) for k, v in tim1},
                           "bounce_ms": {json.dumps(k, sort_keys=True): round(v, 3) for k, v in tim2}},
             "c4_detail": {"workload": WORKLOAD, "schedule_primary": s1, "schedule_bounce": s2, "counted_identical": bool(same), "device_errors": dev_errors,
-                          "nodes": nodes_total, "build_bytes": int(build_bytes), "bounce_rays_ms": round(bounce_gen_ms / K, 3),
+                          "nodes": nodes_total, "build_bytes": int(build_bytes),
+                          "bounce_rays_ms": "in the primary trace" if fused else round(bounce_gen_ms / K, 3),
                           "primary_hits_last": hits1, "active_bounces_last": active_last, "kernels_per_frame": kernels_per_step,
-                          "graphs": "4 CUDA graph replays per frame: build with the primary rays made beside it (one "
-                                    "rt_batch_primary_rays launch on a second stream), trace, bounce rays, trace",
+                          "graphs": (f"{len(stages)} CUDA graph replays per frame: build with the primary rays made beside it (one "
+                                     "rt_batch_primary_rays launch on a second stream), trace"
+                                     + (" writing the bounce rays, trace" if fused else ", bounce rays, trace")),
                           "roofline": roof}}
     del graphs
     # learned proposal on the same frames (fine-tuning, grouped proposals + seeded traversal), hits bit for bit
@@ -474,8 +483,7 @@ def run_e2e(w, args, dev, world, s1, s2):
     def compute(s):
         w.build_and_rays(v[s], aux=aux)
         o = outs[s]
-        core.batch_trace(w.tree, w.orig, w.dir, w.ray_offsets, out=o["h1"], schedule=s1)
-        w.bounce(o["h1"], out=o["b"])
+        w.primary(o["h1"], o["b"])
         core.batch_trace(w.tree, o["b"][0], o["b"][1], w.ray_offsets, tmax=o["b"][2], out=o["h2"], schedule=s2,
                          order=w.bounce_order(o["b"]))
 

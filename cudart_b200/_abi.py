@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librt_core.so")
 
 RT_OK = 0
-ABI_VERSION = 9  # RT_ABI_VERSION of include/rt_core.h that the structs below mirror
+ABI_VERSION = 10  # RT_ABI_VERSION of include/rt_core.h that the structs below mirror
 STATUS_NAMES = {0: "RT_OK", 1: "RT_ERR_INVALID_ARGUMENT", 2: "RT_ERR_NO_DEVICE", 3: "RT_ERR_CUDA",
                 4: "RT_ERR_SCRATCH_TOO_SMALL", 5: "RT_ERR_CAPACITY", 6: "RT_ERR_UNSUPPORTED"}
 DEVERR_NODE_CAPACITY = 0x1
@@ -114,7 +114,7 @@ class BatchTraceDesc(C.Structure):
                 ("face_count", _U32), ("orig", _P), ("dir", _P), ("tmax", _P), ("ray_count", _U32), ("id_mode", _U32),
                 ("hit_id", _P), ("hit_t", _P), ("hit_uv", _P), ("ray_visits", _P), ("ray_tests", _P), ("error_word", _P),
                 ("schedule", _U32), ("work_counter", _P), ("persistent_blocks_per_sm", _U32), ("ray_order", _P),
-                ("lane_threshold", _U32)]
+                ("lane_threshold", _U32), ("bounce_seed", C.c_uint64), ("bounce_orig", _P), ("bounce_dir", _P), ("bounce_tmax", _P)]
 
 
 class SahDesc(C.Structure):

@@ -669,7 +669,8 @@ def batch_ray_order(orig, dir, tmax, ray_offsets, mesh_count: int, box, morton_b
 
 
 def batch_trace(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax=None, id_mode: int = 0, counters: bool = False,
-                while_while: bool = True, out: dict | None = None, schedule: dict | None = None, order=None, stream=None) -> dict:
+                while_while: bool = True, out: dict | None = None, schedule: dict | None = None, order=None, stream=None,
+                bounce=None) -> dict:
     """Closest hits for the rays of all meshes (rays of mesh m: ray_offsets[m] .. ray_offsets[m+1]).
     schedule (results never depend on it): while_while, wide (4-wide records),
     persistent + blocks_per_sm (warps fetching 32 rays at a time), coop
@@ -677,8 +678,20 @@ def batch_trace(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax=None
     height) (every mesh's rays are one image: warps take 8 x 4 pixel tiles) or
     sorted_bits (rays sorted by mesh, octant and that many bits of their
     origin's Morton code, inactive rays last; the sort is part of the call). `order`: a tracing order given by
-    the caller (for instance batch_bounce_rays' order), used in place of the schedule's."""
+    the caller (for instance batch_bounce_rays' order), used in place of the schedule's. `bounce`: (seed, None or
+    three tensors) to get each ray's diffuse bounce too, exactly as batch_bounce_rays(..., seed) makes it from these
+    hits, as out["b"] = (orig, dir, tmax); the packet schedule writes them as each ray finishes (no second pass
+    over the hits)."""
     d, out = batch_trace_desc(tree, orig, dir, ray_offsets, tmax, id_mode, counters, while_while, out, schedule, order)
+    if bounce is not None:
+        seed, bout = bounce
+        if bout is None:
+            R = orig.shape[0]
+            bout = (torch.empty((R, 4), dtype=torch.float32, device=orig.device), torch.empty((R, 4), dtype=torch.float32, device=orig.device),
+                    torch.empty(R, dtype=torch.float32, device=orig.device))
+        d.bounce_seed = int(seed)
+        d.bounce_orig, d.bounce_dir, d.bounce_tmax = bout[0].data_ptr(), bout[1].data_ptr(), bout[2].data_ptr()
+        out["b"] = bout
     _abi.check("rt_batch_trace", _abi.lib().rt_batch_trace(C.byref(d), _stream(stream)))
     return out
 

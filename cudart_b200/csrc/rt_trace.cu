@@ -36,6 +36,11 @@ struct TraceArgs {
   uint32_t* visits;
   uint32_t* tests;
   uint32_t* err;
+  // optional: the packet walks also write each ray's diffuse bounce (bounce_ray / bounce_miss) here
+  float4* b_orig;
+  float4* b_dir;
+  float* b_tmax;
+  uint64_t b_seed;
 };
 
 template <bool kTris, bool kCount>
@@ -705,6 +710,66 @@ __device__ __forceinline__ void write_hit(const uint32_t r, const TraceArgs& A, 
   }
 }
 
+// PCG-XSH-RR 64/32 (O'Neill), pcg32_srandom_r / pcg32_random_r.
+struct Pcg {
+  uint64_t state, inc;
+  __device__ __forceinline__ uint32_t next() {
+    uint64_t old = state;
+    state = old * 6364136223846793005ULL + inc;
+    uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = (uint32_t)(old >> 59u);
+    return (xs >> rot) | (xs << ((-rot) & 31u));
+  }
+  __device__ __forceinline__ void seed(uint64_t initstate, uint64_t initseq) {
+    state = 0u;
+    inc = (initseq << 1u) | 1u;
+    next();
+    state += initstate;
+    next();
+  }
+};
+
+// One diffuse bounce of ray r, which hit the triangle at (global) position pos at distance t: the origin is the hit
+// point moved 1e-4 along the triangle's normal turned against the ray, the direction a cosine-weighted sample of
+// the hemisphere around that normal (a point of the unit disc by rejection from the PCG stream r of `seed`, lifted
+// to the hemisphere, in the orthonormal basis of Duff et al. 2017), tmax huge.
+__device__ __forceinline__ void bounce_ray(const float4* __restrict__ tris, uint32_t pos, const float4& o, const float4& d, float t,
+                                           uint64_t seed, uint32_t r, float4* __restrict__ orig_out, float4* __restrict__ dir_out,
+                                           float* __restrict__ tmax_out) {
+  const float4 e1 = ldg4(tris + 3 * (size_t)pos + 1), e2 = ldg4(tris + 3 * (size_t)pos + 2);
+  float nx = e1.y * e2.z - e1.z * e2.y, ny = e1.z * e2.x - e1.x * e2.z, nz = e1.x * e2.y - e1.y * e2.x;
+  const float inv = 1.0f / sqrtf((nx * nx + ny * ny) + nz * nz);
+  nx = nx * inv; ny = ny * inv; nz = nz * inv;
+  if ((nx * d.x + ny * d.y) + nz * d.z > 0.0f) { nx = -nx; ny = -ny; nz = -nz; }
+  const float px = o.x + t * d.x, py = o.y + t * d.y, pz = o.z + t * d.z;
+  const float eps = 1e-4f;
+  Pcg g;
+  g.seed(seed, (uint64_t)r);
+  float a = 0.0f, b = 0.0f;
+  for (int it = 0; it < 64; ++it) {
+    const float u1 = (float)(g.next() >> 8) * 5.9604644775390625e-8f;
+    const float u2 = (float)(g.next() >> 8) * 5.9604644775390625e-8f;
+    const float aa = 2.0f * u1 - 1.0f, bb = 2.0f * u2 - 1.0f;
+    if (aa * aa + bb * bb < 1.0f) { a = aa; b = bb; break; }
+  }
+  const float c = sqrtf(1.0f - (a * a + b * b));
+  const float sgn = copysignf(1.0f, nz);
+  const float A = -1.0f / (sgn + nz);
+  const float B = nx * ny * A;
+  const float t1x = 1.0f + sgn * nx * nx * A, t1y = sgn * B, t1z = -sgn * nx;
+  const float t2x = B, t2y = sgn + ny * ny * A, t2z = -ny;
+  orig_out[r] = make_float4(px + nx * eps, py + ny * eps, pz + nz * eps, 0.0f);
+  dir_out[r] = make_float4(t1x * a + t2x * b + nx * c, t1y * a + t2y * b + ny * c, t1z * a + t2z * b + nz * c, 0.0f);
+  tmax_out[r] = kHuge;
+}
+// A ray that hit nothing has no bounce: zero origin and direction, tmax -1 (an inactive ray).
+__device__ __forceinline__ void bounce_miss(uint32_t r, float4* __restrict__ orig_out, float4* __restrict__ dir_out,
+                                            float* __restrict__ tmax_out) {
+  orig_out[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+  dir_out[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+  tmax_out[r] = -1.0f;
+}
+
 // The header of the ray's mesh describes a cluster tree built for the mesh's face count; root = its record.
 __device__ __forceinline__ bool cluster_tree_ok(const ClusterArgs& C, uint32_t& root) {
   root = __ldg(C.hdr + kHdrClusterRoot);
@@ -736,7 +801,9 @@ __device__ __forceinline__ bool pop_within(const uint32_t (&st_ref)[kStack], con
 // once it can no longer hold a closer hit). kWW (while-while): each step first
 // descends until the lane holds a cluster, then tests it, so the lanes of a
 // warp test triangles together instead of interleaving box and triangle steps.
-template <bool kCount, bool kWW>
+// kBounce: also write the ray's bounce when A asks for it (the packet kernels' fallback for warps whose rays span
+// meshes).
+template <bool kCount, bool kWW, bool kBounce = false>
 __device__ __forceinline__ void trace_ray_clusters(const uint32_t r, const TraceArgs& A, const ClusterArgs& C) {
   const float tmax0 = A.tmax ? __ldg(A.tmax + r) : kHuge;
   int32_t best = -1;
@@ -826,6 +893,10 @@ __device__ __forceinline__ void trace_ray_clusters(const uint32_t r, const Trace
   if (kCount) {
     if (A.visits) A.visits[r] = visits;
     if (A.tests) A.tests[r] = tests;
+  }
+  if (kBounce && A.b_orig) {  // a packet warp's rays span meshes: the bounce as the packet walk would write it
+    if (best >= 0) bounce_ray(A.tris, C.F + (uint32_t)best, ldg4(A.orig + r), ldg4(A.dir + r), bt, A.b_seed, r, A.b_orig, A.b_dir, A.b_tmax);
+    else bounce_miss(r, A.b_orig, A.b_dir, A.b_tmax);
   }
 }
 
@@ -1088,6 +1159,10 @@ __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, con
   if (kCount) {
     if (A.visits) A.visits[r] = visits;
     if (A.tests) A.tests[r] = tests;
+  }
+  if (A.b_orig) {  // the ray's bounce, from the hit at hand (what rt_batch_bounce_rays makes from the written hit)
+    if (best >= 0) bounce_ray(A.tris, C.F + (uint32_t)best, o, d, bt, A.b_seed, r, A.b_orig, A.b_dir, A.b_tmax);
+    else bounce_miss(r, A.b_orig, A.b_dir, A.b_tmax);
   }
 }
 
@@ -1569,7 +1644,7 @@ __global__ __launch_bounds__(128, 8) void k_batch_trace_clusters_refill(TraceArg
 // Packet walks over batched rays: a warp whose valid rays all belong to one mesh walks it as a packet; a warp
 // spanning meshes falls back to per-lane walks.
 template <bool kCount>
-__global__ __launch_bounds__(128) void k_batch_trace_clusters_packet(TraceArgs A, BatchTraceArgs B, uint32_t* counter,
+__global__ __launch_bounds__(128, 8) void k_batch_trace_clusters_packet(TraceArgs A, BatchTraceArgs B, uint32_t* counter,
                                                                       uint32_t min_lanes) {
   const uint32_t lane = lane_id();
   for (;;) {
@@ -1594,7 +1669,7 @@ __global__ __launch_bounds__(128) void k_batch_trace_clusters_packet(TraceArgs A
       P.n = __shfl_sync(0xffffffffu, C.n, 0);
       trace_warp_packet_clusters<kCount>(r, valid, A, P, min_lanes);
     } else if (valid) {
-      trace_ray_clusters<kCount, false>(r, A, C);
+      trace_ray_clusters<kCount, false, true>(r, A, C);
     }
   }
 }
@@ -1710,25 +1785,6 @@ __global__ __launch_bounds__(256) void k_primary(float4 ro, float4 rd, float4 rx
   }
 }
 
-// PCG-XSH-RR 64/32 (O'Neill), pcg32_srandom_r / pcg32_random_r.
-struct Pcg {
-  uint64_t state, inc;
-  __device__ __forceinline__ uint32_t next() {
-    uint64_t old = state;
-    state = old * 6364136223846793005ULL + inc;
-    uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
-    uint32_t rot = (uint32_t)(old >> 59u);
-    return (xs >> rot) | (xs << ((-rot) & 31u));
-  }
-  __device__ __forceinline__ void seed(uint64_t initstate, uint64_t initseq) {
-    state = 0u;
-    inc = (initseq << 1u) | 1u;
-    next();
-    state += initstate;
-    next();
-  }
-};
-
 // kBatch: hit_pos is a position inside the ray's own mesh of a batched build (the rays of mesh m are
 // ray_off[m] .. ray_off[m + 1]); the mesh's first face position face_off[m] is added before the triangle
 // is read. The PCG stream is the ray index either way.
@@ -1749,38 +1805,10 @@ __global__ __launch_bounds__(256) void k_bounce(const float4* __restrict__ tris,
       pos += (int32_t)__ldg(face_off + lo);
     }
     if (pos < 0) {
-      orig_out[r] = make_float4(0.f, 0.f, 0.f, 0.f);
-      dir_out[r] = make_float4(0.f, 0.f, 0.f, 0.f);
-      tmax_out[r] = -1.0f;
+      bounce_miss(r, orig_out, dir_out, tmax_out);
       continue;
     }
-    const float4 o = orig[r], d = dir[r];
-    const float t = hit_t[r];
-    const float4 e1 = ldg4(tris + 3 * (size_t)pos + 1), e2 = ldg4(tris + 3 * (size_t)pos + 2);
-    float nx = e1.y * e2.z - e1.z * e2.y, ny = e1.z * e2.x - e1.x * e2.z, nz = e1.x * e2.y - e1.y * e2.x;
-    const float inv = 1.0f / sqrtf((nx * nx + ny * ny) + nz * nz);
-    nx = nx * inv; ny = ny * inv; nz = nz * inv;
-    if ((nx * d.x + ny * d.y) + nz * d.z > 0.0f) { nx = -nx; ny = -ny; nz = -nz; }
-    const float px = o.x + t * d.x, py = o.y + t * d.y, pz = o.z + t * d.z;
-    const float eps = 1e-4f;
-    Pcg g;
-    g.seed(seed, (uint64_t)r);
-    float a = 0.0f, b = 0.0f;
-    for (int it = 0; it < 64; ++it) {
-      const float u1 = (float)(g.next() >> 8) * 5.9604644775390625e-8f;
-      const float u2 = (float)(g.next() >> 8) * 5.9604644775390625e-8f;
-      const float aa = 2.0f * u1 - 1.0f, bb = 2.0f * u2 - 1.0f;
-      if (aa * aa + bb * bb < 1.0f) { a = aa; b = bb; break; }
-    }
-    const float c = sqrtf(1.0f - (a * a + b * b));
-    const float sgn = copysignf(1.0f, nz);
-    const float A = -1.0f / (sgn + nz);
-    const float B = nx * ny * A;
-    const float t1x = 1.0f + sgn * nx * nx * A, t1y = sgn * B, t1z = -sgn * nx;
-    const float t2x = B, t2y = sgn + ny * ny * A, t2z = -ny;
-    orig_out[r] = make_float4(px + nx * eps, py + ny * eps, pz + nz * eps, 0.0f);
-    dir_out[r] = make_float4(t1x * a + t2x * b + nx * c, t1y * a + t2y * b + ny * c, t1z * a + t2z * b + nz * c, 0.0f);
-    tmax_out[r] = kHuge;
+    bounce_ray(tris, (uint32_t)pos, orig[r], dir[r], hit_t[r], seed, r, orig_out, dir_out, tmax_out);
   }
 }
 
@@ -1980,6 +2008,7 @@ rt_status trace_args(const rt_trace_desc* d, TraceArgs& A) {
   A.faces = (const uint4*)d->faces; A.indices = d->indices; A.orig = (const float4*)d->orig; A.dir = (const float4*)d->dir;
   A.tmax = d->tmax; A.ray_count = d->ray_count; A.id_mode = d->id_mode; A.hit_id = d->hit_id; A.hit_t = d->hit_t;
   A.hit_uv = (float2*)d->hit_uv; A.visits = d->ray_visits; A.tests = d->ray_tests; A.err = d->error_word;
+  A.b_orig = nullptr; A.b_dir = nullptr; A.b_tmax = nullptr; A.b_seed = 0;
   return RT_OK;
 }
 
@@ -2200,6 +2229,23 @@ rt_status batch_launch_w(const rt_batch_trace_desc* d, const TraceArgs& A, const
   return RT_OK;
 }
 
+// Bounce rays asked of a batched trace: the packet walk writes them itself; every other schedule (and the seeded
+// trace) leaves them to one k_bounce launch after the trace, over the hits it wrote.
+bool bounce_fused(const rt_batch_trace_desc* d) {
+  return d->bounce_orig && (d->schedule & RT_TRACE_CLUSTERS) && (d->schedule & RT_TRACE_PACKET) && d->work_counter;
+}
+rt_status bounce_after(const rt_batch_trace_desc* d, bool fused, cudaStream_t st) {
+  if (!d->bounce_orig || fused) return RT_OK;
+  const uint32_t count = d->ray_count;
+  const uint32_t blocks = (uint32_t)hmin<size_t>((count + 255) / 256, (size_t)sms() * 16);
+  k_bounce<true><<<blocks, 256, 0, st>>>((const float4*)d->tris, (const float4*)d->orig, (const float4*)d->dir, d->hit_id, d->hit_t,
+                                         count, d->bounce_seed, (float4*)d->bounce_orig, (float4*)d->bounce_dir, d->bounce_tmax,
+                                         d->ray_offsets, d->face_offsets, d->mesh_count);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
+}
+
 rt_status batch_launch_clusters(const rt_batch_trace_desc* d, const TraceArgs& A, const BatchTraceArgs& B, cudaStream_t st, bool count) {
   const bool ww = (d->schedule & RT_TRACE_WHILE_WHILE) != 0;
   if (d->work_counter) {
@@ -2241,6 +2287,9 @@ rt_status batch_launch(const rt_batch_trace_desc* d, const SeedArgs& S, cudaStre
   A.tris = (const float4*)d->tris; A.indices = d->indices; A.orig = (const float4*)d->orig; A.dir = (const float4*)d->dir;
   A.tmax = d->tmax; A.ray_count = d->ray_count; A.id_mode = d->id_mode; A.hit_id = d->hit_id; A.hit_t = d->hit_t;
   A.hit_uv = (float2*)d->hit_uv; A.visits = d->ray_visits; A.tests = d->ray_tests; A.err = d->error_word;
+  if (!kSeed && bounce_fused(d)) {
+    A.b_orig = (float4*)d->bounce_orig; A.b_dir = (float4*)d->bounce_dir; A.b_tmax = d->bounce_tmax; A.b_seed = d->bounce_seed;
+  }
   BatchTraceArgs B;
   B.M = d->mesh_count; B.foff = d->face_offsets; B.roff = d->ray_offsets; B.order = d->ray_order;
   Carve c((void*)d->accel, ~(size_t)0);
@@ -2258,6 +2307,8 @@ rt_status batch_check(const rt_batch_trace_desc* d) {
     return RT_ERR_INVALID_ARGUMENT;
   if (d->id_mode == 1 && !d->indices) return RT_ERR_INVALID_ARGUMENT;
   if (d->ray_count > RT_MAX_RAYS) return RT_ERR_INVALID_ARGUMENT;
+  const bool any_bounce = d->bounce_orig || d->bounce_dir || d->bounce_tmax;
+  if (any_bounce && (!d->bounce_orig || !d->bounce_dir || !d->bounce_tmax || d->id_mode != 0)) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   return RT_OK;
 }
@@ -2266,7 +2317,9 @@ rt_status batch_check(const rt_batch_trace_desc* d) {
 extern "C" rt_status rt_batch_trace(const rt_batch_trace_desc* d, rt_stream stream) {
   const rt_status s = batch_check(d);
   if (s != RT_OK || d->ray_count == 0) return s;
-  return batch_launch<false>(d, SeedArgs{}, (cudaStream_t)stream);
+  const rt_status t = batch_launch<false>(d, SeedArgs{}, (cudaStream_t)stream);
+  if (t != RT_OK) return t;
+  return bounce_after(d, bounce_fused(d), (cudaStream_t)stream);
 }
 
 extern "C" rt_status rt_batch_trace_seeded(const rt_batch_trace_desc* d, const rt_seed_desc* sd, rt_stream stream) {
@@ -2277,5 +2330,7 @@ extern "C" rt_status rt_batch_trace_seeded(const rt_batch_trace_desc* d, const r
   SeedArgs S;
   S.proposal = sd->proposal; S.slot_ref = sd->slot_ref; S.slot_box = (const float4*)sd->slot_box; S.slot_count = sd->slot_count;
   S.in_prop = sd->in_proposal;
-  return batch_launch<true>(d, S, (cudaStream_t)stream);
+  const rt_status t = batch_launch<true>(d, S, (cudaStream_t)stream);
+  if (t != RT_OK) return t;
+  return bounce_after(d, false, (cudaStream_t)stream);
 }

@@ -122,15 +122,33 @@ class InstancedFrames:
         self.slots = proposal.batch_subtree_slots(self.tree, self.depth)
         return self.slots
 
+    def bounce_seed(self) -> int:
+        return 1000 + self.frame_index
+
+    def bounce_needs_order(self) -> bool:
+        """Whether a traced schedule reads the bounce generator's active-first order (or no schedule is picked yet)."""
+        return self.schedule_bounce is None or bool(self.schedule_bounce.get("given_order")) or \
+            bool((self.seeded_schedules()[1] or {}).get("given_order"))
+
     def bounce(self, hits, out=None, order=None):
         """One diffuse bounce per primary hit (rt_batch_bounce_rays: hit ids are instance-local positions):
         (orig, dir, tmax, order), the order listing the active bounces first. The order is made when `order` is
         true, by default only when a traced schedule reads it (or before tune() has picked the schedules)."""
         if order is None:
-            order = self.schedule_bounce is None or bool(self.schedule_bounce.get("given_order")) or \
-                bool((self.seeded_schedules()[1] or {}).get("given_order"))
-        return core.batch_bounce_rays(self.tree, self.ray_offsets, self.orig, self.dir, hits["id"], hits["t"], 1000 + self.frame_index,
+            order = self.bounce_needs_order()
+        return core.batch_bounce_rays(self.tree, self.ray_offsets, self.orig, self.dir, hits["id"], hits["t"], self.bounce_seed(),
                                       out=out, order=order)
+
+    def primary(self, out_h1=None, out_b=None):
+        """The primary hits and their bounces (h1, b): in one rt_batch_trace call that writes the bounces too (the
+        packet schedule as each ray finishes) unless a schedule needs the generator's order; then the trace and
+        bounce(). The bounces are the same rays either way."""
+        if self.bounce_needs_order():
+            h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, out=out_h1, schedule=self.schedule_primary)
+            return h1, self.bounce(h1, out=out_b)
+        h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, out=out_h1, schedule=self.schedule_primary,
+                              bounce=(self.bounce_seed(), out_b))
+        return h1, h1["b"]
 
     def bounce_order(self, b):
         """The tracing order of the bounce launch: the generator's active-first order when the bounce schedule asks
@@ -165,10 +183,10 @@ class InstancedFrames:
         return b[3] if (self.seeded_schedules()[1] or {}).get("given_order") else None
 
     def trace_plain(self, out=None):
-        """Primary hits, bounce rays and bounce hits through rt_batch_trace."""
+        """Primary hits, bounce rays and bounce hits through rt_batch_trace (the bounces made by the primary call
+        where the schedules allow, see primary())."""
         out = out or {}
-        h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, out=out.get("h1"), schedule=self.schedule_primary)
-        b = self.bounce(h1, out=out.get("b"))
+        h1, b = self.primary(out.get("h1"), out.get("b"))
         h2 = core.batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], out=out.get("h2"), schedule=self.schedule_bounce,
                               order=self.bounce_order(b))
         return dict(h1=h1, b=b, h2=h2)

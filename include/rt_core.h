@@ -35,7 +35,7 @@ typedef struct CUstream_st* rt_stream; /* a cudaStream_t; NULL = legacy default 
 /* Layout version of the structs below. A caller compiled against this header
  * must check rt_abi_version() == RT_ABI_VERSION before passing any struct:
  * a library built from a different header reads different field offsets. */
-#define RT_ABI_VERSION 9u
+#define RT_ABI_VERSION 10u
 
 typedef enum rt_status {
   RT_OK = 0,
@@ -192,6 +192,14 @@ typedef struct rt_batch_trace_desc {
   const uint32_t* ray_order;      /* optional DEVICE permutation of the rays: threads take rays in this order
                                      (rt_batch_ray_order, rt_image_tile_order); results stay in each ray's own slot */
   uint32_t lane_threshold;        /* as in rt_trace_desc */
+  /* Optional (all three or none; id_mode 0): each ray's diffuse bounce, as rt_batch_bounce_rays makes it from the
+     hits of this call with bounce_seed (float4 origins and directions, float tmax, ray_count entries each; a ray
+     that hit nothing gets tmax -1). The packet schedule (RT_TRACE_CLUSTERS | RT_TRACE_PACKET with a work_counter)
+     writes them as each ray finishes; every other schedule launches rt_batch_bounce_rays' kernel after the trace. */
+  uint64_t bounce_seed;
+  float* bounce_orig;
+  float* bounce_dir;
+  float* bounce_tmax;
 } rt_batch_trace_desc;
 rt_status rt_batch_trace(const rt_batch_trace_desc* desc, rt_stream stream);
 

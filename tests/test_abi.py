@@ -71,7 +71,8 @@ def test_invalid_arguments_rejected():
 
 def test_ray_count_above_limit_refused():
     """More than RT_MAX_RAYS rays is refused before the device check (single and batched traces); the limit itself
-    passes the argument checks, so only the missing device stops it."""
+    passes the argument checks, so only the missing device stops it. So are bounce outputs given in part, or with
+    face ids (id_mode 1) as hit ids."""
     from cudart_b200 import _abi
     lib = _abi.lib()
     desc = _abi.TraceDesc()
@@ -87,6 +88,14 @@ def test_ray_count_above_limit_refused():
     assert lib.rt_batch_trace(C.byref(b), None) == 1
     b.ray_count = _abi.MAX_RAYS
     assert lib.rt_batch_trace(C.byref(b), None) == 2
+    # bounce outputs: all three or none, and only with positions as hit ids
+    b.ray_count = 64
+    b.bounce_orig = 16
+    assert lib.rt_batch_trace(C.byref(b), None) == 1
+    b.bounce_dir = b.bounce_tmax = 16
+    assert lib.rt_batch_trace(C.byref(b), None) == 2
+    b.id_mode, b.indices = 1, 16
+    assert lib.rt_batch_trace(C.byref(b), None) == 1
 
 
 def test_scratch_queries():

@@ -243,3 +243,41 @@ def test_batched_cluster_walks_match_single_mesh(T, oracle):
         T.cuda.synchronize()
         assert int(_host(h["err"])[0]) & _abi.DEVERR_ACCEL_MISSING, sch
         assert (_host(h["id"]) == -1).all(), sch
+
+
+def test_batched_trace_writes_bounce_rays(T, oracle):
+    """rt_batch_trace with bounce outputs: the packet walks write each ray's bounce as it finishes (warps whose rays
+    span meshes through the per-lane fallback), every other schedule through one rt_batch_bounce_rays launch after
+    the trace; either way the bounces equal rt_batch_bounce_rays' from the written hits bit for bit, inactive rays
+    (tmax <= 0) and misses included, and the hits are unchanged."""
+    from cudart_b200 import core
+    meshes = [scenes.soup(1, seed=1), scenes.terrain(9, 3), scenes.soup(5000, seed=5), scenes.terrain(64, 6),
+              scenes.soup(33000, seed=7), scenes.soup(1025, seed=10)]
+    verts, faces, fo, vo = scenes.concat_batch(meshes)
+    bt = core.batch_build(_dev(T, verts), _dev(T, faces.view(np.int32)), fo, vo, clusters=True)
+    rays = [scenes.sphere_rays(m, 40 + 8 * i, seed=200 + i) for i, m in enumerate(meshes)]
+    ro = [0]
+    for o, _ in rays:
+        ro.append(ro[-1] + len(o))
+    O = _dev(T, np.concatenate([o for o, _ in rays]))
+    D = _dev(T, np.concatenate([d for _, d in rays]))
+    R = O.shape[0]
+    tmax = T.full((R,), 1e30, dtype=T.float32, device="cuda")
+    tmax[3::11] = 0.5  # short reach
+    tmax[::7] = -1.0  # inactive rays
+    roff = T.tensor(ro, dtype=T.int32, device="cuda")
+    plain = core.batch_trace(bt, O, D, roff, tmax=tmax, schedule=dict(clusters=True))
+    for sch in [dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True),
+                dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, sorted_bits=21),
+                dict(clusters=True, persistent=True, blocks_per_sm=8, packet=True, lane_threshold=16, sorted_bits=21),
+                dict(clusters=True, persistent=True, blocks_per_sm=8, refill=True, lane_threshold=8),
+                dict(clusters=True), dict(persistent=True, blocks_per_sm=8, coop=True, wide=True)]:
+        for seed in (5, 1234567):
+            h = core.batch_trace(bt, O, D, roff, tmax=tmax, schedule=sch, bounce=(seed, None))
+            ref = core.batch_bounce_rays(bt, roff, O, D, h["id"], h["t"], seed)
+            T.cuda.synchronize()
+            for k in ("id", "t", "uv"):
+                assert T.equal(h[k], plain[k]), (sch, k)
+            for a, b in zip(h["b"], ref[:3]):
+                assert T.equal(a.view(T.int32), b.view(T.int32)), (sch, seed)
+            assert (h["b"][2][::7] == -1.0).all()
