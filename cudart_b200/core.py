@@ -726,13 +726,16 @@ def batch_trace_desc(tree: BatchTree, orig, dir, ray_offsets: torch.Tensor, tmax
         d.ray_order = order.data_ptr()
     elif sch.get("tiles"):  # every mesh's rays are a row-major image of the same size: 8 x 4 pixel tiles per warp
         images, width, height = sch["tiles"]
-        order = image_tile_order(images, width, height, dev)
-        out["_order"] = order
-        d.ray_order = order.data_ptr()
+        key = (int(images), int(width), int(height))
+        if out.get("_tile_key") != key:  # the order depends on the image shape only: made once per output set
+            out["_order"] = image_tile_order(images, width, height, dev)
+            out["_tile_key"] = key
+        d.ray_order = out["_order"].data_ptr()
     elif sch.get("sorted_bits") is not None:  # sorted by mesh, octant and origin Morton code (part of the call)
         order = batch_ray_order(orig, dir, tmax, ray_offsets, tree.mesh_count, batch_tree_box(tree), int(sch["sorted_bits"]),
                                 ray_count=R)
         out["_order"] = order  # keep it alive until the trace has run
+        out.pop("_tile_key", None)
         d.ray_order = order.data_ptr()
     if sch.get("persistent", False) or sch.get("coop", False):
         if "_counter" not in out:

@@ -158,14 +158,15 @@ class InstancedFrames:
     def tune(self):
         """Pick the batched traversal schedules on this frame's rays (untimed): the primary launch's on the
         primary rays (8 x 4 pixel tiles of each instance's image are a candidate), the bounce launch's on their
-        bounces (ray orders by instance, octant and origin are candidates). Returns both and their timings."""
+        bounces (ray orders by instance, octant and origin, and the pixel tiles of the primaries they leave, are
+        candidates). Returns both and their timings."""
         from . import tune
         self.schedule_primary, t1 = tune.tune_batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, use_cache=False,
                                                           images=(self.count, self.width, self.height))
         h1 = core.batch_trace(self.tree, self.orig, self.dir, self.ray_offsets, schedule=self.schedule_primary)
         b = self.bounce(h1, order=True)
         self.schedule_bounce, t2 = tune.tune_batch_trace(self.tree, b[0], b[1], self.ray_offsets, tmax=b[2], use_cache=False,
-                                                         order=b[3])
+                                                         order=b[3], images=(self.count, self.width, self.height))
         # the seeded walks go through the node records: the fastest schedule of those for each launch
         self.seeded_primary = min((x for x in t1 if not x[0].get("clusters")), key=lambda x: x[1])[0]
         self.seeded_bounce = min((x for x in t2 if not x[0].get("clusters")), key=lambda x: x[1])[0]

@@ -135,6 +135,10 @@ def cluster_batch_candidates(images=None):
     for ml, bits, ww in itertools.product((2, 4, 8, 16), (None, 12), (False, True)):
         c = {"clusters": True, "persistent": True, "blocks_per_sm": 8, "refill": True, "lane_threshold": ml, "while_while": ww}
         out.append(c if bits is None else dict(c, sorted_bits=bits))
+    if images is not None and images[1] % 8 == 0 and images[2] % 4 == 0:  # a warp's 32 slots an 8 x 4 pixel tile
+        for ml in (4, 8, 16):
+            out.append({"clusters": True, "persistent": True, "blocks_per_sm": 8, "refill": True, "lane_threshold": ml,
+                        "while_while": False, "tiles": list(images)})
     # warp packets (one node sequence per warp): pixel tiles, and rays ordered by mesh, octant and origin; a warp
     # leaves the packet for per-lane walks once fewer than lane_threshold lanes want its node (0: never)
     for bps in (8, 16):
