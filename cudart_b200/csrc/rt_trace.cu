@@ -2301,6 +2301,12 @@ rt_status batch_launch(const rt_batch_trace_desc* d, const SeedArgs& S, cudaStre
   return batch_launch_w<kSeed, false>(d, A, B, S, st, count, ww);
 }
 
+// Two device ranges [a, a + an) and [b, b + bn) share a byte.
+bool ranges_overlap(const void* a, size_t an, const void* b, size_t bn) {
+  const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+  return a && b && an && bn && x < y + bn && y < x + an;
+}
+
 rt_status batch_check(const rt_batch_trace_desc* d) {
   if (!d || d->mesh_count == 0 || !d->face_offsets || !d->ray_offsets || !d->accel || !d->tris || !d->orig || !d->dir ||
       !d->hit_id || !d->hit_t || !d->hit_uv || d->face_count < d->mesh_count)
@@ -2309,6 +2315,14 @@ rt_status batch_check(const rt_batch_trace_desc* d) {
   if (d->ray_count > RT_MAX_RAYS) return RT_ERR_INVALID_ARGUMENT;
   const bool any_bounce = d->bounce_orig || d->bounce_dir || d->bounce_tmax;
   if (any_bounce && (!d->bounce_orig || !d->bounce_dir || !d->bounce_tmax || d->id_mode != 0)) return RT_ERR_INVALID_ARGUMENT;
+  if (any_bounce) {  // the bounce rays are written while the call still reads its rays and writes its hits: no shared bytes
+    const size_t R = d->ray_count;
+    const void* bufs[9] = {d->bounce_orig, d->bounce_dir, d->bounce_tmax, d->orig, d->dir, d->tmax, d->hit_id, d->hit_t, d->hit_uv};
+    const size_t bytes[9] = {16 * R, 16 * R, 4 * R, 16 * R, 16 * R, 4 * R, 4 * R, 4 * R, 8 * R};
+    for (int i = 0; i < 3; ++i)  // each bounce output against every other buffer of the call
+      for (int j = i + 1; j < 9; ++j)
+        if (ranges_overlap(bufs[i], bytes[i], bufs[j], bytes[j])) return RT_ERR_INVALID_ARGUMENT;
+  }
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   return RT_OK;
 }

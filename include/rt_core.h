@@ -195,7 +195,8 @@ typedef struct rt_batch_trace_desc {
   /* Optional (all three or none; id_mode 0): each ray's diffuse bounce, as rt_batch_bounce_rays makes it from the
      hits of this call with bounce_seed (float4 origins and directions, float tmax, ray_count entries each; a ray
      that hit nothing gets tmax -1). The packet schedule (RT_TRACE_CLUSTERS | RT_TRACE_PACKET with a work_counter)
-     writes them as each ray finishes; every other schedule launches rt_batch_bounce_rays' kernel after the trace. */
+     writes them as each ray finishes; every other schedule launches rt_batch_bounce_rays' kernel after the trace.
+     They share no byte with each other or with orig, dir, tmax and the hit arrays (else RT_ERR_INVALID_ARGUMENT). */
   uint64_t bounce_seed;
   float* bounce_orig;
   float* bounce_dir;

@@ -92,8 +92,15 @@ def test_ray_count_above_limit_refused():
     b.ray_count = 64
     b.bounce_orig = 16
     assert lib.rt_batch_trace(C.byref(b), None) == 1
-    b.bounce_dir = b.bounce_tmax = 16
+    b.bounce_dir = b.bounce_tmax = 16  # all three given, but sharing bytes with each other and the rays
+    assert lib.rt_batch_trace(C.byref(b), None) == 1
+    base = 1 << 20  # separate, never dereferenced ranges of 64 rays
+    b.orig, b.dir, b.tmax, b.hit_id, b.hit_t, b.hit_uv = (base + k * 4096 for k in range(6))
+    b.bounce_orig, b.bounce_dir, b.bounce_tmax = (base + k * 4096 for k in range(6, 9))
     assert lib.rt_batch_trace(C.byref(b), None) == 2
+    b.bounce_dir = b.orig + 512  # overlaps the origins
+    assert lib.rt_batch_trace(C.byref(b), None) == 1
+    b.bounce_dir = base + 9 * 4096
     b.id_mode, b.indices = 1, 16
     assert lib.rt_batch_trace(C.byref(b), None) == 1
 
