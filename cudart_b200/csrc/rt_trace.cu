@@ -732,8 +732,9 @@ struct Pcg {
 // One diffuse bounce of ray r, which hit the triangle at (global) position pos at distance t: the origin is the hit
 // point moved 1e-4 along the triangle's normal turned against the ray, the direction a cosine-weighted sample of
 // the hemisphere around that normal (a point of the unit disc by rejection from the PCG stream r of `seed`, lifted
-// to the hemisphere, in the orthonormal basis of Duff et al. 2017), tmax huge.
-__device__ __forceinline__ void bounce_ray(const float4* __restrict__ tris, uint32_t pos, const float4& o, const float4& d, float t,
+// to the hemisphere, in the orthonormal basis of Duff et al. 2017), tmax huge. Out of line: inlined into the packet
+// walk's epilogue it took that kernel to 72 registers (7 CTAs per SM instead of 8).
+__device__ __noinline__ void bounce_ray(const float4* __restrict__ tris, uint32_t pos, const float4& o, const float4& d, float t,
                                            uint64_t seed, uint32_t r, float4* __restrict__ orig_out, float4* __restrict__ dir_out,
                                            float* __restrict__ tmax_out) {
   const float4 e1 = ldg4(tris + 3 * (size_t)pos + 1), e2 = ldg4(tris + 3 * (size_t)pos + 2);
@@ -1020,7 +1021,9 @@ __device__ __forceinline__ void cswap_packet(uint32_t (&key)[4], float (&t)[4], 
 // min_lanes > 0: once fewer lanes than that want the node the packet is at,
 // the warp leaves the packet walk and every lane walks on alone from its own
 // copy of the stack (which already holds its own entry distances).
-template <bool kCount>
+// kBounce: also write each ray's bounce (A.b_*); a separate instantiation, since the bounce code alone (taken or
+// not) costs the walk about 3% in a kernel that does not write bounces.
+template <bool kCount, bool kBounce = false>
 __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, const bool valid, const TraceArgs& A, const ClusterArgs& C,
                                                            const uint32_t min_lanes) {
   float4 o = make_float4(0.f, 0.f, 0.f, 0.f), d = make_float4(0.f, 0.f, 1.f, 0.f);
@@ -1160,7 +1163,7 @@ __device__ __forceinline__ void trace_warp_packet_clusters(const uint32_t r, con
     if (A.visits) A.visits[r] = visits;
     if (A.tests) A.tests[r] = tests;
   }
-  if (A.b_orig) {  // the ray's bounce, from the hit at hand (what rt_batch_bounce_rays makes from the written hit)
+  if (kBounce && A.b_orig) {  // the ray's bounce, from the hit at hand (what rt_batch_bounce_rays makes from the written hit)
     if (best >= 0) bounce_ray(A.tris, C.F + (uint32_t)best, o, d, bt, A.b_seed, r, A.b_orig, A.b_dir, A.b_tmax);
     else bounce_miss(r, A.b_orig, A.b_dir, A.b_tmax);
   }
@@ -1643,8 +1646,8 @@ __global__ __launch_bounds__(128, 8) void k_batch_trace_clusters_refill(TraceArg
 
 // Packet walks over batched rays: a warp whose valid rays all belong to one mesh walks it as a packet; a warp
 // spanning meshes falls back to per-lane walks.
-template <bool kCount>
-__global__ __launch_bounds__(128, 8) void k_batch_trace_clusters_packet(TraceArgs A, BatchTraceArgs B, uint32_t* counter,
+template <bool kCount, bool kBounce>
+__global__ __launch_bounds__(128) void k_batch_trace_clusters_packet(TraceArgs A, BatchTraceArgs B, uint32_t* counter,
                                                                       uint32_t min_lanes) {
   const uint32_t lane = lane_id();
   for (;;) {
@@ -1667,9 +1670,9 @@ __global__ __launch_bounds__(128, 8) void k_batch_trace_clusters_packet(TraceArg
       P.hdr = (const uint32_t*)__shfl_sync(0xffffffffu, (unsigned long long)C.hdr, 0);
       P.F = F0;
       P.n = __shfl_sync(0xffffffffu, C.n, 0);
-      trace_warp_packet_clusters<kCount>(r, valid, A, P, min_lanes);
+      trace_warp_packet_clusters<kCount, kBounce>(r, valid, A, P, min_lanes);
     } else if (valid) {
-      trace_ray_clusters<kCount, false, true>(r, A, C);
+      trace_ray_clusters<kCount, false, kBounce>(r, A, C);
     }
   }
 }
@@ -2253,8 +2256,10 @@ rt_status batch_launch_clusters(const rt_batch_trace_desc* d, const TraceArgs& A
     const uint32_t per_sm = d->persistent_blocks_per_sm ? d->persistent_blocks_per_sm : 8u;
     const uint32_t blocks = (uint32_t)hmin<uint64_t>((uint64_t)sms() * per_sm, ((uint64_t)d->ray_count + 127) / 128);
     if (d->schedule & RT_TRACE_PACKET) {
-      if (count) k_batch_trace_clusters_packet<true><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold);
-      else k_batch_trace_clusters_packet<false><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold);
+#define RT_LAUNCH_BCK(CNT, BNC) k_batch_trace_clusters_packet<CNT, BNC><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold)
+      if (A.b_orig) { if (count) RT_LAUNCH_BCK(true, true); else RT_LAUNCH_BCK(false, true); }
+      else { if (count) RT_LAUNCH_BCK(true, false); else RT_LAUNCH_BCK(false, false); }
+#undef RT_LAUNCH_BCK
     } else if (d->schedule & RT_TRACE_REFILL) {
 #define RT_LAUNCH_BCR(CNT, WW) k_batch_trace_clusters_refill<CNT, WW><<<blocks, 128, 0, st>>>(A, B, d->work_counter, d->lane_threshold)
       if (count) { if (ww) RT_LAUNCH_BCR(true, true); else RT_LAUNCH_BCR(true, false); }
