@@ -2018,7 +2018,7 @@ rt_status trace_args(const rt_trace_desc* d, TraceArgs& A) {
 }  // namespace
 
 extern "C" rt_status rt_trace_closest(const rt_trace_desc* d, rt_stream stream) {
-  TraceArgs A;
+  TraceArgs A = {};
   const rt_status s = trace_args(d, A);
   if (s != RT_OK) return s;
   if (d->ray_count == 0) return RT_OK;
@@ -2042,7 +2042,7 @@ extern "C" rt_status rt_trace_closest(const rt_trace_desc* d, rt_stream stream) 
 }
 
 extern "C" rt_status rt_trace_closest_seeded(const rt_trace_desc* d, const rt_seed_desc* sd, rt_stream stream) {
-  TraceArgs A;
+  TraceArgs A = {};
   const rt_status s = trace_args(d, A);
   if (s != RT_OK) return s;
   if (!sd || !sd->proposal || !sd->slot_ref || !d->accel || !d->tris) return RT_ERR_INVALID_ARGUMENT;
