@@ -780,6 +780,7 @@ extern "C" rt_status rt_lbvh_accel_bytes(uint32_t face_count, size_t* bytes) {
 }
 
 extern "C" rt_status rt_lbvh_build(const rt_build_desc* d, rt_stream stream_) {
+  const rt::NvtxRange nvtx_range("rt_lbvh_build");
   if (!d || d->face_count == 0 || !d->vertices || !d->faces_in || !d->boxes || !d->indices || !d->nodes || d->max_nodes == 0)
     return RT_ERR_INVALID_ARGUMENT;
   if (d->face_count > 0x7FFFFFFFu) return RT_ERR_INVALID_ARGUMENT;
@@ -1301,6 +1302,7 @@ extern "C" rt_status rt_batch_sizes(uint32_t M, uint32_t N, const rt_build_param
 }
 
 extern "C" rt_status rt_batch_build(const rt_batch_build_desc* d, rt_stream stream_) {
+  const rt::NvtxRange nvtx_range("rt_batch_build");
   if (!d || d->mesh_count == 0 || d->face_count < d->mesh_count || !d->face_offsets || !d->vertex_offsets || !d->vertices ||
       !d->faces_in || !d->faces_out || !d->boxes || !d->indices || !d->codes || !d->nodes || !d->tris || !d->accel || !d->info)
     return RT_ERR_INVALID_ARGUMENT;

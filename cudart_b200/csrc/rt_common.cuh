@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <atomic>
 #include <mutex>
 
@@ -40,6 +42,15 @@ __device__ __forceinline__ void ldg8(const float4* p, float4& a, float4& b) {
 }
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// A named host range around an entry point, for profilers that read NVTX ranges (the header-only NVTX3 API does
+// nothing unless a tool attaches).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 template <typename T>

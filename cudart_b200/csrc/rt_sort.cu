@@ -442,6 +442,7 @@ static uint32_t bits_of(uint32_t bit_depth) {
 
 extern "C" rt_status rt_radix_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t n, uint32_t bit_depth, int init_values,
                                          void* scratch, size_t scratch_bytes, rt_stream stream) {
+  const rt::NvtxRange nvtx_range("rt_radix_sort_pairs");
   if (n && (!keys || !values)) return RT_ERR_INVALID_ARGUMENT;
   if (n > (uint32_t)kTile && (!scratch || scratch_bytes < radix_scratch_bytes(n))) return RT_ERR_SCRATCH_TOO_SMALL;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;

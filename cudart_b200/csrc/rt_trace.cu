@@ -2018,6 +2018,7 @@ rt_status trace_args(const rt_trace_desc* d, TraceArgs& A) {
 }  // namespace
 
 extern "C" rt_status rt_trace_closest(const rt_trace_desc* d, rt_stream stream) {
+  const rt::NvtxRange nvtx_range("rt_trace_closest");
   TraceArgs A = {};
   const rt_status s = trace_args(d, A);
   if (s != RT_OK) return s;
@@ -2042,6 +2043,7 @@ extern "C" rt_status rt_trace_closest(const rt_trace_desc* d, rt_stream stream) 
 }
 
 extern "C" rt_status rt_trace_closest_seeded(const rt_trace_desc* d, const rt_seed_desc* sd, rt_stream stream) {
+  const rt::NvtxRange nvtx_range("rt_trace_closest_seeded");
   TraceArgs A = {};
   const rt_status s = trace_args(d, A);
   if (s != RT_OK) return s;
@@ -2128,6 +2130,7 @@ extern "C" rt_status rt_image_tile_order(uint32_t images, uint32_t width, uint32
 }
 
 extern "C" rt_status rt_primary_rays(const rt_camera* cam, uint32_t w, uint32_t h, float* orig, float* dir, rt_stream stream) {
+  const rt::NvtxRange nvtx_range("rt_primary_rays");
   if (!cam || !orig || !dir || w == 0 || h == 0) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
   float b[16];
@@ -2145,6 +2148,7 @@ extern "C" rt_status rt_primary_rays(const rt_camera* cam, uint32_t w, uint32_t 
 
 extern "C" rt_status rt_batch_primary_rays(const float* bases, uint32_t count, uint32_t w, uint32_t h, float* orig, float* dir,
                                            rt_stream stream) {
+  const rt::NvtxRange nvtx_range("rt_batch_primary_rays");
   if (count == 0) return RT_OK;
   if (!bases || !orig || !dir || w == 0 || h == 0) return RT_ERR_INVALID_ARGUMENT;
   if ((uint64_t)count * w * h > 0xFFFFFFFFull) return RT_ERR_INVALID_ARGUMENT;
@@ -2159,6 +2163,7 @@ extern "C" rt_status rt_batch_primary_rays(const float* bases, uint32_t count, u
 
 extern "C" rt_status rt_bounce_rays(const float* tris, const float* orig, const float* dir, const int32_t* hit_pos, const float* hit_t,
                                     uint32_t count, uint64_t seed, float* orig_out, float* dir_out, float* tmax_out, rt_stream stream) {
+  const rt::NvtxRange nvtx_range("rt_bounce_rays");
   if (count == 0) return RT_OK;
   if (!tris || !orig || !dir || !hit_pos || !hit_t || !orig_out || !dir_out || !tmax_out) return RT_ERR_INVALID_ARGUMENT;
   if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
@@ -2174,6 +2179,7 @@ extern "C" rt_status rt_batch_bounce_rays(const float* tris, const uint32_t* fac
                                           const float* orig, const float* dir, const int32_t* hit_pos, const float* hit_t, uint32_t count,
                                           uint64_t seed, float* orig_out, float* dir_out, float* tmax_out, uint32_t* order_out,
                                           uint32_t* order_counters, rt_stream stream) {
+  const rt::NvtxRange nvtx_range("rt_batch_bounce_rays");
   if (count == 0) return RT_OK;
   if (!tris || !face_offsets || !ray_offsets || mesh_count == 0 || !orig || !dir || !hit_pos || !hit_t || !orig_out || !dir_out ||
       !tmax_out || (order_out && !order_counters))
@@ -2334,6 +2340,7 @@ rt_status batch_check(const rt_batch_trace_desc* d) {
 }  // namespace
 
 extern "C" rt_status rt_batch_trace(const rt_batch_trace_desc* d, rt_stream stream) {
+  const rt::NvtxRange nvtx_range("rt_batch_trace");
   const rt_status s = batch_check(d);
   if (s != RT_OK || d->ray_count == 0) return s;
   const rt_status t = batch_launch<false>(d, SeedArgs{}, (cudaStream_t)stream);
@@ -2342,6 +2349,7 @@ extern "C" rt_status rt_batch_trace(const rt_batch_trace_desc* d, rt_stream stre
 }
 
 extern "C" rt_status rt_batch_trace_seeded(const rt_batch_trace_desc* d, const rt_seed_desc* sd, rt_stream stream) {
+  const rt::NvtxRange nvtx_range("rt_batch_trace_seeded");
   const rt_status s = batch_check(d);
   if (s != RT_OK) return s;
   if (!sd || !sd->proposal || !sd->slot_ref) return RT_ERR_INVALID_ARGUMENT;
