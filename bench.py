@@ -456,11 +456,13 @@ def learned_frames(w, args, dev, world, plain, first_frame):
 def run_e2e(w, args, dev, world, s1, s2):
     """The headline metric through the public API with host buffers, as a frame pipeline: every frame copies
     the 64 instances' displaced vertices from pinned host memory, builds, makes the primary rays, traces them
-    and their bounces, and copies every hit (id, t, u, v of primaries and bounces) back to pinned host memory.
-    The copies run on two copy streams (one per direction) with the device vertices and hits double-buffered,
-    so that frame k+1's upload and frame k-1's download overlap frame k's kernels (one CUDA graph per buffer
-    set); the timed region holds every frame's copies and kernels. The faces (the instances' fixed topology)
-    stay resident."""
+    and their bounces, and brings every hit of both launches back to pinned host memory: the ids of all rays,
+    then the (t, u, v) of the rays that hit, packed on the device by rt_pack_hits (a miss is t = its tmax,
+    uv = 0, so the host has every hit exactly; the last frame's are rebuilt and checked). The copies run on two
+    copy streams (one per direction) with the device vertices and hits double-buffered, so that frame k+1's
+    upload and frame k-1's download overlap frame k's kernels (one CUDA graph per buffer set); the host reads a
+    frame's hit counts before it sizes that frame's packed copies, one frame behind. The timed region holds
+    every frame's copies and kernels. The faces (the instances' fixed topology) stay resident."""
     import torch
 
     from cudart_b200 import core
@@ -473,10 +475,11 @@ def run_e2e(w, args, dev, world, s1, s2):
     for s in range(2):
         v[s].copy_(vh)
     outs = [w.trace_plain() for _ in range(2)]
+    packs = [[core.pack_hits(outs[s][h]) for h in ("h1", "h2")] for s in range(2)]
     out_id = torch.empty((2, 2, R), dtype=torch.int32).pin_memory()
-    out_t = torch.empty((2, 2, R), dtype=torch.float32).pin_memory()
-    out_uv = torch.empty((2, 2, R, 2), dtype=torch.float32).pin_memory()
-    ev = {k: [torch.cuda.Event(), torch.cuda.Event()] for k in ("uploaded", "traced", "downloaded")}
+    out_cnt = torch.zeros((2, 2), dtype=torch.int32).pin_memory()
+    out_pk = torch.empty((2, 2, 3 * R), dtype=torch.float32).pin_memory()
+    ev = {k: [torch.cuda.Event(), torch.cuda.Event()] for k in ("uploaded", "traced", "ids_down", "downloaded")}
 
     aux = torch.cuda.Stream()
 
@@ -486,8 +489,22 @@ def run_e2e(w, args, dev, world, s1, s2):
         w.primary(o["h1"], o["b"])
         core.batch_trace(w.tree, o["b"][0], o["b"][1], w.ray_offsets, tmax=o["b"][2], out=o["h2"], schedule=s2,
                          order=w.bounce_order(o["b"]))
+        for i, h in enumerate(("h1", "h2")):
+            core.pack_hits(o[h], out=packs[s][i])
 
     graphs, _ = capture_graphs([lambda: compute(0), lambda: compute(1)])
+    packed_bytes = [0]
+
+    def finish(j):
+        # frame j's hit counts are on the host once its id copies are: size and queue its packed copies
+        s = j % 2
+        ev["ids_down"][s].synchronize()
+        with torch.cuda.stream(down):
+            for i in range(2):
+                n = int(out_cnt[s, i])
+                out_pk[s, i, :3 * n].copy_(packs[s][i]["packed"][:3 * n], non_blocking=True)
+                packed_bytes[0] += 12 * n
+        ev["downloaded"][s].record(down)
 
     def step(k):
         s = k % 2
@@ -501,35 +518,48 @@ def run_e2e(w, args, dev, world, s1, s2):
             comp.wait_event(ev["downloaded"][s])  # frame k-2's hits have reached the host
         graphs[s].replay()
         ev["traced"][s].record(comp)
+        if k >= 1:
+            finish(k - 1)
         down.wait_event(ev["traced"][s])
         with torch.cuda.stream(down):
-            for i, h in enumerate((outs[s]["h1"], outs[s]["h2"])):
-                out_id[s, i].copy_(h["id"], non_blocking=True)
-                out_t[s, i].copy_(h["t"], non_blocking=True)
-                out_uv[s, i].copy_(h["uv"], non_blocking=True)
-        ev["downloaded"][s].record(down)
+            for i, h in enumerate(("h1", "h2")):
+                out_id[s, i].copy_(outs[s][h]["id"], non_blocking=True)
+                out_cnt[s, i].copy_(packs[s][i]["count"][0], non_blocking=True)
+        ev["ids_down"][s].record(down)
 
     for k in range(args.warmup):
         step(k)
+    finish(args.warmup - 1)
     torch.cuda.synchronize()
     active = sum(int((outs[s]["b"][2] > 0).sum().item()) for s in range(2)) / 2.0
+    packed_bytes[0] = 0
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(comp)
     up.wait_event(e0)
     down.wait_event(e0)
     for k in range(args.steps):
         step(k)
+    finish(args.steps - 1)
     comp.wait_event(ev["downloaded"][(args.steps - 1) % 2])
     e1.record(comp)
     torch.cuda.synchronize()
     ms, = max_over_ranks([e0.elapsed_time(e1)], world, dev)
-    ok = torch.equal(out_id[(args.steps - 1) % 2, 0], outs[(args.steps - 1) % 2]["h1"]["id"].cpu())
+    # the last frame's hits rebuilt on the host from its ids and packed hits equal the device's, bit for bit
+    s = (args.steps - 1) % 2
+    ok = True
+    for i, h in enumerate(("h1", "h2")):
+        tm = None if h == "h1" else outs[s]["b"][2].cpu()
+        t, uv = core.unpack_hits(out_id[s, i], out_pk[s, i], int(out_cnt[s, i]), tmax=tm)
+        d = outs[s][h]
+        ok = ok and torch.equal(out_id[s, i], d["id"].cpu()) and torch.equal(t.view(torch.int32), d["t"].cpu().view(torch.int32)) \
+            and torch.equal(uv.view(torch.int32), d["uv"].cpu().view(torch.int32))
     h2d = vh.numel() * 4
-    d2h = (out_id[0].numel() + out_t[0].numel() + out_uv[0].numel()) * 4
+    d2h = out_id[0].numel() * 4 + out_cnt[0].numel() * 4 + packed_bytes[0] / args.steps
     del graphs
     return {"value": round(world * (R + active) * args.steps / (ms * 1e-3) / 1e6, 2), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "ms_per_step": round(ms / args.steps, 3), "download_checked": bool(ok),
-            "pipeline": "vertices up / hits down on two copy streams, double-buffered around one CUDA graph per frame"}
+            "pipeline": "vertices up / ids, hit counts and packed hits down on two copy streams, double-buffered around one CUDA "
+                        "graph per frame"}
 
 
 # ----------------------------------------------------------------------------

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librt_core.so")
 
 RT_OK = 0
-ABI_VERSION = 10  # RT_ABI_VERSION of include/rt_core.h that the structs below mirror
+ABI_VERSION = 11  # RT_ABI_VERSION of include/rt_core.h that the structs below mirror
 STATUS_NAMES = {0: "RT_OK", 1: "RT_ERR_INVALID_ARGUMENT", 2: "RT_ERR_NO_DEVICE", 3: "RT_ERR_CUDA",
                 4: "RT_ERR_SCRATCH_TOO_SMALL", 5: "RT_ERR_CAPACITY", 6: "RT_ERR_UNSUPPORTED"}
 DEVERR_NODE_CAPACITY = 0x1
@@ -36,7 +36,7 @@ EXPORTS = (
     "rt_lbvh_scratch_bytes", "rt_lbvh_accel_bytes", "rt_lbvh_build", "rt_batch_sizes", "rt_batch_build", "rt_batch_trace", "rt_mesh_boxes", "rt_reorder_faces", "rt_sort_scratch_bytes",
     "rt_radix_sort_pairs", "rt_radix_sort_pairs_static", "rt_radix_sort_keys", "rt_camera_look_at", "rt_camera_basis", "rt_primary_rays", "rt_batch_primary_rays",
     "rt_trace_closest", "rt_ray_order_scratch_bytes", "rt_ray_order", "rt_batch_ray_order_scratch_bytes", "rt_batch_ray_order",
-    "rt_image_tile_order", "rt_interpolate", "rt_bounce_rays", "rt_batch_bounce_rays", "rt_mesh_file_save", "rt_mesh_file_info", "rt_mesh_file_load", "rt_tree_file_save", "rt_tree_file_info",
+    "rt_image_tile_order", "rt_interpolate", "rt_bounce_rays", "rt_batch_bounce_rays", "rt_pack_hits_scratch_bytes", "rt_pack_hits", "rt_mesh_file_save", "rt_mesh_file_info", "rt_mesh_file_load", "rt_tree_file_save", "rt_tree_file_info",
     "rt_tree_file_load", "rt_status_string", "rt_version", "rt_abi_version", "rt_device_check", "rt_launch_count",
 )
 # every symbol include/rt_sah.h declares
@@ -223,6 +223,8 @@ def lib():
         L.rt_image_tile_order.argtypes = [_U32, _U32, _U32, _P, _P]
         L.rt_bounce_rays.argtypes = [_P, _P, _P, _P, _P, _U32, C.c_uint64, _P, _P, _P, _P]
         L.rt_batch_bounce_rays.argtypes = [_P, _P, _P, _U32, _P, _P, _P, _P, _U32, C.c_uint64, _P, _P, _P, _P, _P, _P]
+        L.rt_pack_hits_scratch_bytes.argtypes = [_U32, C.POINTER(C.c_size_t)]
+        L.rt_pack_hits.argtypes = [_P, _P, _P, _U32, _P, _P, _P, C.c_size_t, _P]
         for fn, st in (("mesh", MeshFile), ("tree", TreeFile)):
             getattr(L, f"rt_{fn}_file_save").argtypes = [C.c_char_p, C.c_int, C.POINTER(st)]
             getattr(L, f"rt_{fn}_file_info").argtypes = [C.c_char_p, C.POINTER(st)]

@@ -434,6 +434,36 @@ def batch_bounce_rays(tree, ray_offsets, orig, dir, hit_pos, hit_t, seed: int, o
     return out
 
 
+def pack_hits(hits: dict, out: dict | None = None, stream=None) -> dict:
+    """rt_pack_hits: the (t, u, v) of the rays that hit, in ray order, for a compact download: out["packed"]
+    (float32 [3 R]; the first 3 * count entries hold them) and out["count"] (int32 [1]). Rebuild with unpack_hits."""
+    ids = hits["id"]
+    R = ids.numel()
+    if out is None:
+        nb = C.c_size_t(0)
+        _abi.check("rt_pack_hits_scratch_bytes", _abi.lib().rt_pack_hits_scratch_bytes(R, C.byref(nb)))
+        out = dict(packed=torch.empty(3 * max(R, 1), dtype=torch.float32, device=ids.device),
+                   count=torch.zeros(1, dtype=torch.int32, device=ids.device),
+                   scratch=torch.empty(max(nb.value, 1), dtype=torch.uint8, device=ids.device))
+    _abi.check("rt_pack_hits", _abi.lib().rt_pack_hits(_p(ids), _p(hits["t"]), _p(hits["uv"]), R, _p(out["packed"]), _p(out["count"]),
+                                                        _p(out["scratch"]), out["scratch"].numel(), _stream(stream)))
+    return out
+
+
+def unpack_hits(ids, packed, count: int, tmax=None):
+    """The full hits (t, uv) from the ids and the packed (t, u, v) of the hits (host or device tensors): a miss has
+    t = its tmax (CUDART_NORM_HUGE_F without one) and uv = 0."""
+    hit = ids >= 0
+    R = ids.numel()
+    t = torch.full((R,), 3.402823466e38, dtype=torch.float32) if tmax is None else tmax.to(torch.float32).clone()
+    t = t.to(ids.device)
+    uv = torch.zeros((R, 2), dtype=torch.float32, device=ids.device)
+    p = packed[:3 * count].view(count, 3)
+    t[hit] = p[:, 0]
+    uv[hit] = p[:, 1:]
+    return t, uv
+
+
 def sort_pairs(keys: torch.Tensor, values: torch.Tensor, bit_depth: int = 32, init_values: bool = False, stream=None):
     """In place, stable (CUDA_radixSortGeneral)."""
     _need_cuda(keys, "keys", _I32)

@@ -1866,6 +1866,42 @@ int sms() {
 }
 
 }  // namespace
+// Hit packing for download: blocks of kPackRays rays (256 threads x 8 consecutive rays); one pass counts each
+// block's hits, a scan turns the counts into block offsets (and the total), a second pass writes (t, u, v) of
+// every hit at its block offset plus its rank in the block.
+constexpr uint32_t kPackRays = 2048;
+__global__ __launch_bounds__(256) void k_pack_count(const int32_t* __restrict__ id, uint32_t n, uint32_t* __restrict__ block_hits) {
+  __shared__ uint32_t s_w[8];
+  const uint32_t base = blockIdx.x * kPackRays + threadIdx.x * 8u;
+  uint32_t c = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < 8; ++k) c += (base + k < n && __ldg(id + base + k) >= 0) ? 1u : 0u;
+  uint32_t total;
+  block_excl_scan_nt<256>(c, s_w, total);
+  if (threadIdx.x == 0) block_hits[blockIdx.x] = total;
+}
+__global__ __launch_bounds__(256) void k_pack_write(const int32_t* __restrict__ id, const float* __restrict__ t,
+                                                    const float2* __restrict__ uv, uint32_t n, const uint32_t* __restrict__ block_base,
+                                                    float* __restrict__ packed) {
+  __shared__ uint32_t s_w[8];
+  const uint32_t base = blockIdx.x * kPackRays + threadIdx.x * 8u;
+  uint32_t m = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < 8; ++k)
+    if (base + k < n && __ldg(id + base + k) >= 0) m |= 1u << k;
+  uint32_t total;
+  uint32_t o = block_base[blockIdx.x] + block_excl_scan_nt<256>((uint32_t)__popc(m), s_w, total);
+#pragma unroll
+  for (uint32_t k = 0; k < 8; ++k) {
+    if (!((m >> k) & 1u)) continue;
+    const float2 w = __ldg(uv + base + k);
+    packed[3 * (size_t)o] = __ldg(t + base + k);
+    packed[3 * (size_t)o + 1] = w.x;
+    packed[3 * (size_t)o + 2] = w.y;
+    ++o;
+  }
+}
+
 }  // namespace rt
 
 using namespace rt;
@@ -2360,4 +2396,47 @@ extern "C" rt_status rt_batch_trace_seeded(const rt_batch_trace_desc* d, const r
   const rt_status t = batch_launch<true>(d, S, (cudaStream_t)stream);
   if (t != RT_OK) return t;
   return bounce_after(d, false, (cudaStream_t)stream);
+}
+
+namespace {
+// Scratch of rt_pack_hits: the block counts (scanned in place into block offsets), then the scan's block sums.
+size_t pack_scratch(uint32_t count, uint32_t** counts, uint32_t** sums, void* base) {
+  const uint32_t nb = (count + kPackRays - 1) / kPackRays;
+  Carve c(base, ~(size_t)0);
+  uint32_t* a = c.take<uint32_t>((size_t)nb + 1);
+  uint32_t* b = c.take<uint32_t>((size_t)(nb + 1023) / 1024 + 1);
+  if (counts) *counts = a;
+  if (sums) *sums = b;
+  return c.off;
+}
+}  // namespace
+
+extern "C" rt_status rt_pack_hits_scratch_bytes(uint32_t count, size_t* scratch_bytes) {
+  if (!scratch_bytes) return RT_ERR_INVALID_ARGUMENT;
+  *scratch_bytes = pack_scratch(count, nullptr, nullptr, nullptr);
+  return RT_OK;
+}
+
+extern "C" rt_status rt_pack_hits(const int32_t* hit_id, const float* hit_t, const float* hit_uv, uint32_t count, float* packed,
+                                  uint32_t* packed_count, void* scratch, size_t scratch_bytes, rt_stream stream) {
+  const rt::NvtxRange nvtx_range("rt_pack_hits");
+  if (!packed_count) return RT_ERR_INVALID_ARGUMENT;
+  if (count && (!hit_id || !hit_t || !hit_uv || !packed || !scratch)) return RT_ERR_INVALID_ARGUMENT;
+  if (count > RT_MAX_RAYS) return RT_ERR_INVALID_ARGUMENT;
+  if (count && scratch_bytes < pack_scratch(count, nullptr, nullptr, nullptr)) return RT_ERR_SCRATCH_TOO_SMALL;
+  if (rt_device_check() != RT_OK) return RT_ERR_NO_DEVICE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (count == 0) return cudaMemsetAsync(packed_count, 0, 4, st) == cudaSuccess ? RT_OK : RT_ERR_CUDA;
+  uint32_t *counts = nullptr, *sums = nullptr;
+  pack_scratch(count, &counts, &sums, scratch);
+  const uint32_t nb = (count + kPackRays - 1) / kPackRays;
+  k_pack_count<<<nb, 256, 0, st>>>(hit_id, count, counts);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  excl_scan(counts, nb, sums, packed_count, st);
+  RT_CHECK_LAUNCH();
+  k_pack_write<<<nb, 256, 0, st>>>(hit_id, hit_t, (const float2*)hit_uv, count, counts, packed);
+  note_launch();
+  RT_CHECK_LAUNCH();
+  return RT_OK;
 }

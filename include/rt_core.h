@@ -35,7 +35,7 @@ typedef struct CUstream_st* rt_stream; /* a cudaStream_t; NULL = legacy default 
 /* Layout version of the structs below. A caller compiled against this header
  * must check rt_abi_version() == RT_ABI_VERSION before passing any struct:
  * a library built from a different header reads different field offsets. */
-#define RT_ABI_VERSION 10u
+#define RT_ABI_VERSION 11u
 
 typedef enum rt_status {
   RT_OK = 0,
@@ -382,6 +382,15 @@ rt_status rt_batch_bounce_rays(const float* tris, const uint32_t* face_offsets, 
                                const float* orig, const float* dir, const int32_t* hit_pos, const float* hit_t, uint32_t ray_count,
                                uint64_t seed, float* orig_out, float* dir_out, float* tmax_out, uint32_t* order_out,
                                uint32_t* order_counters, rt_stream stream);
+
+/* Hits packed for download: the (t, u, v) of every ray whose hit_id >= 0, in ray order, as float[3 * hits] in
+ * `packed` (DEVICE, room for 3 * count floats), and the number of those rays in *packed_count (DEVICE word). With
+ * the ids, downloaded as they are, the host rebuilds every hit exactly: a ray with id -1 has t = the tmax it was
+ * traced with (CUDART_NORM_HUGE_F without one) and uv = 0. Scratch: rt_pack_hits_scratch_bytes. No reference
+ * counterpart. */
+rt_status rt_pack_hits_scratch_bytes(uint32_t count, size_t* scratch_bytes);
+rt_status rt_pack_hits(const int32_t* hit_id, const float* hit_t, const float* hit_uv, uint32_t count, float* packed,
+                       uint32_t* packed_count, void* scratch, size_t scratch_bytes, rt_stream stream);
 
 /* Mesh and tree chunk files (HOST calls; arrays may be device or host memory).
  * Same bytes as CUDAMesh::quickSave / CUDAMeshTree::quickSave with

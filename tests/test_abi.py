@@ -105,6 +105,21 @@ def test_ray_count_above_limit_refused():
     assert lib.rt_batch_trace(C.byref(b), None) == 1
 
 
+def test_pack_hits_refusals():
+    """rt_pack_hits: scratch sized by its query, null outputs and too small a scratch refused before the device
+    check; a well-formed call stops only at the missing device."""
+    from cudart_b200 import _abi
+    lib = _abi.lib()
+    nb = C.c_size_t(0)
+    assert lib.rt_pack_hits_scratch_bytes(100000, C.byref(nb)) == 0 and nb.value >= 4 * (100000 // 2048)
+    F = 1 << 20
+    assert lib.rt_pack_hits(F, F, F, 100000, F, None, F, nb.value, None) == 1  # no count word
+    assert lib.rt_pack_hits(F, F, None, 100000, F, F, F, nb.value, None) == 1  # no uv
+    assert lib.rt_pack_hits(F, F, F, 100000, F, F, F, nb.value - 1, None) == 4  # RT_ERR_SCRATCH_TOO_SMALL
+    assert lib.rt_pack_hits(F, F, F, _abi.MAX_RAYS + 1, F, F, F, 1 << 40, None) == 1
+    assert lib.rt_pack_hits(F, F, F, 100000, F, F, F, nb.value, None) == 2
+
+
 def test_scratch_queries():
     from cudart_b200 import core
     nb, mx = core.lbvh_scratch_bytes(1 << 20)

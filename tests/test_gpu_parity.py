@@ -438,3 +438,32 @@ def test_ray_order_puts_inactive_rays_last(T):
     dd = d[order[:n_act]]
     oct_ = (dd[:, 0] < 0).astype(int) | 2 * (dd[:, 1] < 0) | 4 * (dd[:, 2] < 0)
     assert np.all(np.diff(oct_) >= 0)
+
+
+@pytest.mark.parametrize("R", [1, 7, 2047, 2048, 2049, 100003])
+def test_pack_hits_round_trip(T, R):
+    """rt_pack_hits keeps the (t, u, v) of exactly the rays that hit, in ray order (blocks of 2048 rays and
+    partial last blocks), and the ids plus the packed hits rebuild every hit bit for bit."""
+    from cudart_b200 import core
+    rng = np.random.default_rng(R)
+    ids = rng.integers(-1, 5, R).astype(np.int32)
+    ids[rng.random(R) < 0.6] = -1
+    t = rng.uniform(0.0, 10.0, R).astype(np.float32)
+    tmax = rng.uniform(0.0, 10.0, R).astype(np.float32)
+    t[ids < 0] = tmax[ids < 0]
+    uv = rng.uniform(0.0, 1.0, (R, 2)).astype(np.float32)
+    uv[ids < 0] = 0.0
+    h = dict(id=_dev(T, ids), t=_dev(T, t), uv=_dev(T, uv))
+    p = core.pack_hits(h)
+    T.cuda.synchronize()
+    n = int(_host(p["count"])[0])
+    hit = ids >= 0
+    assert n == int(hit.sum())
+    packed = _host(p["packed"])[:3 * n].reshape(n, 3)
+    assert np.array_equal(_u32(packed[:, 0]), _u32(t[hit]))
+    assert np.array_equal(_u32(packed[:, 1:]), _u32(uv[hit]))
+    t2, uv2 = core.unpack_hits(T.from_numpy(ids), T.from_numpy(_host(p["packed"])), n, tmax=T.from_numpy(tmax))
+    assert np.array_equal(_u32(t2.numpy()), _u32(t)) and np.array_equal(_u32(uv2.numpy()), _u32(uv))
+    q = core.pack_hits(h, out=p)  # the same outputs again, in place
+    T.cuda.synchronize()
+    assert int(_host(q["count"])[0]) == n
