@@ -9,8 +9,9 @@
 //     pass (so each pass knows where every digit's run starts);
 //   * per pass, one launch over tiles of 4096 keys (512 threads x 8 keys).
 //     A CTA takes the next tile index from a counter, ranks its keys stably
-//     (__match_any_sync + per-warp counters), publishes its per-digit counts,
-//     and finds how many keys of each digit the earlier tiles hold by reading
+//     (the lanes of equal digit found by one ballot per digit bit, plus
+//     per-warp counters), publishes its per-digit counts, and finds how many
+//     keys of each digit the earlier tiles hold by reading
 //     their published counts backwards until it meets a tile that already
 //     published its inclusive prefix (decoupled look-back, after Merrill and
 //     Adinets, "Onesweep: a faster least significant digit radix sort for
@@ -120,6 +121,19 @@ __global__ __launch_bounds__(256) void k_sort_hist(const uint32_t* __restrict__ 
   }
 }
 
+// The lanes of the warp whose 9-bit digit equals this lane's (digits 0..255, 256 for a lane without a key): one
+// ballot per bit, each lane keeping the lanes that agree with it on that bit -- the mask __match_any_sync gives.
+__device__ __forceinline__ uint32_t match_digit(uint32_t d) {
+  uint32_t m = 0xffffffffu;
+#pragma unroll
+  for (int b = 0; b < 9; ++b) {
+    const bool bit = (d >> b) & 1u;
+    const uint32_t v = __ballot_sync(0xffffffffu, bit);
+    m &= bit ? v : ~v;
+  }
+  return m;
+}
+
 // Optional epilogue of a pass: out[position] = the segment of the value written there (largest m with
 // off[m] <= value, m < count), for a caller that needs each sorted value's segment next.
 struct SegOut {
@@ -171,7 +185,7 @@ __global__ __launch_bounds__(kOsThreads, 3) void k_onesweep(const uint32_t* __re
     key[r] = valid ? __ldg(keys_in + idx) : 0u;
     if (kVals) val[r] = valid ? (vals_in ? __ldg(vals_in + idx) : (uint32_t)idx) : 0u;
     const uint32_t d = valid ? ((key[r] >> shift) & 255u) : (uint32_t)kRadix;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t peers = match_digit(d);
     uint32_t pre = 0;
     if (d < (uint32_t)kRadix) pre = s_cnt[warp][d];
     rank[r] = pre + __popc(peers & lt);
@@ -281,7 +295,7 @@ __global__ __launch_bounds__(kThreads) void k_radix_small(uint32_t* __restrict__
     for (int r = 0; r < kItems; ++r) {
       uint32_t idx = warp * (kItems * 32) + r * 32 + lane;
       uint32_t d = idx < n ? ((kbuf[cur][idx] >> shift) & 255u) : (uint32_t)kRadix;
-      uint32_t peers = __match_any_sync(0xffffffffu, d);
+      uint32_t peers = match_digit(d);
       uint32_t pre = s_cnt[warp][d];
       rank[r] = pre + __popc(peers & lt);
       __syncwarp();
